@@ -1,0 +1,340 @@
+"""Oracle: ctypes binding of the CPU restatement of Rheon's carrier arithmetic.
+
+TEST INFRASTRUCTURE ONLY. Imported by tests/, by ``__graft_entry__.smoke()`` and
+by bench.py's CPU-baseline/reference arm, as the checker and the timed CPU
+baseline. The product package ``rheon_b200`` never imports it.
+
+The C++ source (oracle.cpp) restates, with the reference's operation order and
+serial Neumaier reductions, src/{geometry,sampling,advection,operator,
+pressure}.rs of the Rheon project; see oracle.h for the file:line map.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+
+OK = 0
+UNSUPPORTED = 1
+NONFINITE_OUTPUT = 3
+NONZERO_GAUGE = 4
+QUALITY_GATE = 5
+CANCELLED = 6
+ITERATION_LIMIT = 7
+BREAKDOWN = 8
+INVALID_ARGUMENT = 10
+INCOMPATIBLE_RHS = 11
+NONFINITE_INPUT = 12
+NONZERO_WALL_VELOCITY = 13
+ARITHMETIC_FAILURE = 14
+LENGTH_MISMATCH = 18
+INVALID_GEOMETRY = 19
+INVALID_TIME_STEP = 20
+NONFINITE_POSITION = 21
+
+JACOBI_PCG_V1 = 0
+SGS_PCG_V1 = 1
+
+
+class Grid(C.Structure):
+    _fields_ = [("counts", C.c_uint64 * 3), ("spacing", C.c_double * 3), ("origin", C.c_double * 3)]
+
+
+class Settings(C.Structure):
+    _fields_ = [
+        ("relative_residual", C.c_double),
+        ("absolute_residual", C.c_double),
+        ("divergence_limit", C.c_double),
+        ("max_iterations", C.c_uint64),
+    ]
+
+
+class Report(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_uint64),
+        ("true_residual_l2", C.c_double),
+        ("true_residual_max", C.c_double),
+        ("predicted_divergence_max", C.c_double),
+        ("incompatible_sum", C.c_double),
+        ("incompatible_budget", C.c_double),
+        ("breakdown_iteration", C.c_uint64),
+    ]
+
+
+class Trace(C.Structure):
+    _fields_ = [
+        ("curvature", C.c_double),
+        ("alpha", C.c_double),
+        ("recursive_l2", C.c_double),
+        ("rz", C.c_double),
+        ("beta", C.c_double),
+        ("replaced", C.c_uint32),
+        ("checked", C.c_uint32),
+    ]
+
+
+class StepParams(C.Structure):
+    _fields_ = [
+        ("dt", C.c_double),
+        ("density", C.c_double),
+        ("method", C.c_int),
+        ("settings", Settings),
+        ("buoyancy", C.c_double),
+        ("iteration_limit_ok", C.c_int),
+        ("threads", C.c_int),
+    ]
+
+
+class StepReport(C.Structure):
+    _fields_ = [
+        ("pressure", Report),
+        ("pressure_status", C.c_int),
+        ("actual_divergence_max", C.c_double),
+        ("courant", C.c_double),
+        ("rate_before", C.c_double),
+    ]
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+_P = C.c_void_p
+
+
+def _declare(L):
+    L.orc_grid_validate.argtypes = [C.POINTER(Grid)]
+    L.orc_sample.argtypes = [C.POINTER(Grid), C.c_int, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.orc_backtrace.argtypes = [C.POINTER(Grid), _P, _P, _P, C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double)]
+    L.orc_advect_velocity_f32.argtypes = [C.POINTER(Grid), _P, _P, _P, C.c_double, _P, _P, _P, C.c_int]
+    L.orc_advect_velocity_f64.argtypes = [C.POINTER(Grid), _P, _P, _P, C.c_double, _P, _P, _P, C.c_int]
+    L.orc_advect_tracer_f32.argtypes = [C.POINTER(Grid), _P, _P, _P, _P, C.c_double, _P, C.c_int]
+    L.orc_apply_full.argtypes = [C.POINTER(Grid), C.c_double, _P, _P, C.c_int]
+    L.orc_build_rhs_f32.argtypes = [C.POINTER(Grid), C.c_double, _P, _P, _P, C.c_double, _P]
+    L.orc_build_rhs_f64.argtypes = [C.POINTER(Grid), C.c_double, _P, _P, _P, C.c_double, _P]
+    L.orc_divergence_f32.argtypes = [C.POINTER(Grid), _P, _P, _P, _P]
+    L.orc_divergence_f64.argtypes = [C.POINTER(Grid), _P, _P, _P, _P]
+    L.orc_correct_f32.argtypes = [C.POINTER(Grid), C.c_double, _P, C.c_double, _P, _P, _P]
+    L.orc_correct_f64.argtypes = [C.POINTER(Grid), C.c_double, _P, C.c_double, _P, _P, _P]
+    L.orc_diagonal.argtypes = [C.POINTER(Grid), C.c_double, C.POINTER(C.c_uint64)]
+    L.orc_diagonal.restype = C.c_double
+    L.orc_compensated_sum.argtypes = [_P, C.c_size_t]
+    L.orc_compensated_sum.restype = C.c_double
+    L.orc_dot.argtypes = [_P, _P, C.c_size_t]
+    L.orc_dot.restype = C.c_double
+    L.orc_precondition.argtypes = [C.POINTER(Grid), C.c_double, C.c_int, _P, _P, C.POINTER(C.c_double)]
+    L.orc_solve_rhs.argtypes = [C.POINTER(Grid), C.c_double, C.c_int, _P, C.c_double, C.POINTER(Settings), _P,
+                                C.POINTER(Report), _P, C.c_size_t, C.c_int]
+    L.orc_qualify_pressure.argtypes = [C.POINTER(Grid), C.c_double, _P, C.c_double, C.POINTER(Settings), _P,
+                                       C.POINTER(Report)]
+    L.orc_velocity_rate_f32.argtypes = [C.POINTER(Grid), _P, _P, _P, C.POINTER(C.c_double)]
+    L.orc_velocity_rate_f64.argtypes = [C.POINTER(Grid), _P, _P, _P, C.POINTER(C.c_double)]
+    L.orc_max_abs.argtypes = [_P, C.c_size_t]
+    L.orc_max_abs.restype = C.c_double
+    L.orc_carrier_step_f32.argtypes = [C.POINTER(Grid), C.POINTER(StepParams), _P, _P, _P, _P, C.POINTER(StepReport)]
+    L.orc_carrier_step_f64.argtypes = [C.POINTER(Grid), C.POINTER(StepParams), _P, _P, _P, _P, C.POINTER(StepReport)]
+
+
+def grid(counts, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0)) -> Grid:
+    g = Grid()
+    for d in range(3):
+        g.counts[d] = int(counts[d])
+        g.spacing[d] = float(spacing[d])
+        g.origin[d] = float(origin[d])
+    return g
+
+
+def settings(rel=1e-11, abs_=1e-12, div=1e-9, max_iterations=1000) -> Settings:
+    return Settings(rel, abs_, div, max_iterations)
+
+
+def face_counts(g: Grid, axis: int):
+    n = [int(g.counts[d]) for d in range(3)]
+    n[axis] += 1
+    return n
+
+
+def face_len(g: Grid, axis: int) -> int:
+    f = face_counts(g, axis)
+    return f[0] * f[1] * f[2]
+
+
+def cell_len(g: Grid) -> int:
+    return int(g.counts[0]) * int(g.counts[1]) * int(g.counts[2])
+
+
+def _ptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ------------------------------------------------------------------ wrappers
+def sample(g, axis, values, position):
+    values = _f32(values)
+    pos = (C.c_double * 3)(*position)
+    out = C.c_double()
+    st = lib().orc_sample(C.byref(g), axis, _ptr(values), pos, C.byref(out))
+    return st, out.value
+
+
+def backtrace(g, u, v, w, position, dt):
+    u, v, w = _f32(u), _f32(v), _f32(w)
+    pos = (C.c_double * 3)(*position)
+    out = (C.c_double * 3)()
+    st = lib().orc_backtrace(C.byref(g), _ptr(u), _ptr(v), _ptr(w), pos, dt, out)
+    return st, [out[0], out[1], out[2]]
+
+
+def advect_velocity(g, faces, dt, threads=1):
+    dtype = faces[0].dtype
+    ins = [np.ascontiguousarray(f) for f in faces]
+    outs = [np.zeros_like(f) for f in ins]
+    fn = lib().orc_advect_velocity_f32 if dtype == np.float32 else lib().orc_advect_velocity_f64
+    st = fn(C.byref(g), *[_ptr(a) for a in ins], dt, *[_ptr(a) for a in outs], threads)
+    return st, outs
+
+
+def advect_tracer(g, old, faces, dt, threads=1):
+    old = _f32(old)
+    faces = [_f32(f) for f in faces]
+    out = np.zeros(cell_len(g), np.float32)
+    st = lib().orc_advect_tracer_f32(C.byref(g), _ptr(old), *[_ptr(f) for f in faces], dt, _ptr(out), threads)
+    return st, out
+
+
+def apply_full(g, density, p, threads=1):
+    p = _f64(p)
+    out = np.zeros(cell_len(g), np.float64)
+    st = lib().orc_apply_full(C.byref(g), density, _ptr(p), _ptr(out), threads)
+    return st, out
+
+
+def build_rhs(g, density, faces, dt):
+    out = np.zeros(cell_len(g), np.float64)
+    if faces[0].dtype == np.float32:
+        fs = [_f32(f) for f in faces]
+        st = lib().orc_build_rhs_f32(C.byref(g), density, *[_ptr(f) for f in fs], dt, _ptr(out))
+    else:
+        fs = [_f64(f) for f in faces]
+        st = lib().orc_build_rhs_f64(C.byref(g), density, *[_ptr(f) for f in fs], dt, _ptr(out))
+    return st, out
+
+
+def divergence(g, faces):
+    out = np.zeros(cell_len(g), np.float64)
+    if faces[0].dtype == np.float32:
+        fs = [_f32(f) for f in faces]
+        st = lib().orc_divergence_f32(C.byref(g), *[_ptr(f) for f in fs], _ptr(out))
+    else:
+        fs = [_f64(f) for f in faces]
+        st = lib().orc_divergence_f64(C.byref(g), *[_ptr(f) for f in fs], _ptr(out))
+    return st, out
+
+
+def correct(g, density, p, dt, faces):
+    """Returns (status, corrected copies of faces)."""
+    p = _f64(p)
+    fs = [np.array(f, copy=True, order="C") for f in faces]
+    fn = lib().orc_correct_f32 if fs[0].dtype == np.float32 else lib().orc_correct_f64
+    st = fn(C.byref(g), density, _ptr(p), dt, *[_ptr(f) for f in fs])
+    return st, fs
+
+
+def diagonal(g, density, coordinate):
+    c = (C.c_uint64 * 3)(*coordinate)
+    return lib().orc_diagonal(C.byref(g), density, c)
+
+
+def compensated_sum(values):
+    values = _f64(values)
+    return lib().orc_compensated_sum(_ptr(values), values.size)
+
+
+def dot(a, b):
+    a, b = _f64(a), _f64(b)
+    return lib().orc_dot(_ptr(a), _ptr(b), a.size)
+
+
+def precondition(g, density, method, r):
+    r = np.array(r, dtype=np.float64, copy=True)
+    z = np.zeros_like(r)
+    rz = C.c_double()
+    st = lib().orc_precondition(C.byref(g), density, method, _ptr(r), _ptr(z), C.byref(rz))
+    return st, z, rz.value
+
+
+@dataclass
+class SolveResult:
+    status: int
+    pressure: np.ndarray
+    report: Report
+    trace: list
+
+
+def solve_rhs(g, density, method, rhs, dt, s: Settings, trace=False, threads=1) -> SolveResult:
+    rhs = _f64(rhs)
+    p = np.zeros(cell_len(g), np.float64)
+    rep = Report()
+    cap = int(s.max_iterations) if trace else 0
+    tr = (Trace * max(cap, 1))()
+    st = lib().orc_solve_rhs(C.byref(g), density, method, _ptr(rhs), dt, C.byref(s), _ptr(p), C.byref(rep),
+                             C.cast(tr, C.c_void_p) if cap else None, cap, threads)
+    return SolveResult(st, p, rep, [tr[i] for i in range(cap)] if cap else [])
+
+
+def qualify_pressure(g, density, rhs, dt, s: Settings, pressure):
+    rhs, pressure = _f64(rhs), _f64(pressure)
+    rep = Report()
+    st = lib().orc_qualify_pressure(C.byref(g), density, _ptr(rhs), dt, C.byref(s), _ptr(pressure), C.byref(rep))
+    return st, rep
+
+
+def velocity_rate(g, faces):
+    out = C.c_double()
+    if faces[0].dtype == np.float32:
+        fs = [_f32(f) for f in faces]
+        st = lib().orc_velocity_rate_f32(C.byref(g), *[_ptr(f) for f in fs], C.byref(out))
+    else:
+        fs = [_f64(f) for f in faces]
+        st = lib().orc_velocity_rate_f64(C.byref(g), *[_ptr(f) for f in fs], C.byref(out))
+    return st, out.value
+
+
+def carrier_step(g, faces, params: StepParams, tracer=None):
+    """One carrier step in place on copies; returns (status, faces, tracer, StepReport)."""
+    fs = [np.array(f, copy=True, order="C") for f in faces]
+    tr = None if tracer is None else np.array(tracer, dtype=np.float32, copy=True)
+    rep = StepReport()
+    fn = lib().orc_carrier_step_f32 if fs[0].dtype == np.float32 else lib().orc_carrier_step_f64
+    st = fn(C.byref(g), C.byref(params), *[_ptr(f) for f in fs], _ptr(tr) if tr is not None else None,
+            C.byref(rep))
+    return st, fs, tr, rep

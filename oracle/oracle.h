@@ -1,0 +1,195 @@
+/*
+ * Oracle for the fixed-box carrier step: a CPU restatement of Rheon's Rust
+ * arithmetic for this path. TEST INFRASTRUCTURE ONLY. It is the checker that
+ * the CUDA library is compared against, and the CPU baseline that bench.py
+ * times. Nothing in the product (rheon_b200/, include/) links or calls it.
+ *
+ * Every routine keeps the reference's operation order and its serial
+ * Neumaier-compensated reductions, and is compiled with -ffp-contract=off
+ * (Rust never fuses a multiply and an add). The reference itself is Rust and
+ * cannot be compiled in this image (no cargo/rustc), so parity is pinned by
+ * porting the reference's own known-answer tests onto this restatement.
+ *
+ * Reference files (paths within the Rheon project):
+ *   src/geometry.rs    GridGeometry::new :114-191, cell/face indexing :250-258
+ *   src/sampling.rs    ScalarSampler::sample :74-122, backtrace :151-175
+ *   src/advection.rs   advect_velocity :28-68, advect_tracer :72-102
+ *   src/operator.rs    new :58-97, apply_full :378-456, build_rhs :460-509,
+ *                      divergence :513-568, correct_candidate_in_place :627-668,
+ *                      build_rhs_f64 :672-708, divergence_f64 :711-742,
+ *                      correct_candidate_f64 :746-781, diagonal :813-838
+ *   src/pressure.rs    compensated_sum :135-148, true_report :432-456,
+ *                      precondition_sgs :467-532, precondition_jacobi :534-575,
+ *                      solve_loaded :577-740
+ *   src/solver_provider.rs  ProviderWorkspace::solve_observed :160-327
+ *   src/simulation.rs  velocity_rate :1415-1429, apply_force :1449-1472
+ */
+#ifndef RHEON_B200_ORACLE_H
+#define RHEON_B200_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes share their numeric values with include/rheon_b200.h. */
+enum {
+    ORC_OK = 0,
+    ORC_UNSUPPORTED = 1,
+    ORC_EXECUTION = 2,
+    ORC_NONFINITE_OUTPUT = 3,
+    ORC_NONZERO_GAUGE = 4,
+    ORC_QUALITY_GATE = 5,
+    ORC_CANCELLED = 6,
+    ORC_ITERATION_LIMIT = 7,
+    ORC_BREAKDOWN = 8,
+    ORC_OUT_OF_MEMORY = 9,
+    ORC_INVALID_ARGUMENT = 10,
+    ORC_INCOMPATIBLE_RHS = 11,
+    ORC_NONFINITE_INPUT = 12,
+    ORC_NONZERO_WALL_VELOCITY = 13,
+    ORC_ARITHMETIC_FAILURE = 14,
+    ORC_DIVERGENCE_LIMIT = 15,
+    ORC_COURANT_LIMIT = 16,
+    ORC_LENGTH_MISMATCH = 18,
+    ORC_INVALID_GEOMETRY = 19,
+    ORC_INVALID_TIME_STEP = 20,
+    ORC_NONFINITE_POSITION = 21,
+};
+
+typedef struct orc_grid {
+    uint64_t counts[3];
+    double spacing[3];
+    double origin[3];
+} orc_grid;
+
+typedef struct orc_settings {
+    double relative_residual;
+    double absolute_residual;
+    double divergence_limit;
+    uint64_t max_iterations;
+} orc_settings;
+
+typedef struct orc_report {
+    uint64_t iterations;
+    double true_residual_l2;
+    double true_residual_max;
+    double predicted_divergence_max;
+    /* IncompatibleRhs payload (sum, rounding_budget); Breakdown iteration. */
+    double incompatible_sum;
+    double incompatible_budget;
+    uint64_t breakdown_iteration;
+} orc_report;
+
+/* Per-iteration scalars of the PCG recurrence (for per-iteration parity). */
+typedef struct orc_trace {
+    double curvature;   /* d.Kd                       */
+    double alpha;       /* rz / curvature             */
+    double recursive_l2;/* sqrt(r.r) after the update */
+    double rz;          /* r.z after preconditioning  */
+    double beta;        /* next_rz / rz (0 if replaced)*/
+    uint32_t replaced;  /* 1 when the true residual replaced r */
+    uint32_t checked;   /* 1 when a true residual was evaluated */
+} orc_trace;
+
+enum { ORC_JACOBI_PCG_V1 = 0, ORC_SGS_PCG_V1 = 1 };
+
+int orc_grid_validate(const orc_grid* g);
+
+/* Sampling (sampling.rs). axis 0..2 samples that face field, 3 samples cells. */
+int orc_sample(const orc_grid* g, int axis, const float* values, const double position[3],
+               double* out);
+int orc_backtrace(const orc_grid* g, const float* u, const float* v, const float* w,
+                  const double position[3], double dt, double out[3]);
+
+/* Advection (advection.rs). f32 storage is the reference; f64 storage keeps
+ * the same formulas with the `as f32` casts removed. */
+int orc_advect_velocity_f32(const orc_grid* g, const float* u, const float* v, const float* w,
+                            double dt, float* ou, float* ov, float* ow, int threads);
+int orc_advect_velocity_f64(const orc_grid* g, const double* u, const double* v, const double* w,
+                            double dt, double* ou, double* ov, double* ow, int threads);
+int orc_advect_tracer_f32(const orc_grid* g, const float* old, const float* u, const float* v,
+                          const float* w, double dt, float* out, int threads);
+
+/* Operator (operator.rs). */
+int orc_apply_full(const orc_grid* g, double density, const double* p, double* out, int threads);
+int orc_build_rhs_f32(const orc_grid* g, double density, const float* u, const float* v,
+                      const float* w, double dt, double* out);
+int orc_build_rhs_f64(const orc_grid* g, double density, const double* u, const double* v,
+                      const double* w, double dt, double* out);
+int orc_divergence_f32(const orc_grid* g, const float* u, const float* v, const float* w,
+                       double* out);
+int orc_divergence_f64(const orc_grid* g, const double* u, const double* v, const double* w,
+                       double* out);
+int orc_correct_f32(const orc_grid* g, double density, const double* p, double dt, float* u,
+                    float* v, float* w);
+int orc_correct_f64(const orc_grid* g, double density, const double* p, double dt, double* u,
+                    double* v, double* w);
+double orc_diagonal(const orc_grid* g, double density, const uint64_t coordinate[3]);
+
+/* Reductions (pressure.rs). */
+double orc_compensated_sum(const double* values, size_t n);
+double orc_dot(const double* a, const double* b, size_t n);
+
+/* Preconditioners on a residual r (r[0] is zeroed); z receives M^-1 r.
+ * Returns r.z through *rz. */
+int orc_precondition(const orc_grid* g, double density, int method, double* r, double* z,
+                     double* rz);
+
+/* PressureWorkspace::solve_rhs. pressure_out holds the iterate on every exit
+ * that reaches the loop (including ITERATION_LIMIT). trace (optional) gets one
+ * entry per iteration, up to trace_capacity. */
+int orc_solve_rhs(const orc_grid* g, double density, int method, const double* rhs, double dt,
+                  const orc_settings* s, double* pressure_out, orc_report* report,
+                  orc_trace* trace, size_t trace_capacity, int threads);
+
+/* ProviderWorkspace host qualification of a supplied pressure candidate.
+ * Returns ORC_OK, ORC_NONFINITE_OUTPUT, ORC_NONZERO_GAUGE or ORC_QUALITY_GATE;
+ * the recomputed diagnostics go to *report either way. */
+int orc_qualify_pressure(const orc_grid* g, double density, const double* rhs, double dt,
+                         const orc_settings* s, const double* pressure, orc_report* report);
+
+/* simulation.rs helpers. */
+int orc_velocity_rate_f32(const orc_grid* g, const float* u, const float* v, const float* w,
+                          double* rate);
+int orc_velocity_rate_f64(const orc_grid* g, const double* u, const double* v, const double* w,
+                          double* rate);
+double orc_max_abs(const double* values, size_t n);
+
+/* One carrier step on f32 or f64 faces, composed from the public primitives
+ * exactly as Rheon's step owner orders them: advect -> (optional Y-face
+ * buoyancy from the tracer) -> build_rhs -> PCG -> correct -> actual divergence
+ * -> Courant -> tracer advection with the corrected velocity.
+ * faces[0..2] hold the accepted velocity on entry and the corrected candidate on
+ * exit (also on failure, as scratch). tracer may be NULL.
+ * If iteration_limit_ok is nonzero, an IterationLimit from the PCG still
+ * proceeds to the correction with the iterate (exact-iteration-count mode). */
+typedef struct orc_step_params {
+    double dt;
+    double density;
+    int method;
+    orc_settings settings;
+    double buoyancy;          /* g_b; 0 disables the buoyancy hook */
+    int iteration_limit_ok;
+    int threads;
+} orc_step_params;
+
+typedef struct orc_step_report {
+    orc_report pressure;
+    int pressure_status;
+    double actual_divergence_max;
+    double courant;
+    double rate_before;
+} orc_step_report;
+
+int orc_carrier_step_f32(const orc_grid* g, const orc_step_params* prm, float* u, float* v,
+                         float* w, float* tracer, orc_step_report* rep);
+int orc_carrier_step_f64(const orc_grid* g, const orc_step_params* prm, double* u, double* v,
+                         double* w, float* tracer, orc_step_report* rep);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
