@@ -1,0 +1,312 @@
+/*
+ * rheon_b200 — C ABI of the B200 (sm_100a) fixed-box carrier step.
+ *
+ * Plain pointers and sizes only. Host pointers are borrowed for the duration
+ * of a call; device pointers (the *_device entry points) must be CUDA device
+ * allocations on the handle's device. Every handle owns one CUDA stream and is
+ * not thread-safe: one caller thread at a time, as Rheon's `&mut self` traits.
+ *
+ * Reference interfaces replaced (paths within the Rheon project):
+ *   PressureProvider trait ............ src/solver_provider.rs:67-76
+ *   PressureRequest ................... src/solver_provider.rs:47-52
+ *   ProviderRejection ................. src/solver_provider.rs:55-62
+ *   PressureWorkspace::solve_rhs ...... src/pressure.rs:365-393
+ *   PressureWorkspace::solve_velocity . src/pressure.rs:344-361
+ *   PressureSettings / PressureReport . src/pressure.rs:34-49
+ *   PressureError ..................... src/pressure.rs:52-77
+ *   PressureOperator primitives ....... src/operator.rs:378-781
+ *   advect_velocity / advect_tracer ... src/advection.rs:28-102
+ *   Simulation step owner (composed) .. src/simulation.rs:812-1403
+ */
+#ifndef RHEON_B200_H
+#define RHEON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RB200_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define RB200_API __attribute__((visibility("default")))
+#else
+#define RB200_API
+#endif
+
+/* Status codes. 1-6 map one to one onto ProviderRejection
+ * (src/solver_provider.rs:55-62); 7-11 onto PressureError
+ * (src/pressure.rs:52-77); 12-16 onto OperatorError / SimulationError gates. */
+typedef enum rb200_status {
+    RB200_OK = 0,
+    RB200_UNSUPPORTED = 1,           /* ProviderRejection::Unsupported            */
+    RB200_EXECUTION = 2,             /* ProviderRejection::Execution (CUDA error) */
+    RB200_NONFINITE_OUTPUT = 3,      /* ProviderRejection::NonFiniteOutput        */
+    RB200_NONZERO_GAUGE = 4,         /* ProviderRejection::NonZeroGauge           */
+    RB200_QUALITY_GATE = 5,          /* ProviderRejection::QualityGate            */
+    RB200_CANCELLED = 6,             /* ProviderRejection::Cancelled              */
+    RB200_ITERATION_LIMIT = 7,       /* PressureError::IterationLimit             */
+    RB200_BREAKDOWN = 8,             /* PressureError::Breakdown                  */
+    RB200_OUT_OF_MEMORY = 9,         /* PressureError::AllocationFailed/BufferLimit */
+    RB200_INVALID_ARGUMENT = 10,     /* PressureError::InvalidSettings, bad dt... */
+    RB200_INCOMPATIBLE_RHS = 11,     /* PressureError::IncompatibleRhs            */
+    RB200_NONFINITE_INPUT = 12,      /* OperatorError::NonFiniteInput             */
+    RB200_NONZERO_WALL_VELOCITY = 13,/* OperatorError::NonZeroWallVelocity        */
+    RB200_ARITHMETIC_FAILURE = 14,   /* OperatorError::ArithmeticFailure          */
+    RB200_DIVERGENCE_LIMIT = 15,     /* SimulationError::DivergenceLimit          */
+    RB200_COURANT_LIMIT = 16,        /* SimulationError::CourantLimit             */
+    RB200_NO_DEVICE = 17,            /* no usable sm_100 device                   */
+    RB200_LENGTH_MISMATCH = 18       /* OperatorError::LengthMismatch             */
+} rb200_status;
+
+/* Pressure methods. JACOBI_PCG_V1 reproduces "jacobi-pcg-v1"
+ * (src/pressure.rs:7-29). SGS_PCG_V1 reproduces the exact lexicographic
+ * "sgs-pcg-v1" sweep order. RBSGS_PCG is the device-native red-black symmetric
+ * Gauss-Seidel preconditioner (new). MG_MIXED is flexible CG with an FP32
+ * geometric multigrid V(2,2) preconditioner, FP64 residual/accumulation and an
+ * FP64 coarse solve (new). */
+typedef enum rb200_method {
+    RB200_JACOBI_PCG_V1 = 0,
+    RB200_SGS_PCG_V1 = 1,
+    RB200_RBSGS_PCG = 2,
+    RB200_MG_MIXED = 3
+} rb200_method;
+
+/* Face storage of the resident carrier state. F32 is Rheon's own storage
+ * (src/simulation.rs:167-172); F64 keeps the same formulas without the casts. */
+typedef enum rb200_storage { RB200_FACES_F32 = 0, RB200_FACES_F64 = 1 } rb200_storage;
+
+/* GridGeometry::new(counts, spacing, origin) (src/geometry.rs:114). */
+typedef struct rb200_grid {
+    uint64_t counts[3];
+    double spacing[3];
+    double origin[3];
+} rb200_grid;
+
+/* PressureSettings (src/pressure.rs:34-39). */
+typedef struct rb200_settings {
+    double relative_residual;
+    double absolute_residual;
+    double divergence_limit;
+    uint64_t max_iterations;
+} rb200_settings;
+
+/* PressureReport (src/pressure.rs:44-49) plus the typed-error payloads. */
+typedef struct rb200_report {
+    uint64_t iterations;
+    double true_residual_l2;
+    double true_residual_max;
+    double predicted_divergence_max;
+    double incompatible_sum;      /* IncompatibleRhs { sum, .. }             */
+    double incompatible_budget;   /* IncompatibleRhs { .., rounding_budget } */
+    uint64_t breakdown_iteration; /* Breakdown { iteration }                 */
+} rb200_report;
+
+/* One PCG iteration's scalars (diagnostics / per-iteration parity). */
+typedef struct rb200_trace {
+    double curvature;
+    double alpha;
+    double recursive_l2;
+    double rz;
+    double beta;
+    uint32_t replaced;
+    uint32_t checked;
+} rb200_trace;
+
+/* Cancellation predicate, polled on the caller thread between device chunks.
+ * Nonzero return cancels (never falls back), as `cancelled: &mut dyn FnMut()
+ * -> bool` in src/solver_provider.rs:70-75. */
+typedef int (*rb200_cancel_fn)(void* ctx);
+
+/* ------------------------------------------------------------------ library */
+RB200_API int rb200_abi_version(void);
+/* Static message for a status code. */
+RB200_API const char* rb200_status_string(int status);
+/* Number of visible sm_100 devices (0 when none). */
+RB200_API int rb200_device_count(void);
+
+/* ------------------------------------------------- PressureProvider drop-in
+ * rb200_provider_* are the four trait methods of PressureProvider
+ * (src/solver_provider.rs:67-76) over the C ABI. */
+typedef struct rb200_provider rb200_provider;
+
+typedef struct rb200_provider_config {
+    rb200_grid grid;          /* the only grid this provider accepts        */
+    double density;           /* sealed-box density                         */
+    int method;               /* rb200_method                               */
+    rb200_settings settings;  /* stopping rule used inside predict()        */
+    int device;               /* CUDA ordinal                               */
+} rb200_provider_config;
+
+/* PressureRequest (src/solver_provider.rs:47-52): RHS of the full, ungauged
+ * integrated operator, x-fastest, m^3/s^2. */
+typedef struct rb200_request {
+    rb200_grid grid;
+    double density;
+    double dt;
+    const double* rhs;
+    size_t len;
+} rb200_request;
+
+/* SolverMetadata (src/solver_provider.rs:18-33), as static strings. */
+typedef struct rb200_metadata {
+    const char* id;
+    const char* version;
+    const char* stage;
+    const char* input_layout;
+    const char* input_scalar;
+    const char* input_units;
+    const char* output_layout;
+    const char* output_scalar;
+    const char* output_units;
+    const char* domain;
+    uint64_t shape_xyz[3];
+} rb200_metadata;
+
+/* Allocates every device buffer for the grid; predict() allocates nothing. */
+RB200_API int rb200_provider_create(const rb200_provider_config* config, rb200_provider** out);
+RB200_API void rb200_provider_destroy(rb200_provider* provider);
+/* PressureProvider::metadata */
+RB200_API int rb200_provider_metadata(const rb200_provider* provider, rb200_metadata* out);
+/* PressureProvider::supports: RB200_OK or RB200_UNSUPPORTED. */
+RB200_API int rb200_provider_supports(const rb200_provider* provider, const rb200_request* request);
+/* PressureProvider::predict: writes all len cells of pressure (p[0] == 0).
+ * Returns RB200_OK, RB200_UNSUPPORTED, RB200_EXECUTION, RB200_CANCELLED or
+ * RB200_NONFINITE_OUTPUT; an unconverged solve (iteration limit, breakdown,
+ * incompatible RHS) is RB200_EXECUTION with the detail in last_error and
+ * last_report. The caller re-qualifies the output, as Rheon does. */
+RB200_API int rb200_provider_predict(rb200_provider* provider, const rb200_request* request, double* pressure,
+                           size_t len, rb200_cancel_fn cancelled, void* ctx);
+RB200_API const char* rb200_provider_last_error(const rb200_provider* provider);
+RB200_API int rb200_provider_last_report(const rb200_provider* provider, rb200_report* out, int* solve_status);
+
+/* -------------------------------------------------- PressureWorkspace mirror */
+typedef struct rb200_workspace rb200_workspace;
+
+/* PressureWorkspace::with_implementation(grid, limit, implementation)
+ * (src/pressure.rs:265-314). memory_limit bounds the device bytes. */
+RB200_API int rb200_workspace_create(const rb200_grid* grid, double density, int method,
+                           uint64_t memory_limit, int device, rb200_workspace** out);
+RB200_API void rb200_workspace_destroy(rb200_workspace* ws);
+RB200_API uint64_t rb200_workspace_allocated_bytes(const rb200_workspace* ws);
+/* Opaque cudaStream_t of the workspace. */
+RB200_API void* rb200_workspace_stream(rb200_workspace* ws);
+/* PressureWorkspace::solve_rhs on host buffers. On RB200_ITERATION_LIMIT the
+ * iterate stays readable through rb200_workspace_pressure, as in Rheon. */
+RB200_API int rb200_workspace_solve_rhs(rb200_workspace* ws, const double* rhs, size_t len, double dt,
+                              const rb200_settings* settings, rb200_report* report,
+                              rb200_cancel_fn cancelled, void* ctx);
+/* Same on a device-resident RHS (len doubles on the workspace's device). The
+ * workspace works on its own stream: the RHS must be complete when called. */
+RB200_API int rb200_workspace_solve_rhs_device(rb200_workspace* ws, const double* rhs_device, size_t len,
+                                     double dt, const rb200_settings* settings,
+                                     rb200_report* report, rb200_cancel_fn cancelled, void* ctx);
+/* Last pressure to host / device memory. */
+RB200_API int rb200_workspace_pressure(rb200_workspace* ws, double* out, size_t len);
+RB200_API const double* rb200_workspace_pressure_device(rb200_workspace* ws);
+/* Per-iteration scalars of the next solves (NULL disables). trace points to
+ * capacity rb200_trace records in host memory, filled at the end of a solve. */
+RB200_API int rb200_workspace_set_trace(rb200_workspace* ws, rb200_trace* trace, size_t capacity);
+/* Diagnostics: average device milliseconds of one PCG pass (which = 0: the
+ * fused direction update + operator + curvature pass, 1: the fused update +
+ * preconditioner + dots pass), over `launches` back-to-back launches timed with
+ * CUDA events on the handle's stream, on the current vectors. Leaves the
+ * solver's scalars in a timing state; the next solve resets them. */
+RB200_API int rb200_workspace_profile(rb200_workspace* ws, int which, int launches, double* avg_ms);
+
+/* ----------------------------------------- PressureOperator device primitives
+ * All pointers are device pointers; `stream` is a cudaStream_t (NULL = legacy).
+ * These validate like the reference (walls, finiteness) and return its errors. */
+RB200_API int rb200_apply_full_device(const rb200_grid* grid, double density, const double* pressure,
+                            double* out, void* stream);
+RB200_API int rb200_build_rhs_f32_device(const rb200_grid* grid, double density, const float* u,
+                               const float* v, const float* w, double dt, double* rhs,
+                               void* stream);
+RB200_API int rb200_build_rhs_f64_device(const rb200_grid* grid, double density, const double* u,
+                               const double* v, const double* w, double dt, double* rhs,
+                               void* stream);
+RB200_API int rb200_divergence_f32_device(const rb200_grid* grid, const float* u, const float* v,
+                                const float* w, double* out, void* stream);
+RB200_API int rb200_divergence_f64_device(const rb200_grid* grid, const double* u, const double* v,
+                                const double* w, double* out, void* stream);
+RB200_API int rb200_correct_f32_device(const rb200_grid* grid, double density, const double* pressure,
+                             double dt, float* u, float* v, float* w, void* stream);
+RB200_API int rb200_correct_f64_device(const rb200_grid* grid, double density, const double* pressure,
+                             double dt, double* u, double* v, double* w, void* stream);
+RB200_API int rb200_advect_velocity_f32_device(const rb200_grid* grid, const float* u, const float* v,
+                                     const float* w, double dt, float* out_u, float* out_v,
+                                     float* out_w, void* stream);
+RB200_API int rb200_advect_velocity_f64_device(const rb200_grid* grid, const double* u, const double* v,
+                                     const double* w, double dt, double* out_u, double* out_v,
+                                     double* out_w, void* stream);
+RB200_API int rb200_advect_tracer_f32_device(const rb200_grid* grid, const float* old, const float* u,
+                                   const float* v, const float* w, double dt, float* out,
+                                   void* stream);
+
+/* ---------------------------------------------- resident carrier step owner
+ * Device-resident accepted state, composed as Rheon's step owner orders it
+ * (src/simulation.rs:812-1403): dt policy -> advect_velocity -> optional
+ * buoyancy -> build_rhs -> PCG -> correct_candidate -> actual divergence gate
+ * -> Courant gate -> advect_tracer -> commit. A failed step leaves the
+ * accepted state untouched (transactional, src/simulation.rs:805-811). */
+typedef struct rb200_carrier rb200_carrier;
+
+typedef struct rb200_carrier_config {
+    rb200_grid grid;
+    double density;
+    int storage;                   /* rb200_storage                        */
+    int method;                    /* rb200_method                         */
+    rb200_settings settings;
+    double actual_divergence_limit;/* SimulationConfig (simulation.rs:11)  */
+    double max_courant;
+    int with_tracer;               /* allocate a cell tracer (f32)         */
+    int device;
+} rb200_carrier_config;
+
+typedef struct rb200_step_params {
+    double requested_dt;   /* upper bound on dt                              */
+    double cfl;            /* dt <= cfl / velocity_rate when > 0 (0 = off)   */
+    double buoyancy;       /* g_b on Y faces from the tracer (0 = off)       */
+    int iteration_limit_ok;/* accept an exact-iteration-count solve          */
+    int skip_gates;        /* do not reject on divergence/Courant gates      */
+} rb200_step_params;
+
+/* StepReport (src/simulation.rs:44-53) subset plus solver diagnostics. */
+typedef struct rb200_step_report {
+    double dt;
+    double time;
+    uint64_t generation;
+    rb200_report pressure;
+    int pressure_status;
+    double actual_divergence_max;
+    double courant;
+    double velocity_rate;
+    double pressure_ms;    /* device time of the pressure solve (CUDA events) */
+    uint64_t kernel_launches; /* kernels this step launched (graph nodes included) */
+} rb200_step_report;
+
+RB200_API int rb200_carrier_create(const rb200_carrier_config* config, rb200_carrier** out);
+RB200_API void rb200_carrier_destroy(rb200_carrier* carrier);
+RB200_API uint64_t rb200_carrier_allocated_bytes(const rb200_carrier* carrier);
+RB200_API void* rb200_carrier_stream(rb200_carrier* carrier);
+/* Host faces in the configured storage type (float* or double*); tracer may be
+ * NULL. Validates the fixed-box wall contract. */
+RB200_API int rb200_carrier_upload(rb200_carrier* carrier, const void* u, const void* v, const void* w,
+                         const float* tracer);
+RB200_API int rb200_carrier_download(rb200_carrier* carrier, void* u, void* v, void* w, float* tracer);
+/* Device pointers of the accepted state (valid until the next step). */
+RB200_API int rb200_carrier_state_device(rb200_carrier* carrier, void** u, void** v, void** w,
+                               float** tracer);
+RB200_API int rb200_carrier_step(rb200_carrier* carrier, const rb200_step_params* params,
+                       rb200_step_report* report, rb200_cancel_fn cancelled, void* ctx);
+/* rb200_workspace_profile on the carrier's pressure solver. */
+RB200_API int rb200_carrier_profile(rb200_carrier* carrier, int which, int launches, double* avg_ms);
+/* Last pressure of the carrier (host copy). */
+RB200_API int rb200_carrier_pressure(rb200_carrier* carrier, double* out, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,166 @@
+"""ctypes declarations for librheon_b200.so (the C ABI of include/rheon_b200.h).
+
+There is no fallback: importing the package on a machine without the built
+library raises ImportError, and every compute call goes to the CUDA library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librheon_b200.so")
+
+OK = 0
+UNSUPPORTED = 1
+EXECUTION = 2
+NONFINITE_OUTPUT = 3
+NONZERO_GAUGE = 4
+QUALITY_GATE = 5
+CANCELLED = 6
+ITERATION_LIMIT = 7
+BREAKDOWN = 8
+OUT_OF_MEMORY = 9
+INVALID_ARGUMENT = 10
+INCOMPATIBLE_RHS = 11
+NONFINITE_INPUT = 12
+NONZERO_WALL_VELOCITY = 13
+ARITHMETIC_FAILURE = 14
+DIVERGENCE_LIMIT = 15
+COURANT_LIMIT = 16
+NO_DEVICE = 17
+LENGTH_MISMATCH = 18
+
+STATUS_NAMES = {
+    0: "Ok", 1: "Unsupported", 2: "Execution", 3: "NonFiniteOutput", 4: "NonZeroGauge", 5: "QualityGate",
+    6: "Cancelled", 7: "IterationLimit", 8: "Breakdown", 9: "AllocationFailed", 10: "InvalidArgument",
+    11: "IncompatibleRhs", 12: "NonFiniteInput", 13: "NonZeroWallVelocity", 14: "ArithmeticFailure",
+    15: "DivergenceLimit", 16: "CourantLimit", 17: "NoDevice", 18: "LengthMismatch",
+}
+
+
+class Grid(C.Structure):
+    _fields_ = [("counts", C.c_uint64 * 3), ("spacing", C.c_double * 3), ("origin", C.c_double * 3)]
+
+
+class Settings(C.Structure):
+    _fields_ = [("relative_residual", C.c_double), ("absolute_residual", C.c_double),
+                ("divergence_limit", C.c_double), ("max_iterations", C.c_uint64)]
+
+
+class Report(C.Structure):
+    _fields_ = [("iterations", C.c_uint64), ("true_residual_l2", C.c_double), ("true_residual_max", C.c_double),
+                ("predicted_divergence_max", C.c_double), ("incompatible_sum", C.c_double),
+                ("incompatible_budget", C.c_double), ("breakdown_iteration", C.c_uint64)]
+
+
+class Trace(C.Structure):
+    _fields_ = [("curvature", C.c_double), ("alpha", C.c_double), ("recursive_l2", C.c_double),
+                ("rz", C.c_double), ("beta", C.c_double), ("replaced", C.c_uint32), ("checked", C.c_uint32)]
+
+
+class ProviderConfig(C.Structure):
+    _fields_ = [("grid", Grid), ("density", C.c_double), ("method", C.c_int), ("settings", Settings),
+                ("device", C.c_int)]
+
+
+class Request(C.Structure):
+    _fields_ = [("grid", Grid), ("density", C.c_double), ("dt", C.c_double), ("rhs", C.c_void_p),
+                ("len", C.c_size_t)]
+
+
+class Metadata(C.Structure):
+    _fields_ = [(n, C.c_char_p) for n in ("id", "version", "stage", "input_layout", "input_scalar", "input_units",
+                                          "output_layout", "output_scalar", "output_units", "domain")] + [
+        ("shape_xyz", C.c_uint64 * 3)]
+
+
+class CarrierConfig(C.Structure):
+    _fields_ = [("grid", Grid), ("density", C.c_double), ("storage", C.c_int), ("method", C.c_int),
+                ("settings", Settings), ("actual_divergence_limit", C.c_double), ("max_courant", C.c_double),
+                ("with_tracer", C.c_int), ("device", C.c_int)]
+
+
+class StepParams(C.Structure):
+    _fields_ = [("requested_dt", C.c_double), ("cfl", C.c_double), ("buoyancy", C.c_double),
+                ("iteration_limit_ok", C.c_int), ("skip_gates", C.c_int)]
+
+
+class StepReport(C.Structure):
+    _fields_ = [("dt", C.c_double), ("time", C.c_double), ("generation", C.c_uint64), ("pressure", Report),
+                ("pressure_status", C.c_int), ("actual_divergence_max", C.c_double), ("courant", C.c_double),
+                ("velocity_rate", C.c_double), ("pressure_ms", C.c_double),
+                ("kernel_launches", C.c_uint64)]
+
+
+CANCEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
+
+_P = C.c_void_p
+_I = C.c_int
+_D = C.c_double
+_S = C.c_size_t
+
+# name -> (restype, argtypes); every symbol here is declared in include/rheon_b200.h
+SIGNATURES = {
+    "rb200_abi_version": (_I, []),
+    "rb200_status_string": (C.c_char_p, [_I]),
+    "rb200_device_count": (_I, []),
+    "rb200_provider_create": (_I, [C.POINTER(ProviderConfig), C.POINTER(_P)]),
+    "rb200_provider_destroy": (None, [_P]),
+    "rb200_provider_metadata": (_I, [_P, C.POINTER(Metadata)]),
+    "rb200_provider_supports": (_I, [_P, C.POINTER(Request)]),
+    "rb200_provider_predict": (_I, [_P, C.POINTER(Request), _P, _S, CANCEL_FN, _P]),
+    "rb200_provider_last_error": (C.c_char_p, [_P]),
+    "rb200_provider_last_report": (_I, [_P, C.POINTER(Report), C.POINTER(_I)]),
+    "rb200_workspace_create": (_I, [C.POINTER(Grid), _D, _I, C.c_uint64, _I, C.POINTER(_P)]),
+    "rb200_workspace_destroy": (None, [_P]),
+    "rb200_workspace_allocated_bytes": (C.c_uint64, [_P]),
+    "rb200_workspace_stream": (_P, [_P]),
+    "rb200_workspace_solve_rhs": (_I, [_P, _P, _S, _D, C.POINTER(Settings), C.POINTER(Report), CANCEL_FN, _P]),
+    "rb200_workspace_solve_rhs_device": (_I, [_P, _P, _S, _D, C.POINTER(Settings), C.POINTER(Report), CANCEL_FN,
+                                              _P]),
+    "rb200_workspace_pressure": (_I, [_P, _P, _S]),
+    "rb200_workspace_pressure_device": (_P, [_P]),
+    "rb200_workspace_set_trace": (_I, [_P, _P, _S]),
+    "rb200_workspace_profile": (_I, [_P, _I, _I, C.POINTER(_D)]),
+    "rb200_apply_full_device": (_I, [C.POINTER(Grid), _D, _P, _P, _P]),
+    "rb200_build_rhs_f32_device": (_I, [C.POINTER(Grid), _D, _P, _P, _P, _D, _P, _P]),
+    "rb200_build_rhs_f64_device": (_I, [C.POINTER(Grid), _D, _P, _P, _P, _D, _P, _P]),
+    "rb200_divergence_f32_device": (_I, [C.POINTER(Grid), _P, _P, _P, _P, _P]),
+    "rb200_divergence_f64_device": (_I, [C.POINTER(Grid), _P, _P, _P, _P, _P]),
+    "rb200_correct_f32_device": (_I, [C.POINTER(Grid), _D, _P, _D, _P, _P, _P, _P]),
+    "rb200_correct_f64_device": (_I, [C.POINTER(Grid), _D, _P, _D, _P, _P, _P, _P]),
+    "rb200_advect_velocity_f32_device": (_I, [C.POINTER(Grid), _P, _P, _P, _D, _P, _P, _P, _P]),
+    "rb200_advect_velocity_f64_device": (_I, [C.POINTER(Grid), _P, _P, _P, _D, _P, _P, _P, _P]),
+    "rb200_advect_tracer_f32_device": (_I, [C.POINTER(Grid), _P, _P, _P, _P, _D, _P, _P]),
+    "rb200_carrier_create": (_I, [C.POINTER(CarrierConfig), C.POINTER(_P)]),
+    "rb200_carrier_destroy": (None, [_P]),
+    "rb200_carrier_allocated_bytes": (C.c_uint64, [_P]),
+    "rb200_carrier_stream": (_P, [_P]),
+    "rb200_carrier_upload": (_I, [_P, _P, _P, _P, _P]),
+    "rb200_carrier_download": (_I, [_P, _P, _P, _P, _P]),
+    "rb200_carrier_state_device": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
+    "rb200_carrier_step": (_I, [_P, C.POINTER(StepParams), C.POINTER(StepReport), CANCEL_FN, _P]),
+    "rb200_carrier_profile": (_I, [_P, _I, _I, C.POINTER(_D)]),
+    "rb200_carrier_pressure": (_I, [_P, _P, _S]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load librheon_b200.so; raise if it is not built (no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run `python -m rheon_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+NO_CANCEL = CANCEL_FN()

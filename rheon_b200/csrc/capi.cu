@@ -1,0 +1,736 @@
+// extern "C" entry points of librheon_b200 (declared in include/rheon_b200.h).
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "internal.hpp"
+#include "pcg.hpp"
+
+namespace rb200 {
+
+static thread_local std::string g_error;
+void set_error(const std::string& msg) { g_error = msg; }
+const char* get_error() { return g_error.c_str(); }
+
+int launch_check_finite(const double* x, int n, int* flags, cudaStream_t s);
+
+}  // namespace rb200
+
+using namespace rb200;
+
+namespace {
+
+int select_device(int device) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        set_error("no CUDA device");
+        return RB200_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) {
+        set_error("device ordinal out of range");
+        return RB200_INVALID_ARGUMENT;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return RB200_NO_DEVICE;
+    if (prop.major != 10) {
+        set_error("librheon_b200 is built for sm_100a (B200) only");
+        return RB200_NO_DEVICE;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return RB200_NO_DEVICE;
+    return RB200_OK;
+}
+
+// Flags word for the stream-ordered primitive entry points.
+struct FlagsScope {
+    int* d = nullptr;
+    cudaStream_t s;
+    explicit FlagsScope(cudaStream_t stream) : s(stream) {}
+    int open() {
+        RB200_CUDA(cudaMallocAsync(&d, sizeof(int), s));
+        RB200_CUDA(cudaMemsetAsync(d, 0, sizeof(int), s));
+        return RB200_OK;
+    }
+    int close(int* out) {
+        int h = 0;
+        RB200_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, s));
+        RB200_CUDA(cudaFreeAsync(d, s));
+        d = nullptr;
+        RB200_CUDA(cudaStreamSynchronize(s));
+        *out = h;
+        return RB200_OK;
+    }
+    ~FlagsScope() {
+        if (d) cudaFreeAsync(d, s);
+    }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------- handles
+struct rb200_workspace {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    GridDev g{};
+    rb200_grid grid{};
+    int method = 0;
+    uint64_t limit = 0;
+    PcgSolver solver;
+    std::string err;
+    ~rb200_workspace() {
+        if (stream) {
+            cudaSetDevice(device);
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
+    }
+};
+
+struct rb200_provider {
+    rb200_provider_config cfg{};
+    rb200_workspace* ws = nullptr;
+    std::string err;
+    rb200_report last{};
+    int last_status = RB200_OK;
+    ~rb200_provider() { delete ws; }
+};
+
+struct rb200_carrier {
+    rb200_carrier_config cfg{};
+    GridDev g{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    size_t elem = 4;
+    void* faces[3][3] = {};  // [buffer][axis]
+    int acc = 0;             // accepted buffer
+    float* tracer[2] = {nullptr, nullptr};
+    int tacc = 0;
+    PcgSolver solver;
+    double* d_scalars = nullptr;
+    double* h_scalars = nullptr;
+    int* d_flags = nullptr;
+    int* h_flags = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    double time = 0.0;
+    uint64_t generation = 0;
+    double rate = 0.0;
+    size_t bytes = 0;
+    std::string err;
+    ~rb200_carrier() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& b : faces)
+            for (auto& a : b) cudaFree(a);
+        cudaFree(tracer[0]);
+        cudaFree(tracer[1]);
+        cudaFree(d_scalars);
+        cudaFree(d_flags);
+        if (h_scalars) cudaFreeHost(h_scalars);
+        if (h_flags) cudaFreeHost(h_flags);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+#define RB200_PRIM_BEGIN(grid, density)                 \
+    GridDev g;                                          \
+    int rc = make_grid_dev(grid, density, &g);          \
+    if (rc) return rc;                                  \
+    cudaStream_t s = (cudaStream_t)stream;              \
+    FlagsScope fl(s);                                   \
+    if ((rc = fl.open())) return rc;
+
+static int flags_status(int flags, bool walls_matter) {
+    if (flags & VF_NONFINITE) return RB200_NONFINITE_INPUT;
+    if (walls_matter && (flags & VF_WALL)) return RB200_NONZERO_WALL_VELOCITY;
+    if (flags & (VF_ARITH | VF_F32_RANGE)) return RB200_ARITHMETIC_FAILURE;
+    return RB200_OK;
+}
+
+template <class T>
+static int build_rhs_prim(const rb200_grid* grid, double density, const T* u, const T* v, const T* w, double dt,
+                          double* rhs, void* stream) {
+    if (!std::isfinite(dt) || dt <= 0.0) return RB200_INVALID_ARGUMENT;
+    RB200_PRIM_BEGIN(grid, density)
+    if ((rc = launch_validate_faces<T>(g, u, v, w, fl.d, s))) return rc;
+    if ((rc = launch_build_rhs<T>(g, u, v, w, dt, rhs, fl.d, s))) return rc;
+    int f = 0;
+    if ((rc = fl.close(&f))) return rc;
+    return flags_status(f, true);
+}
+
+template <class T>
+static int divergence_prim(const rb200_grid* grid, const T* u, const T* v, const T* w, double* out, void* stream) {
+    RB200_PRIM_BEGIN(grid, 1.0)
+    if ((rc = launch_validate_faces<T>(g, u, v, w, fl.d, s))) return rc;
+    if ((rc = launch_divergence<T>(g, u, v, w, out, fl.d, s))) return rc;
+    int f = 0;
+    if ((rc = fl.close(&f))) return rc;
+    return flags_status(f, true);
+}
+
+template <class T>
+static int correct_prim(const rb200_grid* grid, double density, const double* p, double dt, T* u, T* v, T* w,
+                        void* stream) {
+    if (!std::isfinite(dt) || dt <= 0.0) return RB200_INVALID_ARGUMENT;
+    RB200_PRIM_BEGIN(grid, density)
+    if ((rc = launch_validate_faces<T>(g, u, v, w, fl.d, s))) return rc;
+    if ((rc = launch_check_finite(p, g.cells, fl.d, s))) return rc;
+    int f = 0;
+    if ((rc = fl.close(&f))) return rc;
+    if ((rc = flags_status(f, true))) return rc;
+    FlagsScope fl2(s);
+    if ((rc = fl2.open())) return rc;
+    if ((rc = launch_correct<T>(g, p, dt, u, v, w, fl2.d, s))) return rc;
+    if ((rc = fl2.close(&f))) return rc;
+    return flags_status(f, true);
+}
+
+template <class T>
+static int advect_prim(const rb200_grid* grid, const T* u, const T* v, const T* w, double dt, T* ou, T* ov, T* ow,
+                       void* stream) {
+    if (!std::isfinite(dt) || dt <= 0.0) return RB200_INVALID_ARGUMENT;
+    RB200_PRIM_BEGIN(grid, 1.0)
+    if ((rc = launch_validate_faces<T>(g, u, v, w, fl.d, s))) return rc;
+    int f = 0;
+    if ((rc = fl.close(&f))) return rc;
+    if (f & VF_NONFINITE) return RB200_NONFINITE_INPUT;
+    FlagsScope fl2(s);
+    if ((rc = fl2.open())) return rc;
+    if ((rc = launch_advect_velocity<T>(g, u, v, w, dt, ou, ov, ow, nullptr, 0.0, fl2.d, s))) return rc;
+    if ((rc = fl2.close(&f))) return rc;
+    return flags_status(f, false);
+}
+
+template <class T>
+static int carrier_step_t(rb200_carrier* c, const rb200_step_params* prm, rb200_step_report* rep,
+                          rb200_cancel_fn cancelled, void* ctx) {
+    const GridDev& g = c->g;
+    // dt policy (src/simulation.rs:952-979): dt = min(requested, budget/rate).
+    double dt = prm->requested_dt;
+    if (prm->cfl > 0.0 && c->rate > 0.0) dt = std::fmin(dt, prm->cfl / c->rate);
+    if (!std::isfinite(dt) || dt <= 0.0 || !std::isfinite(c->time + dt) || c->time + dt <= c->time)
+        return RB200_INVALID_ARGUMENT;
+    rep->dt = dt;
+    if (cancelled && cancelled(ctx)) return RB200_CANCELLED;
+    const int cand = (c->acc + 1) % 3, corr = (c->acc + 2) % 3;
+    const uint64_t launches0 = c->solver.launches();
+    T* const A[3] = {(T*)c->faces[c->acc][0], (T*)c->faces[c->acc][1], (T*)c->faces[c->acc][2]};
+    T* const B[3] = {(T*)c->faces[cand][0], (T*)c->faces[cand][1], (T*)c->faces[cand][2]};
+    T* const Cc[3] = {(T*)c->faces[corr][0], (T*)c->faces[corr][1], (T*)c->faces[corr][2]};
+    const float* tr = c->tracer[0] ? c->tracer[c->tacc] : nullptr;
+    RB200_CUDA(cudaMemsetAsync(c->d_flags, 0, sizeof(int), c->stream));
+    int rc = launch_advect_velocity<T>(g, A[0], A[1], A[2], dt, B[0], B[1], B[2], tr, prm->buoyancy, c->d_flags,
+                                       c->stream);
+    if (rc) return rc;
+    if ((rc = launch_build_rhs<T>(g, B[0], B[1], B[2], dt, c->solver.b(), c->d_flags, c->stream))) return rc;
+    RB200_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    int ps = c->solver.solve(dt, c->cfg.settings, &rep->pressure, cancelled, ctx);
+    RB200_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    RB200_CUDA(cudaEventSynchronize(c->ev[1]));
+    {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+        rep->pressure_ms = double(ms);
+    }
+    rep->pressure_status = ps;
+    if (ps == RB200_CANCELLED) return RB200_CANCELLED;
+    if (ps == RB200_EXECUTION) {
+        c->err = get_error();
+        return ps;
+    }
+    if (ps != RB200_OK && !(ps == RB200_ITERATION_LIMIT && prm->iteration_limit_ok)) return ps;
+    const T* const Bc[3] = {B[0], B[1], B[2]};
+    if ((rc = launch_correct_divergence<T>(g, c->solver.p(), dt, Bc, Cc, c->solver.partials(),
+                                           c->solver.partial_blocks(), c->d_scalars, c->d_flags, c->stream)))
+        return rc;
+    if (tr) {
+        if ((rc = launch_advect_tracer<T>(g, tr, Cc[0], Cc[1], Cc[2], dt, c->tracer[c->tacc ^ 1], c->d_flags,
+                                          c->stream)))
+            return rc;
+    }
+    RB200_CUDA(cudaMemcpyAsync(c->h_scalars, c->d_scalars, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    RB200_CUDA(cudaMemcpyAsync(c->h_flags, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    RB200_CUDA(cudaStreamSynchronize(c->stream));
+    rep->kernel_launches = (c->solver.launches() - launches0) + 3 + (tr ? 1 : 0);
+    if (*c->h_flags & VF_NONFINITE) return RB200_NONFINITE_INPUT;
+    if (*c->h_flags & (VF_ARITH | VF_F32_RANGE)) return RB200_ARITHMETIC_FAILURE;
+    double rate = 0.0;
+    for (int d = 0; d < 3; ++d) rate += c->h_scalars[1 + d] / g.h[d];
+    rep->actual_divergence_max = c->h_scalars[0];
+    rep->velocity_rate = rate;
+    rep->courant = dt * rate;
+    if (!prm->skip_gates) {
+        if (rep->actual_divergence_max > c->cfg.actual_divergence_limit) return RB200_DIVERGENCE_LIMIT;
+        if (!std::isfinite(rep->courant)) return RB200_ARITHMETIC_FAILURE;
+        if (rep->courant > c->cfg.max_courant) return RB200_COURANT_LIMIT;
+    }
+    if (cancelled && cancelled(ctx)) return RB200_CANCELLED;
+    // commit_prepared (src/simulation.rs:805-811): publish the candidate.
+    c->acc = corr;
+    if (tr) c->tacc ^= 1;
+    c->time += dt;
+    c->generation += 1;
+    c->rate = rate;
+    rep->time = c->time;
+    rep->generation = c->generation;
+    return RB200_OK;
+}
+
+extern "C" {
+
+int rb200_abi_version(void) { return RB200_ABI_VERSION; }
+
+const char* rb200_status_string(int status) {
+    switch (status) {
+        case RB200_OK: return "ok";
+        case RB200_UNSUPPORTED: return "unsupported request";
+        case RB200_EXECUTION: return "execution failed";
+        case RB200_NONFINITE_OUTPUT: return "nonfinite output";
+        case RB200_NONZERO_GAUGE: return "nonzero gauge";
+        case RB200_QUALITY_GATE: return "quality gate";
+        case RB200_CANCELLED: return "cancelled";
+        case RB200_ITERATION_LIMIT: return "pressure iteration limit";
+        case RB200_BREAKDOWN: return "pressure arithmetic broke down";
+        case RB200_OUT_OF_MEMORY: return "device allocation failed";
+        case RB200_INVALID_ARGUMENT: return "invalid argument";
+        case RB200_INCOMPATIBLE_RHS: return "sealed-domain RHS sum exceeds rounding budget";
+        case RB200_NONFINITE_INPUT: return "field contains a nonfinite value";
+        case RB200_NONZERO_WALL_VELOCITY: return "fixed wall velocity is nonzero";
+        case RB200_ARITHMETIC_FAILURE: return "numerical operation produced a nonfinite value";
+        case RB200_DIVERGENCE_LIMIT: return "actual divergence limit";
+        case RB200_COURANT_LIMIT: return "Courant limit";
+        case RB200_NO_DEVICE: return "no sm_100 device";
+        case RB200_LENGTH_MISMATCH: return "field length does not match the grid";
+        default: return "unknown status";
+    }
+}
+
+int rb200_device_count(void) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) return 0;
+    int n = 0;
+    for (int d = 0; d < count; ++d) {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, d) == cudaSuccess && prop.major == 10) ++n;
+    }
+    return n;
+}
+
+// ---------------------------------------------------------------- workspace
+int rb200_workspace_create(const rb200_grid* grid, double density, int method, uint64_t memory_limit,
+                           int device, rb200_workspace** out) {
+    if (!out) return RB200_INVALID_ARGUMENT;
+    *out = nullptr;
+    GridDev g;
+    int rc = make_grid_dev(grid, density, &g);
+    if (rc) {
+        set_error("invalid grid or density");
+        return rc;
+    }
+    if (method != RB200_JACOBI_PCG_V1 && method != RB200_RBSGS_PCG) {
+        set_error("method not available on the device");
+        return RB200_UNSUPPORTED;
+    }
+    // Six f64 cell arrays at most (b, p, r, two directions, z) plus partials.
+    uint64_t need = uint64_t(g.cells) * (method == RB200_RBSGS_PCG ? 48 : 40);
+    if (need > memory_limit) {
+        set_error("device buffers exceed the memory limit");
+        return RB200_OUT_OF_MEMORY;
+    }
+    if ((rc = select_device(device))) return rc;
+    std::unique_ptr<rb200_workspace> ws(new (std::nothrow) rb200_workspace());
+    if (!ws) return RB200_OUT_OF_MEMORY;
+    ws->device = device;
+    ws->g = g;
+    ws->grid = *grid;
+    ws->method = method;
+    ws->limit = memory_limit;
+    RB200_CUDA(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
+    if ((rc = ws->solver.init(g, method, ws->stream))) return rc;
+    *out = ws.release();
+    return RB200_OK;
+}
+
+void rb200_workspace_destroy(rb200_workspace* ws) { delete ws; }
+
+uint64_t rb200_workspace_allocated_bytes(const rb200_workspace* ws) { return ws ? ws->solver.bytes() : 0; }
+
+void* rb200_workspace_stream(rb200_workspace* ws) { return ws ? (void*)ws->stream : nullptr; }
+
+static int workspace_solve(rb200_workspace* ws, const double* rhs, bool on_device, size_t len, double dt,
+                           const rb200_settings* settings, rb200_report* report, rb200_cancel_fn cancelled,
+                           void* ctx) {
+    if (!ws || !rhs || !settings) return RB200_INVALID_ARGUMENT;
+    if (report) std::memset(report, 0, sizeof(*report));
+    if (len != size_t(ws->g.cells)) return RB200_LENGTH_MISMATCH;
+    cudaSetDevice(ws->device);
+    if (!std::isfinite(dt) || dt <= 0.0 || !settings_valid(settings)) {
+        // validate_cells(rhs) precedes the settings check (src/pressure.rs:373).
+        if (!on_device)
+            for (size_t i = 0; i < len; ++i)
+                if (!std::isfinite(rhs[i])) return RB200_NONFINITE_INPUT;
+        return RB200_INVALID_ARGUMENT;
+    }
+    if (cancelled && cancelled(ctx)) return RB200_CANCELLED;
+    RB200_CUDA(cudaMemcpyAsync(ws->solver.b(), rhs, len * sizeof(double),
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ws->stream));
+    int rc = ws->solver.solve(dt, *settings, report, cancelled, ctx);
+    if (rc == RB200_EXECUTION) ws->err = get_error();
+    return rc;
+}
+
+int rb200_workspace_solve_rhs(rb200_workspace* ws, const double* rhs, size_t len, double dt,
+                              const rb200_settings* settings, rb200_report* report, rb200_cancel_fn cancelled,
+                              void* ctx) {
+    return workspace_solve(ws, rhs, false, len, dt, settings, report, cancelled, ctx);
+}
+
+int rb200_workspace_solve_rhs_device(rb200_workspace* ws, const double* rhs_device, size_t len, double dt,
+                                     const rb200_settings* settings, rb200_report* report,
+                                     rb200_cancel_fn cancelled, void* ctx) {
+    return workspace_solve(ws, rhs_device, true, len, dt, settings, report, cancelled, ctx);
+}
+
+int rb200_workspace_pressure(rb200_workspace* ws, double* out, size_t len) {
+    if (!ws || !out) return RB200_INVALID_ARGUMENT;
+    if (len != size_t(ws->g.cells)) return RB200_LENGTH_MISMATCH;
+    cudaSetDevice(ws->device);
+    RB200_CUDA(cudaMemcpyAsync(out, ws->solver.p(), len * sizeof(double), cudaMemcpyDeviceToHost, ws->stream));
+    RB200_CUDA(cudaStreamSynchronize(ws->stream));
+    return RB200_OK;
+}
+
+const double* rb200_workspace_pressure_device(rb200_workspace* ws) { return ws ? ws->solver.p() : nullptr; }
+
+int rb200_workspace_set_trace(rb200_workspace* ws, rb200_trace* trace, size_t capacity) {
+    if (!ws) return RB200_INVALID_ARGUMENT;
+    cudaSetDevice(ws->device);
+    return ws->solver.set_trace(trace, capacity);
+}
+
+int rb200_workspace_profile(rb200_workspace* ws, int which, int launches, double* avg_ms) {
+    if (!ws || !avg_ms) return RB200_INVALID_ARGUMENT;
+    cudaSetDevice(ws->device);
+    return ws->solver.profile(which, launches, avg_ms);
+}
+
+// ---------------------------------------------------------------- provider
+static const char* method_id(int method) {
+    switch (method) {
+        case RB200_JACOBI_PCG_V1: return "b200-jacobi-pcg-v1";
+        case RB200_SGS_PCG_V1: return "b200-sgs-pcg-v1";
+        case RB200_RBSGS_PCG: return "b200-rbsgs-pcg";
+        default: return "b200-mg-mixed";
+    }
+}
+
+int rb200_provider_create(const rb200_provider_config* config, rb200_provider** out) {
+    if (!config || !out) return RB200_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!settings_valid(&config->settings)) return RB200_INVALID_ARGUMENT;
+    std::unique_ptr<rb200_provider> p(new (std::nothrow) rb200_provider());
+    if (!p) return RB200_OUT_OF_MEMORY;
+    p->cfg = *config;
+    int rc = rb200_workspace_create(&config->grid, config->density, config->method, UINT64_MAX, config->device,
+                                    &p->ws);
+    if (rc) return rc;
+    *out = p.release();
+    return RB200_OK;
+}
+
+void rb200_provider_destroy(rb200_provider* provider) { delete provider; }
+
+int rb200_provider_metadata(const rb200_provider* provider, rb200_metadata* out) {
+    if (!provider || !out) return RB200_INVALID_ARGUMENT;
+    // Mirrors the sealed-box metadata of src/solver_provider/modal.rs:93-119.
+    out->id = method_id(provider->cfg.method);
+    out->version = "1";
+    out->stage = "pressure";
+    out->input_layout = "x-fastest-cell-centered";
+    out->input_scalar = "f64";
+    out->input_units = "m^3/s^2";
+    out->output_layout = "x-fastest-cell-centered";
+    out->output_scalar = "f64";
+    out->output_units = "Pa";
+    out->domain = "sealed constant-density MAC box";
+    for (int d = 0; d < 3; ++d) out->shape_xyz[d] = provider->cfg.grid.counts[d];
+    return RB200_OK;
+}
+
+int rb200_provider_supports(const rb200_provider* provider, const rb200_request* request) {
+    if (!provider || !request) return RB200_INVALID_ARGUMENT;
+    if (!same_grid(provider->cfg.grid, request->grid)) return RB200_UNSUPPORTED;
+    if (request->density != provider->cfg.density) return RB200_UNSUPPORTED;
+    if (request->len != size_t(provider->ws->g.cells)) return RB200_UNSUPPORTED;
+    return RB200_OK;
+}
+
+int rb200_provider_predict(rb200_provider* provider, const rb200_request* request, double* pressure, size_t len,
+                           rb200_cancel_fn cancelled, void* ctx) {
+    if (!provider || !request || !pressure || !request->rhs) return RB200_INVALID_ARGUMENT;
+    int rc = rb200_provider_supports(provider, request);
+    if (rc) {
+        provider->err = "request grid, density or length differs from the provider's";
+        return rc;
+    }
+    if (len != request->len) {
+        provider->err = "output length differs from the request";
+        return RB200_UNSUPPORTED;
+    }
+    rc = rb200_workspace_solve_rhs(provider->ws, request->rhs, request->len, request->dt, &provider->cfg.settings,
+                                   &provider->last, cancelled, ctx);
+    provider->last_status = rc;
+    if (rc == RB200_CANCELLED) return RB200_CANCELLED;
+    if (rc != RB200_OK) {
+        provider->err = std::string("device solve: ") + rb200_status_string(rc);
+        return rc == RB200_UNSUPPORTED ? RB200_UNSUPPORTED : RB200_EXECUTION;
+    }
+    rc = rb200_workspace_pressure(provider->ws, pressure, len);
+    if (rc) {
+        provider->err = get_error();
+        return RB200_EXECUTION;
+    }
+    for (size_t i = 0; i < len; ++i)
+        if (!std::isfinite(pressure[i])) return RB200_NONFINITE_OUTPUT;
+    provider->err.clear();
+    return RB200_OK;
+}
+
+const char* rb200_provider_last_error(const rb200_provider* provider) {
+    return provider ? provider->err.c_str() : get_error();
+}
+
+int rb200_provider_last_report(const rb200_provider* provider, rb200_report* out, int* solve_status) {
+    if (!provider || !out) return RB200_INVALID_ARGUMENT;
+    *out = provider->last;
+    if (solve_status) *solve_status = provider->last_status;
+    return RB200_OK;
+}
+
+// ---------------------------------------------------------------- primitives
+int rb200_apply_full_device(const rb200_grid* grid, double density, const double* pressure, double* out,
+                            void* stream) {
+    RB200_PRIM_BEGIN(grid, density)
+    if ((rc = launch_check_finite(pressure, g.cells, fl.d, s))) return rc;
+    if ((rc = launch_apply_full(g, pressure, out, fl.d, s))) return rc;
+    int f = 0;
+    if ((rc = fl.close(&f))) return rc;
+    return flags_status(f, false);
+}
+
+
+int rb200_build_rhs_f32_device(const rb200_grid* grid, double density, const float* u, const float* v,
+                               const float* w, double dt, double* rhs, void* stream) {
+    return build_rhs_prim<float>(grid, density, u, v, w, dt, rhs, stream);
+}
+int rb200_build_rhs_f64_device(const rb200_grid* grid, double density, const double* u, const double* v,
+                               const double* w, double dt, double* rhs, void* stream) {
+    return build_rhs_prim<double>(grid, density, u, v, w, dt, rhs, stream);
+}
+
+
+int rb200_divergence_f32_device(const rb200_grid* grid, const float* u, const float* v, const float* w, double* out,
+                                void* stream) {
+    return divergence_prim<float>(grid, u, v, w, out, stream);
+}
+int rb200_divergence_f64_device(const rb200_grid* grid, const double* u, const double* v, const double* w,
+                                double* out, void* stream) {
+    return divergence_prim<double>(grid, u, v, w, out, stream);
+}
+
+
+int rb200_correct_f32_device(const rb200_grid* grid, double density, const double* pressure, double dt, float* u,
+                             float* v, float* w, void* stream) {
+    return correct_prim<float>(grid, density, pressure, dt, u, v, w, stream);
+}
+int rb200_correct_f64_device(const rb200_grid* grid, double density, const double* pressure, double dt, double* u,
+                             double* v, double* w, void* stream) {
+    return correct_prim<double>(grid, density, pressure, dt, u, v, w, stream);
+}
+
+
+int rb200_advect_velocity_f32_device(const rb200_grid* grid, const float* u, const float* v, const float* w,
+                                     double dt, float* ou, float* ov, float* ow, void* stream) {
+    return advect_prim<float>(grid, u, v, w, dt, ou, ov, ow, stream);
+}
+int rb200_advect_velocity_f64_device(const rb200_grid* grid, const double* u, const double* v, const double* w,
+                                     double dt, double* ou, double* ov, double* ow, void* stream) {
+    return advect_prim<double>(grid, u, v, w, dt, ou, ov, ow, stream);
+}
+
+int rb200_advect_tracer_f32_device(const rb200_grid* grid, const float* old, const float* u, const float* v,
+                                   const float* w, double dt, float* out, void* stream) {
+    if (!std::isfinite(dt) || dt <= 0.0) return RB200_INVALID_ARGUMENT;
+    RB200_PRIM_BEGIN(grid, 1.0)
+    if ((rc = launch_validate_faces<float>(g, u, v, w, fl.d, s))) return rc;
+    int f = 0;
+    if ((rc = fl.close(&f))) return rc;
+    if (f & VF_NONFINITE) return RB200_NONFINITE_INPUT;
+    FlagsScope fl2(s);
+    if ((rc = fl2.open())) return rc;
+    if ((rc = launch_advect_tracer<float>(g, old, u, v, w, dt, out, fl2.d, s))) return rc;
+    if ((rc = fl2.close(&f))) return rc;
+    return flags_status(f, false);
+}
+
+// ---------------------------------------------------------------- carrier
+int rb200_carrier_create(const rb200_carrier_config* config, rb200_carrier** out) {
+    if (!config || !out) return RB200_INVALID_ARGUMENT;
+    *out = nullptr;
+    GridDev g;
+    int rc = make_grid_dev(&config->grid, config->density, &g);
+    if (rc) return rc;
+    if (config->storage != RB200_FACES_F32 && config->storage != RB200_FACES_F64) return RB200_INVALID_ARGUMENT;
+    if (!settings_valid(&config->settings)) return RB200_INVALID_ARGUMENT;
+    if (!(config->max_courant > 0.0) || !std::isfinite(config->actual_divergence_limit)) return RB200_INVALID_ARGUMENT;
+    if ((rc = select_device(config->device))) return rc;
+    std::unique_ptr<rb200_carrier> c(new (std::nothrow) rb200_carrier());
+    if (!c) return RB200_OUT_OF_MEMORY;
+    c->cfg = *config;
+    c->g = g;
+    c->device = config->device;
+    c->elem = config->storage == RB200_FACES_F32 ? 4 : 8;
+    RB200_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a) {
+            if (cudaMalloc(&c->faces[b][a], size_t(g.flen[a]) * c->elem) != cudaSuccess) return RB200_OUT_OF_MEMORY;
+            c->bytes += size_t(g.flen[a]) * c->elem;
+            RB200_CUDA(cudaMemsetAsync(c->faces[b][a], 0, size_t(g.flen[a]) * c->elem, c->stream));
+        }
+    if (config->with_tracer)
+        for (int t = 0; t < 2; ++t) {
+            if (cudaMalloc(&c->tracer[t], size_t(g.cells) * 4) != cudaSuccess) return RB200_OUT_OF_MEMORY;
+            c->bytes += size_t(g.cells) * 4;
+            RB200_CUDA(cudaMemsetAsync(c->tracer[t], 0, size_t(g.cells) * 4, c->stream));
+        }
+    RB200_CUDA(cudaMalloc(&c->d_scalars, 8 * sizeof(double)));
+    RB200_CUDA(cudaMalloc(&c->d_flags, sizeof(int)));
+    RB200_CUDA(cudaMallocHost(&c->h_scalars, 8 * sizeof(double)));
+    RB200_CUDA(cudaMallocHost(&c->h_flags, sizeof(int)));
+    for (auto& e : c->ev) RB200_CUDA(cudaEventCreate(&e));
+    if ((rc = c->solver.init(g, config->method, c->stream))) return rc;
+    c->bytes += c->solver.bytes();
+    RB200_CUDA(cudaStreamSynchronize(c->stream));
+    *out = c.release();
+    return RB200_OK;
+}
+
+void rb200_carrier_destroy(rb200_carrier* carrier) { delete carrier; }
+uint64_t rb200_carrier_allocated_bytes(const rb200_carrier* carrier) { return carrier ? carrier->bytes : 0; }
+void* rb200_carrier_stream(rb200_carrier* carrier) { return carrier ? (void*)carrier->stream : nullptr; }
+
+static int carrier_rate(rb200_carrier* c, int buffer, double* rate, int* flags) {
+    const GridDev& g = c->g;
+    RB200_CUDA(cudaMemsetAsync(c->d_flags, 0, sizeof(int), c->stream));
+    int rc;
+    if (c->elem == 4)
+        rc = launch_face_maxima<float>(g, (const float*)c->faces[buffer][0], (const float*)c->faces[buffer][1],
+                                       (const float*)c->faces[buffer][2], c->solver.partials(),
+                                       c->solver.partial_blocks(), c->d_scalars, c->d_flags, c->stream);
+    else
+        rc = launch_face_maxima<double>(g, (const double*)c->faces[buffer][0], (const double*)c->faces[buffer][1],
+                                        (const double*)c->faces[buffer][2], c->solver.partials(),
+                                        c->solver.partial_blocks(), c->d_scalars, c->d_flags, c->stream);
+    if (rc) return rc;
+    if (c->elem == 4)
+        rc = launch_validate_faces<float>(g, (const float*)c->faces[buffer][0], (const float*)c->faces[buffer][1],
+                                          (const float*)c->faces[buffer][2], c->d_flags, c->stream);
+    else
+        rc = launch_validate_faces<double>(g, (const double*)c->faces[buffer][0], (const double*)c->faces[buffer][1],
+                                           (const double*)c->faces[buffer][2], c->d_flags, c->stream);
+    if (rc) return rc;
+    RB200_CUDA(cudaMemcpyAsync(c->h_scalars, c->d_scalars, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    RB200_CUDA(cudaMemcpyAsync(c->h_flags, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    RB200_CUDA(cudaStreamSynchronize(c->stream));
+    // velocity_rate (src/simulation.rs:1415-1429): sum_d max|u_d| / h_d.
+    double r = 0.0;
+    for (int d = 0; d < 3; ++d) r += c->h_scalars[d] / g.h[d];
+    *rate = r;
+    *flags = *c->h_flags;
+    return RB200_OK;
+}
+
+int rb200_carrier_upload(rb200_carrier* carrier, const void* u, const void* v, const void* w, const float* tracer) {
+    if (!carrier || !u || !v || !w) return RB200_INVALID_ARGUMENT;
+    rb200_carrier* c = carrier;
+    cudaSetDevice(c->device);
+    const void* src[3] = {u, v, w};
+    for (int a = 0; a < 3; ++a)
+        RB200_CUDA(cudaMemcpyAsync(c->faces[c->acc][a], src[a], size_t(c->g.flen[a]) * c->elem,
+                                   cudaMemcpyHostToDevice, c->stream));
+    if (tracer) {
+        if (!c->tracer[0]) return RB200_INVALID_ARGUMENT;
+        RB200_CUDA(cudaMemcpyAsync(c->tracer[c->tacc], tracer, size_t(c->g.cells) * 4, cudaMemcpyHostToDevice,
+                                   c->stream));
+    }
+    double rate = 0.0;
+    int flags = 0;
+    int rc = carrier_rate(c, c->acc, &rate, &flags);
+    if (rc) return rc;
+    if (flags & VF_NONFINITE) return RB200_NONFINITE_INPUT;
+    if (flags & VF_WALL) return RB200_NONZERO_WALL_VELOCITY;
+    c->rate = rate;
+    c->time = 0.0;
+    c->generation = 0;
+    return RB200_OK;
+}
+
+int rb200_carrier_download(rb200_carrier* carrier, void* u, void* v, void* w, float* tracer) {
+    if (!carrier) return RB200_INVALID_ARGUMENT;
+    rb200_carrier* c = carrier;
+    cudaSetDevice(c->device);
+    void* dst[3] = {u, v, w};
+    for (int a = 0; a < 3; ++a)
+        if (dst[a])
+            RB200_CUDA(cudaMemcpyAsync(dst[a], c->faces[c->acc][a], size_t(c->g.flen[a]) * c->elem,
+                                       cudaMemcpyDeviceToHost, c->stream));
+    if (tracer && c->tracer[0])
+        RB200_CUDA(cudaMemcpyAsync(tracer, c->tracer[c->tacc], size_t(c->g.cells) * 4, cudaMemcpyDeviceToHost,
+                                   c->stream));
+    RB200_CUDA(cudaStreamSynchronize(c->stream));
+    return RB200_OK;
+}
+
+int rb200_carrier_state_device(rb200_carrier* carrier, void** u, void** v, void** w, float** tracer) {
+    if (!carrier) return RB200_INVALID_ARGUMENT;
+    if (u) *u = carrier->faces[carrier->acc][0];
+    if (v) *v = carrier->faces[carrier->acc][1];
+    if (w) *w = carrier->faces[carrier->acc][2];
+    if (tracer) *tracer = carrier->tracer[0] ? carrier->tracer[carrier->tacc] : nullptr;
+    return RB200_OK;
+}
+
+int rb200_carrier_profile(rb200_carrier* carrier, int which, int launches, double* avg_ms) {
+    if (!carrier || !avg_ms) return RB200_INVALID_ARGUMENT;
+    cudaSetDevice(carrier->device);
+    return carrier->solver.profile(which, launches, avg_ms);
+}
+
+int rb200_carrier_pressure(rb200_carrier* carrier, double* out, size_t len) {
+    if (!carrier || !out) return RB200_INVALID_ARGUMENT;
+    if (len != size_t(carrier->g.cells)) return RB200_LENGTH_MISMATCH;
+    cudaSetDevice(carrier->device);
+    RB200_CUDA(cudaMemcpyAsync(out, carrier->solver.p(), len * sizeof(double), cudaMemcpyDeviceToHost,
+                               carrier->stream));
+    RB200_CUDA(cudaStreamSynchronize(carrier->stream));
+    return RB200_OK;
+}
+
+
+int rb200_carrier_step(rb200_carrier* carrier, const rb200_step_params* params, rb200_step_report* report,
+                       rb200_cancel_fn cancelled, void* ctx) {
+    if (!carrier || !params || !report) return RB200_INVALID_ARGUMENT;
+    std::memset(report, 0, sizeof(*report));
+    cudaSetDevice(carrier->device);
+    int rc = carrier->elem == 4 ? carrier_step_t<float>(carrier, params, report, cancelled, ctx)
+                                : carrier_step_t<double>(carrier, params, report, cancelled, ctx);
+    if (rc == RB200_EXECUTION && carrier->err.empty()) carrier->err = get_error();
+    return rc;
+}
+
+}  // extern "C"

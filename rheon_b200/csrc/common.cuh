@@ -1,0 +1,203 @@
+// Shared device-side definitions for the sm_100a carrier kernels.
+//
+// Layout in HBM follows Rheon's geometry (src/geometry.rs:250-258): cells are
+// x-fastest, index i + nx*(j + ny*k); the faces of axis d have counts[d]+1
+// along d and are also x-fastest, each axis in its own array.
+//
+// The library is compiled with -fmad=false: Rust never contracts a*b+c, so
+// every multiply-add below rounds twice, exactly like the reference.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "../../include/rheon_b200.h"
+
+namespace rb200 {
+
+// Geometry and sealed-box operator coefficients, passed by value to kernels.
+// PressureOperator::new (src/operator.rs:58-97) fixes area, accel, weight and
+// the 64 neighbour-mask diagonals summed lower/upper x X,Y,Z.
+struct GridDev {
+    int n[3];        // cell counts
+    int fc[3][3];    // face counts per axis
+    int flen[3];     // face array lengths
+    int cells;       // n0*n1*n2
+    double h[3];
+    double o[3];
+    double up[3];
+    double area[3];
+    double accel[3];
+    double weight[3];
+    double volume;
+    double diag[64];
+};
+
+__device__ __forceinline__ int cell_idx(const GridDev& g, int i, int j, int k) {
+    return i + g.n[0] * (j + g.n[1] * k);
+}
+__device__ __forceinline__ int face_idx(const GridDev& g, int a, int i, int j, int k) {
+    return i + g.fc[a][0] * (j + g.fc[a][1] * k);
+}
+// PressureOperator::diagonal (src/operator.rs:813-822).
+__device__ __forceinline__ double diag_at(const GridDev& g, int i, int j, int k) {
+    int mask = int(i > 0) | (int(i + 1 < g.n[0]) << 1) | (int(j > 0) << 2) |
+               (int(j + 1 < g.n[1]) << 3) | (int(k > 0) << 4) | (int(k + 1 < g.n[2]) << 5);
+    return g.diag[mask];
+}
+
+// ------------------------------------------------------------ double-double
+// Error-free two-sum (Knuth). With products rounded exactly as the reference
+// rounds them, a double-double accumulation of the rounded products followed
+// by one final rounding lands on the same double as Rheon's serial Neumaier
+// sum (src/pressure.rs:135-148) except in rare near-tie cases.
+struct dd {
+    double hi, lo;
+};
+
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+    s = a + b;
+    double bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
+__device__ __forceinline__ dd dd_add(dd a, dd b) {
+    double s, e;
+    two_sum(a.hi, b.hi, s, e);
+    e = e + (a.lo + b.lo);
+    dd r;
+    two_sum(s, e, r.hi, r.lo);
+    return r;
+}
+
+__device__ __forceinline__ dd dd_add1(dd a, double b) {
+    double s, e;
+    two_sum(a.hi, b, s, e);
+    e = e + a.lo;
+    dd r;
+    two_sum(s, e, r.hi, r.lo);
+    return r;
+}
+
+__device__ __forceinline__ double dd_value(dd a) { return a.hi + a.lo; }
+
+__device__ __forceinline__ dd dd_shfl_xor(dd a, int m) {
+    dd r;
+    r.hi = __shfl_xor_sync(0xffffffffu, a.hi, m);
+    r.lo = __shfl_xor_sync(0xffffffffu, a.lo, m);
+    return r;
+}
+
+__device__ __forceinline__ dd warp_reduce_dd(dd a) {
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) a = dd_add(a, dd_shfl_xor(a, m));
+    return a;
+}
+
+__device__ __forceinline__ double warp_reduce_max(double a) {
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, m));
+    return a;
+}
+
+// Block reduction of K double-double sums and M maxima. Deterministic: fixed
+// lane pattern, fixed warp order. Result valid in thread 0. blockDim.x*y*z
+// must be a multiple of 32 and at most 1024.
+template <int K, int M>
+struct BlockReduce {
+    dd s[32][K > 0 ? K : 1];
+    double m[32][M > 0 ? M : 1];
+};
+
+template <int K, int M>
+__device__ __forceinline__ void block_reduce(BlockReduce<K, M>& sm, dd (&sums)[K > 0 ? K : 1],
+                                             double (&maxs)[M > 0 ? M : 1]) {
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = (nthreads + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < K; ++q) sums[q] = warp_reduce_dd(sums[q]);
+#pragma unroll
+    for (int q = 0; q < M; ++q) maxs[q] = warp_reduce_max(maxs[q]);
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) sm.s[warp][q] = sums[q];
+#pragma unroll
+        for (int q = 0; q < M; ++q) sm.m[warp][q] = maxs[q];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) sums[q] = lane < nwarps ? sm.s[lane][q] : dd{0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < M; ++q) maxs[q] = lane < nwarps ? sm.m[lane][q] : 0.0;
+#pragma unroll
+        for (int q = 0; q < K; ++q) sums[q] = warp_reduce_dd(sums[q]);
+#pragma unroll
+        for (int q = 0; q < M; ++q) maxs[q] = warp_reduce_max(maxs[q]);
+    }
+    __syncthreads();
+}
+
+// Partials of one reduction stage: per block K dd sums and M maxima.
+// The last block to arrive (atomic ticket, no spinning) folds all partials in
+// block order, so the result does not depend on block scheduling.
+struct Partials {
+    double* data;        // [nblocks][2K + M]
+    unsigned* ticket;    // zero between uses
+};
+
+template <int K, int M>
+__device__ __forceinline__ bool publish_and_check_last(const Partials& P, int block_id, int nblocks,
+                                                       const dd (&sums)[K > 0 ? K : 1],
+                                                       const double (&maxs)[M > 0 ? M : 1]) {
+    __shared__ bool last;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    if (tid == 0) {
+        double* slot = P.data + size_t(block_id) * (2 * K + M);
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            slot[2 * q] = sums[q].hi;
+            slot[2 * q + 1] = sums[q].lo;
+        }
+#pragma unroll
+        for (int q = 0; q < M; ++q) slot[2 * K + q] = maxs[q];
+        __threadfence();
+        unsigned t = atomicAdd(P.ticket, 1u);
+        last = (t == unsigned(nblocks - 1));
+    }
+    __syncthreads();
+    return last;
+}
+
+// Called by all threads of the last block: folds nblocks partials.
+template <int K, int M>
+__device__ __forceinline__ void fold_partials(const Partials& P, int nblocks, BlockReduce<K, M>& sm,
+                                              dd (&sums)[K > 0 ? K : 1],
+                                              double (&maxs)[M > 0 ? M : 1]) {
+    __threadfence();
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+#pragma unroll
+    for (int q = 0; q < K; ++q) sums[q] = dd{0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < M; ++q) maxs[q] = 0.0;
+    for (int b = tid; b < nblocks; b += nthreads) {
+        const double* slot = P.data + size_t(b) * (2 * K + M);
+#pragma unroll
+        for (int q = 0; q < K; ++q) sums[q] = dd_add(sums[q], dd{__ldcg(slot + 2 * q), __ldcg(slot + 2 * q + 1)});
+#pragma unroll
+        for (int q = 0; q < M; ++q) maxs[q] = fmax(maxs[q], __ldcg(slot + 2 * K + q));
+    }
+    block_reduce<K, M>(sm, sums, maxs);
+    if (tid == 0) *P.ticket = 0u;
+}
+
+// Wall-normal faces of axis a are the ones with coordinate 0 or n_a.
+__device__ __forceinline__ bool is_wall_face(const GridDev& g, int a, int i, int j, int k) {
+    int c = a == 0 ? i : (a == 1 ? j : k);
+    return c == 0 || c == g.n[a];
+}
+
+}  // namespace rb200

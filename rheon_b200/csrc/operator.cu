@@ -1,0 +1,339 @@
+// Sealed-box PressureOperator primitives on the device (src/operator.rs).
+// Each kernel keeps the reference's per-element operation order; the library
+// is built with -fmad=false so no multiply-add is fused.
+#include "internal.hpp"
+#include "stencil.cuh"
+
+namespace rb200 {
+
+constexpr int EW_THREADS = 256;
+constexpr int EW_BLOCKS_CAP = 148 * 8;
+constexpr float kF32Max = 3.40282346638528859811704183484516925440e+38f;
+
+static inline int ew_blocks(long long n) {
+    long long b = (n + EW_THREADS - 1) / EW_THREADS;
+    if (b < 1) b = 1;
+    return int(b < EW_BLOCKS_CAP ? b : EW_BLOCKS_CAP);
+}
+
+int partials_blocks_needed(const GridDev& g) {
+    MarchGrid m1 = march_grid(g.n, 1);
+    int need = m1.nblocks;  // the deepest split any marching kernel may use
+    return need > EW_BLOCKS_CAP ? need : EW_BLOCKS_CAP;
+}
+
+// ------------------------------------------------------------ apply_full
+__global__ void __launch_bounds__(TILE_THREADS) k_apply_full(GridDev g, int zc, const double* __restrict__ p,
+                                                              double* __restrict__ out, int* flags) {
+    march(
+        g, zc, [&](int c, int, int, int) { return p[c]; },
+        [&](int c, int i, int j, int k, const Neigh& v) {
+            double q = apply_row(g, i, j, k, v);
+            if (!isfinite(q)) atomicOr(flags, VF_ARITH);
+            out[c] = q;
+        });
+}
+
+int launch_apply_full(const GridDev& g, const double* p, double* out, int* flags, cudaStream_t s) {
+    MarchGrid m = march_grid(g.n, 16);
+    k_apply_full<<<m.grid, m.block, 0, s>>>(g, m.zc, p, out, flags);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+
+// ------------------------------------------------------------ finiteness
+// validate_cells (src/operator.rs:840-848): every value finite.
+__global__ void k_check_finite(const double* __restrict__ x, int n, int* flags) {
+    int local = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+        if (!isfinite(x[c])) local = VF_NONFINITE;
+    if (local) atomicOr(flags, local);
+}
+
+int launch_check_finite(const double* x, int n, int* flags, cudaStream_t s) {
+    k_check_finite<<<ew_blocks(n), EW_THREADS, 0, s>>>(x, n, flags);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+
+// ------------------------------------------------------------ validation
+// validate_velocity (src/operator.rs:850-875): finite, wall-normal faces zero.
+template <class T>
+__global__ void k_validate_faces(GridDev g, const T* __restrict__ u, const T* __restrict__ v,
+                                 const T* __restrict__ w, int* flags) {
+    const long long total = (long long)g.flen[0] + g.flen[1] + g.flen[2];
+    int local = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int a = 0;
+        long long f = t;
+        if (f >= g.flen[0]) {
+            f -= g.flen[0];
+            a = 1;
+            if (f >= g.flen[1]) {
+                f -= g.flen[1];
+                a = 2;
+            }
+        }
+        const T* src = a == 0 ? u : (a == 1 ? v : w);
+        T x = src[f];
+        if (!isfinite(double(x))) local |= VF_NONFINITE;
+        int fi = int(f % g.fc[a][0]);
+        int fj = int((f / g.fc[a][0]) % g.fc[a][1]);
+        int fk = int(f / ((long long)g.fc[a][0] * g.fc[a][1]));
+        if (is_wall_face(g, a, fi, fj, fk) && x != T(0)) local |= VF_WALL;
+    }
+    if (local) atomicOr(flags, local);
+}
+
+template <class T>
+int launch_validate_faces(const GridDev& g, const T* u, const T* v, const T* w, int* flags,
+                          cudaStream_t s) {
+    long long total = (long long)g.flen[0] + g.flen[1] + g.flen[2];
+    k_validate_faces<T><<<ew_blocks(total), EW_THREADS, 0, s>>>(g, u, v, w, flags);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+
+// ------------------------------------------------------------ build_rhs
+// build_rhs (src/operator.rs:460-509) / build_rhs_f64 (:672-708):
+//   flux = 0; flux += area_d * (f64(u_lo) - f64(u_hi)) for d = X,Y,Z; b = flux/dt
+template <class T>
+__global__ void k_build_rhs(GridDev g, const T* __restrict__ u, const T* __restrict__ v,
+                            const T* __restrict__ w, double dt, double* __restrict__ out, int* flags) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+        double flux = 0.0;
+        flux += g.area[0] * (double(u[face_idx(g, 0, i, j, k)]) - double(u[face_idx(g, 0, i + 1, j, k)]));
+        flux += g.area[1] * (double(v[face_idx(g, 1, i, j, k)]) - double(v[face_idx(g, 1, i, j + 1, k)]));
+        flux += g.area[2] * (double(w[face_idx(g, 2, i, j, k)]) - double(w[face_idx(g, 2, i, j, k + 1)]));
+        double value = flux / dt;
+        if (!isfinite(value)) atomicOr(flags, VF_ARITH);
+        out[c] = value;
+    }
+}
+
+template <class T>
+int launch_build_rhs(const GridDev& g, const T* u, const T* v, const T* w, double dt, double* out,
+                     int* flags, cudaStream_t s) {
+    k_build_rhs<T><<<ew_blocks(g.cells), EW_THREADS, 0, s>>>(g, u, v, w, dt, out, flags);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+
+// ------------------------------------------------------------ divergence
+// f32 faces (src/operator.rs:543-567): ((dx/h0 + dy/h1) + dz/h2).
+// f64 faces (src/operator.rs:711-742): value = 0; value += diff_d/h_d.
+template <class T>
+__device__ __forceinline__ double cell_divergence(const GridDev& g, double xl, double xh, double yl,
+                                                  double yh, double zl, double zh) {
+    if (sizeof(T) == 4) {
+        return (xh - xl) / g.h[0] + (yh - yl) / g.h[1] + (zh - zl) / g.h[2];
+    } else {
+        double value = 0.0;
+        value += (xh - xl) / g.h[0];
+        value += (yh - yl) / g.h[1];
+        value += (zh - zl) / g.h[2];
+        return value;
+    }
+}
+
+template <class T>
+__global__ void k_divergence(GridDev g, const T* __restrict__ u, const T* __restrict__ v,
+                             const T* __restrict__ w, double* __restrict__ out, int* flags) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+        double value = cell_divergence<T>(
+            g, double(u[face_idx(g, 0, i, j, k)]), double(u[face_idx(g, 0, i + 1, j, k)]),
+            double(v[face_idx(g, 1, i, j, k)]), double(v[face_idx(g, 1, i, j + 1, k)]),
+            double(w[face_idx(g, 2, i, j, k)]), double(w[face_idx(g, 2, i, j, k + 1)]));
+        if (!isfinite(value)) atomicOr(flags, VF_ARITH);
+        out[c] = value;
+    }
+}
+
+template <class T>
+int launch_divergence(const GridDev& g, const T* u, const T* v, const T* w, double* out,
+                      int* flags, cudaStream_t s) {
+    k_divergence<T><<<ew_blocks(g.cells), EW_THREADS, 0, s>>>(g, u, v, w, out, flags);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+
+// ------------------------------------------------------------ correction
+// f32: u <- f32( f64(u) - (dt*accel_d)*(p_c - p_l) )   (src/operator.rs:651-662)
+// f64: u <- u - dt*(accel_d*(p_c - p_l))               (src/operator.rs:767-775)
+template <class T>
+__device__ __forceinline__ T corrected(const GridDev& g, int a, T u, double pc, double pl, double dt,
+                                       int& flag) {
+    if (sizeof(T) == 4) {
+        double value = double(u) - dt * g.accel[a] * (pc - pl);
+        if (!isfinite(value) || fabs(value) > double(kF32Max)) flag |= VF_ARITH;
+        return T(value);
+    } else {
+        double gradient = g.accel[a] * (pc - pl);
+        double value = double(u) - dt * gradient;
+        if (!isfinite(value)) flag |= VF_ARITH;
+        return T(value);
+    }
+}
+
+template <class T>
+__global__ void k_correct(GridDev g, const double* __restrict__ p, double dt, T* u, T* v, T* w,
+                          int* flags) {
+    const long long total = (long long)g.flen[0] + g.flen[1] + g.flen[2];
+    const int s[3] = {1, g.n[0], g.n[0] * g.n[1]};
+    int local = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int a = 0;
+        long long f = t;
+        if (f >= g.flen[0]) {
+            f -= g.flen[0];
+            a = 1;
+            if (f >= g.flen[1]) {
+                f -= g.flen[1];
+                a = 2;
+            }
+        }
+        int fi = int(f % g.fc[a][0]);
+        int fj = int((f / g.fc[a][0]) % g.fc[a][1]);
+        int fk = int(f / ((long long)g.fc[a][0] * g.fc[a][1]));
+        if (is_wall_face(g, a, fi, fj, fk)) continue;
+        T* dst = a == 0 ? u : (a == 1 ? v : w);
+        int c = cell_idx(g, fi, fj, fk);
+        dst[f] = corrected<T>(g, a, dst[f], p[c], p[c - s[a]], dt, local);
+    }
+    if (local) atomicOr(flags, local);
+}
+
+template <class T>
+int launch_correct(const GridDev& g, const double* p, double dt, T* u, T* v, T* w, int* flags,
+                   cudaStream_t s) {
+    long long total = (long long)g.flen[0] + g.flen[1] + g.flen[2];
+    k_correct<T><<<ew_blocks(total), EW_THREADS, 0, s>>>(g, p, dt, u, v, w, flags);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+
+// ------------------------------------------------------------ fused epilogue
+// One thread per cell: corrects the three lower faces the cell owns (writes
+// them, wall faces copied through), recomputes its three upper faces to form
+// the actual divergence of the stored values (actual_divergence_max,
+// src/pressure.rs:330-342), and reduces max|div| and max|u_d| per axis
+// (velocity_rate, src/simulation.rs:1415-1429).
+template <class T>
+__global__ void __launch_bounds__(EW_THREADS) k_correct_divergence(GridDev g, const double* __restrict__ p, double dt,
+                                                                   const T* __restrict__ iu, const T* __restrict__ iv,
+                                                                   const T* __restrict__ iw, T* __restrict__ ou,
+                                                                   T* __restrict__ ov, T* __restrict__ ow,
+                                                                   Partials part, double* out_scalars, int* flags) {
+    __shared__ BlockReduce<0, 4> sm;
+    const T* in[3] = {iu, iv, iw};
+    T* out[3] = {ou, ov, ow};
+    const int s[3] = {1, g.n[0], g.n[0] * g.n[1]};
+    double mx[4] = {0.0, 0.0, 0.0, 0.0};
+    int local = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        int ijk[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
+        double lo[3], hi[3];
+        const double pc = p[c];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            int flo = face_idx(g, a, ijk[0], ijk[1], ijk[2]);
+            int fhi = flo + (a == 0 ? 1 : (a == 1 ? g.fc[1][0] : g.fc[2][0] * g.fc[2][1]));
+            T vlo = in[a][flo];
+            if (ijk[a] > 0) vlo = corrected<T>(g, a, vlo, pc, p[c - s[a]], dt, local);
+            out[a][flo] = vlo;
+            T vhi = in[a][fhi];
+            if (ijk[a] + 1 < g.n[a]) {
+                vhi = corrected<T>(g, a, vhi, p[c + s[a]], pc, dt, local);
+            } else {
+                out[a][fhi] = vhi;
+                mx[1 + a] = fmax(mx[1 + a], fabs(double(vhi)));
+            }
+            mx[1 + a] = fmax(mx[1 + a], fabs(double(vlo)));
+            lo[a] = double(vlo);
+            hi[a] = double(vhi);
+        }
+        double div = cell_divergence<T>(g, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]);
+        if (!isfinite(div)) local |= VF_ARITH;
+        mx[0] = fmax(mx[0], fabs(div));
+    }
+    if (local) atomicOr(flags, local);
+    dd none[1];
+    block_reduce<0, 4>(sm, none, mx);
+    const int bid = blockIdx.x;
+    if (publish_and_check_last<0, 4>(part, bid, gridDim.x, none, mx)) {
+        fold_partials<0, 4>(part, gridDim.x, sm, none, mx);
+        if (threadIdx.x == 0)
+            for (int q = 0; q < 4; ++q) out_scalars[q] = mx[q];
+    }
+}
+
+template <class T>
+int launch_correct_divergence(const GridDev& g, const double* p, double dt, const T* const in[3],
+                              T* const out[3], Partials part, int nblocks_cap, double* out_scalars,
+                              int* flags, cudaStream_t s) {
+    int nb = ew_blocks(g.cells);
+    if (nb > nblocks_cap) nb = nblocks_cap;
+    k_correct_divergence<T><<<nb, EW_THREADS, 0, s>>>(g, p, dt, in[0], in[1], in[2], out[0], out[1],
+                                                      out[2], part, out_scalars, flags);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+
+template <class T>
+__global__ void __launch_bounds__(EW_THREADS) k_face_maxima(GridDev g, const T* __restrict__ u,
+                                                            const T* __restrict__ v, const T* __restrict__ w,
+                                                            Partials part, double* out_scalars, int* flags) {
+    __shared__ BlockReduce<0, 3> sm;
+    double mx[3] = {0.0, 0.0, 0.0};
+    int local = 0;
+    const T* f3[3] = {u, v, w};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < g.flen[a]; f += gridDim.x * blockDim.x) {
+            double x = double(f3[a][f]);
+            if (!isfinite(x)) local |= VF_NONFINITE;
+            mx[a] = fmax(mx[a], fabs(x));
+        }
+    if (local) atomicOr(flags, local);
+    dd none[1];
+    block_reduce<0, 3>(sm, none, mx);
+    if (publish_and_check_last<0, 3>(part, blockIdx.x, gridDim.x, none, mx)) {
+        fold_partials<0, 3>(part, gridDim.x, sm, none, mx);
+        if (threadIdx.x == 0)
+            for (int q = 0; q < 3; ++q) out_scalars[q] = mx[q];
+    }
+}
+
+template <class T>
+int launch_face_maxima(const GridDev& g, const T* u, const T* v, const T* w, Partials part,
+                       int nblocks_cap, double* out_scalars, int* flags, cudaStream_t s) {
+    int nb = ew_blocks(g.flen[0]);
+    if (nb > nblocks_cap) nb = nblocks_cap;
+    k_face_maxima<T><<<nb, EW_THREADS, 0, s>>>(g, u, v, w, part, out_scalars, flags);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+
+#define RB200_INSTANTIATE(T)                                                                        \
+    template int launch_validate_faces<T>(const GridDev&, const T*, const T*, const T*, int*,       \
+                                          cudaStream_t);                                            \
+    template int launch_build_rhs<T>(const GridDev&, const T*, const T*, const T*, double, double*, \
+                                     int*, cudaStream_t);                                           \
+    template int launch_divergence<T>(const GridDev&, const T*, const T*, const T*, double*, int*,  \
+                                      cudaStream_t);                                                \
+    template int launch_correct<T>(const GridDev&, const double*, double, T*, T*, T*, int*,         \
+                                   cudaStream_t);                                                   \
+    template int launch_correct_divergence<T>(const GridDev&, const double*, double,                \
+                                              const T* const[3], T* const[3], Partials, int,        \
+                                              double*, int*, cudaStream_t);                         \
+    template int launch_face_maxima<T>(const GridDev&, const T*, const T*, const T*, Partials, int, \
+                                       double*, int*, cudaStream_t);
+RB200_INSTANTIATE(float)
+RB200_INSTANTIATE(double)
+#undef RB200_INSTANTIATE
+
+}  // namespace rb200

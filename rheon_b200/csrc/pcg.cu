@@ -1,0 +1,730 @@
+// Device-driven gauge-eliminated PCG (PressureWorkspace::solve_loaded,
+// src/pressure.rs:577-740) on the sealed-box operator.
+//
+// One PCG iteration of the Jacobi method is two marching passes:
+//   pass 1  d <- z + beta*d (z = r/D recomputed, never stored), q = K d,
+//           curvature = d.q                                     (24N bytes)
+//   pass 2  q = K d recomputed from d, p += alpha*d, r -= alpha*q,
+//           z = r/D, r.r and r.z                                 (40N bytes)
+// instead of the four array passes of the reference (88N). Scalars never leave
+// the device: the last block of each pass takes solve_loaded's decision
+// (alpha, beta, breakdown, candidate, restart) and writes it to SolveState.
+// The true-residual check and the restart run as flag-gated kernels at the end
+// of each captured chunk of iterations, so the host only launches graphs and
+// polls one word per chunk.
+#include <algorithm>
+#include <vector>
+
+#include "pcg.hpp"
+#include "stencil.cuh"
+
+namespace rb200 {
+
+constexpr int EW = 256;
+constexpr int EW_CAP = 148 * 8;
+constexpr double kEps = 2.220446049250313e-16;
+
+enum Mode : int { MODE_INIT = 0, MODE_ITER = 1, MODE_REPLACE = 2 };
+constexpr int F_CANDIDATE = 32;  // RB-SGS: candidate decided in pass 2, acted on after z
+
+__device__ __forceinline__ bool gate(int flags, int mode) {
+    if (mode == MODE_INIT) return !(flags & F_DONE);
+    if (mode == MODE_ITER) return !(flags & F_STOP);
+    return (flags & F_NEED_REPLACE) != 0;
+}
+
+__device__ __forceinline__ int block_id3() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
+__device__ __forceinline__ int nblocks3() { return gridDim.x * gridDim.y * gridDim.z; }
+__device__ __forceinline__ int tid3() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
+
+__device__ __forceinline__ void finish(SolveState* st, int status, int flags) {
+    st->status = status;
+    st->flags = flags | F_DONE | F_STOP;
+}
+
+__device__ __forceinline__ void breakdown(SolveState* st, int iteration, int flags) {
+    st->breakdown_it = iteration;
+    finish(st, RB200_BREAKDOWN, flags);
+}
+
+// Decision after a fresh r.z (precondition's return value).
+__device__ __forceinline__ void decide_rz(SolveState* st, rb200_trace* trace, double rz, int mode) {
+    int flags = st->flags;
+    const int it = st->it;
+    if (mode == MODE_INIT) {
+        st->rz = rz;  // checked at iteration 1 (src/pressure.rs:662)
+        st->flags = flags | F_REPLACED;
+        return;
+    }
+    if (mode == MODE_REPLACE) {
+        if (trace && it >= 1) {
+            trace[it - 1].rz = rz;
+            trace[it - 1].beta = 0.0;
+            trace[it - 1].replaced = 1;
+        }
+        if (!isfinite(rz) || rz <= 0.0) {
+            breakdown(st, it, flags);
+            return;
+        }
+        st->rz = rz;
+        st->flags = (flags & ~(F_STOP | F_NEED_TRUE | F_NEED_REPLACE | F_CANDIDATE)) | F_REPLACED;
+        return;
+    }
+    // MODE_ITER
+    if (flags & F_CANDIDATE) {
+        st->rz_next = rz;
+        st->flags = (flags & ~F_CANDIDATE) | F_STOP | F_NEED_TRUE;
+        return;
+    }
+    if (!isfinite(rz) || rz <= 0.0) {
+        breakdown(st, it, flags);
+        return;
+    }
+    double beta = rz / st->rz;
+    if (trace) {
+        trace[it - 1].rz = rz;
+        trace[it - 1].beta = beta;
+    }
+    st->beta = beta;
+    st->rz = rz;
+}
+
+// ------------------------------------------------------------------ init
+// Compatibility sums, threshold and the true report of p = 0
+// (src/pressure.rs:603-647). p is zeroed here.
+__global__ void __launch_bounds__(EW) k_init_sums(GridDev g, SolveState* st, const double* __restrict__ b,
+                                                  double* __restrict__ p, Partials part) {
+    __shared__ BlockReduce<3, 2> sm;
+    dd s[3] = {{0, 0}, {0, 0}, {0, 0}};
+    double m[2] = {0.0, 0.0};
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        double x = b[c];
+        p[c] = 0.0;
+        if (!isfinite(x)) m[1] = 1.0;
+        s[0] = dd_add1(s[0], x);
+        s[1] = dd_add1(s[1], fabs(x));
+        s[2] = dd_add1(s[2], x * x);
+        m[0] = fmax(m[0], fabs(x));
+    }
+    block_reduce<3, 2>(sm, s, m);
+    if (publish_and_check_last<3, 2>(part, blockIdx.x, gridDim.x, s, m)) {
+        fold_partials<3, 2>(part, gridDim.x, sm, s, m);
+        if (threadIdx.x == 0) {
+            int flags = st->flags;
+            if (m[1] != 0.0) {
+                finish(st, RB200_NONFINITE_INPUT, flags);
+                return;
+            }
+            double sum = dd_value(s[0]), sum_abs = dd_value(s[1]), sq = dd_value(s[2]);
+            double budget = (64.0 * kEps) * sum_abs;
+            if (!isfinite(sum) || !isfinite(sum_abs)) {
+                breakdown(st, 0, flags);
+                return;
+            }
+            if (fabs(sum) > budget) {
+                st->incompatible_sum = sum;
+                st->incompatible_budget = budget;
+                finish(st, RB200_INCOMPATIBLE_RHS, flags);
+                return;
+            }
+            double rhs_l2 = sqrt(sq);
+            double threshold = fmax(st->absolute, st->relative * rhs_l2);
+            if (!isfinite(rhs_l2) || !isfinite(threshold)) {
+                breakdown(st, 0, flags);
+                return;
+            }
+            st->threshold = threshold;
+            // true_report(p = 0): the product is exactly b.
+            double div = m[0] * st->dt / g.volume;
+            if (!isfinite(sq) || !isfinite(div)) {
+                breakdown(st, 0, flags);
+                return;
+            }
+            st->true_l2 = rhs_l2;
+            st->true_max = m[0];
+            st->true_div = div;
+            if (rhs_l2 <= threshold && div <= st->divergence_limit) {
+                finish(st, RB200_OK, flags);
+                return;
+            }
+            if (st->max_it == 0) {
+                finish(st, RB200_ITERATION_LIMIT, flags);
+                return;
+            }
+        }
+    }
+}
+
+// r <- src (r[0] = 0). Jacobi also forms z = r/D and r.z and decides; the
+// SGS methods leave z to their sweep kernels. Used for the initial residual
+// (MODE_INIT, src = b) and for the restart (MODE_REPLACE, src = true residual).
+template <bool JACOBI>
+__global__ void __launch_bounds__(EW) k_load_residual(GridDev g, SolveState* st, const double* b,
+                                                      double* d0, double* d1, double* __restrict__ r,
+                                                      int mode, Partials part, rb200_trace* trace) {
+    __shared__ BlockReduce<1, 0> sm;
+    const int flags = st->flags;
+    if (!gate(flags, mode)) return;
+    const double* src = mode == MODE_INIT ? b : (st->dsel ? d0 : d1);
+    dd acc[1] = {{0, 0}};
+    double none[1];
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        double rc = c == 0 ? 0.0 : src[c];
+        r[c] = rc;
+        if (JACOBI && c != 0) {
+            int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+            double z = rc / diag_at(g, i, j, k);
+            acc[0] = dd_add1(acc[0], rc * z);
+        }
+    }
+    if (!JACOBI) return;
+    block_reduce<1, 0>(sm, acc, none);
+    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, acc, none)) {
+        fold_partials<1, 0>(part, gridDim.x, sm, acc, none);
+        if (threadIdx.x == 0) decide_rz(st, trace, dd_value(acc[0]), mode);
+    }
+}
+
+// ------------------------------------------------------------ pass 1
+// direction update fused with q = K d and the curvature d.q.
+template <bool ZARRAY>
+__global__ void __launch_bounds__(TILE_THREADS) k_direction_apply(GridDev g, int zc, SolveState* st,
+                                                                  const double* __restrict__ r,
+                                                                  const double* __restrict__ zarr, double* d0,
+                                                                  double* d1, Partials part, rb200_trace* trace) {
+    __shared__ BlockReduce<1, 0> sm;
+    const int flags = st->flags;
+    if (flags & F_STOP) return;
+    const bool fresh = (flags & F_REPLACED) != 0;
+    const double beta = st->beta;
+    const int dsel = st->dsel;
+    const double* __restrict__ src = dsel ? d1 : d0;
+    double* __restrict__ dst = dsel ? d0 : d1;
+    dd acc[1] = {{0, 0}};
+    double none[1];
+    march(
+        g, zc,
+        [&](int c, int i, int j, int k) -> double {
+            if (c == 0) return 0.0;
+            double z = ZARRAY ? zarr[c] : r[c] / diag_at(g, i, j, k);
+            // src/pressure.rs:720-731: d = z (restart) or d = z + beta*d.
+            return fresh ? z : z + beta * src[c];
+        },
+        [&](int c, int i, int j, int k, const Neigh& v) {
+            double q = c == 0 ? 0.0 : apply_row(g, i, j, k, v);
+            dst[c] = v.c;
+            acc[0] = dd_add1(acc[0], v.c * q);
+        });
+    block_reduce<1, 0>(sm, acc, none);
+    const int nb = nblocks3();
+    if (publish_and_check_last<1, 0>(part, block_id3(), nb, acc, none)) {
+        fold_partials<1, 0>(part, nb, sm, acc, none);
+        if (tid3() == 0) {
+            if (flags & F_PROFILE) {
+                st->curvature = dd_value(acc[0]);
+                st->dsel = dsel ^ 1;
+                return;
+            }
+            double curvature = dd_value(acc[0]);
+            double rz = st->rz;
+            int it = st->it + 1;
+            int fl = flags & ~F_REPLACED;
+            st->curvature = curvature;
+            st->dsel = dsel ^ 1;
+            if (trace) {
+                trace[it - 1].curvature = curvature;
+                trace[it - 1].replaced = 0;
+                trace[it - 1].checked = 0;
+            }
+            // src/pressure.rs:661-668.
+            if (!isfinite(curvature) || curvature <= 0.0 || !isfinite(rz) || rz <= 0.0) {
+                breakdown(st, it, fl);
+                return;
+            }
+            double alpha = rz / curvature;
+            if (!isfinite(alpha)) {
+                breakdown(st, it, fl);
+                return;
+            }
+            if (trace) trace[it - 1].alpha = alpha;
+            st->alpha = alpha;
+            st->flags = fl;
+        }
+    }
+}
+
+// ------------------------------------------------------------ pass 2
+// p += alpha*d, r -= alpha*K d (src/pressure.rs:669-680), the recursive norm
+// and, for Jacobi, z = r/D with r.z (precondition_jacobi, :534-575).
+template <bool JACOBI>
+__global__ void __launch_bounds__(TILE_THREADS) k_update(GridDev g, int zc, SolveState* st, double* __restrict__ p,
+                                                         double* __restrict__ r, const double* d0, const double* d1,
+                                                         Partials part, rb200_trace* trace) {
+    __shared__ BlockReduce<2, 0> sm;
+    const int flags = st->flags;
+    if (flags & F_STOP) return;
+    const double alpha = st->alpha;
+    const double* __restrict__ d = st->dsel ? d1 : d0;
+    dd acc[2] = {{0, 0}, {0, 0}};
+    double none[1];
+    march(
+        g, zc, [&](int c, int, int, int) -> double { return d[c]; },
+        [&](int c, int i, int j, int k, const Neigh& v) {
+            if (c == 0) return;  // gauge row: p[0], r[0] stay 0
+            double q = apply_row(g, i, j, k, v);
+            p[c] = p[c] + alpha * v.c;
+            double rc = r[c] - alpha * q;
+            r[c] = rc;
+            acc[0] = dd_add1(acc[0], rc * rc);
+            if (JACOBI) {
+                double z = rc / diag_at(g, i, j, k);
+                acc[1] = dd_add1(acc[1], rc * z);
+            }
+        });
+    block_reduce<2, 0>(sm, acc, none);
+    const int nb = nblocks3();
+    if (publish_and_check_last<2, 0>(part, block_id3(), nb, acc, none)) {
+        fold_partials<2, 0>(part, nb, sm, acc, none);
+        if (tid3() == 0) {
+            if (flags & F_PROFILE) {
+                st->recursive_l2 = dd_value(acc[0]);
+                st->rz_next = dd_value(acc[1]);
+                return;
+            }
+            int it = st->it + 1;
+            st->it = it;
+            double recursive_l2 = sqrt(dd_value(acc[0]));
+            st->recursive_l2 = recursive_l2;
+            if (trace) trace[it - 1].recursive_l2 = recursive_l2;
+            bool candidate = recursive_l2 <= st->threshold || it == st->max_it;
+            if (JACOBI) {
+                double rz = dd_value(acc[1]);
+                if (candidate) {
+                    st->rz_next = rz;
+                    st->flags = flags | F_STOP | F_NEED_TRUE;
+                } else {
+                    decide_rz(st, trace, rz, MODE_ITER);
+                }
+            } else if (candidate) {
+                st->flags = flags | F_CANDIDATE;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ true residual
+// true_report (src/pressure.rs:432-456): t = b - K p on every cell (the gauge
+// row included), |t|_2, max|t|, max|t|*dt/V; then the acceptance and restart
+// decisions of solve_loaded (:686-715). t is kept in the spare direction
+// buffer for a restart.
+__global__ void __launch_bounds__(TILE_THREADS) k_true_residual(GridDev g, int zc, SolveState* st,
+                                                                const double* __restrict__ b,
+                                                                const double* __restrict__ p, double* d0, double* d1,
+                                                                Partials part, rb200_trace* trace) {
+    __shared__ BlockReduce<1, 1> sm;
+    const int flags = st->flags;
+    if (!(flags & F_NEED_TRUE)) return;
+    double* __restrict__ spare = st->dsel ? d0 : d1;
+    dd acc[1] = {{0, 0}};
+    double mx[1] = {0.0};
+    march(
+        g, zc, [&](int c, int, int, int) -> double { return p[c]; },
+        [&](int c, int i, int j, int k, const Neigh& v) {
+            double t = b[c] - apply_row(g, i, j, k, v);
+            spare[c] = t;
+            acc[0] = dd_add1(acc[0], t * t);
+            mx[0] = fmax(mx[0], fabs(t));
+        });
+    block_reduce<1, 1>(sm, acc, mx);
+    const int nb = nblocks3();
+    if (publish_and_check_last<1, 1>(part, block_id3(), nb, acc, mx)) {
+        fold_partials<1, 1>(part, nb, sm, acc, mx);
+        if (tid3() == 0) {
+            const int it = st->it;
+            double squared = dd_value(acc[0]);
+            double maximum = mx[0];
+            double div = maximum * st->dt / g.volume;
+            if (trace && it >= 1) trace[it - 1].checked = 1;
+            if (!isfinite(squared) || !isfinite(div)) {
+                breakdown(st, it, flags);
+                return;
+            }
+            double l2 = sqrt(squared);
+            st->true_l2 = l2;
+            st->true_max = maximum;
+            st->true_div = div;
+            if (l2 <= st->threshold && div <= st->divergence_limit) {
+                finish(st, RB200_OK, flags);
+                return;
+            }
+            bool replaced = l2 > st->threshold;
+            if (it == st->max_it) {
+                finish(st, RB200_ITERATION_LIMIT, flags);
+                return;
+            }
+            if (replaced) {
+                st->flags = (flags & ~F_NEED_TRUE) | F_NEED_REPLACE;
+                return;
+            }
+            // Keep the recurrence: precondition the recursive residual.
+            double rz = st->rz_next;
+            if (!isfinite(rz) || rz <= 0.0) {
+                breakdown(st, it, flags);
+                return;
+            }
+            double beta = rz / st->rz;
+            if (trace) {
+                trace[it - 1].rz = rz;
+                trace[it - 1].beta = beta;
+            }
+            st->beta = beta;
+            st->rz = rz;
+            st->flags = flags & ~(F_STOP | F_NEED_TRUE);
+        }
+    }
+}
+
+// ------------------------------------------------------------ red-black SGS
+// Symmetric Gauss-Seidel preconditioner in red-black order on the
+// gauge-eliminated system (cell 0, red, is removed): forward reds then blacks,
+// backward blacks then reds. With reds first, the forward red solve and the
+// backward black solve are diagonal, so M^-1 r is two half-sweeps:
+//   black:  z_b = (r_b + sum_nb w * r_nb/D_nb) / D_b
+//   red:    z_r = r_r/D_r + (sum_nb w * z_nb) / D_r
+// A symmetric M, as PCG needs; new (the reference sweeps lexicographically).
+__device__ __forceinline__ bool is_black(int i, int j, int k) { return ((i + j + k) & 1) != 0; }
+
+__global__ void __launch_bounds__(EW) k_rbsgs_black(GridDev g, SolveState* st, const double* __restrict__ r,
+                                                    double* __restrict__ z, int mode) {
+    if (!gate(st->flags, mode)) return;
+    const int s[3] = {1, g.n[0], g.n[0] * g.n[1]};
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        int ijk[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
+        if (!is_black(ijk[0], ijk[1], ijk[2])) continue;
+        double y = r[c];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (ijk[a] > 0) {
+                int nb = c - s[a];
+                int q[3] = {ijk[0], ijk[1], ijk[2]};
+                q[a] -= 1;
+                double yr = nb == 0 ? 0.0 : r[nb] / diag_at(g, q[0], q[1], q[2]);
+                y += g.weight[a] * yr;
+            }
+            if (ijk[a] + 1 < g.n[a]) {
+                int nb = c + s[a];
+                int q[3] = {ijk[0], ijk[1], ijk[2]};
+                q[a] += 1;
+                double yr = r[nb] / diag_at(g, q[0], q[1], q[2]);
+                y += g.weight[a] * yr;
+            }
+        }
+        z[c] = y / diag_at(g, ijk[0], ijk[1], ijk[2]);
+    }
+}
+
+__global__ void __launch_bounds__(EW) k_rbsgs_red_dot(GridDev g, SolveState* st, const double* __restrict__ r,
+                                                      double* __restrict__ z, int mode, Partials part,
+                                                      rb200_trace* trace) {
+    __shared__ BlockReduce<1, 0> sm;
+    if (!gate(st->flags, mode)) return;
+    const int s[3] = {1, g.n[0], g.n[0] * g.n[1]};
+    dd acc[1] = {{0, 0}};
+    double none[1];
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        int ijk[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
+        double zc;
+        if (c == 0) {
+            zc = 0.0;
+            z[0] = 0.0;
+        } else if (is_black(ijk[0], ijk[1], ijk[2])) {
+            zc = z[c];
+        } else {
+            double D = diag_at(g, ijk[0], ijk[1], ijk[2]);
+            double corr = 0.0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (ijk[a] > 0) corr += g.weight[a] * z[c - s[a]];
+                if (ijk[a] + 1 < g.n[a]) corr += g.weight[a] * z[c + s[a]];
+            }
+            zc = r[c] / D + corr / D;
+            z[c] = zc;
+        }
+        if (c != 0) acc[0] = dd_add1(acc[0], r[c] * zc);
+    }
+    block_reduce<1, 0>(sm, acc, none);
+    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, acc, none)) {
+        fold_partials<1, 0>(part, gridDim.x, sm, acc, none);
+        if (threadIdx.x == 0) decide_rz(st, trace, dd_value(acc[0]), mode);
+    }
+}
+
+// ------------------------------------------------------------ host side
+int choose_zc(const GridDev& g) {
+    const int gx = (g.n[0] + TX - 1) / TX, gy = (g.n[1] + TY - 1) / TY;
+    const int target = 148 * 4;
+    int gz = (target + gx * gy - 1) / (gx * gy);
+    if (gz < 1) gz = 1;
+    int zc = (g.n[2] + gz - 1) / gz;
+    if (zc < 2) zc = 2;
+    if (zc > g.n[2]) zc = g.n[2];
+    return zc;
+}
+
+static int ew_blocks(int n) {
+    int b = (n + EW - 1) / EW;
+    return b < 1 ? 1 : (b < EW_CAP ? b : EW_CAP);
+}
+
+PcgSolver::~PcgSolver() {
+    if (chunk_exec_) cudaGraphExecDestroy(chunk_exec_);
+    for (auto& e : ev_)
+        if (e) cudaEventDestroy(e);
+    cudaFree(b_);
+    cudaFree(p_);
+    cudaFree(r_);
+    cudaFree(d_[0]);
+    cudaFree(d_[1]);
+    cudaFree(z_);
+    cudaFree(part_.data);
+    cudaFree(part_.ticket);
+    cudaFree(st_);
+    cudaFree(d_trace_);
+    if (h_st_) cudaFreeHost(h_st_);
+}
+
+int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
+    g_ = g;
+    method_ = method;
+    stream_ = stream;
+    if (method != RB200_JACOBI_PCG_V1 && method != RB200_RBSGS_PCG) return RB200_UNSUPPORTED;
+    zc_ = choose_zc(g);
+    MarchGrid mg = march_grid(g.n, zc_);
+    part_blocks_ = std::max(mg.nblocks, EW_CAP);
+    const size_t n = size_t(g.cells);
+    auto alloc = [&](double** ptr, size_t count) -> int {
+        cudaError_t e = cudaMalloc(ptr, count * sizeof(double));
+        if (e != cudaSuccess) {
+            set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            return RB200_OUT_OF_MEMORY;
+        }
+        bytes_ += count * sizeof(double);
+        return RB200_OK;
+    };
+    int rc;
+    if ((rc = alloc(&b_, n)) || (rc = alloc(&p_, n)) || (rc = alloc(&r_, n)) || (rc = alloc(&d_[0], n)) ||
+        (rc = alloc(&d_[1], n)))
+        return rc;
+    if (method == RB200_RBSGS_PCG && (rc = alloc(&z_, n))) return rc;
+    if ((rc = alloc(&part_.data, size_t(part_blocks_) * 8))) return rc;
+    RB200_CUDA(cudaMalloc(&part_.ticket, sizeof(unsigned)));
+    RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), stream_));
+    RB200_CUDA(cudaMalloc(&st_, sizeof(SolveState)));
+    RB200_CUDA(cudaMallocHost(&h_st_, 2 * sizeof(SolveState)));
+    RB200_CUDA(cudaMemsetAsync(d_[0], 0, n * sizeof(double), stream_));
+    RB200_CUDA(cudaMemsetAsync(d_[1], 0, n * sizeof(double), stream_));
+    for (auto& e : ev_) RB200_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    chunk_ = g.cells >= (1 << 20) ? 32 : 16;
+    return capture_chunk();
+}
+
+int PcgSolver::set_trace(rb200_trace* host, size_t capacity) {
+    if (d_trace_) {
+        cudaFree(d_trace_);
+        d_trace_ = nullptr;
+    }
+    h_trace_ = host;
+    trace_cap_ = host ? capacity : 0;
+    if (trace_cap_) RB200_CUDA(cudaMalloc(&d_trace_, trace_cap_ * sizeof(rb200_trace)));
+    if (chunk_exec_) {
+        cudaGraphExecDestroy(chunk_exec_);
+        chunk_exec_ = nullptr;
+    }
+    return capture_chunk();
+}
+
+// One chunk: `chunk_` iterations of the method's passes, then the gated
+// true-residual and restart kernels.
+int PcgSolver::capture_chunk() {
+    MarchGrid mg = march_grid(g_.n, zc_);
+    const int eb = ew_blocks(g_.cells);
+    cudaGraph_t graph = nullptr;
+    RB200_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    const bool jac = method_ == RB200_JACOBI_PCG_V1;
+    for (int q = 0; q < chunk_; ++q) {
+        if (jac) {
+            k_direction_apply<false><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, r_, nullptr, d_[0], d_[1],
+                                                                        part_, d_trace_);
+            k_update<true><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, p_, r_, d_[0], d_[1], part_, d_trace_);
+        } else {
+            k_direction_apply<true><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, r_, z_, d_[0], d_[1], part_,
+                                                                       d_trace_);
+            k_update<false><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, p_, r_, d_[0], d_[1], part_, d_trace_);
+            k_rbsgs_black<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_ITER);
+            k_rbsgs_red_dot<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_ITER, part_, d_trace_);
+        }
+    }
+    k_true_residual<<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, b_, p_, d_[0], d_[1], part_, d_trace_);
+    if (jac) {
+        k_load_residual<true><<<eb, EW, 0, stream_>>>(g_, st_, b_, d_[0], d_[1], r_, MODE_REPLACE, part_, d_trace_);
+    } else {
+        k_load_residual<false><<<eb, EW, 0, stream_>>>(g_, st_, b_, d_[0], d_[1], r_, MODE_REPLACE, part_, d_trace_);
+        k_rbsgs_black<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_REPLACE);
+        k_rbsgs_red_dot<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_REPLACE, part_, d_trace_);
+    }
+    nodes_per_chunk_ = chunk_ * (jac ? 2 : 4) + (jac ? 2 : 4);
+    cudaError_t launch_err = cudaGetLastError();
+    cudaError_t end_err = cudaStreamEndCapture(stream_, &graph);
+    if (launch_err != cudaSuccess || end_err != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        set_error(std::string("chunk capture: ") +
+                  cudaGetErrorString(launch_err != cudaSuccess ? launch_err : end_err));
+        return RB200_EXECUTION;
+    }
+    cudaError_t e = cudaGraphInstantiate(&chunk_exec_, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+        return RB200_EXECUTION;
+    }
+    return RB200_OK;
+}
+
+int PcgSolver::launch_chunk(int slot) {
+    RB200_CUDA(cudaGraphLaunch(chunk_exec_, stream_));
+    launches_ += uint64_t(nodes_per_chunk_);
+    return record_flags(slot);
+}
+
+int PcgSolver::record_flags(int slot) {
+    RB200_CUDA(cudaMemcpyAsync(&h_st_[slot], st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
+    RB200_CUDA(cudaEventRecord(ev_[slot], stream_));
+    return RB200_OK;
+}
+
+int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, rb200_cancel_fn cancelled,
+                     void* ctx) {
+    if (report) std::memset(report, 0, sizeof(*report));
+    SolveState init{};
+    init.dt = dt;
+    init.relative = s.relative_residual;
+    init.absolute = s.absolute_residual;
+    init.divergence_limit = s.divergence_limit;
+    init.max_it = s.max_iterations > 0x7fffffffull ? 0x7fffffff : int(s.max_iterations);
+    if (d_trace_ && uint64_t(init.max_it) > trace_cap_) {
+        set_error("trace capacity is smaller than max_iterations");
+        return RB200_INVALID_ARGUMENT;
+    }
+    init.status = ST_RUNNING;
+    h_st_[0] = init;
+    RB200_CUDA(cudaMemcpyAsync(st_, &h_st_[0], sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
+    if (d_trace_) RB200_CUDA(cudaMemsetAsync(d_trace_, 0, trace_cap_ * sizeof(rb200_trace), stream_));
+    const int eb = ew_blocks(g_.cells);
+    k_init_sums<<<eb, EW, 0, stream_>>>(g_, st_, b_, p_, part_);
+    if (method_ == RB200_JACOBI_PCG_V1) {
+        k_load_residual<true><<<eb, EW, 0, stream_>>>(g_, st_, b_, d_[0], d_[1], r_, MODE_INIT, part_, d_trace_);
+    } else {
+        k_load_residual<false><<<eb, EW, 0, stream_>>>(g_, st_, b_, d_[0], d_[1], r_, MODE_INIT, part_, d_trace_);
+        k_rbsgs_black<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_INIT);
+        k_rbsgs_red_dot<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_INIT, part_, d_trace_);
+    }
+    launches_ += method_ == RB200_JACOBI_PCG_V1 ? 2 : 4;
+    RB200_CUDA(cudaGetLastError());
+    // The host copy of the state must be stable before the chunk copies reuse
+    // h_st_ slots.
+    RB200_CUDA(cudaStreamSynchronize(stream_));
+    int rc;
+    if ((rc = record_flags(0))) return rc;
+    if ((rc = launch_chunk(1))) return rc;
+    int slot = 0, last_it = -1, stalls = 0, final_flags = 0;
+    bool cancelled_now = false;
+    for (;;) {
+        RB200_CUDA(cudaEventSynchronize(ev_[slot]));
+        const SolveState& h = h_st_[slot];
+        final_flags = h.flags;
+        if (h.flags & F_DONE) break;
+        if (cancelled && cancelled(ctx)) {
+            cancelled_now = true;
+            break;
+        }
+        if (h.it == last_it) {
+            if (++stalls > 4) {
+                RB200_CUDA(cudaStreamSynchronize(stream_));
+                set_error("pressure solve made no progress");
+                return RB200_EXECUTION;
+            }
+        } else {
+            stalls = 0;
+            last_it = h.it;
+        }
+        if ((rc = launch_chunk(slot))) return rc;
+        slot ^= 1;
+    }
+    (void)final_flags;
+    RB200_CUDA(cudaStreamSynchronize(stream_));
+    RB200_CUDA(cudaMemcpy(&h_st_[0], st_, sizeof(SolveState), cudaMemcpyDeviceToHost));
+    const SolveState& f = h_st_[0];
+    if (d_trace_ && h_trace_) {
+        size_t n = std::min(trace_cap_, size_t(f.it));
+        RB200_CUDA(cudaMemcpy(h_trace_, d_trace_, n * sizeof(rb200_trace), cudaMemcpyDeviceToHost));
+    }
+    if (report) {
+        report->iterations = uint64_t(f.it);
+        report->true_residual_l2 = f.true_l2;
+        report->true_residual_max = f.true_max;
+        report->predicted_divergence_max = f.true_div;
+        report->incompatible_sum = f.incompatible_sum;
+        report->incompatible_budget = f.incompatible_budget;
+        report->breakdown_iteration = uint64_t(f.breakdown_it);
+    }
+    if (cancelled_now) return RB200_CANCELLED;
+    return f.status;
+}
+
+int PcgSolver::profile(int which, int launches, double* avg_ms) {
+    if (launches < 1 || (which != 0 && which != 1)) return RB200_INVALID_ARGUMENT;
+    SolveState prof{};
+    prof.rz = 1.0;
+    prof.alpha = 1e-6;
+    prof.beta = 0.5;
+    prof.threshold = -1.0;
+    prof.max_it = 0x7fffffff;
+    prof.flags = F_PROFILE;
+    prof.status = ST_RUNNING;
+    h_st_[0] = prof;
+    RB200_CUDA(cudaMemcpyAsync(st_, &h_st_[0], sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
+    MarchGrid mg = march_grid(g_.n, zc_);
+    const bool jac = method_ == RB200_JACOBI_PCG_V1;
+    auto launch = [&]() {
+        if (which == 0) {
+            if (jac)
+                k_direction_apply<false><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, r_, nullptr, d_[0], d_[1],
+                                                                            part_, nullptr);
+            else
+                k_direction_apply<true><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, r_, z_, d_[0], d_[1], part_,
+                                                                           nullptr);
+        } else {
+            if (jac)
+                k_update<true><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, p_, r_, d_[0], d_[1], part_, nullptr);
+            else
+                k_update<false><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, p_, r_, d_[0], d_[1], part_, nullptr);
+        }
+    };
+    launch();  // warm
+    cudaEvent_t a, b;
+    RB200_CUDA(cudaEventCreate(&a));
+    RB200_CUDA(cudaEventCreate(&b));
+    RB200_CUDA(cudaEventRecord(a, stream_));
+    for (int q = 0; q < launches; ++q) launch();
+    RB200_CUDA(cudaEventRecord(b, stream_));
+    RB200_CUDA(cudaEventSynchronize(b));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    RB200_CUDA(cudaGetLastError());
+    *avg_ms = double(ms) / launches;
+    return RB200_OK;
+}
+
+}  // namespace rb200

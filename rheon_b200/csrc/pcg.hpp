@@ -1,0 +1,100 @@
+// Device-driven PCG for the gauge-eliminated sealed-box pressure system
+// (PressureWorkspace::solve_loaded, src/pressure.rs:577-740).
+#pragma once
+
+#include "internal.hpp"
+
+namespace rb200 {
+
+// Device-resident solver state. Every control decision of solve_loaded is
+// taken on the device by the last block of the kernel that produces the
+// deciding scalar; the host only pumps chunks and polls `flags`.
+struct SolveState {
+    double rz;          // r.z of the current direction
+    double rz_next;     // r.z of the recursive residual after the update
+    double alpha, beta;
+    double curvature, recursive_l2;
+    double threshold, dt, divergence_limit, relative, absolute;
+    double true_l2, true_max, true_div;
+    double incompatible_sum, incompatible_budget;
+    int it;             // completed iterations
+    int max_it;
+    int dsel;           // which direction buffer holds the current direction
+    int flags;
+    int status;         // rb200_status, or ST_RUNNING
+    int breakdown_it;
+    int pad0, pad1;
+};
+
+enum : int {
+    F_STOP = 1,          // iteration kernels are no-ops
+    F_NEED_TRUE = 2,     // evaluate the true residual b - K p
+    F_REPLACED = 4,      // the next direction is z (fresh start)
+    F_DONE = 8,          // solve finished; status is final
+    F_NEED_REPLACE = 16, // replace r by the true residual, re-precondition
+    F_PROFILE = 64       // timing mode: passes do their work, decisions are skipped
+};
+constexpr int ST_RUNNING = -1;
+
+class PcgSolver {
+public:
+    PcgSolver() = default;
+    ~PcgSolver();
+    PcgSolver(const PcgSolver&) = delete;
+    PcgSolver& operator=(const PcgSolver&) = delete;
+
+    // Allocates b, p, r, two direction buffers, partials and the state.
+    int init(const GridDev& g, int method, cudaStream_t stream);
+    // Solve K p = b for the RHS already in b(). dt is the step's dt (for the
+    // divergence gate). On return p() holds the iterate (also on
+    // ITERATION_LIMIT). `status` receives the PressureError-style outcome.
+    int solve(double dt, const rb200_settings& s, rb200_report* report, rb200_cancel_fn cancelled,
+              void* ctx);
+    double* b() { return b_; }
+    double* p() { return p_; }
+    double* scratch() { return d_[1]; }
+    size_t bytes() const { return bytes_; }
+    int set_trace(rb200_trace* host, size_t capacity);
+    // Average device time of `launches` back-to-back launches of one PCG pass
+    // (which = 0: direction+apply, 1: update), timed with CUDA events on the
+    // solver's stream, on the current vectors. Scalars are left in a timing
+    // state; the next solve() resets them.
+    int profile(int which, int launches, double* avg_ms);
+    const GridDev& grid() const { return g_; }
+    Partials partials() const { return part_; }
+    int partial_blocks() const { return part_blocks_; }
+    // Kernels launched by solve() so far (graph nodes included).
+    uint64_t launches() const { return launches_; }
+
+private:
+    int capture_chunk();
+    int launch_chunk(int slot);
+    int record_flags(int slot);
+
+    GridDev g_{};
+    int method_ = RB200_JACOBI_PCG_V1;
+    cudaStream_t stream_ = nullptr;
+    double* b_ = nullptr;
+    double* p_ = nullptr;
+    double* r_ = nullptr;
+    double* d_[2] = {nullptr, nullptr};
+    double* z_ = nullptr;  // preconditioned residual for the SGS methods
+    Partials part_{nullptr, nullptr};
+    int part_blocks_ = 0;
+    SolveState* st_ = nullptr;
+    SolveState* h_st_ = nullptr;  // pinned, one slot per in-flight chunk
+    cudaEvent_t ev_[2] = {nullptr, nullptr};
+    cudaGraphExec_t chunk_exec_ = nullptr;
+    int chunk_ = 16;
+    int zc_ = 8;
+    rb200_trace* d_trace_ = nullptr;
+    rb200_trace* h_trace_ = nullptr;
+    size_t trace_cap_ = 0;
+    size_t bytes_ = 0;
+    int nodes_per_chunk_ = 0;
+    uint64_t launches_ = 0;
+};
+
+int choose_zc(const GridDev& g);
+
+}  // namespace rb200
