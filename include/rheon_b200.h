@@ -216,6 +216,30 @@ RB200_API int rb200_workspace_set_trace(rb200_workspace* ws, rb200_trace* trace,
  * solver's scalars in a timing state; the next solve resets them. */
 RB200_API int rb200_workspace_profile(rb200_workspace* ws, int which, int launches, double* avg_ms);
 
+/* Allocation-free Jacobi-PCG solve. No counterpart in the reference.
+ *
+ * For callers that must not allocate device memory: code running while a CUDA
+ * graph is being captured in global mode (cudaMalloc is illegal then), or a
+ * host application whose device memory is owned by its own allocator under a
+ * fixed budget. It solves like rb200_workspace_solve_rhs_device with
+ * RB200_JACOBI_PCG_V1 (same kernels, same results) on caller-owned device
+ * buffers: rhs_device (read) and pressure_device (written, len doubles).
+ * It calls no cudaMalloc/cudaFree or allocating routine. Its scratch is one
+ * fixed device array of about 1.2 MB inside the library, which every GPU that
+ * loads the library holds until the process exits; grids of more than 32768
+ * cells (32^3) are rejected with RB200_UNSUPPORTED.
+ *   - The first call on a device looks up that array's device address (once
+ *     per device, with the device current); make that first call before any
+ *     stream capture begins.
+ *   - Every call shares the one array and leaves its contents behind; calls
+ *     whose work overlaps on the GPU (other threads, other streams) race and
+ *     corrupt each other. Serialize them.
+ *   - The call is synchronous: it polls the solver state from the host.
+ * `stream` is a cudaStream_t (NULL = legacy default stream). */
+RB200_API int rb200_pressure_solve_static(const rb200_grid* grid, double density, const double* rhs_device,
+                                          double* pressure_device, size_t len, double dt,
+                                          const rb200_settings* settings, rb200_report* report, void* stream);
+
 /* ----------------------------------------- PressureOperator device primitives
  * All pointers are device pointers; `stream` is a cudaStream_t (NULL = legacy).
  * These validate like the reference (walls, finiteness) and return its errors. */

@@ -123,6 +123,8 @@ SIGNATURES = {
     "rb200_workspace_pressure_device": (_P, [_P]),
     "rb200_workspace_set_trace": (_I, [_P, _P, _S]),
     "rb200_workspace_profile": (_I, [_P, _I, _I, C.POINTER(_D)]),
+    "rb200_pressure_solve_static": (_I, [C.POINTER(Grid), _D, _P, _P, _S, _D, C.POINTER(Settings),
+                                         C.POINTER(Report), _P]),
     "rb200_apply_full_device": (_I, [C.POINTER(Grid), _D, _P, _P, _P]),
     "rb200_build_rhs_f32_device": (_I, [C.POINTER(Grid), _D, _P, _P, _P, _D, _P, _P]),
     "rb200_build_rhs_f64_device": (_I, [C.POINTER(Grid), _D, _P, _P, _P, _D, _P, _P]),

@@ -13,6 +13,7 @@
 // of each captured chunk of iterations, so the host only launches graphs and
 // polls one word per chunk.
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "pcg.hpp"
@@ -727,4 +728,138 @@ int PcgSolver::profile(int which, int launches, double* avg_ms) {
     return RB200_OK;
 }
 
+// ------------------------------------------------------------ allocation-free solve
+// A Jacobi-PCG solve for callers that cannot allocate device memory: code that
+// runs while a CUDA graph is being captured in global mode (cudaMalloc is not
+// allowed then), or inside a host process whose device memory is owned by
+// another allocator under a fixed budget. Its scratch (residual, two
+// direction buffers, preconditioned residual, reduction partials, solver state
+// and ticket) lives in this fixed file-scope device array, which every GPU that
+// loads the library holds until the process exits. It has no counterpart in
+// the reference.
+constexpr int kStaticMaxCells = 32768;   // 32^3 cells
+constexpr int kStaticMaxBlocks = 2048;   // reduction partials of one pass
+constexpr size_t kStaticStateDoubles = 64;
+constexpr size_t kStaticDoubles =
+    4 * size_t(kStaticMaxCells) + size_t(kStaticMaxBlocks) * 8 + kStaticStateDoubles;
+static __device__ __align__(256) double g_static_scratch[kStaticDoubles];
+
+static_assert(sizeof(SolveState) + sizeof(unsigned) <= kStaticStateDoubles * sizeof(double),
+              "state does not fit the static scratch");
+
+// Device address of g_static_scratch per device, resolved once per device
+// with that device current. In host code the symbol itself is only a host-side
+// stand-in, never a device address.
+static double* static_scratch_address(int device, int* rc) {
+    static std::mutex mu;
+    static double* addr[64] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 0 || device >= 64) {
+        *rc = RB200_INVALID_ARGUMENT;
+        return nullptr;
+    }
+    if (!addr[device]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess || !ptr) {
+            set_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            *rc = RB200_EXECUTION;
+            return nullptr;
+        }
+        addr[device] = static_cast<double*>(ptr);
+    }
+    *rc = RB200_OK;
+    return addr[device];
+}
+
+int static_solve_jacobi(const GridDev& g, const double* rhs, double* pressure, double dt, const rb200_settings& s,
+                        rb200_report* report, cudaStream_t stream) {
+    if (g.cells > kStaticMaxCells) {
+        set_error("grid exceeds the 32768-cell limit of the allocation-free solve");
+        return RB200_UNSUPPORTED;
+    }
+    const int zc = choose_zc(g);
+    const MarchGrid mg = march_grid(g.n, zc);
+    const int eb = ew_blocks(g.cells);
+    if (mg.nblocks > kStaticMaxBlocks || eb > kStaticMaxBlocks) {
+        set_error("grid shape needs more reduction blocks than the allocation-free solve holds");
+        return RB200_UNSUPPORTED;
+    }
+    int device = 0;
+    RB200_CUDA(cudaGetDevice(&device));
+    int rc = RB200_OK;
+    double* base = static_scratch_address(device, &rc);
+    if (rc) return rc;
+    double* r = base;
+    double* d0 = r + kStaticMaxCells;
+    double* d1 = d0 + kStaticMaxCells;
+    Partials part;
+    part.data = d1 + 2 * kStaticMaxCells;  // the fourth cell slot is reserved
+    double* state_slot = part.data + size_t(kStaticMaxBlocks) * 8;
+    SolveState* st = reinterpret_cast<SolveState*>(state_slot);
+    part.ticket = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(state_slot) + sizeof(SolveState));
+
+    SolveState init{};
+    init.dt = dt;
+    init.relative = s.relative_residual;
+    init.absolute = s.absolute_residual;
+    init.divergence_limit = s.divergence_limit;
+    init.max_it = s.max_iterations > 0x7fffffffull ? 0x7fffffff : int(s.max_iterations);
+    init.status = ST_RUNNING;
+    // The array keeps the previous call's contents: the ticket must start at 0.
+    RB200_CUDA(cudaMemsetAsync(part.ticket, 0, sizeof(unsigned), stream));
+    RB200_CUDA(cudaMemcpyAsync(st, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream));
+    k_init_sums<<<eb, EW, 0, stream>>>(g, st, rhs, pressure, part);
+    k_load_residual<true><<<eb, EW, 0, stream>>>(g, st, rhs, d0, d1, r, MODE_INIT, part, nullptr);
+    RB200_CUDA(cudaGetLastError());
+    const int chunk = 16;
+    int last_it = -1, stalls = 0;
+    SolveState h{};
+    for (;;) {
+        RB200_CUDA(cudaMemcpyAsync(&h, st, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+        RB200_CUDA(cudaStreamSynchronize(stream));
+        if (h.flags & F_DONE) break;
+        if (h.it == last_it) {
+            if (++stalls > 4) {
+                set_error("pressure solve made no progress");
+                return RB200_EXECUTION;
+            }
+        } else {
+            stalls = 0;
+            last_it = h.it;
+        }
+        for (int q = 0; q < chunk; ++q) {
+            k_direction_apply<false><<<mg.grid, mg.block, 0, stream>>>(g, zc, st, r, nullptr, d0, d1, part, nullptr);
+            k_update<true><<<mg.grid, mg.block, 0, stream>>>(g, zc, st, pressure, r, d0, d1, part, nullptr);
+        }
+        k_true_residual<<<mg.grid, mg.block, 0, stream>>>(g, zc, st, rhs, pressure, d0, d1, part, nullptr);
+        k_load_residual<true><<<eb, EW, 0, stream>>>(g, st, rhs, d0, d1, r, MODE_REPLACE, part, nullptr);
+        RB200_CUDA(cudaGetLastError());
+    }
+    if (report) {
+        std::memset(report, 0, sizeof(*report));
+        report->iterations = uint64_t(h.it);
+        report->true_residual_l2 = h.true_l2;
+        report->true_residual_max = h.true_max;
+        report->predicted_divergence_max = h.true_div;
+        report->incompatible_sum = h.incompatible_sum;
+        report->incompatible_budget = h.incompatible_budget;
+        report->breakdown_iteration = uint64_t(h.breakdown_it);
+    }
+    return h.status;
+}
+
 }  // namespace rb200
+
+extern "C" int rb200_pressure_solve_static(const rb200_grid* grid, double density, const double* rhs_device,
+                                           double* pressure_device, size_t len, double dt,
+                                           const rb200_settings* settings, rb200_report* report, void* stream) {
+    using namespace rb200;
+    if (!grid || !rhs_device || !pressure_device || !settings) return RB200_INVALID_ARGUMENT;
+    GridDev g;
+    int rc = make_grid_dev(grid, density, &g);
+    if (rc) return rc;
+    if (len != size_t(g.cells)) return RB200_LENGTH_MISMATCH;
+    if (!std::isfinite(dt) || dt <= 0.0 || !settings_valid(settings)) return RB200_INVALID_ARGUMENT;
+    return static_solve_jacobi(g, rhs_device, pressure_device, dt, *settings, report, (cudaStream_t)stream);
+}
