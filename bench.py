@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of CPU work for the CPU baseline")
+    ap.add_argument("--max-iters", type=int, default=0,
+                    help="cap PCG iterations per step (profiling runs only; 0 = solve to 1e-8)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-profile", action="store_true")
     return ap.parse_args()
 
 
@@ -124,6 +128,46 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def run_e2e(args, g, cfg, faces, prm, flush, local, world):
+    """Same metric through the public API with host buffers: per step, H2D of
+    the step's input faces from pinned memory, the step, D2H of the result."""
+    import torch
+
+    import rheon_b200 as R
+
+    pinned = [torch.from_numpy(f).pin_memory() for f in faces]
+    sim = R.CarrierSimulation(g, cfg)
+    sim.upload(faces)
+    ptrs = [int(p.data_ptr()) for p in pinned]
+    for _ in range(max(1, args.warmup)):
+        sim.upload_ptrs(*ptrs)
+        sim.step(prm)
+        sim.download_ptrs(*ptrs)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    total = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.upload_ptrs(*ptrs)
+        sim.step(prm)
+        sim.download_ptrs(*ptrs)
+        b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b)
+    sim.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([total], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total = float(tt.item())
+    return total
+
+
 # ------------------------------------------------------------------ our arm
 def run_ours(args, world, rank, local):
     import torch
@@ -137,13 +181,13 @@ def run_ours(args, world, rank, local):
     dtype = np.float64 if args.storage == "f64" else np.float32
     faces = W.fourier_faces(n, seed=args.seed + rank, dtype=dtype)
     method = R.PressureImplementation.JACOBI_PCG_V1 if args.method == "jacobi" else R.PressureImplementation.RBSGS_PCG
-    settings = R.PressureSettings(1e-8, 0.0, MAXF, 1000000)
+    settings = R.PressureSettings(1e-8, 0.0, MAXF, args.max_iters if args.max_iters > 0 else 1000000)
     cfg = R.CarrierConfig(pressure=settings, storage=args.storage, implementation=method, device=local,
                           max_courant=1.0)
     sim = R.CarrierSimulation(g, cfg)
     sim.upload(faces)
     stream = torch.cuda.ExternalStream(sim.stream(), device=local)
-    prm = R.StepParams(MAXF, cfl=0.5)
+    prm = R.StepParams(MAXF, cfl=0.5, iteration_limit_ok=args.max_iters > 0)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 256 MB > 126 MB L2
 
     def barrier():
@@ -189,43 +233,18 @@ def run_ours(args, world, rank, local):
     # roofline of the dominant kernel (PCG pass 2: update + preconditioner + dots),
     # timed on the carrier's stream on the current vectors.
     hbm, hbm_kind = peaks()
-    pass_ms = {0: sim.profile(0, 50), 1: sim.profile(1, 50)}
-    bytes_pass = {0: 24 * cells, 1: 40 * cells}
+    launches_prof = 3 if args.no_profile else 50
+    pass_ms = {0: sim.profile(0, launches_prof), 1: sim.profile(1, launches_prof)}
+    # algorithmic bytes: pass 1 reads z, d_old and writes d_new (24N); pass 2
+    # reads p, d, r and writes p, r, z (48N)
+    bytes_pass = {0: 24 * cells, 1: 48 * cells}
     dominant = 1 if pass_ms[1] >= pass_ms[0] else 0
     achieved = bytes_pass[dominant] / (pass_ms[dominant] / 1e3) / 1e9
 
     # end to end through the public API with host buffers: per step, H2D of the
     # step's input faces from pinned memory, the step, D2H of the corrected faces.
-    pinned = [torch.from_numpy(f).pin_memory() for f in faces]
-    sim_e2e = R.CarrierSimulation(g, cfg)
-    sim_e2e.upload(faces)
-    for _ in range(max(1, args.warmup)):
-        sim_e2e.upload_ptrs(*[int(p.data_ptr()) for p in pinned])
-        sim_e2e.step(prm)
-        sim_e2e.download_ptrs(*[int(p.data_ptr()) for p in pinned])
-    torch.cuda.synchronize()
-    e2e_ms = 0.0
-    e2e_stream = torch.cuda.ExternalStream(sim_e2e.stream(), device=local)
-    for _ in range(args.steps):
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(e2e_stream)
-        sim_e2e.upload_ptrs(*[int(p.data_ptr()) for p in pinned])
-        sim_e2e.step(prm)
-        sim_e2e.download_ptrs(*[int(p.data_ptr()) for p in pinned])
-        b.record(e2e_stream)
-        b.synchronize()
-        e2e_ms += a.elapsed_time(b)
-    if world > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
     face_bytes = sum(f.nbytes for f in faces)
-    sim_e2e.close()
+    e2e_ms = float("nan") if args.no_e2e else run_e2e(args, g, cfg, faces, prm, flush, local, world)
 
     variants = {}
     if not args.no_variants and rank == 0 and world == 1:
@@ -286,7 +305,7 @@ def run_ours(args, world, rank, local):
             "other_pass_ms": pass_ms[1 - dominant],
             "note": "vectors of a 128^3 solve (5 x 16.8 MB) stay resident in the 126 MB L2 across passes",
         },
-        "e2e": {
+        "e2e": None if args.no_e2e else {
             "value": world * cells * args.steps / (e2e_ms / 1e3),
             "unit": UNIT,
             "h2d_bytes_per_step": face_bytes,

@@ -337,7 +337,7 @@ int rb200_workspace_create(const rb200_grid* grid, double density, int method, u
         return RB200_UNSUPPORTED;
     }
     // Six f64 cell arrays at most (b, p, r, two directions, z) plus partials.
-    uint64_t need = uint64_t(g.cells) * (method == RB200_RBSGS_PCG ? 48 : 40);
+    uint64_t need = uint64_t(g.cells) * 48;
     if (need > memory_limit) {
         set_error("device buffers exceed the memory limit");
         return RB200_OUT_OF_MEMORY;

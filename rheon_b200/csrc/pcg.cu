@@ -1,22 +1,24 @@
 // Device-driven gauge-eliminated PCG (PressureWorkspace::solve_loaded,
 // src/pressure.rs:577-740) on the sealed-box operator.
 //
-// One PCG iteration of the Jacobi method is two marching passes:
-//   pass 1  d <- z + beta*d (z = r/D recomputed, never stored), q = K d,
-//           curvature = d.q                                     (24N bytes)
-//   pass 2  q = K d recomputed from d, p += alpha*d, r -= alpha*q,
-//           z = r/D, r.r and r.z                                 (40N bytes)
-// instead of the four array passes of the reference (88N). Scalars never leave
+// One PCG iteration of the Jacobi method is two slab passes:
+//   pass 1  d <- z + beta*d, q = K d, curvature = d.q           (24N bytes)
+//   pass 2  q = K d re-applied from d, p += alpha*d, r -= alpha*q,
+//           z = r/D stored, r.r and r.z                         (48N bytes)
+// instead of the four array passes of the reference (88N); q is never stored. Scalars never leave
 // the device: the last block of each pass takes solve_loaded's decision
 // (alpha, beta, breakdown, candidate, restart) and writes it to SolveState.
 // The true-residual check and the restart run as flag-gated kernels at the end
 // of each captured chunk of iterations, so the host only launches graphs and
 // polls one word per chunk.
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <mutex>
 #include <vector>
 
 #include "pcg.hpp"
+#include "slab.cuh"
 #include "stencil.cuh"
 
 namespace rb200 {
@@ -156,44 +158,109 @@ __global__ void __launch_bounds__(EW) k_init_sums(GridDev g, SolveState* st, con
     }
 }
 
-// r <- src (r[0] = 0). Jacobi also forms z = r/D and r.z and decides; the
-// SGS methods leave z to their sweep kernels. Used for the initial residual
-// (MODE_INIT, src = b) and for the restart (MODE_REPLACE, src = true residual).
+// r <- src (r[0] = 0) and the preconditioned start. Jacobi stores z = r/D and
+// reduces r.z, then decides; the red-black SGS method stores y = r/D on the
+// red cells (its forward red solve) and leaves the rest to its sweep kernels.
+// Used for the initial residual (MODE_INIT, src = b) and for the restart
+// (MODE_REPLACE, src = the true residual in the spare direction buffer).
 template <bool JACOBI>
 __global__ void __launch_bounds__(EW) k_load_residual(GridDev g, SolveState* st, const double* b,
                                                       double* d0, double* d1, double* __restrict__ r,
-                                                      int mode, Partials part, rb200_trace* trace) {
+                                                      double* __restrict__ z, int mode, Partials part,
+                                                      rb200_trace* trace) {
     __shared__ BlockReduce<1, 0> sm;
     const int flags = st->flags;
     if (!gate(flags, mode)) return;
     const double* src = mode == MODE_INIT ? b : (st->dsel ? d0 : d1);
-    dd acc[1] = {{0, 0}};
-    double none[1];
+    Neu acc;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
         double rc = c == 0 ? 0.0 : src[c];
         r[c] = rc;
-        if (JACOBI && c != 0) {
-            int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
-            double z = rc / diag_at(g, i, j, k);
-            acc[0] = dd_add1(acc[0], rc * z);
+        if (c == 0) {
+            z[0] = 0.0;
+            continue;
+        }
+        int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+        if (JACOBI) {
+            double zc = rc / diag_at(g, i, j, k);
+            z[c] = zc;
+            acc.add(rc * zc);
+        } else if (((i + j + k) & 1) == 0) {
+            z[c] = rc / diag_at(g, i, j, k);
         }
     }
     if (!JACOBI) return;
-    block_reduce<1, 0>(sm, acc, none);
-    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, acc, none)) {
-        fold_partials<1, 0>(part, gridDim.x, sm, acc, none);
-        if (threadIdx.x == 0) decide_rz(st, trace, dd_value(acc[0]), mode);
+    dd sums[1] = {acc.as_dd()};
+    double none[1];
+    block_reduce<1, 0>(sm, sums, none);
+    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
+        fold_partials<1, 0>(part, gridDim.x, sm, sums, none);
+        if (threadIdx.x == 0) decide_rz(st, trace, dd_value(sums[0]), mode);
     }
 }
 
+// ------------------------------------------------------------ slab staging
+// Stage one or two slabs of the block's brick into shared memory.
+template <int ZC>
+__device__ __forceinline__ void stage_issue(const GridDev& g, const TmaMaps& maps, uint64_t* bar, double* sm0,
+                                            const double* src0, const CUtensorMap* m0, double* sm1,
+                                            const double* src1, const CUtensorMap* m1, int x0, int y0, int k0) {
+    const int tid = threadIdx.x + TX * threadIdx.y;
+    if (maps.use) {
+        if (tid == 0) {
+            mbar_init(bar, 1);
+            fence_mbar_init();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            mbar_expect_tx(bar, (sm1 ? 2u : 1u) * Slab<ZC>::BYTES);
+            tma_load_slab(sm0, m0, x0 - 2, y0 - 1, k0 - 1, bar);
+            if (sm1) tma_load_slab(sm1, m1, x0 - 2, y0 - 1, k0 - 1, bar);
+        }
+    } else {
+        slab_issue_rows<ZC>(g, sm0, src0, x0, y0, k0);
+        if (sm1) slab_issue_rows<ZC>(g, sm1, src1, x0, y0, k0);
+        cp_async_commit();
+    }
+}
+
+// Wait for the staged slabs. A TMA wait that runs out records an execution
+// error in the solver state, waits once more for the copy in flight, and the
+// whole block returns false (the decision is block-uniform).
+__device__ __forceinline__ bool stage_wait(const TmaMaps& maps, uint64_t* bar, SolveState* st) {
+    bool ok = true;
+    if (maps.use)
+        ok = mbar_wait_bounded(bar, 0);
+    else
+        cp_async_wait_all();
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            st->status = RB200_EXECUTION;
+            st->flags = st->flags | F_DONE | F_STOP;
+        }
+        mbar_wait_bounded(bar, 0);
+        __syncthreads();
+    }
+    return ok;
+}
+
 // ------------------------------------------------------------ pass 1
-// direction update fused with q = K d and the curvature d.q.
-template <bool ZARRAY>
-__global__ void __launch_bounds__(TILE_THREADS) k_direction_apply(GridDev g, int zc, SolveState* st,
-                                                                  const double* __restrict__ r,
-                                                                  const double* __restrict__ zarr, double* d0,
-                                                                  double* d1, Partials part, rb200_trace* trace) {
-    __shared__ BlockReduce<1, 0> sm;
+// Direction update fused with q = K d and the curvature d.q
+// (src/pressure.rs:657-668, :720-731). The slabs hold z and the old direction;
+// the new direction d = z (restart) or z + beta*d is formed in shared memory
+// for the whole slab (out-of-domain and gauge entries are 0 in both inputs, so
+// they stay 0), then each cell's row of K d is applied.
+template <int ZC>
+__global__ void __launch_bounds__(TILE_THREADS) k_pass1(GridDev g, SolveState* st, const double* __restrict__ zarr,
+                                                        double* d0, double* d1, const __grid_constant__ TmaMaps maps,
+                                                        Partials part, rb200_trace* trace) {
+    using S = Slab<ZC>;
+    extern __shared__ __align__(128) double smem[];
+    __shared__ BlockReduce<1, 0> red;
+    __shared__ __align__(8) uint64_t bar;
+    double* sz = smem;
+    double* sd = smem + S::SIZE;
     const int flags = st->flags;
     if (flags & F_STOP) return;
     const bool fresh = (flags & F_REPLACED) != 0;
@@ -201,32 +268,41 @@ __global__ void __launch_bounds__(TILE_THREADS) k_direction_apply(GridDev g, int
     const int dsel = st->dsel;
     const double* __restrict__ src = dsel ? d1 : d0;
     double* __restrict__ dst = dsel ? d0 : d1;
-    dd acc[1] = {{0, 0}};
-    double none[1];
-    march(
-        g, zc,
-        [&](int c, int i, int j, int k) -> double {
-            if (c == 0) return 0.0;
-            double z = ZARRAY ? zarr[c] : r[c] / diag_at(g, i, j, k);
-            // src/pressure.rs:720-731: d = z (restart) or d = z + beta*d.
-            return fresh ? z : z + beta * src[c];
-        },
-        [&](int c, int i, int j, int k, const Neigh& v) {
-            double q = c == 0 ? 0.0 : apply_row(g, i, j, k, v);
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, k0 = blockIdx.z * ZC;
+    stage_issue<ZC>(g, maps, &bar, sz, zarr, &maps.z, fresh ? nullptr : sd, src, dsel ? &maps.d1 : &maps.d0, x0,
+                    y0, k0);
+    if (!stage_wait(maps, &bar, st)) return;
+    const int tid = threadIdx.x + TX * threadIdx.y;
+    if (!fresh)
+        for (int e = tid; e < S::SIZE; e += TILE_THREADS) sz[e] = sz[e] + beta * sd[e];
+    __syncthreads();
+    Neu acc;
+    const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
+    if (i < g.n[0] && j < g.n[1]) {
+        const int kend = min(ZC, g.n[2] - k0);
+        int e = S::own(threadIdx.x, threadIdx.y, 0);
+        int c = cell_idx(g, i, j, k0);
+        const int plane = g.n[0] * g.n[1];
+        for (int q = 0; q < kend; ++q, e += S::PLANE, c += plane) {
+            Neigh v = slab_neigh<ZC>(sz, e);
+            double qv = c == 0 ? 0.0 : apply_row(g, i, j, k0 + q, v);
             dst[c] = v.c;
-            acc[0] = dd_add1(acc[0], v.c * q);
-        });
-    block_reduce<1, 0>(sm, acc, none);
+            acc.add(v.c * qv);
+        }
+    }
+    dd sums[1] = {acc.as_dd()};
+    double none[1];
+    block_reduce<1, 0>(red, sums, none);
     const int nb = nblocks3();
-    if (publish_and_check_last<1, 0>(part, block_id3(), nb, acc, none)) {
-        fold_partials<1, 0>(part, nb, sm, acc, none);
+    if (publish_and_check_last<1, 0>(part, block_id3(), nb, sums, none)) {
+        fold_partials<1, 0>(part, nb, red, sums, none);
         if (tid3() == 0) {
+            double curvature = dd_value(sums[0]);
             if (flags & F_PROFILE) {
-                st->curvature = dd_value(acc[0]);
+                st->curvature = curvature;
                 st->dsel = dsel ^ 1;
                 return;
             }
-            double curvature = dd_value(acc[0]);
             double rz = st->rz;
             int it = st->it + 1;
             int fl = flags & ~F_REPLACED;
@@ -255,51 +331,82 @@ __global__ void __launch_bounds__(TILE_THREADS) k_direction_apply(GridDev g, int
 }
 
 // ------------------------------------------------------------ pass 2
-// p += alpha*d, r -= alpha*K d (src/pressure.rs:669-680), the recursive norm
-// and, for Jacobi, z = r/D with r.z (precondition_jacobi, :534-575).
-template <bool JACOBI>
-__global__ void __launch_bounds__(TILE_THREADS) k_update(GridDev g, int zc, SolveState* st, double* __restrict__ p,
-                                                         double* __restrict__ r, const double* d0, const double* d1,
-                                                         Partials part, rb200_trace* trace) {
-    __shared__ BlockReduce<2, 0> sm;
+// p += alpha*d, r -= alpha*K d (src/pressure.rs:669-680) with K d re-applied
+// from the direction slab, the recursive norm, and the preconditioner's local
+// part: Jacobi z = r/D with r.z (precondition_jacobi, :534-575); red-black SGS
+// stores y = r/D on the red cells.
+template <int ZC, bool JACOBI>
+__global__ void __launch_bounds__(TILE_THREADS) k_pass2(GridDev g, SolveState* st, double* __restrict__ p,
+                                                        double* __restrict__ r, double* __restrict__ z,
+                                                        const double* d0, const double* d1,
+                                                        const __grid_constant__ TmaMaps maps, Partials part,
+                                                        rb200_trace* trace) {
+    using S = Slab<ZC>;
+    extern __shared__ __align__(128) double smem[];
+    __shared__ BlockReduce<2, 0> red;
+    __shared__ __align__(8) uint64_t bar;
     const int flags = st->flags;
     if (flags & F_STOP) return;
     const double alpha = st->alpha;
-    const double* __restrict__ d = st->dsel ? d1 : d0;
-    dd acc[2] = {{0, 0}, {0, 0}};
+    const int dsel = st->dsel;
+    const double* __restrict__ d = dsel ? d1 : d0;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, k0 = blockIdx.z * ZC;
+    stage_issue<ZC>(g, maps, &bar, smem, d, dsel ? &maps.d1 : &maps.d0, nullptr, nullptr, nullptr, x0, y0, k0);
+    const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
+    const bool own = i < g.n[0] && j < g.n[1];
+    const int kend = own ? min(ZC, g.n[2] - k0) : 0;
+    const int plane = g.n[0] * g.n[1];
+    const int c0 = own ? cell_idx(g, i, j, k0) : 0;
+    double pv[ZC], rv[ZC];
+#pragma unroll
+    for (int q = 0; q < ZC; ++q) {
+        if (q < kend) {
+            pv[q] = p[c0 + q * plane];
+            rv[q] = r[c0 + q * plane];
+        }
+    }
+    if (!stage_wait(maps, &bar, st)) return;
+    Neu acc_rr, acc_rz;
+#pragma unroll
+    for (int q = 0; q < ZC; ++q) {
+        if (q >= kend) break;
+        const int c = c0 + q * plane;
+        if (c == 0) continue;  // gauge row: p[0], r[0] stay 0
+        Neigh v = slab_neigh<ZC>(smem, S::own(threadIdx.x, threadIdx.y, q));
+        const int k = k0 + q;
+        double qv = apply_row(g, i, j, k, v);
+        p[c] = pv[q] + alpha * v.c;
+        double rc = rv[q] - alpha * qv;
+        r[c] = rc;
+        acc_rr.add(rc * rc);
+        if (JACOBI) {
+            double zc = rc / diag_at(g, i, j, k);
+            z[c] = zc;
+            acc_rz.add(rc * zc);
+        } else if (((i + j + k) & 1) == 0) {
+            z[c] = rc / diag_at(g, i, j, k);
+        }
+    }
+    dd sums[2] = {acc_rr.as_dd(), acc_rz.as_dd()};
     double none[1];
-    march(
-        g, zc, [&](int c, int, int, int) -> double { return d[c]; },
-        [&](int c, int i, int j, int k, const Neigh& v) {
-            if (c == 0) return;  // gauge row: p[0], r[0] stay 0
-            double q = apply_row(g, i, j, k, v);
-            p[c] = p[c] + alpha * v.c;
-            double rc = r[c] - alpha * q;
-            r[c] = rc;
-            acc[0] = dd_add1(acc[0], rc * rc);
-            if (JACOBI) {
-                double z = rc / diag_at(g, i, j, k);
-                acc[1] = dd_add1(acc[1], rc * z);
-            }
-        });
-    block_reduce<2, 0>(sm, acc, none);
+    block_reduce<2, 0>(red, sums, none);
     const int nb = nblocks3();
-    if (publish_and_check_last<2, 0>(part, block_id3(), nb, acc, none)) {
-        fold_partials<2, 0>(part, nb, sm, acc, none);
+    if (publish_and_check_last<2, 0>(part, block_id3(), nb, sums, none)) {
+        fold_partials<2, 0>(part, nb, red, sums, none);
         if (tid3() == 0) {
             if (flags & F_PROFILE) {
-                st->recursive_l2 = dd_value(acc[0]);
-                st->rz_next = dd_value(acc[1]);
+                st->recursive_l2 = dd_value(sums[0]);
+                st->rz_next = dd_value(sums[1]);
                 return;
             }
             int it = st->it + 1;
             st->it = it;
-            double recursive_l2 = sqrt(dd_value(acc[0]));
+            double recursive_l2 = sqrt(dd_value(sums[0]));
             st->recursive_l2 = recursive_l2;
             if (trace) trace[it - 1].recursive_l2 = recursive_l2;
             bool candidate = recursive_l2 <= st->threshold || it == st->max_it;
             if (JACOBI) {
-                double rz = dd_value(acc[1]);
+                double rz = dd_value(sums[1]);
                 if (candidate) {
                     st->rz_next = rz;
                     st->flags = flags | F_STOP | F_NEED_TRUE;
@@ -318,31 +425,45 @@ __global__ void __launch_bounds__(TILE_THREADS) k_update(GridDev g, int zc, Solv
 // row included), |t|_2, max|t|, max|t|*dt/V; then the acceptance and restart
 // decisions of solve_loaded (:686-715). t is kept in the spare direction
 // buffer for a restart.
-__global__ void __launch_bounds__(TILE_THREADS) k_true_residual(GridDev g, int zc, SolveState* st,
-                                                                const double* __restrict__ b,
+template <int ZC>
+__global__ void __launch_bounds__(TILE_THREADS) k_true_residual(GridDev g, SolveState* st, const double* __restrict__ b,
                                                                 const double* __restrict__ p, double* d0, double* d1,
-                                                                Partials part, rb200_trace* trace) {
-    __shared__ BlockReduce<1, 1> sm;
+                                                                const __grid_constant__ TmaMaps maps, Partials part,
+                                                                rb200_trace* trace) {
+    using S = Slab<ZC>;
+    extern __shared__ __align__(128) double smem[];
+    __shared__ BlockReduce<1, 1> red;
+    __shared__ __align__(8) uint64_t bar;
     const int flags = st->flags;
     if (!(flags & F_NEED_TRUE)) return;
     double* __restrict__ spare = st->dsel ? d0 : d1;
-    dd acc[1] = {{0, 0}};
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, k0 = blockIdx.z * ZC;
+    stage_issue<ZC>(g, maps, &bar, smem, p, &maps.p, nullptr, nullptr, nullptr, x0, y0, k0);
+    if (!stage_wait(maps, &bar, st)) return;
+    Neu acc;
     double mx[1] = {0.0};
-    march(
-        g, zc, [&](int c, int, int, int) -> double { return p[c]; },
-        [&](int c, int i, int j, int k, const Neigh& v) {
-            double t = b[c] - apply_row(g, i, j, k, v);
+    const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
+    if (i < g.n[0] && j < g.n[1]) {
+        const int kend = min(ZC, g.n[2] - k0);
+        const int plane = g.n[0] * g.n[1];
+        int c = cell_idx(g, i, j, k0);
+        int e = S::own(threadIdx.x, threadIdx.y, 0);
+        for (int q = 0; q < kend; ++q, e += S::PLANE, c += plane) {
+            Neigh v = slab_neigh<ZC>(smem, e);
+            double t = b[c] - apply_row(g, i, j, k0 + q, v);
             spare[c] = t;
-            acc[0] = dd_add1(acc[0], t * t);
+            acc.add(t * t);
             mx[0] = fmax(mx[0], fabs(t));
-        });
-    block_reduce<1, 1>(sm, acc, mx);
+        }
+    }
+    dd sums[1] = {acc.as_dd()};
+    block_reduce<1, 1>(red, sums, mx);
     const int nb = nblocks3();
-    if (publish_and_check_last<1, 1>(part, block_id3(), nb, acc, mx)) {
-        fold_partials<1, 1>(part, nb, sm, acc, mx);
+    if (publish_and_check_last<1, 1>(part, block_id3(), nb, sums, mx)) {
+        fold_partials<1, 1>(part, nb, red, sums, mx);
         if (tid3() == 0) {
             const int it = st->it;
-            double squared = dd_value(acc[0]);
+            double squared = dd_value(sums[0]);
             double maximum = mx[0];
             double div = maximum * st->dt / g.volume;
             if (trace && it >= 1) trace[it - 1].checked = 1;
@@ -389,9 +510,10 @@ __global__ void __launch_bounds__(TILE_THREADS) k_true_residual(GridDev g, int z
 // Symmetric Gauss-Seidel preconditioner in red-black order on the
 // gauge-eliminated system (cell 0, red, is removed): forward reds then blacks,
 // backward blacks then reds. With reds first, the forward red solve and the
-// backward black solve are diagonal, so M^-1 r is two half-sweeps:
-//   black:  z_b = (r_b + sum_nb w * r_nb/D_nb) / D_b
-//   red:    z_r = r_r/D_r + (sum_nb w * z_nb) / D_r
+// backward black solve are diagonal, so M^-1 r is
+//   red:    y_r = r_r/D_r                     (stored by the pass that forms r)
+//   black:  z_b = (r_b + sum_nb w * y_nb) / D_b
+//   red:    z_r = y_r + (sum_nb w * z_nb) / D_r
 // A symmetric M, as PCG needs; new (the reference sweeps lexicographically).
 __device__ __forceinline__ bool is_black(int i, int j, int k) { return ((i + j + k) & 1) != 0; }
 
@@ -405,20 +527,8 @@ __global__ void __launch_bounds__(EW) k_rbsgs_black(GridDev g, SolveState* st, c
         double y = r[c];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            if (ijk[a] > 0) {
-                int nb = c - s[a];
-                int q[3] = {ijk[0], ijk[1], ijk[2]};
-                q[a] -= 1;
-                double yr = nb == 0 ? 0.0 : r[nb] / diag_at(g, q[0], q[1], q[2]);
-                y += g.weight[a] * yr;
-            }
-            if (ijk[a] + 1 < g.n[a]) {
-                int nb = c + s[a];
-                int q[3] = {ijk[0], ijk[1], ijk[2]};
-                q[a] += 1;
-                double yr = r[nb] / diag_at(g, q[0], q[1], q[2]);
-                y += g.weight[a] * yr;
-            }
+            if (ijk[a] > 0) y += g.weight[a] * z[c - s[a]];
+            if (ijk[a] + 1 < g.n[a]) y += g.weight[a] * z[c + s[a]];
         }
         z[c] = y / diag_at(g, ijk[0], ijk[1], ijk[2]);
     }
@@ -430,51 +540,179 @@ __global__ void __launch_bounds__(EW) k_rbsgs_red_dot(GridDev g, SolveState* st,
     __shared__ BlockReduce<1, 0> sm;
     if (!gate(st->flags, mode)) return;
     const int s[3] = {1, g.n[0], g.n[0] * g.n[1]};
-    dd acc[1] = {{0, 0}};
-    double none[1];
+    Neu acc;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        if (c == 0) continue;  // z[0] = 0 is kept by k_load_residual
         int ijk[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
-        double zc;
-        if (c == 0) {
-            zc = 0.0;
-            z[0] = 0.0;
-        } else if (is_black(ijk[0], ijk[1], ijk[2])) {
-            zc = z[c];
-        } else {
-            double D = diag_at(g, ijk[0], ijk[1], ijk[2]);
+        double zc = z[c];
+        if (!is_black(ijk[0], ijk[1], ijk[2])) {
             double corr = 0.0;
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 if (ijk[a] > 0) corr += g.weight[a] * z[c - s[a]];
                 if (ijk[a] + 1 < g.n[a]) corr += g.weight[a] * z[c + s[a]];
             }
-            zc = r[c] / D + corr / D;
+            zc = zc + corr / diag_at(g, ijk[0], ijk[1], ijk[2]);
             z[c] = zc;
         }
-        if (c != 0) acc[0] = dd_add1(acc[0], r[c] * zc);
+        acc.add(r[c] * zc);
     }
-    block_reduce<1, 0>(sm, acc, none);
-    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, acc, none)) {
-        fold_partials<1, 0>(part, gridDim.x, sm, acc, none);
-        if (threadIdx.x == 0) decide_rz(st, trace, dd_value(acc[0]), mode);
+    dd sums[1] = {acc.as_dd()};
+    double none[1];
+    block_reduce<1, 0>(sm, sums, none);
+    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
+        fold_partials<1, 0>(part, gridDim.x, sm, sums, none);
+        if (threadIdx.x == 0) decide_rz(st, trace, dd_value(sums[0]), mode);
     }
 }
 
 // ------------------------------------------------------------ host side
-int choose_zc(const GridDev& g) {
-    const int gx = (g.n[0] + TX - 1) / TX, gy = (g.n[1] + TY - 1) / TY;
-    const int target = 148 * 4;
-    int gz = (target + gx * gy - 1) / (gx * gy);
-    if (gz < 1) gz = 1;
-    int zc = (g.n[2] + gz - 1) / gz;
-    if (zc < 2) zc = 2;
-    if (zc > g.n[2]) zc = g.n[2];
-    return zc;
+constexpr int ZC = 8;
+constexpr size_t kSmemPass1 = 2 * size_t(Slab<ZC>::SIZE) * sizeof(double);
+constexpr size_t kSmemSlab = size_t(Slab<ZC>::SIZE) * sizeof(double);
+
+static dim3 slab_grid(const GridDev& g) {
+    return dim3((g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.n[2] + ZC - 1) / ZC);
+}
+int slab_blocks(const GridDev& g) {
+    dim3 d = slab_grid(g);
+    return int(d.x * d.y * d.z);
 }
 
 static int ew_blocks(int n) {
     int b = (n + EW - 1) / EW;
     return b < 1 ? 1 : (b < EW_CAP ? b : EW_CAP);
+}
+
+// Dynamic shared memory above 48 KB must be opted into per kernel.
+static int set_smem_attrs() {
+    RB200_CUDA(cudaFuncSetAttribute(k_pass1<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemPass1)));
+    RB200_CUDA(cudaFuncSetAttribute(k_pass2<ZC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemSlab)));
+    RB200_CUDA(cudaFuncSetAttribute(k_pass2<ZC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemSlab)));
+    RB200_CUDA(cudaFuncSetAttribute(k_true_residual<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(kSmemSlab)));
+    return RB200_OK;
+}
+
+struct Bufs {
+    double *b, *p, *r, *z, *d0, *d1;
+    SolveState* st;
+    Partials part;
+    rb200_trace* trace;
+    TmaMaps maps;
+};
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda). The encoder validates base, strides and box on the host.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    });
+    return fn;
+}
+
+// TMA slabs need a row pitch that is a multiple of 16 bytes (nx even) and, to
+// stay well inside the encoder's documented limits, a grid at least one box
+// large in every direction. Other grids take the cp.async path.
+static bool tma_eligible(const GridDev& g) {
+    return (g.n[0] % 2) == 0 && g.n[0] >= Slab<ZC>::SX && g.n[1] >= Slab<ZC>::SY && g.n[2] >= Slab<ZC>::SZ;
+}
+
+static bool encode_slab_map(CUtensorMap* m, const double* base, const GridDev& g) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    cuuint64_t dims[3] = {cuuint64_t(g.n[0]), cuuint64_t(g.n[1]), cuuint64_t(g.n[2])};
+    cuuint64_t strides[2] = {cuuint64_t(g.n[0]) * 8, cuuint64_t(g.n[0]) * cuuint64_t(g.n[1]) * 8};
+    cuuint32_t box[3] = {cuuint32_t(Slab<ZC>::SX), cuuint32_t(Slab<ZC>::SY), cuuint32_t(Slab<ZC>::SZ)};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+static TmaMaps make_maps(const GridDev& g, const double* z, const double* d0, const double* d1, const double* p) {
+    TmaMaps m;
+    std::memset(&m, 0, sizeof(m));
+    if (tma_eligible(g) && encode_slab_map(&m.z, z, g) && encode_slab_map(&m.d0, d0, g) &&
+        encode_slab_map(&m.d1, d1, g) && encode_slab_map(&m.p, p, g))
+        m.use = 1;
+    else
+        std::memset(&m, 0, sizeof(m));
+    return m;
+}
+
+// Initial residual and preconditioned start (src/pressure.rs:603-650).
+static void launch_start(const GridDev& g, bool jac, const Bufs& B, cudaStream_t s) {
+    const int eb = ew_blocks(g.cells);
+    k_init_sums<<<eb, EW, 0, s>>>(g, B.st, B.b, B.p, B.part);
+    if (jac) {
+        k_load_residual<true><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part, B.trace);
+    } else {
+        k_load_residual<false><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part, B.trace);
+        k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_INIT);
+        k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_INIT, B.part, B.trace);
+    }
+}
+
+// One PCG iteration (src/pressure.rs:651-734).
+static int launch_iteration(const GridDev& g, bool jac, const Bufs& B, cudaStream_t s) {
+    const dim3 grid = slab_grid(g), block(TX, TY, 1);
+    k_pass1<ZC><<<grid, block, kSmemPass1, s>>>(g, B.st, B.z, B.d0, B.d1, B.maps, B.part, B.trace);
+    if (jac) {
+        k_pass2<ZC, true><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part,
+                                                         B.trace);
+        return 2;
+    }
+    const int eb = ew_blocks(g.cells);
+    k_pass2<ZC, false><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part, B.trace);
+    k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_ITER);
+    k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_ITER, B.part, B.trace);
+    return 4;
+}
+
+// The gated true-residual check and restart (src/pressure.rs:686-715).
+static int launch_check(const GridDev& g, bool jac, const Bufs& B, cudaStream_t s) {
+    const dim3 grid = slab_grid(g), block(TX, TY, 1);
+    const int eb = ew_blocks(g.cells);
+    k_true_residual<ZC><<<grid, block, kSmemSlab, s>>>(g, B.st, B.b, B.p, B.d0, B.d1, B.maps, B.part, B.trace);
+    if (jac) {
+        k_load_residual<true><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part, B.trace);
+        return 2;
+    }
+    k_load_residual<false><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part, B.trace);
+    k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_REPLACE);
+    k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_REPLACE, B.part, B.trace);
+    return 4;
+}
+
+static SolveState initial_state(double dt, const rb200_settings& s) {
+    SolveState init{};
+    init.dt = dt;
+    init.relative = s.relative_residual;
+    init.absolute = s.absolute_residual;
+    init.divergence_limit = s.divergence_limit;
+    init.max_it = s.max_iterations > 0x7fffffffull ? 0x7fffffff : int(s.max_iterations);
+    init.status = ST_RUNNING;
+    return init;
+}
+
+static void fill_report(const SolveState& f, rb200_report* report) {
+    if (!report) return;
+    std::memset(report, 0, sizeof(*report));
+    report->iterations = uint64_t(f.it);
+    report->true_residual_l2 = f.true_l2;
+    report->true_residual_max = f.true_max;
+    report->predicted_divergence_max = f.true_div;
+    report->incompatible_sum = f.incompatible_sum;
+    report->incompatible_budget = f.incompatible_budget;
+    report->breakdown_iteration = uint64_t(f.breakdown_it);
 }
 
 PcgSolver::~PcgSolver() {
@@ -499,9 +737,9 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
     method_ = method;
     stream_ = stream;
     if (method != RB200_JACOBI_PCG_V1 && method != RB200_RBSGS_PCG) return RB200_UNSUPPORTED;
-    zc_ = choose_zc(g);
-    MarchGrid mg = march_grid(g.n, zc_);
-    part_blocks_ = std::max(mg.nblocks, EW_CAP);
+    int rc = set_smem_attrs();
+    if (rc) return rc;
+    part_blocks_ = std::max(slab_blocks(g), EW_CAP);
     const size_t n = size_t(g.cells);
     auto alloc = [&](double** ptr, size_t count) -> int {
         cudaError_t e = cudaMalloc(ptr, count * sizeof(double));
@@ -512,19 +750,16 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
         bytes_ += count * sizeof(double);
         return RB200_OK;
     };
-    int rc;
-    if ((rc = alloc(&b_, n)) || (rc = alloc(&p_, n)) || (rc = alloc(&r_, n)) || (rc = alloc(&d_[0], n)) ||
-        (rc = alloc(&d_[1], n)))
+    if ((rc = alloc(&b_, n)) || (rc = alloc(&p_, n)) || (rc = alloc(&r_, n)) || (rc = alloc(&z_, n)) ||
+        (rc = alloc(&d_[0], n)) || (rc = alloc(&d_[1], n)))
         return rc;
-    if (method == RB200_RBSGS_PCG && (rc = alloc(&z_, n))) return rc;
     if ((rc = alloc(&part_.data, size_t(part_blocks_) * 8))) return rc;
     RB200_CUDA(cudaMalloc(&part_.ticket, sizeof(unsigned)));
     RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), stream_));
     RB200_CUDA(cudaMalloc(&st_, sizeof(SolveState)));
     RB200_CUDA(cudaMallocHost(&h_st_, 2 * sizeof(SolveState)));
-    RB200_CUDA(cudaMemsetAsync(d_[0], 0, n * sizeof(double), stream_));
-    RB200_CUDA(cudaMemsetAsync(d_[1], 0, n * sizeof(double), stream_));
     for (auto& e : ev_) RB200_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    maps_ = make_maps(g, z_, d_[0], d_[1], p_);
     chunk_ = g.cells >= (1 << 20) ? 32 : 16;
     return capture_chunk();
 }
@@ -544,36 +779,16 @@ int PcgSolver::set_trace(rb200_trace* host, size_t capacity) {
     return capture_chunk();
 }
 
-// One chunk: `chunk_` iterations of the method's passes, then the gated
-// true-residual and restart kernels.
+// One chunk: `chunk_` iterations, then the gated true-residual and restart.
 int PcgSolver::capture_chunk() {
-    MarchGrid mg = march_grid(g_.n, zc_);
-    const int eb = ew_blocks(g_.cells);
+    const bool jac = method_ == RB200_JACOBI_PCG_V1;
+    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], st_, part_, d_trace_, maps_};
     cudaGraph_t graph = nullptr;
     RB200_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    const bool jac = method_ == RB200_JACOBI_PCG_V1;
-    for (int q = 0; q < chunk_; ++q) {
-        if (jac) {
-            k_direction_apply<false><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, r_, nullptr, d_[0], d_[1],
-                                                                        part_, d_trace_);
-            k_update<true><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, p_, r_, d_[0], d_[1], part_, d_trace_);
-        } else {
-            k_direction_apply<true><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, r_, z_, d_[0], d_[1], part_,
-                                                                       d_trace_);
-            k_update<false><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, p_, r_, d_[0], d_[1], part_, d_trace_);
-            k_rbsgs_black<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_ITER);
-            k_rbsgs_red_dot<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_ITER, part_, d_trace_);
-        }
-    }
-    k_true_residual<<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, b_, p_, d_[0], d_[1], part_, d_trace_);
-    if (jac) {
-        k_load_residual<true><<<eb, EW, 0, stream_>>>(g_, st_, b_, d_[0], d_[1], r_, MODE_REPLACE, part_, d_trace_);
-    } else {
-        k_load_residual<false><<<eb, EW, 0, stream_>>>(g_, st_, b_, d_[0], d_[1], r_, MODE_REPLACE, part_, d_trace_);
-        k_rbsgs_black<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_REPLACE);
-        k_rbsgs_red_dot<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_REPLACE, part_, d_trace_);
-    }
-    nodes_per_chunk_ = chunk_ * (jac ? 2 : 4) + (jac ? 2 : 4);
+    int nodes = 0;
+    for (int q = 0; q < chunk_; ++q) nodes += launch_iteration(g_, jac, B, stream_);
+    nodes += launch_check(g_, jac, B, stream_);
+    nodes_per_chunk_ = nodes;
     cudaError_t launch_err = cudaGetLastError();
     cudaError_t end_err = cudaStreamEndCapture(stream_, &graph);
     if (launch_err != cudaSuccess || end_err != cudaSuccess) {
@@ -606,30 +821,18 @@ int PcgSolver::record_flags(int slot) {
 int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, rb200_cancel_fn cancelled,
                      void* ctx) {
     if (report) std::memset(report, 0, sizeof(*report));
-    SolveState init{};
-    init.dt = dt;
-    init.relative = s.relative_residual;
-    init.absolute = s.absolute_residual;
-    init.divergence_limit = s.divergence_limit;
-    init.max_it = s.max_iterations > 0x7fffffffull ? 0x7fffffff : int(s.max_iterations);
+    SolveState init = initial_state(dt, s);
     if (d_trace_ && uint64_t(init.max_it) > trace_cap_) {
         set_error("trace capacity is smaller than max_iterations");
         return RB200_INVALID_ARGUMENT;
     }
-    init.status = ST_RUNNING;
     h_st_[0] = init;
     RB200_CUDA(cudaMemcpyAsync(st_, &h_st_[0], sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     if (d_trace_) RB200_CUDA(cudaMemsetAsync(d_trace_, 0, trace_cap_ * sizeof(rb200_trace), stream_));
-    const int eb = ew_blocks(g_.cells);
-    k_init_sums<<<eb, EW, 0, stream_>>>(g_, st_, b_, p_, part_);
-    if (method_ == RB200_JACOBI_PCG_V1) {
-        k_load_residual<true><<<eb, EW, 0, stream_>>>(g_, st_, b_, d_[0], d_[1], r_, MODE_INIT, part_, d_trace_);
-    } else {
-        k_load_residual<false><<<eb, EW, 0, stream_>>>(g_, st_, b_, d_[0], d_[1], r_, MODE_INIT, part_, d_trace_);
-        k_rbsgs_black<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_INIT);
-        k_rbsgs_red_dot<<<eb, EW, 0, stream_>>>(g_, st_, r_, z_, MODE_INIT, part_, d_trace_);
-    }
-    launches_ += method_ == RB200_JACOBI_PCG_V1 ? 2 : 4;
+    const bool jac = method_ == RB200_JACOBI_PCG_V1;
+    RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), stream_));
+    launch_start(g_, jac, Bufs{b_, p_, r_, z_, d_[0], d_[1], st_, part_, d_trace_, maps_}, stream_);
+    launches_ += jac ? 2 : 4;
     RB200_CUDA(cudaGetLastError());
     // The host copy of the state must be stable before the chunk copies reuse
     // h_st_ slots.
@@ -637,12 +840,11 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
     int rc;
     if ((rc = record_flags(0))) return rc;
     if ((rc = launch_chunk(1))) return rc;
-    int slot = 0, last_it = -1, stalls = 0, final_flags = 0;
+    int slot = 0, last_it = -1, stalls = 0;
     bool cancelled_now = false;
     for (;;) {
         RB200_CUDA(cudaEventSynchronize(ev_[slot]));
         const SolveState& h = h_st_[slot];
-        final_flags = h.flags;
         if (h.flags & F_DONE) break;
         if (cancelled && cancelled(ctx)) {
             cancelled_now = true;
@@ -661,7 +863,6 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
         if ((rc = launch_chunk(slot))) return rc;
         slot ^= 1;
     }
-    (void)final_flags;
     RB200_CUDA(cudaStreamSynchronize(stream_));
     RB200_CUDA(cudaMemcpy(&h_st_[0], st_, sizeof(SolveState), cudaMemcpyDeviceToHost));
     const SolveState& f = h_st_[0];
@@ -669,15 +870,7 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
         size_t n = std::min(trace_cap_, size_t(f.it));
         RB200_CUDA(cudaMemcpy(h_trace_, d_trace_, n * sizeof(rb200_trace), cudaMemcpyDeviceToHost));
     }
-    if (report) {
-        report->iterations = uint64_t(f.it);
-        report->true_residual_l2 = f.true_l2;
-        report->true_residual_max = f.true_max;
-        report->predicted_divergence_max = f.true_div;
-        report->incompatible_sum = f.incompatible_sum;
-        report->incompatible_budget = f.incompatible_budget;
-        report->breakdown_iteration = uint64_t(f.breakdown_it);
-    }
+    fill_report(f, report);
     if (cancelled_now) return RB200_CANCELLED;
     return f.status;
 }
@@ -694,22 +887,17 @@ int PcgSolver::profile(int which, int launches, double* avg_ms) {
     prof.status = ST_RUNNING;
     h_st_[0] = prof;
     RB200_CUDA(cudaMemcpyAsync(st_, &h_st_[0], sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
-    MarchGrid mg = march_grid(g_.n, zc_);
     const bool jac = method_ == RB200_JACOBI_PCG_V1;
+    const dim3 grid = slab_grid(g_), block(TX, TY, 1);
     auto launch = [&]() {
-        if (which == 0) {
-            if (jac)
-                k_direction_apply<false><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, r_, nullptr, d_[0], d_[1],
-                                                                            part_, nullptr);
-            else
-                k_direction_apply<true><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, r_, z_, d_[0], d_[1], part_,
-                                                                           nullptr);
-        } else {
-            if (jac)
-                k_update<true><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, p_, r_, d_[0], d_[1], part_, nullptr);
-            else
-                k_update<false><<<mg.grid, mg.block, 0, stream_>>>(g_, zc_, st_, p_, r_, d_[0], d_[1], part_, nullptr);
-        }
+        if (which == 0)
+            k_pass1<ZC><<<grid, block, kSmemPass1, stream_>>>(g_, st_, z_, d_[0], d_[1], maps_, part_, nullptr);
+        else if (jac)
+            k_pass2<ZC, true><<<grid, block, kSmemSlab, stream_>>>(g_, st_, p_, r_, z_, d_[0], d_[1], maps_, part_,
+                                                                   nullptr);
+        else
+            k_pass2<ZC, false><<<grid, block, kSmemSlab, stream_>>>(g_, st_, p_, r_, z_, d_[0], d_[1], maps_, part_,
+                                                                    nullptr);
     };
     launch();  // warm
     cudaEvent_t a, b;
@@ -778,10 +966,7 @@ int static_solve_jacobi(const GridDev& g, const double* rhs, double* pressure, d
         set_error("grid exceeds the 32768-cell limit of the allocation-free solve");
         return RB200_UNSUPPORTED;
     }
-    const int zc = choose_zc(g);
-    const MarchGrid mg = march_grid(g.n, zc);
-    const int eb = ew_blocks(g.cells);
-    if (mg.nblocks > kStaticMaxBlocks || eb > kStaticMaxBlocks) {
+    if (slab_blocks(g) > kStaticMaxBlocks || ew_blocks(g.cells) > kStaticMaxBlocks) {
         set_error("grid shape needs more reduction blocks than the allocation-free solve holds");
         return RB200_UNSUPPORTED;
     }
@@ -790,33 +975,32 @@ int static_solve_jacobi(const GridDev& g, const double* rhs, double* pressure, d
     int rc = RB200_OK;
     double* base = static_scratch_address(device, &rc);
     if (rc) return rc;
-    double* r = base;
-    double* d0 = r + kStaticMaxCells;
-    double* d1 = d0 + kStaticMaxCells;
-    Partials part;
-    part.data = d1 + 2 * kStaticMaxCells;  // the fourth cell slot is reserved
-    double* state_slot = part.data + size_t(kStaticMaxBlocks) * 8;
-    SolveState* st = reinterpret_cast<SolveState*>(state_slot);
-    part.ticket = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(state_slot) + sizeof(SolveState));
+    if ((rc = set_smem_attrs())) return rc;
+    Bufs B;
+    B.b = const_cast<double*>(rhs);  // read only
+    B.p = pressure;
+    B.r = base;
+    B.d0 = B.r + kStaticMaxCells;
+    B.d1 = B.d0 + kStaticMaxCells;
+    B.z = B.d1 + kStaticMaxCells;
+    B.part.data = B.z + kStaticMaxCells;
+    double* state_slot = B.part.data + size_t(kStaticMaxBlocks) * 8;
+    B.st = reinterpret_cast<SolveState*>(state_slot);
+    B.part.ticket = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(state_slot) + sizeof(SolveState));
+    B.trace = nullptr;
+    B.maps = make_maps(g, B.z, B.d0, B.d1, B.p);
 
-    SolveState init{};
-    init.dt = dt;
-    init.relative = s.relative_residual;
-    init.absolute = s.absolute_residual;
-    init.divergence_limit = s.divergence_limit;
-    init.max_it = s.max_iterations > 0x7fffffffull ? 0x7fffffff : int(s.max_iterations);
-    init.status = ST_RUNNING;
+    SolveState init = initial_state(dt, s);
     // The array keeps the previous call's contents: the ticket must start at 0.
-    RB200_CUDA(cudaMemsetAsync(part.ticket, 0, sizeof(unsigned), stream));
-    RB200_CUDA(cudaMemcpyAsync(st, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream));
-    k_init_sums<<<eb, EW, 0, stream>>>(g, st, rhs, pressure, part);
-    k_load_residual<true><<<eb, EW, 0, stream>>>(g, st, rhs, d0, d1, r, MODE_INIT, part, nullptr);
+    RB200_CUDA(cudaMemsetAsync(B.part.ticket, 0, sizeof(unsigned), stream));
+    RB200_CUDA(cudaMemcpyAsync(B.st, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream));
+    launch_start(g, true, B, stream);
     RB200_CUDA(cudaGetLastError());
     const int chunk = 16;
     int last_it = -1, stalls = 0;
     SolveState h{};
     for (;;) {
-        RB200_CUDA(cudaMemcpyAsync(&h, st, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+        RB200_CUDA(cudaMemcpyAsync(&h, B.st, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
         RB200_CUDA(cudaStreamSynchronize(stream));
         if (h.flags & F_DONE) break;
         if (h.it == last_it) {
@@ -828,24 +1012,11 @@ int static_solve_jacobi(const GridDev& g, const double* rhs, double* pressure, d
             stalls = 0;
             last_it = h.it;
         }
-        for (int q = 0; q < chunk; ++q) {
-            k_direction_apply<false><<<mg.grid, mg.block, 0, stream>>>(g, zc, st, r, nullptr, d0, d1, part, nullptr);
-            k_update<true><<<mg.grid, mg.block, 0, stream>>>(g, zc, st, pressure, r, d0, d1, part, nullptr);
-        }
-        k_true_residual<<<mg.grid, mg.block, 0, stream>>>(g, zc, st, rhs, pressure, d0, d1, part, nullptr);
-        k_load_residual<true><<<eb, EW, 0, stream>>>(g, st, rhs, d0, d1, r, MODE_REPLACE, part, nullptr);
+        for (int q = 0; q < chunk; ++q) launch_iteration(g, true, B, stream);
+        launch_check(g, true, B, stream);
         RB200_CUDA(cudaGetLastError());
     }
-    if (report) {
-        std::memset(report, 0, sizeof(*report));
-        report->iterations = uint64_t(h.it);
-        report->true_residual_l2 = h.true_l2;
-        report->true_residual_max = h.true_max;
-        report->predicted_divergence_max = h.true_div;
-        report->incompatible_sum = h.incompatible_sum;
-        report->incompatible_budget = h.incompatible_budget;
-        report->breakdown_iteration = uint64_t(h.breakdown_it);
-    }
+    fill_report(h, report);
     return h.status;
 }
 

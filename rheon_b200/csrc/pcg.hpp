@@ -2,6 +2,8 @@
 // (PressureWorkspace::solve_loaded, src/pressure.rs:577-740).
 #pragma once
 
+#include <cuda.h>
+
 #include "internal.hpp"
 
 namespace rb200 {
@@ -35,6 +37,13 @@ enum : int {
     F_PROFILE = 64       // timing mode: passes do their work, decisions are skipped
 };
 constexpr int ST_RUNNING = -1;
+
+// Tensor maps of the solver's vectors for the TMA slab loads (unused when the
+// grid takes the cp.async path).
+struct TmaMaps {
+    CUtensorMap z, d0, d1, p;
+    int use;
+};
 
 class PcgSolver {
 public:
@@ -78,7 +87,8 @@ private:
     double* p_ = nullptr;
     double* r_ = nullptr;
     double* d_[2] = {nullptr, nullptr};
-    double* z_ = nullptr;  // preconditioned residual for the SGS methods
+    double* z_ = nullptr;  // preconditioned residual
+    TmaMaps maps_{};
     Partials part_{nullptr, nullptr};
     int part_blocks_ = 0;
     SolveState* st_ = nullptr;
@@ -86,7 +96,6 @@ private:
     cudaEvent_t ev_[2] = {nullptr, nullptr};
     cudaGraphExec_t chunk_exec_ = nullptr;
     int chunk_ = 16;
-    int zc_ = 8;
     rb200_trace* d_trace_ = nullptr;
     rb200_trace* h_trace_ = nullptr;
     size_t trace_cap_ = 0;
@@ -95,6 +104,7 @@ private:
     uint64_t launches_ = 0;
 };
 
-int choose_zc(const GridDev& g);
+// Blocks of the slab passes (reduction partials needed per pass).
+int slab_blocks(const GridDev& g);
 
 }  // namespace rb200

@@ -251,7 +251,9 @@ def compatible_rhs(g, seed=11, dtype=np.float64):
     return rhs
 
 
-@pytest.mark.parametrize("counts", [[32, 32, 32], [17, 10, 9], [48, 20, 7]])
+# [64, 40, 24] and [96, 16, 12] take the TMA slab path (even nx, at least one
+# slab box in every direction); the others take the cp.async path.
+@pytest.mark.parametrize("counts", [[32, 32, 32], [17, 10, 9], [48, 20, 7], [64, 40, 24], [96, 16, 12]])
 def test_jacobi_pcg_per_iteration_parity(counts):
     """Every iteration's scalars and the iterates track the oracle to 1e-12."""
     g = R.GridGeometry(counts)
@@ -299,8 +301,9 @@ def test_jacobi_converged_solve_matches_oracle_iterations_and_report():
     assert relerr(ws.pressure(), ref.pressure) <= 1e-12
 
 
-def test_rbsgs_converges_to_the_same_pressure():
-    g = R.GridGeometry([32, 32, 32])
+@pytest.mark.parametrize("counts", [[32, 32, 32], [64, 48, 40]])
+def test_rbsgs_converges_to_the_same_pressure(counts):
+    g = R.GridGeometry(counts)
     rhs = compatible_rhs(g, seed=9)
     s = S(1e-10, 0.0, 1.7976931348623157e308, 5000)
     ref = O.solve_rhs(og(g), 1.0, O.JACOBI_PCG_V1, rhs, 0.25, O.settings(1e-10, 0.0, 1.7976931348623157e308, 5000))
