@@ -248,24 +248,39 @@ def run_ours(args, world, rank, local):
 
     variants = {}
     if not args.no_variants and rank == 0 and world == 1:
-        for name, m in (("rbsgs_pcg_f64", R.PressureImplementation.RBSGS_PCG),):
-            if m == method:
+        mixed_pressure = R.PressureSettings(1e-8, 0.0, MAXF, 1000)
+        cases = (
+            ("rbsgs_pcg_f64", R.CarrierConfig(pressure=settings, storage=args.storage,
+                                              implementation=R.PressureImplementation.RBSGS_PCG, device=local),
+             faces),
+            ("mixed_mg_f32", R.CarrierConfig.mixed(pressure=mixed_pressure, device=local),
+             [f.astype(np.float32) for f in faces]),
+        )
+        for name, vcfg, vfaces in cases:
+            if vcfg.implementation == method and vcfg.storage == args.storage:
                 continue
-            vs = R.CarrierSimulation(g, R.CarrierConfig(pressure=settings, storage=args.storage, implementation=m,
-                                                        device=local))
-            vs.upload(faces)
+            vs = R.CarrierSimulation(g, vcfg)
+            vs.upload(vfaces)
+            vstream = torch.cuda.ExternalStream(vs.stream(), device=local)
             for _ in range(args.warmup):
                 vs.step(prm)
-            vms, vit = 0.0, []
+            vms, vit, vdiv = 0.0, [], 0.0
             for _ in range(args.steps):
                 flush.fill_(1.0)
                 torch.cuda.synchronize()
-                s0 = time.perf_counter()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(vstream)
                 r = vs.step(prm)
-                vms += (time.perf_counter() - s0) * 1e3
+                b.record(vstream)
+                b.synchronize()
+                vms += a.elapsed_time(b)
                 vit.append(r.pressure.iterations)
-            variants[name] = {"value": cells * args.steps / (vms / 1e3), "unit": UNIT,
-                              "iterations_per_step": statistics.mean(vit)}
+                vdiv = max(vdiv, r.actual_divergence_max)
+            vvalue = cells * args.steps / (vms / 1e3)
+            variants[name] = {"value": vvalue, "unit": UNIT, "ms_per_step": vms / args.steps,
+                              "iterations_per_step": statistics.mean(vit), "actual_divergence_max": vdiv,
+                              "vs_plain_f64": vvalue / value}
             vs.close()
 
     result = {

@@ -287,6 +287,7 @@ typedef struct rb200_carrier_config {
     double max_courant;
     int with_tracer;               /* allocate a cell tracer (f32)         */
     int device;
+    int fp32_advection;            /* sample/backtrace in FP32 arithmetic  */
 } rb200_carrier_config;
 
 typedef struct rb200_step_params {

@@ -472,6 +472,17 @@ class CarrierConfig:
     implementation: PressureImplementation = PressureImplementation.JACOBI_PCG_V1
     with_tracer: bool = False
     device: int = 0
+    fp32_advection: bool = False
+
+    @staticmethod
+    def mixed(**kw) -> "CarrierConfig":
+        """The mixed-precision carrier: FP32 faces and FP32 advection
+        arithmetic, FP32 multigrid V(2,2) smoothing inside FP64 flexible CG
+        (FP64 residual, pressure accumulation and coarsest solve)."""
+        kw.setdefault("storage", "f32")
+        kw.setdefault("implementation", PressureImplementation.MG_MIXED)
+        kw.setdefault("fp32_advection", True)
+        return CarrierConfig(**kw)
 
 
 @dataclass
@@ -508,7 +519,8 @@ class CarrierSimulation:
         self.dtype = np.float32 if config.storage == "f32" else np.float64
         c = N.CarrierConfig(grid.c(), config.density, 0 if config.storage == "f32" else 1,
                             int(config.implementation), config.pressure.c(), config.actual_divergence_limit,
-                            config.max_courant, 1 if config.with_tracer else 0, config.device)
+                            config.max_courant, 1 if config.with_tracer else 0, config.device,
+                            1 if config.fp32_advection else 0)
         h = C.c_void_p()
         st = lib().rb200_carrier_create(C.byref(c), C.byref(h))
         if st != N.OK:

@@ -78,7 +78,7 @@ class Metadata(C.Structure):
 class CarrierConfig(C.Structure):
     _fields_ = [("grid", Grid), ("density", C.c_double), ("storage", C.c_int), ("method", C.c_int),
                 ("settings", Settings), ("actual_divergence_limit", C.c_double), ("max_courant", C.c_double),
-                ("with_tracer", C.c_int), ("device", C.c_int)]
+                ("with_tracer", C.c_int), ("device", C.c_int), ("fp32_advection", C.c_int)]
 
 
 class StepParams(C.Structure):

@@ -7,34 +7,36 @@ namespace rb200 {
 
 constexpr int ADV_THREADS = 256;
 
-__device__ __forceinline__ double clampd(double x, double lo, double hi) {
+template <class R>
+__device__ __forceinline__ R clampd(R x, R lo, R hi) {
     // f64::clamp: if x < min { min } then if x > max { max }.
     if (x < lo) x = lo;
     if (x > hi) x = hi;
     return x;
 }
 
-// ScalarSampler::sample (src/sampling.rs:74-122).
-template <class T>
-__device__ __forceinline__ double sample(const GridDev& g, const T* __restrict__ values, const int dims[3],
-                                         const double off[3], const double pos[3], int& flag) {
+// ScalarSampler::sample (src/sampling.rs:74-122) in arithmetic type R: double
+// reproduces the reference; float is the mixed-precision path.
+template <class T, class R>
+__device__ __forceinline__ R sample(const GridDev& g, const T* __restrict__ values, const int dims[3], const R off[3],
+                                    const R pos[3], int& flag) {
     int lo[3], hi[3];
-    double t[3];
+    R t[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        double x = clampd(pos[d], g.o[d], g.up[d]);
-        double q = clampd((x - g.o[d]) / g.h[d] - off[d], 0.0, double(dims[d] - 1));
+        R x = clampd<R>(pos[d], R(g.o[d]), R(g.up[d]));
+        R q = clampd<R>((x - R(g.o[d])) / R(g.h[d]) - off[d], R(0), R(dims[d] - 1));
         if (!isfinite(q)) {
             flag |= VF_ARITH;
-            q = 0.0;
+            q = R(0);
         }
         lo[d] = int(floor(q));
         hi[d] = min(lo[d] + 1, dims[d] - 1);
-        t[d] = q - double(lo[d]);
+        t[d] = q - R(lo[d]);
     }
-    double result = 0.0;
-    double minimum = CUDART_INF;
-    double maximum = -CUDART_INF;
+    R result = R(0);
+    R minimum = R(CUDART_INF);
+    R maximum = R(-CUDART_INF);
 #pragma unroll
     for (int z = 0; z < 2; ++z)
 #pragma unroll
@@ -44,17 +46,17 @@ __device__ __forceinline__ double sample(const GridDev& g, const T* __restrict__
                 int px = x ? hi[0] : lo[0];
                 int py = y ? hi[1] : lo[1];
                 int pz = z ? hi[2] : lo[2];
-                double weight = 1.0;
-                weight = weight * (x ? t[0] : 1.0 - t[0]);
-                weight = weight * (y ? t[1] : 1.0 - t[1]);
-                weight = weight * (z ? t[2] : 1.0 - t[2]);
-                double value = double(__ldg(values + (px + dims[0] * (py + dims[1] * pz))));
+                R weight = R(1);
+                weight = weight * (x ? t[0] : R(1) - t[0]);
+                weight = weight * (y ? t[1] : R(1) - t[1]);
+                weight = weight * (z ? t[2] : R(1) - t[2]);
+                R value = R(__ldg(values + (px + dims[0] * (py + dims[1] * pz))));
                 minimum = fmin(minimum, value);
                 maximum = fmax(maximum, value);
                 result += weight * value;
             }
     if (!isfinite(result)) flag |= VF_ARITH;
-    return clampd(result, minimum, maximum);
+    return clampd<R>(result, minimum, maximum);
 }
 
 template <class T>
@@ -62,51 +64,53 @@ struct Faces {
     const T* f[3];
 };
 
-__device__ __forceinline__ void face_geometry(const GridDev& g, int a, int dims[3], double off[3]) {
+template <class R>
+__device__ __forceinline__ void face_geometry(const GridDev& g, int a, int dims[3], R off[3]) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         dims[d] = g.fc[a][d];
-        off[d] = d == a ? 0.0 : 0.5;
+        off[d] = d == a ? R(0) : R(0.5);
     }
 }
 
-template <class T>
-__device__ __forceinline__ void velocity_sample(const GridDev& g, const Faces<T>& vel, const double pos[3],
-                                                double out[3], int& flag) {
+template <class T, class R>
+__device__ __forceinline__ void velocity_sample(const GridDev& g, const Faces<T>& vel, const R pos[3], R out[3],
+                                                int& flag) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         int dims[3];
-        double off[3];
-        face_geometry(g, a, dims, off);
-        out[a] = sample<T>(g, vel.f[a], dims, off, pos, flag);
+        R off[3];
+        face_geometry<R>(g, a, dims, off);
+        out[a] = sample<T, R>(g, vel.f[a], dims, off, pos, flag);
     }
 }
 
 // VelocitySampler::departure (src/sampling.rs:160-175).
-__device__ __forceinline__ void departure(const GridDev& g, const double pos[3], const double vel[3],
-                                          double dt, double out[3], int& flag) {
+template <class R>
+__device__ __forceinline__ void departure(const GridDev& g, const R pos[3], const R vel[3], R dt, R out[3],
+                                          int& flag) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        double value = pos[d] - dt * vel[d];
+        R value = pos[d] - dt * vel[d];
         if (!isfinite(value)) flag |= VF_ARITH;
-        out[d] = clampd(value, g.o[d], g.up[d]);
+        out[d] = clampd<R>(value, R(g.o[d]), R(g.up[d]));
     }
 }
 
 // VelocitySampler::backtrace (src/sampling.rs:151-159): midpoint RK2.
-template <class T>
-__device__ __forceinline__ void backtrace(const GridDev& g, const Faces<T>& vel, const double pos[3],
-                                          double dt, double out[3], int& flag) {
-    double initial[3], mid[3], v1[3];
-    velocity_sample<T>(g, vel, pos, initial, flag);
-    departure(g, pos, initial, 0.5 * dt, mid, flag);
-    velocity_sample<T>(g, vel, mid, v1, flag);
-    departure(g, pos, v1, dt, out, flag);
+template <class T, class R>
+__device__ __forceinline__ void backtrace(const GridDev& g, const Faces<T>& vel, const R pos[3], R dt, R out[3],
+                                          int& flag) {
+    R initial[3], mid[3], v1[3];
+    velocity_sample<T, R>(g, vel, pos, initial, flag);
+    departure<R>(g, pos, initial, R(0.5) * dt, mid, flag);
+    velocity_sample<T, R>(g, vel, mid, v1, flag);
+    departure<R>(g, pos, v1, dt, out, flag);
 }
 
 // advect_velocity (src/advection.rs:28-68): wall-normal faces are exactly 0,
 // every other face samples its own component at the RK2 departure point.
-template <class T>
+template <class T, class R>
 __global__ void __launch_bounds__(ADV_THREADS) k_advect_velocity(GridDev g, Faces<T> vel, double dt, T* ou, T* ov, T* ow,
                                                                  const float* __restrict__ tracer, double gb,
                                                                  int* flags) {
@@ -133,15 +137,15 @@ __global__ void __launch_bounds__(ADV_THREADS) k_advect_velocity(GridDev g, Face
             dst[f] = T(0);
             continue;
         }
-        double pos[3];
+        R pos[3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) pos[d] = g.o[d] + (double(p[d]) + (d == a ? 0.0 : 0.5)) * g.h[d];
-        double dep[3];
-        backtrace<T>(g, vel, pos, dt, dep, local);
+        for (int d = 0; d < 3; ++d) pos[d] = R(g.o[d] + (double(p[d]) + (d == a ? 0.0 : 0.5)) * g.h[d]);
+        R dep[3];
+        backtrace<T, R>(g, vel, pos, R(dt), dep, local);
         int dims[3];
-        double off[3];
-        face_geometry(g, a, dims, off);
-        T value = T(sample<T>(g, vel.f[a], dims, off, dep, local));
+        R off[3];
+        face_geometry<R>(g, a, dims, off);
+        T value = T(sample<T, R>(g, vel.f[a], dims, off, dep, local));
         if (a == 1 && tracer != nullptr && gb != 0.0) {
             // Buoyancy hook (new): interior Y face, after advection, before pressure.
             int below = cell_idx(g, p[0], p[1] - 1, p[2]);
@@ -158,57 +162,64 @@ __global__ void __launch_bounds__(ADV_THREADS) k_advect_velocity(GridDev g, Face
 
 template <class T>
 int launch_advect_velocity(const GridDev& g, const T* u, const T* v, const T* w, double dt, T* ou,
-                           T* ov, T* ow, const float* tracer, double gb, int* flags, cudaStream_t s) {
+                           T* ov, T* ow, const float* tracer, double gb, int* flags, cudaStream_t s,
+                           bool fp32_math) {
     long long total = (long long)g.flen[0] + g.flen[1] + g.flen[2];
     long long blocks = (total + ADV_THREADS - 1) / ADV_THREADS;
     if (blocks > 148 * 64) blocks = 148 * 64;
     Faces<T> vel{{u, v, w}};
-    k_advect_velocity<T><<<int(blocks), ADV_THREADS, 0, s>>>(g, vel, dt, ou, ov, ow, tracer, gb, flags);
+    if (fp32_math)
+        k_advect_velocity<T, float><<<int(blocks), ADV_THREADS, 0, s>>>(g, vel, dt, ou, ov, ow, tracer, gb, flags);
+    else
+        k_advect_velocity<T, double><<<int(blocks), ADV_THREADS, 0, s>>>(g, vel, dt, ou, ov, ow, tracer, gb, flags);
     RB200_CUDA(cudaGetLastError());
     return RB200_OK;
 }
 
 // advect_tracer (src/advection.rs:72-102), evaluated densely; the reference's
 // zero-support skip produces the same bits (tests/advection_contract.rs:7-41).
-template <class T>
+template <class T, class R>
 __global__ void __launch_bounds__(ADV_THREADS) k_advect_tracer(GridDev g, const float* __restrict__ old, Faces<T> vel,
                                                                double dt, float* __restrict__ out, int* flags) {
     int local = 0;
     int dims[3] = {g.n[0], g.n[1], g.n[2]};
-    double off[3] = {0.5, 0.5, 0.5};
+    R off[3] = {R(0.5), R(0.5), R(0.5)};
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
         int p[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
-        double pos[3];
+        R pos[3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) pos[d] = g.o[d] + (double(p[d]) + 0.5) * g.h[d];
-        double dep[3];
-        backtrace<T>(g, vel, pos, dt, dep, local);
-        out[c] = float(sample<float>(g, old, dims, off, dep, local));
+        for (int d = 0; d < 3; ++d) pos[d] = R(g.o[d] + (double(p[d]) + 0.5) * g.h[d]);
+        R dep[3];
+        backtrace<T, R>(g, vel, pos, R(dt), dep, local);
+        out[c] = float(sample<float, R>(g, old, dims, off, dep, local));
     }
     if (local) atomicOr(flags, local);
 }
 
 template <class T>
 int launch_advect_tracer(const GridDev& g, const float* old, const T* u, const T* v, const T* w,
-                         double dt, float* out, int* flags, cudaStream_t s) {
+                         double dt, float* out, int* flags, cudaStream_t s, bool fp32_math) {
     long long blocks = ((long long)g.cells + ADV_THREADS - 1) / ADV_THREADS;
     if (blocks > 148 * 64) blocks = 148 * 64;
     Faces<T> vel{{u, v, w}};
-    k_advect_tracer<T><<<int(blocks), ADV_THREADS, 0, s>>>(g, old, vel, dt, out, flags);
+    if (fp32_math)
+        k_advect_tracer<T, float><<<int(blocks), ADV_THREADS, 0, s>>>(g, old, vel, dt, out, flags);
+    else
+        k_advect_tracer<T, double><<<int(blocks), ADV_THREADS, 0, s>>>(g, old, vel, dt, out, flags);
     RB200_CUDA(cudaGetLastError());
     return RB200_OK;
 }
 
 template int launch_advect_velocity<float>(const GridDev&, const float*, const float*, const float*,
                                            double, float*, float*, float*, const float*, double,
-                                           int*, cudaStream_t);
+                                           int*, cudaStream_t, bool);
 template int launch_advect_velocity<double>(const GridDev&, const double*, const double*,
                                             const double*, double, double*, double*, double*,
-                                            const float*, double, int*, cudaStream_t);
+                                            const float*, double, int*, cudaStream_t, bool);
 template int launch_advect_tracer<float>(const GridDev&, const float*, const float*, const float*,
-                                         const float*, double, float*, int*, cudaStream_t);
+                                         const float*, double, float*, int*, cudaStream_t, bool);
 template int launch_advect_tracer<double>(const GridDev&, const float*, const double*,
                                           const double*, const double*, double, float*, int*,
-                                          cudaStream_t);
+                                          cudaStream_t, bool);
 
 }  // namespace rb200

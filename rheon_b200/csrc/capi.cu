@@ -224,8 +224,9 @@ static int carrier_step_t(rb200_carrier* c, const rb200_step_params* prm, rb200_
     T* const Cc[3] = {(T*)c->faces[corr][0], (T*)c->faces[corr][1], (T*)c->faces[corr][2]};
     const float* tr = c->tracer[0] ? c->tracer[c->tacc] : nullptr;
     RB200_CUDA(cudaMemsetAsync(c->d_flags, 0, sizeof(int), c->stream));
+    const bool fp32 = c->cfg.fp32_advection != 0;
     int rc = launch_advect_velocity<T>(g, A[0], A[1], A[2], dt, B[0], B[1], B[2], tr, prm->buoyancy, c->d_flags,
-                                       c->stream);
+                                       c->stream, fp32);
     if (rc) return rc;
     if ((rc = launch_build_rhs<T>(g, B[0], B[1], B[2], dt, c->solver.b(), c->d_flags, c->stream))) return rc;
     RB200_CUDA(cudaEventRecord(c->ev[0], c->stream));
@@ -250,7 +251,7 @@ static int carrier_step_t(rb200_carrier* c, const rb200_step_params* prm, rb200_
         return rc;
     if (tr) {
         if ((rc = launch_advect_tracer<T>(g, tr, Cc[0], Cc[1], Cc[2], dt, c->tracer[c->tacc ^ 1], c->d_flags,
-                                          c->stream)))
+                                          c->stream, fp32)))
             return rc;
     }
     RB200_CUDA(cudaMemcpyAsync(c->h_scalars, c->d_scalars, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -332,12 +333,13 @@ int rb200_workspace_create(const rb200_grid* grid, double density, int method, u
         set_error("invalid grid or density");
         return rc;
     }
-    if (method != RB200_JACOBI_PCG_V1 && method != RB200_RBSGS_PCG) {
+    if (method != RB200_JACOBI_PCG_V1 && method != RB200_RBSGS_PCG && method != RB200_MG_MIXED) {
         set_error("method not available on the device");
         return RB200_UNSUPPORTED;
     }
-    // Six f64 cell arrays at most (b, p, r, two directions, z) plus partials.
-    uint64_t need = uint64_t(g.cells) * 48;
+    // Six f64 cell arrays (b, p, r, two directions, z), q and the FP32
+    // hierarchy (about 5.2 bytes per fine cell) for multigrid, plus partials.
+    uint64_t need = uint64_t(g.cells) * (method == RB200_MG_MIXED ? 62 : 48);
     if (need > memory_limit) {
         set_error("device buffers exceed the memory limit");
         return RB200_OUT_OF_MEMORY;

@@ -153,12 +153,14 @@ int partials_blocks_needed(const GridDev& g);
 // --------------------------------------------------------------- advection.cu
 // buoyancy: if tracer != nullptr and gb != 0, interior Y faces get
 // v <- T(f64(v) + dt*(gb*0.5*(c_below + c_above))) after advection.
+// fp32_math: sample and backtrace in FP32 arithmetic (mixed-precision path);
+// otherwise FP64 arithmetic, as the reference.
 template <class T>
 int launch_advect_velocity(const GridDev& g, const T* u, const T* v, const T* w, double dt,
                            T* ou, T* ov, T* ow, const float* tracer, double gb, int* flags,
-                           cudaStream_t s);
+                           cudaStream_t s, bool fp32_math = false);
 template <class T>
 int launch_advect_tracer(const GridDev& g, const float* old, const T* u, const T* v, const T* w,
-                         double dt, float* out, int* flags, cudaStream_t s);
+                         double dt, float* out, int* flags, cudaStream_t s, bool fp32_math = false);
 
 }  // namespace rb200

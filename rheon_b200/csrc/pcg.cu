@@ -163,7 +163,10 @@ __global__ void __launch_bounds__(EW) k_init_sums(GridDev g, SolveState* st, con
 // red cells (its forward red solve) and leaves the rest to its sweep kernels.
 // Used for the initial residual (MODE_INIT, src = b) and for the restart
 // (MODE_REPLACE, src = the true residual in the spare direction buffer).
-template <bool JACOBI>
+// KIND: 0 Jacobi, 1 red-black SGS, 2 multigrid (copy only; the V-cycle and
+// k_mg_finish form z).
+enum : int { KIND_JACOBI = 0, KIND_RBSGS = 1, KIND_MG = 2 };
+template <int KIND>
 __global__ void __launch_bounds__(EW) k_load_residual(GridDev g, SolveState* st, const double* b,
                                                       double* d0, double* d1, double* __restrict__ r,
                                                       double* __restrict__ z, int mode, Partials part,
@@ -180,8 +183,9 @@ __global__ void __launch_bounds__(EW) k_load_residual(GridDev g, SolveState* st,
             z[0] = 0.0;
             continue;
         }
+        if (KIND == KIND_MG) continue;
         int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
-        if (JACOBI) {
+        if (KIND == KIND_JACOBI) {
             double zc = rc / diag_at(g, i, j, k);
             z[c] = zc;
             acc.add(rc * zc);
@@ -189,7 +193,7 @@ __global__ void __launch_bounds__(EW) k_load_residual(GridDev g, SolveState* st,
             z[c] = rc / diag_at(g, i, j, k);
         }
     }
-    if (!JACOBI) return;
+    if (KIND != KIND_JACOBI) return;
     dd sums[1] = {acc.as_dd()};
     double none[1];
     block_reduce<1, 0>(sm, sums, none);
@@ -253,8 +257,9 @@ __device__ __forceinline__ bool stage_wait(const TmaMaps& maps, uint64_t* bar, S
 // they stay 0), then each cell's row of K d is applied.
 template <int ZC>
 __global__ void __launch_bounds__(TILE_THREADS) k_pass1(GridDev g, SolveState* st, const double* __restrict__ zarr,
-                                                        double* d0, double* d1, const __grid_constant__ TmaMaps maps,
-                                                        Partials part, rb200_trace* trace) {
+                                                        double* d0, double* d1, double* __restrict__ qout,
+                                                        const __grid_constant__ TmaMaps maps, Partials part,
+                                                        rb200_trace* trace) {
     using S = Slab<ZC>;
     extern __shared__ __align__(128) double smem[];
     __shared__ BlockReduce<1, 0> red;
@@ -287,6 +292,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_pass1(GridDev g, SolveState* s
             Neigh v = slab_neigh<ZC>(sz, e);
             double qv = c == 0 ? 0.0 : apply_row(g, i, j, k0 + q, v);
             dst[c] = v.c;
+            if (qout) qout[c] = qv;
             acc.add(v.c * qv);
         }
     }
@@ -494,7 +500,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_true_residual(GridDev g, Solve
                 breakdown(st, it, flags);
                 return;
             }
-            double beta = rz / st->rz;
+            double beta = st->flexible ? st->beta_next : rz / st->rz;
             if (trace) {
                 trace[it - 1].rz = rz;
                 trace[it - 1].beta = beta;
@@ -502,6 +508,93 @@ __global__ void __launch_bounds__(TILE_THREADS) k_true_residual(GridDev g, Solve
             st->beta = beta;
             st->rz = rz;
             st->flags = flags & ~(F_STOP | F_NEED_TRUE);
+        }
+    }
+}
+
+// ------------------------------------------------------------ multigrid outer passes
+// Flexible CG around the FP32 multigrid preconditioner: q = K d is stored by
+// pass 1; the update pass is elementwise; the finish pass converts the FP32
+// V-cycle output to z (FP64, z[0] = 0), reduces r.z and z.q and takes the
+// decision with beta = -z.q / d.q (Polak-Ribiere form, tolerant of a
+// preconditioner that is symmetric only up to FP32 rounding).
+__global__ void __launch_bounds__(EW) k_mg_update(GridDev g, SolveState* st, double* __restrict__ p,
+                                                  double* __restrict__ r, const double* d0, const double* d1,
+                                                  const double* __restrict__ q, Partials part, rb200_trace* trace) {
+    __shared__ BlockReduce<1, 0> red;
+    const int flags = st->flags;
+    if (flags & F_STOP) return;
+    const double alpha = st->alpha;
+    const double* __restrict__ d = st->dsel ? d1 : d0;
+    Neu acc;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        if (c == 0) continue;
+        p[c] = p[c] + alpha * d[c];
+        double rc = r[c] - alpha * q[c];
+        r[c] = rc;
+        acc.add(rc * rc);
+    }
+    dd sums[1] = {acc.as_dd()};
+    double none[1];
+    block_reduce<1, 0>(red, sums, none);
+    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
+        fold_partials<1, 0>(part, gridDim.x, red, sums, none);
+        if (threadIdx.x == 0) {
+            if (flags & F_PROFILE) return;
+            int it = st->it + 1;
+            st->it = it;
+            double recursive_l2 = sqrt(dd_value(sums[0]));
+            st->recursive_l2 = recursive_l2;
+            if (trace) trace[it - 1].recursive_l2 = recursive_l2;
+            if (recursive_l2 <= st->threshold || it == st->max_it) st->flags = flags | F_CANDIDATE;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(EW) k_mg_finish(GridDev g, SolveState* st, const float* __restrict__ x0,
+                                                  double* __restrict__ z, const double* __restrict__ r,
+                                                  const double* __restrict__ q, int mode, Partials part,
+                                                  rb200_trace* trace) {
+    __shared__ BlockReduce<2, 0> red;
+    const int flags = st->flags;
+    if (!gate(flags, mode)) return;
+    Neu rz, zq;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        const double zc = c == 0 ? 0.0 : double(x0[c]);
+        z[c] = zc;
+        if (c == 0) continue;
+        rz.add(r[c] * zc);
+        if (mode == MODE_ITER) zq.add(zc * q[c]);
+    }
+    dd sums[2] = {rz.as_dd(), zq.as_dd()};
+    double none[1];
+    block_reduce<2, 0>(red, sums, none);
+    if (publish_and_check_last<2, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
+        fold_partials<2, 0>(part, gridDim.x, red, sums, none);
+        if (threadIdx.x == 0) {
+            const double rzv = dd_value(sums[0]);
+            if (mode != MODE_ITER) {
+                decide_rz(st, trace, rzv, mode);
+                return;
+            }
+            const int it = st->it;
+            const double beta = -dd_value(sums[1]) / st->curvature;
+            if (flags & F_CANDIDATE) {
+                st->rz_next = rzv;
+                st->beta_next = beta;
+                st->flags = (flags & ~F_CANDIDATE) | F_STOP | F_NEED_TRUE;
+                return;
+            }
+            if (!isfinite(rzv) || rzv <= 0.0 || !isfinite(beta)) {
+                breakdown(st, it, flags);
+                return;
+            }
+            if (trace) {
+                trace[it - 1].rz = rzv;
+                trace[it - 1].beta = beta;
+            }
+            st->beta = beta;
+            st->rz = rzv;
         }
     }
 }
@@ -595,7 +688,7 @@ static int set_smem_attrs() {
 }
 
 struct Bufs {
-    double *b, *p, *r, *z, *d0, *d1;
+    double *b, *p, *r, *z, *d0, *d1, *q;
     SolveState* st;
     Partials part;
     rb200_trace* trace;
@@ -649,47 +742,74 @@ static TmaMaps make_maps(const GridDev& g, const double* z, const double* d0, co
 }
 
 // Initial residual and preconditioned start (src/pressure.rs:603-650).
-static void launch_start(const GridDev& g, bool jac, const Bufs& B, cudaStream_t s) {
+// `mg` is the multigrid hierarchy of the mixed method (nullptr otherwise).
+static int launch_start(const GridDev& g, int method, const Bufs& B, const Multigrid* mg, cudaStream_t s) {
     const int eb = ew_blocks(g.cells);
     k_init_sums<<<eb, EW, 0, s>>>(g, B.st, B.b, B.p, B.part);
-    if (jac) {
-        k_load_residual<true><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part, B.trace);
-    } else {
-        k_load_residual<false><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part, B.trace);
+    if (method == RB200_JACOBI_PCG_V1) {
+        k_load_residual<KIND_JACOBI><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part,
+                                                       B.trace);
+        return 2;
+    }
+    if (method == RB200_RBSGS_PCG) {
+        k_load_residual<KIND_RBSGS><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part,
+                                                      B.trace);
         k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_INIT);
         k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_INIT, B.part, B.trace);
+        return 4;
     }
+    k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part, B.trace);
+    int n = 2 + mg->enqueue(B.r, B.st, MODE_INIT, s);
+    k_mg_finish<<<eb, EW, 0, s>>>(g, B.st, mg->x0(), B.z, B.r, B.q, MODE_INIT, B.part, B.trace);
+    return n + 1;
 }
 
 // One PCG iteration (src/pressure.rs:651-734).
-static int launch_iteration(const GridDev& g, bool jac, const Bufs& B, cudaStream_t s) {
+static int launch_iteration(const GridDev& g, int method, const Bufs& B, const Multigrid* mg, cudaStream_t s) {
     const dim3 grid = slab_grid(g), block(TX, TY, 1);
-    k_pass1<ZC><<<grid, block, kSmemPass1, s>>>(g, B.st, B.z, B.d0, B.d1, B.maps, B.part, B.trace);
-    if (jac) {
+    const int eb = ew_blocks(g.cells);
+    const bool flexible = method == RB200_MG_MIXED;
+    k_pass1<ZC><<<grid, block, kSmemPass1, s>>>(g, B.st, B.z, B.d0, B.d1, flexible ? B.q : nullptr, B.maps, B.part,
+                                                B.trace);
+    if (method == RB200_JACOBI_PCG_V1) {
         k_pass2<ZC, true><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part,
                                                          B.trace);
         return 2;
     }
-    const int eb = ew_blocks(g.cells);
-    k_pass2<ZC, false><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part, B.trace);
-    k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_ITER);
-    k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_ITER, B.part, B.trace);
-    return 4;
+    if (method == RB200_RBSGS_PCG) {
+        k_pass2<ZC, false><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part,
+                                                          B.trace);
+        k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_ITER);
+        k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_ITER, B.part, B.trace);
+        return 4;
+    }
+    k_mg_update<<<eb, EW, 0, s>>>(g, B.st, B.p, B.r, B.d0, B.d1, B.q, B.part, B.trace);
+    int n = 2 + mg->enqueue(B.r, B.st, MODE_ITER, s);
+    k_mg_finish<<<eb, EW, 0, s>>>(g, B.st, mg->x0(), B.z, B.r, B.q, MODE_ITER, B.part, B.trace);
+    return n + 1;
 }
 
 // The gated true-residual check and restart (src/pressure.rs:686-715).
-static int launch_check(const GridDev& g, bool jac, const Bufs& B, cudaStream_t s) {
+static int launch_check(const GridDev& g, int method, const Bufs& B, const Multigrid* mg, cudaStream_t s) {
     const dim3 grid = slab_grid(g), block(TX, TY, 1);
     const int eb = ew_blocks(g.cells);
     k_true_residual<ZC><<<grid, block, kSmemSlab, s>>>(g, B.st, B.b, B.p, B.d0, B.d1, B.maps, B.part, B.trace);
-    if (jac) {
-        k_load_residual<true><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part, B.trace);
+    if (method == RB200_JACOBI_PCG_V1) {
+        k_load_residual<KIND_JACOBI><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part,
+                                                       B.trace);
         return 2;
     }
-    k_load_residual<false><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part, B.trace);
-    k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_REPLACE);
-    k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_REPLACE, B.part, B.trace);
-    return 4;
+    if (method == RB200_RBSGS_PCG) {
+        k_load_residual<KIND_RBSGS><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part,
+                                                      B.trace);
+        k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_REPLACE);
+        k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_REPLACE, B.part, B.trace);
+        return 4;
+    }
+    k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part, B.trace);
+    int n = 2 + mg->enqueue(B.r, B.st, MODE_REPLACE, s);
+    k_mg_finish<<<eb, EW, 0, s>>>(g, B.st, mg->x0(), B.z, B.r, B.q, MODE_REPLACE, B.part, B.trace);
+    return n + 1;
 }
 
 static SolveState initial_state(double dt, const rb200_settings& s) {
@@ -725,6 +845,7 @@ PcgSolver::~PcgSolver() {
     cudaFree(d_[0]);
     cudaFree(d_[1]);
     cudaFree(z_);
+    cudaFree(q_);
     cudaFree(part_.data);
     cudaFree(part_.ticket);
     cudaFree(st_);
@@ -736,7 +857,8 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
     g_ = g;
     method_ = method;
     stream_ = stream;
-    if (method != RB200_JACOBI_PCG_V1 && method != RB200_RBSGS_PCG) return RB200_UNSUPPORTED;
+    if (method != RB200_JACOBI_PCG_V1 && method != RB200_RBSGS_PCG && method != RB200_MG_MIXED)
+        return RB200_UNSUPPORTED;
     int rc = set_smem_attrs();
     if (rc) return rc;
     part_blocks_ = std::max(slab_blocks(g), EW_CAP);
@@ -753,6 +875,11 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
     if ((rc = alloc(&b_, n)) || (rc = alloc(&p_, n)) || (rc = alloc(&r_, n)) || (rc = alloc(&z_, n)) ||
         (rc = alloc(&d_[0], n)) || (rc = alloc(&d_[1], n)))
         return rc;
+    if (method == RB200_MG_MIXED) {
+        if ((rc = alloc(&q_, n))) return rc;
+        if ((rc = mg_.init(g, stream_))) return rc;
+        bytes_ += mg_.bytes();
+    }
     if ((rc = alloc(&part_.data, size_t(part_blocks_) * 8))) return rc;
     RB200_CUDA(cudaMalloc(&part_.ticket, sizeof(unsigned)));
     RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), stream_));
@@ -760,7 +887,7 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
     RB200_CUDA(cudaMallocHost(&h_st_, 2 * sizeof(SolveState)));
     for (auto& e : ev_) RB200_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     maps_ = make_maps(g, z_, d_[0], d_[1], p_);
-    chunk_ = g.cells >= (1 << 20) ? 32 : 16;
+    chunk_ = method == RB200_MG_MIXED ? 4 : (g.cells >= (1 << 20) ? 32 : 16);
     return capture_chunk();
 }
 
@@ -781,13 +908,13 @@ int PcgSolver::set_trace(rb200_trace* host, size_t capacity) {
 
 // One chunk: `chunk_` iterations, then the gated true-residual and restart.
 int PcgSolver::capture_chunk() {
-    const bool jac = method_ == RB200_JACOBI_PCG_V1;
-    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], st_, part_, d_trace_, maps_};
+    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_};
+    const Multigrid* mg = method_ == RB200_MG_MIXED ? &mg_ : nullptr;
     cudaGraph_t graph = nullptr;
     RB200_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     int nodes = 0;
-    for (int q = 0; q < chunk_; ++q) nodes += launch_iteration(g_, jac, B, stream_);
-    nodes += launch_check(g_, jac, B, stream_);
+    for (int q = 0; q < chunk_; ++q) nodes += launch_iteration(g_, method_, B, mg, stream_);
+    nodes += launch_check(g_, method_, B, mg, stream_);
     nodes_per_chunk_ = nodes;
     cudaError_t launch_err = cudaGetLastError();
     cudaError_t end_err = cudaStreamEndCapture(stream_, &graph);
@@ -822,6 +949,7 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
                      void* ctx) {
     if (report) std::memset(report, 0, sizeof(*report));
     SolveState init = initial_state(dt, s);
+    init.flexible = method_ == RB200_MG_MIXED ? 1 : 0;
     if (d_trace_ && uint64_t(init.max_it) > trace_cap_) {
         set_error("trace capacity is smaller than max_iterations");
         return RB200_INVALID_ARGUMENT;
@@ -829,10 +957,9 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
     h_st_[0] = init;
     RB200_CUDA(cudaMemcpyAsync(st_, &h_st_[0], sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     if (d_trace_) RB200_CUDA(cudaMemsetAsync(d_trace_, 0, trace_cap_ * sizeof(rb200_trace), stream_));
-    const bool jac = method_ == RB200_JACOBI_PCG_V1;
     RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), stream_));
-    launch_start(g_, jac, Bufs{b_, p_, r_, z_, d_[0], d_[1], st_, part_, d_trace_, maps_}, stream_);
-    launches_ += jac ? 2 : 4;
+    launches_ += uint64_t(launch_start(g_, method_, Bufs{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_},
+                                       method_ == RB200_MG_MIXED ? &mg_ : nullptr, stream_));
     RB200_CUDA(cudaGetLastError());
     // The host copy of the state must be stable before the chunk copies reuse
     // h_st_ slots.
@@ -877,6 +1004,7 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
 
 int PcgSolver::profile(int which, int launches, double* avg_ms) {
     if (launches < 1 || (which != 0 && which != 1)) return RB200_INVALID_ARGUMENT;
+    if (method_ == RB200_MG_MIXED && which == 1) return RB200_UNSUPPORTED;
     SolveState prof{};
     prof.rz = 1.0;
     prof.alpha = 1e-6;
@@ -891,7 +1019,7 @@ int PcgSolver::profile(int which, int launches, double* avg_ms) {
     const dim3 grid = slab_grid(g_), block(TX, TY, 1);
     auto launch = [&]() {
         if (which == 0)
-            k_pass1<ZC><<<grid, block, kSmemPass1, stream_>>>(g_, st_, z_, d_[0], d_[1], maps_, part_, nullptr);
+            k_pass1<ZC><<<grid, block, kSmemPass1, stream_>>>(g_, st_, z_, d_[0], d_[1], q_, maps_, part_, nullptr);
         else if (jac)
             k_pass2<ZC, true><<<grid, block, kSmemSlab, stream_>>>(g_, st_, p_, r_, z_, d_[0], d_[1], maps_, part_,
                                                                    nullptr);
@@ -983,6 +1111,7 @@ int static_solve_jacobi(const GridDev& g, const double* rhs, double* pressure, d
     B.d0 = B.r + kStaticMaxCells;
     B.d1 = B.d0 + kStaticMaxCells;
     B.z = B.d1 + kStaticMaxCells;
+    B.q = nullptr;
     B.part.data = B.z + kStaticMaxCells;
     double* state_slot = B.part.data + size_t(kStaticMaxBlocks) * 8;
     B.st = reinterpret_cast<SolveState*>(state_slot);
@@ -994,7 +1123,7 @@ int static_solve_jacobi(const GridDev& g, const double* rhs, double* pressure, d
     // The array keeps the previous call's contents: the ticket must start at 0.
     RB200_CUDA(cudaMemsetAsync(B.part.ticket, 0, sizeof(unsigned), stream));
     RB200_CUDA(cudaMemcpyAsync(B.st, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream));
-    launch_start(g, true, B, stream);
+    launch_start(g, RB200_JACOBI_PCG_V1, B, nullptr, stream);
     RB200_CUDA(cudaGetLastError());
     const int chunk = 16;
     int last_it = -1, stalls = 0;
@@ -1012,8 +1141,8 @@ int static_solve_jacobi(const GridDev& g, const double* rhs, double* pressure, d
             stalls = 0;
             last_it = h.it;
         }
-        for (int q = 0; q < chunk; ++q) launch_iteration(g, true, B, stream);
-        launch_check(g, true, B, stream);
+        for (int q = 0; q < chunk; ++q) launch_iteration(g, RB200_JACOBI_PCG_V1, B, nullptr, stream);
+        launch_check(g, RB200_JACOBI_PCG_V1, B, nullptr, stream);
         RB200_CUDA(cudaGetLastError());
     }
     fill_report(h, report);

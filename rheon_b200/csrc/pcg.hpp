@@ -5,6 +5,7 @@
 #include <cuda.h>
 
 #include "internal.hpp"
+#include "mg.hpp"
 
 namespace rb200 {
 
@@ -19,13 +20,15 @@ struct SolveState {
     double threshold, dt, divergence_limit, relative, absolute;
     double true_l2, true_max, true_div;
     double incompatible_sum, incompatible_budget;
+    double beta_next;   // flexible method: beta pending a true-residual check
     int it;             // completed iterations
     int max_it;
     int dsel;           // which direction buffer holds the current direction
     int flags;
     int status;         // rb200_status, or ST_RUNNING
     int breakdown_it;
-    int pad0, pad1;
+    int flexible;       // beta = -z.q / d.q (flexible CG) instead of rz'/rz
+    int pad1;
 };
 
 enum : int {
@@ -88,6 +91,8 @@ private:
     double* r_ = nullptr;
     double* d_[2] = {nullptr, nullptr};
     double* z_ = nullptr;  // preconditioned residual
+    double* q_ = nullptr;  // K d, stored by the flexible (multigrid) method
+    Multigrid mg_;
     TmaMaps maps_{};
     Partials part_{nullptr, nullptr};
     int part_blocks_ = 0;

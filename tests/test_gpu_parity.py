@@ -435,3 +435,58 @@ def test_buoyant_tracer_step_matches_the_oracle():
         for d in range(3):
             assert relerr(got[d].astype(np.float64), ref[d].astype(np.float64)) <= 1e-6
         assert relerr(gtr.astype(np.float64), tr.astype(np.float64)) <= 1e-6
+
+
+# ------------------------------------------------------------------ mixed-precision multigrid
+MG = R.PressureImplementation.MG_MIXED
+
+
+@pytest.mark.parametrize("counts", [[1, 1, 1], [3, 1, 1], [5, 4, 3]])
+def test_multigrid_recovers_manufactured_pressure_on_small_grids(counts):
+    # tests/implementation_contract.rs:57-84, with the multigrid method.
+    g = R.GridGeometry(counts, [0.2, 0.35, 0.7])
+    exact = np.sin(np.arange(g.cell_len()) * 0.7)
+    _, rhs = O.apply_full(og(g), 1.3, exact)
+    ws = R.PressureWorkspace(g, 1 << 30, MG, density=1.3)
+    rep = ws.solve_rhs(R.PressureOperator(g, 1.3), rhs, 0.02, S())
+    assert rep.predicted_divergence_max <= 1e-9
+    assert np.max(np.abs(ws.pressure() - exact + exact[0])) < 1e-8
+
+
+@pytest.mark.parametrize("counts", [[32, 32, 32], [64, 64, 64], [40, 40, 40], [64, 32, 16], [48, 24, 96]])
+@pytest.mark.parametrize("rel", [1e-8, 1e-10])
+def test_multigrid_reaches_the_target_residual_in_few_iterations(counts, rel):
+    g = R.GridGeometry(counts)
+    rhs = compatible_rhs(g, seed=21)
+    ws = R.PressureWorkspace(g, 1 << 34, MG)
+    rep = ws.solve_rhs(R.PressureOperator(g, 1.0), rhs, 0.25, S(rel, 0.0, 1.7976931348623157e308, 500))
+    # judged at convergence by the FP64 true residual, recomputed by the oracle
+    st, q = O.qualify_pressure(og(g), 1.0, rhs, 0.25, O.settings(rel, 0.0, 1.7976931348623157e308, 1),
+                               ws.pressure())
+    assert st == O.OK, (q.true_residual_l2, rel * np.linalg.norm(rhs))
+    assert rep.iterations <= 40, rep.iterations
+    ref = O.solve_rhs(og(g), 1.0, O.JACOBI_PCG_V1, rhs, 0.25, O.settings(1e-12, 0.0, 1.7976931348623157e308, 100000))
+    assert relerr(ws.pressure(), ref.pressure) < 1e3 * rel
+
+
+def test_mixed_carrier_tracks_the_fp64_oracle():
+    """Mixed precision (FP32 faces, FP32 advection, FP32 V-cycles in FP64 FCG)
+    against the FP64-storage oracle step: divergence of the stored faces and
+    velocity error per step."""
+    n = (64, 64, 64)
+    g = R.GridGeometry(n)
+    faces64 = W.fourier_faces(n, dtype=np.float64)
+    sim = R.CarrierSimulation(g, R.CarrierConfig.mixed(pressure=S(1e-8, 0.0, 1.7976931348623157e308, 500)))
+    sim.upload([f.astype(np.float32) for f in faces64])
+    s = O.settings(1e-8, 0.0, 1.7976931348623157e308, 100000)
+    ref = faces64
+    for step in range(3):
+        rep = sim.step(R.StepParams(1e30, cfl=0.5))
+        prm = O.StepParams(rep.dt, 1.0, O.JACOBI_PCG_V1, s, 0.0, 0, 8)
+        st, ref, _, orep = O.carrier_step(og(g), ref, prm)
+        assert st == O.OK
+        got = sim.download()
+        err = max(relerr(got[d].astype(np.float64), ref[d]) for d in range(3))
+        assert err < 1e-4, (step, err)
+        assert rep.actual_divergence_max < 1e-3, rep.actual_divergence_max
+        assert rep.pressure.iterations <= 40
