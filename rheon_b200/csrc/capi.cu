@@ -333,7 +333,7 @@ int rb200_workspace_create(const rb200_grid* grid, double density, int method, u
         set_error("invalid grid or density");
         return rc;
     }
-    if (method != RB200_JACOBI_PCG_V1 && method != RB200_RBSGS_PCG && method != RB200_MG_MIXED) {
+    if (method < RB200_JACOBI_PCG_V1 || method > RB200_MG_MIXED) {
         set_error("method not available on the device");
         return RB200_UNSUPPORTED;
     }

@@ -163,8 +163,8 @@ __global__ void __launch_bounds__(EW) k_init_sums(GridDev g, SolveState* st, con
 // red cells (its forward red solve) and leaves the rest to its sweep kernels.
 // Used for the initial residual (MODE_INIT, src = b) and for the restart
 // (MODE_REPLACE, src = the true residual in the spare direction buffer).
-// KIND: 0 Jacobi, 1 red-black SGS, 2 multigrid (copy only; the V-cycle and
-// k_mg_finish form z).
+// KIND: 0 Jacobi, 1 red-black SGS, 2 copy only (multigrid and lexicographic
+// SGS form z in their own kernels).
 enum : int { KIND_JACOBI = 0, KIND_RBSGS = 1, KIND_MG = 2 };
 template <int KIND>
 __global__ void __launch_bounds__(EW) k_load_residual(GridDev g, SolveState* st, const double* b,
@@ -341,7 +341,9 @@ __global__ void __launch_bounds__(TILE_THREADS) k_pass1(GridDev g, SolveState* s
 // from the direction slab, the recursive norm, and the preconditioner's local
 // part: Jacobi z = r/D with r.z (precondition_jacobi, :534-575); red-black SGS
 // stores y = r/D on the red cells.
-template <int ZC, bool JACOBI>
+// PRE: 0 Jacobi (z = r/D and r.z here), 1 red-black SGS (y = r/D on red
+// cells), 2 none (lexicographic SGS forms z in its sweeps).
+template <int ZC, int PRE>
 __global__ void __launch_bounds__(TILE_THREADS) k_pass2(GridDev g, SolveState* st, double* __restrict__ p,
                                                         double* __restrict__ r, double* __restrict__ z,
                                                         const double* d0, const double* d1,
@@ -385,11 +387,11 @@ __global__ void __launch_bounds__(TILE_THREADS) k_pass2(GridDev g, SolveState* s
         double rc = rv[q] - alpha * qv;
         r[c] = rc;
         acc_rr.add(rc * rc);
-        if (JACOBI) {
+        if (PRE == 0) {
             double zc = rc / diag_at(g, i, j, k);
             z[c] = zc;
             acc_rz.add(rc * zc);
-        } else if (((i + j + k) & 1) == 0) {
+        } else if (PRE == 1 && ((i + j + k) & 1) == 0) {
             z[c] = rc / diag_at(g, i, j, k);
         }
     }
@@ -411,7 +413,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_pass2(GridDev g, SolveState* s
             st->recursive_l2 = recursive_l2;
             if (trace) trace[it - 1].recursive_l2 = recursive_l2;
             bool candidate = recursive_l2 <= st->threshold || it == st->max_it;
-            if (JACOBI) {
+            if (PRE == 0) {
                 double rz = dd_value(sums[1]);
                 if (candidate) {
                     st->rz_next = rz;
@@ -599,6 +601,73 @@ __global__ void __launch_bounds__(EW) k_mg_finish(GridDev g, SolveState* st, con
     }
 }
 
+// ------------------------------------------------------------ lexicographic SGS
+// precondition_sgs (src/pressure.rs:467-532): forward
+//   y_i = (r_i + sum_{lower d} w_d y_{i-s_d}) / D_i    (d = X, Y, Z in order)
+// then reverse
+//   z_i = y_i + (sum_{upper d} w_d z_{i+s_d}) / D_i
+// over rows 1..N-1 (row 0 is the eliminated gauge row, z_0 = 0). Each row
+// depends only on its lower (upper) neighbours, so any order that respects
+// those dependencies computes the reference's lexicographic sweep bit for bit
+// (the reference's own tiled wavefront, src/sgs.rs:56-104, uses the same
+// fact). Here a launch handles one diagonal wave of 8^3 tiles
+// (tx + ty + tz = wave) and a block walks its tile's hyperplanes
+// lx + ly + lz = l with a barrier between them.
+constexpr int SGS_T = 8;
+
+__global__ void __launch_bounds__(SGS_T * SGS_T * SGS_T) k_sgs_wave(GridDev g, SolveState* st,
+                                                                    const double* __restrict__ r, double* z,
+                                                                    int wave, int reverse, int mode) {
+    if (!gate(st->flags, mode)) return;
+    const int ntz = (g.n[2] + SGS_T - 1) / SGS_T;
+    const int tx = blockIdx.x, ty = blockIdx.y, tz = wave - tx - ty;
+    if (tz < 0 || tz >= ntz) return;
+    const int lx = threadIdx.x % SGS_T, ly = (threadIdx.x / SGS_T) % SGS_T, lz = threadIdx.x / (SGS_T * SGS_T);
+    const int i = tx * SGS_T + lx, j = ty * SGS_T + ly, k = tz * SGS_T + lz;
+    const bool in = i < g.n[0] && j < g.n[1] && k < g.n[2];
+    const int c = in ? cell_idx(g, i, j, k) : 0;
+    const int sy = g.n[0], sz = g.n[0] * g.n[1];
+    const int mine = lx + ly + lz;
+    for (int step = 0; step < 3 * SGS_T - 2; ++step) {
+        const int l = reverse ? 3 * SGS_T - 3 - step : step;
+        if (in && mine == l && c != 0) {
+            const double D = diag_at(g, i, j, k);
+            if (!reverse) {
+                double value = r[c];
+                if (i > 0) value += g.weight[0] * z[c - 1];
+                if (j > 0) value += g.weight[1] * z[c - sy];
+                if (k > 0) value += g.weight[2] * z[c - sz];
+                z[c] = value / D;
+            } else {
+                double correction = 0.0;
+                if (i + 1 < g.n[0]) correction += g.weight[0] * z[c + 1];
+                if (j + 1 < g.n[1]) correction += g.weight[1] * z[c + sy];
+                if (k + 1 < g.n[2]) correction += g.weight[2] * z[c + sz];
+                z[c] = z[c] + correction / D;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// r.z after a lexicographic SGS application, then the preconditioner decision.
+__global__ void __launch_bounds__(EW) k_sgs_dot(GridDev g, SolveState* st, const double* __restrict__ r,
+                                                const double* __restrict__ z, int mode, Partials part,
+                                                rb200_trace* trace) {
+    __shared__ BlockReduce<1, 0> sm;
+    if (!gate(st->flags, mode)) return;
+    Neu acc;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x)
+        if (c != 0) acc.add(r[c] * z[c]);
+    dd sums[1] = {acc.as_dd()};
+    double none[1];
+    block_reduce<1, 0>(sm, sums, none);
+    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
+        fold_partials<1, 0>(part, gridDim.x, sm, sums, none);
+        if (threadIdx.x == 0) decide_rz(st, trace, dd_value(sums[0]), mode);
+    }
+}
+
 // ------------------------------------------------------------ red-black SGS
 // Symmetric Gauss-Seidel preconditioner in red-black order on the
 // gauge-eliminated system (cell 0, red, is removed): forward reds then blacks,
@@ -680,8 +749,9 @@ static int ew_blocks(int n) {
 // Dynamic shared memory above 48 KB must be opted into per kernel.
 static int set_smem_attrs() {
     RB200_CUDA(cudaFuncSetAttribute(k_pass1<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemPass1)));
-    RB200_CUDA(cudaFuncSetAttribute(k_pass2<ZC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemSlab)));
-    RB200_CUDA(cudaFuncSetAttribute(k_pass2<ZC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemSlab)));
+    RB200_CUDA(cudaFuncSetAttribute(k_pass2<ZC, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemSlab)));
+    RB200_CUDA(cudaFuncSetAttribute(k_pass2<ZC, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemSlab)));
+    RB200_CUDA(cudaFuncSetAttribute(k_pass2<ZC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemSlab)));
     RB200_CUDA(cudaFuncSetAttribute(k_true_residual<ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     int(kSmemSlab)));
     return RB200_OK;
@@ -741,6 +811,19 @@ static TmaMaps make_maps(const GridDev& g, const double* z, const double* d0, co
     return m;
 }
 
+// One lexicographic SGS application: forward waves, reverse waves, r.z.
+static int launch_sgs(const GridDev& g, const Bufs& B, int mode, cudaStream_t s) {
+    const int nt[3] = {(g.n[0] + SGS_T - 1) / SGS_T, (g.n[1] + SGS_T - 1) / SGS_T, (g.n[2] + SGS_T - 1) / SGS_T};
+    const int waves = nt[0] + nt[1] + nt[2] - 2;
+    const dim3 grid(nt[0], nt[1]);
+    for (int w = 0; w < waves; ++w)
+        k_sgs_wave<<<grid, SGS_T * SGS_T * SGS_T, 0, s>>>(g, B.st, B.r, B.z, w, 0, mode);
+    for (int w = waves - 1; w >= 0; --w)
+        k_sgs_wave<<<grid, SGS_T * SGS_T * SGS_T, 0, s>>>(g, B.st, B.r, B.z, w, 1, mode);
+    k_sgs_dot<<<ew_blocks(g.cells), EW, 0, s>>>(g, B.st, B.r, B.z, mode, B.part, B.trace);
+    return 2 * waves + 1;
+}
+
 // Initial residual and preconditioned start (src/pressure.rs:603-650).
 // `mg` is the multigrid hierarchy of the mixed method (nullptr otherwise).
 static int launch_start(const GridDev& g, int method, const Bufs& B, const Multigrid* mg, cudaStream_t s) {
@@ -759,6 +842,7 @@ static int launch_start(const GridDev& g, int method, const Bufs& B, const Multi
         return 4;
     }
     k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part, B.trace);
+    if (method == RB200_SGS_PCG_V1) return 2 + launch_sgs(g, B, MODE_INIT, s);
     int n = 2 + mg->enqueue(B.r, B.st, MODE_INIT, s);
     k_mg_finish<<<eb, EW, 0, s>>>(g, B.st, mg->x0(), B.z, B.r, B.q, MODE_INIT, B.part, B.trace);
     return n + 1;
@@ -772,16 +856,21 @@ static int launch_iteration(const GridDev& g, int method, const Bufs& B, const M
     k_pass1<ZC><<<grid, block, kSmemPass1, s>>>(g, B.st, B.z, B.d0, B.d1, flexible ? B.q : nullptr, B.maps, B.part,
                                                 B.trace);
     if (method == RB200_JACOBI_PCG_V1) {
-        k_pass2<ZC, true><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part,
+        k_pass2<ZC, 0><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part,
                                                          B.trace);
         return 2;
     }
     if (method == RB200_RBSGS_PCG) {
-        k_pass2<ZC, false><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part,
+        k_pass2<ZC, 1><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part,
                                                           B.trace);
         k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_ITER);
         k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_ITER, B.part, B.trace);
         return 4;
+    }
+    if (method == RB200_SGS_PCG_V1) {
+        k_pass2<ZC, 2><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part,
+                                                          B.trace);
+        return 2 + launch_sgs(g, B, MODE_ITER, s);
     }
     k_mg_update<<<eb, EW, 0, s>>>(g, B.st, B.p, B.r, B.d0, B.d1, B.q, B.part, B.trace);
     int n = 2 + mg->enqueue(B.r, B.st, MODE_ITER, s);
@@ -807,6 +896,7 @@ static int launch_check(const GridDev& g, int method, const Bufs& B, const Multi
         return 4;
     }
     k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part, B.trace);
+    if (method == RB200_SGS_PCG_V1) return 2 + launch_sgs(g, B, MODE_REPLACE, s);
     int n = 2 + mg->enqueue(B.r, B.st, MODE_REPLACE, s);
     k_mg_finish<<<eb, EW, 0, s>>>(g, B.st, mg->x0(), B.z, B.r, B.q, MODE_REPLACE, B.part, B.trace);
     return n + 1;
@@ -857,8 +947,7 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
     g_ = g;
     method_ = method;
     stream_ = stream;
-    if (method != RB200_JACOBI_PCG_V1 && method != RB200_RBSGS_PCG && method != RB200_MG_MIXED)
-        return RB200_UNSUPPORTED;
+    if (method < RB200_JACOBI_PCG_V1 || method > RB200_MG_MIXED) return RB200_UNSUPPORTED;
     int rc = set_smem_attrs();
     if (rc) return rc;
     part_blocks_ = std::max(slab_blocks(g), EW_CAP);
@@ -887,7 +976,7 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
     RB200_CUDA(cudaMallocHost(&h_st_, 2 * sizeof(SolveState)));
     for (auto& e : ev_) RB200_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     maps_ = make_maps(g, z_, d_[0], d_[1], p_);
-    chunk_ = method == RB200_MG_MIXED ? 4 : (g.cells >= (1 << 20) ? 32 : 16);
+    chunk_ = (method == RB200_MG_MIXED || method == RB200_SGS_PCG_V1) ? 4 : (g.cells >= (1 << 20) ? 32 : 16);
     return capture_chunk();
 }
 
@@ -1021,10 +1110,13 @@ int PcgSolver::profile(int which, int launches, double* avg_ms) {
         if (which == 0)
             k_pass1<ZC><<<grid, block, kSmemPass1, stream_>>>(g_, st_, z_, d_[0], d_[1], q_, maps_, part_, nullptr);
         else if (jac)
-            k_pass2<ZC, true><<<grid, block, kSmemSlab, stream_>>>(g_, st_, p_, r_, z_, d_[0], d_[1], maps_, part_,
+            k_pass2<ZC, 0><<<grid, block, kSmemSlab, stream_>>>(g_, st_, p_, r_, z_, d_[0], d_[1], maps_, part_,
+                                                                   nullptr);
+        else if (method_ == RB200_SGS_PCG_V1)
+            k_pass2<ZC, 2><<<grid, block, kSmemSlab, stream_>>>(g_, st_, p_, r_, z_, d_[0], d_[1], maps_, part_,
                                                                    nullptr);
         else
-            k_pass2<ZC, false><<<grid, block, kSmemSlab, stream_>>>(g_, st_, p_, r_, z_, d_[0], d_[1], maps_, part_,
+            k_pass2<ZC, 1><<<grid, block, kSmemSlab, stream_>>>(g_, st_, p_, r_, z_, d_[0], d_[1], maps_, part_,
                                                                     nullptr);
     };
     launch();  // warm

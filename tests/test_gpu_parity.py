@@ -178,7 +178,10 @@ def S(rel=1e-11, abs_=1e-12, div=1e-9, it=1000):
     return R.PressureSettings(rel, abs_, div, it)
 
 
-METHODS = [R.PressureImplementation.JACOBI_PCG_V1, R.PressureImplementation.RBSGS_PCG]
+METHODS = [R.PressureImplementation.JACOBI_PCG_V1, R.PressureImplementation.SGS_PCG_V1,
+           R.PressureImplementation.RBSGS_PCG]
+# device method -> oracle method it must reproduce per iteration
+EXACT = {R.PressureImplementation.JACOBI_PCG_V1: O.JACOBI_PCG_V1, R.PressureImplementation.SGS_PCG_V1: O.SGS_PCG_V1}
 
 
 @pytest.mark.parametrize("method", METHODS)
@@ -253,17 +256,18 @@ def compatible_rhs(g, seed=11, dtype=np.float64):
 
 # [64, 40, 24] and [96, 16, 12] take the TMA slab path (even nx, at least one
 # slab box in every direction); the others take the cp.async path.
+@pytest.mark.parametrize("method", list(EXACT))
 @pytest.mark.parametrize("counts", [[32, 32, 32], [17, 10, 9], [48, 20, 7], [64, 40, 24], [96, 16, 12]])
-def test_jacobi_pcg_per_iteration_parity(counts):
+def test_pcg_per_iteration_parity(counts, method):
     """Every iteration's scalars and the iterates track the oracle to 1e-12."""
     g = R.GridGeometry(counts)
     rhs = compatible_rhs(g)
-    iters = 200
+    iters = 200 if method == R.PressureImplementation.JACOBI_PCG_V1 else 60
     s = S(0.0, 0.0, 1.7976931348623157e308, iters)
-    ref = O.solve_rhs(og(g), 1.0, O.JACOBI_PCG_V1, rhs, 0.25, O.settings(0.0, 0.0, 1.7976931348623157e308, iters),
+    ref = O.solve_rhs(og(g), 1.0, EXACT[method], rhs, 0.25, O.settings(0.0, 0.0, 1.7976931348623157e308, iters),
                       trace=True)
     assert ref.status == O.ITERATION_LIMIT
-    ws = R.PressureWorkspace(g, 1 << 34)
+    ws = R.PressureWorkspace(g, 1 << 34, method)
     ws.set_trace(iters)
     with pytest.raises(R.PressureError) as e:
         ws.solve_rhs(R.PressureOperator(g, 1.0), rhs, 0.25, s)
@@ -282,7 +286,7 @@ def test_jacobi_pcg_per_iteration_parity(counts):
     assert relerr(ws.pressure(), ref.pressure) <= 1e-12
     # iterates at intermediate counts (IterationLimit leaves the k-th iterate)
     for k in (1, 7, 50):
-        refk = O.solve_rhs(og(g), 1.0, O.JACOBI_PCG_V1, rhs, 0.25, O.settings(0.0, 0.0, 1.7976931348623157e308, k))
+        refk = O.solve_rhs(og(g), 1.0, EXACT[method], rhs, 0.25, O.settings(0.0, 0.0, 1.7976931348623157e308, k))
         with pytest.raises(R.PressureError):
             ws.solve_rhs(R.PressureOperator(g, 1.0), rhs, 0.25, S(0.0, 0.0, 1.7976931348623157e308, k))
         assert relerr(ws.pressure(), refk.pressure) <= 1e-12
