@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--max-iters", type=int, default=0,
                     help="cap PCG iterations per step (profiling runs only; 0 = solve to 1e-8)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-instances", type=int, default=64)
+    ap.add_argument("--batched-steps", type=int, default=20)
     ap.add_argument("--no-profile", action="store_true")
     return ap.parse_args()
 
@@ -166,6 +169,69 @@ def run_e2e(args, g, cfg, faces, prm, flush, local, world):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         total = float(tt.item())
     return total
+
+
+def run_batched(args, local, flush):
+    """Batched uneven instances: boxes with edges drawn by seed from
+    {32, 48, 64, 96, 128}, each with its own random-Fourier velocity, in the
+    mixed-precision configuration at rel. residual 1e-8. Every batched step
+    launches one step graph per instance (each on its own stream) and waits for
+    all; the makespan is timed with CUDA events (a start event every instance
+    stream waits on, and a join stream that waits on every instance's end)."""
+    import torch
+
+    import rheon_b200 as R
+    from rheon_b200 import workloads as W
+
+    edges = np.array([32, 48, 64, 96, 128])
+    pick = ((W.uniform(args.seed, 40, args.batched_instances) + 1.0) * 0.5 * len(edges)).astype(int)
+    sizes = [int(edges[min(i, len(edges) - 1)]) for i in pick]
+    cfg = R.CarrierConfig.mixed(pressure=R.PressureSettings(1e-8, 0.0, MAXF, 1000), device=local)
+    sims = []
+    for i, n in enumerate(sizes):
+        sim = R.CarrierSimulation(R.GridGeometry((n, n, n)), cfg)
+        sim.upload(W.fourier_faces((n, n, n), seed=args.seed + 1000 + i, dtype=np.float32))
+        sims.append(sim)
+    streams = [torch.cuda.ExternalStream(s.stream(), device=local) for s in sims]
+    join = torch.cuda.Stream(device=local)
+    prm = R.StepParams(MAXF, cfl=0.5)
+    for _ in range(max(3, args.warmup)):
+        out = R.step_all(sims, [prm] * len(sims))
+        if any(st != 0 for st, _ in out):
+            raise RuntimeError("batched warm-up step rejected")
+    total_ms, cell_steps, iters = 0.0, 0, []
+    for _ in range(args.batched_steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(join)
+        for st in streams:
+            st.wait_event(a)
+        for sim in sims:
+            sim.step_async(prm)
+        for st in streams:
+            e = torch.cuda.Event()
+            e.record(st)
+            join.wait_event(e)
+        b.record(join)
+        reps = [sim.step_wait() for sim in sims]
+        b.synchronize()
+        total_ms += a.elapsed_time(b)
+        cell_steps += sum(n ** 3 for n in sizes)
+        iters += [r.pressure.iterations for r in reps]
+    for sim in sims:
+        sim.close()
+    return {
+        "value": cell_steps / (total_ms / 1e3),
+        "unit": UNIT,
+        "instances": len(sizes),
+        "edges": {str(e): sizes.count(int(e)) for e in edges},
+        "steps": args.batched_steps,
+        "ms_per_batched_step": total_ms / args.batched_steps,
+        "iterations_per_step": statistics.mean(iters),
+        "dtype": "mixed (f32 faces and V-cycles, f64 residual/accumulation/coarse solve)",
+    }
 
 
 # ------------------------------------------------------------------ our arm
@@ -283,6 +349,10 @@ def run_ours(args, world, rank, local):
                               "vs_plain_f64": vvalue / value}
             vs.close()
 
+    batched = None
+    if not args.no_batched and rank == 0 and world == 1:
+        batched = run_batched(args, local, flush)
+
     result = {
         "metric": METRIC,
         "value": value,
@@ -330,6 +400,8 @@ def run_ours(args, world, rank, local):
     }
     if variants:
         result["variants"] = variants
+    if batched:
+        result["batched"] = batched
     sim.close()
     return result
 

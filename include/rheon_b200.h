@@ -324,8 +324,21 @@ RB200_API int rb200_carrier_download(rb200_carrier* carrier, void* u, void* v, v
 /* Device pointers of the accepted state (valid until the next step). */
 RB200_API int rb200_carrier_state_device(rb200_carrier* carrier, void** u, void** v, void** w,
                                float** tracer);
+/* One step as one CUDA graph (dt policy, advection, RHS, the pressure solve
+ * as a device-controlled WHILE loop, correction, gates, tracer, commit), then
+ * a wait for its report. Cancellation is polled before the step. Returns the
+ * step status (RB200_OK when the step was accepted and published). */
 RB200_API int rb200_carrier_step(rb200_carrier* carrier, const rb200_step_params* params,
-                       rb200_step_report* report, rb200_cancel_fn cancelled, void* ctx);
+                                 rb200_step_report* report, rb200_cancel_fn cancelled, void* ctx);
+/* Launch a step without waiting (one per carrier in flight); carriers on
+ * different streams overlap on the device. rb200_carrier_step_wait blocks for
+ * the report and returns the step status. */
+RB200_API int rb200_carrier_step_async(rb200_carrier* carrier, const rb200_step_params* params);
+RB200_API int rb200_carrier_step_wait(rb200_carrier* carrier, rb200_step_report* report);
+/* Batched instances: launch one step of every carrier, then wait for all.
+ * statuses[i] receives each step's status; returns the first launch error. */
+RB200_API int rb200_carriers_step(rb200_carrier* const* carriers, size_t count, const rb200_step_params* params,
+                                  rb200_step_report* reports, int* statuses);
 /* rb200_workspace_profile on the carrier's pressure solver. */
 RB200_API int rb200_carrier_profile(rb200_carrier* carrier, int which, int launches, double* avg_ms);
 /* Last pressure of the carrier (host copy). */

@@ -26,7 +26,7 @@ __all__ = [
     "GridGeometry", "PressureImplementation", "PressureSettings", "PressureReport", "PressureError",
     "OperatorError", "ProviderRejection", "PressureOperator", "PressureWorkspace", "PressureRequest",
     "B200PressureProvider", "CarrierSimulation", "CarrierConfig", "StepParams", "StepReport",
-    "SimulationError", "advect_velocity", "advect_tracer", "device_count", "status_name",
+    "SimulationError", "advect_velocity", "advect_tracer", "device_count", "status_name", "step_all",
 ]
 
 
@@ -595,14 +595,49 @@ class CarrierSimulation:
             raise SimulationError(st)
         return out
 
+    @staticmethod
+    def _params(params: StepParams) -> N.StepParams:
+        return N.StepParams(params.requested_dt, params.cfl, params.buoyancy, int(params.iteration_limit_ok),
+                            int(params.skip_gates))
+
+    @staticmethod
+    def _report(r: N.StepReport) -> StepReport:
+        return StepReport(r.dt, r.time, int(r.generation), PressureReport.from_c(r.pressure), r.pressure_status,
+                          r.actual_divergence_max, r.courant, r.velocity_rate, r.pressure_ms,
+                          int(r.kernel_launches))
+
     def step(self, params: StepParams, cancelled: Optional[Callable[[], bool]] = None) -> StepReport:
-        p = N.StepParams(params.requested_dt, params.cfl, params.buoyancy, int(params.iteration_limit_ok),
-                         int(params.skip_gates))
+        """One step (one CUDA graph); raises SimulationError if it is rejected."""
         r = N.StepReport()
-        st = lib().rb200_carrier_step(self._handle, C.byref(p), C.byref(r), _cancel_cb(cancelled), None)
-        rep = StepReport(r.dt, r.time, int(r.generation), PressureReport.from_c(r.pressure), r.pressure_status,
-                         r.actual_divergence_max, r.courant, r.velocity_rate, r.pressure_ms,
-                         int(r.kernel_launches))
+        st = lib().rb200_carrier_step(self._handle, C.byref(self._params(params)), C.byref(r),
+                                      _cancel_cb(cancelled), None)
+        rep = self._report(r)
         if st != N.OK:
             raise SimulationError(st, rep)
         return rep
+
+    def step_async(self, params: StepParams) -> None:
+        """Launch one step without waiting; pair with step_wait()."""
+        st = lib().rb200_carrier_step_async(self._handle, C.byref(self._params(params)))
+        if st != N.OK:
+            raise SimulationError(st)
+
+    def step_wait(self) -> StepReport:
+        r = N.StepReport()
+        st = lib().rb200_carrier_step_wait(self._handle, C.byref(r))
+        rep = self._report(r)
+        if st != N.OK:
+            raise SimulationError(st, rep)
+        return rep
+
+
+def step_all(sims: Sequence["CarrierSimulation"], params: Sequence[StepParams]):
+    """Batched instances: one step of every carrier, launched together so that
+    they overlap on the device; returns [(status, StepReport)]."""
+    n = len(sims)
+    handles = (C.c_void_p * n)(*[s._handle.value for s in sims])
+    prm = (N.StepParams * n)(*[CarrierSimulation._params(p) for p in params])
+    reps = (N.StepReport * n)()
+    sts = (C.c_int * n)()
+    lib().rb200_carriers_step(handles, n, prm, reps, sts)
+    return [(int(sts[i]), CarrierSimulation._report(reps[i])) for i in range(n)]

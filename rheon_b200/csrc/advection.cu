@@ -1,163 +1,20 @@
-// Semi-Lagrangian advection on the device (src/advection.rs, src/sampling.rs).
-// One thread per face (or cell); f64 arithmetic on T-stored samples exactly as
-// the reference orders it, so f32 storage reproduces Rheon bit for bit.
-#include "internal.hpp"
+// Standalone semi-Lagrangian advection kernels (src/advection.rs); the device
+// bodies are in advect.cuh.
+#include "advect.cuh"
 
 namespace rb200 {
 
-constexpr int ADV_THREADS = 256;
-
-template <class R>
-__device__ __forceinline__ R clampd(R x, R lo, R hi) {
-    // f64::clamp: if x < min { min } then if x > max { max }.
-    if (x < lo) x = lo;
-    if (x > hi) x = hi;
-    return x;
-}
-
-// ScalarSampler::sample (src/sampling.rs:74-122) in arithmetic type R: double
-// reproduces the reference; float is the mixed-precision path.
-template <class T, class R>
-__device__ __forceinline__ R sample(const GridDev& g, const T* __restrict__ values, const int dims[3], const R off[3],
-                                    const R pos[3], int& flag) {
-    int lo[3], hi[3];
-    R t[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        R x = clampd<R>(pos[d], R(g.o[d]), R(g.up[d]));
-        R q = clampd<R>((x - R(g.o[d])) / R(g.h[d]) - off[d], R(0), R(dims[d] - 1));
-        if (!isfinite(q)) {
-            flag |= VF_ARITH;
-            q = R(0);
-        }
-        lo[d] = int(floor(q));
-        hi[d] = min(lo[d] + 1, dims[d] - 1);
-        t[d] = q - R(lo[d]);
-    }
-    R result = R(0);
-    R minimum = R(CUDART_INF);
-    R maximum = R(-CUDART_INF);
-#pragma unroll
-    for (int z = 0; z < 2; ++z)
-#pragma unroll
-        for (int y = 0; y < 2; ++y)
-#pragma unroll
-            for (int x = 0; x < 2; ++x) {
-                int px = x ? hi[0] : lo[0];
-                int py = y ? hi[1] : lo[1];
-                int pz = z ? hi[2] : lo[2];
-                R weight = R(1);
-                weight = weight * (x ? t[0] : R(1) - t[0]);
-                weight = weight * (y ? t[1] : R(1) - t[1]);
-                weight = weight * (z ? t[2] : R(1) - t[2]);
-                R value = R(__ldg(values + (px + dims[0] * (py + dims[1] * pz))));
-                minimum = fmin(minimum, value);
-                maximum = fmax(maximum, value);
-                result += weight * value;
-            }
-    if (!isfinite(result)) flag |= VF_ARITH;
-    return clampd<R>(result, minimum, maximum);
-}
-
-template <class T>
-struct Faces {
-    const T* f[3];
-};
-
-template <class R>
-__device__ __forceinline__ void face_geometry(const GridDev& g, int a, int dims[3], R off[3]) {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        dims[d] = g.fc[a][d];
-        off[d] = d == a ? R(0) : R(0.5);
-    }
-}
-
-template <class T, class R>
-__device__ __forceinline__ void velocity_sample(const GridDev& g, const Faces<T>& vel, const R pos[3], R out[3],
-                                                int& flag) {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        int dims[3];
-        R off[3];
-        face_geometry<R>(g, a, dims, off);
-        out[a] = sample<T, R>(g, vel.f[a], dims, off, pos, flag);
-    }
-}
-
-// VelocitySampler::departure (src/sampling.rs:160-175).
-template <class R>
-__device__ __forceinline__ void departure(const GridDev& g, const R pos[3], const R vel[3], R dt, R out[3],
-                                          int& flag) {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        R value = pos[d] - dt * vel[d];
-        if (!isfinite(value)) flag |= VF_ARITH;
-        out[d] = clampd<R>(value, R(g.o[d]), R(g.up[d]));
-    }
-}
-
-// VelocitySampler::backtrace (src/sampling.rs:151-159): midpoint RK2.
-template <class T, class R>
-__device__ __forceinline__ void backtrace(const GridDev& g, const Faces<T>& vel, const R pos[3], R dt, R out[3],
-                                          int& flag) {
-    R initial[3], mid[3], v1[3];
-    velocity_sample<T, R>(g, vel, pos, initial, flag);
-    departure<R>(g, pos, initial, R(0.5) * dt, mid, flag);
-    velocity_sample<T, R>(g, vel, mid, v1, flag);
-    departure<R>(g, pos, v1, dt, out, flag);
-}
-
-// advect_velocity (src/advection.rs:28-68): wall-normal faces are exactly 0,
-// every other face samples its own component at the RK2 departure point.
 template <class T, class R>
 __global__ void __launch_bounds__(ADV_THREADS) k_advect_velocity(GridDev g, Faces<T> vel, double dt, T* ou, T* ov, T* ow,
                                                                  const float* __restrict__ tracer, double gb,
                                                                  int* flags) {
-    const long long total = (long long)g.flen[0] + g.flen[1] + g.flen[2];
-    int local = 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        int a = 0;
-        long long f = t;
-        if (f >= g.flen[0]) {
-            f -= g.flen[0];
-            a = 1;
-            if (f >= g.flen[1]) {
-                f -= g.flen[1];
-                a = 2;
-            }
-        }
-        int p[3];
-        p[0] = int(f % g.fc[a][0]);
-        p[1] = int((f / g.fc[a][0]) % g.fc[a][1]);
-        p[2] = int(f / ((long long)g.fc[a][0] * g.fc[a][1]));
-        T* dst = a == 0 ? ou : (a == 1 ? ov : ow);
-        if (p[a] == 0 || p[a] + 1 == g.fc[a][a]) {
-            dst[f] = T(0);
-            continue;
-        }
-        R pos[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) pos[d] = R(g.o[d] + (double(p[d]) + (d == a ? 0.0 : 0.5)) * g.h[d]);
-        R dep[3];
-        backtrace<T, R>(g, vel, pos, R(dt), dep, local);
-        int dims[3];
-        R off[3];
-        face_geometry<R>(g, a, dims, off);
-        T value = T(sample<T, R>(g, vel.f[a], dims, off, dep, local));
-        if (a == 1 && tracer != nullptr && gb != 0.0) {
-            // Buoyancy hook (new): interior Y face, after advection, before pressure.
-            int below = cell_idx(g, p[0], p[1] - 1, p[2]);
-            int above = cell_idx(g, p[0], p[1], p[2]);
-            double c = 0.5 * (double(tracer[below]) + double(tracer[above]));
-            double forced = double(value) + dt * (gb * c);
-            if (!isfinite(forced)) local |= VF_ARITH;
-            value = T(forced);
-        }
-        dst[f] = value;
-    }
-    if (local) atomicOr(flags, local);
+    advect_velocity_body<T, R>(g, vel, dt, ou, ov, ow, tracer, gb, flags);
+}
+
+template <class T, class R>
+__global__ void __launch_bounds__(ADV_THREADS) k_advect_tracer(GridDev g, const float* __restrict__ old, Faces<T> vel,
+                                                               double dt, float* __restrict__ out, int* flags) {
+    advect_tracer_body<T, R>(g, old, vel, dt, out, flags);
 }
 
 template <class T>
@@ -174,26 +31,6 @@ int launch_advect_velocity(const GridDev& g, const T* u, const T* v, const T* w,
         k_advect_velocity<T, double><<<int(blocks), ADV_THREADS, 0, s>>>(g, vel, dt, ou, ov, ow, tracer, gb, flags);
     RB200_CUDA(cudaGetLastError());
     return RB200_OK;
-}
-
-// advect_tracer (src/advection.rs:72-102), evaluated densely; the reference's
-// zero-support skip produces the same bits (tests/advection_contract.rs:7-41).
-template <class T, class R>
-__global__ void __launch_bounds__(ADV_THREADS) k_advect_tracer(GridDev g, const float* __restrict__ old, Faces<T> vel,
-                                                               double dt, float* __restrict__ out, int* flags) {
-    int local = 0;
-    int dims[3] = {g.n[0], g.n[1], g.n[2]};
-    R off[3] = {R(0.5), R(0.5), R(0.5)};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
-        int p[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
-        R pos[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) pos[d] = R(g.o[d] + (double(p[d]) + 0.5) * g.h[d]);
-        R dep[3];
-        backtrace<T, R>(g, vel, pos, R(dt), dep, local);
-        out[c] = float(sample<float, R>(g, old, dims, off, dep, local));
-    }
-    if (local) atomicOr(flags, local);
 }
 
 template <class T>

@@ -98,44 +98,6 @@ struct rb200_provider {
     ~rb200_provider() { delete ws; }
 };
 
-struct rb200_carrier {
-    rb200_carrier_config cfg{};
-    GridDev g{};
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    size_t elem = 4;
-    void* faces[3][3] = {};  // [buffer][axis]
-    int acc = 0;             // accepted buffer
-    float* tracer[2] = {nullptr, nullptr};
-    int tacc = 0;
-    PcgSolver solver;
-    double* d_scalars = nullptr;
-    double* h_scalars = nullptr;
-    int* d_flags = nullptr;
-    int* h_flags = nullptr;
-    cudaEvent_t ev[2] = {nullptr, nullptr};
-    double time = 0.0;
-    uint64_t generation = 0;
-    double rate = 0.0;
-    size_t bytes = 0;
-    std::string err;
-    ~rb200_carrier() {
-        cudaSetDevice(device);
-        if (stream) cudaStreamSynchronize(stream);
-        for (auto& b : faces)
-            for (auto& a : b) cudaFree(a);
-        cudaFree(tracer[0]);
-        cudaFree(tracer[1]);
-        cudaFree(d_scalars);
-        cudaFree(d_flags);
-        if (h_scalars) cudaFreeHost(h_scalars);
-        if (h_flags) cudaFreeHost(h_flags);
-        for (auto& e : ev)
-            if (e) cudaEventDestroy(e);
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
-
 #define RB200_PRIM_BEGIN(grid, density)                 \
     GridDev g;                                          \
     int rc = make_grid_dev(grid, density, &g);          \
@@ -206,81 +168,6 @@ static int advect_prim(const rb200_grid* grid, const T* u, const T* v, const T* 
     return flags_status(f, false);
 }
 
-template <class T>
-static int carrier_step_t(rb200_carrier* c, const rb200_step_params* prm, rb200_step_report* rep,
-                          rb200_cancel_fn cancelled, void* ctx) {
-    const GridDev& g = c->g;
-    // dt policy (src/simulation.rs:952-979): dt = min(requested, budget/rate).
-    double dt = prm->requested_dt;
-    if (prm->cfl > 0.0 && c->rate > 0.0) dt = std::fmin(dt, prm->cfl / c->rate);
-    if (!std::isfinite(dt) || dt <= 0.0 || !std::isfinite(c->time + dt) || c->time + dt <= c->time)
-        return RB200_INVALID_ARGUMENT;
-    rep->dt = dt;
-    if (cancelled && cancelled(ctx)) return RB200_CANCELLED;
-    const int cand = (c->acc + 1) % 3, corr = (c->acc + 2) % 3;
-    const uint64_t launches0 = c->solver.launches();
-    T* const A[3] = {(T*)c->faces[c->acc][0], (T*)c->faces[c->acc][1], (T*)c->faces[c->acc][2]};
-    T* const B[3] = {(T*)c->faces[cand][0], (T*)c->faces[cand][1], (T*)c->faces[cand][2]};
-    T* const Cc[3] = {(T*)c->faces[corr][0], (T*)c->faces[corr][1], (T*)c->faces[corr][2]};
-    const float* tr = c->tracer[0] ? c->tracer[c->tacc] : nullptr;
-    RB200_CUDA(cudaMemsetAsync(c->d_flags, 0, sizeof(int), c->stream));
-    const bool fp32 = c->cfg.fp32_advection != 0;
-    int rc = launch_advect_velocity<T>(g, A[0], A[1], A[2], dt, B[0], B[1], B[2], tr, prm->buoyancy, c->d_flags,
-                                       c->stream, fp32);
-    if (rc) return rc;
-    if ((rc = launch_build_rhs<T>(g, B[0], B[1], B[2], dt, c->solver.b(), c->d_flags, c->stream))) return rc;
-    RB200_CUDA(cudaEventRecord(c->ev[0], c->stream));
-    int ps = c->solver.solve(dt, c->cfg.settings, &rep->pressure, cancelled, ctx);
-    RB200_CUDA(cudaEventRecord(c->ev[1], c->stream));
-    RB200_CUDA(cudaEventSynchronize(c->ev[1]));
-    {
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
-        rep->pressure_ms = double(ms);
-    }
-    rep->pressure_status = ps;
-    if (ps == RB200_CANCELLED) return RB200_CANCELLED;
-    if (ps == RB200_EXECUTION) {
-        c->err = get_error();
-        return ps;
-    }
-    if (ps != RB200_OK && !(ps == RB200_ITERATION_LIMIT && prm->iteration_limit_ok)) return ps;
-    const T* const Bc[3] = {B[0], B[1], B[2]};
-    if ((rc = launch_correct_divergence<T>(g, c->solver.p(), dt, Bc, Cc, c->solver.partials(),
-                                           c->solver.partial_blocks(), c->d_scalars, c->d_flags, c->stream)))
-        return rc;
-    if (tr) {
-        if ((rc = launch_advect_tracer<T>(g, tr, Cc[0], Cc[1], Cc[2], dt, c->tracer[c->tacc ^ 1], c->d_flags,
-                                          c->stream, fp32)))
-            return rc;
-    }
-    RB200_CUDA(cudaMemcpyAsync(c->h_scalars, c->d_scalars, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    RB200_CUDA(cudaMemcpyAsync(c->h_flags, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    RB200_CUDA(cudaStreamSynchronize(c->stream));
-    rep->kernel_launches = (c->solver.launches() - launches0) + 3 + (tr ? 1 : 0);
-    if (*c->h_flags & VF_NONFINITE) return RB200_NONFINITE_INPUT;
-    if (*c->h_flags & (VF_ARITH | VF_F32_RANGE)) return RB200_ARITHMETIC_FAILURE;
-    double rate = 0.0;
-    for (int d = 0; d < 3; ++d) rate += c->h_scalars[1 + d] / g.h[d];
-    rep->actual_divergence_max = c->h_scalars[0];
-    rep->velocity_rate = rate;
-    rep->courant = dt * rate;
-    if (!prm->skip_gates) {
-        if (rep->actual_divergence_max > c->cfg.actual_divergence_limit) return RB200_DIVERGENCE_LIMIT;
-        if (!std::isfinite(rep->courant)) return RB200_ARITHMETIC_FAILURE;
-        if (rep->courant > c->cfg.max_courant) return RB200_COURANT_LIMIT;
-    }
-    if (cancelled && cancelled(ctx)) return RB200_CANCELLED;
-    // commit_prepared (src/simulation.rs:805-811): publish the candidate.
-    c->acc = corr;
-    if (tr) c->tacc ^= 1;
-    c->time += dt;
-    c->generation += 1;
-    c->rate = rate;
-    rep->time = c->time;
-    rep->generation = c->generation;
-    return RB200_OK;
-}
 
 extern "C" {
 
@@ -578,161 +465,6 @@ int rb200_advect_tracer_f32_device(const rb200_grid* grid, const float* old, con
     if ((rc = launch_advect_tracer<float>(g, old, u, v, w, dt, out, fl2.d, s))) return rc;
     if ((rc = fl2.close(&f))) return rc;
     return flags_status(f, false);
-}
-
-// ---------------------------------------------------------------- carrier
-int rb200_carrier_create(const rb200_carrier_config* config, rb200_carrier** out) {
-    if (!config || !out) return RB200_INVALID_ARGUMENT;
-    *out = nullptr;
-    GridDev g;
-    int rc = make_grid_dev(&config->grid, config->density, &g);
-    if (rc) return rc;
-    if (config->storage != RB200_FACES_F32 && config->storage != RB200_FACES_F64) return RB200_INVALID_ARGUMENT;
-    if (!settings_valid(&config->settings)) return RB200_INVALID_ARGUMENT;
-    if (!(config->max_courant > 0.0) || !std::isfinite(config->actual_divergence_limit)) return RB200_INVALID_ARGUMENT;
-    if ((rc = select_device(config->device))) return rc;
-    std::unique_ptr<rb200_carrier> c(new (std::nothrow) rb200_carrier());
-    if (!c) return RB200_OUT_OF_MEMORY;
-    c->cfg = *config;
-    c->g = g;
-    c->device = config->device;
-    c->elem = config->storage == RB200_FACES_F32 ? 4 : 8;
-    RB200_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    for (int b = 0; b < 3; ++b)
-        for (int a = 0; a < 3; ++a) {
-            if (cudaMalloc(&c->faces[b][a], size_t(g.flen[a]) * c->elem) != cudaSuccess) return RB200_OUT_OF_MEMORY;
-            c->bytes += size_t(g.flen[a]) * c->elem;
-            RB200_CUDA(cudaMemsetAsync(c->faces[b][a], 0, size_t(g.flen[a]) * c->elem, c->stream));
-        }
-    if (config->with_tracer)
-        for (int t = 0; t < 2; ++t) {
-            if (cudaMalloc(&c->tracer[t], size_t(g.cells) * 4) != cudaSuccess) return RB200_OUT_OF_MEMORY;
-            c->bytes += size_t(g.cells) * 4;
-            RB200_CUDA(cudaMemsetAsync(c->tracer[t], 0, size_t(g.cells) * 4, c->stream));
-        }
-    RB200_CUDA(cudaMalloc(&c->d_scalars, 8 * sizeof(double)));
-    RB200_CUDA(cudaMalloc(&c->d_flags, sizeof(int)));
-    RB200_CUDA(cudaMallocHost(&c->h_scalars, 8 * sizeof(double)));
-    RB200_CUDA(cudaMallocHost(&c->h_flags, sizeof(int)));
-    for (auto& e : c->ev) RB200_CUDA(cudaEventCreate(&e));
-    if ((rc = c->solver.init(g, config->method, c->stream))) return rc;
-    c->bytes += c->solver.bytes();
-    RB200_CUDA(cudaStreamSynchronize(c->stream));
-    *out = c.release();
-    return RB200_OK;
-}
-
-void rb200_carrier_destroy(rb200_carrier* carrier) { delete carrier; }
-uint64_t rb200_carrier_allocated_bytes(const rb200_carrier* carrier) { return carrier ? carrier->bytes : 0; }
-void* rb200_carrier_stream(rb200_carrier* carrier) { return carrier ? (void*)carrier->stream : nullptr; }
-
-static int carrier_rate(rb200_carrier* c, int buffer, double* rate, int* flags) {
-    const GridDev& g = c->g;
-    RB200_CUDA(cudaMemsetAsync(c->d_flags, 0, sizeof(int), c->stream));
-    int rc;
-    if (c->elem == 4)
-        rc = launch_face_maxima<float>(g, (const float*)c->faces[buffer][0], (const float*)c->faces[buffer][1],
-                                       (const float*)c->faces[buffer][2], c->solver.partials(),
-                                       c->solver.partial_blocks(), c->d_scalars, c->d_flags, c->stream);
-    else
-        rc = launch_face_maxima<double>(g, (const double*)c->faces[buffer][0], (const double*)c->faces[buffer][1],
-                                        (const double*)c->faces[buffer][2], c->solver.partials(),
-                                        c->solver.partial_blocks(), c->d_scalars, c->d_flags, c->stream);
-    if (rc) return rc;
-    if (c->elem == 4)
-        rc = launch_validate_faces<float>(g, (const float*)c->faces[buffer][0], (const float*)c->faces[buffer][1],
-                                          (const float*)c->faces[buffer][2], c->d_flags, c->stream);
-    else
-        rc = launch_validate_faces<double>(g, (const double*)c->faces[buffer][0], (const double*)c->faces[buffer][1],
-                                           (const double*)c->faces[buffer][2], c->d_flags, c->stream);
-    if (rc) return rc;
-    RB200_CUDA(cudaMemcpyAsync(c->h_scalars, c->d_scalars, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    RB200_CUDA(cudaMemcpyAsync(c->h_flags, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    RB200_CUDA(cudaStreamSynchronize(c->stream));
-    // velocity_rate (src/simulation.rs:1415-1429): sum_d max|u_d| / h_d.
-    double r = 0.0;
-    for (int d = 0; d < 3; ++d) r += c->h_scalars[d] / g.h[d];
-    *rate = r;
-    *flags = *c->h_flags;
-    return RB200_OK;
-}
-
-int rb200_carrier_upload(rb200_carrier* carrier, const void* u, const void* v, const void* w, const float* tracer) {
-    if (!carrier || !u || !v || !w) return RB200_INVALID_ARGUMENT;
-    rb200_carrier* c = carrier;
-    cudaSetDevice(c->device);
-    const void* src[3] = {u, v, w};
-    for (int a = 0; a < 3; ++a)
-        RB200_CUDA(cudaMemcpyAsync(c->faces[c->acc][a], src[a], size_t(c->g.flen[a]) * c->elem,
-                                   cudaMemcpyHostToDevice, c->stream));
-    if (tracer) {
-        if (!c->tracer[0]) return RB200_INVALID_ARGUMENT;
-        RB200_CUDA(cudaMemcpyAsync(c->tracer[c->tacc], tracer, size_t(c->g.cells) * 4, cudaMemcpyHostToDevice,
-                                   c->stream));
-    }
-    double rate = 0.0;
-    int flags = 0;
-    int rc = carrier_rate(c, c->acc, &rate, &flags);
-    if (rc) return rc;
-    if (flags & VF_NONFINITE) return RB200_NONFINITE_INPUT;
-    if (flags & VF_WALL) return RB200_NONZERO_WALL_VELOCITY;
-    c->rate = rate;
-    c->time = 0.0;
-    c->generation = 0;
-    return RB200_OK;
-}
-
-int rb200_carrier_download(rb200_carrier* carrier, void* u, void* v, void* w, float* tracer) {
-    if (!carrier) return RB200_INVALID_ARGUMENT;
-    rb200_carrier* c = carrier;
-    cudaSetDevice(c->device);
-    void* dst[3] = {u, v, w};
-    for (int a = 0; a < 3; ++a)
-        if (dst[a])
-            RB200_CUDA(cudaMemcpyAsync(dst[a], c->faces[c->acc][a], size_t(c->g.flen[a]) * c->elem,
-                                       cudaMemcpyDeviceToHost, c->stream));
-    if (tracer && c->tracer[0])
-        RB200_CUDA(cudaMemcpyAsync(tracer, c->tracer[c->tacc], size_t(c->g.cells) * 4, cudaMemcpyDeviceToHost,
-                                   c->stream));
-    RB200_CUDA(cudaStreamSynchronize(c->stream));
-    return RB200_OK;
-}
-
-int rb200_carrier_state_device(rb200_carrier* carrier, void** u, void** v, void** w, float** tracer) {
-    if (!carrier) return RB200_INVALID_ARGUMENT;
-    if (u) *u = carrier->faces[carrier->acc][0];
-    if (v) *v = carrier->faces[carrier->acc][1];
-    if (w) *w = carrier->faces[carrier->acc][2];
-    if (tracer) *tracer = carrier->tracer[0] ? carrier->tracer[carrier->tacc] : nullptr;
-    return RB200_OK;
-}
-
-int rb200_carrier_profile(rb200_carrier* carrier, int which, int launches, double* avg_ms) {
-    if (!carrier || !avg_ms) return RB200_INVALID_ARGUMENT;
-    cudaSetDevice(carrier->device);
-    return carrier->solver.profile(which, launches, avg_ms);
-}
-
-int rb200_carrier_pressure(rb200_carrier* carrier, double* out, size_t len) {
-    if (!carrier || !out) return RB200_INVALID_ARGUMENT;
-    if (len != size_t(carrier->g.cells)) return RB200_LENGTH_MISMATCH;
-    cudaSetDevice(carrier->device);
-    RB200_CUDA(cudaMemcpyAsync(out, carrier->solver.p(), len * sizeof(double), cudaMemcpyDeviceToHost,
-                               carrier->stream));
-    RB200_CUDA(cudaStreamSynchronize(carrier->stream));
-    return RB200_OK;
-}
-
-
-int rb200_carrier_step(rb200_carrier* carrier, const rb200_step_params* params, rb200_step_report* report,
-                       rb200_cancel_fn cancelled, void* ctx) {
-    if (!carrier || !params || !report) return RB200_INVALID_ARGUMENT;
-    std::memset(report, 0, sizeof(*report));
-    cudaSetDevice(carrier->device);
-    int rc = carrier->elem == 4 ? carrier_step_t<float>(carrier, params, report, cancelled, ctx)
-                                : carrier_step_t<double>(carrier, params, report, cancelled, ctx);
-    if (rc == RB200_EXECUTION && carrier->err.empty()) carrier->err = get_error();
-    return rc;
 }
 
 }  // extern "C"

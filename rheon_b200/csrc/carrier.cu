@@ -1,0 +1,507 @@
+// Resident fixed-box carrier step: the state stays in HBM and one step is
+// one CUDA graph, composed as Rheon's step owner orders it
+// (Simulation::prepare_impl, src/simulation.rs:812-1403):
+//   dt policy -> advect_velocity (+ buoyancy hook) -> build_rhs -> pressure
+//   solve (WHILE node over iteration chunks) -> correct_candidate + actual
+//   divergence + velocity rate -> gates -> advect_tracer -> commit.
+// Every decision (dt, solve control, gates, commit) is taken on the device;
+// the host launches the graph and reads one small report afterwards. The
+// accepted state is never written by a rejected step (transactional, as
+// commit_prepared, src/simulation.rs:805-811): the step writes candidate and
+// corrected buffers and publishes by rotating buffer indices on the device.
+#include <cmath>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "advect.cuh"
+#include "internal.hpp"
+#include "pcg.hpp"
+#include "project.cuh"
+
+namespace rb200 {
+
+constexpr int STEP_RUNNING = -1;
+
+// Device-resident carrier descriptor (one per carrier).
+struct CarrierDev {
+    void* faces[3][3];   // [buffer][axis]
+    float* tracer[2];
+    int acc, tacc;       // accepted face buffer, accepted tracer
+    int status;          // step status (STEP_RUNNING while the step runs)
+    int skip;            // nonzero: skip the pressure solve (step already failed)
+    int flags;           // validation flags of the step's kernels
+    int pad;
+    // step parameters (written by the host before each launch)
+    double requested_dt, cfl, buoyancy;
+    int iteration_limit_ok, skip_gates;
+    // configuration
+    double max_courant, divergence_limit;
+    // accepted-state bookkeeping
+    double dt, rate, time;
+    unsigned long long generation;
+    double scalars[4];   // max|div|, max|u|, max|v|, max|w| of the corrected faces
+    rb200_step_report report;
+    int step_status;
+    int trips;
+};
+
+__device__ __forceinline__ bool step_running(const CarrierDev* cd) { return cd->status == STEP_RUNNING; }
+
+// Proceed to the correction: the solve converged, or an exact-iteration-count
+// solve reached its limit.
+__device__ __forceinline__ bool solve_usable(const CarrierDev* cd, const SolveState* st) {
+    return step_running(cd) &&
+           (st->status == RB200_OK || (st->status == RB200_ITERATION_LIMIT && cd->iteration_limit_ok));
+}
+
+// dt policy (src/simulation.rs:952-979): dt = min(requested, cfl/rate).
+__global__ void k_step_begin(CarrierDev* cd) {
+    double dt = cd->requested_dt;
+    if (cd->cfl > 0.0 && cd->rate > 0.0) dt = fmin(dt, cd->cfl / cd->rate);
+    cd->dt = dt;
+    cd->flags = 0;
+    cd->skip = 0;
+    cd->status = STEP_RUNNING;
+    const double next = cd->time + dt;
+    if (!isfinite(dt) || dt <= 0.0 || !isfinite(next) || next <= cd->time) {
+        cd->status = RB200_INVALID_ARGUMENT;
+        cd->skip = 1;
+    }
+}
+
+template <class T, class R>
+__global__ void __launch_bounds__(ADV_THREADS) k_carrier_advect(GridDev g, CarrierDev* cd) {
+    if (!step_running(cd)) return;
+    const int a = cd->acc, b = (a + 1) % 3;
+    Faces<T> vel{{(const T*)cd->faces[a][0], (const T*)cd->faces[a][1], (const T*)cd->faces[a][2]}};
+    const float* tr = cd->tracer[0] ? cd->tracer[cd->tacc] : nullptr;
+    advect_velocity_body<T, R>(g, vel, cd->dt, (T*)cd->faces[b][0], (T*)cd->faces[b][1], (T*)cd->faces[b][2], tr,
+                               cd->buoyancy, &cd->flags);
+}
+
+template <class T>
+__global__ void k_carrier_rhs(GridDev g, CarrierDev* cd, double* __restrict__ rhs) {
+    if (!step_running(cd)) return;
+    const int b = (cd->acc + 1) % 3;
+    build_rhs_body<T>(g, (const T*)cd->faces[b][0], (const T*)cd->faces[b][1], (const T*)cd->faces[b][2], cd->dt,
+                      rhs, &cd->flags);
+}
+
+template <class T>
+__global__ void __launch_bounds__(EW_THREADS) k_carrier_correct(GridDev g, CarrierDev* cd, const SolveState* st,
+                                                                const double* __restrict__ p, Partials part) {
+    if (!solve_usable(cd, st)) return;
+    const int b = (cd->acc + 1) % 3, c = (cd->acc + 2) % 3;
+    correct_divergence_body<T>(g, p, cd->dt, (const T*)cd->faces[b][0], (const T*)cd->faces[b][1],
+                               (const T*)cd->faces[b][2], (T*)cd->faces[c][0], (T*)cd->faces[c][1],
+                               (T*)cd->faces[c][2], part, cd->scalars, &cd->flags);
+}
+
+template <class T, class R>
+__global__ void __launch_bounds__(ADV_THREADS) k_carrier_tracer(GridDev g, CarrierDev* cd, const SolveState* st) {
+    if (!cd->tracer[0] || !solve_usable(cd, st)) return;
+    const int c = (cd->acc + 2) % 3;
+    Faces<T> vel{{(const T*)cd->faces[c][0], (const T*)cd->faces[c][1], (const T*)cd->faces[c][2]}};
+    advect_tracer_body<T, R>(g, cd->tracer[cd->tacc], vel, cd->dt, cd->tracer[cd->tacc ^ 1], &cd->flags);
+}
+
+// Gates and commit: actual divergence (simulation.rs:1235-1243), Courant
+// (simulation.rs:1268-1277), then publication by index rotation.
+__global__ void k_step_end(GridDev g, CarrierDev* cd, const SolveState* st) {
+    rb200_step_report& rep = cd->report;
+    rep.dt = cd->dt;
+    rep.pressure.iterations = uint64_t(st->it);
+    rep.pressure.true_residual_l2 = st->true_l2;
+    rep.pressure.true_residual_max = st->true_max;
+    rep.pressure.predicted_divergence_max = st->true_div;
+    rep.pressure.incompatible_sum = st->incompatible_sum;
+    rep.pressure.incompatible_budget = st->incompatible_budget;
+    rep.pressure.breakdown_iteration = uint64_t(st->breakdown_it);
+    rep.pressure_status = st->status;
+    cd->trips = st->trips;
+    int status = cd->status;
+    if (status == STEP_RUNNING) {
+        if (!solve_usable(cd, st)) {
+            status = st->status;
+        } else if (cd->flags & VF_NONFINITE) {
+            status = RB200_NONFINITE_INPUT;
+        } else if (cd->flags & (VF_ARITH | VF_F32_RANGE)) {
+            status = RB200_ARITHMETIC_FAILURE;
+        } else {
+            // velocity_rate (src/simulation.rs:1415-1429): sum_d max|u_d| / h_d
+            double rate = 0.0;
+            for (int d = 0; d < 3; ++d) rate += cd->scalars[1 + d] / g.h[d];
+            rep.actual_divergence_max = cd->scalars[0];
+            rep.velocity_rate = rate;
+            rep.courant = cd->dt * rate;
+            status = RB200_OK;
+            if (!cd->skip_gates) {
+                if (rep.actual_divergence_max > cd->divergence_limit)
+                    status = RB200_DIVERGENCE_LIMIT;
+                else if (!isfinite(rep.courant))
+                    status = RB200_ARITHMETIC_FAILURE;
+                else if (rep.courant > cd->max_courant)
+                    status = RB200_COURANT_LIMIT;
+            }
+            if (status == RB200_OK) {
+                cd->acc = (cd->acc + 2) % 3;
+                if (cd->tracer[0]) cd->tacc ^= 1;
+                cd->time += cd->dt;
+                cd->generation += 1;
+                cd->rate = rate;
+            }
+        }
+    }
+    rep.time = cd->time;
+    rep.generation = cd->generation;
+    cd->step_status = status;
+    cd->status = status;
+}
+
+// Per-axis face maxima and validation of an uploaded state.
+template <class T>
+int launch_validate_faces(const GridDev& g, const T* u, const T* v, const T* w, int* flags, cudaStream_t s);
+
+}  // namespace rb200
+
+using namespace rb200;
+
+// Host side of the carrier (opaque handle of include/rheon_b200.h).
+struct rb200_carrier {
+    rb200_carrier_config cfg{};
+    GridDev g{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t body_stream = nullptr;
+    size_t elem = 4;
+    void* faces[3][3] = {};
+    float* tracer[2] = {nullptr, nullptr};
+    PcgSolver solver;
+    CarrierDev* cd = nullptr;      // device
+    CarrierDev* h_cd = nullptr;    // pinned host mirror
+    cudaEvent_t ev[4] = {};
+    cudaGraphExec_t step_exec = nullptr;
+    int fixed_nodes = 0;
+    size_t bytes = 0;
+    bool in_flight = false;
+    std::string err;
+    ~rb200_carrier() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        if (step_exec) cudaGraphExecDestroy(step_exec);
+        for (auto& b : faces)
+            for (auto& a : b) cudaFree(a);
+        cudaFree(tracer[0]);
+        cudaFree(tracer[1]);
+        cudaFree(cd);
+        if (h_cd) cudaFreeHost(h_cd);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (body_stream) cudaStreamDestroy(body_stream);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+int select_carrier_device(int device) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        set_error("no CUDA device");
+        return RB200_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return RB200_INVALID_ARGUMENT;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+        set_error("librheon_b200 is built for sm_100a (B200) only");
+        return RB200_NO_DEVICE;
+    }
+    return cudaSetDevice(device) == cudaSuccess ? RB200_OK : RB200_NO_DEVICE;
+}
+
+int blocks_for(long long n, int threads, int cap) {
+    long long b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    return int(b < cap ? b : cap);
+}
+
+template <class T>
+int capture_step(rb200_carrier* c) {
+    const GridDev& g = c->g;
+    cudaStream_t s = c->stream;
+    const long long faces = (long long)g.flen[0] + g.flen[1] + g.flen[2];
+    const int fb = blocks_for(faces, ADV_THREADS, 148 * 64);
+    const int cb = blocks_for(g.cells, ADV_THREADS, 148 * 64);
+    const int eb = blocks_for(g.cells, EW_THREADS, std::min(EW_BLOCKS_CAP, c->solver.partial_blocks()));
+    const bool fp32 = c->cfg.fp32_advection != 0;
+    cudaGraph_t graph = nullptr;
+    RB200_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    k_step_begin<<<1, 1, 0, s>>>(c->cd);
+    if (fp32)
+        k_carrier_advect<T, float><<<fb, ADV_THREADS, 0, s>>>(g, c->cd);
+    else
+        k_carrier_advect<T, double><<<fb, ADV_THREADS, 0, s>>>(g, c->cd);
+    k_carrier_rhs<T><<<cb, ADV_THREADS, 0, s>>>(g, c->cd, c->solver.b());
+    RB200_CUDA(cudaEventRecordWithFlags(c->ev[0], s, cudaEventRecordExternal));
+    int rc = c->solver.enqueue_reset(&c->cd->dt, &c->cd->skip, c->cfg.settings, s);
+    if (!rc) rc = c->solver.enqueue_loop(s, c->body_stream, c->cfg.settings);
+    if (rc) {
+        cudaGraph_t dummy = nullptr;
+        cudaStreamEndCapture(s, &dummy);
+        if (dummy) cudaGraphDestroy(dummy);
+        return rc;
+    }
+    RB200_CUDA(cudaEventRecordWithFlags(c->ev[1], s, cudaEventRecordExternal));
+    k_carrier_correct<T><<<eb, EW_THREADS, 0, s>>>(g, c->cd, c->solver.state(), c->solver.p(), c->solver.partials());
+    if (c->tracer[0]) {
+        if (fp32)
+            k_carrier_tracer<T, float><<<cb, ADV_THREADS, 0, s>>>(g, c->cd, c->solver.state());
+        else
+            k_carrier_tracer<T, double><<<cb, ADV_THREADS, 0, s>>>(g, c->cd, c->solver.state());
+    }
+    k_step_end<<<1, 1, 0, s>>>(g, c->cd, c->solver.state());
+    RB200_CUDA(cudaMemcpyAsync(c->h_cd, c->cd, sizeof(CarrierDev), cudaMemcpyDeviceToHost, s));
+    cudaError_t le = cudaGetLastError();
+    cudaError_t ee = cudaStreamEndCapture(s, &graph);
+    if (le != cudaSuccess || ee != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        set_error(std::string("step capture: ") + cudaGetErrorString(le != cudaSuccess ? le : ee));
+        return RB200_EXECUTION;
+    }
+    cudaError_t ie = cudaGraphInstantiate(&c->step_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+        set_error(std::string("step graph instantiate: ") + cudaGetErrorString(ie));
+        return RB200_EXECUTION;
+    }
+    // begin, advect, rhs, reset (+start kernels counted by the solver), correct, tracer, end
+    c->fixed_nodes = 5 + (c->tracer[0] ? 1 : 0);
+    return RB200_OK;
+}
+
+int upload_rate(rb200_carrier* c) {
+    // velocity rate and validation of the accepted state (after an upload)
+    const GridDev& g = c->g;
+    int* d_flags = &c->cd->flags;
+    double* sc = c->cd->scalars;
+    RB200_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(int), c->stream));
+    const int a = c->h_cd->acc;
+    int rc;
+    if (c->elem == 4) {
+        rc = launch_face_maxima<float>(g, (const float*)c->faces[a][0], (const float*)c->faces[a][1],
+                                       (const float*)c->faces[a][2], c->solver.partials(), c->solver.partial_blocks(),
+                                       sc, d_flags, c->stream);
+        if (!rc)
+            rc = launch_validate_faces<float>(g, (const float*)c->faces[a][0], (const float*)c->faces[a][1],
+                                              (const float*)c->faces[a][2], d_flags, c->stream);
+    } else {
+        rc = launch_face_maxima<double>(g, (const double*)c->faces[a][0], (const double*)c->faces[a][1],
+                                        (const double*)c->faces[a][2], c->solver.partials(),
+                                        c->solver.partial_blocks(), sc, d_flags, c->stream);
+        if (!rc)
+            rc = launch_validate_faces<double>(g, (const double*)c->faces[a][0], (const double*)c->faces[a][1],
+                                               (const double*)c->faces[a][2], d_flags, c->stream);
+    }
+    if (rc) return rc;
+    RB200_CUDA(cudaMemcpyAsync(c->h_cd, c->cd, sizeof(CarrierDev), cudaMemcpyDeviceToHost, c->stream));
+    RB200_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->h_cd->flags & VF_NONFINITE) return RB200_NONFINITE_INPUT;
+    if (c->h_cd->flags & VF_WALL) return RB200_NONZERO_WALL_VELOCITY;
+    double r = 0.0;
+    for (int d = 0; d < 3; ++d) r += c->h_cd->scalars[d] / g.h[d];
+    c->h_cd->rate = r;
+    c->h_cd->time = 0.0;
+    c->h_cd->generation = 0;
+    c->h_cd->status = RB200_OK;
+    c->h_cd->flags = 0;
+    RB200_CUDA(cudaMemcpyAsync(c->cd, c->h_cd, sizeof(CarrierDev), cudaMemcpyHostToDevice, c->stream));
+    RB200_CUDA(cudaStreamSynchronize(c->stream));
+    return RB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rb200_carrier_create(const rb200_carrier_config* config, rb200_carrier** out) {
+    if (!config || !out) return RB200_INVALID_ARGUMENT;
+    *out = nullptr;
+    GridDev g;
+    int rc = make_grid_dev(&config->grid, config->density, &g);
+    if (rc) return rc;
+    if (config->storage != RB200_FACES_F32 && config->storage != RB200_FACES_F64) return RB200_INVALID_ARGUMENT;
+    if (!settings_valid(&config->settings)) return RB200_INVALID_ARGUMENT;
+    if (!(config->max_courant > 0.0) || !std::isfinite(config->actual_divergence_limit)) return RB200_INVALID_ARGUMENT;
+    if ((rc = select_carrier_device(config->device))) return rc;
+    std::unique_ptr<rb200_carrier> c(new (std::nothrow) rb200_carrier());
+    if (!c) return RB200_OUT_OF_MEMORY;
+    c->cfg = *config;
+    c->g = g;
+    c->device = config->device;
+    c->elem = config->storage == RB200_FACES_F32 ? 4 : 8;
+    RB200_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    RB200_CUDA(cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking));
+    for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a) {
+            if (cudaMalloc(&c->faces[b][a], size_t(g.flen[a]) * c->elem) != cudaSuccess) return RB200_OUT_OF_MEMORY;
+            c->bytes += size_t(g.flen[a]) * c->elem;
+            RB200_CUDA(cudaMemsetAsync(c->faces[b][a], 0, size_t(g.flen[a]) * c->elem, c->stream));
+        }
+    if (config->with_tracer)
+        for (int t = 0; t < 2; ++t) {
+            if (cudaMalloc(&c->tracer[t], size_t(g.cells) * 4) != cudaSuccess) return RB200_OUT_OF_MEMORY;
+            c->bytes += size_t(g.cells) * 4;
+            RB200_CUDA(cudaMemsetAsync(c->tracer[t], 0, size_t(g.cells) * 4, c->stream));
+        }
+    RB200_CUDA(cudaMalloc(&c->cd, sizeof(CarrierDev)));
+    RB200_CUDA(cudaMallocHost(&c->h_cd, sizeof(CarrierDev)));
+    std::memset(c->h_cd, 0, sizeof(CarrierDev));
+    for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a) c->h_cd->faces[b][a] = c->faces[b][a];
+    c->h_cd->tracer[0] = c->tracer[0];
+    c->h_cd->tracer[1] = c->tracer[1];
+    c->h_cd->max_courant = config->max_courant;
+    c->h_cd->divergence_limit = config->actual_divergence_limit;
+    c->h_cd->status = RB200_OK;
+    RB200_CUDA(cudaMemcpyAsync(c->cd, c->h_cd, sizeof(CarrierDev), cudaMemcpyHostToDevice, c->stream));
+    for (auto& e : c->ev) RB200_CUDA(cudaEventCreate(&e));
+    if ((rc = c->solver.init(g, config->method, c->stream))) return rc;
+    c->bytes += c->solver.bytes();
+    RB200_CUDA(cudaStreamSynchronize(c->stream));
+    rc = c->elem == 4 ? capture_step<float>(c.get()) : capture_step<double>(c.get());
+    if (rc) return rc;
+    *out = c.release();
+    return RB200_OK;
+}
+
+void rb200_carrier_destroy(rb200_carrier* carrier) { delete carrier; }
+uint64_t rb200_carrier_allocated_bytes(const rb200_carrier* carrier) { return carrier ? carrier->bytes : 0; }
+void* rb200_carrier_stream(rb200_carrier* carrier) { return carrier ? (void*)carrier->stream : nullptr; }
+
+int rb200_carrier_upload(rb200_carrier* carrier, const void* u, const void* v, const void* w, const float* tracer) {
+    if (!carrier || !u || !v || !w) return RB200_INVALID_ARGUMENT;
+    rb200_carrier* c = carrier;
+    if (c->in_flight) return RB200_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    const int a = c->h_cd->acc;
+    const void* src[3] = {u, v, w};
+    for (int d = 0; d < 3; ++d)
+        RB200_CUDA(cudaMemcpyAsync(c->faces[a][d], src[d], size_t(c->g.flen[d]) * c->elem, cudaMemcpyHostToDevice,
+                                   c->stream));
+    if (tracer) {
+        if (!c->tracer[0]) return RB200_INVALID_ARGUMENT;
+        RB200_CUDA(cudaMemcpyAsync(c->tracer[c->h_cd->tacc], tracer, size_t(c->g.cells) * 4, cudaMemcpyHostToDevice,
+                                   c->stream));
+    }
+    return upload_rate(c);
+}
+
+int rb200_carrier_download(rb200_carrier* carrier, void* u, void* v, void* w, float* tracer) {
+    if (!carrier) return RB200_INVALID_ARGUMENT;
+    rb200_carrier* c = carrier;
+    if (c->in_flight) return RB200_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    const int a = c->h_cd->acc;
+    void* dst[3] = {u, v, w};
+    for (int d = 0; d < 3; ++d)
+        if (dst[d])
+            RB200_CUDA(cudaMemcpyAsync(dst[d], c->faces[a][d], size_t(c->g.flen[d]) * c->elem, cudaMemcpyDeviceToHost,
+                                       c->stream));
+    if (tracer && c->tracer[0])
+        RB200_CUDA(cudaMemcpyAsync(tracer, c->tracer[c->h_cd->tacc], size_t(c->g.cells) * 4, cudaMemcpyDeviceToHost,
+                                   c->stream));
+    RB200_CUDA(cudaStreamSynchronize(c->stream));
+    return RB200_OK;
+}
+
+int rb200_carrier_state_device(rb200_carrier* carrier, void** u, void** v, void** w, float** tracer) {
+    if (!carrier) return RB200_INVALID_ARGUMENT;
+    const int a = carrier->h_cd->acc;
+    if (u) *u = carrier->faces[a][0];
+    if (v) *v = carrier->faces[a][1];
+    if (w) *w = carrier->faces[a][2];
+    if (tracer) *tracer = carrier->tracer[0] ? carrier->tracer[carrier->h_cd->tacc] : nullptr;
+    return RB200_OK;
+}
+
+int rb200_carrier_pressure(rb200_carrier* carrier, double* out, size_t len) {
+    if (!carrier || !out) return RB200_INVALID_ARGUMENT;
+    if (len != size_t(carrier->g.cells)) return RB200_LENGTH_MISMATCH;
+    cudaSetDevice(carrier->device);
+    RB200_CUDA(cudaMemcpyAsync(out, carrier->solver.p(), len * sizeof(double), cudaMemcpyDeviceToHost,
+                               carrier->stream));
+    RB200_CUDA(cudaStreamSynchronize(carrier->stream));
+    return RB200_OK;
+}
+
+int rb200_carrier_profile(rb200_carrier* carrier, int which, int launches, double* avg_ms) {
+    if (!carrier || !avg_ms) return RB200_INVALID_ARGUMENT;
+    if (carrier->in_flight) return RB200_INVALID_ARGUMENT;
+    cudaSetDevice(carrier->device);
+    return carrier->solver.profile(which, launches, avg_ms);
+}
+
+int rb200_carrier_step_async(rb200_carrier* carrier, const rb200_step_params* params) {
+    if (!carrier || !params) return RB200_INVALID_ARGUMENT;
+    rb200_carrier* c = carrier;
+    if (c->in_flight) return RB200_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    // Step parameters into the device descriptor, then the step graph; both
+    // ordered on the carrier's stream.
+    c->h_cd->requested_dt = params->requested_dt;
+    c->h_cd->cfl = params->cfl;
+    c->h_cd->buoyancy = params->buoyancy;
+    c->h_cd->iteration_limit_ok = params->iteration_limit_ok;
+    c->h_cd->skip_gates = params->skip_gates;
+    RB200_CUDA(cudaMemcpyAsync(&c->cd->requested_dt, &c->h_cd->requested_dt,
+                               offsetof(CarrierDev, max_courant) - offsetof(CarrierDev, requested_dt),
+                               cudaMemcpyHostToDevice, c->stream));
+    RB200_CUDA(cudaEventRecord(c->ev[2], c->stream));
+    RB200_CUDA(cudaGraphLaunch(c->step_exec, c->stream));
+    RB200_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    c->in_flight = true;
+    return RB200_OK;
+}
+
+int rb200_carrier_step_wait(rb200_carrier* carrier, rb200_step_report* report) {
+    if (!carrier || !report) return RB200_INVALID_ARGUMENT;
+    rb200_carrier* c = carrier;
+    if (!c->in_flight) return RB200_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    c->in_flight = false;
+    RB200_CUDA(cudaStreamSynchronize(c->stream));
+    const CarrierDev& h = *c->h_cd;
+    *report = h.report;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]) == cudaSuccess) report->pressure_ms = double(ms);
+    report->kernel_launches = uint64_t(c->fixed_nodes) + uint64_t(h.trips) * uint64_t(c->solver.nodes_per_chunk());
+    return h.step_status;
+}
+
+int rb200_carrier_step(rb200_carrier* carrier, const rb200_step_params* params, rb200_step_report* report,
+                       rb200_cancel_fn cancelled, void* ctx) {
+    if (!carrier || !params || !report) return RB200_INVALID_ARGUMENT;
+    std::memset(report, 0, sizeof(*report));
+    if (cancelled && cancelled(ctx)) return RB200_CANCELLED;
+    int rc = rb200_carrier_step_async(carrier, params);
+    if (rc) return rc;
+    return rb200_carrier_step_wait(carrier, report);
+}
+
+int rb200_carriers_step(rb200_carrier* const* carriers, size_t count, const rb200_step_params* params,
+                        rb200_step_report* reports, int* statuses) {
+    if (!carriers || !params || !reports || !statuses) return RB200_INVALID_ARGUMENT;
+    int first_error = RB200_OK;
+    for (size_t i = 0; i < count; ++i) {
+        statuses[i] = rb200_carrier_step_async(carriers[i], &params[i]);
+        if (statuses[i] && !first_error) first_error = statuses[i];
+    }
+    for (size_t i = 0; i < count; ++i) {
+        if (statuses[i]) continue;
+        statuses[i] = rb200_carrier_step_wait(carriers[i], &reports[i]);
+    }
+    return first_error;
+}
+
+}  // extern "C"

@@ -98,6 +98,7 @@ __device__ __forceinline__ void decide_rz(SolveState* st, rb200_trace* trace, do
 __global__ void __launch_bounds__(EW) k_init_sums(GridDev g, SolveState* st, const double* __restrict__ b,
                                                   double* __restrict__ p, Partials part) {
     __shared__ BlockReduce<3, 2> sm;
+    if (st->flags & F_DONE) return;
     dd s[3] = {{0, 0}, {0, 0}, {0, 0}};
     double m[2] = {0.0, 0.0};
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
@@ -728,6 +729,37 @@ __global__ void __launch_bounds__(EW) k_rbsgs_red_dot(GridDev g, SolveState* st,
     }
 }
 
+// ------------------------------------------------------------ graph embedding
+// Device-side reset of the solver state (what solve() uploads from the host).
+__global__ void k_solve_reset(SolveState* st, rb200_settings s, const double* __restrict__ dt_dev,
+                              const int* __restrict__ skip, int flexible) {
+    SolveState init{};
+    init.dt = *dt_dev;
+    init.relative = s.relative_residual;
+    init.absolute = s.absolute_residual;
+    init.divergence_limit = s.divergence_limit;
+    init.max_it = s.max_iterations > 0x7fffffffull ? 0x7fffffff : int(s.max_iterations);
+    init.status = ST_RUNNING;
+    init.flexible = flexible;
+    if (skip && *skip != 0) init.flags = F_DONE | F_STOP;
+    *st = init;
+}
+
+// Condition of the WHILE node: repeat while the solve is running. The trip
+// count is bounded; running out of trips ends the solve with an execution
+// error instead of looping on.
+__global__ void k_loop_cond(SolveState* st, cudaGraphConditionalHandle handle, int max_trips) {
+    const int trips = st->trips + 1;
+    st->trips = trips;
+    unsigned go = (st->flags & F_DONE) ? 0u : 1u;
+    if (go && trips >= max_trips) {
+        st->status = RB200_EXECUTION;
+        st->flags = st->flags | F_DONE | F_STOP;
+        go = 0u;
+    }
+    cudaGraphSetConditional(handle, go);
+}
+
 // ------------------------------------------------------------ host side
 constexpr int ZC = 8;
 constexpr size_t kSmemPass1 = 2 * size_t(Slab<ZC>::SIZE) * sizeof(double);
@@ -1089,6 +1121,56 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
     fill_report(f, report);
     if (cancelled_now) return RB200_CANCELLED;
     return f.status;
+}
+
+int PcgSolver::enqueue_reset(const double* dt_dev, const int* skip, const rb200_settings& settings, cudaStream_t s) {
+    k_solve_reset<<<1, 1, 0, s>>>(st_, settings, dt_dev, skip, method_ == RB200_MG_MIXED ? 1 : 0);
+    RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), s));
+    launches_ += 1;
+    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_};
+    launch_start(g_, method_, B, method_ == RB200_MG_MIXED ? &mg_ : nullptr, s);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+
+int PcgSolver::enqueue_loop(cudaStream_t cs, cudaStream_t body_stream, const rb200_settings& settings) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    RB200_CUDA(cudaStreamGetCaptureInfo(cs, &status, nullptr, &graph, &deps, &ndeps));
+    if (status != cudaStreamCaptureStatusActive) {
+        set_error("enqueue_loop needs an active stream capture");
+        return RB200_EXECUTION;
+    }
+    cudaGraphConditionalHandle handle;
+    RB200_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    RB200_CUDA(cudaGraphAddNode(&node, graph, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    // The loop body: one chunk of iterations, the gated check, the condition.
+    RB200_CUDA(cudaStreamBeginCaptureToGraph(body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_};
+    const Multigrid* mg = method_ == RB200_MG_MIXED ? &mg_ : nullptr;
+    for (int q = 0; q < chunk_; ++q) launch_iteration(g_, method_, B, mg, body_stream);
+    launch_check(g_, method_, B, mg, body_stream);
+    const uint64_t mi = settings.max_iterations;
+    const uint64_t trips = (mi / uint64_t(chunk_)) * 2 + 64;
+    k_loop_cond<<<1, 1, 0, body_stream>>>(st_, handle, trips > (1u << 24) ? (1 << 24) : int(trips));
+    cudaError_t le = cudaGetLastError();
+    cudaGraph_t captured = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(body_stream, &captured);
+    if (le != cudaSuccess || ee != cudaSuccess) {
+        set_error(std::string("loop body capture: ") + cudaGetErrorString(le != cudaSuccess ? le : ee));
+        return RB200_EXECUTION;
+    }
+    RB200_CUDA(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
+    return RB200_OK;
 }
 
 int PcgSolver::profile(int which, int launches, double* avg_ms) {

@@ -28,7 +28,7 @@ struct SolveState {
     int status;         // rb200_status, or ST_RUNNING
     int breakdown_it;
     int flexible;       // beta = -z.q / d.q (flexible CG) instead of rz'/rz
-    int pad1;
+    int trips;          // loop-body passes of the graph-embedded solve
 };
 
 enum : int {
@@ -72,6 +72,17 @@ public:
     // solver's stream, on the current vectors. Scalars are left in a timing
     // state; the next solve() resets them.
     int profile(int which, int launches, double* avg_ms);
+
+    // Graph embedding (the resident carrier step is one CUDA graph):
+    // enqueue_reset initialises the state on the device from `settings` and the
+    // device dt (*dt_dev); when *skip != 0 the solve is marked done and every
+    // solver kernel is a no-op. enqueue_loop adds a WHILE conditional node that
+    // repeats the iteration chunk until the state is done, with the trip count
+    // bounded so that the loop always ends. Both run during a stream capture.
+    int enqueue_reset(const double* dt_dev, const int* skip, const rb200_settings& settings, cudaStream_t s);
+    int enqueue_loop(cudaStream_t capture_stream, cudaStream_t body_stream, const rb200_settings& settings);
+    int nodes_per_chunk() const { return nodes_per_chunk_ + 1; }
+    SolveState* state() { return st_; }
     const GridDev& grid() const { return g_; }
     Partials partials() const { return part_; }
     int partial_blocks() const { return part_blocks_; }
