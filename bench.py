@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=128)
-    ap.add_argument("--method", default="jacobi", choices=["jacobi", "rbsgs"])
+    ap.add_argument("--method", default="jacobi", choices=["jacobi", "rbsgs", "sgs", "mixed"])
     ap.add_argument("--storage", default="f64", choices=["f64", "f32"])
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--no-variants", action="store_true")
@@ -57,6 +57,10 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-instances", type=int, default=64)
     ap.add_argument("--batched-steps", type=int, default=20)
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=200)
+    ap.add_argument("--serving-plain-requests", type=int, default=12)
+    ap.add_argument("--serving-budget-gb", type=float, default=150.0)
     ap.add_argument("--no-profile", action="store_true")
     return ap.parse_args()
 
@@ -234,6 +238,54 @@ def run_batched(args, local, flush):
     }
 
 
+def run_serving(args, local):
+    """Serving loop: requests of k in [1, 20] steps on boxes with edges
+    log-uniform in [32, 256] (multiples of 8), random-Fourier initial velocity,
+    mixed precision at rel. residual 1e-8, admitted while the pooled carriers
+    fit the HBM budget. Capacity is measured first with every request arriving
+    at once (this also warms the carrier pool); then a Poisson stream at 80 % of
+    that capacity is served. The plain per-request f64 path (one request at a
+    time, Jacobi-PCG f64 carriers) runs on the first requests of the same stream
+    for comparison. Latency = finish - arrival (queueing included)."""
+    import torch
+
+    import rheon_b200 as R
+    from rheon_b200 import serving as SV
+
+    free, _total = torch.cuda.mem_get_info(local)
+    budget = int(min(args.serving_budget_gb * 1e9, free - 8e9))
+    cfg = R.CarrierConfig.mixed(pressure=R.PressureSettings(1e-8, 0.0, MAXF, 1000), device=local)
+    loop = SV.ServingLoop(cfg, budget)
+    n_cap = max(8, min(args.serving_requests, 64))
+    cap_reqs = SV.make_requests(n_cap, rate_hz=0.0, seed=args.seed + 5)
+    cap_done = loop.run(cap_reqs)
+    capacity = len(cap_done) / loop.elapsed
+    rate = 0.8 * capacity
+    reqs = SV.make_requests(args.serving_requests, rate_hz=rate, seed=args.seed + 6)
+    done = loop.run(reqs)
+    served = SV.summarize(done, loop.elapsed)
+    pool_gb = loop.pool.used / 1e9
+    loop.close()
+    plain_cfg = R.CarrierConfig(pressure=R.PressureSettings(1e-8, 0.0, MAXF, 1000000), storage="f64",
+                                implementation=R.PressureImplementation.JACOBI_PCG_V1, device=local)
+    plain_reqs = reqs[: args.serving_plain_requests]
+    plain = SV.ServingLoop(plain_cfg, budget, max_in_flight=1)
+    plain_done = plain.run(plain_reqs)
+    plain_summary = SV.summarize(plain_done, plain.elapsed)
+    plain.close()
+    return {
+        "workload": "requests of k in [1,20] steps, edge log-uniform in [32,256] (multiple of 8), random-Fourier "
+                    "init, mixed precision to rel residual 1e-8, Poisson arrivals at 0.8 x measured capacity",
+        "requests": args.serving_requests,
+        "capacity_requests_per_s": capacity,
+        "arrival_rate_per_s": rate,
+        "hbm_budget_gb": budget / 1e9,
+        "pool_gb": pool_gb,
+        "mixed": served,
+        "plain_f64_per_request": dict(plain_summary, requests_run=len(plain_reqs)),
+    }
+
+
 # ------------------------------------------------------------------ our arm
 def run_ours(args, world, rank, local):
     import torch
@@ -244,12 +296,18 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(local)
     n = (args.n,) * 3
     g = R.GridGeometry(n)
+    if args.method == "mixed":
+        args.storage = "f32"
     dtype = np.float64 if args.storage == "f64" else np.float32
     faces = W.fourier_faces(n, seed=args.seed + rank, dtype=dtype)
-    method = R.PressureImplementation.JACOBI_PCG_V1 if args.method == "jacobi" else R.PressureImplementation.RBSGS_PCG
+    method = {"jacobi": R.PressureImplementation.JACOBI_PCG_V1, "rbsgs": R.PressureImplementation.RBSGS_PCG,
+              "sgs": R.PressureImplementation.SGS_PCG_V1, "mixed": R.PressureImplementation.MG_MIXED}[args.method]
     settings = R.PressureSettings(1e-8, 0.0, MAXF, args.max_iters if args.max_iters > 0 else 1000000)
-    cfg = R.CarrierConfig(pressure=settings, storage=args.storage, implementation=method, device=local,
-                          max_courant=1.0)
+    if args.method == "mixed":
+        cfg = R.CarrierConfig.mixed(pressure=settings, device=local)
+    else:
+        cfg = R.CarrierConfig(pressure=settings, storage=args.storage, implementation=method, device=local,
+                              max_courant=1.0)
     sim = R.CarrierSimulation(g, cfg)
     sim.upload(faces)
     stream = torch.cuda.ExternalStream(sim.stream(), device=local)
@@ -300,7 +358,8 @@ def run_ours(args, world, rank, local):
     # timed on the carrier's stream on the current vectors.
     hbm, hbm_kind = peaks()
     launches_prof = 3 if args.no_profile else 50
-    pass_ms = {0: sim.profile(0, launches_prof), 1: sim.profile(1, launches_prof)}
+    pass_ms = {0: sim.profile(0, launches_prof),
+               1: sim.profile(1, launches_prof) if method != R.PressureImplementation.MG_MIXED else 0.0}
     # algorithmic bytes: pass 1 reads z, d_old and writes d_new (24N); pass 2
     # reads p, d, r and writes p, r, z (48N)
     bytes_pass = {0: 24 * cells, 1: 48 * cells}
@@ -352,6 +411,9 @@ def run_ours(args, world, rank, local):
     batched = None
     if not args.no_batched and rank == 0 and world == 1:
         batched = run_batched(args, local, flush)
+    serving = None
+    if not args.no_serving and rank == 0 and world == 1:
+        serving = run_serving(args, local)
 
     result = {
         "metric": METRIC,
@@ -368,7 +430,8 @@ def run_ours(args, world, rank, local):
         "data": "synthetic (seeded SplitMix64 random-Fourier velocity, host-generated)",
         "config": {
             "workload": WORKLOAD.format(n=args.n, storage=args.storage,
-                                        method="Jacobi-PCG" if args.method == "jacobi" else "RB-SGS-PCG"),
+                                        method={"jacobi": "Jacobi-PCG", "rbsgs": "RB-SGS-PCG", "sgs": "SGS-PCG (v1)",
+                                                "mixed": "FP32-multigrid FCG"}[args.method]),
             "cells": cells,
             "parallelism": f"replicas x{world} (independent boxes, no collective)",
             "l2": "256 MB buffer written between timed steps; per-step working set > 126 MB L2",
@@ -402,6 +465,8 @@ def run_ours(args, world, rank, local):
         result["variants"] = variants
     if batched:
         result["batched"] = batched
+    if serving:
+        result["serving"] = serving
     sim.close()
     return result
 

@@ -321,6 +321,13 @@ RB200_API void* rb200_carrier_stream(rb200_carrier* carrier);
 RB200_API int rb200_carrier_upload(rb200_carrier* carrier, const void* u, const void* v, const void* w,
                          const float* tracer);
 RB200_API int rb200_carrier_download(rb200_carrier* carrier, void* u, void* v, void* w, float* tracer);
+/* Random-Fourier accepted state generated on the device: u_d(x) = amplitude *
+ * sum_m amp[m][d] sin(2 pi k_m.x/L + phase[m]) + noise * U(-1,1) at the face
+ * centres (x in cell units, L the cell counts), wall-normal faces 0; k and amp
+ * are modes x 3 row-major, modes <= 8. U is SplitMix64 stream 16+d of `seed`,
+ * as the host generator. The tracer, if any, is cleared. */
+RB200_API int rb200_carrier_init_fourier(rb200_carrier* carrier, uint64_t seed, int modes, const double* k,
+                                         const double* phase, const double* amp, double amplitude, double noise);
 /* Device pointers of the accepted state (valid until the next step). */
 RB200_API int rb200_carrier_state_device(rb200_carrier* carrier, void** u, void** v, void** w,
                                float** tracer);
@@ -335,6 +342,10 @@ RB200_API int rb200_carrier_step(rb200_carrier* carrier, const rb200_step_params
  * the report and returns the step status. */
 RB200_API int rb200_carrier_step_async(rb200_carrier* carrier, const rb200_step_params* params);
 RB200_API int rb200_carrier_step_wait(rb200_carrier* carrier, rb200_step_report* report);
+/* Nonblocking: 1 when the launched step has finished on the device (its
+ * report is ready for rb200_carrier_step_wait), 0 while it runs or when no
+ * step is in flight. */
+RB200_API int rb200_carrier_step_poll(const rb200_carrier* carrier);
 /* Batched instances: launch one step of every carrier, then wait for all.
  * statuses[i] receives each step's status; returns the first launch error. */
 RB200_API int rb200_carriers_step(rb200_carrier* const* carriers, size_t count, const rb200_step_params* params,

@@ -555,6 +555,21 @@ class CarrierSimulation:
         if st != N.OK:
             raise SimulationError(st)
 
+    def init_fourier(self, seed: int, modes: int = 8, kmax: int = 8, amplitude: float = 1.0, noise: float = 0.05):
+        """Random-Fourier accepted state generated on the device (the same
+        modes and noise stream as workloads.fourier_faces)."""
+        from . import workloads as W
+
+        k, phase, amp = W.fourier_modes(seed, modes, kmax)
+        k = np.ascontiguousarray(k, dtype=np.float64)
+        phase = np.ascontiguousarray(phase, dtype=np.float64)
+        amp = np.ascontiguousarray(amp, dtype=np.float64)
+        st = lib().rb200_carrier_init_fourier(self._handle, seed & 0xFFFFFFFFFFFFFFFF, modes,
+                                              k.ctypes.data_as(C.c_void_p), phase.ctypes.data_as(C.c_void_p),
+                                              amp.ctypes.data_as(C.c_void_p), amplitude, noise)
+        if st != N.OK:
+            raise SimulationError(st)
+
     def upload_ptrs(self, u: int, v: int, w: int, tracer: int = 0):
         """Upload from host pointers (e.g. pinned buffers)."""
         st = lib().rb200_carrier_upload(self._handle, u, v, w, tracer or None)
@@ -621,6 +636,10 @@ class CarrierSimulation:
         st = lib().rb200_carrier_step_async(self._handle, C.byref(self._params(params)))
         if st != N.OK:
             raise SimulationError(st)
+
+    def step_done(self) -> bool:
+        """Nonblocking: has the step launched by step_async finished?"""
+        return bool(lib().rb200_carrier_step_poll(self._handle))
 
     def step_wait(self) -> StepReport:
         r = N.StepReport()

@@ -141,10 +141,12 @@ SIGNATURES = {
     "rb200_carrier_stream": (_P, [_P]),
     "rb200_carrier_upload": (_I, [_P, _P, _P, _P, _P]),
     "rb200_carrier_download": (_I, [_P, _P, _P, _P, _P]),
+    "rb200_carrier_init_fourier": (_I, [_P, C.c_uint64, _I, _P, _P, _P, _D, _D]),
     "rb200_carrier_state_device": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "rb200_carrier_step": (_I, [_P, C.POINTER(StepParams), C.POINTER(StepReport), CANCEL_FN, _P]),
     "rb200_carrier_step_async": (_I, [_P, C.POINTER(StepParams)]),
     "rb200_carrier_step_wait": (_I, [_P, C.POINTER(StepReport)]),
+    "rb200_carrier_step_poll": (_I, [_P]),
     "rb200_carriers_step": (_I, [C.POINTER(_P), _S, C.POINTER(StepParams), C.POINTER(StepReport), C.POINTER(_I)]),
     "rb200_carrier_profile": (_I, [_P, _I, _I, C.POINTER(_D)]),
     "rb200_carrier_pressure": (_I, [_P, _P, _S]),

@@ -159,6 +159,65 @@ __global__ void k_step_end(GridDev g, CarrierDev* cd, const SolveState* st) {
     cd->status = status;
 }
 
+// Random-Fourier initial state on the device: u_d(x) = sum_m a_{m,d}
+// sin(2 pi k_m.x/L + phi_m) + noise * U(-1,1) at the face centres, wall-normal
+// faces 0. The noise is the counter-based SplitMix64 stream 16+d of the host
+// generator (rheon_b200/workloads.py), so it matches the host bit for bit;
+// sin is the device's double-precision sine.
+struct FourierModes {
+    double k[8][3];
+    double phase[8];
+    double amp[8][3];
+    int modes;
+    double amplitude, noise;
+    unsigned long long seed;
+};
+
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
+    unsigned long long z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+template <class T>
+__global__ void k_fourier_init(GridDev g, CarrierDev* cd, FourierModes fm) {
+    const long long total = (long long)g.flen[0] + g.flen[1] + g.flen[2];
+    const double two_pi = 6.283185307179586;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int a = 0;
+        long long f = t;
+        if (f >= g.flen[0]) {
+            f -= g.flen[0];
+            a = 1;
+            if (f >= g.flen[1]) {
+                f -= g.flen[1];
+                a = 2;
+            }
+        }
+        const int p[3] = {int(f % g.fc[a][0]), int((f / g.fc[a][0]) % g.fc[a][1]),
+                          int(f / ((long long)g.fc[a][0] * g.fc[a][1]))};
+        T* dst = (T*)cd->faces[cd->acc][a];
+        if (p[a] == 0 || p[a] == g.n[a]) {
+            dst[f] = T(0);
+            continue;
+        }
+        double x[3];
+        for (int d = 0; d < 3; ++d) x[d] = double(p[d]) + (d == a ? 0.0 : 0.5);
+        double val = 0.0;
+        for (int m = 0; m < fm.modes; ++m) {
+            double arg = two_pi * (fm.k[m][0] * x[0] / g.n[0] + fm.k[m][1] * x[1] / g.n[1] +
+                                   fm.k[m][2] * x[2] / g.n[2]) + fm.phase[m];
+            val += fm.amplitude * fm.amp[m][a] * sin(arg);
+        }
+        const unsigned long long key = fm.seed ^ ((unsigned long long)(16 + a) << 48);
+        const unsigned long long u = splitmix64((unsigned long long)f ^ key);
+        const double r = 2.0 * double(u >> 11) * 1.1102230246251565e-16 - 1.0;
+        dst[f] = T(val + fm.noise * r);
+    }
+}
+
 // Per-axis face maxima and validation of an uploaded state.
 template <class T>
 int launch_validate_faces(const GridDev& g, const T* u, const T* v, const T* w, int* flags, cudaStream_t s);
@@ -397,6 +456,36 @@ int rb200_carrier_upload(rb200_carrier* carrier, const void* u, const void* v, c
     return upload_rate(c);
 }
 
+int rb200_carrier_init_fourier(rb200_carrier* carrier, uint64_t seed, int modes, const double* k, const double* phase,
+                               const double* amp, double amplitude, double noise) {
+    if (!carrier || modes < 0 || modes > 8 || (modes > 0 && (!k || !phase || !amp))) return RB200_INVALID_ARGUMENT;
+    rb200_carrier* c = carrier;
+    if (c->in_flight) return RB200_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    FourierModes fm{};
+    fm.modes = modes;
+    for (int m = 0; m < modes; ++m) {
+        for (int d = 0; d < 3; ++d) {
+            fm.k[m][d] = k[3 * m + d];
+            fm.amp[m][d] = amp[3 * m + d];
+        }
+        fm.phase[m] = phase[m];
+    }
+    fm.amplitude = amplitude;
+    fm.noise = noise;
+    fm.seed = seed;
+    const GridDev& g = c->g;
+    const long long faces = (long long)g.flen[0] + g.flen[1] + g.flen[2];
+    const int fb = blocks_for(faces, 256, 148 * 64);
+    if (c->elem == 4)
+        k_fourier_init<float><<<fb, 256, 0, c->stream>>>(g, c->cd, fm);
+    else
+        k_fourier_init<double><<<fb, 256, 0, c->stream>>>(g, c->cd, fm);
+    RB200_CUDA(cudaGetLastError());
+    if (c->tracer[0]) RB200_CUDA(cudaMemsetAsync(c->tracer[c->h_cd->tacc], 0, size_t(g.cells) * 4, c->stream));
+    return upload_rate(c);
+}
+
 int rb200_carrier_download(rb200_carrier* carrier, void* u, void* v, void* w, float* tracer) {
     if (!carrier) return RB200_INVALID_ARGUMENT;
     rb200_carrier* c = carrier;
@@ -462,6 +551,12 @@ int rb200_carrier_step_async(rb200_carrier* carrier, const rb200_step_params* pa
     RB200_CUDA(cudaEventRecord(c->ev[3], c->stream));
     c->in_flight = true;
     return RB200_OK;
+}
+
+int rb200_carrier_step_poll(const rb200_carrier* carrier) {
+    if (!carrier || !carrier->in_flight) return 0;
+    cudaSetDevice(carrier->device);
+    return cudaEventQuery(carrier->ev[3]) == cudaSuccess ? 1 : 0;
 }
 
 int rb200_carrier_step_wait(rb200_carrier* carrier, rb200_step_report* report) {
