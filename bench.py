@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--batched-instances", type=int, default=64)
     ap.add_argument("--batched-steps", type=int, default=20)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--solve-only", action="store_true",
+                    help="profiling aid: time pressure solves of one step's RHS through the workspace")
     ap.add_argument("--serving-requests", type=int, default=200)
     ap.add_argument("--serving-plain-requests", type=int, default=12)
     ap.add_argument("--serving-budget-gb", type=float, default=150.0)
@@ -284,6 +286,43 @@ def run_serving(args, local):
         "mixed": served,
         "plain_f64_per_request": dict(plain_summary, requests_run=len(plain_reqs)),
     }
+
+
+def run_solve_only(args, local):
+    """Profiling aid: pressure solves (method of --method) of the RHS of the
+    workload's first step, through a PressureWorkspace, whose iteration chunks
+    are plain CUDA graphs (listed kernel by kernel by ncu)."""
+    import torch
+
+    import rheon_b200 as R
+    from rheon_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    n = (args.n,) * 3
+    g = R.GridGeometry(n)
+    faces = [torch.from_numpy(f).cuda() for f in W.fourier_faces(n, seed=args.seed, dtype=np.float64)]
+    op = R.PressureOperator(g, 1.0)
+    rhs = torch.empty(g.cell_len(), dtype=torch.float64, device="cuda")
+    op.build_rhs(faces, 0.05, rhs)
+    method = {"jacobi": R.PressureImplementation.JACOBI_PCG_V1, "rbsgs": R.PressureImplementation.RBSGS_PCG,
+              "sgs": R.PressureImplementation.SGS_PCG_V1, "mixed": R.PressureImplementation.MG_MIXED}[args.method]
+    ws = R.PressureWorkspace(g, 1 << 40, method, device=local)
+    settings = R.PressureSettings(1e-8, 0.0, MAXF, args.max_iters if args.max_iters > 0 else 1000000)
+    stream = torch.cuda.ExternalStream(ws.stream(), device=local)
+    for _ in range(args.warmup):
+        ws.solve_rhs(op, rhs, 0.05, settings)
+    total, its = 0.0, []
+    for _ in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rep = ws.solve_rhs(op, rhs, 0.05, settings)
+        b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b)
+        its.append(rep.iterations)
+    return {"mode": "solve-only", "method": args.method, "n": args.n, "ms_per_solve": total / args.steps,
+            "iterations": statistics.mean(its)}
 
 
 # ------------------------------------------------------------------ our arm
@@ -551,6 +590,9 @@ def main():
             import torch.distributed as dist
 
             dist.destroy_process_group()
+        return
+    if args.solve_only:
+        print(json.dumps(run_solve_only(args, local)), flush=True)
         return
     result = run_ours(args, world, rank, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

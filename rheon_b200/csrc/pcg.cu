@@ -19,6 +19,7 @@
 
 #include "pcg.hpp"
 #include "slab.cuh"
+#include "solve_state.cuh"
 #include "stencil.cuh"
 
 namespace rb200 {
@@ -26,71 +27,6 @@ namespace rb200 {
 constexpr int EW = 256;
 constexpr int EW_CAP = 148 * 8;
 constexpr double kEps = 2.220446049250313e-16;
-
-enum Mode : int { MODE_INIT = 0, MODE_ITER = 1, MODE_REPLACE = 2 };
-constexpr int F_CANDIDATE = 32;  // RB-SGS: candidate decided in pass 2, acted on after z
-
-__device__ __forceinline__ bool gate(int flags, int mode) {
-    if (mode == MODE_INIT) return !(flags & F_DONE);
-    if (mode == MODE_ITER) return !(flags & F_STOP);
-    return (flags & F_NEED_REPLACE) != 0;
-}
-
-__device__ __forceinline__ int block_id3() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
-__device__ __forceinline__ int nblocks3() { return gridDim.x * gridDim.y * gridDim.z; }
-__device__ __forceinline__ int tid3() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
-
-__device__ __forceinline__ void finish(SolveState* st, int status, int flags) {
-    st->status = status;
-    st->flags = flags | F_DONE | F_STOP;
-}
-
-__device__ __forceinline__ void breakdown(SolveState* st, int iteration, int flags) {
-    st->breakdown_it = iteration;
-    finish(st, RB200_BREAKDOWN, flags);
-}
-
-// Decision after a fresh r.z (precondition's return value).
-__device__ __forceinline__ void decide_rz(SolveState* st, rb200_trace* trace, double rz, int mode) {
-    int flags = st->flags;
-    const int it = st->it;
-    if (mode == MODE_INIT) {
-        st->rz = rz;  // checked at iteration 1 (src/pressure.rs:662)
-        st->flags = flags | F_REPLACED;
-        return;
-    }
-    if (mode == MODE_REPLACE) {
-        if (trace && it >= 1) {
-            trace[it - 1].rz = rz;
-            trace[it - 1].beta = 0.0;
-            trace[it - 1].replaced = 1;
-        }
-        if (!isfinite(rz) || rz <= 0.0) {
-            breakdown(st, it, flags);
-            return;
-        }
-        st->rz = rz;
-        st->flags = (flags & ~(F_STOP | F_NEED_TRUE | F_NEED_REPLACE | F_CANDIDATE)) | F_REPLACED;
-        return;
-    }
-    // MODE_ITER
-    if (flags & F_CANDIDATE) {
-        st->rz_next = rz;
-        st->flags = (flags & ~F_CANDIDATE) | F_STOP | F_NEED_TRUE;
-        return;
-    }
-    if (!isfinite(rz) || rz <= 0.0) {
-        breakdown(st, it, flags);
-        return;
-    }
-    double beta = rz / st->rz;
-    if (trace) {
-        trace[it - 1].rz = rz;
-        trace[it - 1].beta = beta;
-    }
-    st->beta = beta;
-    st->rz = rz;
-}
 
 // ------------------------------------------------------------------ init
 // Compatibility sums, threshold and the true report of p = 0
@@ -554,54 +490,6 @@ __global__ void __launch_bounds__(EW) k_mg_update(GridDev g, SolveState* st, dou
     }
 }
 
-__global__ void __launch_bounds__(EW) k_mg_finish(GridDev g, SolveState* st, const float* __restrict__ x0,
-                                                  double* __restrict__ z, const double* __restrict__ r,
-                                                  const double* __restrict__ q, int mode, Partials part,
-                                                  rb200_trace* trace) {
-    __shared__ BlockReduce<2, 0> red;
-    const int flags = st->flags;
-    if (!gate(flags, mode)) return;
-    Neu rz, zq;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
-        const double zc = c == 0 ? 0.0 : double(x0[c]);
-        z[c] = zc;
-        if (c == 0) continue;
-        rz.add(r[c] * zc);
-        if (mode == MODE_ITER) zq.add(zc * q[c]);
-    }
-    dd sums[2] = {rz.as_dd(), zq.as_dd()};
-    double none[1];
-    block_reduce<2, 0>(red, sums, none);
-    if (publish_and_check_last<2, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
-        fold_partials<2, 0>(part, gridDim.x, red, sums, none);
-        if (threadIdx.x == 0) {
-            const double rzv = dd_value(sums[0]);
-            if (mode != MODE_ITER) {
-                decide_rz(st, trace, rzv, mode);
-                return;
-            }
-            const int it = st->it;
-            const double beta = -dd_value(sums[1]) / st->curvature;
-            if (flags & F_CANDIDATE) {
-                st->rz_next = rzv;
-                st->beta_next = beta;
-                st->flags = (flags & ~F_CANDIDATE) | F_STOP | F_NEED_TRUE;
-                return;
-            }
-            if (!isfinite(rzv) || rzv <= 0.0 || !isfinite(beta)) {
-                breakdown(st, it, flags);
-                return;
-            }
-            if (trace) {
-                trace[it - 1].rz = rzv;
-                trace[it - 1].beta = beta;
-            }
-            st->beta = beta;
-            st->rz = rzv;
-        }
-    }
-}
-
 // ------------------------------------------------------------ lexicographic SGS
 // precondition_sgs (src/pressure.rs:467-532): forward
 //   y_i = (r_i + sum_{lower d} w_d y_{i-s_d}) / D_i    (d = X, Y, Z in order)
@@ -876,8 +764,7 @@ static int launch_start(const GridDev& g, int method, const Bufs& B, const Multi
     k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part, B.trace);
     if (method == RB200_SGS_PCG_V1) return 2 + launch_sgs(g, B, MODE_INIT, s);
     int n = 2 + mg->enqueue(B.r, B.st, MODE_INIT, s);
-    k_mg_finish<<<eb, EW, 0, s>>>(g, B.st, mg->x0(), B.z, B.r, B.q, MODE_INIT, B.part, B.trace);
-    return n + 1;
+    return n + mg->enqueue_finish(B.st, B.z, B.r, B.q, MODE_INIT, B.part, B.trace, s);
 }
 
 // One PCG iteration (src/pressure.rs:651-734).
@@ -906,8 +793,7 @@ static int launch_iteration(const GridDev& g, int method, const Bufs& B, const M
     }
     k_mg_update<<<eb, EW, 0, s>>>(g, B.st, B.p, B.r, B.d0, B.d1, B.q, B.part, B.trace);
     int n = 2 + mg->enqueue(B.r, B.st, MODE_ITER, s);
-    k_mg_finish<<<eb, EW, 0, s>>>(g, B.st, mg->x0(), B.z, B.r, B.q, MODE_ITER, B.part, B.trace);
-    return n + 1;
+    return n + mg->enqueue_finish(B.st, B.z, B.r, B.q, MODE_ITER, B.part, B.trace, s);
 }
 
 // The gated true-residual check and restart (src/pressure.rs:686-715).
@@ -930,8 +816,7 @@ static int launch_check(const GridDev& g, int method, const Bufs& B, const Multi
     k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part, B.trace);
     if (method == RB200_SGS_PCG_V1) return 2 + launch_sgs(g, B, MODE_REPLACE, s);
     int n = 2 + mg->enqueue(B.r, B.st, MODE_REPLACE, s);
-    k_mg_finish<<<eb, EW, 0, s>>>(g, B.st, mg->x0(), B.z, B.r, B.q, MODE_REPLACE, B.part, B.trace);
-    return n + 1;
+    return n + mg->enqueue_finish(B.st, B.z, B.r, B.q, MODE_REPLACE, B.part, B.trace, s);
 }
 
 static SolveState initial_state(double dt, const rb200_settings& s) {

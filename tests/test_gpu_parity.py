@@ -457,7 +457,8 @@ def test_multigrid_recovers_manufactured_pressure_on_small_grids(counts):
     assert np.max(np.abs(ws.pressure() - exact + exact[0])) < 1e-8
 
 
-@pytest.mark.parametrize("counts", [[32, 32, 32], [64, 64, 64], [40, 40, 40], [64, 32, 16], [48, 24, 96]])
+@pytest.mark.parametrize("counts", [[32, 32, 32], [64, 64, 64], [40, 40, 40], [64, 32, 16], [48, 24, 96],
+                                    [9, 9, 9], [17, 9, 33], [72, 40, 24], [100, 52, 20], [13, 1, 70]])
 @pytest.mark.parametrize("rel", [1e-8, 1e-10])
 def test_multigrid_reaches_the_target_residual_in_few_iterations(counts, rel):
     g = R.GridGeometry(counts)
@@ -471,6 +472,19 @@ def test_multigrid_reaches_the_target_residual_in_few_iterations(counts, rel):
     assert rep.iterations <= 40, rep.iterations
     ref = O.solve_rhs(og(g), 1.0, O.JACOBI_PCG_V1, rhs, 0.25, O.settings(1e-12, 0.0, 1.7976931348623157e308, 100000))
     assert relerr(ws.pressure(), ref.pressure) < 1e3 * rel
+
+
+@pytest.mark.parametrize("edge", [8, 24, 56, 104, 136, 200, 248])
+def test_multigrid_hierarchy_exists_for_every_serving_edge(edge):
+    """Every edge the serving workload draws (multiples of 8 up to 256) gets a
+    hierarchy whose coarsest grid is small enough for the dense solve."""
+    g = R.GridGeometry((edge, edge, edge))
+    sim = R.CarrierSimulation(g, R.CarrierConfig.mixed(pressure=S(1e-8, 0.0, 1.7976931348623157e308, 500)))
+    sim.init_fourier(5)
+    rep = sim.step(R.StepParams(1e30, cfl=0.5))
+    assert rep.pressure.iterations <= 40
+    assert rep.actual_divergence_max < 1e-3
+    sim.close()
 
 
 def test_mixed_carrier_tracks_the_fp64_oracle():
