@@ -212,8 +212,11 @@ RB200_API int rb200_workspace_set_trace(rb200_workspace* ws, rb200_trace* trace,
 /* Diagnostics: average device milliseconds of one PCG pass (which = 0: the
  * fused direction update + operator + curvature pass, 1: the fused update +
  * preconditioner + dots pass), over `launches` back-to-back launches timed with
- * CUDA events on the handle's stream, on the current vectors. Leaves the
- * solver's scalars in a timing state; the next solve resets them. */
+ * CUDA events on the handle's stream, on the current vectors; or (which = 2)
+ * of one iteration of the persistent Jacobi-PCG kernel, run for `launches`
+ * iterations in one launch (RB200_UNSUPPORTED when the handle does not use
+ * it). Leaves the solver's scalars in a timing state; the next solve resets
+ * them. */
 RB200_API int rb200_workspace_profile(rb200_workspace* ws, int which, int launches, double* avg_ms);
 
 /* Allocation-free Jacobi-PCG solve. No counterpart in the reference.

@@ -596,7 +596,8 @@ class CarrierSimulation:
         return [x.value or 0 for x in p]
 
     def profile(self, which: int, launches: int = 20) -> float:
-        """Average device ms of one PCG pass (0: direction+apply, 1: update)."""
+        """Average device ms of one PCG pass (0: direction+apply, 1: update),
+        or of one iteration of the persistent Jacobi-PCG kernel (2)."""
         ms = C.c_double()
         st = lib().rb200_carrier_profile(self._handle, which, launches, C.byref(ms))
         if st != N.OK:

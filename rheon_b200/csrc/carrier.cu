@@ -11,6 +11,7 @@
 // corrected buffers and publishes by rotating buffer indices on the device.
 #include <cmath>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 
@@ -531,6 +532,19 @@ int rb200_carrier_profile(rb200_carrier* carrier, int which, int launches, doubl
     return carrier->solver.profile(which, launches, avg_ms);
 }
 
+// Steps whose solve is the persistent (cooperative, grid-barrier) kernel are
+// ordered one after another on each device: two such kernels never compete
+// for co-residency. Other carriers' steps overlap freely.
+static cudaEvent_t cooperative_lane(int device) {
+    static std::mutex mu;
+    static cudaEvent_t lanes[64] = {};
+    if (device < 0 || device >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!lanes[device] && cudaEventCreateWithFlags(&lanes[device], cudaEventDisableTiming) != cudaSuccess)
+        lanes[device] = nullptr;
+    return lanes[device];
+}
+
 int rb200_carrier_step_async(rb200_carrier* carrier, const rb200_step_params* params) {
     if (!carrier || !params) return RB200_INVALID_ARGUMENT;
     rb200_carrier* c = carrier;
@@ -546,9 +560,13 @@ int rb200_carrier_step_async(rb200_carrier* carrier, const rb200_step_params* pa
     RB200_CUDA(cudaMemcpyAsync(&c->cd->requested_dt, &c->h_cd->requested_dt,
                                offsetof(CarrierDev, max_courant) - offsetof(CarrierDev, requested_dt),
                                cudaMemcpyHostToDevice, c->stream));
+    cudaEvent_t lane = c->solver.persistent_blocks() ? cooperative_lane(c->device) : nullptr;
+    if (c->solver.persistent_blocks() && !lane) return RB200_EXECUTION;
+    if (lane) RB200_CUDA(cudaStreamWaitEvent(c->stream, lane, 0));
     RB200_CUDA(cudaEventRecord(c->ev[2], c->stream));
     RB200_CUDA(cudaGraphLaunch(c->step_exec, c->stream));
     RB200_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    if (lane) RB200_CUDA(cudaEventRecord(lane, c->stream));
     c->in_flight = true;
     return RB200_OK;
 }

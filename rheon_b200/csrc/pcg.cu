@@ -239,37 +239,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_pass1(GridDev g, SolveState* s
     const int nb = nblocks3();
     if (publish_and_check_last<1, 0>(part, block_id3(), nb, sums, none)) {
         fold_partials<1, 0>(part, nb, red, sums, none);
-        if (tid3() == 0) {
-            double curvature = dd_value(sums[0]);
-            if (flags & F_PROFILE) {
-                st->curvature = curvature;
-                st->dsel = dsel ^ 1;
-                return;
-            }
-            double rz = st->rz;
-            int it = st->it + 1;
-            int fl = flags & ~F_REPLACED;
-            st->curvature = curvature;
-            st->dsel = dsel ^ 1;
-            if (trace) {
-                trace[it - 1].curvature = curvature;
-                trace[it - 1].replaced = 0;
-                trace[it - 1].checked = 0;
-            }
-            // src/pressure.rs:661-668.
-            if (!isfinite(curvature) || curvature <= 0.0 || !isfinite(rz) || rz <= 0.0) {
-                breakdown(st, it, fl);
-                return;
-            }
-            double alpha = rz / curvature;
-            if (!isfinite(alpha)) {
-                breakdown(st, it, fl);
-                return;
-            }
-            if (trace) trace[it - 1].alpha = alpha;
-            st->alpha = alpha;
-            st->flags = fl;
-        }
+        if (tid3() == 0) decide_pass1(st, trace, dd_value(sums[0]), flags, dsel);
     }
 }
 
@@ -338,30 +308,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_pass2(GridDev g, SolveState* s
     const int nb = nblocks3();
     if (publish_and_check_last<2, 0>(part, block_id3(), nb, sums, none)) {
         fold_partials<2, 0>(part, nb, red, sums, none);
-        if (tid3() == 0) {
-            if (flags & F_PROFILE) {
-                st->recursive_l2 = dd_value(sums[0]);
-                st->rz_next = dd_value(sums[1]);
-                return;
-            }
-            int it = st->it + 1;
-            st->it = it;
-            double recursive_l2 = sqrt(dd_value(sums[0]));
-            st->recursive_l2 = recursive_l2;
-            if (trace) trace[it - 1].recursive_l2 = recursive_l2;
-            bool candidate = recursive_l2 <= st->threshold || it == st->max_it;
-            if (PRE == 0) {
-                double rz = dd_value(sums[1]);
-                if (candidate) {
-                    st->rz_next = rz;
-                    st->flags = flags | F_STOP | F_NEED_TRUE;
-                } else {
-                    decide_rz(st, trace, rz, MODE_ITER);
-                }
-            } else if (candidate) {
-                st->flags = flags | F_CANDIDATE;
-            }
-        }
+        if (tid3() == 0) decide_pass2(st, trace, dd_value(sums[0]), dd_value(sums[1]), flags, PRE == 0);
     }
 }
 
@@ -406,48 +353,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_true_residual(GridDev g, Solve
     const int nb = nblocks3();
     if (publish_and_check_last<1, 1>(part, block_id3(), nb, sums, mx)) {
         fold_partials<1, 1>(part, nb, red, sums, mx);
-        if (tid3() == 0) {
-            const int it = st->it;
-            double squared = dd_value(sums[0]);
-            double maximum = mx[0];
-            double div = maximum * st->dt / g.volume;
-            if (trace && it >= 1) trace[it - 1].checked = 1;
-            if (!isfinite(squared) || !isfinite(div)) {
-                breakdown(st, it, flags);
-                return;
-            }
-            double l2 = sqrt(squared);
-            st->true_l2 = l2;
-            st->true_max = maximum;
-            st->true_div = div;
-            if (l2 <= st->threshold && div <= st->divergence_limit) {
-                finish(st, RB200_OK, flags);
-                return;
-            }
-            bool replaced = l2 > st->threshold;
-            if (it == st->max_it) {
-                finish(st, RB200_ITERATION_LIMIT, flags);
-                return;
-            }
-            if (replaced) {
-                st->flags = (flags & ~F_NEED_TRUE) | F_NEED_REPLACE;
-                return;
-            }
-            // Keep the recurrence: precondition the recursive residual.
-            double rz = st->rz_next;
-            if (!isfinite(rz) || rz <= 0.0) {
-                breakdown(st, it, flags);
-                return;
-            }
-            double beta = st->flexible ? st->beta_next : rz / st->rz;
-            if (trace) {
-                trace[it - 1].rz = rz;
-                trace[it - 1].beta = beta;
-            }
-            st->beta = beta;
-            st->rz = rz;
-            st->flags = flags & ~(F_STOP | F_NEED_TRUE);
-        }
+        if (tid3() == 0) decide_true(st, trace, dd_value(sums[0]), mx[0], flags, g.volume);
     }
 }
 
@@ -707,24 +613,35 @@ static bool tma_eligible(const GridDev& g) {
     return (g.n[0] % 2) == 0 && g.n[0] >= Slab<ZC>::SX && g.n[1] >= Slab<ZC>::SY && g.n[2] >= Slab<ZC>::SZ;
 }
 
-static bool encode_slab_map(CUtensorMap* m, const double* base, const GridDev& g) {
+static bool encode_map(CUtensorMap* m, const double* base, const GridDev& g, const cuuint32_t box[3]) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc) return false;
     cuuint64_t dims[3] = {cuuint64_t(g.n[0]), cuuint64_t(g.n[1]), cuuint64_t(g.n[2])};
     cuuint64_t strides[2] = {cuuint64_t(g.n[0]) * 8, cuuint64_t(g.n[0]) * cuuint64_t(g.n[1]) * 8};
-    cuuint32_t box[3] = {cuuint32_t(Slab<ZC>::SX), cuuint32_t(Slab<ZC>::SY), cuuint32_t(Slab<ZC>::SZ)};
     cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides,
+                     const_cast<cuuint32_t*>(box), estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
 
-static TmaMaps make_maps(const GridDev& g, const double* z, const double* d0, const double* d1, const double* p) {
+static bool encode_slab_map(CUtensorMap* m, const double* base, const GridDev& g) {
+    const cuuint32_t box[3] = {cuuint32_t(Slab<ZC>::SX), cuuint32_t(Slab<ZC>::SY), cuuint32_t(Slab<ZC>::SZ)};
+    return encode_map(m, base, g, box);
+}
+
+static bool encode_box_map(CUtensorMap* m, const double* base, const GridDev& g) {
+    const cuuint32_t box[3] = {cuuint32_t(TX), cuuint32_t(TY), cuuint32_t(ZC)};
+    return encode_map(m, base, g, box);
+}
+
+static TmaMaps make_maps(const GridDev& g, const double* z, const double* d0, const double* d1, const double* p,
+                         const double* r) {
     TmaMaps m;
     std::memset(&m, 0, sizeof(m));
     if (tma_eligible(g) && encode_slab_map(&m.z, z, g) && encode_slab_map(&m.d0, d0, g) &&
-        encode_slab_map(&m.d1, d1, g) && encode_slab_map(&m.p, p, g))
+        encode_slab_map(&m.d1, d1, g) && encode_slab_map(&m.p, p, g) && encode_box_map(&m.p_box, p, g) &&
+        encode_box_map(&m.r_box, r, g))
         m.use = 1;
     else
         std::memset(&m, 0, sizeof(m));
@@ -857,7 +774,72 @@ PcgSolver::~PcgSolver() {
     cudaFree(part_.ticket);
     cudaFree(st_);
     cudaFree(d_trace_);
+    cudaFree(gbar_);
+    cudaFree(ppart_);
     if (h_st_) cudaFreeHost(h_st_);
+}
+
+// Whether a cooperative launch of the persistent kernel can sit in a CUDA
+// graph, inside the body of a WHILE conditional node (the resident carrier's
+// form). Checked once per process by capturing and instantiating such a graph
+// (nothing is launched).
+static bool persistent_graphs_supported(PcgSolver& solver) {
+    static std::once_flag once;
+    static bool supported = false;
+    std::call_once(once, [&] {
+        cudaStream_t outer = nullptr, body_stream = nullptr;
+        if (cudaStreamCreateWithFlags(&outer, cudaStreamNonBlocking) != cudaSuccess) return;
+        if (cudaStreamCreateWithFlags(&body_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaStreamDestroy(outer);
+            return;
+        }
+        bool ok = cudaStreamBeginCapture(outer, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        cudaGraph_t graph = nullptr;
+        if (ok) {
+            cudaStreamCaptureStatus status;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t ndeps = 0;
+            cudaGraph_t g = nullptr;
+            ok = cudaStreamGetCaptureInfo(outer, &status, nullptr, &g, &deps, &ndeps) == cudaSuccess;
+            cudaGraphConditionalHandle handle;
+            ok = ok && cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+            cudaGraphNodeParams cp{};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = handle;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            ok = ok && cudaGraphAddNode(&node, g, deps, ndeps, &cp) == cudaSuccess;
+            if (ok) {
+                cudaGraph_t body = cp.conditional.phGraph_out[0];
+                ok = cudaStreamBeginCaptureToGraph(body_stream, body, nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeRelaxed) == cudaSuccess;
+                if (ok) {
+                    const GridDev& gd = solver.grid();
+                    cudaError_t le = solver.launch_persistent_chunk(body_stream, 1);
+                    cudaGraph_t captured = nullptr;
+                    cudaError_t ee = cudaStreamEndCapture(body_stream, &captured);
+                    (void)gd;
+                    ok = le == cudaSuccess && ee == cudaSuccess;
+                }
+                ok = ok && cudaStreamUpdateCaptureDependencies(outer, &node, 1, cudaStreamSetCaptureDependencies) ==
+                               cudaSuccess;
+            }
+        }
+        cudaError_t end = cudaStreamEndCapture(outer, &graph);
+        ok = ok && end == cudaSuccess;
+        if (ok) {
+            cudaGraphExec_t exec = nullptr;
+            ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+            if (exec) cudaGraphExecDestroy(exec);
+        }
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        cudaStreamDestroy(body_stream);
+        cudaStreamDestroy(outer);
+        supported = ok;
+    });
+    return supported;
 }
 
 int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
@@ -892,9 +874,26 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
     RB200_CUDA(cudaMalloc(&st_, sizeof(SolveState)));
     RB200_CUDA(cudaMallocHost(&h_st_, 2 * sizeof(SolveState)));
     for (auto& e : ev_) RB200_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    maps_ = make_maps(g, z_, d_[0], d_[1], p_);
+    maps_ = make_maps(g, z_, d_[0], d_[1], p_, r_);
     chunk_ = (method == RB200_MG_MIXED || method == RB200_SGS_PCG_V1) ? 4 : (g.cells >= (1 << 20) ? 32 : 16);
+    if (method == RB200_JACOBI_PCG_V1 && maps_.use) {
+        int blocks = 0;
+        if ((rc = persistent_setup(g, &blocks))) return rc;
+        if (blocks > 0) {
+            RB200_CUDA(cudaMalloc(&gbar_, sizeof(GridBarrier)));
+            RB200_CUDA(cudaMemsetAsync(gbar_, 0, sizeof(GridBarrier), stream_));
+            if ((rc = alloc(&ppart_, persistent_partial_doubles(blocks)))) return rc;
+            persist_blocks_ = blocks;
+            if (!persistent_graphs_supported(*this)) persist_blocks_ = 0;
+            else chunk_ = 64;
+        }
+    }
     return capture_chunk();
+}
+
+cudaError_t PcgSolver::launch_persistent_chunk(cudaStream_t s, int budget) {
+    return launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, d_trace_, maps_, persist_blocks_,
+                             budget, s);
 }
 
 int PcgSolver::set_trace(rb200_trace* host, size_t capacity) {
@@ -919,10 +918,17 @@ int PcgSolver::capture_chunk() {
     cudaGraph_t graph = nullptr;
     RB200_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     int nodes = 0;
-    for (int q = 0; q < chunk_; ++q) nodes += launch_iteration(g_, method_, B, mg, stream_);
-    nodes += launch_check(g_, method_, B, mg, stream_);
+    cudaError_t launch_err = cudaSuccess;
+    if (persist_blocks_) {
+        launch_err = launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, d_trace_, maps_,
+                                       persist_blocks_, chunk_, stream_);
+        nodes = 1;
+    } else {
+        for (int q = 0; q < chunk_; ++q) nodes += launch_iteration(g_, method_, B, mg, stream_);
+        nodes += launch_check(g_, method_, B, mg, stream_);
+    }
     nodes_per_chunk_ = nodes;
-    cudaError_t launch_err = cudaGetLastError();
+    if (launch_err == cudaSuccess) launch_err = cudaGetLastError();
     cudaError_t end_err = cudaStreamEndCapture(stream_, &graph);
     if (launch_err != cudaSuccess || end_err != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -964,6 +970,7 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
     RB200_CUDA(cudaMemcpyAsync(st_, &h_st_[0], sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     if (d_trace_) RB200_CUDA(cudaMemsetAsync(d_trace_, 0, trace_cap_ * sizeof(rb200_trace), stream_));
     RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), stream_));
+    if (gbar_) RB200_CUDA(cudaMemsetAsync(gbar_, 0, sizeof(GridBarrier), stream_));
     launches_ += uint64_t(launch_start(g_, method_, Bufs{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_},
                                        method_ == RB200_MG_MIXED ? &mg_ : nullptr, stream_));
     RB200_CUDA(cudaGetLastError());
@@ -1011,6 +1018,7 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
 int PcgSolver::enqueue_reset(const double* dt_dev, const int* skip, const rb200_settings& settings, cudaStream_t s) {
     k_solve_reset<<<1, 1, 0, s>>>(st_, settings, dt_dev, skip, method_ == RB200_MG_MIXED ? 1 : 0);
     RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), s));
+    if (gbar_) RB200_CUDA(cudaMemsetAsync(gbar_, 0, sizeof(GridBarrier), s));
     launches_ += 1;
     const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_};
     launch_start(g_, method_, B, method_ == RB200_MG_MIXED ? &mg_ : nullptr, s);
@@ -1042,8 +1050,13 @@ int PcgSolver::enqueue_loop(cudaStream_t cs, cudaStream_t body_stream, const rb2
     RB200_CUDA(cudaStreamBeginCaptureToGraph(body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_};
     const Multigrid* mg = method_ == RB200_MG_MIXED ? &mg_ : nullptr;
-    for (int q = 0; q < chunk_; ++q) launch_iteration(g_, method_, B, mg, body_stream);
-    launch_check(g_, method_, B, mg, body_stream);
+    if (persist_blocks_) {
+        RB200_CUDA(launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, d_trace_, maps_,
+                                     persist_blocks_, chunk_, body_stream));
+    } else {
+        for (int q = 0; q < chunk_; ++q) launch_iteration(g_, method_, B, mg, body_stream);
+        launch_check(g_, method_, B, mg, body_stream);
+    }
     const uint64_t mi = settings.max_iterations;
     const uint64_t trips = (mi / uint64_t(chunk_)) * 2 + 64;
     k_loop_cond<<<1, 1, 0, body_stream>>>(st_, handle, trips > (1u << 24) ? (1 << 24) : int(trips));
@@ -1059,8 +1072,9 @@ int PcgSolver::enqueue_loop(cudaStream_t cs, cudaStream_t body_stream, const rb2
 }
 
 int PcgSolver::profile(int which, int launches, double* avg_ms) {
-    if (launches < 1 || (which != 0 && which != 1)) return RB200_INVALID_ARGUMENT;
+    if (launches < 1 || which < 0 || which > 2) return RB200_INVALID_ARGUMENT;
     if (method_ == RB200_MG_MIXED && which == 1) return RB200_UNSUPPORTED;
+    if (which == 2 && !persist_blocks_) return RB200_UNSUPPORTED;
     SolveState prof{};
     prof.rz = 1.0;
     prof.alpha = 1e-6;
@@ -1073,6 +1087,32 @@ int PcgSolver::profile(int which, int launches, double* avg_ms) {
     RB200_CUDA(cudaMemcpyAsync(st_, &h_st_[0], sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     const bool jac = method_ == RB200_JACOBI_PCG_V1;
     const dim3 grid = slab_grid(g_), block(TX, TY, 1);
+    if (which == 2) {
+        // one warm iteration, then `launches` iterations in one launch
+        RB200_CUDA(cudaMemsetAsync(gbar_, 0, sizeof(GridBarrier), stream_));
+        RB200_CUDA(launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, nullptr, maps_,
+                                     persist_blocks_, 1, stream_));
+        cudaEvent_t a, b;
+        RB200_CUDA(cudaEventCreate(&a));
+        RB200_CUDA(cudaEventCreate(&b));
+        RB200_CUDA(cudaEventRecord(a, stream_));
+        RB200_CUDA(launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, nullptr, maps_,
+                                     persist_blocks_, launches, stream_));
+        RB200_CUDA(cudaEventRecord(b, stream_));
+        RB200_CUDA(cudaEventSynchronize(b));
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, a, b);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        RB200_CUDA(cudaGetLastError());
+        RB200_CUDA(cudaMemcpy(&h_st_[0], st_, sizeof(SolveState), cudaMemcpyDeviceToHost));
+        if (h_st_[0].status == RB200_EXECUTION) {
+            set_error("persistent solver timing run failed");
+            return RB200_EXECUTION;
+        }
+        *avg_ms = double(ms) / launches;
+        return RB200_OK;
+    }
     auto launch = [&]() {
         if (which == 0)
             k_pass1<ZC><<<grid, block, kSmemPass1, stream_>>>(g_, st_, z_, d_[0], d_[1], q_, maps_, part_, nullptr);
@@ -1176,7 +1216,7 @@ int static_solve_jacobi(const GridDev& g, const double* rhs, double* pressure, d
     B.st = reinterpret_cast<SolveState*>(state_slot);
     B.part.ticket = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(state_slot) + sizeof(SolveState));
     B.trace = nullptr;
-    B.maps = make_maps(g, B.z, B.d0, B.d1, B.p);
+    B.maps = make_maps(g, B.z, B.d0, B.d1, B.p, B.r);
 
     SolveState init = initial_state(dt, s);
     // The array keeps the previous call's contents: the ticket must start at 0.

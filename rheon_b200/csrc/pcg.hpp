@@ -43,10 +43,28 @@ constexpr int ST_RUNNING = -1;
 
 // Tensor maps of the solver's vectors for the TMA slab loads (unused when the
 // grid takes the cp.async path).
+// z, d0, d1, p: halo slabs ((TX+4) x (TY+2) x (ZC+2)); p_box, r_box: one
+// brick without halo (TX x TY x ZC), for the persistent solver.
 struct TmaMaps {
     CUtensorMap z, d0, d1, p;
+    CUtensorMap p_box, r_box;
     int use;
 };
+
+// Grid barrier of the persistent solver kernel (zeroed before each solve).
+struct GridBarrier {
+    unsigned count;   // blocks arrived at the current barrier
+    unsigned gen;     // barrier generation
+    unsigned abort;   // a block gave up: every waiting block leaves
+    unsigned pad;
+};
+
+// Persistent Jacobi-PCG kernel (persist.cu).
+int persistent_setup(const GridDev& g, int* blocks);
+size_t persistent_partial_doubles(int blocks);
+cudaError_t launch_persistent(const GridDev& g, SolveState* st, const double* b, double* p, double* r, double* z,
+                              double* d0, double* d1, double* part, GridBarrier* bar, rb200_trace* trace,
+                              const TmaMaps& maps, int blocks, int budget, cudaStream_t s);
 
 class PcgSolver {
 public:
@@ -68,7 +86,9 @@ public:
     size_t bytes() const { return bytes_; }
     int set_trace(rb200_trace* host, size_t capacity);
     // Average device time of `launches` back-to-back launches of one PCG pass
-    // (which = 0: direction+apply, 1: update), timed with CUDA events on the
+    // (which = 0: direction+apply, 1: update), or (which = 2, persistent
+    // solver only) of one iteration of the persistent kernel run for
+    // `launches` iterations in one launch; timed with CUDA events on the
     // solver's stream, on the current vectors. Scalars are left in a timing
     // state; the next solve() resets them.
     int profile(int which, int launches, double* avg_ms);
@@ -82,6 +102,10 @@ public:
     int enqueue_reset(const double* dt_dev, const int* skip, const rb200_settings& settings, cudaStream_t s);
     int enqueue_loop(cudaStream_t capture_stream, cudaStream_t body_stream, const rb200_settings& settings);
     int nodes_per_chunk() const { return nodes_per_chunk_ + 1; }
+    // Blocks of the persistent solver kernel (0: the per-pass kernels run).
+    int persistent_blocks() const { return persist_blocks_; }
+    // One launch of the persistent kernel for at most `budget` iterations.
+    cudaError_t launch_persistent_chunk(cudaStream_t s, int budget);
     SolveState* state() { return st_; }
     const GridDev& grid() const { return g_; }
     Partials partials() const { return part_; }
@@ -118,6 +142,9 @@ private:
     size_t bytes_ = 0;
     int nodes_per_chunk_ = 0;
     uint64_t launches_ = 0;
+    int persist_blocks_ = 0;
+    GridBarrier* gbar_ = nullptr;
+    double* ppart_ = nullptr;
 };
 
 // Blocks of the slab passes (reduction partials needed per pass).

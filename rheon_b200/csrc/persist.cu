@@ -1,0 +1,446 @@
+// Persistent Jacobi-PCG: one cooperative kernel runs a whole chunk of
+// iterations of PressureWorkspace::solve_loaded (src/pressure.rs:577-740)
+// with the "jacobi-pcg-v1" preconditioner (:534-575), true-residual checks and
+// restarts included, without returning to the host or the graph between
+// passes.
+//
+// Each block owns a fixed, strided set of 32 x 8 x 8 bricks (one block per SM,
+// 512 threads, two threads per cell column). Every phase streams the block's
+// bricks through a two-stage TMA pipeline (the next brick's slab is in flight
+// while the current one is computed), reduces its dot products per block,
+// publishes them, and meets the other blocks at a grid barrier. Every block
+// then folds all partials in the same fixed order and takes the same
+// decision on its own shared-memory copy of the solver state, so the blocks
+// stay in lock-step without a second barrier; block 0 writes the state back
+// at the end of the launch.
+//
+// Phases per iteration (bytes per cell, f64):
+//   1  d <- z + beta d (or z after a restart), q = K d, d.q      read z, d; write d    24
+//   2  p += alpha d, r -= alpha K d, z = r/D, r.r, r.z           read d, p, r; write p, r, z  48
+// and on a candidate:
+//   3  t = b - K p, |t|_2, max|t| -> accept / stop / restart     read p, b; write t    24
+//   4  (restart) r = t, z = r/D, r.z                             read t; write r, z    24
+//
+// Liveness: the kernel is launched cooperatively, so all blocks are
+// co-resident. Every wait is bounded: a TMA wait or a grid barrier that runs
+// out marks the solve as failed (execution error) and raises an abort word
+// that ends every other block's barrier wait, and the kernel returns.
+#include "pcg.hpp"
+#include "slab.cuh"
+#include "solve_state.cuh"
+
+namespace rb200 {
+
+namespace {
+
+constexpr int PZ = 2;                        // threads per cell column
+constexpr int PT = TX * TY * PZ;             // threads per block
+constexpr int PZC = 8;                       // brick depth (the slab maps' box depth)
+constexpr int QPT = PZC / PZ;                // cells per thread per brick
+using PS = Slab<PZC>;
+constexpr int BOX = TX * TY * PZC;           // cells of one brick (no halo)
+constexpr unsigned BOX_BYTES = unsigned(BOX) * 8u;
+// A stage holds two slabs (phase 1), or one slab and two bricks (phase 2).
+constexpr int STAGE = (2 * PS::SIZE > PS::SIZE + 2 * BOX) ? 2 * PS::SIZE : PS::SIZE + 2 * BOX;
+constexpr size_t kPersistSmem = 2 * size_t(STAGE) * sizeof(double);
+constexpr unsigned kBarrierSpins = 1u << 24;
+constexpr int PSTRIDE = 4;                   // doubles per block per partial set
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+// Order this thread's generic-proxy memory accesses with its (or, through a
+// barrier, its block's) later TMA (async-proxy) accesses.
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+struct PersistArgs {
+    GridDev g;
+    SolveState* st;
+    const double* b;
+    double* p;
+    double* r;
+    double* z;
+    double* d0;
+    double* d1;
+    double* part;      // [2][blocks][PSTRIDE]
+    GridBarrier* bar;
+    rb200_trace* trace;
+    int budget;        // iterations this launch may start
+};
+
+// Per-block context.
+struct Ctx {
+    int nbx, nby, nbricks;
+    int tid, tx, ty, tz;
+    unsigned par[2];   // mbarrier phase parity per stage (uniform)
+    unsigned gen;      // barrier generation (thread 0)
+    int set;           // partial set parity
+};
+
+__device__ __forceinline__ void brick_origin(const Ctx& c, int b, int& x0, int& y0, int& k0) {
+    const int bx = b % c.nbx;
+    const int rest = b / c.nbx;
+    x0 = bx * TX;
+    y0 = (rest % c.nby) * TY;
+    k0 = (rest / c.nby) * PZC;
+}
+
+// Grid barrier: arrive (release), wait for the generation to move (acquire).
+// Returns false, with the abort word raised, when the wait runs out or
+// another block aborted.
+__device__ bool grid_barrier(Ctx& c, GridBarrier* gb) {
+    __shared__ int s_ok;
+    fence_proxy_async_global();
+    __syncthreads();
+    if (c.tid == 0) {
+        int ok = 1;
+        __threadfence();
+        const unsigned arrived = atomicAdd(&gb->count, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(&gb->count, 0u);
+            __threadfence();
+            st_release_gpu(&gb->gen, c.gen + 1u);
+        } else {
+            unsigned n = 0;
+            while (ld_acquire_gpu(&gb->gen) == c.gen) {
+                if (*(volatile unsigned*)&gb->abort != 0u || ++n > kBarrierSpins) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        fence_proxy_async_global();
+        c.gen += 1u;
+        if (!ok) atomicExch(&gb->abort, 1u);
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Publish this block's K sums and M maxima, meet the other blocks, fold all
+// blocks' partials in block order. The fold is identical in every block.
+// Result valid in thread 0.
+template <int K, int M>
+__device__ bool reduce_grid(Ctx& c, const PersistArgs& A, dd (&sums)[K > 0 ? K : 1], double (&maxs)[M > 0 ? M : 1]) {
+    __shared__ BlockReduce<K, M> red;
+    block_reduce<K, M>(red, sums, maxs);
+    double* base = A.part + size_t(c.set) * gridDim.x * PSTRIDE;
+    if (c.tid == 0) {
+        double* slot = base + size_t(blockIdx.x) * PSTRIDE;
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            slot[2 * q] = sums[q].hi;
+            slot[2 * q + 1] = sums[q].lo;
+        }
+#pragma unroll
+        for (int q = 0; q < M; ++q) slot[2 * K + q] = maxs[q];
+    }
+    c.set ^= 1;
+    if (!grid_barrier(c, A.bar)) return false;
+#pragma unroll
+    for (int q = 0; q < K; ++q) sums[q] = dd{0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < M; ++q) maxs[q] = 0.0;
+    for (int b = c.tid; b < int(gridDim.x); b += PT) {
+        const double* slot = base + size_t(b) * PSTRIDE;
+#pragma unroll
+        for (int q = 0; q < K; ++q) sums[q] = dd_add(sums[q], dd{__ldcg(slot + 2 * q), __ldcg(slot + 2 * q + 1)});
+#pragma unroll
+        for (int q = 0; q < M; ++q) maxs[q] = fmax(maxs[q], __ldcg(slot + 2 * K + q));
+    }
+    block_reduce<K, M>(red, sums, maxs);
+    return true;
+}
+
+// Stream the block's bricks through the two-stage pipeline. issue(b, s) runs
+// on thread 0 and arms stage s's mbarrier; body(b, s) runs on all threads.
+template <class Issue, class Body>
+__device__ bool for_bricks(Ctx& c, uint64_t* bars, Issue issue, Body body) {
+    const int first = blockIdx.x, stride = gridDim.x;
+    if (first >= c.nbricks) return true;
+    if (c.tid == 0) issue(first, 0);
+    int n = 0;
+    for (int b = first; b < c.nbricks; b += stride, ++n) {
+        const int s = n & 1;
+        const int nb = b + stride;
+        const bool next = nb < c.nbricks;
+        if (next && c.tid == 0) issue(nb, s ^ 1);
+        bool ok = mbar_wait_bounded(&bars[s], c.par[s]);
+        c.par[s] ^= 1u;
+        ok = __syncthreads_and(ok) != 0;
+        if (!ok) {
+            // Let the copies in flight land before the block gives up.
+            if (c.tid == 0) {
+                mbar_wait_bounded(&bars[s], c.par[s] ^ 1u);
+                if (next) mbar_wait_bounded(&bars[s ^ 1], c.par[s ^ 1]);
+            }
+            __syncthreads();
+            return false;
+        }
+        body(b, s);
+        fence_proxy_async_smem();  // the stage is refilled by TMA next
+        __syncthreads();
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_constant__ PersistArgs A,
+                                                             const __grid_constant__ TmaMaps maps) {
+    extern __shared__ __align__(128) double smem[];
+    __shared__ SolveState sst;
+    __shared__ __align__(8) uint64_t bars[2];
+    const GridDev& g = A.g;
+    Ctx c;
+    c.tx = threadIdx.x;
+    c.ty = threadIdx.y;
+    c.tz = threadIdx.z;
+    c.tid = c.tx + TX * (c.ty + TY * c.tz);
+    c.nbx = (g.n[0] + TX - 1) / TX;
+    c.nby = (g.n[1] + TY - 1) / TY;
+    c.nbricks = c.nbx * c.nby * ((g.n[2] + PZC - 1) / PZC);
+    c.par[0] = c.par[1] = 0u;
+    c.gen = 0u;
+    c.set = 0;
+    if (c.tid == 0) {
+        sst = *A.st;
+        c.gen = ld_acquire_gpu(&A.bar->gen);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    rb200_trace* trace = blockIdx.x == 0 ? A.trace : nullptr;
+    const int plane = g.n[0] * g.n[1];
+    const int qb = c.tz * QPT;
+    bool ok = true;
+    int iters = 0;
+    for (;;) {
+        const int flags = sst.flags;
+        if (flags & F_DONE) break;
+        if (flags & F_NEED_TRUE) {
+            // ---------------------------------------------- phase 3: true residual
+            double* spare = sst.dsel ? A.d0 : A.d1;
+            Neu acc;
+            double mx = 0.0;
+            ok = for_bricks(
+                c, bars,
+                [&](int b, int s) {
+                    int x0, y0, k0;
+                    brick_origin(c, b, x0, y0, k0);
+                    mbar_expect_tx(&bars[s], PS::BYTES);
+                    tma_load_slab(smem + s * STAGE, &maps.p, x0 - 2, y0 - 1, k0 - 1, &bars[s]);
+                },
+                [&](int b, int s) {
+                    int x0, y0, k0;
+                    brick_origin(c, b, x0, y0, k0);
+                    const double* sp = smem + s * STAGE;
+                    const int i = x0 + c.tx, j = y0 + c.ty;
+                    if (i >= g.n[0] || j >= g.n[1]) return;
+                    const int kend = min(PZC, g.n[2] - k0);
+                    for (int q = qb; q < qb + QPT && q < kend; ++q) {
+                        const int cc = cell_idx(g, i, j, k0 + q);
+                        Neigh v = slab_neigh<PZC>(sp, PS::own(c.tx, c.ty, q));
+                        const double t = __ldcg(A.b + cc) - apply_row(g, i, j, k0 + q, v);
+                        spare[cc] = t;
+                        acc.add(t * t);
+                        mx = fmax(mx, fabs(t));
+                    }
+                });
+            if (!ok) break;
+            dd sums[1] = {acc.as_dd()};
+            double maxs[1] = {mx};
+            if (!(ok = reduce_grid<1, 1>(c, A, sums, maxs))) break;
+            if (c.tid == 0) decide_true(&sst, trace, dd_value(sums[0]), maxs[0], flags, g.volume);
+            __syncthreads();
+            continue;
+        }
+        if (flags & F_NEED_REPLACE) {
+            // ---------------------------------------------- phase 4: restart
+            const double* spare = sst.dsel ? A.d0 : A.d1;
+            Neu acc;
+            for (int b = blockIdx.x; b < c.nbricks; b += gridDim.x) {
+                int x0, y0, k0;
+                brick_origin(c, b, x0, y0, k0);
+                const int i = x0 + c.tx, j = y0 + c.ty;
+                if (i >= g.n[0] || j >= g.n[1]) continue;
+                const int kend = min(PZC, g.n[2] - k0);
+                for (int q = qb; q < qb + QPT && q < kend; ++q) {
+                    const int cc = cell_idx(g, i, j, k0 + q);
+                    const double rc = cc == 0 ? 0.0 : __ldcg(spare + cc);
+                    A.r[cc] = rc;
+                    if (cc == 0) {
+                        A.z[0] = 0.0;
+                        continue;
+                    }
+                    const double zc = rc / diag_at(g, i, j, k0 + q);
+                    A.z[cc] = zc;
+                    acc.add(rc * zc);
+                }
+            }
+            dd sums[1] = {acc.as_dd()};
+            double none[1] = {0.0};
+            if (!(ok = reduce_grid<1, 0>(c, A, sums, none))) break;
+            if (c.tid == 0) decide_rz(&sst, trace, dd_value(sums[0]), MODE_REPLACE);
+            __syncthreads();
+            continue;
+        }
+        if (flags & F_STOP) break;  // stopped without a pending check: nothing to do
+        if (iters >= A.budget) break;
+
+        // -------------------------------------------------- phase 1: direction + K d
+        {
+            const bool fresh = (flags & F_REPLACED) != 0;
+            const double beta = sst.beta;
+            const int dsel = sst.dsel;
+            double* __restrict__ dst = dsel ? A.d0 : A.d1;
+            const CUtensorMap* dmap = dsel ? &maps.d1 : &maps.d0;
+            Neu acc;
+            ok = for_bricks(
+                c, bars,
+                [&](int b, int s) {
+                    int x0, y0, k0;
+                    brick_origin(c, b, x0, y0, k0);
+                    double* sz = smem + s * STAGE;
+                    mbar_expect_tx(&bars[s], (fresh ? 1u : 2u) * PS::BYTES);
+                    tma_load_slab(sz, &maps.z, x0 - 2, y0 - 1, k0 - 1, &bars[s]);
+                    if (!fresh) tma_load_slab(sz + PS::SIZE, dmap, x0 - 2, y0 - 1, k0 - 1, &bars[s]);
+                },
+                [&](int b, int s) {
+                    int x0, y0, k0;
+                    brick_origin(c, b, x0, y0, k0);
+                    double* sz = smem + s * STAGE;
+                    const double* sd = sz + PS::SIZE;
+                    if (!fresh) {
+                        for (int e = c.tid; e < PS::SIZE; e += PT) sz[e] = sz[e] + beta * sd[e];
+                        __syncthreads();
+                    }
+                    const int i = x0 + c.tx, j = y0 + c.ty;
+                    if (i >= g.n[0] || j >= g.n[1]) return;
+                    const int kend = min(PZC, g.n[2] - k0);
+                    int cc = cell_idx(g, i, j, k0 + qb);
+                    for (int q = qb; q < qb + QPT && q < kend; ++q, cc += plane) {
+                        Neigh v = slab_neigh<PZC>(sz, PS::own(c.tx, c.ty, q));
+                        const double qv = cc == 0 ? 0.0 : apply_row(g, i, j, k0 + q, v);
+                        dst[cc] = v.c;
+                        acc.add(v.c * qv);
+                    }
+                });
+            if (!ok) break;
+            dd sums[1] = {acc.as_dd()};
+            double none[1] = {0.0};
+            if (!(ok = reduce_grid<1, 0>(c, A, sums, none))) break;
+            if (c.tid == 0) decide_pass1(&sst, trace, dd_value(sums[0]), flags, dsel);
+            __syncthreads();
+            if (sst.flags & F_DONE) continue;
+        }
+        // -------------------------------------------------- phase 2: update + Jacobi
+        {
+            const int flags2 = sst.flags;
+            const double alpha = sst.alpha;
+            const int dsel = sst.dsel;
+            const CUtensorMap* dmap = dsel ? &maps.d1 : &maps.d0;
+            Neu acc_rr, acc_rz;
+            ok = for_bricks(
+                c, bars,
+                [&](int b, int s) {
+                    int x0, y0, k0;
+                    brick_origin(c, b, x0, y0, k0);
+                    double* sd = smem + s * STAGE;
+                    mbar_expect_tx(&bars[s], PS::BYTES + 2u * BOX_BYTES);
+                    tma_load_slab(sd, dmap, x0 - 2, y0 - 1, k0 - 1, &bars[s]);
+                    tma_load_slab(sd + PS::SIZE, &maps.p_box, x0, y0, k0, &bars[s]);
+                    tma_load_slab(sd + PS::SIZE + BOX, &maps.r_box, x0, y0, k0, &bars[s]);
+                },
+                [&](int b, int s) {
+                    int x0, y0, k0;
+                    brick_origin(c, b, x0, y0, k0);
+                    const double* sd = smem + s * STAGE;
+                    const double* sp = sd + PS::SIZE;
+                    const double* sr = sp + BOX;
+                    const int i = x0 + c.tx, j = y0 + c.ty;
+                    if (i >= g.n[0] || j >= g.n[1]) return;
+                    const int kend = min(PZC, g.n[2] - k0);
+                    int cc = cell_idx(g, i, j, k0 + qb);
+                    for (int q = qb; q < qb + QPT && q < kend; ++q, cc += plane) {
+                        if (cc == 0) continue;  // gauge row: p[0], r[0] stay 0
+                        Neigh v = slab_neigh<PZC>(sd, PS::own(c.tx, c.ty, q));
+                        const int k = k0 + q;
+                        const double qv = apply_row(g, i, j, k, v);
+                        const int bi = c.tx + TX * (c.ty + TY * q);
+                        A.p[cc] = sp[bi] + alpha * v.c;
+                        const double rc = sr[bi] - alpha * qv;
+                        A.r[cc] = rc;
+                        acc_rr.add(rc * rc);
+                        const double zc = rc / diag_at(g, i, j, k);
+                        A.z[cc] = zc;
+                        acc_rz.add(rc * zc);
+                    }
+                });
+            if (!ok) break;
+            dd sums[2] = {acc_rr.as_dd(), acc_rz.as_dd()};
+            double none[1] = {0.0};
+            if (!(ok = reduce_grid<2, 0>(c, A, sums, none))) break;
+            if (c.tid == 0) decide_pass2(&sst, trace, dd_value(sums[0]), dd_value(sums[1]), flags2, true);
+            __syncthreads();
+            ++iters;
+        }
+    }
+    if (!ok) {
+        if (c.tid == 0) {
+            atomicExch(&A.bar->abort, 1u);
+            A.st->status = RB200_EXECUTION;
+            A.st->flags = A.st->flags | F_DONE | F_STOP;
+        }
+        return;
+    }
+    if (blockIdx.x == 0 && c.tid == 0) *A.st = sst;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ host side
+int persistent_setup(const GridDev& g, int* blocks) {
+    *blocks = 0;
+    RB200_CUDA(cudaFuncSetAttribute(k_jacobi_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(kPersistSmem)));
+    int dev = 0, sms = 0, coop = 0, per_sm = 0;
+    RB200_CUDA(cudaGetDevice(&dev));
+    RB200_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    RB200_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    RB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi_persistent, PT, kPersistSmem));
+    if (!coop || per_sm < 1) return RB200_OK;
+    const int nbricks = ((g.n[0] + TX - 1) / TX) * ((g.n[1] + TY - 1) / TY) * ((g.n[2] + PZC - 1) / PZC);
+    const int cap = sms * per_sm;
+    *blocks = nbricks < cap ? nbricks : cap;
+    return RB200_OK;
+}
+
+size_t persistent_partial_doubles(int blocks) { return 2 * size_t(blocks) * PSTRIDE; }
+
+cudaError_t launch_persistent(const GridDev& g, SolveState* st, const double* b, double* p, double* r, double* z,
+                              double* d0, double* d1, double* part, GridBarrier* bar, rb200_trace* trace,
+                              const TmaMaps& maps, int blocks, int budget, cudaStream_t s) {
+    PersistArgs A{g, st, b, p, r, z, d0, d1, part, bar, trace, budget};
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(unsigned(blocks), 1, 1);
+    cfg.blockDim = dim3(TX, TY, PZ);
+    cfg.dynamicSmemBytes = kPersistSmem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_jacobi_persistent, A, maps);
+}
+
+}  // namespace rb200

@@ -101,4 +101,109 @@ __device__ __forceinline__ void decide_flexible(SolveState* st, rb200_trace* tra
     st->rz = rz;
 }
 
+// Pass 1 (src/pressure.rs:657-668): the curvature d.q of the new direction
+// gives alpha = r.z / d.q, or a breakdown. `flags` and `dsel` are the values
+// the pass started with; the direction buffers swap roles.
+__device__ __forceinline__ void decide_pass1(SolveState* st, rb200_trace* trace, double curvature, int flags,
+                                             int dsel) {
+    st->curvature = curvature;
+    st->dsel = dsel ^ 1;
+    if (flags & F_PROFILE) return;
+    const double rz = st->rz;
+    const int it = st->it + 1;
+    const int fl = flags & ~F_REPLACED;
+    if (trace) {
+        trace[it - 1].curvature = curvature;
+        trace[it - 1].replaced = 0;
+        trace[it - 1].checked = 0;
+    }
+    if (!isfinite(curvature) || curvature <= 0.0 || !isfinite(rz) || rz <= 0.0) {
+        breakdown(st, it, fl);
+        return;
+    }
+    const double alpha = rz / curvature;
+    if (!isfinite(alpha)) {
+        breakdown(st, it, fl);
+        return;
+    }
+    if (trace) trace[it - 1].alpha = alpha;
+    st->alpha = alpha;
+    st->flags = fl;
+}
+
+// Pass 2 (src/pressure.rs:669-685): the iteration is complete; the recursive
+// norm decides whether the true residual is checked (a candidate, or the last
+// allowed iteration). With the Jacobi preconditioner r.z is already known
+// (`has_rz`) and beta follows; the other preconditioners only mark the
+// candidate and decide after forming z.
+__device__ __forceinline__ void decide_pass2(SolveState* st, rb200_trace* trace, double rr, double rz, int flags,
+                                             bool has_rz) {
+    if (flags & F_PROFILE) {
+        st->recursive_l2 = rr;
+        st->rz_next = rz;
+        return;
+    }
+    const int it = st->it + 1;
+    st->it = it;
+    const double recursive_l2 = sqrt(rr);
+    st->recursive_l2 = recursive_l2;
+    if (trace) trace[it - 1].recursive_l2 = recursive_l2;
+    const bool candidate = recursive_l2 <= st->threshold || it == st->max_it;
+    if (has_rz) {
+        if (candidate) {
+            st->rz_next = rz;
+            st->flags = flags | F_STOP | F_NEED_TRUE;
+        } else {
+            decide_rz(st, trace, rz, MODE_ITER);
+        }
+    } else if (candidate) {
+        st->flags = flags | F_CANDIDATE;
+    }
+}
+
+// True-residual check (true_report, src/pressure.rs:432-456, and the
+// acceptance/restart decisions of solve_loaded, :686-715): accept, stop at the
+// iteration limit, restart from the true residual, or keep the recurrence.
+__device__ __forceinline__ void decide_true(SolveState* st, rb200_trace* trace, double squared, double maximum,
+                                            int flags, double volume) {
+    const int it = st->it;
+    const double div = maximum * st->dt / volume;
+    if (trace && it >= 1) trace[it - 1].checked = 1;
+    if (!isfinite(squared) || !isfinite(div)) {
+        breakdown(st, it, flags);
+        return;
+    }
+    const double l2 = sqrt(squared);
+    st->true_l2 = l2;
+    st->true_max = maximum;
+    st->true_div = div;
+    if (l2 <= st->threshold && div <= st->divergence_limit) {
+        finish(st, RB200_OK, flags);
+        return;
+    }
+    const bool replaced = l2 > st->threshold;
+    if (it == st->max_it) {
+        finish(st, RB200_ITERATION_LIMIT, flags);
+        return;
+    }
+    if (replaced) {
+        st->flags = (flags & ~F_NEED_TRUE) | F_NEED_REPLACE;
+        return;
+    }
+    // Keep the recurrence: precondition the recursive residual.
+    const double rz = st->rz_next;
+    if (!isfinite(rz) || rz <= 0.0) {
+        breakdown(st, it, flags);
+        return;
+    }
+    const double beta = st->flexible ? st->beta_next : rz / st->rz;
+    if (trace) {
+        trace[it - 1].rz = rz;
+        trace[it - 1].beta = beta;
+    }
+    st->beta = beta;
+    st->rz = rz;
+    st->flags = flags & ~(F_STOP | F_NEED_TRUE);
+}
+
 }  // namespace rb200

@@ -292,11 +292,14 @@ def test_pcg_per_iteration_parity(counts, method):
         assert relerr(ws.pressure(), refk.pressure) <= 1e-12
 
 
-def test_jacobi_converged_solve_matches_oracle_iterations_and_report():
-    g = R.GridGeometry([24, 20, 16], [0.1, 0.12, 0.15])
+# [64, 40, 24] runs the persistent Jacobi-PCG kernel (true-residual checks
+# and restarts inside the kernel); [24, 20, 16] the per-pass kernels.
+@pytest.mark.parametrize("counts, rel", [([24, 20, 16], 1e-8), ([64, 40, 24], 1e-8), ([64, 40, 24], 1e-12)])
+def test_jacobi_converged_solve_matches_oracle_iterations_and_report(counts, rel):
+    g = R.GridGeometry(counts, [0.1, 0.12, 0.15])
     rhs = compatible_rhs(g, seed=5)
-    s = S(1e-8, 0.0, 1.7976931348623157e308, 5000)
-    ref = O.solve_rhs(og(g), 1.0, O.JACOBI_PCG_V1, rhs, 0.25, O.settings(1e-8, 0.0, 1.7976931348623157e308, 5000))
+    s = S(rel, 0.0, 1.7976931348623157e308, 5000)
+    ref = O.solve_rhs(og(g), 1.0, O.JACOBI_PCG_V1, rhs, 0.25, O.settings(rel, 0.0, 1.7976931348623157e308, 5000))
     assert ref.status == O.OK
     ws = R.PressureWorkspace(g, 1 << 34)
     rep = ws.solve_rhs(R.PressureOperator(g, 1.0), rhs, 0.25, s)
