@@ -78,7 +78,7 @@ struct PersistArgs {
 struct Ctx {
     int nbx, nby, nbricks;
     int tid, tx, ty, tz;
-    unsigned par[2];   // mbarrier phase parity per stage (uniform)
+    unsigned par;      // mbarrier phase parity of stage s in bit s (uniform)
     unsigned gen;      // barrier generation (thread 0)
     int set;           // partial set parity
 };
@@ -91,10 +91,52 @@ __device__ __forceinline__ void brick_origin(const Ctx& c, int b, int& x0, int& 
     k0 = (rest / c.nby) * PZC;
 }
 
+// One thread's column of a brick: cells (i, j, k0 + qb .. k0 + qb + QPT - 1).
+struct Col {
+    int k0, kend;   // brick origin in z; cells of the brick in z
+    int cc0;        // cell index of the column's first cell
+    int e0;         // slab element of the column's first cell
+    int bi0;        // brick (no halo) element of the column's first cell
+    int mxy;        // neighbour-mask bits of x and y (src/operator.rs:813-822 order)
+    bool own;       // the column lies inside the domain
+};
+
+__device__ __forceinline__ Col column(const GridDev& g, const Ctx& c, int b, int qb) {
+    int x0, y0, k0;
+    brick_origin(c, b, x0, y0, k0);
+    const int i = x0 + c.tx, j = y0 + c.ty;
+    Col col;
+    col.own = i < g.n[0] && j < g.n[1];
+    col.k0 = k0;
+    col.kend = min(PZC, g.n[2] - k0);
+    col.cc0 = i + g.n[0] * (j + g.n[1] * (k0 + qb));
+    col.e0 = PS::own(c.tx, c.ty, qb);
+    col.bi0 = c.tx + TX * (c.ty + TY * qb);
+    col.mxy = int(i > 0) | (int(i + 1 < g.n[0]) << 1) | (int(j > 0) << 2) | (int(j + 1 < g.n[1]) << 3);
+    return col;
+}
+
+// Row of K applied to one cell (apply_full, src/operator.rs:400-416): the
+// terms in the order X lower, X upper, Y lower, Y upper, Z lower, Z upper,
+// with the x/y masks precomputed per column.
+__device__ __forceinline__ double row7(const GridDev& g, int mxy, int k, double cv, double xm, double xp, double ym,
+                                       double yp, double zm, double zp) {
+    double q = 0.0;
+    if (mxy & 1) q += g.weight[0] * (cv - xm);
+    if (mxy & 2) q += g.weight[0] * (cv - xp);
+    if (mxy & 4) q += g.weight[1] * (cv - ym);
+    if (mxy & 8) q += g.weight[1] * (cv - yp);
+    if (k > 0) q += g.weight[2] * (cv - zm);
+    if (k + 1 < g.n[2]) q += g.weight[2] * (cv - zp);
+    return q;
+}
+
+__device__ __forceinline__ int zmask(const GridDev& g, int k) { return (int(k > 0) << 4) | (int(k + 1 < g.n[2]) << 5); }
+
 // Grid barrier: arrive (release), wait for the generation to move (acquire).
 // Returns false, with the abort word raised, when the wait runs out or
 // another block aborted.
-__device__ bool grid_barrier(Ctx& c, GridBarrier* gb) {
+__device__ __forceinline__ bool grid_barrier(Ctx& c, GridBarrier* gb) {
     __shared__ int s_ok;
     fence_proxy_async_global();
     __syncthreads();
@@ -130,7 +172,7 @@ __device__ bool grid_barrier(Ctx& c, GridBarrier* gb) {
 // blocks' partials in block order. The fold is identical in every block.
 // Result valid in thread 0.
 template <int K, int M>
-__device__ bool reduce_grid(Ctx& c, const PersistArgs& A, dd (&sums)[K > 0 ? K : 1], double (&maxs)[M > 0 ? M : 1]) {
+__device__ __forceinline__ bool reduce_grid(Ctx& c, const PersistArgs& A, dd (&sums)[K > 0 ? K : 1], double (&maxs)[M > 0 ? M : 1]) {
     __shared__ BlockReduce<K, M> red;
     block_reduce<K, M>(red, sums, maxs);
     double* base = A.part + size_t(c.set) * gridDim.x * PSTRIDE;
@@ -164,7 +206,7 @@ __device__ bool reduce_grid(Ctx& c, const PersistArgs& A, dd (&sums)[K > 0 ? K :
 // Stream the block's bricks through the two-stage pipeline. issue(b, s) runs
 // on thread 0 and arms stage s's mbarrier; body(b, s) runs on all threads.
 template <class Issue, class Body>
-__device__ bool for_bricks(Ctx& c, uint64_t* bars, Issue issue, Body body) {
+__device__ __forceinline__ bool for_bricks(Ctx& c, uint64_t* bars, Issue issue, Body body) {
     const int first = blockIdx.x, stride = gridDim.x;
     if (first >= c.nbricks) return true;
     if (c.tid == 0) issue(first, 0);
@@ -174,14 +216,14 @@ __device__ bool for_bricks(Ctx& c, uint64_t* bars, Issue issue, Body body) {
         const int nb = b + stride;
         const bool next = nb < c.nbricks;
         if (next && c.tid == 0) issue(nb, s ^ 1);
-        bool ok = mbar_wait_bounded(&bars[s], c.par[s]);
-        c.par[s] ^= 1u;
+        bool ok = mbar_wait_bounded(&bars[s], (c.par >> s) & 1u);
+        c.par ^= 1u << s;
         ok = __syncthreads_and(ok) != 0;
         if (!ok) {
             // Let the copies in flight land before the block gives up.
             if (c.tid == 0) {
-                mbar_wait_bounded(&bars[s], c.par[s] ^ 1u);
-                if (next) mbar_wait_bounded(&bars[s ^ 1], c.par[s ^ 1]);
+                mbar_wait_bounded(&bars[s], ((c.par >> s) & 1u) ^ 1u);
+                if (next) mbar_wait_bounded(&bars[s ^ 1], (c.par >> (s ^ 1)) & 1u);
             }
             __syncthreads();
             return false;
@@ -198,6 +240,7 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
     extern __shared__ __align__(128) double smem[];
     __shared__ SolveState sst;
     __shared__ __align__(8) uint64_t bars[2];
+    __shared__ double sdiag[64];
     const GridDev& g = A.g;
     Ctx c;
     c.tx = threadIdx.x;
@@ -207,9 +250,10 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
     c.nbx = (g.n[0] + TX - 1) / TX;
     c.nby = (g.n[1] + TY - 1) / TY;
     c.nbricks = c.nbx * c.nby * ((g.n[2] + PZC - 1) / PZC);
-    c.par[0] = c.par[1] = 0u;
+    c.par = 0u;
     c.gen = 0u;
     c.set = 0;
+    if (c.tid < 64) sdiag[c.tid] = g.diag[c.tid];
     if (c.tid == 0) {
         sst = *A.st;
         c.gen = ld_acquire_gpu(&A.bar->gen);
@@ -240,16 +284,20 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
                     tma_load_slab(smem + s * STAGE, &maps.p, x0 - 2, y0 - 1, k0 - 1, &bars[s]);
                 },
                 [&](int b, int s) {
-                    int x0, y0, k0;
-                    brick_origin(c, b, x0, y0, k0);
                     const double* sp = smem + s * STAGE;
-                    const int i = x0 + c.tx, j = y0 + c.ty;
-                    if (i >= g.n[0] || j >= g.n[1]) return;
-                    const int kend = min(PZC, g.n[2] - k0);
-                    for (int q = qb; q < qb + QPT && q < kend; ++q) {
-                        const int cc = cell_idx(g, i, j, k0 + q);
-                        Neigh v = slab_neigh<PZC>(sp, PS::own(c.tx, c.ty, q));
-                        const double t = __ldcg(A.b + cc) - apply_row(g, i, j, k0 + q, v);
+                    const Col col = column(g, c, b, qb);
+                    if (!col.own) return;
+                    double v[QPT + 2];
+#pragma unroll
+                    for (int u = 0; u < QPT + 2; ++u) v[u] = sp[col.e0 + (u - 1) * PS::PLANE];
+#pragma unroll
+                    for (int u = 0; u < QPT; ++u) {
+                        if (qb + u >= col.kend) break;
+                        const int e = col.e0 + u * PS::PLANE;
+                        const int cc = col.cc0 + u * plane;
+                        const double kp = row7(g, col.mxy, col.k0 + qb + u, v[u + 1], sp[e - 1], sp[e + 1],
+                                               sp[e - PS::SX], sp[e + PS::SX], v[u], v[u + 2]);
+                        const double t = __ldcg(A.b + cc) - kp;
                         spare[cc] = t;
                         acc.add(t * t);
                         mx = fmax(mx, fabs(t));
@@ -268,20 +316,19 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
             const double* spare = sst.dsel ? A.d0 : A.d1;
             Neu acc;
             for (int b = blockIdx.x; b < c.nbricks; b += gridDim.x) {
-                int x0, y0, k0;
-                brick_origin(c, b, x0, y0, k0);
-                const int i = x0 + c.tx, j = y0 + c.ty;
-                if (i >= g.n[0] || j >= g.n[1]) continue;
-                const int kend = min(PZC, g.n[2] - k0);
-                for (int q = qb; q < qb + QPT && q < kend; ++q) {
-                    const int cc = cell_idx(g, i, j, k0 + q);
+                const Col col = column(g, c, b, qb);
+                if (!col.own) continue;
+#pragma unroll
+                for (int u = 0; u < QPT; ++u) {
+                    if (qb + u >= col.kend) break;
+                    const int cc = col.cc0 + u * plane;
                     const double rc = cc == 0 ? 0.0 : __ldcg(spare + cc);
                     A.r[cc] = rc;
                     if (cc == 0) {
                         A.z[0] = 0.0;
                         continue;
                     }
-                    const double zc = rc / diag_at(g, i, j, k0 + q);
+                    const double zc = rc / sdiag[col.mxy | zmask(g, col.k0 + qb + u)];
                     A.z[cc] = zc;
                     acc.add(rc * zc);
                 }
@@ -315,23 +362,35 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
                     if (!fresh) tma_load_slab(sz + PS::SIZE, dmap, x0 - 2, y0 - 1, k0 - 1, &bars[s]);
                 },
                 [&](int b, int s) {
-                    int x0, y0, k0;
-                    brick_origin(c, b, x0, y0, k0);
                     double* sz = smem + s * STAGE;
-                    const double* sd = sz + PS::SIZE;
                     if (!fresh) {
-                        for (int e = c.tid; e < PS::SIZE; e += PT) sz[e] = sz[e] + beta * sd[e];
+                        double2* z2 = reinterpret_cast<double2*>(sz);
+                        const double2* d2 = reinterpret_cast<const double2*>(sz + PS::SIZE);
+                        for (int e = c.tid; e < PS::SIZE / 2; e += PT) {
+                            double2 a = z2[e];
+                            const double2 o = d2[e];
+                            a.x = a.x + beta * o.x;
+                            a.y = a.y + beta * o.y;
+                            z2[e] = a;
+                        }
                         __syncthreads();
                     }
-                    const int i = x0 + c.tx, j = y0 + c.ty;
-                    if (i >= g.n[0] || j >= g.n[1]) return;
-                    const int kend = min(PZC, g.n[2] - k0);
-                    int cc = cell_idx(g, i, j, k0 + qb);
-                    for (int q = qb; q < qb + QPT && q < kend; ++q, cc += plane) {
-                        Neigh v = slab_neigh<PZC>(sz, PS::own(c.tx, c.ty, q));
-                        const double qv = cc == 0 ? 0.0 : apply_row(g, i, j, k0 + q, v);
-                        dst[cc] = v.c;
-                        acc.add(v.c * qv);
+                    const Col col = column(g, c, b, qb);
+                    if (!col.own) return;
+                    double v[QPT + 2];
+#pragma unroll
+                    for (int u = 0; u < QPT + 2; ++u) v[u] = sz[col.e0 + (u - 1) * PS::PLANE];
+#pragma unroll
+                    for (int u = 0; u < QPT; ++u) {
+                        if (qb + u >= col.kend) break;
+                        const int e = col.e0 + u * PS::PLANE;
+                        const int cc = col.cc0 + u * plane;
+                        const double qv =
+                            cc == 0 ? 0.0
+                                    : row7(g, col.mxy, col.k0 + qb + u, v[u + 1], sz[e - 1], sz[e + 1],
+                                           sz[e - PS::SX], sz[e + PS::SX], v[u], v[u + 2]);
+                        dst[cc] = v[u + 1];
+                        acc.add(v[u + 1] * qv);
                     }
                 });
             if (!ok) break;
@@ -361,26 +420,29 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
                     tma_load_slab(sd + PS::SIZE + BOX, &maps.r_box, x0, y0, k0, &bars[s]);
                 },
                 [&](int b, int s) {
-                    int x0, y0, k0;
-                    brick_origin(c, b, x0, y0, k0);
                     const double* sd = smem + s * STAGE;
                     const double* sp = sd + PS::SIZE;
                     const double* sr = sp + BOX;
-                    const int i = x0 + c.tx, j = y0 + c.ty;
-                    if (i >= g.n[0] || j >= g.n[1]) return;
-                    const int kend = min(PZC, g.n[2] - k0);
-                    int cc = cell_idx(g, i, j, k0 + qb);
-                    for (int q = qb; q < qb + QPT && q < kend; ++q, cc += plane) {
+                    const Col col = column(g, c, b, qb);
+                    if (!col.own) return;
+                    double v[QPT + 2];
+#pragma unroll
+                    for (int u = 0; u < QPT + 2; ++u) v[u] = sd[col.e0 + (u - 1) * PS::PLANE];
+#pragma unroll
+                    for (int u = 0; u < QPT; ++u) {
+                        if (qb + u >= col.kend) break;
+                        const int cc = col.cc0 + u * plane;
                         if (cc == 0) continue;  // gauge row: p[0], r[0] stay 0
-                        Neigh v = slab_neigh<PZC>(sd, PS::own(c.tx, c.ty, q));
-                        const int k = k0 + q;
-                        const double qv = apply_row(g, i, j, k, v);
-                        const int bi = c.tx + TX * (c.ty + TY * q);
-                        A.p[cc] = sp[bi] + alpha * v.c;
+                        const int e = col.e0 + u * PS::PLANE;
+                        const int k = col.k0 + qb + u;
+                        const double qv = row7(g, col.mxy, k, v[u + 1], sd[e - 1], sd[e + 1], sd[e - PS::SX],
+                                               sd[e + PS::SX], v[u], v[u + 2]);
+                        const int bi = col.bi0 + u * (TX * TY);
+                        A.p[cc] = sp[bi] + alpha * v[u + 1];
                         const double rc = sr[bi] - alpha * qv;
                         A.r[cc] = rc;
                         acc_rr.add(rc * rc);
-                        const double zc = rc / diag_at(g, i, j, k);
+                        const double zc = rc / sdiag[col.mxy | zmask(g, k)];
                         A.z[cc] = zc;
                         acc_rz.add(rc * zc);
                     }
