@@ -4,27 +4,33 @@
 // restarts included, without returning to the host or the graph between
 // passes.
 //
-// Each block owns a fixed, strided set of 32 x 8 x 8 bricks (one block per SM,
-// 512 threads, two threads per cell column). Every phase streams the block's
-// bricks through a two-stage TMA pipeline (the next brick's slab is in flight
-// while the current one is computed), reduces its dot products per block,
-// publishes them, and meets the other blocks at a grid barrier. Every block
-// then folds all partials in the same fixed order and takes the same
-// decision on its own shared-memory copy of the solver state, so the blocks
-// stay in lock-step without a second barrier; block 0 writes the state back
-// at the end of the launch.
+// Each block (one per SM) owns a fixed, strided set of 32 x 8 x 8 bricks and
+// is warp-specialised: one producer warp streams the bricks' slabs into a
+// three-stage shared-memory ring with TMA (a stage is refilled once the 16
+// consumer warps have released it through its "empty" mbarrier), and the 16
+// consumer warps (512 threads, two threads per cell column, four cells each)
+// compute from the ring without block-wide barriers. At the end of a phase the
+// block reduces its dot products, publishes them and meets the other blocks
+// at a grid barrier; every block then folds all partials in the same fixed
+// order and takes the same decision on its own shared-memory copy of the
+// solver state, so the blocks stay in lock-step without a second barrier.
+// Block 0 writes the state back at the end of the launch.
 //
 // Phases per iteration (bytes per cell, f64):
-//   1  d <- z + beta d (or z after a restart), q = K d, d.q      read z, d; write d    24
+//   1  d <- z + beta d (or z after a restart), q = K d, d.q      read z, d; write d          24
 //   2  p += alpha d, r -= alpha K d, z = r/D, r.r, r.z           read d, p, r; write p, r, z  48
 // and on a candidate:
-//   3  t = b - K p, |t|_2, max|t| -> accept / stop / restart     read p, b; write t    24
-//   4  (restart) r = t, z = r/D, r.z                             read t; write r, z    24
+//   3  t = b - K p, |t|_2, max|t| -> accept / stop / restart     read p, b; write t          24
+//   4  (restart) r = t, z = r/D, r.z                             read t; write r, z          24
+// Phase 1 forms the new direction on the fly from the z and d slabs for
+// every value the stencil reads (the same z + beta*d per element), so the
+// slabs are never written.
 //
 // Liveness: the kernel is launched cooperatively, so all blocks are
-// co-resident. Every wait is bounded: a TMA wait or a grid barrier that runs
-// out marks the solve as failed (execution error) and raises an abort word
-// that ends every other block's barrier wait, and the kernel returns.
+// co-resident. Every wait is bounded: a TMA or ring wait or a grid barrier
+// that runs out marks the solve as failed (execution error) and raises an
+// abort word that ends every other block's barrier wait, and the kernel
+// returns.
 #include "pcg.hpp"
 #include "slab.cuh"
 #include "solve_state.cuh"
@@ -33,16 +39,19 @@ namespace rb200 {
 
 namespace {
 
-constexpr int PZ = 2;                        // threads per cell column
-constexpr int PT = TX * TY * PZ;             // threads per block
+constexpr int PZ = 2;                        // consumer threads per cell column
+constexpr int CONSUMERS = TX * TY * PZ;      // consumer threads (16 warps)
+constexpr int CONSUMER_WARPS = CONSUMERS / 32;
+constexpr int PT = CONSUMERS + 32;           // + one producer warp
 constexpr int PZC = 8;                       // brick depth (the slab maps' box depth)
 constexpr int QPT = PZC / PZ;                // cells per thread per brick
+constexpr int NS = 3;                        // ring stages
 using PS = Slab<PZC>;
 constexpr int BOX = TX * TY * PZC;           // cells of one brick (no halo)
 constexpr unsigned BOX_BYTES = unsigned(BOX) * 8u;
 // A stage holds two slabs (phase 1), or one slab and two bricks (phase 2).
 constexpr int STAGE = (2 * PS::SIZE > PS::SIZE + 2 * BOX) ? 2 * PS::SIZE : PS::SIZE + 2 * BOX;
-constexpr size_t kPersistSmem = 2 * size_t(STAGE) * sizeof(double);
+constexpr size_t kPersistSmem = NS * size_t(STAGE) * sizeof(double);
 constexpr unsigned kBarrierSpins = 1u << 24;
 constexpr int PSTRIDE = 4;                   // doubles per block per partial set
 
@@ -54,10 +63,12 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
 __device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
-// Order this thread's generic-proxy memory accesses with its (or, through a
+// Order this thread's generic-proxy global accesses with its (or, through a
 // barrier, its block's) later TMA (async-proxy) accesses.
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
 
 struct PersistArgs {
     GridDev g;
@@ -76,9 +87,10 @@ struct PersistArgs {
 
 // Per-block context.
 struct Ctx {
-    int nbx, nby, nbricks;
-    int tid, tx, ty, tz;
-    unsigned par;      // mbarrier phase parity of stage s in bit s (uniform)
+    int nbx, nby, nbricks, mine;  // bricks along x, y; in total; of this block
+    int tid, lane, tx, ty, tz;
+    bool producer;
+    unsigned ring;     // ring slots used so far (same count in every thread)
     unsigned gen;      // barrier generation (thread 0)
     int set;           // partial set parity
 };
@@ -91,7 +103,7 @@ __device__ __forceinline__ void brick_origin(const Ctx& c, int b, int& x0, int& 
     k0 = (rest / c.nby) * PZC;
 }
 
-// One thread's column of a brick: cells (i, j, k0 + qb .. k0 + qb + QPT - 1).
+// One consumer thread's column of a brick: cells (i, j, k0 + qb .. + QPT - 1).
 struct Col {
     int k0, kend;   // brick origin in z; cells of the brick in z
     int cc0;        // cell index of the column's first cell
@@ -133,6 +145,13 @@ __device__ __forceinline__ double row7(const GridDev& g, int mxy, int k, double 
 
 __device__ __forceinline__ int zmask(const GridDev& g, int k) { return (int(k > 0) << 4) | (int(k + 1 < g.n[2]) << 5); }
 
+// Two interleaved compensated accumulators (even and odd terms), merged in
+// double-double: half the dependent-add chain of one.
+struct Neu2 {
+    Neu a, b;
+    __device__ __forceinline__ dd as_dd() const { return dd_add(a.as_dd(), b.as_dd()); }
+};
+
 // Grid barrier: arrive (release), wait for the generation to move (acquire).
 // Returns false, with the abort word raised, when the wait runs out or
 // another block aborted.
@@ -170,10 +189,13 @@ __device__ __forceinline__ bool grid_barrier(Ctx& c, GridBarrier* gb) {
 
 // Publish this block's K sums and M maxima, meet the other blocks, fold all
 // blocks' partials in block order. The fold is identical in every block.
-// Result valid in thread 0.
+// `ok` is this thread's pipeline outcome; a failure anywhere in the block
+// fails the block before it arrives. Result valid in thread 0.
 template <int K, int M>
-__device__ __forceinline__ bool reduce_grid(Ctx& c, const PersistArgs& A, dd (&sums)[K > 0 ? K : 1], double (&maxs)[M > 0 ? M : 1]) {
+__device__ __forceinline__ bool reduce_grid(Ctx& c, const PersistArgs& A, bool ok, dd (&sums)[K > 0 ? K : 1],
+                                            double (&maxs)[M > 0 ? M : 1]) {
     __shared__ BlockReduce<K, M> red;
+    if (!__syncthreads_and(ok)) return false;
     block_reduce<K, M>(red, sums, maxs);
     double* base = A.part + size_t(c.set) * gridDim.x * PSTRIDE;
     if (c.tid == 0) {
@@ -203,62 +225,71 @@ __device__ __forceinline__ bool reduce_grid(Ctx& c, const PersistArgs& A, dd (&s
     return true;
 }
 
-// Stream the block's bricks through the two-stage pipeline. issue(b, s) runs
-// on thread 0 and arms stage s's mbarrier; body(b, s) runs on all threads.
+// Stream the block's bricks through the ring. The producer's lane 0 waits for
+// a free slot and runs issue(b, slot) (which arms full[slot] and starts the
+// copies); every consumer thread waits for the slot's data, runs
+// body(b, slot) and its warp releases the slot. Returns this thread's outcome.
 template <class Issue, class Body>
-__device__ __forceinline__ bool for_bricks(Ctx& c, uint64_t* bars, Issue issue, Body body) {
-    const int first = blockIdx.x, stride = gridDim.x;
-    if (first >= c.nbricks) return true;
-    if (c.tid == 0) issue(first, 0);
-    int n = 0;
-    for (int b = first; b < c.nbricks; b += stride, ++n) {
-        const int s = n & 1;
-        const int nb = b + stride;
-        const bool next = nb < c.nbricks;
-        if (next && c.tid == 0) issue(nb, s ^ 1);
-        bool ok = mbar_wait_bounded(&bars[s], (c.par >> s) & 1u);
-        c.par ^= 1u << s;
-        ok = __syncthreads_and(ok) != 0;
-        if (!ok) {
-            // Let the copies in flight land before the block gives up.
-            if (c.tid == 0) {
-                mbar_wait_bounded(&bars[s], ((c.par >> s) & 1u) ^ 1u);
-                if (next) mbar_wait_bounded(&bars[s ^ 1], (c.par >> (s ^ 1)) & 1u);
+__device__ __forceinline__ bool run_bricks(Ctx& c, uint64_t* full, uint64_t* empty, Issue issue, Body body) {
+    bool ok = true;
+    unsigned slot_count = c.ring;
+    if (c.producer) {
+        if (c.lane == 0) {
+            for (int b = blockIdx.x; b < c.nbricks; b += gridDim.x, ++slot_count) {
+                const unsigned slot = slot_count % NS, phase = (slot_count / NS) & 1u;
+                if (!mbar_wait_bounded(&empty[slot], phase ^ 1u)) {
+                    ok = false;
+                    break;
+                }
+                issue(b, int(slot));
             }
-            __syncthreads();
-            return false;
         }
-        body(b, s);
-        fence_proxy_async_smem();  // the stage is refilled by TMA next
-        __syncthreads();
+    } else {
+        for (int b = blockIdx.x; b < c.nbricks; b += gridDim.x, ++slot_count) {
+            const unsigned slot = slot_count % NS, phase = (slot_count / NS) & 1u;
+            if (!mbar_wait_bounded(&full[slot], phase)) {
+                ok = false;
+                break;
+            }
+            body(b, int(slot));
+            __syncwarp();
+            if (c.lane == 0) mbar_arrive(&empty[slot]);
+        }
     }
-    return true;
+    c.ring += unsigned(c.mine);
+    return ok;
 }
 
 __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_constant__ PersistArgs A,
                                                              const __grid_constant__ TmaMaps maps) {
     extern __shared__ __align__(128) double smem[];
     __shared__ SolveState sst;
-    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ __align__(8) uint64_t full[NS];
+    __shared__ __align__(8) uint64_t empty[NS];
     __shared__ double sdiag[64];
     const GridDev& g = A.g;
     Ctx c;
-    c.tx = threadIdx.x;
-    c.ty = threadIdx.y;
-    c.tz = threadIdx.z;
-    c.tid = c.tx + TX * (c.ty + TY * c.tz);
+    c.tid = threadIdx.x;
+    c.lane = c.tid & 31;
+    c.producer = c.tid >= CONSUMERS;
+    c.tx = c.tid & 31;
+    c.ty = (c.tid >> 5) & (TY - 1);
+    c.tz = (c.tid >> 8) & (PZ - 1);
     c.nbx = (g.n[0] + TX - 1) / TX;
     c.nby = (g.n[1] + TY - 1) / TY;
     c.nbricks = c.nbx * c.nby * ((g.n[2] + PZC - 1) / PZC);
-    c.par = 0u;
+    c.mine = c.nbricks > int(blockIdx.x) ? (c.nbricks - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x) : 0;
+    c.ring = 0u;
     c.gen = 0u;
     c.set = 0;
     if (c.tid < 64) sdiag[c.tid] = g.diag[c.tid];
     if (c.tid == 0) {
         sst = *A.st;
         c.gen = ld_acquire_gpu(&A.bar->gen);
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], CONSUMER_WARPS);
+        }
         fence_mbar_init();
     }
     __syncthreads();
@@ -273,15 +304,15 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
         if (flags & F_NEED_TRUE) {
             // ---------------------------------------------- phase 3: true residual
             double* spare = sst.dsel ? A.d0 : A.d1;
-            Neu acc;
+            Neu2 acc;
             double mx = 0.0;
-            ok = for_bricks(
-                c, bars,
+            const bool mine_ok = run_bricks(
+                c, full, empty,
                 [&](int b, int s) {
                     int x0, y0, k0;
                     brick_origin(c, b, x0, y0, k0);
-                    mbar_expect_tx(&bars[s], PS::BYTES);
-                    tma_load_slab(smem + s * STAGE, &maps.p, x0 - 2, y0 - 1, k0 - 1, &bars[s]);
+                    mbar_expect_tx(&full[s], PS::BYTES);
+                    tma_load_slab(smem + s * STAGE, &maps.p, x0 - 2, y0 - 1, k0 - 1, &full[s]);
                 },
                 [&](int b, int s) {
                     const double* sp = smem + s * STAGE;
@@ -299,14 +330,13 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
                                                sp[e - PS::SX], sp[e + PS::SX], v[u], v[u + 2]);
                         const double t = __ldcg(A.b + cc) - kp;
                         spare[cc] = t;
-                        acc.add(t * t);
+                        (u & 1 ? acc.b : acc.a).add(t * t);
                         mx = fmax(mx, fabs(t));
                     }
                 });
-            if (!ok) break;
             dd sums[1] = {acc.as_dd()};
             double maxs[1] = {mx};
-            if (!(ok = reduce_grid<1, 1>(c, A, sums, maxs))) break;
+            if (!(ok = reduce_grid<1, 1>(c, A, mine_ok, sums, maxs))) break;
             if (c.tid == 0) decide_true(&sst, trace, dd_value(sums[0]), maxs[0], flags, g.volume);
             __syncthreads();
             continue;
@@ -314,28 +344,30 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
         if (flags & F_NEED_REPLACE) {
             // ---------------------------------------------- phase 4: restart
             const double* spare = sst.dsel ? A.d0 : A.d1;
-            Neu acc;
-            for (int b = blockIdx.x; b < c.nbricks; b += gridDim.x) {
-                const Col col = column(g, c, b, qb);
-                if (!col.own) continue;
+            Neu2 acc;
+            if (!c.producer) {
+                for (int b = blockIdx.x; b < c.nbricks; b += gridDim.x) {
+                    const Col col = column(g, c, b, qb);
+                    if (!col.own) continue;
 #pragma unroll
-                for (int u = 0; u < QPT; ++u) {
-                    if (qb + u >= col.kend) break;
-                    const int cc = col.cc0 + u * plane;
-                    const double rc = cc == 0 ? 0.0 : __ldcg(spare + cc);
-                    A.r[cc] = rc;
-                    if (cc == 0) {
-                        A.z[0] = 0.0;
-                        continue;
+                    for (int u = 0; u < QPT; ++u) {
+                        if (qb + u >= col.kend) break;
+                        const int cc = col.cc0 + u * plane;
+                        const double rc = cc == 0 ? 0.0 : __ldcg(spare + cc);
+                        A.r[cc] = rc;
+                        if (cc == 0) {
+                            A.z[0] = 0.0;
+                            continue;
+                        }
+                        const double zc = rc / sdiag[col.mxy | zmask(g, col.k0 + qb + u)];
+                        A.z[cc] = zc;
+                        (u & 1 ? acc.b : acc.a).add(rc * zc);
                     }
-                    const double zc = rc / sdiag[col.mxy | zmask(g, col.k0 + qb + u)];
-                    A.z[cc] = zc;
-                    acc.add(rc * zc);
                 }
             }
             dd sums[1] = {acc.as_dd()};
             double none[1] = {0.0};
-            if (!(ok = reduce_grid<1, 0>(c, A, sums, none))) break;
+            if (!(ok = reduce_grid<1, 0>(c, A, true, sums, none))) break;
             if (c.tid == 0) decide_rz(&sst, trace, dd_value(sums[0]), MODE_REPLACE);
             __syncthreads();
             continue;
@@ -350,53 +382,42 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
             const int dsel = sst.dsel;
             double* __restrict__ dst = dsel ? A.d0 : A.d1;
             const CUtensorMap* dmap = dsel ? &maps.d1 : &maps.d0;
-            Neu acc;
-            ok = for_bricks(
-                c, bars,
+            Neu2 acc;
+            const bool mine_ok = run_bricks(
+                c, full, empty,
                 [&](int b, int s) {
                     int x0, y0, k0;
                     brick_origin(c, b, x0, y0, k0);
                     double* sz = smem + s * STAGE;
-                    mbar_expect_tx(&bars[s], (fresh ? 1u : 2u) * PS::BYTES);
-                    tma_load_slab(sz, &maps.z, x0 - 2, y0 - 1, k0 - 1, &bars[s]);
-                    if (!fresh) tma_load_slab(sz + PS::SIZE, dmap, x0 - 2, y0 - 1, k0 - 1, &bars[s]);
+                    mbar_expect_tx(&full[s], (fresh ? 1u : 2u) * PS::BYTES);
+                    tma_load_slab(sz, &maps.z, x0 - 2, y0 - 1, k0 - 1, &full[s]);
+                    if (!fresh) tma_load_slab(sz + PS::SIZE, dmap, x0 - 2, y0 - 1, k0 - 1, &full[s]);
                 },
                 [&](int b, int s) {
-                    double* sz = smem + s * STAGE;
-                    if (!fresh) {
-                        double2* z2 = reinterpret_cast<double2*>(sz);
-                        const double2* d2 = reinterpret_cast<const double2*>(sz + PS::SIZE);
-                        for (int e = c.tid; e < PS::SIZE / 2; e += PT) {
-                            double2 a = z2[e];
-                            const double2 o = d2[e];
-                            a.x = a.x + beta * o.x;
-                            a.y = a.y + beta * o.y;
-                            z2[e] = a;
-                        }
-                        __syncthreads();
-                    }
+                    const double* sz = smem + s * STAGE;
+                    const double* sd = sz + PS::SIZE;
+                    // the new direction at slab element e (src/pressure.rs:720-731)
+                    auto dn = [&](int e) { return fresh ? sz[e] : sz[e] + beta * sd[e]; };
                     const Col col = column(g, c, b, qb);
                     if (!col.own) return;
                     double v[QPT + 2];
 #pragma unroll
-                    for (int u = 0; u < QPT + 2; ++u) v[u] = sz[col.e0 + (u - 1) * PS::PLANE];
+                    for (int u = 0; u < QPT + 2; ++u) v[u] = dn(col.e0 + (u - 1) * PS::PLANE);
 #pragma unroll
                     for (int u = 0; u < QPT; ++u) {
                         if (qb + u >= col.kend) break;
                         const int e = col.e0 + u * PS::PLANE;
                         const int cc = col.cc0 + u * plane;
-                        const double qv =
-                            cc == 0 ? 0.0
-                                    : row7(g, col.mxy, col.k0 + qb + u, v[u + 1], sz[e - 1], sz[e + 1],
-                                           sz[e - PS::SX], sz[e + PS::SX], v[u], v[u + 2]);
+                        const double qv = cc == 0 ? 0.0
+                                                  : row7(g, col.mxy, col.k0 + qb + u, v[u + 1], dn(e - 1), dn(e + 1),
+                                                         dn(e - PS::SX), dn(e + PS::SX), v[u], v[u + 2]);
                         dst[cc] = v[u + 1];
-                        acc.add(v[u + 1] * qv);
+                        (u & 1 ? acc.b : acc.a).add(v[u + 1] * qv);
                     }
                 });
-            if (!ok) break;
             dd sums[1] = {acc.as_dd()};
             double none[1] = {0.0};
-            if (!(ok = reduce_grid<1, 0>(c, A, sums, none))) break;
+            if (!(ok = reduce_grid<1, 0>(c, A, mine_ok, sums, none))) break;
             if (c.tid == 0) decide_pass1(&sst, trace, dd_value(sums[0]), flags, dsel);
             __syncthreads();
             if (sst.flags & F_DONE) continue;
@@ -407,17 +428,17 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
             const double alpha = sst.alpha;
             const int dsel = sst.dsel;
             const CUtensorMap* dmap = dsel ? &maps.d1 : &maps.d0;
-            Neu acc_rr, acc_rz;
-            ok = for_bricks(
-                c, bars,
+            Neu2 acc_rr, acc_rz;
+            const bool mine_ok = run_bricks(
+                c, full, empty,
                 [&](int b, int s) {
                     int x0, y0, k0;
                     brick_origin(c, b, x0, y0, k0);
                     double* sd = smem + s * STAGE;
-                    mbar_expect_tx(&bars[s], PS::BYTES + 2u * BOX_BYTES);
-                    tma_load_slab(sd, dmap, x0 - 2, y0 - 1, k0 - 1, &bars[s]);
-                    tma_load_slab(sd + PS::SIZE, &maps.p_box, x0, y0, k0, &bars[s]);
-                    tma_load_slab(sd + PS::SIZE + BOX, &maps.r_box, x0, y0, k0, &bars[s]);
+                    mbar_expect_tx(&full[s], PS::BYTES + 2u * BOX_BYTES);
+                    tma_load_slab(sd, dmap, x0 - 2, y0 - 1, k0 - 1, &full[s]);
+                    tma_load_slab(sd + PS::SIZE, &maps.p_box, x0, y0, k0, &full[s]);
+                    tma_load_slab(sd + PS::SIZE + BOX, &maps.r_box, x0, y0, k0, &full[s]);
                 },
                 [&](int b, int s) {
                     const double* sd = smem + s * STAGE;
@@ -441,16 +462,15 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
                         A.p[cc] = sp[bi] + alpha * v[u + 1];
                         const double rc = sr[bi] - alpha * qv;
                         A.r[cc] = rc;
-                        acc_rr.add(rc * rc);
+                        (u & 1 ? acc_rr.b : acc_rr.a).add(rc * rc);
                         const double zc = rc / sdiag[col.mxy | zmask(g, k)];
                         A.z[cc] = zc;
-                        acc_rz.add(rc * zc);
+                        (u & 1 ? acc_rz.b : acc_rz.a).add(rc * zc);
                     }
                 });
-            if (!ok) break;
             dd sums[2] = {acc_rr.as_dd(), acc_rz.as_dd()};
             double none[1] = {0.0};
-            if (!(ok = reduce_grid<2, 0>(c, A, sums, none))) break;
+            if (!(ok = reduce_grid<2, 0>(c, A, mine_ok, sums, none))) break;
             if (c.tid == 0) decide_pass2(&sst, trace, dd_value(sums[0]), dd_value(sums[1]), flags2, true);
             __syncthreads();
             ++iters;
@@ -494,7 +514,7 @@ cudaError_t launch_persistent(const GridDev& g, SolveState* st, const double* b,
     PersistArgs A{g, st, b, p, r, z, d0, d1, part, bar, trace, budget};
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(unsigned(blocks), 1, 1);
-    cfg.blockDim = dim3(TX, TY, PZ);
+    cfg.blockDim = dim3(PT, 1, 1);
     cfg.dynamicSmemBytes = kPersistSmem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
