@@ -248,6 +248,11 @@ RB200_API int rb200_pressure_solve_static(const rb200_grid* grid, double density
  * These validate like the reference (walls, finiteness) and return its errors. */
 RB200_API int rb200_apply_full_device(const rb200_grid* grid, double density, const double* pressure,
                             double* out, void* stream);
+/* precondition_jacobi (src/pressure.rs:534-575): z = r/D on every row but the
+ * eliminated gauge row (z[0] = 0); *rz receives r.z over rows >= 1
+ * (compensated). Returns RB200_NONFINITE_INPUT for a non-finite r. */
+RB200_API int rb200_precondition_jacobi_device(const rb200_grid* grid, double density, const double* r, double* z,
+                                               size_t len, double* rz, void* stream);
 RB200_API int rb200_build_rhs_f32_device(const rb200_grid* grid, double density, const float* u,
                                const float* v, const float* w, double dt, double* rhs,
                                void* stream);

@@ -226,6 +226,15 @@ class PressureOperator:
         self._check(lib().rb200_apply_full_device(C.byref(self.grid.c()), self.density, _ptr(pressure), _ptr(out),
                                                   _stream_of(pressure)))
 
+    def precondition_jacobi(self, residual, out) -> float:
+        """precondition_jacobi (src/pressure.rs:534-575): out = r/D with
+        out[0] = 0 (eliminated gauge row); returns r.z over rows >= 1."""
+        rz = C.c_double()
+        n = int(residual.numel()) if hasattr(residual, "numel") else int(residual.size)
+        self._check(lib().rb200_precondition_jacobi_device(C.byref(self.grid.c()), self.density, _ptr(residual),
+                                                           _ptr(out), n, C.byref(rz), _stream_of(residual)))
+        return rz.value
+
     def build_rhs(self, velocity: Sequence, dt: float, out):
         u, v, w = velocity
         fn = lib().rb200_build_rhs_f32_device if _is_f32(u) else lib().rb200_build_rhs_f64_device

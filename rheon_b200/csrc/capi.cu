@@ -413,6 +413,32 @@ int rb200_apply_full_device(const rb200_grid* grid, double density, const double
 }
 
 
+int rb200_precondition_jacobi_device(const rb200_grid* grid, double density, const double* r, double* z, size_t len,
+                                     double* rz, void* stream) {
+    if (!r || !z || !rz) return RB200_INVALID_ARGUMENT;
+    RB200_PRIM_BEGIN(grid, density)
+    if (len != size_t(g.cells)) return RB200_LENGTH_MISMATCH;
+    if ((rc = launch_check_finite(r, g.cells, fl.d, s))) return rc;
+    // scratch: partials [blocks][2], the result, the ticket
+    const size_t nb = size_t(precondition_partials_blocks());
+    const size_t bytes = (2 * nb + 1) * sizeof(double) + sizeof(unsigned);
+    char* scratch = nullptr;
+    RB200_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&scratch), bytes, s));
+    Partials part{reinterpret_cast<double*>(scratch), reinterpret_cast<unsigned*>(scratch + (2 * nb + 1) * 8)};
+    double* rz_dev = part.data + 2 * nb;
+    cudaMemsetAsync(part.ticket, 0, sizeof(unsigned), s);
+    rc = launch_precondition_jacobi(g, r, z, part, rz_dev, s);
+    double h = 0.0;
+    if (!rc && cudaMemcpyAsync(&h, rz_dev, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        rc = RB200_EXECUTION;
+    cudaFreeAsync(scratch, s);
+    if (rc) return rc;
+    int f = 0;
+    if ((rc = fl.close(&f))) return rc;
+    *rz = h;
+    return flags_status(f, false);
+}
+
 int rb200_build_rhs_f32_device(const rb200_grid* grid, double density, const float* u, const float* v,
                                const float* w, double dt, double* rhs, void* stream) {
     return build_rhs_prim<float>(grid, density, u, v, w, dt, rhs, stream);

@@ -32,6 +32,7 @@ struct GridDev {
     double weight[3];
     double volume;
     double diag[64];
+    double rdiag[64];  // RN(1/diag) where div_diag may use it, else 0
 };
 
 __device__ __forceinline__ int cell_idx(const GridDev& g, int i, int j, int k) {
@@ -40,11 +41,30 @@ __device__ __forceinline__ int cell_idx(const GridDev& g, int i, int j, int k) {
 __device__ __forceinline__ int face_idx(const GridDev& g, int a, int i, int j, int k) {
     return i + g.fc[a][0] * (j + g.fc[a][1] * k);
 }
+// Neighbour mask of a cell: bit 0/1 lower/upper X, 2/3 Y, 4/5 Z.
+__device__ __forceinline__ int diag_mask(const GridDev& g, int i, int j, int k) {
+    return int(i > 0) | (int(i + 1 < g.n[0]) << 1) | (int(j > 0) << 2) | (int(j + 1 < g.n[1]) << 3) |
+           (int(k > 0) << 4) | (int(k + 1 < g.n[2]) << 5);
+}
 // PressureOperator::diagonal (src/operator.rs:813-822).
-__device__ __forceinline__ double diag_at(const GridDev& g, int i, int j, int k) {
-    int mask = int(i > 0) | (int(i + 1 < g.n[0]) << 1) | (int(j > 0) << 2) |
-               (int(j + 1 < g.n[1]) << 3) | (int(k > 0) << 4) | (int(k + 1 < g.n[2]) << 5);
-    return g.diag[mask];
+__device__ __forceinline__ double diag_at(const GridDev& g, int i, int j, int k) { return g.diag[diag_mask(g, i, j, k)]; }
+
+// r / D rounded to nearest, as IEEE division rounds it, through y = RN(1/D):
+// q = RN(r*y) is within one ulp of r/D, the remainder r - q*D is exact by
+// FMA, and RN(q + rem*y) is the correctly rounded quotient (Markstein's
+// theorem for round-to-nearest: y within half an ulp of 1/D, q within one ulp
+// of r/D). Three floating-point operations instead of a division. The
+// theorem's conditions (no underflow or overflow in q and the remainder) are
+// met for 2^-900 <= |r| <= 2^900 and a table entry y != 0 (set only for
+// 2^-500 < D < 2^500); every other case divides.
+__device__ __forceinline__ double div_diag(double r, double D, double y) {
+    const double a = fabs(r);
+    if (y != 0.0 && a >= 0x1p-900 && a <= 0x1p900) {
+        const double q = r * y;
+        const double rem = fma(-q, D, r);
+        return fma(rem, y, q);
+    }
+    return r / D;
 }
 
 // ------------------------------------------------------------ double-double

@@ -94,6 +94,7 @@ inline int make_grid_dev(const rb200_grid* in, double density, GridDev* g) {
         for (int side = 0; side < 6; ++side)
             if (mask & (1 << side)) v += g->weight[side / 2];
         g->diag[mask] = v;
+        g->rdiag[mask] = (v > 0x1p-500 && v < 0x1p500) ? 1.0 / v : 0.0;
     }
     return RB200_OK;
 }
@@ -123,6 +124,11 @@ enum : int {
 
 // ---------------------------------------------------------------- operator.cu
 int launch_apply_full(const GridDev& g, const double* p, double* out, int* flags, cudaStream_t s);
+// z = r/D (z[0] = 0) and r.z into *rz_out (device), with `part` holding
+// precondition_partials_blocks() blocks of partials and a zeroed ticket.
+int launch_precondition_jacobi(const GridDev& g, const double* r, double* z, Partials part, double* rz_out,
+                               cudaStream_t s);
+int precondition_partials_blocks();
 template <class T>
 int launch_validate_faces(const GridDev& g, const T* u, const T* v, const T* w, int* flags,
                           cudaStream_t s);

@@ -123,7 +123,8 @@ __global__ void __launch_bounds__(EW) k_load_residual(GridDev g, SolveState* st,
         if (KIND == KIND_MG) continue;
         int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
         if (KIND == KIND_JACOBI) {
-            double zc = rc / diag_at(g, i, j, k);
+            const int m = diag_mask(g, i, j, k);
+            double zc = div_diag(rc, g.diag[m], g.rdiag[m]);
             z[c] = zc;
             acc.add(rc * zc);
         } else if (((i + j + k) & 1) == 0) {
@@ -137,6 +138,34 @@ __global__ void __launch_bounds__(EW) k_load_residual(GridDev g, SolveState* st,
     if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
         fold_partials<1, 0>(part, gridDim.x, sm, sums, none);
         if (threadIdx.x == 0) decide_rz(st, trace, dd_value(sums[0]), mode);
+    }
+}
+
+// precondition_jacobi (src/pressure.rs:534-575) as a primitive: z = r/D on
+// every row but the eliminated gauge row (z[0] = 0), and r.z over rows >= 1.
+__global__ void __launch_bounds__(EW) k_precondition_jacobi(GridDev g, const double* __restrict__ r,
+                                                            double* __restrict__ z, Partials part,
+                                                            double* __restrict__ rz_out) {
+    __shared__ BlockReduce<1, 0> sm;
+    Neu acc;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        if (c == 0) {
+            z[0] = 0.0;
+            continue;
+        }
+        const int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+        const int m = diag_mask(g, i, j, k);
+        const double rc = r[c];
+        const double zc = div_diag(rc, g.diag[m], g.rdiag[m]);
+        z[c] = zc;
+        acc.add(rc * zc);
+    }
+    dd sums[1] = {acc.as_dd()};
+    double none[1];
+    block_reduce<1, 0>(sm, sums, none);
+    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
+        fold_partials<1, 0>(part, gridDim.x, sm, sums, none);
+        if (threadIdx.x == 0) *rz_out = dd_value(sums[0]);
     }
 }
 
@@ -295,7 +324,8 @@ __global__ void __launch_bounds__(TILE_THREADS) k_pass2(GridDev g, SolveState* s
         r[c] = rc;
         acc_rr.add(rc * rc);
         if (PRE == 0) {
-            double zc = rc / diag_at(g, i, j, k);
+            const int m = diag_mask(g, i, j, k);
+            double zc = div_diag(rc, g.diag[m], g.rdiag[m]);
             z[c] = zc;
             acc_rz.add(rc * zc);
         } else if (PRE == 1 && ((i + j + k) & 1) == 0) {
@@ -1142,6 +1172,14 @@ int PcgSolver::profile(int which, int launches, double* avg_ms) {
     *avg_ms = double(ms) / launches;
     return RB200_OK;
 }
+
+int launch_precondition_jacobi(const GridDev& g, const double* r, double* z, Partials part, double* rz_out,
+                               cudaStream_t s) {
+    k_precondition_jacobi<<<ew_blocks(g.cells), EW, 0, s>>>(g, r, z, part, rz_out);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+int precondition_partials_blocks() { return EW_CAP; }
 
 // ------------------------------------------------------------ allocation-free solve
 // A Jacobi-PCG solve for callers that cannot allocate device memory: code that

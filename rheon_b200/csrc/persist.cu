@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
     __shared__ SolveState sst;
     __shared__ __align__(8) uint64_t full[NS];
     __shared__ __align__(8) uint64_t empty[NS];
-    __shared__ double sdiag[64];
+    __shared__ double sdiag[64], srdiag[64];
     const GridDev& g = A.g;
     Ctx c;
     c.tid = threadIdx.x;
@@ -282,7 +282,10 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
     c.ring = 0u;
     c.gen = 0u;
     c.set = 0;
-    if (c.tid < 64) sdiag[c.tid] = g.diag[c.tid];
+    if (c.tid < 64) {
+        sdiag[c.tid] = g.diag[c.tid];
+        srdiag[c.tid] = g.rdiag[c.tid];
+    }
     if (c.tid == 0) {
         sst = *A.st;
         c.gen = ld_acquire_gpu(&A.bar->gen);
@@ -359,7 +362,8 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
                             A.z[0] = 0.0;
                             continue;
                         }
-                        const double zc = rc / sdiag[col.mxy | zmask(g, col.k0 + qb + u)];
+                        const int m = col.mxy | zmask(g, col.k0 + qb + u);
+                        const double zc = div_diag(rc, sdiag[m], srdiag[m]);
                         A.z[cc] = zc;
                         (u & 1 ? acc.b : acc.a).add(rc * zc);
                     }
@@ -463,7 +467,8 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
                         const double rc = sr[bi] - alpha * qv;
                         A.r[cc] = rc;
                         (u & 1 ? acc_rr.b : acc_rr.a).add(rc * rc);
-                        const double zc = rc / sdiag[col.mxy | zmask(g, k)];
+                        const int m = col.mxy | zmask(g, k);
+                        const double zc = div_diag(rc, sdiag[m], srdiag[m]);
                         A.z[cc] = zc;
                         (u & 1 ? acc_rz.b : acc_rz.a).add(rc * zc);
                     }
