@@ -88,6 +88,8 @@ struct PersistArgs {
 // Per-block context.
 struct Ctx {
     int nbx, nby, nbricks, mine;  // bricks along x, y; in total; of this block
+    int bx0, by0, bz0;            // brick coordinates of this block's first brick
+    int sx, sy, sz;               // the grid stride (gridDim.x bricks) as brick coordinates
     int tid, lane, tx, ty, tz;
     bool producer;
     unsigned ring;     // ring slots used so far (same count in every thread)
@@ -95,13 +97,25 @@ struct Ctx {
     int set;           // partial set parity
 };
 
-__device__ __forceinline__ void brick_origin(const Ctx& c, int b, int& x0, int& y0, int& k0) {
-    const int bx = b % c.nbx;
-    const int rest = b / c.nbx;
-    x0 = bx * TX;
-    y0 = (rest % c.nby) * TY;
-    k0 = (rest / c.nby) * PZC;
-}
+// Walks the block's bricks b = blockIdx.x + n * gridDim.x, keeping their
+// coordinates by carries instead of divisions.
+struct BrickWalk {
+    int b, bx, by, bz;
+    __device__ __forceinline__ explicit BrickWalk(const Ctx& c) : b(blockIdx.x), bx(c.bx0), by(c.by0), bz(c.bz0) {}
+    __device__ __forceinline__ void next(const Ctx& c) {
+        b += gridDim.x;
+        bx += c.sx;
+        int carry = bx >= c.nbx;
+        bx -= carry ? c.nbx : 0;
+        by += c.sy + carry;
+        carry = by >= c.nby;
+        by -= carry ? c.nby : 0;
+        bz += c.sz + carry;
+    }
+    __device__ __forceinline__ int x0() const { return bx * TX; }
+    __device__ __forceinline__ int y0() const { return by * TY; }
+    __device__ __forceinline__ int k0() const { return bz * PZC; }
+};
 
 // One consumer thread's column of a brick: cells (i, j, k0 + qb .. + QPT - 1).
 struct Col {
@@ -113,9 +127,8 @@ struct Col {
     bool own;       // the column lies inside the domain
 };
 
-__device__ __forceinline__ Col column(const GridDev& g, const Ctx& c, int b, int qb) {
-    int x0, y0, k0;
-    brick_origin(c, b, x0, y0, k0);
+__device__ __forceinline__ Col column(const GridDev& g, const Ctx& c, const BrickWalk& w, int qb) {
+    const int x0 = w.x0(), y0 = w.y0(), k0 = w.k0();
     const int i = x0 + c.tx, j = y0 + c.ty;
     Col col;
     col.own = i < g.n[0] && j < g.n[1];
@@ -235,23 +248,23 @@ __device__ __forceinline__ bool run_bricks(Ctx& c, uint64_t* full, uint64_t* emp
     unsigned slot_count = c.ring;
     if (c.producer) {
         if (c.lane == 0) {
-            for (int b = blockIdx.x; b < c.nbricks; b += gridDim.x, ++slot_count) {
+            for (BrickWalk w(c); w.b < c.nbricks; w.next(c), ++slot_count) {
                 const unsigned slot = slot_count % NS, phase = (slot_count / NS) & 1u;
                 if (!mbar_wait_bounded(&empty[slot], phase ^ 1u)) {
                     ok = false;
                     break;
                 }
-                issue(b, int(slot));
+                issue(w, int(slot));
             }
         }
     } else {
-        for (int b = blockIdx.x; b < c.nbricks; b += gridDim.x, ++slot_count) {
+        for (BrickWalk w(c); w.b < c.nbricks; w.next(c), ++slot_count) {
             const unsigned slot = slot_count % NS, phase = (slot_count / NS) & 1u;
             if (!mbar_wait_bounded(&full[slot], phase)) {
                 ok = false;
                 break;
             }
-            body(b, int(slot));
+            body(w, int(slot));
             __syncwarp();
             if (c.lane == 0) mbar_arrive(&empty[slot]);
         }
@@ -279,6 +292,12 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
     c.nby = (g.n[1] + TY - 1) / TY;
     c.nbricks = c.nbx * c.nby * ((g.n[2] + PZC - 1) / PZC);
     c.mine = c.nbricks > int(blockIdx.x) ? (c.nbricks - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x) : 0;
+    c.bx0 = int(blockIdx.x) % c.nbx;
+    c.by0 = (int(blockIdx.x) / c.nbx) % c.nby;
+    c.bz0 = int(blockIdx.x) / (c.nbx * c.nby);
+    c.sx = int(gridDim.x) % c.nbx;
+    c.sy = (int(gridDim.x) / c.nbx) % c.nby;
+    c.sz = int(gridDim.x) / (c.nbx * c.nby);
     c.ring = 0u;
     c.gen = 0u;
     c.set = 0;
@@ -311,15 +330,14 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
             double mx = 0.0;
             const bool mine_ok = run_bricks(
                 c, full, empty,
-                [&](int b, int s) {
-                    int x0, y0, k0;
-                    brick_origin(c, b, x0, y0, k0);
+                [&](const BrickWalk& w, int s) {
+                    const int x0 = w.x0(), y0 = w.y0(), k0 = w.k0();
                     mbar_expect_tx(&full[s], PS::BYTES);
                     tma_load_slab(smem + s * STAGE, &maps.p, x0 - 2, y0 - 1, k0 - 1, &full[s]);
                 },
-                [&](int b, int s) {
+                [&](const BrickWalk& w, int s) {
                     const double* sp = smem + s * STAGE;
-                    const Col col = column(g, c, b, qb);
+                    const Col col = column(g, c, w, qb);
                     if (!col.own) return;
                     double v[QPT + 2];
 #pragma unroll
@@ -349,8 +367,8 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
             const double* spare = sst.dsel ? A.d0 : A.d1;
             Neu2 acc;
             if (!c.producer) {
-                for (int b = blockIdx.x; b < c.nbricks; b += gridDim.x) {
-                    const Col col = column(g, c, b, qb);
+                for (BrickWalk w(c); w.b < c.nbricks; w.next(c)) {
+                    const Col col = column(g, c, w, qb);
                     if (!col.own) continue;
 #pragma unroll
                     for (int u = 0; u < QPT; ++u) {
@@ -389,20 +407,19 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
             Neu2 acc;
             const bool mine_ok = run_bricks(
                 c, full, empty,
-                [&](int b, int s) {
-                    int x0, y0, k0;
-                    brick_origin(c, b, x0, y0, k0);
+                [&](const BrickWalk& w, int s) {
+                    const int x0 = w.x0(), y0 = w.y0(), k0 = w.k0();
                     double* sz = smem + s * STAGE;
                     mbar_expect_tx(&full[s], (fresh ? 1u : 2u) * PS::BYTES);
                     tma_load_slab(sz, &maps.z, x0 - 2, y0 - 1, k0 - 1, &full[s]);
                     if (!fresh) tma_load_slab(sz + PS::SIZE, dmap, x0 - 2, y0 - 1, k0 - 1, &full[s]);
                 },
-                [&](int b, int s) {
+                [&](const BrickWalk& w, int s) {
                     const double* sz = smem + s * STAGE;
                     const double* sd = sz + PS::SIZE;
                     // the new direction at slab element e (src/pressure.rs:720-731)
                     auto dn = [&](int e) { return fresh ? sz[e] : sz[e] + beta * sd[e]; };
-                    const Col col = column(g, c, b, qb);
+                    const Col col = column(g, c, w, qb);
                     if (!col.own) return;
                     double v[QPT + 2];
 #pragma unroll
@@ -435,20 +452,19 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
             Neu2 acc_rr, acc_rz;
             const bool mine_ok = run_bricks(
                 c, full, empty,
-                [&](int b, int s) {
-                    int x0, y0, k0;
-                    brick_origin(c, b, x0, y0, k0);
+                [&](const BrickWalk& w, int s) {
+                    const int x0 = w.x0(), y0 = w.y0(), k0 = w.k0();
                     double* sd = smem + s * STAGE;
                     mbar_expect_tx(&full[s], PS::BYTES + 2u * BOX_BYTES);
                     tma_load_slab(sd, dmap, x0 - 2, y0 - 1, k0 - 1, &full[s]);
                     tma_load_slab(sd + PS::SIZE, &maps.p_box, x0, y0, k0, &full[s]);
                     tma_load_slab(sd + PS::SIZE + BOX, &maps.r_box, x0, y0, k0, &full[s]);
                 },
-                [&](int b, int s) {
+                [&](const BrickWalk& w, int s) {
                     const double* sd = smem + s * STAGE;
                     const double* sp = sd + PS::SIZE;
                     const double* sr = sp + BOX;
-                    const Col col = column(g, c, b, qb);
+                    const Col col = column(g, c, w, qb);
                     if (!col.own) return;
                     double v[QPT + 2];
 #pragma unroll

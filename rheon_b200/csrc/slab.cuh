@@ -126,14 +126,15 @@ __device__ __forceinline__ Neigh slab_neigh(const double* sm, int e) {
 
 // Reference-order compensated accumulation (Neumaier, src/pressure.rs:135-148)
 // of one thread's terms; folded into a double-double for the block reduction.
+// The rounding error of each s + x is formed branch-free by two-sum; it is
+// the exact error, so it equals Neumaier's (s - t) + x or (x - t) + s and the
+// compensation c is the same value bit for bit.
 struct Neu {
     double s = 0.0, c = 0.0;
     __device__ __forceinline__ void add(double x) {
-        double t = s + x;
-        if (fabs(s) >= fabs(x))
-            c += (s - t) + x;
-        else
-            c += (x - t) + s;
+        double t, e;
+        two_sum(s, x, t, e);
+        c += e;
         s = t;
     }
     __device__ __forceinline__ dd as_dd() const {
