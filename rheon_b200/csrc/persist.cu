@@ -63,6 +63,16 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
 __device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ void st_relaxed_gpu(unsigned* p, unsigned v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+// Arrival: releases this block's writes (ordered before it by the block
+// barrier) and, for the last arriver, acquires everyone else's.
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;\n" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 // Order this thread's generic-proxy global accesses with its (or, through a
 // barrier, its block's) later TMA (async-proxy) accesses.
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
@@ -174,11 +184,9 @@ __device__ __forceinline__ bool grid_barrier(Ctx& c, GridBarrier* gb) {
     __syncthreads();
     if (c.tid == 0) {
         int ok = 1;
-        __threadfence();
-        const unsigned arrived = atomicAdd(&gb->count, 1u);
+        const unsigned arrived = atom_add_acq_rel_gpu(&gb->count, 1u);
         if (arrived == gridDim.x - 1) {
-            atomicExch(&gb->count, 0u);
-            __threadfence();
+            st_relaxed_gpu(&gb->count, 0u);
             st_release_gpu(&gb->gen, c.gen + 1u);
         } else {
             unsigned n = 0;
@@ -190,7 +198,6 @@ __device__ __forceinline__ bool grid_barrier(Ctx& c, GridBarrier* gb) {
                 __nanosleep(64);
             }
         }
-        __threadfence();
         fence_proxy_async_global();
         c.gen += 1u;
         if (!ok) atomicExch(&gb->abort, 1u);
@@ -248,6 +255,9 @@ __device__ __forceinline__ bool run_bricks(Ctx& c, uint64_t* full, uint64_t* emp
     unsigned slot_count = c.ring;
     if (c.producer) {
         if (c.lane == 0) {
+            // order the data this block saw through the grid barrier before
+            // the TMA (async-proxy) reads below
+            fence_proxy_async_global();
             for (BrickWalk w(c); w.b < c.nbricks; w.next(c), ++slot_count) {
                 const unsigned slot = slot_count % NS, phase = (slot_count / NS) & 1u;
                 if (!mbar_wait_bounded(&empty[slot], phase ^ 1u)) {
