@@ -324,8 +324,10 @@ RB200_API int rb200_carrier_create(const rb200_carrier_config* config, rb200_car
 RB200_API void rb200_carrier_destroy(rb200_carrier* carrier);
 RB200_API uint64_t rb200_carrier_allocated_bytes(const rb200_carrier* carrier);
 RB200_API void* rb200_carrier_stream(rb200_carrier* carrier);
-/* Host faces in the configured storage type (float* or double*); tracer may be
- * NULL. Validates the fixed-box wall contract. */
+/* Faces in the configured storage type (float* or double*), in host memory or
+ * in this device's memory (the copy direction is inferred); tracer may be
+ * NULL. Validates the fixed-box wall contract. rb200_carrier_download copies
+ * the accepted state out the same way. */
 RB200_API int rb200_carrier_upload(rb200_carrier* carrier, const void* u, const void* v, const void* w,
                          const float* tracer);
 RB200_API int rb200_carrier_download(rb200_carrier* carrier, void* u, void* v, void* w, float* tracer);

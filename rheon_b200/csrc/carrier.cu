@@ -447,11 +447,11 @@ int rb200_carrier_upload(rb200_carrier* carrier, const void* u, const void* v, c
     const int a = c->h_cd->acc;
     const void* src[3] = {u, v, w};
     for (int d = 0; d < 3; ++d)
-        RB200_CUDA(cudaMemcpyAsync(c->faces[a][d], src[d], size_t(c->g.flen[d]) * c->elem, cudaMemcpyHostToDevice,
+        RB200_CUDA(cudaMemcpyAsync(c->faces[a][d], src[d], size_t(c->g.flen[d]) * c->elem, cudaMemcpyDefault,
                                    c->stream));
     if (tracer) {
         if (!c->tracer[0]) return RB200_INVALID_ARGUMENT;
-        RB200_CUDA(cudaMemcpyAsync(c->tracer[c->h_cd->tacc], tracer, size_t(c->g.cells) * 4, cudaMemcpyHostToDevice,
+        RB200_CUDA(cudaMemcpyAsync(c->tracer[c->h_cd->tacc], tracer, size_t(c->g.cells) * 4, cudaMemcpyDefault,
                                    c->stream));
     }
     return upload_rate(c);
@@ -496,10 +496,10 @@ int rb200_carrier_download(rb200_carrier* carrier, void* u, void* v, void* w, fl
     void* dst[3] = {u, v, w};
     for (int d = 0; d < 3; ++d)
         if (dst[d])
-            RB200_CUDA(cudaMemcpyAsync(dst[d], c->faces[a][d], size_t(c->g.flen[d]) * c->elem, cudaMemcpyDeviceToHost,
+            RB200_CUDA(cudaMemcpyAsync(dst[d], c->faces[a][d], size_t(c->g.flen[d]) * c->elem, cudaMemcpyDefault,
                                        c->stream));
     if (tracer && c->tracer[0])
-        RB200_CUDA(cudaMemcpyAsync(tracer, c->tracer[c->h_cd->tacc], size_t(c->g.cells) * 4, cudaMemcpyDeviceToHost,
+        RB200_CUDA(cudaMemcpyAsync(tracer, c->tracer[c->h_cd->tacc], size_t(c->g.cells) * 4, cudaMemcpyDefault,
                                    c->stream));
     RB200_CUDA(cudaStreamSynchronize(c->stream));
     return RB200_OK;

@@ -539,6 +539,44 @@ def test_mixed_carrier_tracks_the_fp64_oracle():
         assert rep.pressure.iterations <= 40
 
 
+def test_mixed_buoyant_blob_tracks_the_fp64_oracle():
+    """The buoyant-blob workload in miniature (40^3, sigma 6 cells, rel
+    1e-10): mixed carrier against the FP64-storage oracle step with the same
+    tracer and buoyancy, per step."""
+    n = (40, 40, 40)
+    g = R.GridGeometry(n)
+    faces64 = W.fourier_faces(n, seed=3, dtype=np.float64)
+    blob = W.gaussian_blob(n, sigma=6.0)
+    sim = R.CarrierSimulation(g, R.CarrierConfig.mixed(pressure=S(1e-10, 0.0, 1.7976931348623157e308, 500),
+                                                       with_tracer=True))
+    sim.upload([f.astype(np.float32) for f in faces64], blob)
+    s = O.settings(1e-10, 0.0, 1.7976931348623157e308, 100000)
+    ref, tr = faces64, blob
+    for step in range(3):
+        rep = sim.step(R.StepParams(0.05, buoyancy=1.0))
+        prm = O.StepParams(0.05, 1.0, O.JACOBI_PCG_V1, s, 1.0, 0, 8)
+        st, ref, tr, _ = O.carrier_step(og(g), ref, prm, tracer=tr)
+        assert st == O.OK
+        got, gtr = sim.download(with_tracer=True)
+        err = max(relerr(got[d].astype(np.float64), ref[d]) for d in range(3))
+        assert err < 1e-4, (step, err)
+        assert relerr(gtr.astype(np.float64), tr.astype(np.float64)) < 1e-4
+        assert rep.actual_divergence_max < 1e-4, rep.actual_divergence_max
+
+
+def test_carrier_state_round_trips_through_device_memory():
+    """upload/download accept device pointers (the copy direction is inferred)."""
+    n = (24, 20, 16)
+    g = R.GridGeometry(n)
+    faces = W.fourier_faces(n, seed=4, dtype=np.float64)
+    sim = R.CarrierSimulation(g, R.CarrierConfig(storage="f64"))
+    sim.upload(faces)
+    bufs = [torch.empty(g.face_len(d), dtype=torch.float64, device="cuda") for d in range(3)]
+    sim.download_ptrs(*[b.data_ptr() for b in bufs])
+    for d in range(3):
+        assert np.array_equal(host(bufs[d]), faces[d])
+
+
 # ------------------------------------------------------------------ batched instances
 def test_batched_instances_match_the_same_instances_stepped_alone():
     """Uneven boxes stepped together (one graph per instance, overlapping on
