@@ -11,7 +11,7 @@
 namespace rb200 {
 
 constexpr int MG_THREADS = 256;
-constexpr int MG_BOTTOM_THREADS = 1024;
+constexpr int MG_LOWER_THREADS = 1024;
 
 __device__ __forceinline__ bool mg_gate(const SolveState* st, int mode) { return gate(st->flags, mode); }
 
@@ -24,89 +24,111 @@ __host__ __device__ __forceinline__ long mg_pairs(const MgLevelDev& L) {
     return long((L.n[0] + 1) >> 1) * L.n[1] * L.n[2];
 }
 
-// Pair mapping of a red-black half-sweep: pair t covers cells 2m and 2m+1 of
-// row (j, k); (i, j, k) is the cell of colour `color` in it (i may be n0).
-__device__ __forceinline__ void pair_cell(const MgLevelDev& L, long t, int color, int& i, int& j, int& k) {
-    const int hx = (L.n[0] + 1) >> 1;
-    const int m = int(t % hx);
-    const long row = t / hx;
-    j = int(row % L.n[1]);
-    k = int(row / L.n[1]);
-    i = 2 * m + ((color + j + k) & 1);
+// Work mapping of the level loops: the rows (j, k) of a level are dealt to
+// warps (row = j + n1*k), and a warp's lanes take the pair index m of the row;
+// pair m holds cells 2m and 2m+1, of which the one of colour `color` has
+// i = 2m + ((color + j + k) & 1) (i may be n0 for an odd row length).
+struct Warps {
+    int w0, nw, lane;
+};
+__device__ __forceinline__ Warps grid_warps() {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    return Warps{t >> 5, int((gridDim.x * blockDim.x) >> 5), int(threadIdx.x & 31)};
+}
+
+// Loads of level data: through L1 in the grid kernels, from L2 in the cluster
+// kernel (its CTAs exchange level data through global memory between
+// cluster barriers).
+template <bool CG>
+__device__ __forceinline__ float ldv(const float* p) {
+    if (CG) return __ldcg(p);
+    return *p;
 }
 
 // Gauss-Seidel value x = (b + sum_nb w x_nb) / D, summed x-, x+, y-, y+, z-, z+.
+template <bool CG>
 __device__ __forceinline__ float gs_value(const MgLevelDev& L, float b, int i, int j, int k, int c) {
     const int sy = L.n[0], sz = L.n[0] * L.n[1];
     const float* __restrict__ x = L.x;
     float s = b;
-    if (i > 0) s += L.w[0] * x[c - 1];
-    if (i + 1 < L.n[0]) s += L.w[0] * x[c + 1];
-    if (j > 0) s += L.w[1] * x[c - sy];
-    if (j + 1 < L.n[1]) s += L.w[1] * x[c + sy];
-    if (k > 0) s += L.w[2] * x[c - sz];
-    if (k + 1 < L.n[2]) s += L.w[2] * x[c + sz];
+    if (i > 0) s += L.w[0] * ldv<CG>(x + c - 1);
+    if (i + 1 < L.n[0]) s += L.w[0] * ldv<CG>(x + c + 1);
+    if (j > 0) s += L.w[1] * ldv<CG>(x + c - sy);
+    if (j + 1 < L.n[1]) s += L.w[1] * ldv<CG>(x + c + sy);
+    if (k > 0) s += L.w[2] * ldv<CG>(x + c - sz);
+    if (k + 1 < L.n[2]) s += L.w[2] * ldv<CG>(x + c + sz);
     return s * L.dinv[mask_of(L.n, i, j, k)];
 }
 
-// Half-sweep of colour `color` over pairs [t0, pairs) step dt. With `first`
-// the correction starts from zero (red = b/D, black cleared); with r0 the FP32
-// right-hand side of the finest level is converted from the FP64 residual on
-// the way (both cells of the pair).
-__device__ __forceinline__ void smooth_pairs(const MgLevelDev& L, const double* __restrict__ r0, int color,
-                                             bool first, long t0, long dt) {
-    const long pairs = mg_pairs(L);
-    for (long t = t0; t < pairs; t += dt) {
-        int i, j, k;
-        pair_cell(L, t, color, i, j, k);
-        const int io = i ^ 1;
-        const int row = L.n[0] * (j + L.n[1] * k);
-        if (first && io < L.n[0]) {
-            if (r0) L.b[io + row] = float(r0[io + row]);
-            L.x[io + row] = 0.0f;
+// Half-sweep of colour `color` over the level. With `first` the correction
+// starts from zero (red = b/D, black cleared); with r0 the FP32 right-hand
+// side of the finest level is converted from the FP64 residual on the way
+// (both cells of the pair).
+template <bool CG>
+__device__ __forceinline__ void smooth_rows(const MgLevelDev& L, const double* __restrict__ r0, int color, bool first,
+                                            const Warps& W) {
+    const int hx = (L.n[0] + 1) >> 1;
+    const int rows = L.n[1] * L.n[2];
+    for (int row = W.w0; row < rows; row += W.nw) {
+        const int j = row % L.n[1], k = row / L.n[1];
+        const int base = L.n[0] * row;
+        const int par = (color + j + k) & 1;
+        for (int m = W.lane; m < hx; m += 32) {
+            const int i = 2 * m + par;
+            const int io = i ^ 1;
+            if (first && io < L.n[0]) {
+                if (r0) L.b[io + base] = float(r0[io + base]);
+                L.x[io + base] = 0.0f;
+            }
+            if (i >= L.n[0]) continue;
+            const int c = i + base;
+            float b;
+            if (r0) {
+                b = float(r0[c]);
+                L.b[c] = b;
+            } else {
+                b = ldv<CG>(L.b + c);
+            }
+            L.x[c] = first ? b * L.dinv[mask_of(L.n, i, j, k)] : gs_value<CG>(L, b, i, j, k, c);
         }
-        if (i >= L.n[0]) continue;
-        const int c = i + row;
-        float b;
-        if (r0) {
-            b = float(r0[c]);
-            L.b[c] = b;
-        } else {
-            b = L.b[c];
-        }
-        L.x[c] = first ? b * L.dinv[mask_of(L.n, i, j, k)] : gs_value(L, b, i, j, k, c);
     }
 }
 
 // Residual b - K x on the fine cells summed over each coarse cell's children
-// (restriction = transpose of the piecewise-constant prolongation).
-__device__ __forceinline__ void restrict_cells(const MgLevelDev& L, const MgLevelDev& C, int c0, int dc) {
+// (restriction = transpose of the piecewise-constant prolongation). Warps
+// take coarse rows, lanes coarse cells along x.
+template <bool CG>
+__device__ __forceinline__ void restrict_rows(const MgLevelDev& L, const MgLevelDev& C, const Warps& W) {
     const int sy = L.n[0], sz = L.n[0] * L.n[1];
-    for (int cc = c0; cc < C.cells; cc += dc) {
-        const int I = cc % C.n[0], J = (cc / C.n[0]) % C.n[1], K = cc / (C.n[0] * C.n[1]);
-        float sum = 0.0f;
-        for (int dk = 0; dk < L.cf[2]; ++dk)
-            for (int dj = 0; dj < L.cf[1]; ++dj)
-                for (int di = 0; di < L.cf[0]; ++di) {
-                    const int i = I * L.cf[0] + di, j = J * L.cf[1] + dj, k = K * L.cf[2] + dk;
-                    if (i >= L.n[0] || j >= L.n[1] || k >= L.n[2]) continue;
-                    const int c = i + L.n[0] * (j + L.n[1] * k);
-                    const float xc = L.x[c];
-                    float kx = 0.0f;
-                    if (i > 0) kx += L.w[0] * (xc - L.x[c - 1]);
-                    if (i + 1 < L.n[0]) kx += L.w[0] * (xc - L.x[c + 1]);
-                    if (j > 0) kx += L.w[1] * (xc - L.x[c - sy]);
-                    if (j + 1 < L.n[1]) kx += L.w[1] * (xc - L.x[c + sy]);
-                    if (k > 0) kx += L.w[2] * (xc - L.x[c - sz]);
-                    if (k + 1 < L.n[2]) kx += L.w[2] * (xc - L.x[c + sz]);
-                    sum += L.b[c] - kx;
-                }
-        C.b[cc] = sum;
+    const int rows = C.n[1] * C.n[2];
+    for (int row = W.w0; row < rows; row += W.nw) {
+        const int J = row % C.n[1], K = row / C.n[1];
+        for (int I = W.lane; I < C.n[0]; I += 32) {
+            float sum = 0.0f;
+            for (int dk = 0; dk < L.cf[2]; ++dk)
+                for (int dj = 0; dj < L.cf[1]; ++dj)
+                    for (int di = 0; di < L.cf[0]; ++di) {
+                        const int i = I * L.cf[0] + di, j = J * L.cf[1] + dj, k = K * L.cf[2] + dk;
+                        if (i >= L.n[0] || j >= L.n[1] || k >= L.n[2]) continue;
+                        const int c = i + L.n[0] * (j + L.n[1] * k);
+                        const float xc = ldv<CG>(L.x + c);
+                        float kx = 0.0f;
+                        if (i > 0) kx += L.w[0] * (xc - ldv<CG>(L.x + c - 1));
+                        if (i + 1 < L.n[0]) kx += L.w[0] * (xc - ldv<CG>(L.x + c + 1));
+                        if (j > 0) kx += L.w[1] * (xc - ldv<CG>(L.x + c - sy));
+                        if (j + 1 < L.n[1]) kx += L.w[1] * (xc - ldv<CG>(L.x + c + sy));
+                        if (k > 0) kx += L.w[2] * (xc - ldv<CG>(L.x + c - sz));
+                        if (k + 1 < L.n[2]) kx += L.w[2] * (xc - ldv<CG>(L.x + c + sz));
+                        sum += ldv<CG>(L.b + c) - kx;
+                    }
+            C.b[I + C.n[0] * row] = sum;
+        }
     }
 }
 
+template <bool CG>
 __device__ __forceinline__ float coarse_at(const MgLevelDev& L, const MgLevelDev& C, int i, int j, int k) {
-    return C.x[(i >> (L.cf[0] - 1)) + C.n[0] * ((j >> (L.cf[1] - 1)) + C.n[1] * (k >> (L.cf[2] - 1)))];
+    return ldv<CG>(C.x + ((i >> (L.cf[0] - 1)) + C.n[0] * ((j >> (L.cf[1] - 1)) + C.n[1] * (k >> (L.cf[2] - 1)))));
 }
 
 // Prolongation fused with the first post-smoothing half-sweep (black): black
@@ -114,105 +136,121 @@ __device__ __forceinline__ float coarse_at(const MgLevelDev& L, const MgLevelDev
 // formed on the fly. Red cells are not written: the red half-sweep that
 // follows replaces every red value without reading it. Nothing this pass reads
 // is written by it.
-__device__ __forceinline__ void prolong_black_pairs(const MgLevelDev& L, const MgLevelDev& C, long t0, long dt) {
-    const long pairs = mg_pairs(L);
+template <bool CG>
+__device__ __forceinline__ void prolong_black_rows(const MgLevelDev& L, const MgLevelDev& C, const Warps& W) {
+    const int hx = (L.n[0] + 1) >> 1;
+    const int rows = L.n[1] * L.n[2];
     const int sy = L.n[0], sz = L.n[0] * L.n[1];
-    for (long t = t0; t < pairs; t += dt) {
-        int i, j, k;
-        pair_cell(L, t, 1, i, j, k);
-        if (i >= L.n[0]) continue;
-        const int c = i + L.n[0] * (j + L.n[1] * k);
-        float s = L.b[c];
-        if (i > 0) s += L.w[0] * (L.x[c - 1] + coarse_at(L, C, i - 1, j, k));
-        if (i + 1 < L.n[0]) s += L.w[0] * (L.x[c + 1] + coarse_at(L, C, i + 1, j, k));
-        if (j > 0) s += L.w[1] * (L.x[c - sy] + coarse_at(L, C, i, j - 1, k));
-        if (j + 1 < L.n[1]) s += L.w[1] * (L.x[c + sy] + coarse_at(L, C, i, j + 1, k));
-        if (k > 0) s += L.w[2] * (L.x[c - sz] + coarse_at(L, C, i, j, k - 1));
-        if (k + 1 < L.n[2]) s += L.w[2] * (L.x[c + sz] + coarse_at(L, C, i, j, k + 1));
-        L.x[c] = s * L.dinv[mask_of(L.n, i, j, k)];
+    for (int row = W.w0; row < rows; row += W.nw) {
+        const int j = row % L.n[1], k = row / L.n[1];
+        const int base = L.n[0] * row;
+        const int par = (1 + j + k) & 1;
+        for (int m = W.lane; m < hx; m += 32) {
+            const int i = 2 * m + par;
+            if (i >= L.n[0]) continue;
+            const int c = i + base;
+            float s = ldv<CG>(L.b + c);
+            if (i > 0) s += L.w[0] * (ldv<CG>(L.x + c - 1) + coarse_at<CG>(L, C, i - 1, j, k));
+            if (i + 1 < L.n[0]) s += L.w[0] * (ldv<CG>(L.x + c + 1) + coarse_at<CG>(L, C, i + 1, j, k));
+            if (j > 0) s += L.w[1] * (ldv<CG>(L.x + c - sy) + coarse_at<CG>(L, C, i, j - 1, k));
+            if (j + 1 < L.n[1]) s += L.w[1] * (ldv<CG>(L.x + c + sy) + coarse_at<CG>(L, C, i, j + 1, k));
+            if (k > 0) s += L.w[2] * (ldv<CG>(L.x + c - sz) + coarse_at<CG>(L, C, i, j, k - 1));
+            if (k + 1 < L.n[2]) s += L.w[2] * (ldv<CG>(L.x + c + sz) + coarse_at<CG>(L, C, i, j, k + 1));
+            L.x[c] = s * L.dinv[mask_of(L.n, i, j, k)];
+        }
     }
 }
 
-// ------------------------------------------------------------ grid kernels
+// ------------------------------------------------------------ grid kernels (large levels)
 __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(MgLevelDev L, const double* __restrict__ r0, int color,
                                                           int first, const SolveState* st, int mode) {
     if (!mg_gate(st, mode)) return;
-    smooth_pairs(L, r0, color, first != 0, blockIdx.x * long(blockDim.x) + threadIdx.x, long(gridDim.x) * blockDim.x);
+    smooth_rows<false>(L, r0, color, first != 0, grid_warps());
 }
 
 __global__ void __launch_bounds__(MG_THREADS) k_mg_restrict(MgLevelDev L, MgLevelDev C, const SolveState* st,
                                                             int mode) {
     if (!mg_gate(st, mode)) return;
-    restrict_cells(L, C, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+    restrict_rows<false>(L, C, grid_warps());
 }
 
 __global__ void __launch_bounds__(MG_THREADS) k_mg_prolong_black(MgLevelDev L, MgLevelDev C, const SolveState* st,
                                                                  int mode) {
     if (!mg_gate(st, mode)) return;
-    prolong_black_pairs(L, C, blockIdx.x * long(blockDim.x) + threadIdx.x, long(gridDim.x) * blockDim.x);
+    prolong_black_rows<false>(L, C, grid_warps());
 }
 
-// ------------------------------------------------------------ bottom levels
-// The descent through the small levels in one block: two red-black sweeps,
-// restriction, next level; barriers between the half-sweeps. r0 is non-null
-// when the first bottom level is the finest level.
-__global__ void __launch_bounds__(MG_BOTTOM_THREADS) k_mg_bottom_down(MgBottom B, const double* __restrict__ r0,
-                                                                      const SolveState* st, int mode) {
-    if (!mg_gate(st, mode)) return;
-    for (int l = 0; l < B.count; ++l) {
-        const MgLevelDev& L = B.lv[l];
-        const double* src = l == 0 ? r0 : nullptr;
-        for (int sweep = 0; sweep < 2; ++sweep) {
-            smooth_pairs(L, sweep == 0 ? src : nullptr, 0, sweep == 0, threadIdx.x, blockDim.x);
-            __syncthreads();
-            smooth_pairs(L, nullptr, 1, false, threadIdx.x, blockDim.x);
-            __syncthreads();
-        }
-        restrict_cells(L, B.lv[l + 1], threadIdx.x, blockDim.x);
-        __syncthreads();
-    }
+// ------------------------------------------------------------ lower levels (one cluster)
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_rank() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ unsigned cluster_size() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
+    return r;
 }
 
-// The ascent: prolongation + black, red, black, red per level; the final red
-// half-sweep of the finest level is skipped when skip_last_red is set (the
-// caller fuses it with its dot products).
-__global__ void __launch_bounds__(MG_BOTTOM_THREADS) k_mg_bottom_up(MgBottom B, int skip_last_red,
-                                                                    const SolveState* st, int mode) {
-    if (!mg_gate(st, mode)) return;
-    for (int l = B.count - 1; l >= 0; --l) {
-        const MgLevelDev& L = B.lv[l];
-        prolong_black_pairs(L, B.lv[l + 1], threadIdx.x, blockDim.x);
-        __syncthreads();
-        smooth_pairs(L, nullptr, 0, false, threadIdx.x, blockDim.x);
-        __syncthreads();
-        smooth_pairs(L, nullptr, 1, false, threadIdx.x, blockDim.x);
-        __syncthreads();
-        if (!(l == 0 && skip_last_red)) {
-            smooth_pairs(L, nullptr, 0, false, threadIdx.x, blockDim.x);
-            __syncthreads();
-        }
-    }
-}
-
-// ------------------------------------------------------------ coarsest level
-// x = G b in FP64, G the mean-projected pseudo-inverse of the coarsest
-// operator; one warp per row, lanes over columns, a fixed shuffle tree.
-// r0 is the right-hand side when the whole grid is the coarsest level.
-__global__ void __launch_bounds__(256) k_mg_dense(MgLevelDev C, const double* __restrict__ G,
-                                                  const double* __restrict__ r0, const SolveState* st, int mode) {
-    if (!mg_gate(st, mode)) return;
+// The whole V-cycle below the grid-kernel levels in one thread-block cluster:
+// the CTAs split every half-sweep, restriction and prolongation, and meet at
+// hardware cluster barriers (release/acquire) instead of kernel boundaries.
+// Level data moves through L2. The coarsest level is solved densely in FP64
+// (x = G b, one warp per row). r0 is the FP64 residual when the first level
+// here is the finest level; skip_last_red leaves that level's final red
+// half-sweep to the finish kernel.
+__global__ void __launch_bounds__(MG_LOWER_THREADS, 1) k_mg_lower(MgLower P, const double* __restrict__ r0,
+                                                               const double* __restrict__ G,
+                                                               const SolveState* st, int mode, int skip_last_red) {
     __shared__ double bs[512];
-    const int M = C.cells;
-    for (int c = threadIdx.x; c < M; c += blockDim.x) bs[c] = r0 ? r0[c] : double(C.b[c]);
-    __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (row >= M) return;
-    const double* g = G + size_t(row) * M;
-    double s = 0.0;
-    for (int c = lane; c < M; c += 32) s += g[c] * bs[c];
-    for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
-    if (lane == 0) C.x[row] = float(s);
+    if (!mg_gate(st, mode)) return;  // uniform: every CTA reads the same flags
+    const unsigned rank = cluster_rank(), nct = cluster_size();
+    const Warps W{int((rank * blockDim.x + threadIdx.x) >> 5), int((nct * blockDim.x) >> 5), int(threadIdx.x & 31)};
+    const int last = P.count - 1;
+    for (int l = 0; l < last; ++l) {
+        const MgLevelDev& L = P.lv[l];
+        for (int sweep = 0; sweep < 2; ++sweep) {
+            smooth_rows<true>(L, (l == 0 && sweep == 0) ? r0 : nullptr, 0, sweep == 0, W);
+            cluster_sync_all();
+            smooth_rows<true>(L, nullptr, 1, false, W);
+            cluster_sync_all();
+        }
+        restrict_rows<true>(L, P.lv[l + 1], W);
+        cluster_sync_all();
+    }
+    {
+        const MgLevelDev& C = P.lv[last];
+        const int M = C.cells;
+        const double* src = last == 0 ? r0 : nullptr;
+        for (int c = threadIdx.x; c < M; c += blockDim.x) bs[c] = src ? src[c] : double(__ldcg(C.b + c));
+        __syncthreads();
+        const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+        for (int row = int(rank) * warps + (threadIdx.x >> 5); row < M; row += int(nct) * warps) {
+            const double* g = G + size_t(row) * M;
+            double acc = 0.0;
+            for (int c = lane; c < M; c += 32) acc += __ldcg(g + c) * bs[c];
+            for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+            if (lane == 0) C.x[row] = float(acc);
+        }
+        cluster_sync_all();
+    }
+    for (int l = last - 1; l >= 0; --l) {
+        const MgLevelDev& L = P.lv[l];
+        prolong_black_rows<true>(L, P.lv[l + 1], W);
+        cluster_sync_all();
+        smooth_rows<true>(L, nullptr, 0, false, W);
+        cluster_sync_all();
+        smooth_rows<true>(L, nullptr, 1, false, W);
+        cluster_sync_all();
+        if (!(l == 0 && skip_last_red)) {
+            smooth_rows<true>(L, nullptr, 0, false, W);
+            cluster_sync_all();
+        }
+    }
 }
 
 // ------------------------------------------------------------ host side
@@ -331,15 +369,47 @@ int Multigrid::init(const GridDev& g, cudaStream_t s) {
     RB200_CUDA(cudaMemcpyAsync(dense_, G.data(), G.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     RB200_CUDA(cudaStreamSynchronize(s));
     const int nl = int(levels_.size());
-    bottom_first_ = nl - 1;
-    while (bottom_first_ > 0 && levels_[bottom_first_ - 1].cells <= kMgBottomCells &&
-           (nl - 1) - (bottom_first_ - 1) <= kMgMaxBottom)
-        --bottom_first_;
+    lower_first_ = nl - 1;
+    while (lower_first_ > 0 && levels_[lower_first_ - 1].cells <= kMgLowerCells) --lower_first_;
+    if (nl - lower_first_ > kMgMaxLower) {
+        set_error("multigrid hierarchy too deep for one cluster kernel");
+        return RB200_UNSUPPORTED;
+    }
+    // The largest cluster the device schedules for the lower-level kernel:
+    // 16 CTAs (non-portable) where available, else 8.
+    RB200_CUDA(cudaFuncSetAttribute(k_mg_lower, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cluster_ = 0;
+    for (int cl : {16, 8, 4, 2, 1}) {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(unsigned(cl), 1, 1);
+        cfg.blockDim = dim3(MG_LOWER_THREADS, 1, 1);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = unsigned(cl);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, k_mg_lower, &cfg) == cudaSuccess && clusters >= 1) {
+            cluster_ = cl;
+            break;
+        }
+        cudaGetLastError();
+    }
+    if (!cluster_) {
+        set_error("no thread-block cluster fits the multigrid lower-level kernel");
+        return RB200_UNSUPPORTED;
+    }
     return RB200_OK;
 }
 
-static int mg_blocks(long work) {
-    long b = (work + MG_THREADS - 1) / MG_THREADS;
+// Blocks of a level loop: one warp per row (j, k) of the level, at most 16
+// blocks per SM.
+static int row_blocks(const MgLevelDev& L) {
+    const long rows = long(L.n[1]) * L.n[2];
+    const long per_block = MG_THREADS / 32;
+    long b = (rows + per_block - 1) / per_block;
     if (b < 1) b = 1;
     return int(b < 148 * 16 ? b : 148 * 16);
 }
@@ -347,42 +417,45 @@ static int mg_blocks(long work) {
 int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_t s) const {
     const SolveState* st = static_cast<const SolveState*>(state);
     const int nl = int(levels_.size());
-    const MgLevelDev& C = levels_[nl - 1];
-    const int dense_blocks = (C.cells + 7) / 8;
-    if (nl == 1) {
-        k_mg_dense<<<dense_blocks, 256, 0, s>>>(C, dense_, r, st, mode);
-        return 1;
-    }
     int launches = 0;
     // Descent on the large levels.
-    for (int l = 0; l < bottom_first_; ++l) {
+    for (int l = 0; l < lower_first_; ++l) {
         const MgLevelDev& L = levels_[l];
-        const int pb = mg_blocks(mg_pairs(L));
+        const int pb = row_blocks(L);
         for (int sweep = 0; sweep < 2; ++sweep) {
             k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, (l == 0 && sweep == 0) ? r : nullptr, 0, sweep == 0, st, mode);
             k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 1, 0, st, mode);
         }
-        k_mg_restrict<<<mg_blocks(levels_[l + 1].cells), MG_THREADS, 0, s>>>(L, levels_[l + 1], st, mode);
+        k_mg_restrict<<<row_blocks(levels_[l + 1]), MG_THREADS, 0, s>>>(L, levels_[l + 1], st, mode);
         launches += 5;
     }
-    MgBottom B{};
-    B.count = (nl - 1) - bottom_first_;
-    for (int q = 0; q <= B.count; ++q) B.lv[q] = levels_[bottom_first_ + q];
-    if (B.count > 0) {
-        k_mg_bottom_down<<<1, MG_BOTTOM_THREADS, 0, s>>>(B, bottom_first_ == 0 ? r : nullptr, st, mode);
-        launches += 1;
-    }
-    k_mg_dense<<<dense_blocks, 256, 0, s>>>(C, dense_, nullptr, st, mode);
-    launches += 1;
-    if (B.count > 0) {
-        k_mg_bottom_up<<<1, MG_BOTTOM_THREADS, 0, s>>>(B, bottom_first_ == 0 ? 1 : 0, st, mode);
+    // The lower levels, coarsest solve included, in one cluster.
+    MgLower P{};
+    P.count = nl - lower_first_;
+    for (int q = 0; q < P.count; ++q) P.lv[q] = levels_[lower_first_ + q];
+    {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(unsigned(cluster_), 1, 1);
+        cfg.blockDim = dim3(MG_LOWER_THREADS, 1, 1);
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = unsigned(cluster_);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const double* r0 = lower_first_ == 0 ? r : nullptr;
+        const double* G = dense_;
+        const int skip = (lower_first_ == 0 && nl > 1) ? 1 : 0;
+        cudaLaunchKernelEx(&cfg, k_mg_lower, P, r0, G, st, mode, skip);
         launches += 1;
     }
     // Ascent on the large levels; the finest level's last red half-sweep is
     // fused by the caller into its finish kernel.
-    for (int l = bottom_first_ - 1; l >= 0; --l) {
+    for (int l = lower_first_ - 1; l >= 0; --l) {
         const MgLevelDev& L = levels_[l];
-        const int pb = mg_blocks(mg_pairs(L));
+        const int pb = row_blocks(L);
         k_mg_prolong_black<<<pb, MG_THREADS, 0, s>>>(L, levels_[l + 1], st, mode);
         k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 0, 0, st, mode);
         k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 1, 0, st, mode);
@@ -407,33 +480,38 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int 
     __shared__ BlockReduce<2, 0> red;
     if (!gate(st->flags, mode)) return;
     Neu rz, zq;
-    const long pairs = mg_pairs(L);
-    for (long t = blockIdx.x * long(blockDim.x) + threadIdx.x; t < pairs; t += long(gridDim.x) * blockDim.x) {
-        int i, j, k;
-        pair_cell(L, t, 0, i, j, k);
-        const int row = L.n[0] * (j + L.n[1] * k);
-        const int ib = i ^ 1;
-        if (ib < L.n[0]) {  // the black cell of the pair: its value is final
-            const int c = ib + row;
-            const double zc = c == 0 ? 0.0 : double(L.x[c]);
-            z[c] = zc;
-            if (c != 0) {
-                rz.add(r[c] * zc);
-                if (mode == MODE_ITER) zq.add(zc * q[c]);
+    const Warps W = grid_warps();
+    const int hx = (L.n[0] + 1) >> 1;
+    const int rows = L.n[1] * L.n[2];
+    for (int rw = W.w0; rw < rows; rw += W.nw) {
+        const int j = rw % L.n[1], k = rw / L.n[1];
+        const int row = L.n[0] * rw;
+        const int par = (j + k) & 1;
+        for (int m = W.lane; m < hx; m += 32) {
+            const int i = 2 * m + par;  // the red cell of the pair
+            const int ib = i ^ 1;
+            if (ib < L.n[0]) {  // the black cell of the pair: its value is final
+                const int c = ib + row;
+                const double zc = c == 0 ? 0.0 : double(L.x[c]);
+                z[c] = zc;
+                if (c != 0) {
+                    rz.add(r[c] * zc);
+                    if (mode == MODE_ITER) zq.add(zc * q[c]);
+                }
             }
-        }
-        if (i < L.n[0]) {
-            const int c = i + row;
-            float xv = L.x[c];
-            if (smooth) {
-                xv = gs_value(L, L.b[c], i, j, k, c);
-                L.x[c] = xv;
-            }
-            const double zc = c == 0 ? 0.0 : double(xv);
-            z[c] = zc;
-            if (c != 0) {
-                rz.add(r[c] * zc);
-                if (mode == MODE_ITER) zq.add(zc * q[c]);
+            if (i < L.n[0]) {
+                const int c = i + row;
+                float xv = L.x[c];
+                if (smooth) {
+                    xv = gs_value<false>(L, L.b[c], i, j, k, c);
+                    L.x[c] = xv;
+                }
+                const double zc = c == 0 ? 0.0 : double(xv);
+                z[c] = zc;
+                if (c != 0) {
+                    rz.add(r[c] * zc);
+                    if (mode == MODE_ITER) zq.add(zc * q[c]);
+                }
             }
         }
     }
@@ -449,7 +527,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int 
 int Multigrid::enqueue_finish(void* state, double* z, const double* r, const double* q, int mode, Partials part,
                               rb200_trace* trace, cudaStream_t s) const {
     const MgLevelDev& L = levels_[0];
-    int pb = mg_blocks(mg_pairs(L));
+    int pb = row_blocks(L);
     if (pb > 148 * 8) pb = 148 * 8;  // reduction partials capacity
     k_mg_finish_red<<<pb, MG_THREADS, 0, s>>>(L, levels_.size() > 1 ? 1 : 0, static_cast<SolveState*>(state), z, r,
                                               q, mode, part, trace);

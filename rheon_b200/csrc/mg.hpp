@@ -12,11 +12,12 @@
 // fixed symmetric operator up to FP32 rounding; the outer FP64 flexible CG
 // absorbs the rest.
 //
-// Launch structure of one cycle: grid-wide kernels for the levels above 4096
-// cells, one single-block kernel for the whole descent and one for the ascent
-// through the levels of at most 4096 cells, a many-block dense coarse solve.
-// The last red half-sweep of the finest level is left to the caller, which
-// fuses it with the outer method's dot products (k_mg_finish_red).
+// Launch structure of one cycle: grid-wide kernels for the levels above 32^3
+// cells; one kernel on a thread-block cluster (16 CTAs where the device
+// schedules them) for every level of at most 32^3 cells, the dense coarsest
+// solve included, whose half-sweeps meet at hardware cluster barriers. The
+// last red half-sweep of the finest level is left to the caller, which fuses
+// it with the outer method's dot products (k_mg_finish_red).
 #pragma once
 
 #include <vector>
@@ -36,12 +37,13 @@ struct MgLevelDev {
     float* b;         // right-hand side (FP32); level 0's is f32(r)
 };
 
-constexpr int kMgBottomCells = 4096;   // levels handled by single-block kernels
-constexpr int kMgMaxBottom = 6;
+constexpr int kMgLowerCells = 32768;   // levels of at most 32^3 cells: one cluster kernel
+constexpr int kMgMaxLower = 16;
 
-struct MgBottom {
-    MgLevelDev lv[kMgMaxBottom + 1];   // bottom levels and the coarsest level
-    int count;                         // bottom levels (excluding the coarsest)
+// The levels handled by the cluster kernel, the coarsest last.
+struct MgLower {
+    MgLevelDev lv[kMgMaxLower];
+    int count;
 };
 
 class Multigrid {
@@ -68,7 +70,8 @@ public:
 private:
     std::vector<MgLevelDev> levels_;
     double* dense_ = nullptr;   // coarsest-grid pseudo-inverse, cells x cells (FP64)
-    int bottom_first_ = 0;      // first level handled by the single-block kernels
+    int lower_first_ = 0;       // first level handled by the cluster kernel
+    int cluster_ = 0;           // CTAs of that kernel's cluster
     size_t bytes_ = 0;
 };
 
