@@ -37,6 +37,7 @@ LENGTH_MISMATCH = 18
 INVALID_GEOMETRY = 19
 INVALID_TIME_STEP = 20
 NONFINITE_POSITION = 21
+INVALID_INITIAL_PRESSURE = 22
 
 JACOBI_PCG_V1 = 0
 SGS_PCG_V1 = 1
@@ -154,6 +155,11 @@ def _declare(L):
     L.orc_max_abs.restype = C.c_double
     L.orc_carrier_step_f32.argtypes = [C.POINTER(Grid), C.POINTER(StepParams), _P, _P, _P, _P, C.POINTER(StepReport)]
     L.orc_carrier_step_f64.argtypes = [C.POINTER(Grid), C.POINTER(StepParams), _P, _P, _P, _P, C.POINTER(StepReport)]
+    L.orc_solve_rhs_initial.argtypes = [C.POINTER(Grid), C.c_double, C.c_int, _P, _P, C.c_double,
+                                        C.POINTER(Settings), _P, C.POINTER(Report), _P, C.c_size_t, C.c_int]
+    for name in ("orc_carrier_step_seeded_f32", "orc_carrier_step_seeded_f64"):
+        getattr(L, name).argtypes = [C.POINTER(Grid), C.POINTER(StepParams), _P, _P, _P, _P, _P, _P,
+                                     C.POINTER(StepReport)]
 
 
 def grid(counts, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0)) -> Grid:
@@ -300,14 +306,19 @@ class SolveResult:
     trace: list
 
 
-def solve_rhs(g, density, method, rhs, dt, s: Settings, trace=False, threads=1) -> SolveResult:
+def solve_rhs(g, density, method, rhs, dt, s: Settings, trace=False, threads=1, initial=None) -> SolveResult:
+    """solve_rhs, or solve_rhs_with_initial_pressure when `initial` is given."""
     rhs = _f64(rhs)
     p = np.zeros(cell_len(g), np.float64)
     rep = Report()
     cap = int(s.max_iterations) if trace else 0
     tr = (Trace * max(cap, 1))()
-    st = lib().orc_solve_rhs(C.byref(g), density, method, _ptr(rhs), dt, C.byref(s), _ptr(p), C.byref(rep),
-                             C.cast(tr, C.c_void_p) if cap else None, cap, threads)
+    init = None if initial is None else _f64(initial)
+    if init is not None and init.size != rhs.size:
+        return SolveResult(LENGTH_MISMATCH, p, rep, [])
+    st = lib().orc_solve_rhs_initial(C.byref(g), density, method, _ptr(rhs), _ptr(init) if init is not None else None,
+                                     dt, C.byref(s), _ptr(p), C.byref(rep), C.cast(tr, C.c_void_p) if cap else None,
+                                     cap, threads)
     return SolveResult(st, p, rep, [tr[i] for i in range(cap)] if cap else [])
 
 
@@ -329,12 +340,18 @@ def velocity_rate(g, faces):
     return st, out.value
 
 
-def carrier_step(g, faces, params: StepParams, tracer=None):
-    """One carrier step in place on copies; returns (status, faces, tracer, StepReport)."""
+def carrier_step(g, faces, params: StepParams, tracer=None, initial=None, keep_pressure=False):
+    """One carrier step in place on copies; returns (status, faces, tracer,
+    StepReport), plus the step's pressure when keep_pressure. `initial` seeds
+    the solve (solve_rhs_with_initial_pressure)."""
     fs = [np.array(f, copy=True, order="C") for f in faces]
     tr = None if tracer is None else np.array(tracer, dtype=np.float32, copy=True)
     rep = StepReport()
-    fn = lib().orc_carrier_step_f32 if fs[0].dtype == np.float32 else lib().orc_carrier_step_f64
+    init = None if initial is None else _f64(initial)
+    pout = np.zeros(cell_len(g), np.float64) if keep_pressure else None
+    fn = lib().orc_carrier_step_seeded_f32 if fs[0].dtype == np.float32 else lib().orc_carrier_step_seeded_f64
     st = fn(C.byref(g), C.byref(params), *[_ptr(f) for f in fs], _ptr(tr) if tr is not None else None,
-            C.byref(rep))
+            _ptr(init) if init is not None else None, _ptr(pout) if pout is not None else None, C.byref(rep))
+    if keep_pressure:
+        return st, fs, tr, rep, pout
     return st, fs, tr, rep

@@ -624,9 +624,12 @@ int true_report(const Grid& g, const Operator& op, const double* pressure, Works
 }
 
 // solve_loaded (src/pressure.rs:577-740) with a cold start (p = 0).
+// `initial`, when not null, is the caller's initial pressure
+// (solve_*_with_initial_pressure, feature "accepted-pressure-warm-start",
+// src/pressure.rs:395-430 and :615-624, :697-704).
 int solve_loaded(const Grid& g, const Operator& op, int method, Workspace& w, double* pressure,
                  double dt, const orc_settings& s, orc_report* rep, orc_trace* trace, size_t cap,
-                 int threads) {
+                 int threads, const double* initial) {
     const int64_t n = g.cells;
     if (!std::isfinite(dt) || dt <= 0.0) return ORC_INVALID_ARGUMENT;
     const double vals[3] = {s.relative_residual, s.absolute_residual, s.divergence_limit};
@@ -646,7 +649,15 @@ int solve_loaded(const Grid& g, const Operator& op, int method, Workspace& w, do
         rep->incompatible_budget = budget;
         return ORC_INCOMPATIBLE_RHS;
     }
-    std::fill(pressure, pressure + n, 0.0);
+    if (initial) {
+        // operator.validate_cells(initial), then the sealed gauge p[0] == 0.
+        for (int64_t i = 0; i < n; ++i)
+            if (!std::isfinite(initial[i])) return ORC_NONFINITE_INPUT;
+        if (initial[0] != 0.0) return ORC_INVALID_INITIAL_PRESSURE;
+        std::copy(initial, initial + n, pressure);
+    } else {
+        std::fill(pressure, pressure + n, 0.0);
+    }
     double rhs_l2 = std::sqrt(dot(w.rhs.data(), w.rhs.data(), n));
     double threshold = fmax_r(s.absolute_residual, s.relative_residual * rhs_l2);
     if (!std::isfinite(rhs_l2) || !std::isfinite(threshold)) {
@@ -699,7 +710,11 @@ int solve_loaded(const Grid& g, const Operator& op, int method, Workspace& w, do
             if ((st = true_report(g, op, pressure, w, dt, it, rep, threads))) return st;
             if (tr) tr->checked = 1;
             if (accepted(*rep)) return ORC_OK;
-            if (rep->true_residual_l2 > threshold) {
+            // A seeded solve judges the restart without the gauge row
+            // (src/pressure.rs:697-704).
+            double replacement_l2 = rep->true_residual_l2;
+            if (initial) replacement_l2 = std::sqrt(dot(w.product.data() + 1, w.product.data() + 1, n - 1));
+            if (replacement_l2 > threshold) {
                 std::copy(w.product.begin(), w.product.end(), w.residual.begin());
                 replaced = true;
             }
@@ -764,7 +779,7 @@ int apply_buoyancy(const Grid& g, T* v, const float* tracer, double gb, double d
 
 template <class T>
 int carrier_step(const Grid& g, const orc_step_params* prm, T* u, T* v, T* w, float* tracer,
-                 orc_step_report* rep) {
+                 orc_step_report* rep, const double* initial, double* pressure_out) {
     std::memset(rep, 0, sizeof(*rep));
     Operator op;
     int st = make_operator(g, prm->density, &op);
@@ -786,8 +801,9 @@ int carrier_step(const Grid& g, const orc_step_params* prm, T* u, T* v, T* w, fl
     if ((st = build_rhs<T>(g, op, cand, prm->dt, ws.rhs.data()))) return st;
     std::vector<double> pressure(g.cells, 0.0);
     st = solve_loaded(g, op, prm->method, ws, pressure.data(), prm->dt, prm->settings,
-                      &rep->pressure, nullptr, 0, prm->threads);
+                      &rep->pressure, nullptr, 0, prm->threads, initial);
     rep->pressure_status = st;
+    if (pressure_out) std::copy(pressure.begin(), pressure.end(), pressure_out);
     if (st && !(st == ORC_ITERATION_LIMIT && prm->iteration_limit_ok)) {
         std::copy(nu.begin(), nu.end(), u);
         std::copy(nv.begin(), nv.end(), v);
@@ -977,6 +993,15 @@ int orc_precondition(const orc_grid* in, double density, int method, double* r, 
 int orc_solve_rhs(const orc_grid* in, double density, int method, const double* rhs, double dt,
                   const orc_settings* s, double* pressure_out, orc_report* report,
                   orc_trace* trace, size_t trace_capacity, int threads) {
+    return orc_solve_rhs_initial(in, density, method, rhs, nullptr, dt, s, pressure_out, report, trace,
+                                 trace_capacity, threads);
+}
+
+// PressureWorkspace::solve_rhs_with_initial_pressure (src/pressure.rs:415-430);
+// initial == NULL is solve_rhs.
+int orc_solve_rhs_initial(const orc_grid* in, double density, int method, const double* rhs,
+                          const double* initial, double dt, const orc_settings* s, double* pressure_out,
+                          orc_report* report, orc_trace* trace, size_t trace_capacity, int threads) {
     std::memset(report, 0, sizeof(*report));
     Grid g;
     Operator op;
@@ -990,7 +1015,7 @@ int orc_solve_rhs(const orc_grid* in, double density, int method, const double* 
     w.product.assign(g.cells, 0.0);
     w.pre.assign(g.cells, 0.0);
     return solve_loaded(g, op, method, w, pressure_out, dt, *s, report, trace, trace_capacity,
-                        threads < 1 ? 1 : threads);
+                        threads < 1 ? 1 : threads, initial);
 }
 
 // ProviderWorkspace::solve_observed qualification (src/solver_provider.rs:239-270).
@@ -1051,18 +1076,30 @@ double orc_max_abs(const double* values, size_t n) {
 
 int orc_carrier_step_f32(const orc_grid* in, const orc_step_params* prm, float* u, float* v,
                          float* w, float* tracer, orc_step_report* rep) {
-    Grid g;
-    int st = make_grid(in, &g);
-    if (st) return st;
-    return carrier_step<float>(g, prm, u, v, w, tracer, rep);
+    return orc_carrier_step_seeded_f32(in, prm, u, v, w, tracer, nullptr, nullptr, rep);
 }
 
 int orc_carrier_step_f64(const orc_grid* in, const orc_step_params* prm, double* u, double* v,
                          double* w, float* tracer, orc_step_report* rep) {
+    return orc_carrier_step_seeded_f64(in, prm, u, v, w, tracer, nullptr, nullptr, rep);
+}
+
+int orc_carrier_step_seeded_f32(const orc_grid* in, const orc_step_params* prm, float* u, float* v,
+                                float* w, float* tracer, const double* initial, double* pressure_out,
+                                orc_step_report* rep) {
     Grid g;
     int st = make_grid(in, &g);
     if (st) return st;
-    return carrier_step<double>(g, prm, u, v, w, tracer, rep);
+    return carrier_step<float>(g, prm, u, v, w, tracer, rep, initial, pressure_out);
+}
+
+int orc_carrier_step_seeded_f64(const orc_grid* in, const orc_step_params* prm, double* u, double* v,
+                                double* w, float* tracer, const double* initial, double* pressure_out,
+                                orc_step_report* rep) {
+    Grid g;
+    int st = make_grid(in, &g);
+    if (st) return st;
+    return carrier_step<double>(g, prm, u, v, w, tracer, rep, initial, pressure_out);
 }
 
 }  // extern "C"

@@ -57,6 +57,7 @@ enum {
     ORC_INVALID_GEOMETRY = 19,
     ORC_INVALID_TIME_STEP = 20,
     ORC_NONFINITE_POSITION = 21,
+    ORC_INVALID_INITIAL_PRESSURE = 22,  /* PressureError::InvalidInitialPressure */
 };
 
 typedef struct orc_grid {
@@ -144,6 +145,10 @@ int orc_precondition(const orc_grid* g, double density, int method, double* r, d
 int orc_solve_rhs(const orc_grid* g, double density, int method, const double* rhs, double dt,
                   const orc_settings* s, double* pressure_out, orc_report* report,
                   orc_trace* trace, size_t trace_capacity, int threads);
+/* solve_rhs_with_initial_pressure (seeded PCG); initial == NULL is solve_rhs. */
+int orc_solve_rhs_initial(const orc_grid* g, double density, int method, const double* rhs,
+                          const double* initial, double dt, const orc_settings* s, double* pressure_out,
+                          orc_report* report, orc_trace* trace, size_t trace_capacity, int threads);
 
 /* ProviderWorkspace host qualification of a supplied pressure candidate.
  * Returns ORC_OK, ORC_NONFINITE_OUTPUT, ORC_NONZERO_GAUGE or ORC_QUALITY_GATE;
@@ -188,6 +193,14 @@ int orc_carrier_step_f32(const orc_grid* g, const orc_step_params* prm, float* u
                          float* w, float* tracer, orc_step_report* rep);
 int orc_carrier_step_f64(const orc_grid* g, const orc_step_params* prm, double* u, double* v,
                          double* w, float* tracer, orc_step_report* rep);
+/* The same step with the solve seeded by `initial` (NULL: cold), the step's
+ * pressure copied to `pressure_out` (NULL: not kept). */
+int orc_carrier_step_seeded_f32(const orc_grid* g, const orc_step_params* prm, float* u, float* v,
+                                float* w, float* tracer, const double* initial, double* pressure_out,
+                                orc_step_report* rep);
+int orc_carrier_step_seeded_f64(const orc_grid* g, const orc_step_params* prm, double* u, double* v,
+                                double* w, float* tracer, const double* initial, double* pressure_out,
+                                orc_step_report* rep);
 
 #ifdef __cplusplus
 }

@@ -419,3 +419,96 @@ def test_exact_candidate_qualifies_and_bad_ones_are_rejected(orc):
     assert st == O.NONZERO_GAUGE
     st, _ = O.qualify_pressure(g, 1.25, rhs, 0.01, s, np.zeros(24))
     assert st == O.QUALITY_GATE
+
+
+# ------------------------------------------------------------ pressure_initial_guess.rs
+# Seeded solves (solve_rhs_with_initial_pressure, feature
+# "accepted-pressure-warm-start"), both methods.
+METHODS = (O.JACOBI_PCG_V1, O.SGS_PCG_V1)
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_exact_and_approximate_guesses_recover_independent_chain(orc, method):
+    # tests/pressure_initial_guess.rs:17-52
+    g = O.grid([3, 1, 1])
+    r = O.solve_rhs(g, 1.0, method, [-4.0, 6.0, -2.0], 0.5, S(), initial=[0.0, 4.0, 2.0])
+    assert r.status == O.OK and r.report.iterations == 0 and r.report.true_residual_l2 == 0.0
+    r = O.solve_rhs(g, 1.0, method, [-4.0, 6.0, -2.0], 0.125, S(), initial=[0.0, 3.0, -1.0])
+    assert r.status == O.OK and r.report.iterations > 0
+    assert np.max(np.abs(r.pressure - [0.0, 4.0, 2.0])) < 1e-10
+
+
+def test_zero_rhs_still_checks_seed_and_current_rhs_threshold(orc):
+    # tests/pressure_initial_guess.rs:54-83
+    g = O.grid([3, 1, 1])
+    r = O.solve_rhs(g, 1.0, O.JACOBI_PCG_V1, [0.0] * 3, 1.0, O.settings(1.0, 0.0, 100.0, 0), initial=[0.0, 4.0, 2.0])
+    assert r.status == O.ITERATION_LIMIT and r.report.iterations == 0
+    r = O.solve_rhs(g, 1.0, O.JACOBI_PCG_V1, [0.0] * 3, 1.0, S(), initial=[0.0, 4.0, 2.0])
+    assert r.status == O.OK and r.report.iterations > 0
+    assert np.all(np.abs(r.pressure) < 1e-10)
+
+
+def test_full_gauge_row_and_compatibility_are_not_hidden_by_guess(orc):
+    # tests/pressure_initial_guess.rs:85-118
+    g = O.grid([4, 1, 1])
+    r = O.solve_rhs(g, 1.0, O.JACOBI_PCG_V1, [-0.003, 0.001, 0.001, 0.001], 1.0, O.settings(1.0, 1.0, 0.0015, 0),
+                    initial=[0.0] * 4)
+    assert r.status == O.ITERATION_LIMIT
+    r = O.solve_rhs(g, 1.0, O.JACOBI_PCG_V1, [1.0, 0.0, 0.0, 0.0], 1.0, S(), initial=[0.0] * 4)
+    assert r.status == O.INCOMPATIBLE_RHS
+
+
+def test_invalid_guesses_are_rejected(orc):
+    # tests/pressure_initial_guess.rs:120-172 (the seed validation part)
+    g = O.grid([3, 1, 1])
+    rhs = [-4.0, 6.0, -2.0]
+    assert O.solve_rhs(g, 1.0, 0, rhs, 0.5, S(), initial=[0.0, 1.0]).status == O.LENGTH_MISMATCH
+    assert O.solve_rhs(g, 1.0, 0, rhs, 0.5, S(), initial=[0.0, math.nan, 0.0]).status == O.NONFINITE_INPUT
+    assert O.solve_rhs(g, 1.0, 0, rhs, 0.5, S(), initial=[0.0, math.inf, 0.0]).status == O.NONFINITE_INPUT
+    assert O.solve_rhs(g, 1.0, 0, rhs, 0.5, S(), initial=[1.0, 4.0, 2.0]).status == O.INVALID_INITIAL_PRESSURE
+    seeded = O.solve_rhs(g, 1.0, 0, rhs, 0.5, S(), initial=[0.0, 3.0, -1.0])
+    again = O.solve_rhs(g, 1.0, 0, rhs, 0.5, S(), initial=[0.0, 3.0, -1.0])
+    assert seeded.report.iterations == again.report.iterations
+    assert np.array_equal(seeded.pressure, again.pressure)
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("seeded", [False, True])
+def test_neumann_cosine_refines_at_second_order_for_both_initializations(orc, method, seeded):
+    # tests/pressure_initial_guess.rs:175-218
+    previous = None
+    for n in (8, 16, 32, 64):
+        h = 1.0 / n
+        g = O.grid([n, 1, 1], [h, 1.0, 1.0])
+        x = (np.arange(n) + 0.5) * h
+        cosine = np.cos(math.pi * x)
+        rhs = h * math.pi * math.pi * cosine
+        seed = 0.75 * (cosine - cosine[0])
+        r = O.solve_rhs(g, 1.0, method, rhs, 0.125, S(), initial=seed if seeded else None)
+        assert r.status == O.OK
+        eigen = 4.0 * math.sin(math.pi * h / 2.0) ** 2 / (h * h)
+        continuum = cosine - cosine[0]
+        discrete = math.pi * math.pi / eigen * continuum
+        assert np.max(np.abs(r.pressure - discrete)) < 1e-8
+        error = np.max(np.abs(r.pressure - continuum))
+        if previous is not None:
+            assert 3.8 <= previous / error <= 4.2
+        previous = error
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_seeded_chain_retains_full_gauge_acceptance(orc, method):
+    # tests/pressure_initial_guess.rs:220-253
+    n = 64
+    g = O.grid([n, 1, 1])
+    seed = np.array([i * (2 * n - 1 - i) * 0.1e-5 for i in range(n)])
+    s = O.settings(0.0, 1e-4, 1e-4, 100)
+    r = O.solve_rhs(g, 1.0, method, np.zeros(n), 1.0, s, initial=seed)
+    assert r.status == O.OK and r.report.iterations > 0
+    assert r.report.true_residual_l2 <= 1e-4
+    p = r.pressure
+    squared = p[1] * p[1]
+    for i in range(1, n):
+        res = p[i] - p[i - 1] if i == n - 1 else 2.0 * p[i] - p[i - 1] - p[i + 1]
+        squared += res * res
+    assert math.sqrt(squared) <= 1e-4
