@@ -58,7 +58,8 @@ typedef enum rb200_status {
     RB200_DIVERGENCE_LIMIT = 15,     /* SimulationError::DivergenceLimit          */
     RB200_COURANT_LIMIT = 16,        /* SimulationError::CourantLimit             */
     RB200_NO_DEVICE = 17,            /* no usable sm_100 device                   */
-    RB200_LENGTH_MISMATCH = 18       /* OperatorError::LengthMismatch             */
+    RB200_LENGTH_MISMATCH = 18,      /* OperatorError::LengthMismatch             */
+    RB200_INVALID_INITIAL_PRESSURE = 22 /* PressureError::InvalidInitialPressure  */
 } rb200_status;
 
 /* Pressure methods. JACOBI_PCG_V1 reproduces "jacobi-pcg-v1"
@@ -198,6 +199,14 @@ RB200_API void* rb200_workspace_stream(rb200_workspace* ws);
 RB200_API int rb200_workspace_solve_rhs(rb200_workspace* ws, const double* rhs, size_t len, double dt,
                               const rb200_settings* settings, rb200_report* report,
                               rb200_cancel_fn cancelled, void* ctx);
+/* PressureWorkspace::solve_rhs_with_initial_pressure (src/pressure.rs:415-430,
+ * feature "accepted-pressure-warm-start"): PCG seeded by `initial` (len
+ * values, finite, initial[0] == 0, else RB200_NONFINITE_INPUT or
+ * RB200_INVALID_INITIAL_PRESSURE). rhs and initial may be host or device
+ * memory (the copy direction is inferred). */
+RB200_API int rb200_workspace_solve_rhs_initial(rb200_workspace* ws, const double* rhs, const double* initial,
+                                                size_t len, double dt, const rb200_settings* settings,
+                                                rb200_report* report, rb200_cancel_fn cancelled, void* ctx);
 /* Same on a device-resident RHS (len doubles on the workspace's device). The
  * workspace works on its own stream: the RHS must be complete when called. */
 RB200_API int rb200_workspace_solve_rhs_device(rb200_workspace* ws, const double* rhs_device, size_t len,
@@ -296,6 +305,9 @@ typedef struct rb200_carrier_config {
     int with_tracer;               /* allocate a cell tracer (f32)         */
     int device;
     int fp32_advection;            /* sample/backtrace in FP32 arithmetic  */
+    int warm_start;                /* PressureInitializationPolicy: 0 Cold, 1 AcceptedPreviousV1
+                                      (src/pressure_initialization.rs:7-12): seed each
+                                      solve with the last accepted step's pressure */
 } rb200_carrier_config;
 
 typedef struct rb200_step_params {
@@ -318,6 +330,8 @@ typedef struct rb200_step_report {
     double velocity_rate;
     double pressure_ms;    /* device time of the pressure solve (CUDA events) */
     uint64_t kernel_launches; /* kernels this step launched (graph nodes included) */
+    int pressure_initialization; /* the policy this step's solve actually used: 0 cold,
+                                    1 seeded by the accepted previous pressure */
 } rb200_step_report;
 
 RB200_API int rb200_carrier_create(const rb200_carrier_config* config, rb200_carrier** out);

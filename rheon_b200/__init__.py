@@ -339,11 +339,37 @@ class PressureWorkspace:
         return [self._trace[i] for i in range(min(count, len(self._trace)))]
 
     def solve_rhs(self, operator: PressureOperator, rhs, dt: float, settings: PressureSettings,
-                  cancelled: Optional[Callable[[], bool]] = None) -> PressureReport:
+                  cancelled: Optional[Callable[[], bool]] = None, initial=None) -> PressureReport:
+        """solve_rhs (src/pressure.rs:365-393); with `initial`,
+        solve_rhs_with_initial_pressure (:415-430): PCG seeded by the given
+        pressure (finite, initial[0] == 0)."""
         if operator.density != self._density:
             self._create(operator.density)
         rep = N.Report()
         cb = _cancel_cb(cancelled)
+        if initial is not None:
+            keep = []
+
+            def ptr(a):
+                if hasattr(a, "data_ptr"):
+                    if hasattr(a, "device"):
+                        import torch
+
+                        torch.cuda.current_stream(a.device).synchronize()
+                    return _ptr(a), int(a.numel())
+                h = np.ascontiguousarray(a, dtype=np.float64)
+                keep.append(h)
+                return h.ctypes.data_as(C.c_void_p), h.size
+
+            (rp, n), (ip, ni) = ptr(rhs), ptr(initial)
+            if ni != n:
+                raise PressureError(N.LENGTH_MISMATCH)
+            st = lib().rb200_workspace_solve_rhs_initial(self._handle, rp, ip, n, dt, C.byref(settings.c()),
+                                                         C.byref(rep), cb, None)
+            self.last_report = PressureReport.from_c(rep)
+            if st != N.OK:
+                raise PressureError(st, rep)
+            return self.last_report
         if hasattr(rhs, "data_ptr"):
             # The workspace runs on its own stream: the producer of rhs must be done.
             if hasattr(rhs, "device"):
@@ -482,6 +508,10 @@ class CarrierConfig:
     with_tracer: bool = False
     device: int = 0
     fp32_advection: bool = False
+    # PressureInitializationPolicy (src/pressure_initialization.rs:7-12):
+    # False = Cold, True = AcceptedPreviousV1 (seed each solve with the last
+    # accepted step's pressure).
+    warm_start: bool = False
 
     @staticmethod
     def mixed(**kw) -> "CarrierConfig":
@@ -517,6 +547,7 @@ class StepReport:
     velocity_rate: float
     pressure_ms: float = 0.0
     kernel_launches: int = 0
+    pressure_initialization: int = 0   # the policy actually used: 0 cold, 1 accepted previous
 
 
 class CarrierSimulation:
@@ -529,7 +560,7 @@ class CarrierSimulation:
         c = N.CarrierConfig(grid.c(), config.density, 0 if config.storage == "f32" else 1,
                             int(config.implementation), config.pressure.c(), config.actual_divergence_limit,
                             config.max_courant, 1 if config.with_tracer else 0, config.device,
-                            1 if config.fp32_advection else 0)
+                            1 if config.fp32_advection else 0, 1 if config.warm_start else 0)
         h = C.c_void_p()
         st = lib().rb200_carrier_create(C.byref(c), C.byref(h))
         if st != N.OK:
@@ -629,7 +660,7 @@ class CarrierSimulation:
     def _report(r: N.StepReport) -> StepReport:
         return StepReport(r.dt, r.time, int(r.generation), PressureReport.from_c(r.pressure), r.pressure_status,
                           r.actual_divergence_max, r.courant, r.velocity_rate, r.pressure_ms,
-                          int(r.kernel_launches))
+                          int(r.kernel_launches), int(r.pressure_initialization))
 
     def step(self, params: StepParams, cancelled: Optional[Callable[[], bool]] = None) -> StepReport:
         """One step (one CUDA graph); raises SimulationError if it is rejected."""

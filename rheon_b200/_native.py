@@ -30,12 +30,14 @@ DIVERGENCE_LIMIT = 15
 COURANT_LIMIT = 16
 NO_DEVICE = 17
 LENGTH_MISMATCH = 18
+INVALID_INITIAL_PRESSURE = 22
 
 STATUS_NAMES = {
     0: "Ok", 1: "Unsupported", 2: "Execution", 3: "NonFiniteOutput", 4: "NonZeroGauge", 5: "QualityGate",
     6: "Cancelled", 7: "IterationLimit", 8: "Breakdown", 9: "AllocationFailed", 10: "InvalidArgument",
     11: "IncompatibleRhs", 12: "NonFiniteInput", 13: "NonZeroWallVelocity", 14: "ArithmeticFailure",
     15: "DivergenceLimit", 16: "CourantLimit", 17: "NoDevice", 18: "LengthMismatch",
+    22: "InvalidInitialPressure",
 }
 
 
@@ -78,7 +80,8 @@ class Metadata(C.Structure):
 class CarrierConfig(C.Structure):
     _fields_ = [("grid", Grid), ("density", C.c_double), ("storage", C.c_int), ("method", C.c_int),
                 ("settings", Settings), ("actual_divergence_limit", C.c_double), ("max_courant", C.c_double),
-                ("with_tracer", C.c_int), ("device", C.c_int), ("fp32_advection", C.c_int)]
+                ("with_tracer", C.c_int), ("device", C.c_int), ("fp32_advection", C.c_int),
+                ("warm_start", C.c_int)]
 
 
 class StepParams(C.Structure):
@@ -90,7 +93,7 @@ class StepReport(C.Structure):
     _fields_ = [("dt", C.c_double), ("time", C.c_double), ("generation", C.c_uint64), ("pressure", Report),
                 ("pressure_status", C.c_int), ("actual_divergence_max", C.c_double), ("courant", C.c_double),
                 ("velocity_rate", C.c_double), ("pressure_ms", C.c_double),
-                ("kernel_launches", C.c_uint64)]
+                ("kernel_launches", C.c_uint64), ("pressure_initialization", C.c_int)]
 
 
 CANCEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
@@ -117,6 +120,8 @@ SIGNATURES = {
     "rb200_workspace_allocated_bytes": (C.c_uint64, [_P]),
     "rb200_workspace_stream": (_P, [_P]),
     "rb200_workspace_solve_rhs": (_I, [_P, _P, _S, _D, C.POINTER(Settings), C.POINTER(Report), CANCEL_FN, _P]),
+    "rb200_workspace_solve_rhs_initial": (_I, [_P, _P, _P, _S, _D, C.POINTER(Settings), C.POINTER(Report),
+                                               CANCEL_FN, _P]),
     "rb200_workspace_solve_rhs_device": (_I, [_P, _P, _S, _D, C.POINTER(Settings), C.POINTER(Report), CANCEL_FN,
                                               _P]),
     "rb200_workspace_pressure": (_I, [_P, _P, _S]),

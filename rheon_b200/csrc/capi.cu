@@ -194,6 +194,7 @@ const char* rb200_status_string(int status) {
         case RB200_COURANT_LIMIT: return "Courant limit";
         case RB200_NO_DEVICE: return "no sm_100 device";
         case RB200_LENGTH_MISMATCH: return "field length does not match the grid";
+        case RB200_INVALID_INITIAL_PRESSURE: return "initial pressure requires a sealed operator and zero gauge";
         default: return "unknown status";
     }
 }
@@ -253,7 +254,7 @@ void* rb200_workspace_stream(rb200_workspace* ws) { return ws ? (void*)ws->strea
 
 static int workspace_solve(rb200_workspace* ws, const double* rhs, bool on_device, size_t len, double dt,
                            const rb200_settings* settings, rb200_report* report, rb200_cancel_fn cancelled,
-                           void* ctx) {
+                           void* ctx, const double* initial = nullptr) {
     if (!ws || !rhs || !settings) return RB200_INVALID_ARGUMENT;
     if (report) std::memset(report, 0, sizeof(*report));
     if (len != size_t(ws->g.cells)) return RB200_LENGTH_MISMATCH;
@@ -267,8 +268,8 @@ static int workspace_solve(rb200_workspace* ws, const double* rhs, bool on_devic
     }
     if (cancelled && cancelled(ctx)) return RB200_CANCELLED;
     RB200_CUDA(cudaMemcpyAsync(ws->solver.b(), rhs, len * sizeof(double),
-                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ws->stream));
-    int rc = ws->solver.solve(dt, *settings, report, cancelled, ctx);
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDefault, ws->stream));
+    int rc = ws->solver.solve(dt, *settings, report, cancelled, ctx, initial);
     if (rc == RB200_EXECUTION) ws->err = get_error();
     return rc;
 }
@@ -277,6 +278,13 @@ int rb200_workspace_solve_rhs(rb200_workspace* ws, const double* rhs, size_t len
                               const rb200_settings* settings, rb200_report* report, rb200_cancel_fn cancelled,
                               void* ctx) {
     return workspace_solve(ws, rhs, false, len, dt, settings, report, cancelled, ctx);
+}
+
+int rb200_workspace_solve_rhs_initial(rb200_workspace* ws, const double* rhs, const double* initial, size_t len,
+                                      double dt, const rb200_settings* settings, rb200_report* report,
+                                      rb200_cancel_fn cancelled, void* ctx) {
+    if (!initial) return RB200_INVALID_ARGUMENT;
+    return workspace_solve(ws, rhs, false, len, dt, settings, report, cancelled, ctx, initial);
 }
 
 int rb200_workspace_solve_rhs_device(rb200_workspace* ws, const double* rhs_device, size_t len, double dt,

@@ -45,6 +45,11 @@ struct CarrierDev {
     rb200_step_report report;
     int step_status;
     int trips;
+    // AcceptedPreviousV1 initialization (src/pressure_initialization.rs:7-12)
+    int warm_policy;     // configured policy
+    int history;         // an accepted pressure of this state exists
+    int warm;            // this step's solve is seeded
+    double* accepted_p;  // the last accepted step's pressure (device)
 };
 
 __device__ __forceinline__ bool step_running(const CarrierDev* cd) { return cd->status == STEP_RUNNING; }
@@ -69,6 +74,7 @@ __global__ void k_step_begin(CarrierDev* cd) {
         cd->status = RB200_INVALID_ARGUMENT;
         cd->skip = 1;
     }
+    cd->warm = (cd->warm_policy && cd->history) ? 1 : 0;
 }
 
 template <class T, class R>
@@ -156,8 +162,18 @@ __global__ void k_step_end(GridDev g, CarrierDev* cd, const SolveState* st) {
     }
     rep.time = cd->time;
     rep.generation = cd->generation;
+    rep.pressure_initialization = cd->warm;
     cd->step_status = status;
     cd->status = status;
+}
+
+// Keeps the pressure of an accepted step as the next step's seed; a rejected
+// step leaves the previous one in place.
+__global__ void __launch_bounds__(EW_THREADS) k_keep_pressure(GridDev g, CarrierDev* cd, const double* __restrict__ p) {
+    if (cd->step_status != RB200_OK) return;
+    double* dst = cd->accepted_p;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) dst[c] = p[c];
+    if (blockIdx.x == 0 && threadIdx.x == 0) cd->history = 1;
 }
 
 // Random-Fourier initial state on the device: u_d(x) = sum_m a_{m,d}
@@ -237,6 +253,7 @@ struct rb200_carrier {
     size_t elem = 4;
     void* faces[3][3] = {};
     float* tracer[2] = {nullptr, nullptr};
+    double* accepted_p = nullptr;   // warm start: the last accepted pressure
     PcgSolver solver;
     CarrierDev* cd = nullptr;      // device
     CarrierDev* h_cd = nullptr;    // pinned host mirror
@@ -254,6 +271,7 @@ struct rb200_carrier {
             for (auto& a : b) cudaFree(a);
         cudaFree(tracer[0]);
         cudaFree(tracer[1]);
+        cudaFree(accepted_p);
         cudaFree(cd);
         if (h_cd) cudaFreeHost(h_cd);
         for (auto& e : ev)
@@ -304,7 +322,9 @@ int capture_step(rb200_carrier* c) {
         k_carrier_advect<T, double><<<fb, ADV_THREADS, 0, s>>>(g, c->cd);
     k_carrier_rhs<T><<<cb, ADV_THREADS, 0, s>>>(g, c->cd, c->solver.b());
     RB200_CUDA(cudaEventRecordWithFlags(c->ev[0], s, cudaEventRecordExternal));
-    int rc = c->solver.enqueue_reset(&c->cd->dt, &c->cd->skip, c->cfg.settings, s);
+    int rc = c->accepted_p
+                 ? c->solver.enqueue_reset(&c->cd->dt, &c->cd->skip, c->cfg.settings, s, &c->cd->warm, c->accepted_p)
+                 : c->solver.enqueue_reset(&c->cd->dt, &c->cd->skip, c->cfg.settings, s);
     if (!rc) rc = c->solver.enqueue_loop(s, c->body_stream, c->cfg.settings);
     if (rc) {
         cudaGraph_t dummy = nullptr;
@@ -321,6 +341,7 @@ int capture_step(rb200_carrier* c) {
             k_carrier_tracer<T, double><<<cb, ADV_THREADS, 0, s>>>(g, c->cd, c->solver.state());
     }
     k_step_end<<<1, 1, 0, s>>>(g, c->cd, c->solver.state());
+    if (c->accepted_p) k_keep_pressure<<<eb, EW_THREADS, 0, s>>>(g, c->cd, c->solver.p());
     RB200_CUDA(cudaMemcpyAsync(c->h_cd, c->cd, sizeof(CarrierDev), cudaMemcpyDeviceToHost, s));
     cudaError_t le = cudaGetLastError();
     cudaError_t ee = cudaStreamEndCapture(s, &graph);
@@ -336,7 +357,8 @@ int capture_step(rb200_carrier* c) {
         return RB200_EXECUTION;
     }
     // begin, advect, rhs, reset (+start kernels counted by the solver), correct, tracer, end
-    c->fixed_nodes = 5 + (c->tracer[0] ? 1 : 0);
+    // (+ seed and keep kernels with the warm-start policy)
+    c->fixed_nodes = 5 + (c->tracer[0] ? 1 : 0) + (c->accepted_p ? 2 : 0);
     return RB200_OK;
 }
 
@@ -375,6 +397,9 @@ int upload_rate(rb200_carrier* c) {
     c->h_cd->generation = 0;
     c->h_cd->status = RB200_OK;
     c->h_cd->flags = 0;
+    // a new accepted state has no accepted pressure: the next seeded step
+    // starts cold (PressureColdReason::Invalidated, src/pressure_initialization.rs:31-36)
+    c->h_cd->history = 0;
     RB200_CUDA(cudaMemcpyAsync(c->cd, c->h_cd, sizeof(CarrierDev), cudaMemcpyHostToDevice, c->stream));
     RB200_CUDA(cudaStreamSynchronize(c->stream));
     return RB200_OK;
@@ -414,9 +439,16 @@ int rb200_carrier_create(const rb200_carrier_config* config, rb200_carrier** out
             c->bytes += size_t(g.cells) * 4;
             RB200_CUDA(cudaMemsetAsync(c->tracer[t], 0, size_t(g.cells) * 4, c->stream));
         }
+    if (config->warm_start != 0 && config->warm_start != 1) return RB200_INVALID_ARGUMENT;
+    if (config->warm_start) {
+        if (cudaMalloc(&c->accepted_p, size_t(g.cells) * sizeof(double)) != cudaSuccess) return RB200_OUT_OF_MEMORY;
+        c->bytes += size_t(g.cells) * sizeof(double);
+    }
     RB200_CUDA(cudaMalloc(&c->cd, sizeof(CarrierDev)));
     RB200_CUDA(cudaMallocHost(&c->h_cd, sizeof(CarrierDev)));
     std::memset(c->h_cd, 0, sizeof(CarrierDev));
+    c->h_cd->warm_policy = config->warm_start;
+    c->h_cd->accepted_p = c->accepted_p;
     for (int b = 0; b < 3; ++b)
         for (int a = 0; a < 3; ++a) c->h_cd->faces[b][a] = c->faces[b][a];
     c->h_cd->tracer[0] = c->tracer[0];

@@ -30,25 +30,33 @@ constexpr double kEps = 2.220446049250313e-16;
 
 // ------------------------------------------------------------------ init
 // Compatibility sums, threshold and the true report of p = 0
-// (src/pressure.rs:603-647). p is zeroed here.
+// (src/pressure.rs:603-647); p is zeroed here. A seeded solve (F_WARM) keeps p,
+// validates it after the compatibility check (finite, p[0] == 0,
+// :615-624) and leaves its true report to the true-residual kernel.
 __global__ void __launch_bounds__(EW) k_init_sums(GridDev g, SolveState* st, const double* __restrict__ b,
                                                   double* __restrict__ p, Partials part) {
-    __shared__ BlockReduce<3, 2> sm;
-    if (st->flags & F_DONE) return;
+    __shared__ BlockReduce<3, 3> sm;
+    const int flags0 = st->flags;
+    if (flags0 & F_DONE) return;
+    const bool warm = (flags0 & F_WARM) != 0;
     dd s[3] = {{0, 0}, {0, 0}, {0, 0}};
-    double m[2] = {0.0, 0.0};
+    double m[3] = {0.0, 0.0, 0.0};
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
         double x = b[c];
-        p[c] = 0.0;
+        if (warm) {
+            if (!isfinite(p[c])) m[2] = 1.0;
+        } else {
+            p[c] = 0.0;
+        }
         if (!isfinite(x)) m[1] = 1.0;
         s[0] = dd_add1(s[0], x);
         s[1] = dd_add1(s[1], fabs(x));
         s[2] = dd_add1(s[2], x * x);
         m[0] = fmax(m[0], fabs(x));
     }
-    block_reduce<3, 2>(sm, s, m);
-    if (publish_and_check_last<3, 2>(part, blockIdx.x, gridDim.x, s, m)) {
-        fold_partials<3, 2>(part, gridDim.x, sm, s, m);
+    block_reduce<3, 3>(sm, s, m);
+    if (publish_and_check_last<3, 3>(part, blockIdx.x, gridDim.x, s, m)) {
+        fold_partials<3, 3>(part, gridDim.x, sm, s, m);
         if (threadIdx.x == 0) {
             int flags = st->flags;
             if (m[1] != 0.0) {
@@ -67,6 +75,16 @@ __global__ void __launch_bounds__(EW) k_init_sums(GridDev g, SolveState* st, con
                 finish(st, RB200_INCOMPATIBLE_RHS, flags);
                 return;
             }
+            if (warm) {
+                if (m[2] != 0.0) {
+                    finish(st, RB200_NONFINITE_INPUT, flags);
+                    return;
+                }
+                if (p[0] != 0.0) {
+                    finish(st, RB200_INVALID_INITIAL_PRESSURE, flags);
+                    return;
+                }
+            }
             double rhs_l2 = sqrt(sq);
             double threshold = fmax(st->absolute, st->relative * rhs_l2);
             if (!isfinite(rhs_l2) || !isfinite(threshold)) {
@@ -74,6 +92,11 @@ __global__ void __launch_bounds__(EW) k_init_sums(GridDev g, SolveState* st, con
                 return;
             }
             st->threshold = threshold;
+            if (warm) {
+                // true_report(p0) runs next, in the true-residual kernel.
+                st->flags = flags | F_STOP | F_NEED_TRUE;
+                return;
+            }
             // true_report(p = 0): the product is exactly b.
             double div = m[0] * st->dt / g.volume;
             if (!isfinite(sq) || !isfinite(div)) {
@@ -354,7 +377,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_true_residual(GridDev g, Solve
                                                                 rb200_trace* trace) {
     using S = Slab<ZC>;
     extern __shared__ __align__(128) double smem[];
-    __shared__ BlockReduce<1, 1> red;
+    __shared__ BlockReduce<2, 1> red;
     __shared__ __align__(8) uint64_t bar;
     const int flags = st->flags;
     if (!(flags & F_NEED_TRUE)) return;
@@ -363,6 +386,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_true_residual(GridDev g, Solve
     stage_issue<ZC>(g, maps, &bar, smem, p, &maps.p, nullptr, nullptr, nullptr, x0, y0, k0);
     if (!stage_wait(maps, &bar, st)) return;
     Neu acc;
+    double gauge_sq = 0.0;  // t[0]^2 when this thread holds cell 0
     double mx[1] = {0.0};
     const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
     if (i < g.n[0] && j < g.n[1]) {
@@ -375,15 +399,17 @@ __global__ void __launch_bounds__(TILE_THREADS) k_true_residual(GridDev g, Solve
             double t = b[c] - apply_row(g, i, j, k0 + q, v);
             spare[c] = t;
             acc.add(t * t);
+            if (c == 0) gauge_sq = t * t;
             mx[0] = fmax(mx[0], fabs(t));
         }
     }
-    dd sums[1] = {acc.as_dd()};
-    block_reduce<1, 1>(red, sums, mx);
+    // the second sum leaves out the gauge row: |t[1..]|^2
+    dd sums[2] = {acc.as_dd(), dd_add1(acc.as_dd(), -gauge_sq)};
+    block_reduce<2, 1>(red, sums, mx);
     const int nb = nblocks3();
-    if (publish_and_check_last<1, 1>(part, block_id3(), nb, sums, mx)) {
-        fold_partials<1, 1>(part, nb, red, sums, mx);
-        if (tid3() == 0) decide_true(st, trace, dd_value(sums[0]), mx[0], flags, g.volume);
+    if (publish_and_check_last<2, 1>(part, block_id3(), nb, sums, mx)) {
+        fold_partials<2, 1>(part, nb, red, sums, mx);
+        if (tid3() == 0) decide_true(st, trace, dd_value(sums[0]), dd_value(sums[1]), mx[0], flags, g.volume);
     }
 }
 
@@ -555,8 +581,16 @@ __global__ void __launch_bounds__(EW) k_rbsgs_red_dot(GridDev g, SolveState* st,
 
 // ------------------------------------------------------------ graph embedding
 // Device-side reset of the solver state (what solve() uploads from the host).
+// The seeded start of the resident carrier: p = the accepted previous
+// pressure when `warm` is set.
+__global__ void __launch_bounds__(EW) k_seed_pressure(int n, double* __restrict__ p, const double* __restrict__ seed,
+                                                      const int* __restrict__ warm) {
+    if (!*warm) return;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) p[c] = seed[c];
+}
+
 __global__ void k_solve_reset(SolveState* st, rb200_settings s, const double* __restrict__ dt_dev,
-                              const int* __restrict__ skip, int flexible) {
+                              const int* __restrict__ skip, int flexible, const int* __restrict__ warm) {
     SolveState init{};
     init.dt = *dt_dev;
     init.relative = s.relative_residual;
@@ -565,6 +599,7 @@ __global__ void k_solve_reset(SolveState* st, rb200_settings s, const double* __
     init.max_it = s.max_iterations > 0x7fffffffull ? 0x7fffffff : int(s.max_iterations);
     init.status = ST_RUNNING;
     init.flexible = flexible;
+    if (warm && *warm != 0) init.flags = F_WARM;
     if (skip && *skip != 0) init.flags = F_DONE | F_STOP;
     *st = init;
 }
@@ -898,7 +933,8 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
         if ((rc = mg_.init(g, stream_))) return rc;
         bytes_ += mg_.bytes();
     }
-    if ((rc = alloc(&part_.data, size_t(part_blocks_) * 8))) return rc;
+    // up to 2K + M = 9 doubles per block (the init sums)
+    if ((rc = alloc(&part_.data, size_t(part_blocks_) * 12))) return rc;
     RB200_CUDA(cudaMalloc(&part_.ticket, sizeof(unsigned)));
     RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), stream_));
     RB200_CUDA(cudaMalloc(&st_, sizeof(SolveState)));
@@ -988,10 +1024,14 @@ int PcgSolver::record_flags(int slot) {
 }
 
 int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, rb200_cancel_fn cancelled,
-                     void* ctx) {
+                     void* ctx, const double* initial) {
     if (report) std::memset(report, 0, sizeof(*report));
     SolveState init = initial_state(dt, s);
     init.flexible = method_ == RB200_MG_MIXED ? 1 : 0;
+    if (initial) {
+        RB200_CUDA(cudaMemcpyAsync(p_, initial, size_t(g_.cells) * sizeof(double), cudaMemcpyDefault, stream_));
+        init.flags |= F_WARM;
+    }
     if (d_trace_ && uint64_t(init.max_it) > trace_cap_) {
         set_error("trace capacity is smaller than max_iterations");
         return RB200_INVALID_ARGUMENT;
@@ -1045,8 +1085,14 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
     return f.status;
 }
 
-int PcgSolver::enqueue_reset(const double* dt_dev, const int* skip, const rb200_settings& settings, cudaStream_t s) {
-    k_solve_reset<<<1, 1, 0, s>>>(st_, settings, dt_dev, skip, method_ == RB200_MG_MIXED ? 1 : 0);
+int PcgSolver::enqueue_reset(const double* dt_dev, const int* skip, const rb200_settings& settings, cudaStream_t s,
+                             const int* warm, const double* seed) {
+    if (warm && seed) {
+        k_seed_pressure<<<ew_blocks(g_.cells), EW, 0, s>>>(g_.cells, p_, seed, warm);
+        launches_ += 1;
+    }
+    k_solve_reset<<<1, 1, 0, s>>>(st_, settings, dt_dev, skip, method_ == RB200_MG_MIXED ? 1 : 0,
+                                  (warm && seed) ? warm : nullptr);
     RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), s));
     if (gbar_) RB200_CUDA(cudaMemsetAsync(gbar_, 0, sizeof(GridBarrier), s));
     launches_ += 1;

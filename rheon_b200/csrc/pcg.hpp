@@ -37,7 +37,8 @@ enum : int {
     F_REPLACED = 4,      // the next direction is z (fresh start)
     F_DONE = 8,          // solve finished; status is final
     F_NEED_REPLACE = 16, // replace r by the true residual, re-precondition
-    F_PROFILE = 64       // timing mode: passes do their work, decisions are skipped
+    F_PROFILE = 64,      // timing mode: passes do their work, decisions are skipped
+    F_WARM = 128         // seeded solve: p holds the caller's initial pressure
 };
 constexpr int ST_RUNNING = -1;
 
@@ -78,8 +79,10 @@ public:
     // Solve K p = b for the RHS already in b(). dt is the step's dt (for the
     // divergence gate). On return p() holds the iterate (also on
     // ITERATION_LIMIT). `status` receives the PressureError-style outcome.
+    // `initial` (host or device memory, g.cells values, or nullptr) seeds the
+    // solve: solve_*_with_initial_pressure (src/pressure.rs:395-430).
     int solve(double dt, const rb200_settings& s, rb200_report* report, rb200_cancel_fn cancelled,
-              void* ctx);
+              void* ctx, const double* initial = nullptr);
     double* b() { return b_; }
     double* p() { return p_; }
     double* scratch() { return d_[1]; }
@@ -99,7 +102,10 @@ public:
     // solver kernel is a no-op. enqueue_loop adds a WHILE conditional node that
     // repeats the iteration chunk until the state is done, with the trip count
     // bounded so that the loop always ends. Both run during a stream capture.
-    int enqueue_reset(const double* dt_dev, const int* skip, const rb200_settings& settings, cudaStream_t s);
+    // With `warm` (device flag) set, the solve is seeded from `seed` (device,
+    // g.cells values): the resident carrier's accepted previous pressure.
+    int enqueue_reset(const double* dt_dev, const int* skip, const rb200_settings& settings, cudaStream_t s,
+                      const int* warm = nullptr, const double* seed = nullptr);
     int enqueue_loop(cudaStream_t capture_stream, cudaStream_t body_stream, const rb200_settings& settings);
     int nodes_per_chunk() const { return nodes_per_chunk_ + 1; }
     // Blocks of the persistent solver kernel (0: the per-pass kernels run).

@@ -53,7 +53,7 @@ constexpr unsigned BOX_BYTES = unsigned(BOX) * 8u;
 constexpr int STAGE = (2 * PS::SIZE > PS::SIZE + 2 * BOX) ? 2 * PS::SIZE : PS::SIZE + 2 * BOX;
 constexpr size_t kPersistSmem = NS * size_t(STAGE) * sizeof(double);
 constexpr unsigned kBarrierSpins = 1u << 24;
-constexpr int PSTRIDE = 4;                   // doubles per block per partial set
+constexpr int PSTRIDE = 6;                   // doubles per block per partial set (2K + M <= 5)
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
     unsigned v;
@@ -337,6 +337,7 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
             // ---------------------------------------------- phase 3: true residual
             double* spare = sst.dsel ? A.d0 : A.d1;
             Neu2 acc;
+            double gauge_sq = 0.0;  // t[0]^2 in the thread that holds cell 0
             double mx = 0.0;
             const bool mine_ok = run_bricks(
                 c, full, empty,
@@ -362,13 +363,16 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
                         const double t = __ldcg(A.b + cc) - kp;
                         spare[cc] = t;
                         (u & 1 ? acc.b : acc.a).add(t * t);
+                        if (cc == 0) gauge_sq = t * t;
                         mx = fmax(mx, fabs(t));
                     }
                 });
-            dd sums[1] = {acc.as_dd()};
+            // |t|^2 and |t[1..]|^2 (the restart test of a seeded solve)
+            dd sums[2] = {acc.as_dd(), dd_add1(acc.as_dd(), -gauge_sq)};
             double maxs[1] = {mx};
-            if (!(ok = reduce_grid<1, 1>(c, A, mine_ok, sums, maxs))) break;
-            if (c.tid == 0) decide_true(&sst, trace, dd_value(sums[0]), maxs[0], flags, g.volume);
+            if (!(ok = reduce_grid<2, 1>(c, A, mine_ok, sums, maxs))) break;
+            if (c.tid == 0)
+                decide_true(&sst, trace, dd_value(sums[0]), dd_value(sums[1]), maxs[0], flags, g.volume);
             __syncthreads();
             continue;
         }

@@ -10,8 +10,11 @@ namespace rb200 {
 enum Mode : int { MODE_INIT = 0, MODE_ITER = 1, MODE_REPLACE = 2 };
 constexpr int F_CANDIDATE = 32;  // RB-SGS: candidate decided in pass 2, acted on after z
 
+// Kernels of one mode run while the flags allow: the start of a cold solve
+// (a seeded solve starts with its true-residual check instead), iterations
+// until a stop, the restart when one is pending.
 __device__ __forceinline__ bool gate(int flags, int mode) {
-    if (mode == MODE_INIT) return !(flags & F_DONE);
+    if (mode == MODE_INIT) return !(flags & (F_DONE | F_WARM));
     if (mode == MODE_ITER) return !(flags & F_STOP);
     return (flags & F_NEED_REPLACE) != 0;
 }
@@ -164,8 +167,12 @@ __device__ __forceinline__ void decide_pass2(SolveState* st, rb200_trace* trace,
 // True-residual check (true_report, src/pressure.rs:432-456, and the
 // acceptance/restart decisions of solve_loaded, :686-715): accept, stop at the
 // iteration limit, restart from the true residual, or keep the recurrence.
-__device__ __forceinline__ void decide_true(SolveState* st, rb200_trace* trace, double squared, double maximum,
-                                            int flags, double volume) {
+// `squared` is |t|^2 over every row, `squared_tail` over the rows after the
+// gauge row: a seeded solve judges the restart by the latter (:697-704). At
+// iteration 0 (the seeded start, :634-650) an unaccepted residual becomes the
+// first residual unless no iteration is allowed.
+__device__ __forceinline__ void decide_true(SolveState* st, rb200_trace* trace, double squared, double squared_tail,
+                                            double maximum, int flags, double volume) {
     const int it = st->it;
     const double div = maximum * st->dt / volume;
     if (trace && it >= 1) trace[it - 1].checked = 1;
@@ -181,7 +188,16 @@ __device__ __forceinline__ void decide_true(SolveState* st, rb200_trace* trace, 
         finish(st, RB200_OK, flags);
         return;
     }
-    const bool replaced = l2 > st->threshold;
+    if (it == 0) {
+        if (st->max_it == 0) {
+            finish(st, RB200_ITERATION_LIMIT, flags);
+            return;
+        }
+        st->flags = (flags & ~F_NEED_TRUE) | F_NEED_REPLACE;
+        return;
+    }
+    const double replacement_l2 = (flags & F_WARM) ? sqrt(squared_tail) : l2;
+    const bool replaced = replacement_l2 > st->threshold;
     if (it == st->max_it) {
         finish(st, RB200_ITERATION_LIMIT, flags);
         return;

@@ -100,7 +100,7 @@ def carrier_bytes_estimate(edge: int, config: CarrierConfig) -> int:
     n = edge ** 3
     faces = 3 * edge * edge * (edge + 1)
     elem = 4 if config.storage == "f32" else 8
-    per_cell = 8 * 7 + (6 if config.implementation == 3 else 0)
+    per_cell = 8 * 7 + (6 if config.implementation == 3 else 0) + (8 if config.warm_start else 0)
     return 3 * faces * elem + n * per_cell + (1 << 20)
 
 
