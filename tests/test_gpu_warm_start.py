@@ -216,7 +216,7 @@ def test_seeded_converged_solve_matches_the_oracle(counts):
 def test_carrier_accepted_previous_policy_matches_seeded_oracle_steps():
     """AcceptedPreviousV1: the first step is cold, every later step is seeded
     by the previous accepted pressure; each matches the oracle step seeded the
-    same way, and the seeded steps need fewer iterations than cold ones."""
+    same way."""
     n = (48, 48, 48)
     g = R.GridGeometry(n)
     faces = W.fourier_faces(n, dtype=np.float64)
@@ -239,8 +239,30 @@ def test_carrier_accepted_previous_policy_matches_seeded_oracle_steps():
         got = warm.download()
         for d in range(3):
             assert relerr(got[d], ref[d]) <= 1e-10
-        if step > 0:
-            assert rep.pressure.iterations < crep.pressure.iterations
     # a new accepted state invalidates the history: the next step is cold
     warm.upload(faces)
     assert warm.step(R.StepParams(0.05)).pressure_initialization == 0
+
+
+def test_seeding_cuts_iterations_under_steady_forcing():
+    """A density blob released from rest: the pressure that balances its
+    buoyancy changes little from step to step, so the accepted previous
+    pressure is a good start (the case the reference's warm start targets)."""
+    n = (32, 32, 32)
+    g = R.GridGeometry(n)
+    zero = [np.zeros(g.face_len(d)) for d in range(3)]
+    blob = W.gaussian_blob(n, sigma=5.0)
+    settings = S(1e-8, 0.0, MAXF, 100000)
+    sims = {}
+    for name, warm in (("warm", True), ("cold", False)):
+        sims[name] = R.CarrierSimulation(g, R.CarrierConfig(pressure=settings, storage="f64", with_tracer=True,
+                                                            warm_start=warm))
+        sims[name].upload(zero, blob)
+    its = {"warm": [], "cold": []}
+    for _ in range(6):
+        for name in ("warm", "cold"):
+            its[name].append(sims[name].step(R.StepParams(0.01, buoyancy=1.0)).pressure.iterations)
+    assert its["warm"][0] == its["cold"][0]
+    # the seed is about 1e-2 off in relative terms, so to a relative residual
+    # of 1e-8 it saves about a quarter of the iterations
+    assert sum(its["warm"][1:]) < 0.8 * sum(its["cold"][1:]), its
