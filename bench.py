@@ -506,9 +506,13 @@ def run_ours(args, world, rank, local):
              faces),
             ("mixed_mg_f32", R.CarrierConfig.mixed(pressure=mixed_pressure, device=local),
              [f.astype(np.float32) for f in faces]),
+            # the plain method with the AcceptedPreviousV1 initialization policy
+            ("jacobi_warm_start_f64", R.CarrierConfig(pressure=settings, storage=args.storage,
+                                                      implementation=R.PressureImplementation.JACOBI_PCG_V1,
+                                                      device=local, warm_start=True), faces),
         )
         for name, vcfg, vfaces in cases:
-            if vcfg.implementation == method and vcfg.storage == args.storage:
+            if vcfg.implementation == method and vcfg.storage == args.storage and not vcfg.warm_start:
                 continue
             vs = R.CarrierSimulation(g, vcfg)
             vs.upload(vfaces)
@@ -573,7 +577,9 @@ def run_ours(args, world, rank, local):
             "peak_kind": hbm_kind,
             "unit": "GB/s",
             "frac": achieved / hbm,
-            "traffic": None,
+            # DRAM bytes per iteration from one ncu capture of a 64-iteration
+            # launch at 128^3 (profiles/jacobi_persistent_128cube.md)
+            "traffic": 55.8e6 if roof_kernel.startswith("k_jacobi_persistent") and args.n == 128 else None,
             "algorithmic_bytes_per_launch": roof_bytes,
             "avg_launch_ms": roof_ms,
             "other_pass_ms": other_ms,
