@@ -577,8 +577,8 @@ def run_ours(args, world, rank, local):
             "peak_kind": hbm_kind,
             "unit": "GB/s",
             "frac": achieved / hbm,
-            # DRAM bytes per iteration from one ncu capture of a 64-iteration
-            # launch at 128^3 (profiles/jacobi_persistent_128cube.md)
+            # DRAM bytes per iteration: dram__bytes_read.sum + dram__bytes_write.sum
+            # of one ncu capture of a 64-iteration launch at 128^3, divided by 64
             "traffic": 55.8e6 if roof_kernel.startswith("k_jacobi_persistent") and args.n == 128 else None,
             "algorithmic_bytes_per_launch": roof_bytes,
             "avg_launch_ms": roof_ms,
