@@ -262,6 +262,30 @@ RB200_API int rb200_apply_full_device(const rb200_grid* grid, double density, co
  * (compensated). Returns RB200_NONFINITE_INPUT for a non-finite r. */
 RB200_API int rb200_precondition_jacobi_device(const rb200_grid* grid, double density, const double* r, double* z,
                                                size_t len, double* rz, void* stream);
+/* ProviderWorkspace's qualification of a candidate pressure on the device
+ * (src/solver_provider.rs:239-270): RB200_NONFINITE_OUTPUT for a non-finite
+ * pressure or product K p, RB200_NONZERO_GAUGE for pressure[0] != 0,
+ * RB200_QUALITY_GATE when |b - K p|_2 exceeds max(absolute, relative |b|_2)
+ * or max|b - K p| dt / V exceeds settings.divergence_limit, else RB200_OK.
+ * report (may be NULL) receives the candidate's residual l2, max and
+ * predicted divergence (iterations 0). Synchronous on `stream`. */
+RB200_API int rb200_qualify_pressure_device(const rb200_grid* grid, double density, const double* rhs,
+                                            const double* pressure, size_t len, double dt,
+                                            const rb200_settings* settings, rb200_report* report, void* stream);
+/* The momentum witness of a supplied projection
+ * (solver_provider/composition/projection.rs:515-542): the supplied velocity
+ * (su, sv, sw) must equal, bit for bit, the input velocity (u, v, w)
+ * corrected with the supplied pressure. RB200_OK, or RB200_QUALITY_GATE with
+ * *axis (0, 1, 2) and *index the first mismatching face (MomentumWitness);
+ * field validation errors as the primitives above. Synchronous on `stream`. */
+RB200_API int rb200_projection_witness_f32_device(const rb200_grid* grid, double density, const double* pressure,
+                                                  double dt, const float* u, const float* v, const float* w,
+                                                  const float* su, const float* sv, const float* sw, int* axis,
+                                                  uint64_t* index, void* stream);
+RB200_API int rb200_projection_witness_f64_device(const rb200_grid* grid, double density, const double* pressure,
+                                                  double dt, const double* u, const double* v, const double* w,
+                                                  const double* su, const double* sv, const double* sw, int* axis,
+                                                  uint64_t* index, void* stream);
 RB200_API int rb200_build_rhs_f32_device(const rb200_grid* grid, double density, const float* u,
                                const float* v, const float* w, double dt, double* rhs,
                                void* stream);

@@ -226,6 +226,38 @@ class PressureOperator:
         self._check(lib().rb200_apply_full_device(C.byref(self.grid.c()), self.density, _ptr(pressure), _ptr(out),
                                                   _stream_of(pressure)))
 
+    def qualify_pressure(self, rhs, pressure, dt: float, settings: "PressureSettings") -> "PressureReport":
+        """ProviderWorkspace's qualification of a candidate pressure
+        (src/solver_provider.rs:239-270) on device arrays; raises
+        ProviderRejection (NonFiniteOutput, NonZeroGauge, QualityGate) with the
+        candidate's report attached."""
+        rep = N.Report()
+        n = int(pressure.numel()) if hasattr(pressure, "numel") else int(pressure.size)
+        st = lib().rb200_qualify_pressure_device(C.byref(self.grid.c()), self.density, _ptr(rhs), _ptr(pressure), n,
+                                                 dt, C.byref(settings.c()), C.byref(rep), _stream_of(pressure))
+        report = PressureReport.from_c(rep)
+        if st != N.OK:
+            err = ProviderRejection(st)
+            err.report = report
+            raise err
+        return report
+
+    def projection_witness(self, pressure, dt: float, velocity: Sequence, supplied: Sequence):
+        """The momentum witness of a supplied projection
+        (composition/projection.rs:515-542): None when `supplied` equals
+        `velocity` corrected with `pressure` bit for bit, else (axis, index)
+        of the first mismatching face."""
+        u, v, w = velocity
+        su, sv, sw = supplied
+        fn = lib().rb200_projection_witness_f32_device if _is_f32(u) else lib().rb200_projection_witness_f64_device
+        axis, index = C.c_int(), C.c_uint64()
+        st = fn(C.byref(self.grid.c()), self.density, _ptr(pressure), dt, _ptr(u), _ptr(v), _ptr(w), _ptr(su),
+                _ptr(sv), _ptr(sw), C.byref(axis), C.byref(index), _stream_of(u))
+        if st == N.QUALITY_GATE:
+            return int(axis.value), int(index.value)
+        self._check(st)
+        return None
+
     def precondition_jacobi(self, residual, out) -> float:
         """precondition_jacobi (src/pressure.rs:534-575): out = r/D with
         out[0] = 0 (eliminated gauge row); returns r.z over rows >= 1."""

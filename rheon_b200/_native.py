@@ -131,6 +131,12 @@ SIGNATURES = {
     "rb200_pressure_solve_static": (_I, [C.POINTER(Grid), _D, _P, _P, _S, _D, C.POINTER(Settings),
                                          C.POINTER(Report), _P]),
     "rb200_apply_full_device": (_I, [C.POINTER(Grid), _D, _P, _P, _P]),
+    "rb200_qualify_pressure_device": (_I, [C.POINTER(Grid), _D, _P, _P, C.c_size_t, _D, C.POINTER(Settings),
+                                           C.POINTER(Report), _P]),
+    "rb200_projection_witness_f32_device": (_I, [C.POINTER(Grid), _D, _P, _D, _P, _P, _P, _P, _P, _P,
+                                                 C.POINTER(C.c_int), C.POINTER(C.c_uint64), _P]),
+    "rb200_projection_witness_f64_device": (_I, [C.POINTER(Grid), _D, _P, _D, _P, _P, _P, _P, _P, _P,
+                                                 C.POINTER(C.c_int), C.POINTER(C.c_uint64), _P]),
     "rb200_precondition_jacobi_device": (_I, [C.POINTER(Grid), _D, _P, _P, C.c_size_t, C.POINTER(_D), _P]),
     "rb200_build_rhs_f32_device": (_I, [C.POINTER(Grid), _D, _P, _P, _P, _D, _P, _P]),
     "rb200_build_rhs_f64_device": (_I, [C.POINTER(Grid), _D, _P, _P, _P, _D, _P, _P]),

@@ -169,6 +169,43 @@ static int advect_prim(const rb200_grid* grid, const T* u, const T* v, const T* 
 }
 
 
+template <class T>
+static int witness_prim(const rb200_grid* grid, double density, const double* pressure, double dt, const T* iu,
+                        const T* iv, const T* iw, const T* su, const T* sv, const T* sw, int* axis, uint64_t* index,
+                        void* stream) {
+    if (!pressure || !iu || !iv || !iw || !su || !sv || !sw) return RB200_INVALID_ARGUMENT;
+    if (axis) *axis = -1;
+    if (index) *index = 0;
+    if (!std::isfinite(dt) || dt <= 0.0) return RB200_INVALID_ARGUMENT;
+    RB200_PRIM_BEGIN(grid, density)
+    // validate_cells(pressure), validate_velocity(supplied) (projection.rs:521-526)
+    if ((rc = launch_check_finite(pressure, g.cells, fl.d, s))) return rc;
+    if ((rc = launch_validate_faces<T>(g, su, sv, sw, fl.d, s))) return rc;
+    if ((rc = launch_validate_faces<T>(g, iu, iv, iw, fl.d, s))) return rc;
+    unsigned long long* first = nullptr;
+    RB200_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&first), 3 * sizeof(unsigned long long), s));
+    cudaMemsetAsync(first, 0xff, 3 * sizeof(unsigned long long), s);
+    const T* in[3] = {iu, iv, iw};
+    const T* sup[3] = {su, sv, sw};
+    rc = launch_projection_witness<T>(g, pressure, dt, in, sup, first, s);
+    unsigned long long h[3] = {0, 0, 0};
+    if (!rc && cudaMemcpyAsync(h, first, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess) rc = RB200_EXECUTION;
+    cudaFreeAsync(first, s);
+    int f = 0;
+    int rc2 = fl.close(&f);
+    if (rc) return rc;
+    if (rc2) return rc2;
+    if ((rc = flags_status(f, true))) return rc;
+    for (int a = 0; a < 3; ++a)
+        if (h[a] != ~0ull) {
+            if (axis) *axis = a;
+            if (index) *index = uint64_t(h[a]);
+            return RB200_QUALITY_GATE;
+        }
+    return RB200_OK;
+}
+
+
 extern "C" {
 
 int rb200_abi_version(void) { return RB200_ABI_VERSION; }
@@ -420,6 +457,60 @@ int rb200_apply_full_device(const rb200_grid* grid, double density, const double
     return flags_status(f, false);
 }
 
+
+int rb200_qualify_pressure_device(const rb200_grid* grid, double density, const double* rhs,
+                                  const double* pressure, size_t len, double dt, const rb200_settings* settings,
+                                  rb200_report* report, void* stream) {
+    if (!rhs || !pressure || !settings) return RB200_INVALID_ARGUMENT;
+    if (report) std::memset(report, 0, sizeof(*report));
+    if (!std::isfinite(dt) || dt <= 0.0 || !settings_valid(settings)) return RB200_INVALID_ARGUMENT;
+    GridDev g;
+    int rc = make_grid_dev(grid, density, &g);
+    if (rc) return rc;
+    if (len != size_t(g.cells)) return RB200_LENGTH_MISMATCH;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nb = size_t(precondition_partials_blocks());
+    const size_t bytes = (4 * nb + 5) * sizeof(double) + sizeof(unsigned);
+    char* scratch = nullptr;
+    RB200_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&scratch), bytes, s));
+    Partials part{reinterpret_cast<double*>(scratch), reinterpret_cast<unsigned*>(scratch + (4 * nb + 5) * 8)};
+    double* out = part.data + 4 * nb;
+    cudaMemsetAsync(part.ticket, 0, sizeof(unsigned), s);
+    rc = launch_qualify_pressure(g, rhs, pressure, part, out, s);
+    double h[5] = {0, 0, 0, 0, 0};
+    if (!rc && cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess) rc = RB200_EXECUTION;
+    cudaFreeAsync(scratch, s);
+    if (!rc && cudaStreamSynchronize(s) != cudaSuccess) rc = RB200_EXECUTION;
+    if (rc) return rc;
+    // the order of the reference's checks: non-finite output, gauge, product
+    if (h[3] == 1.0) return RB200_NONFINITE_OUTPUT;
+    if (h[4] != 0.0) return RB200_NONZERO_GAUGE;
+    if (h[3] != 0.0) return RB200_NONFINITE_OUTPUT;
+    const double l2 = std::sqrt(h[0]);
+    const double threshold = std::fmax(settings->absolute_residual, settings->relative_residual * std::sqrt(h[1]));
+    const double divergence = h[2] * dt / g.volume;
+    if (report) {
+        report->true_residual_l2 = l2;
+        report->true_residual_max = h[2];
+        report->predicted_divergence_max = divergence;
+    }
+    if (!std::isfinite(l2) || !std::isfinite(divergence) || l2 > threshold || divergence > settings->divergence_limit)
+        return RB200_QUALITY_GATE;
+    return RB200_OK;
+}
+
+int rb200_projection_witness_f32_device(const rb200_grid* grid, double density, const double* pressure, double dt,
+                                        const float* u, const float* v, const float* w, const float* su,
+                                        const float* sv, const float* sw, int* axis, uint64_t* index, void* stream) {
+    return witness_prim<float>(grid, density, pressure, dt, u, v, w, su, sv, sw, axis, index, stream);
+}
+
+int rb200_projection_witness_f64_device(const rb200_grid* grid, double density, const double* pressure, double dt,
+                                        const double* u, const double* v, const double* w, const double* su,
+                                        const double* sv, const double* sw, int* axis, uint64_t* index,
+                                        void* stream) {
+    return witness_prim<double>(grid, density, pressure, dt, u, v, w, su, sv, sw, axis, index, stream);
+}
 
 int rb200_precondition_jacobi_device(const rb200_grid* grid, double density, const double* r, double* z, size_t len,
                                      double* rz, void* stream) {

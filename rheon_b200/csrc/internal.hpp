@@ -129,6 +129,13 @@ int launch_apply_full(const GridDev& g, const double* p, double* out, int* flags
 int launch_precondition_jacobi(const GridDev& g, const double* r, double* z, Partials part, double* rz_out,
                                cudaStream_t s);
 int precondition_partials_blocks();
+// Qualification sums of a candidate pressure into out[5] (device), `part` as
+// for launch_precondition_jacobi.
+int launch_qualify_pressure(const GridDev& g, const double* b, const double* p, Partials part, double* out,
+                            cudaStream_t s);
+template <class T>
+int launch_projection_witness(const GridDev& g, const double* p, double dt, const T* const in[3],
+                              const T* const sup[3], unsigned long long* first, cudaStream_t s);
 template <class T>
 int launch_validate_faces(const GridDev& g, const T* u, const T* v, const T* w, int* flags,
                           cudaStream_t s);

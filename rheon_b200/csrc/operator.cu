@@ -225,6 +225,60 @@ int launch_face_maxima(const GridDev& g, const T* u, const T* v, const T* w, Par
     return RB200_OK;
 }
 
+// The momentum witness of a supplied projection
+// (composition/projection.rs:515-542): each face of the supplied velocity must
+// equal, bit for bit, the input velocity corrected with the supplied pressure
+// (walls unchanged). The lowest mismatching face index of each axis is kept.
+template <class T>
+__global__ void k_projection_witness(GridDev g, const double* __restrict__ p, double dt, const T* __restrict__ iu,
+                                     const T* __restrict__ iv, const T* __restrict__ iw, const T* __restrict__ su,
+                                     const T* __restrict__ sv, const T* __restrict__ sw,
+                                     unsigned long long* __restrict__ first) {
+    const long long total = (long long)g.flen[0] + g.flen[1] + g.flen[2];
+    const int s[3] = {1, g.n[0], g.n[0] * g.n[1]};
+    int local = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int a = 0;
+        long long f = t;
+        if (f >= g.flen[0]) {
+            f -= g.flen[0];
+            a = 1;
+            if (f >= g.flen[1]) {
+                f -= g.flen[1];
+                a = 2;
+            }
+        }
+        const T* in = a == 0 ? iu : (a == 1 ? iv : iw);
+        const T* sup = a == 0 ? su : (a == 1 ? sv : sw);
+        int fi = int(f % g.fc[a][0]);
+        int fj = int((f / g.fc[a][0]) % g.fc[a][1]);
+        int fk = int(f / ((long long)g.fc[a][0] * g.fc[a][1]));
+        T expect = in[f];
+        if (!is_wall_face(g, a, fi, fj, fk)) {
+            const int c = cell_idx(g, fi, fj, fk);
+            expect = corrected<T>(g, a, expect, p[c], p[c - s[a]], dt, local);
+        }
+        const T got = sup[f];
+        bool same;
+        if (sizeof(T) == 4)
+            same = __float_as_uint(float(expect)) == __float_as_uint(float(got));
+        else
+            same = __double_as_longlong(double(expect)) == __double_as_longlong(double(got));
+        if (!same) atomicMin(&first[a], (unsigned long long)f);
+    }
+}
+
+template <class T>
+int launch_projection_witness(const GridDev& g, const double* p, double dt, const T* const in[3],
+                              const T* const sup[3], unsigned long long* first, cudaStream_t s) {
+    const long long total = (long long)g.flen[0] + g.flen[1] + g.flen[2];
+    k_projection_witness<T><<<ew_blocks(total), EW_THREADS, 0, s>>>(g, p, dt, in[0], in[1], in[2], sup[0], sup[1],
+                                                                    sup[2], first);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+
 #define RB200_INSTANTIATE(T)                                                                        \
     template int launch_validate_faces<T>(const GridDev&, const T*, const T*, const T*, int*,       \
                                           cudaStream_t);                                            \
@@ -238,7 +292,9 @@ int launch_face_maxima(const GridDev& g, const T* u, const T* v, const T* w, Par
                                               const T* const[3], T* const[3], Partials, int,        \
                                               double*, int*, cudaStream_t);                         \
     template int launch_face_maxima<T>(const GridDev&, const T*, const T*, const T*, Partials, int, \
-                                       double*, int*, cudaStream_t);
+                                       double*, int*, cudaStream_t);                                \
+    template int launch_projection_witness<T>(const GridDev&, const double*, double, const T* const[3], \
+                                              const T* const[3], unsigned long long*, cudaStream_t);
 RB200_INSTANTIATE(float)
 RB200_INSTANTIATE(double)
 #undef RB200_INSTANTIATE

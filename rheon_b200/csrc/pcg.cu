@@ -1219,6 +1219,57 @@ int PcgSolver::profile(int which, int launches, double* avg_ms) {
     return RB200_OK;
 }
 
+// ProviderWorkspace's qualification of a candidate pressure
+// (src/solver_provider.rs:239-270) in one pass: t = b - K p, |t|^2 and |b|^2
+// (compensated), max|t|, and flags for a non-finite pressure (1) or product
+// (2). out = {|t|^2, |b|^2, max|t|, flags, p[0]}.
+__global__ void __launch_bounds__(EW) k_qualify_pressure(GridDev g, const double* __restrict__ b,
+                                                         const double* __restrict__ p, Partials part,
+                                                         double* __restrict__ out) {
+    __shared__ BlockReduce<2, 2> sm;
+    Neu tt, bb;
+    double m[2] = {0.0, 0.0};
+    const int sy = g.n[0], sz = g.n[0] * g.n[1];
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+        const int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+        Neigh v;
+        v.c = p[c];
+        v.xm = i > 0 ? p[c - 1] : 0.0;
+        v.xp = i + 1 < g.n[0] ? p[c + 1] : 0.0;
+        v.ym = j > 0 ? p[c - sy] : 0.0;
+        v.yp = j + 1 < g.n[1] ? p[c + sy] : 0.0;
+        v.zm = k > 0 ? p[c - sz] : 0.0;
+        v.zp = k + 1 < g.n[2] ? p[c + sz] : 0.0;
+        if (!isfinite(v.c)) m[1] = fmax(m[1], 1.0);
+        const double q = apply_row(g, i, j, k, v);
+        if (!isfinite(q)) m[1] = fmax(m[1], 2.0);
+        const double bc = b[c];
+        const double t = bc - q;
+        tt.add(t * t);
+        bb.add(bc * bc);
+        m[0] = fmax(m[0], fabs(t));
+    }
+    dd sums[2] = {tt.as_dd(), bb.as_dd()};
+    block_reduce<2, 2>(sm, sums, m);
+    if (publish_and_check_last<2, 2>(part, blockIdx.x, gridDim.x, sums, m)) {
+        fold_partials<2, 2>(part, gridDim.x, sm, sums, m);
+        if (threadIdx.x == 0) {
+            out[0] = dd_value(sums[0]);
+            out[1] = dd_value(sums[1]);
+            out[2] = m[0];
+            out[3] = m[1];
+            out[4] = p[0];
+        }
+    }
+}
+
+int launch_qualify_pressure(const GridDev& g, const double* b, const double* p, Partials part, double* out,
+                            cudaStream_t s) {
+    k_qualify_pressure<<<ew_blocks(g.cells), EW, 0, s>>>(g, b, p, part, out);
+    RB200_CUDA(cudaGetLastError());
+    return RB200_OK;
+}
+
 int launch_precondition_jacobi(const GridDev& g, const double* r, double* z, Partials part, double* rz_out,
                                cudaStream_t s) {
     k_precondition_jacobi<<<ew_blocks(g.cells), EW, 0, s>>>(g, r, z, part, rz_out);
