@@ -536,6 +536,18 @@ def run_ours(args, world, rank, local):
             variants[name] = {"value": vvalue, "unit": UNIT, "ms_per_step": vms / args.steps,
                               "iterations_per_step": statistics.mean(vit), "actual_divergence_max": vdiv,
                               "vs_plain_f64": vvalue / value}
+            if vcfg.implementation == R.PressureImplementation.MG_MIXED:
+                # whole-step roofline under the algorithmic byte model of a
+                # mixed outer cycle: an FP32 V(2,2) with levels summed (about
+                # 82N) plus the FP64 defect and accumulation (48N) = 130N per
+                # outer iteration, and the step's non-iterative traffic
+                # (advection, RHS, correction: 5 F s + 16N with s = 4 bytes)
+                faces_total = sum(g.face_len(d) for d in range(3))
+                step_bytes = statistics.mean(vit) * 130 * cells + 5 * faces_total * 4 + 16 * cells
+                ach = step_bytes / (vms / args.steps / 1e3) / 1e9
+                variants[name]["roofline"] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                                              "frac": ach / hbm, "bytes_per_step": step_bytes,
+                                              "model": "130N per outer iteration + 5Fs + 16N per step"}
             vs.close()
 
     batched = None

@@ -182,11 +182,61 @@ __device__ __forceinline__ void smooth_rows(const MgLevelDev& L, const double* _
     }
 }
 
+// restrict_rows for fine rows whose length is a multiple of 4 (halved along
+// x): a lane takes two coarse cells, i.e. 4 fine cells of each child row, with
+// 16-byte loads; the sums run in the same order as restrict_rows.
+template <bool CG>
+__device__ __forceinline__ void restrict_rows_v4(const MgLevelDev& L, const MgLevelDev& C, const Warps& W) {
+    const int n0 = L.n[0], sy = n0, sz = n0 * L.n[1];
+    const int rows = C.n[1] * C.n[2];
+    const int cpairs = C.n[0] >> 1;
+    const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (int row = W.w0; row < rows; row += W.nw) {
+        const int J = row % C.n[1], K = row / C.n[1];
+        for (int P = W.lane; P < cpairs; P += 32) {
+            const int i0 = 4 * P;
+            float sum[2] = {0.0f, 0.0f};
+            for (int dk = 0; dk < L.cf[2]; ++dk)
+                for (int dj = 0; dj < L.cf[1]; ++dj) {
+                    const int j = J * L.cf[1] + dj, k = K * L.cf[2] + dk;
+                    if (j >= L.n[1] || k >= L.n[2]) continue;
+                    const int c0 = i0 + n0 * (j + L.n[1] * k);
+                    const float4 xc = ld4<CG>(L.x + c0);
+                    const float4 bq = ld4<CG>(L.b + c0);
+                    const float xl = i0 > 0 ? ldv<CG>(L.x + c0 - 1) : 0.0f;
+                    const float xr = i0 + 4 < n0 ? ldv<CG>(L.x + c0 + 4) : 0.0f;
+                    const float4 ym = j > 0 ? ld4<CG>(L.x + c0 - sy) : z4;
+                    const float4 yp = j + 1 < L.n[1] ? ld4<CG>(L.x + c0 + sy) : z4;
+                    const float4 zm = k > 0 ? ld4<CG>(L.x + c0 - sz) : z4;
+                    const float4 zp = k + 1 < L.n[2] ? ld4<CG>(L.x + c0 + sz) : z4;
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int i = i0 + e;
+                        const float x0 = f4get(xc, e);
+                        float kx = 0.0f;
+                        if (i > 0) kx += L.w[0] * (x0 - (e == 0 ? xl : f4get(xc, e - 1)));
+                        if (i + 1 < n0) kx += L.w[0] * (x0 - (e == 3 ? xr : f4get(xc, e + 1)));
+                        if (j > 0) kx += L.w[1] * (x0 - f4get(ym, e));
+                        if (j + 1 < L.n[1]) kx += L.w[1] * (x0 - f4get(yp, e));
+                        if (k > 0) kx += L.w[2] * (x0 - f4get(zm, e));
+                        if (k + 1 < L.n[2]) kx += L.w[2] * (x0 - f4get(zp, e));
+                        sum[e >> 1] += f4get(bq, e) - kx;
+                    }
+                }
+            *reinterpret_cast<float2*>(C.b + 2 * P + C.n[0] * row) = make_float2(sum[0], sum[1]);
+        }
+    }
+}
+
 // Residual b - K x on the fine cells summed over each coarse cell's children
 // (restriction = transpose of the piecewise-constant prolongation). Warps
 // take coarse rows, lanes coarse cells along x.
 template <bool CG>
 __device__ __forceinline__ void restrict_rows(const MgLevelDev& L, const MgLevelDev& C, const Warps& W) {
+    if ((L.n[0] & 3) == 0 && L.cf[0] == 2) {
+        restrict_rows_v4<CG>(L, C, W);
+        return;
+    }
     const int sy = L.n[0], sz = L.n[0] * L.n[1];
     const int rows = C.n[1] * C.n[2];
     for (int row = W.w0; row < rows; row += W.nw) {
@@ -224,8 +274,58 @@ __device__ __forceinline__ float coarse_at(const MgLevelDev& L, const MgLevelDev
 // formed on the fly. Red cells are not written: the red half-sweep that
 // follows replaces every red value without reading it. Nothing this pass reads
 // is written by it.
+// prolong_black_rows for rows whose length is a multiple of 4, with 16-byte
+// loads and stores of the fine rows (the red cells are stored back unchanged:
+// the red half-sweep that follows replaces them without reading them).
+template <bool CG>
+__device__ __forceinline__ void prolong_black_rows_v4(const MgLevelDev& L, const MgLevelDev& C, const Warps& W) {
+    const int n0 = L.n[0], quads = n0 >> 2;
+    const int rows = L.n[1] * L.n[2];
+    const int sy = n0, sz = n0 * L.n[1];
+    const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (int row = W.w0; row < rows; row += W.nw) {
+        const int j = row % L.n[1], k = row / L.n[1];
+        const int base = n0 * row;
+        const int par = (1 + j + k) & 1;
+        const int myz = (int(j > 0) << 2) | (int(j + 1 < L.n[1]) << 3) | (int(k > 0) << 4) |
+                        (int(k + 1 < L.n[2]) << 5);
+        for (int q = W.lane; q < quads; q += 32) {
+            const int i0 = 4 * q;
+            const int c0 = base + i0;
+            const float4 bq = ld4<CG>(L.b + c0);
+            const float4 xc = ld4<CG>(L.x + c0);
+            const float xl = (i0 > 0) ? ldv<CG>(L.x + c0 - 1) : 0.0f;
+            const float xr = (i0 + 4 < n0) ? ldv<CG>(L.x + c0 + 4) : 0.0f;
+            const float4 ym = (myz & 4) ? ld4<CG>(L.x + c0 - sy) : z4;
+            const float4 yp = (myz & 8) ? ld4<CG>(L.x + c0 + sy) : z4;
+            const float4 zm = (myz & 16) ? ld4<CG>(L.x + c0 - sz) : z4;
+            const float4 zp = (myz & 32) ? ld4<CG>(L.x + c0 + sz) : z4;
+            float4 out = xc;
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                const int e = par + 2 * t;
+                const int i = i0 + e;
+                float s = f4get(bq, e);
+                if (i > 0) s += L.w[0] * ((e == 0 ? xl : f4get(xc, e - 1)) + coarse_at<CG>(L, C, i - 1, j, k));
+                if (i + 1 < n0) s += L.w[0] * ((e == 3 ? xr : f4get(xc, e + 1)) + coarse_at<CG>(L, C, i + 1, j, k));
+                if (myz & 4) s += L.w[1] * (f4get(ym, e) + coarse_at<CG>(L, C, i, j - 1, k));
+                if (myz & 8) s += L.w[1] * (f4get(yp, e) + coarse_at<CG>(L, C, i, j + 1, k));
+                if (myz & 16) s += L.w[2] * (f4get(zm, e) + coarse_at<CG>(L, C, i, j, k - 1));
+                if (myz & 32) s += L.w[2] * (f4get(zp, e) + coarse_at<CG>(L, C, i, j, k + 1));
+                const int mask = int(i > 0) | (int(i + 1 < n0) << 1) | myz;
+                f4put(out, e, s * L.dinv[mask]);
+            }
+            *reinterpret_cast<float4*>(L.x + c0) = out;
+        }
+    }
+}
+
 template <bool CG>
 __device__ __forceinline__ void prolong_black_rows(const MgLevelDev& L, const MgLevelDev& C, const Warps& W) {
+    if ((L.n[0] & 3) == 0) {
+        prolong_black_rows_v4<CG>(L, C, W);
+        return;
+    }
     const int hx = (L.n[0] + 1) >> 1;
     const int rows = L.n[1] * L.n[2];
     const int sy = L.n[0], sz = L.n[0] * L.n[1];
@@ -571,6 +671,69 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int 
     const Warps W = grid_warps();
     const int hx = (L.n[0] + 1) >> 1;
     const int rows = L.n[1] * L.n[2];
+    if ((L.n[0] & 3) == 0) {
+        // quads of 4 cells with 16-byte loads (the same values as the pairs below)
+        const int n0 = L.n[0], quads = n0 >> 2, sy = n0, sz = n0 * L.n[1];
+        const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (int rw = W.w0; rw < rows; rw += W.nw) {
+            const int j = rw % L.n[1], k = rw / L.n[1];
+            const int par = (j + k) & 1;  // the red cells of the quad: par, par + 2
+            const int myz = (int(j > 0) << 2) | (int(j + 1 < L.n[1]) << 3) | (int(k > 0) << 4) |
+                            (int(k + 1 < L.n[2]) << 5);
+            for (int qd = W.lane; qd < quads; qd += 32) {
+                const int i0 = 4 * qd;
+                const int c0 = n0 * rw + i0;
+                const float4 xc = *reinterpret_cast<const float4*>(L.x + c0);
+                float4 out = xc;
+                if (smooth) {
+                    const float4 bq = *reinterpret_cast<const float4*>(L.b + c0);
+                    const float xl = i0 > 0 ? L.x[c0 - 1] : 0.0f;
+                    const float xr = i0 + 4 < n0 ? L.x[c0 + 4] : 0.0f;
+                    const float4 ym = (myz & 4) ? *reinterpret_cast<const float4*>(L.x + c0 - sy) : z4;
+                    const float4 yp = (myz & 8) ? *reinterpret_cast<const float4*>(L.x + c0 + sy) : z4;
+                    const float4 zm = (myz & 16) ? *reinterpret_cast<const float4*>(L.x + c0 - sz) : z4;
+                    const float4 zp = (myz & 32) ? *reinterpret_cast<const float4*>(L.x + c0 + sz) : z4;
+#pragma unroll
+                    for (int t = 0; t < 2; ++t) {
+                        const int e = par + 2 * t;
+                        const int i = i0 + e;
+                        float sacc = f4get(bq, e);
+                        if (i > 0) sacc += L.w[0] * (e == 0 ? xl : f4get(xc, e - 1));
+                        if (i + 1 < n0) sacc += L.w[0] * (e == 3 ? xr : f4get(xc, e + 1));
+                        if (myz & 4) sacc += L.w[1] * f4get(ym, e);
+                        if (myz & 8) sacc += L.w[1] * f4get(yp, e);
+                        if (myz & 16) sacc += L.w[2] * f4get(zm, e);
+                        if (myz & 32) sacc += L.w[2] * f4get(zp, e);
+                        f4put(out, e, sacc * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz]);
+                    }
+                    *reinterpret_cast<float4*>(L.x + c0) = out;
+                }
+                double zc[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) zc[e] = (c0 + e == 0) ? 0.0 : double(f4get(out, e));
+                *reinterpret_cast<double2*>(z + c0) = make_double2(zc[0], zc[1]);
+                *reinterpret_cast<double2*>(z + c0 + 2) = make_double2(zc[2], zc[3]);
+                const double2 r01 = *reinterpret_cast<const double2*>(r + c0);
+                const double2 r23 = *reinterpret_cast<const double2*>(r + c0 + 2);
+                const double rr[4] = {r01.x, r01.y, r23.x, r23.y};
+                double qq[4] = {0.0, 0.0, 0.0, 0.0};
+                if (mode == MODE_ITER) {
+                    const double2 q01 = *reinterpret_cast<const double2*>(q + c0);
+                    const double2 q23 = *reinterpret_cast<const double2*>(q + c0 + 2);
+                    qq[0] = q01.x;
+                    qq[1] = q01.y;
+                    qq[2] = q23.x;
+                    qq[3] = q23.y;
+                }
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    if (c0 + e == 0) continue;
+                    rz.add(rr[e] * zc[e]);
+                    if (mode == MODE_ITER) zq.add(zc[e] * qq[e]);
+                }
+            }
+        }
+    } else
     for (int rw = W.w0; rw < rows; rw += W.nw) {
         const int j = rw % L.n[1], k = rw / L.n[1];
         const int row = L.n[0] * rw;
