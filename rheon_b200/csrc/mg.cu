@@ -662,7 +662,7 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
 // r.z and z.q reduced and the flexible-CG decision taken. Without a hierarchy
 // (a single level solved densely) z is copied from x.
 __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int smooth, SolveState* st,
-                                                              double* __restrict__ z, const double* __restrict__ r,
+                                                              const double* __restrict__ r,
                                                               const double* __restrict__ q, int mode, Partials part,
                                                               rb200_trace* trace) {
     __shared__ BlockReduce<2, 0> red;
@@ -711,8 +711,6 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int 
                 double zc[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) zc[e] = (c0 + e == 0) ? 0.0 : double(f4get(out, e));
-                *reinterpret_cast<double2*>(z + c0) = make_double2(zc[0], zc[1]);
-                *reinterpret_cast<double2*>(z + c0 + 2) = make_double2(zc[2], zc[3]);
                 const double2 r01 = *reinterpret_cast<const double2*>(r + c0);
                 const double2 r23 = *reinterpret_cast<const double2*>(r + c0 + 2);
                 const double rr[4] = {r01.x, r01.y, r23.x, r23.y};
@@ -744,7 +742,6 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int 
             if (ib < L.n[0]) {  // the black cell of the pair: its value is final
                 const int c = ib + row;
                 const double zc = c == 0 ? 0.0 : double(L.x[c]);
-                z[c] = zc;
                 if (c != 0) {
                     rz.add(r[c] * zc);
                     if (mode == MODE_ITER) zq.add(zc * q[c]);
@@ -758,7 +755,6 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int 
                     L.x[c] = xv;
                 }
                 const double zc = c == 0 ? 0.0 : double(xv);
-                z[c] = zc;
                 if (c != 0) {
                     rz.add(r[c] * zc);
                     if (mode == MODE_ITER) zq.add(zc * q[c]);
@@ -775,12 +771,127 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int 
     }
 }
 
-int Multigrid::enqueue_finish(void* state, double* z, const double* r, const double* q, int mode, Partials part,
+// The flexible-CG direction pass of the mixed method (src/pressure.rs:657-668,
+// :720-731): d = z + beta d (d = z after a restart), q = K d stored, d.q and
+// the decision for alpha. z is read straight from the V-cycle's FP32 output x
+// of the finest level (z = f64(x), z[0] = 0 for the eliminated gauge row), so
+// no FP64 copy of z is stored. One warp per cell row, lanes along x.
+__global__ void __launch_bounds__(MG_THREADS) k_mg_pass1(GridDev g, MgLevelDev L, SolveState* st, double* d0,
+                                                         double* d1, double* __restrict__ q, Partials part,
+                                                         rb200_trace* trace) {
+    __shared__ BlockReduce<1, 0> red;
+    const int flags = st->flags;
+    if (flags & F_STOP) return;
+    const bool fresh = (flags & F_REPLACED) != 0;
+    const double beta = st->beta;
+    const int dsel = st->dsel;
+    const double* __restrict__ src = dsel ? d1 : d0;
+    double* __restrict__ dst = dsel ? d0 : d1;
+    const float* __restrict__ x = L.x;
+    auto dn = [&](int c) -> double {
+        const double zc = c == 0 ? 0.0 : double(x[c]);
+        return fresh ? zc : zc + beta * src[c];
+    };
+    const int sy = g.n[0], sz = g.n[0] * g.n[1];
+    Neu acc;
+    const Warps W = grid_warps();
+    const int rows = g.n[1] * g.n[2];
+    if ((g.n[0] & 3) == 0) {
+        // quads of 4 cells: x with 16-byte loads, d with two 16-byte loads
+        const int n0 = g.n[0], quads = n0 >> 2;
+        auto dn4 = [&](int c0, double (&o)[4]) {
+            const float4 xv = *reinterpret_cast<const float4*>(x + c0);
+            const double zc[4] = {c0 == 0 ? 0.0 : double(xv.x), double(xv.y), double(xv.z), double(xv.w)};
+            if (fresh) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) o[e] = zc[e];
+            } else {
+                const double2 a = *reinterpret_cast<const double2*>(src + c0);
+                const double2 b2 = *reinterpret_cast<const double2*>(src + c0 + 2);
+                o[0] = zc[0] + beta * a.x;
+                o[1] = zc[1] + beta * a.y;
+                o[2] = zc[2] + beta * b2.x;
+                o[3] = zc[3] + beta * b2.y;
+            }
+        };
+        for (int rw = W.w0; rw < rows; rw += W.nw) {
+            const int j = rw % g.n[1], k = rw / g.n[1];
+            const int base = n0 * rw;
+            for (int qd = W.lane; qd < quads; qd += 32) {
+                const int i0 = 4 * qd;
+                const int c0 = base + i0;
+                double dc[4], ym[4] = {0, 0, 0, 0}, yp[4] = {0, 0, 0, 0}, zm[4] = {0, 0, 0, 0}, zp[4] = {0, 0, 0, 0};
+                dn4(c0, dc);
+                if (j > 0) dn4(c0 - sy, ym);
+                if (j + 1 < g.n[1]) dn4(c0 + sy, yp);
+                if (k > 0) dn4(c0 - sz, zm);
+                if (k + 1 < g.n[2]) dn4(c0 + sz, zp);
+                const double xl = i0 > 0 ? dn(c0 - 1) : 0.0;
+                const double xr = i0 + 4 < n0 ? dn(c0 + 4) : 0.0;
+                double qq[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    Neigh v;
+                    v.c = dc[e];
+                    v.xm = e == 0 ? xl : dc[e - 1];
+                    v.xp = e == 3 ? xr : dc[e + 1];
+                    v.ym = ym[e];
+                    v.yp = yp[e];
+                    v.zm = zm[e];
+                    v.zp = zp[e];
+                    qq[e] = (c0 + e == 0) ? 0.0 : apply_row(g, i0 + e, j, k, v);
+                }
+                *reinterpret_cast<double2*>(dst + c0) = make_double2(dc[0], dc[1]);
+                *reinterpret_cast<double2*>(dst + c0 + 2) = make_double2(dc[2], dc[3]);
+                *reinterpret_cast<double2*>(q + c0) = make_double2(qq[0], qq[1]);
+                *reinterpret_cast<double2*>(q + c0 + 2) = make_double2(qq[2], qq[3]);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc.add(dc[e] * qq[e]);
+            }
+        }
+    } else
+    for (int rw = W.w0; rw < rows; rw += W.nw) {
+        const int j = rw % g.n[1], k = rw / g.n[1];
+        const int base = g.n[0] * rw;
+        for (int i = W.lane; i < g.n[0]; i += 32) {
+            const int c = base + i;
+            Neigh v;
+            v.c = dn(c);
+            v.xm = i > 0 ? dn(c - 1) : 0.0;
+            v.xp = i + 1 < g.n[0] ? dn(c + 1) : 0.0;
+            v.ym = j > 0 ? dn(c - sy) : 0.0;
+            v.yp = j + 1 < g.n[1] ? dn(c + sy) : 0.0;
+            v.zm = k > 0 ? dn(c - sz) : 0.0;
+            v.zp = k + 1 < g.n[2] ? dn(c + sz) : 0.0;
+            const double qv = c == 0 ? 0.0 : apply_row(g, i, j, k, v);
+            dst[c] = v.c;
+            q[c] = qv;
+            acc.add(v.c * qv);
+        }
+    }
+    dd sums[1] = {acc.as_dd()};
+    double none[1];
+    block_reduce<1, 0>(red, sums, none);
+    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
+        fold_partials<1, 0>(part, gridDim.x, red, sums, none);
+        if (threadIdx.x == 0) decide_pass1(st, trace, dd_value(sums[0]), flags, dsel);
+    }
+}
+
+int Multigrid::enqueue_pass1(const GridDev& g, void* state, double* d0, double* d1, double* q, Partials part,
+                             rb200_trace* trace, cudaStream_t s) const {
+    int pb = row_blocks(levels_[0]);
+    if (pb > 148 * 8) pb = 148 * 8;  // reduction partials capacity
+    k_mg_pass1<<<pb, MG_THREADS, 0, s>>>(g, levels_[0], static_cast<SolveState*>(state), d0, d1, q, part, trace);
+    return 1;
+}
+
+int Multigrid::enqueue_finish(void* state, const double* r, const double* q, int mode, Partials part,
                               rb200_trace* trace, cudaStream_t s) const {
     const MgLevelDev& L = levels_[0];
     int pb = row_blocks(L);
     if (pb > 148 * 8) pb = 148 * 8;  // reduction partials capacity
-    k_mg_finish_red<<<pb, MG_THREADS, 0, s>>>(L, levels_.size() > 1 ? 1 : 0, static_cast<SolveState*>(state), z, r,
+    k_mg_finish_red<<<pb, MG_THREADS, 0, s>>>(L, levels_.size() > 1 ? 1 : 0, static_cast<SolveState*>(state), r,
                                               q, mode, part, trace);
     return 1;
 }

@@ -60,9 +60,13 @@ public:
     // 2 restart). Returns the number of launches.
     int enqueue(const double* r, const void* state, int mode, cudaStream_t s) const;
     // The finish: last red half-sweep of level 0 (when there is a hierarchy),
-    // z = x with z[0] = 0, r.z and z.q, and the flexible-CG decision.
-    int enqueue_finish(void* state, double* z, const double* r, const double* q, int mode, Partials part,
+    // r.z and z.q with z = x (z[0] = 0), and the flexible-CG decision. z stays
+    // in the finest level's x (FP32); enqueue_pass1 reads it there.
+    int enqueue_finish(void* state, const double* r, const double* q, int mode, Partials part,
                        rb200_trace* trace, cudaStream_t s) const;
+    // The flexible-CG direction pass reading z from the finest level's x.
+    int enqueue_pass1(const GridDev& g, void* state, double* d0, double* d1, double* q, Partials part,
+                      rb200_trace* trace, cudaStream_t s) const;
     const MgLevelDev& fine() const { return levels_[0]; }
     int levels() const { return int(levels_.size()); }
     size_t bytes() const { return bytes_; }

@@ -746,7 +746,7 @@ static int launch_start(const GridDev& g, int method, const Bufs& B, const Multi
     k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part, B.trace);
     if (method == RB200_SGS_PCG_V1) return 2 + launch_sgs(g, B, MODE_INIT, s);
     int n = 2 + mg->enqueue(B.r, B.st, MODE_INIT, s);
-    return n + mg->enqueue_finish(B.st, B.z, B.r, B.q, MODE_INIT, B.part, B.trace, s);
+    return n + mg->enqueue_finish(B.st, B.r, B.q, MODE_INIT, B.part, B.trace, s);
 }
 
 // One PCG iteration (src/pressure.rs:651-734).
@@ -754,8 +754,10 @@ static int launch_iteration(const GridDev& g, int method, const Bufs& B, const M
     const dim3 grid = slab_grid(g), block(TX, TY, 1);
     const int eb = ew_blocks(g.cells);
     const bool flexible = method == RB200_MG_MIXED;
-    k_pass1<ZC><<<grid, block, kSmemPass1, s>>>(g, B.st, B.z, B.d0, B.d1, flexible ? B.q : nullptr, B.maps, B.part,
-                                                B.trace);
+    if (flexible)
+        mg->enqueue_pass1(g, B.st, B.d0, B.d1, B.q, B.part, B.trace, s);
+    else
+        k_pass1<ZC><<<grid, block, kSmemPass1, s>>>(g, B.st, B.z, B.d0, B.d1, nullptr, B.maps, B.part, B.trace);
     if (method == RB200_JACOBI_PCG_V1) {
         k_pass2<ZC, 0><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part,
                                                          B.trace);
@@ -775,7 +777,7 @@ static int launch_iteration(const GridDev& g, int method, const Bufs& B, const M
     }
     k_mg_update<<<eb, EW, 0, s>>>(g, B.st, B.p, B.r, B.d0, B.d1, B.q, B.part, B.trace);
     int n = 2 + mg->enqueue(B.r, B.st, MODE_ITER, s);
-    return n + mg->enqueue_finish(B.st, B.z, B.r, B.q, MODE_ITER, B.part, B.trace, s);
+    return n + mg->enqueue_finish(B.st, B.r, B.q, MODE_ITER, B.part, B.trace, s);
 }
 
 // The gated true-residual check and restart (src/pressure.rs:686-715).
@@ -798,7 +800,7 @@ static int launch_check(const GridDev& g, int method, const Bufs& B, const Multi
     k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part, B.trace);
     if (method == RB200_SGS_PCG_V1) return 2 + launch_sgs(g, B, MODE_REPLACE, s);
     int n = 2 + mg->enqueue(B.r, B.st, MODE_REPLACE, s);
-    return n + mg->enqueue_finish(B.st, B.z, B.r, B.q, MODE_REPLACE, B.part, B.trace, s);
+    return n + mg->enqueue_finish(B.st, B.r, B.q, MODE_REPLACE, B.part, B.trace, s);
 }
 
 static SolveState initial_state(double dt, const rb200_settings& s) {
