@@ -602,7 +602,7 @@ static int row_blocks(const MgLevelDev& L) {
     return int(b < 148 * 16 ? b : 148 * 16);
 }
 
-int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_t s) const {
+int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_t s, bool first_done) const {
     const SolveState* st = static_cast<const SolveState*>(state);
     const int nl = int(levels_.size());
     int launches = 0;
@@ -611,11 +611,17 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
         const MgLevelDev& L = levels_[l];
         const int pb = row_blocks(L);
         for (int sweep = 0; sweep < 2; ++sweep) {
-            k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, (l == 0 && sweep == 0) ? r : nullptr, 0, sweep == 0, st, mode);
+            // the finest level's first red half-sweep may already be done
+            // (k_mg_update_first)
+            if (!(l == 0 && sweep == 0 && first_done)) {
+                k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, (l == 0 && sweep == 0) ? r : nullptr, 0, sweep == 0, st,
+                                                      mode);
+                launches += 1;
+            }
             k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 1, 0, st, mode);
         }
         k_mg_restrict<<<row_blocks(levels_[l + 1]), MG_THREADS, 0, s>>>(L, levels_[l + 1], st, mode);
-        launches += 5;
+        launches += 3;
     }
     // The lower levels, coarsest solve included, in one cluster.
     MgLower P{};
@@ -876,6 +882,108 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_pass1(GridDev g, MgLevelDev L
         fold_partials<1, 0>(part, gridDim.x, red, sums, none);
         if (threadIdx.x == 0) decide_pass1(st, trace, dd_value(sums[0]), flags, dsel);
     }
+}
+
+// The flexible-CG update (p += alpha d, r -= alpha q, |r|^2 and the candidate
+// test) fused with the V-cycle's first half-sweep on the finest level, which
+// needs no neighbour: b = f32(r), red x = b / D, black x = 0. Used when the
+// finest level is a grid-kernel level.
+__global__ void __launch_bounds__(MG_THREADS) k_mg_update_first(GridDev g, MgLevelDev L, SolveState* st,
+                                                                double* __restrict__ p, double* __restrict__ r,
+                                                                const double* d0, const double* d1,
+                                                                const double* __restrict__ q, Partials part,
+                                                                rb200_trace* trace) {
+    __shared__ BlockReduce<1, 0> red;
+    const int flags = st->flags;
+    if (flags & F_STOP) return;
+    const double alpha = st->alpha;
+    const double* __restrict__ d = st->dsel ? d1 : d0;
+    Neu acc;
+    const Warps W = grid_warps();
+    const int n0 = g.n[0], rows = g.n[1] * g.n[2];
+    for (int rw = W.w0; rw < rows; rw += W.nw) {
+        const int j = rw % g.n[1], k = rw / g.n[1];
+        const int base = n0 * rw;
+        const int par = (j + k) & 1;  // the red cells of a quad: par, par + 2
+        const int myz = (int(j > 0) << 2) | (int(j + 1 < g.n[1]) << 3) | (int(k > 0) << 4) |
+                        (int(k + 1 < g.n[2]) << 5);
+        if ((n0 & 3) == 0) {
+            for (int qd = W.lane; qd < (n0 >> 2); qd += 32) {
+                const int i0 = 4 * qd;
+                const int c0 = base + i0;
+                double pv[4], rv[4], dv[4], qv[4];
+                *reinterpret_cast<double2*>(pv) = *reinterpret_cast<const double2*>(p + c0);
+                *reinterpret_cast<double2*>(pv + 2) = *reinterpret_cast<const double2*>(p + c0 + 2);
+                *reinterpret_cast<double2*>(rv) = *reinterpret_cast<const double2*>(r + c0);
+                *reinterpret_cast<double2*>(rv + 2) = *reinterpret_cast<const double2*>(r + c0 + 2);
+                *reinterpret_cast<double2*>(dv) = *reinterpret_cast<const double2*>(d + c0);
+                *reinterpret_cast<double2*>(dv + 2) = *reinterpret_cast<const double2*>(d + c0 + 2);
+                *reinterpret_cast<double2*>(qv) = *reinterpret_cast<const double2*>(q + c0);
+                *reinterpret_cast<double2*>(qv + 2) = *reinterpret_cast<const double2*>(q + c0 + 2);
+                float4 bq, xq = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    if (c0 + e != 0) {  // the gauge row keeps p[0] = r[0] = 0
+                        pv[e] = pv[e] + alpha * dv[e];
+                        rv[e] = rv[e] - alpha * qv[e];
+                        acc.add(rv[e] * rv[e]);
+                    }
+                    f4put(bq, e, float(rv[e]));
+                }
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                    const int e = par + 2 * t;
+                    const int i = i0 + e;
+                    f4put(xq, e, f4get(bq, e) * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz]);
+                }
+                *reinterpret_cast<double2*>(p + c0) = *reinterpret_cast<double2*>(pv);
+                *reinterpret_cast<double2*>(p + c0 + 2) = *reinterpret_cast<double2*>(pv + 2);
+                *reinterpret_cast<double2*>(r + c0) = *reinterpret_cast<double2*>(rv);
+                *reinterpret_cast<double2*>(r + c0 + 2) = *reinterpret_cast<double2*>(rv + 2);
+                *reinterpret_cast<float4*>(L.b + c0) = bq;
+                *reinterpret_cast<float4*>(L.x + c0) = xq;
+            }
+        } else {
+            for (int i = W.lane; i < n0; i += 32) {
+                const int c = base + i;
+                double rc = r[c];
+                if (c != 0) {
+                    p[c] = p[c] + alpha * d[c];
+                    rc = rc - alpha * q[c];
+                    r[c] = rc;
+                    acc.add(rc * rc);
+                }
+                const float b = float(rc);
+                L.b[c] = b;
+                const bool isred = ((i + j + k) & 1) == 0;
+                L.x[c] = isred ? b * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz] : 0.0f;
+            }
+        }
+    }
+    dd sums[1] = {acc.as_dd()};
+    double none[1];
+    block_reduce<1, 0>(red, sums, none);
+    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
+        fold_partials<1, 0>(part, gridDim.x, red, sums, none);
+        if (threadIdx.x == 0) {
+            if (flags & F_PROFILE) return;
+            const int it = st->it + 1;
+            st->it = it;
+            const double recursive_l2 = sqrt(dd_value(sums[0]));
+            st->recursive_l2 = recursive_l2;
+            if (trace) trace[it - 1].recursive_l2 = recursive_l2;
+            if (recursive_l2 <= st->threshold || it == st->max_it) st->flags = flags | F_CANDIDATE;
+        }
+    }
+}
+
+int Multigrid::enqueue_update_first(const GridDev& g, void* state, double* p, double* r, double* d0, double* d1,
+                                    const double* q, Partials part, rb200_trace* trace, cudaStream_t s) const {
+    int pb = row_blocks(levels_[0]);
+    if (pb > 148 * 8) pb = 148 * 8;  // reduction partials capacity
+    k_mg_update_first<<<pb, MG_THREADS, 0, s>>>(g, levels_[0], static_cast<SolveState*>(state), p, r, d0, d1, q,
+                                                part, trace);
+    return 1;
 }
 
 int Multigrid::enqueue_pass1(const GridDev& g, void* state, double* d0, double* d1, double* q, Partials part,

@@ -58,7 +58,14 @@ public:
     // of level 0 (k_mg_finish_red) when the hierarchy has more than one level.
     // Kernels are gated on the solver flags by `mode` (0 init, 1 iteration,
     // 2 restart). Returns the number of launches.
-    int enqueue(const double* r, const void* state, int mode, cudaStream_t s) const;
+    // With first_done the finest level's first red half-sweep is taken as done
+    // (by enqueue_update_first).
+    int enqueue(const double* r, const void* state, int mode, cudaStream_t s, bool first_done = false) const;
+    // Whether enqueue_update_first applies (the finest level is a grid-kernel
+    // level), and the fused flexible-CG update + first red half-sweep.
+    bool fuses_update() const { return lower_first_ > 0; }
+    int enqueue_update_first(const GridDev& g, void* state, double* p, double* r, double* d0, double* d1,
+                             const double* q, Partials part, rb200_trace* trace, cudaStream_t s) const;
     // The finish: last red half-sweep of level 0 (when there is a hierarchy),
     // r.z and z.q with z = x (z[0] = 0), and the flexible-CG decision. z stays
     // in the finest level's x (FP32); enqueue_pass1 reads it there.

@@ -775,8 +775,14 @@ static int launch_iteration(const GridDev& g, int method, const Bufs& B, const M
                                                           B.trace);
         return 2 + launch_sgs(g, B, MODE_ITER, s);
     }
-    k_mg_update<<<eb, EW, 0, s>>>(g, B.st, B.p, B.r, B.d0, B.d1, B.q, B.part, B.trace);
-    int n = 2 + mg->enqueue(B.r, B.st, MODE_ITER, s);
+    int n = 2;
+    if (mg->fuses_update()) {
+        mg->enqueue_update_first(g, B.st, B.p, B.r, B.d0, B.d1, B.q, B.part, B.trace, s);
+        n += mg->enqueue(B.r, B.st, MODE_ITER, s, true);
+    } else {
+        k_mg_update<<<eb, EW, 0, s>>>(g, B.st, B.p, B.r, B.d0, B.d1, B.q, B.part, B.trace);
+        n += mg->enqueue(B.r, B.st, MODE_ITER, s);
+    }
     return n + mg->enqueue_finish(B.st, B.r, B.q, MODE_ITER, B.part, B.trace, s);
 }
 
