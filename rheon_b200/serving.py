@@ -227,12 +227,20 @@ class ServingLoop:
 
 
 def summarize(completions: Sequence[Completion], elapsed: float) -> dict:
+    from . import status_name
+
     ok = [c for c in completions if c.status == 0]
+    rejected: Dict[str, int] = {}
+    for c in completions:
+        if c.status != 0:
+            name = status_name(c.status) if c.status >= 0 else "Error"
+            rejected[name] = rejected.get(name, 0) + 1
     cell_steps = sum(c.edge ** 3 * c.steps for c in ok)
     lat = percentiles([c.latency for c in ok])
     return {
         "requests": len(completions),
         "accepted": len(ok),
+        "rejected": rejected,
         "elapsed_s": elapsed,
         "requests_per_s": len(ok) / elapsed if elapsed > 0 else float("nan"),
         "cell_steps_per_s": cell_steps / elapsed if elapsed > 0 else float("nan"),
