@@ -36,6 +36,29 @@ __device__ __forceinline__ Warps grid_warps() {
     return Warps{t >> 5, int((gridDim.x * blockDim.x) >> 5), int(threadIdx.x & 31)};
 }
 
+// Rows with fewer than 32 work items share a warp: the warp splits into
+// groups of `lanes` lanes (the largest power of two not above the items per
+// row), one row per group.
+__host__ __device__ __forceinline__ int lanes_for(int per) {
+    int lanes = 32;
+    while (lanes > 1 && lanes > per) lanes >>= 1;
+    return lanes;
+}
+struct RowSplit {
+    int first, step, lane, lanes;
+};
+__device__ __forceinline__ RowSplit split_rows(const Warps& W, int per) {
+    const int lanes = lanes_for(per), rpw = 32 / lanes;
+    return RowSplit{W.w0 * rpw + W.lane / lanes, W.nw * rpw, W.lane % lanes, lanes};
+}
+// Work items per row of the level loops (quads of 4 cells, or red-black pairs).
+__host__ __device__ __forceinline__ int sweep_items(const MgLevelDev& L) {
+    return (L.n[0] & 3) == 0 ? (L.n[0] >> 2) : ((L.n[0] + 1) >> 1);
+}
+__host__ __device__ __forceinline__ int restrict_items(const MgLevelDev& L, const MgLevelDev& C) {
+    return ((L.n[0] & 3) == 0 && L.cf[0] == 2) ? (C.n[0] >> 1) : C.n[0];
+}
+
 // Loads of level data: through L1 in the grid kernels, from L2 in the cluster
 // kernel (its CTAs exchange level data through global memory between
 // cluster barriers).
@@ -86,13 +109,14 @@ __device__ __forceinline__ void smooth_rows_v4(const MgLevelDev& L, const double
     const int n0 = L.n[0], quads = n0 >> 2;
     const int rows = L.n[1] * L.n[2];
     const int sy = n0, sz = n0 * L.n[1];
-    for (int row = W.w0; row < rows; row += W.nw) {
+    const RowSplit S = split_rows(W, quads);
+    for (int row = S.first; row < rows; row += S.step) {
         const int j = row % L.n[1], k = row / L.n[1];
         const int base = n0 * row;
         const int par = (color + j + k) & 1;
         const int myz = (int(j > 0) << 2) | (int(j + 1 < L.n[1]) << 3) | (int(k > 0) << 4) |
                         (int(k + 1 < L.n[2]) << 5);
-        for (int q = W.lane; q < quads; q += 32) {
+        for (int q = S.lane; q < quads; q += S.lanes) {
             const int i0 = 4 * q;
             const int c0 = base + i0;
             float4 bq;
@@ -157,11 +181,12 @@ __device__ __forceinline__ void smooth_rows(const MgLevelDev& L, const double* _
     }
     const int hx = (L.n[0] + 1) >> 1;
     const int rows = L.n[1] * L.n[2];
-    for (int row = W.w0; row < rows; row += W.nw) {
+    const RowSplit S = split_rows(W, hx);
+    for (int row = S.first; row < rows; row += S.step) {
         const int j = row % L.n[1], k = row / L.n[1];
         const int base = L.n[0] * row;
         const int par = (color + j + k) & 1;
-        for (int m = W.lane; m < hx; m += 32) {
+        for (int m = S.lane; m < hx; m += S.lanes) {
             const int i = 2 * m + par;
             const int io = i ^ 1;
             if (first && io < L.n[0]) {
@@ -191,9 +216,10 @@ __device__ __forceinline__ void restrict_rows_v4(const MgLevelDev& L, const MgLe
     const int rows = C.n[1] * C.n[2];
     const int cpairs = C.n[0] >> 1;
     const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    for (int row = W.w0; row < rows; row += W.nw) {
+    const RowSplit S = split_rows(W, cpairs);
+    for (int row = S.first; row < rows; row += S.step) {
         const int J = row % C.n[1], K = row / C.n[1];
-        for (int P = W.lane; P < cpairs; P += 32) {
+        for (int P = S.lane; P < cpairs; P += S.lanes) {
             const int i0 = 4 * P;
             float sum[2] = {0.0f, 0.0f};
             for (int dk = 0; dk < L.cf[2]; ++dk)
@@ -239,9 +265,10 @@ __device__ __forceinline__ void restrict_rows(const MgLevelDev& L, const MgLevel
     }
     const int sy = L.n[0], sz = L.n[0] * L.n[1];
     const int rows = C.n[1] * C.n[2];
-    for (int row = W.w0; row < rows; row += W.nw) {
+    const RowSplit S = split_rows(W, C.n[0]);
+    for (int row = S.first; row < rows; row += S.step) {
         const int J = row % C.n[1], K = row / C.n[1];
-        for (int I = W.lane; I < C.n[0]; I += 32) {
+        for (int I = S.lane; I < C.n[0]; I += S.lanes) {
             float sum = 0.0f;
             for (int dk = 0; dk < L.cf[2]; ++dk)
                 for (int dj = 0; dj < L.cf[1]; ++dj)
@@ -283,13 +310,14 @@ __device__ __forceinline__ void prolong_black_rows_v4(const MgLevelDev& L, const
     const int rows = L.n[1] * L.n[2];
     const int sy = n0, sz = n0 * L.n[1];
     const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    for (int row = W.w0; row < rows; row += W.nw) {
+    const RowSplit S = split_rows(W, quads);
+    for (int row = S.first; row < rows; row += S.step) {
         const int j = row % L.n[1], k = row / L.n[1];
         const int base = n0 * row;
         const int par = (1 + j + k) & 1;
         const int myz = (int(j > 0) << 2) | (int(j + 1 < L.n[1]) << 3) | (int(k > 0) << 4) |
                         (int(k + 1 < L.n[2]) << 5);
-        for (int q = W.lane; q < quads; q += 32) {
+        for (int q = S.lane; q < quads; q += S.lanes) {
             const int i0 = 4 * q;
             const int c0 = base + i0;
             const float4 bq = ld4<CG>(L.b + c0);
@@ -329,11 +357,12 @@ __device__ __forceinline__ void prolong_black_rows(const MgLevelDev& L, const Mg
     const int hx = (L.n[0] + 1) >> 1;
     const int rows = L.n[1] * L.n[2];
     const int sy = L.n[0], sz = L.n[0] * L.n[1];
-    for (int row = W.w0; row < rows; row += W.nw) {
+    const RowSplit S = split_rows(W, hx);
+    for (int row = S.first; row < rows; row += S.step) {
         const int j = row % L.n[1], k = row / L.n[1];
         const int base = L.n[0] * row;
         const int par = (1 + j + k) & 1;
-        for (int m = W.lane; m < hx; m += 32) {
+        for (int m = S.lane; m < hx; m += S.lanes) {
             const int i = 2 * m + par;
             if (i >= L.n[0]) continue;
             const int c = i + base;
@@ -594,10 +623,12 @@ int Multigrid::init(const GridDev& g, cudaStream_t s) {
 
 // Blocks of a level loop: one warp per row (j, k) of the level, at most 16
 // blocks per SM.
-static int row_blocks(const MgLevelDev& L) {
+static int row_blocks(const MgLevelDev& L, int per = 32) {
     const long rows = long(L.n[1]) * L.n[2];
+    const long rpw = 32 / lanes_for(per);  // rows per warp
+    const long warps = (rows + rpw - 1) / rpw;
     const long per_block = MG_THREADS / 32;
-    long b = (rows + per_block - 1) / per_block;
+    long b = (warps + per_block - 1) / per_block;
     if (b < 1) b = 1;
     return int(b < 148 * 16 ? b : 148 * 16);
 }
@@ -609,7 +640,7 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
     // Descent on the large levels.
     for (int l = 0; l < lower_first_; ++l) {
         const MgLevelDev& L = levels_[l];
-        const int pb = row_blocks(L);
+        const int pb = row_blocks(L, sweep_items(L));
         for (int sweep = 0; sweep < 2; ++sweep) {
             // the finest level's first red half-sweep may already be done
             // (k_mg_update_first)
@@ -620,7 +651,8 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
             }
             k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 1, 0, st, mode);
         }
-        k_mg_restrict<<<row_blocks(levels_[l + 1]), MG_THREADS, 0, s>>>(L, levels_[l + 1], st, mode);
+        k_mg_restrict<<<row_blocks(levels_[l + 1], restrict_items(L, levels_[l + 1])), MG_THREADS, 0, s>>>(
+            L, levels_[l + 1], st, mode);
         launches += 3;
     }
     // The lower levels, coarsest solve included, in one cluster.
@@ -649,7 +681,7 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
     // fused by the caller into its finish kernel.
     for (int l = lower_first_ - 1; l >= 0; --l) {
         const MgLevelDev& L = levels_[l];
-        const int pb = row_blocks(L);
+        const int pb = row_blocks(L, sweep_items(L));
         k_mg_prolong_black<<<pb, MG_THREADS, 0, s>>>(L, levels_[l + 1], st, mode);
         k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 0, 0, st, mode);
         k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 1, 0, st, mode);
