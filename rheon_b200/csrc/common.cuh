@@ -54,16 +54,25 @@ __device__ __forceinline__ double diag_at(const GridDev& g, int i, int j, int k)
 // FMA, and RN(q + rem*y) is the correctly rounded quotient (Markstein's
 // theorem for round-to-nearest: y within half an ulp of 1/D, q within one ulp
 // of r/D). Three floating-point operations instead of a division. The
-// theorem's conditions (no underflow or overflow in q and the remainder) are
-// met for 2^-900 <= |r| <= 2^900 and a table entry y != 0 (set only for
-// 2^-500 < D < 2^500); every other case divides.
+// theorem's conditions (q and the remainder neither overflow nor underflow)
+// hold for 2^-450 <= |r| < 2^451 with a table entry y != 0 (set only for
+// 2^-500 < D < 2^500): q stays within (2^-950, 2^951) and the remainder above
+// 2^-504. r = +-0 gives +0, so the sign is taken from r (r / D has the sign of
+// r for D > 0). div_diag_fast_ok tells the cases covered; every other case
+// divides.
+__device__ __forceinline__ bool div_diag_range_ok(double r) {
+    const unsigned ahi = unsigned(__double2hiint(r)) & 0x7fffffffu;
+    const unsigned e = ahi >> 20;  // biased exponent; 573..1473: 2^-450 <= |r| < 2^451
+    return e - 573u <= 900u || (ahi | unsigned(__double2loint(r))) == 0u;
+}
+__device__ __forceinline__ bool div_diag_fast_ok(double r, double y) { return y != 0.0 && div_diag_range_ok(r); }
+__device__ __forceinline__ double div_diag_fast(double r, double D, double y) {
+    const double q = r * y;
+    const double rem = fma(-q, D, r);
+    return copysign(fma(rem, y, q), r);
+}
 __device__ __forceinline__ double div_diag(double r, double D, double y) {
-    const double a = fabs(r);
-    if (y != 0.0 && a >= 0x1p-900 && a <= 0x1p900) {
-        const double q = r * y;
-        const double rem = fma(-q, D, r);
-        return fma(rem, y, q);
-    }
+    if (div_diag_fast_ok(r, y)) return div_diag_fast(r, D, y);
     return r / D;
 }
 

@@ -53,10 +53,11 @@ struct TmaMaps {
 };
 
 // Grid barrier of the persistent solver kernel (zeroed before each solve).
+// `count` only grows: barrier m of a solve is passed once it reaches
+// m x (blocks of the grid), so no reset is needed between barriers.
 struct GridBarrier {
-    unsigned count;   // blocks arrived at the current barrier
-    unsigned gen;     // barrier generation
-    unsigned abort;   // a block gave up: every waiting block leaves
+    unsigned long long count;  // arrivals since the solve began
+    unsigned abort;            // a block gave up: every waiting block leaves
     unsigned pad;
 };
 

@@ -31,6 +31,8 @@
 // that runs out marks the solve as failed (execution error) and raises an
 // abort word that ends every other block's barrier wait, and the kernel
 // returns.
+#include <type_traits>
+
 #include "pcg.hpp"
 #include "slab.cuh"
 #include "solve_state.cuh"
@@ -54,24 +56,18 @@ constexpr int STAGE = (2 * PS::SIZE > PS::SIZE + 2 * BOX) ? 2 * PS::SIZE : PS::S
 constexpr size_t kPersistSmem = NS * size_t(STAGE) * sizeof(double);
 constexpr unsigned kBarrierSpins = 1u << 24;
 constexpr int PSTRIDE = 6;                   // doubles per block per partial set (2K + M <= 5)
+constexpr int kFoldPerLane = 8;              // blocks folded per lane: grids of up to 256 blocks
+constexpr int kMaxPersistBlocks = 32 * kFoldPerLane;
 
-__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_acquire_gpu(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];\n" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ void st_relaxed_gpu(unsigned* p, unsigned v) {
-    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
-}
-// Arrival: releases this block's writes (ordered before it by the block
-// barrier) and, for the last arriver, acquires everyone else's.
-__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v) {
-    unsigned old;
-    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;\n" : "=r"(old) : "l"(p), "r"(v) : "memory");
-    return old;
+// Arrival without a return value: releases this block's writes (ordered
+// before it by the block barrier); the waiting loads acquire everyone's.
+__device__ __forceinline__ void red_add_release_gpu(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
 }
 // Order this thread's generic-proxy global accesses with its (or, through a
 // barrier, its block's) later TMA (async-proxy) accesses.
@@ -103,7 +99,7 @@ struct Ctx {
     int tid, lane, tx, ty, tz;
     bool producer;
     unsigned ring;     // ring slots used so far (same count in every thread)
-    unsigned gen;      // barrier generation (thread 0)
+    unsigned long long target;  // arrival count that ends the next barrier (thread 0)
     int set;           // partial set parity
 };
 
@@ -153,7 +149,9 @@ __device__ __forceinline__ Col column(const GridDev& g, const Ctx& c, const Bric
 
 // Row of K applied to one cell (apply_full, src/operator.rs:400-416): the
 // terms in the order X lower, X upper, Y lower, Y upper, Z lower, Z upper,
-// with the x/y masks precomputed per column.
+// with the x/y masks precomputed per column. ZIN: the cell has both z
+// neighbours (a brick strictly inside the box in z).
+template <bool ZIN = false>
 __device__ __forceinline__ double row7(const GridDev& g, int mxy, int k, double cv, double xm, double xp, double ym,
                                        double yp, double zm, double zp) {
     double q = 0.0;
@@ -161,8 +159,8 @@ __device__ __forceinline__ double row7(const GridDev& g, int mxy, int k, double 
     if (mxy & 2) q += g.weight[0] * (cv - xp);
     if (mxy & 4) q += g.weight[1] * (cv - ym);
     if (mxy & 8) q += g.weight[1] * (cv - yp);
-    if (k > 0) q += g.weight[2] * (cv - zm);
-    if (k + 1 < g.n[2]) q += g.weight[2] * (cv - zp);
+    if (ZIN || k > 0) q += g.weight[2] * (cv - zm);
+    if (ZIN || k + 1 < g.n[2]) q += g.weight[2] * (cv - zp);
     return q;
 }
 
@@ -175,31 +173,26 @@ struct Neu2 {
     __device__ __forceinline__ dd as_dd() const { return dd_add(a.as_dd(), b.as_dd()); }
 };
 
-// Grid barrier: arrive (release), wait for the generation to move (acquire).
-// Returns false, with the abort word raised, when the wait runs out or
-// another block aborted.
+// Grid barrier: arrive (release), wait until every block of the grid has
+// arrived (acquire). Returns false, with the abort word raised, when the wait
+// runs out or another block aborted.
 __device__ __forceinline__ bool grid_barrier(Ctx& c, GridBarrier* gb) {
     __shared__ int s_ok;
     fence_proxy_async_global();
     __syncthreads();
     if (c.tid == 0) {
         int ok = 1;
-        const unsigned arrived = atom_add_acq_rel_gpu(&gb->count, 1u);
-        if (arrived == gridDim.x - 1) {
-            st_relaxed_gpu(&gb->count, 0u);
-            st_release_gpu(&gb->gen, c.gen + 1u);
-        } else {
-            unsigned n = 0;
-            while (ld_acquire_gpu(&gb->gen) == c.gen) {
-                if (*(volatile unsigned*)&gb->abort != 0u || ++n > kBarrierSpins) {
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
+        c.target += gridDim.x;
+        red_add_release_gpu(&gb->count, 1ull);
+        unsigned n = 0;
+        while (ld_acquire_gpu(&gb->count) < c.target) {
+            if ((++n & 7u) == 0u && (*(volatile unsigned*)&gb->abort != 0u || n > kBarrierSpins)) {
+                ok = 0;
+                break;
             }
+            __nanosleep(32);
         }
         fence_proxy_async_global();
-        c.gen += 1u;
         if (!ok) atomicExch(&gb->abort, 1u);
         s_ok = ok;
     }
@@ -207,16 +200,48 @@ __device__ __forceinline__ bool grid_barrier(Ctx& c, GridBarrier* gb) {
     return s_ok != 0;
 }
 
-// Publish this block's K sums and M maxima, meet the other blocks, fold all
-// blocks' partials in block order. The fold is identical in every block.
-// `ok` is this thread's pipeline outcome; a failure anywhere in the block
-// fails the block before it arrives. Result valid in thread 0.
+// Block reduction of this block's K sums and M maxima into thread 0, with the
+// block's pipeline outcome `ok` and-reduced at the same barrier.
+template <int K, int M>
+__device__ __forceinline__ bool block_reduce_ok(BlockReduce<K, M>& sm, dd (&sums)[K > 0 ? K : 1],
+                                                double (&maxs)[M > 0 ? M : 1], bool ok) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = PT / 32;
+#pragma unroll
+    for (int q = 0; q < K; ++q) sums[q] = warp_reduce_dd(sums[q]);
+#pragma unroll
+    for (int q = 0; q < M; ++q) maxs[q] = warp_reduce_max(maxs[q]);
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) sm.s[warp][q] = sums[q];
+#pragma unroll
+        for (int q = 0; q < M; ++q) sm.m[warp][q] = maxs[q];
+    }
+    if (!__syncthreads_and(ok)) return false;
+    if (warp == 0) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) sums[q] = lane < NW ? sm.s[lane][q] : dd{0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < M; ++q) maxs[q] = lane < NW ? sm.m[lane][q] : 0.0;
+#pragma unroll
+        for (int q = 0; q < K; ++q) sums[q] = warp_reduce_dd(sums[q]);
+#pragma unroll
+        for (int q = 0; q < M; ++q) maxs[q] = warp_reduce_max(maxs[q]);
+    }
+    return true;
+}
+
+// Publish this block's K sums and M maxima, meet the other blocks, and fold
+// all blocks' partials in warp 0 (lane l takes blocks l, l + 32, ... and adds
+// them pairwise, then the lanes are combined by the butterfly). The fold is
+// identical in every block. `ok` is this thread's pipeline outcome; a failure
+// anywhere in the block fails the block before it arrives. Result valid in
+// thread 0.
 template <int K, int M>
 __device__ __forceinline__ bool reduce_grid(Ctx& c, const PersistArgs& A, bool ok, dd (&sums)[K > 0 ? K : 1],
                                             double (&maxs)[M > 0 ? M : 1]) {
     __shared__ BlockReduce<K, M> red;
-    if (!__syncthreads_and(ok)) return false;
-    block_reduce<K, M>(red, sums, maxs);
+    if (!block_reduce_ok<K, M>(red, sums, maxs, ok)) return false;
     double* base = A.part + size_t(c.set) * gridDim.x * PSTRIDE;
     if (c.tid == 0) {
         double* slot = base + size_t(blockIdx.x) * PSTRIDE;
@@ -230,18 +255,33 @@ __device__ __forceinline__ bool reduce_grid(Ctx& c, const PersistArgs& A, bool o
     }
     c.set ^= 1;
     if (!grid_barrier(c, A.bar)) return false;
+    if (c.tid < 32) {
+        dd v[kFoldPerLane][K > 0 ? K : 1];
+        double mv[M > 0 ? M : 1];
 #pragma unroll
-    for (int q = 0; q < K; ++q) sums[q] = dd{0.0, 0.0};
+        for (int q = 0; q < M; ++q) mv[q] = 0.0;
 #pragma unroll
-    for (int q = 0; q < M; ++q) maxs[q] = 0.0;
-    for (int b = c.tid; b < int(gridDim.x); b += PT) {
-        const double* slot = base + size_t(b) * PSTRIDE;
+        for (int u = 0; u < kFoldPerLane; ++u) {
+            const int b = c.lane + 32 * u;
+            const double* slot = base + size_t(b) * PSTRIDE;
+            const bool have = b < int(gridDim.x);
 #pragma unroll
-        for (int q = 0; q < K; ++q) sums[q] = dd_add(sums[q], dd{__ldcg(slot + 2 * q), __ldcg(slot + 2 * q + 1)});
+            for (int q = 0; q < K; ++q)
+                v[u][q] = have ? dd{__ldcg(slot + 2 * q), __ldcg(slot + 2 * q + 1)} : dd{0.0, 0.0};
 #pragma unroll
-        for (int q = 0; q < M; ++q) maxs[q] = fmax(maxs[q], __ldcg(slot + 2 * K + q));
+            for (int q = 0; q < M; ++q) mv[q] = have ? fmax(mv[q], __ldcg(slot + 2 * K + q)) : mv[q];
+        }
+#pragma unroll
+        for (int w = 1; w < kFoldPerLane; w *= 2)
+#pragma unroll
+            for (int u = 0; u + w < kFoldPerLane; u += 2 * w)
+#pragma unroll
+                for (int q = 0; q < K; ++q) v[u][q] = dd_add(v[u][q], v[u + w][q]);
+#pragma unroll
+        for (int q = 0; q < K; ++q) sums[q] = warp_reduce_dd(v[0][q]);
+#pragma unroll
+        for (int q = 0; q < M; ++q) maxs[q] = warp_reduce_max(mv[q]);
     }
-    block_reduce<K, M>(red, sums, maxs);
     return true;
 }
 
@@ -309,7 +349,7 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
     c.sy = (int(gridDim.x) / c.nbx) % c.nby;
     c.sz = int(gridDim.x) / (c.nbx * c.nby);
     c.ring = 0u;
-    c.gen = 0u;
+    c.target = 0ull;
     c.set = 0;
     if (c.tid < 64) {
         sdiag[c.tid] = g.diag[c.tid];
@@ -317,7 +357,10 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
     }
     if (c.tid == 0) {
         sst = *A.st;
-        c.gen = ld_acquire_gpu(&A.bar->gen);
+        // every barrier of earlier launches was passed by the whole grid, so
+        // the count is a multiple of the grid size plus arrivals at this
+        // launch's first barrier (fewer than the grid: this block has not)
+        c.target = ld_acquire_gpu(&A.bar->count) / gridDim.x * gridDim.x;
         for (int s = 0; s < NS; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], CONSUMER_WARPS);
@@ -431,23 +474,51 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
                 [&](const BrickWalk& w, int s) {
                     const double* sz = smem + s * STAGE;
                     const double* sd = sz + PS::SIZE;
-                    // the new direction at slab element e (src/pressure.rs:720-731)
-                    auto dn = [&](int e) { return fresh ? sz[e] : sz[e] + beta * sd[e]; };
                     const Col col = column(g, c, w, qb);
                     if (!col.own) return;
-                    double v[QPT + 2];
+                    // straight-line cells (no per-cell branch) so that the
+                    // column's cells interleave. FRESH: d = z (after a
+                    // restart); FULL: the brick is whole in z; ZIN: it lies
+                    // strictly inside the box in z (no gauge cell, both z
+                    // neighbours everywhere).
+                    auto cells = [&](auto fresh_t, auto full_t, auto zin_t) {
+                        constexpr bool FRESH = decltype(fresh_t)::value;
+                        constexpr bool FULL = decltype(full_t)::value;
+                        constexpr bool ZIN = decltype(zin_t)::value;
+                        // the new direction at slab element e (src/pressure.rs:720-731)
+                        auto dn = [&](int e) { return FRESH ? sz[e] : sz[e] + beta * sd[e]; };
+                        double v[QPT + 2];
 #pragma unroll
-                    for (int u = 0; u < QPT + 2; ++u) v[u] = dn(col.e0 + (u - 1) * PS::PLANE);
+                        for (int u = 0; u < QPT + 2; ++u) v[u] = dn(col.e0 + (u - 1) * PS::PLANE);
 #pragma unroll
-                    for (int u = 0; u < QPT; ++u) {
-                        if (qb + u >= col.kend) break;
-                        const int e = col.e0 + u * PS::PLANE;
-                        const int cc = col.cc0 + u * plane;
-                        const double qv = cc == 0 ? 0.0
-                                                  : row7(g, col.mxy, col.k0 + qb + u, v[u + 1], dn(e - 1), dn(e + 1),
-                                                         dn(e - PS::SX), dn(e + PS::SX), v[u], v[u + 2]);
-                        dst[cc] = v[u + 1];
-                        (u & 1 ? acc.b : acc.a).add(v[u + 1] * qv);
+                        for (int u = 0; u < QPT; ++u) {
+                            if (!FULL && qb + u >= col.kend) break;
+                            const int e = col.e0 + u * PS::PLANE;
+                            const int cc = col.cc0 + u * plane;
+                            const double kd = row7<ZIN>(g, col.mxy, col.k0 + qb + u, v[u + 1], dn(e - 1), dn(e + 1),
+                                                        dn(e - PS::SX), dn(e + PS::SX), v[u], v[u + 2]);
+                            const double qv = (!ZIN && cc == 0) ? 0.0 : kd;  // gauge row
+                            dst[cc] = v[u + 1];
+                            (u & 1 ? acc.b : acc.a).add(v[u + 1] * qv);
+                        }
+                    };
+                    using T = std::true_type;
+                    using F = std::false_type;
+                    const bool zin = col.k0 > 0 && col.k0 + PZC < g.n[2];
+                    if (fresh) {
+                        if (zin)
+                            cells(T{}, T{}, T{});
+                        else if (col.kend == PZC)
+                            cells(T{}, T{}, F{});
+                        else
+                            cells(T{}, F{}, F{});
+                    } else {
+                        if (zin)
+                            cells(F{}, T{}, T{});
+                        else if (col.kend == PZC)
+                            cells(F{}, T{}, F{});
+                        else
+                            cells(F{}, F{}, F{});
                     }
                 });
             dd sums[1] = {acc.as_dd()};
@@ -480,28 +551,65 @@ __global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_consta
                     const double* sr = sp + BOX;
                     const Col col = column(g, c, w, qb);
                     if (!col.own) return;
-                    double v[QPT + 2];
+                    // straight-line cells; the rare quotient outside the
+                    // fast division's range is redone after the column.
+                    // Gauge row: p[0] + alpha d[0] = p[0] (d[0] = 0), and
+                    // r[0] = z[0] = 0 add nothing to the sums.
+                    auto cells = [&](auto full_t, auto zin_t) {
+                        constexpr bool FULL = decltype(full_t)::value;
+                        constexpr bool ZIN = decltype(zin_t)::value;
+                        double v[QPT + 2];
+                        unsigned slow = 0u;  // cells whose quotient is redone
+                        // ZIN: one diagonal for the whole column
+                        const int mz = col.mxy | 0x30;
+                        const double Dz = sdiag[mz], yz = srdiag[mz];
 #pragma unroll
-                    for (int u = 0; u < QPT + 2; ++u) v[u] = sd[col.e0 + (u - 1) * PS::PLANE];
+                        for (int u = 0; u < QPT + 2; ++u) v[u] = sd[col.e0 + (u - 1) * PS::PLANE];
 #pragma unroll
-                    for (int u = 0; u < QPT; ++u) {
-                        if (qb + u >= col.kend) break;
-                        const int cc = col.cc0 + u * plane;
-                        if (cc == 0) continue;  // gauge row: p[0], r[0] stay 0
-                        const int e = col.e0 + u * PS::PLANE;
-                        const int k = col.k0 + qb + u;
-                        const double qv = row7(g, col.mxy, k, v[u + 1], sd[e - 1], sd[e + 1], sd[e - PS::SX],
-                                               sd[e + PS::SX], v[u], v[u + 2]);
-                        const int bi = col.bi0 + u * (TX * TY);
-                        A.p[cc] = sp[bi] + alpha * v[u + 1];
-                        const double rc = sr[bi] - alpha * qv;
-                        A.r[cc] = rc;
-                        (u & 1 ? acc_rr.b : acc_rr.a).add(rc * rc);
-                        const int m = col.mxy | zmask(g, k);
-                        const double zc = div_diag(rc, sdiag[m], srdiag[m]);
-                        A.z[cc] = zc;
-                        (u & 1 ? acc_rz.b : acc_rz.a).add(rc * zc);
-                    }
+                        for (int u = 0; u < QPT; ++u) {
+                            if (!FULL && qb + u >= col.kend) break;
+                            const int cc = col.cc0 + u * plane;
+                            const int e = col.e0 + u * PS::PLANE;
+                            const int k = col.k0 + qb + u;
+                            const double qv = row7<ZIN>(g, col.mxy, k, v[u + 1], sd[e - 1], sd[e + 1],
+                                                        sd[e - PS::SX], sd[e + PS::SX], v[u], v[u + 2]);
+                            const int bi = col.bi0 + u * (TX * TY);
+                            A.p[cc] = sp[bi] + alpha * v[u + 1];
+                            const double rc = (!ZIN && cc == 0) ? 0.0 : sr[bi] - alpha * qv;
+                            A.r[cc] = rc;
+                            (u & 1 ? acc_rr.b : acc_rr.a).add(rc * rc);
+                            const int m = ZIN ? mz : (col.mxy | zmask(g, k));
+                            const double y = ZIN ? yz : srdiag[m];
+                            const double zc = div_diag_fast(rc, ZIN ? Dz : sdiag[m], y);
+                            const bool fast = ZIN ? div_diag_range_ok(rc) : div_diag_fast_ok(rc, y);
+                            slow |= fast ? 0u : 1u << u;
+                            A.z[cc] = zc;
+                            (u & 1 ? acc_rz.b : acc_rz.a).add(fast ? rc * zc : 0.0);
+                        }
+                        if (ZIN && yz == 0.0) slow = (1u << QPT) - 1u;
+                        if (slow) {
+                            // r / D by division; the residual is re-read
+                            // from this thread's own store above
+#pragma unroll
+                            for (int u = 0; u < QPT; ++u) {
+                                if (!FULL && qb + u >= col.kend) break;
+                                if (!((slow >> u) & 1u)) continue;
+                                const int cc = col.cc0 + u * plane;
+                                const double rc = A.r[cc];
+                                const double zc = rc / sdiag[col.mxy | zmask(g, col.k0 + qb + u)];
+                                A.z[cc] = zc;
+                                (u & 1 ? acc_rz.b : acc_rz.a).add(rc * zc);
+                            }
+                        }
+                    };
+                    using T = std::true_type;
+                    using F = std::false_type;
+                    if (col.k0 > 0 && col.k0 + PZC < g.n[2])
+                        cells(T{}, T{});
+                    else if (col.kend == PZC)
+                        cells(T{}, F{});
+                    else
+                        cells(F{}, F{});
                 });
             dd sums[2] = {acc_rr.as_dd(), acc_rz.as_dd()};
             double none[1] = {0.0};
@@ -536,7 +644,8 @@ int persistent_setup(const GridDev& g, int* blocks) {
     RB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi_persistent, PT, kPersistSmem));
     if (!coop || per_sm < 1) return RB200_OK;
     const int nbricks = ((g.n[0] + TX - 1) / TX) * ((g.n[1] + TY - 1) / TY) * ((g.n[2] + PZC - 1) / PZC);
-    const int cap = sms * per_sm;
+    int cap = sms * per_sm;
+    if (cap > kMaxPersistBlocks) cap = kMaxPersistBlocks;
     *blocks = nbricks < cap ? nbricks : cap;
     return RB200_OK;
 }
