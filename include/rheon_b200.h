@@ -59,7 +59,11 @@ typedef enum rb200_status {
     RB200_COURANT_LIMIT = 16,        /* SimulationError::CourantLimit             */
     RB200_NO_DEVICE = 17,            /* no usable sm_100 device                   */
     RB200_LENGTH_MISMATCH = 18,      /* OperatorError::LengthMismatch             */
-    RB200_INVALID_INITIAL_PRESSURE = 22 /* PressureError::InvalidInitialPressure  */
+    RB200_INVALID_INITIAL_PRESSURE = 22,/* PressureError::InvalidInitialPressure  */
+    RB200_DENSE3D_INVALID_STATE = 23,/* Dense3dError::InvalidState (src/dense3d_sequence.rs:21-27) */
+    RB200_DENSE3D_LIMIT = 24,        /* Dense3dError::Limit                       */
+    RB200_DENSE3D_ABORTED = 25,      /* Dense3dError::Aborted                     */
+    RB200_DENSE3D_IO = 26            /* Dense3dError::Io                          */
 } rb200_status;
 
 /* Pressure methods. JACOBI_PCG_V1 reproduces "jacobi-pcg-v1"
@@ -402,6 +406,103 @@ RB200_API int rb200_carriers_step(rb200_carrier* const* carriers, size_t count, 
 RB200_API int rb200_carrier_profile(rb200_carrier* carrier, int which, int launches, double* avg_ms);
 /* Last pressure of the carrier (host copy). */
 RB200_API int rb200_carrier_pressure(rb200_carrier* carrier, double* out, size_t len);
+/* The carrier's accepted state as dense3D frame fields (device pointers,
+ * valid until the next step or upload): faces, tracer (NULL without one),
+ * fraction NULL, and the pressure of the last accepted step (NULL, i.e.
+ * zeros, before the first accepted step after an upload). Without the
+ * warm-start copy of the accepted pressure, a carrier whose last step was
+ * rejected holds no accepted pressure: RB200_DENSE3D_INVALID_STATE. */
+struct rb200_dense3d_fields;
+RB200_API int rb200_carrier_dense3d_fields(rb200_carrier* carrier, struct rb200_dense3d_fields* fields);
+
+/* ------------------------------------------------------------------------
+ * dense3D accepted-state frames (src/dense3d_sequence.rs). A frame is one
+ * JSON line, byte-identical to write_dense3d_frame (:412-564): header
+ * (frame, time_s, dt_s, carrier/liquid stamps), the fields velocity_x/y/z and
+ * tracer as Rust `{:.9e}` f32 text, fraction and pressure as `{:.17e}` f64
+ * text, then the diagnostics object or null. The encoder formats a
+ * device-resident state on the device; the writer streams frames to a file
+ * descriptor with the limits and terminal errors of Dense3dSequence
+ * (:42-120, :224-341).
+ * ------------------------------------------------------------------------ */
+typedef struct rb200_dense3d_encoder rb200_dense3d_encoder;
+typedef struct rb200_dense3d_writer rb200_dense3d_writer;
+
+/* The frame's scalars: LiquidTransportView clocks/stamps and, for accepted
+ * steps, the LiquidStepReport diagnostics (src/dense3d_sequence.rs:494-556).
+ * has_diagnostics = 0 is the constructor frame (frame 0, time 0, carrier
+ * stamp version 0; "diagnostics":null, dt_s printed as 0). */
+typedef struct rb200_dense3d_frame {
+    uint64_t frame;
+    double time_s;
+    double dt_s;
+    uint64_t carrier_stamp_id, carrier_stamp_version;
+    uint64_t liquid_stamp_id, liquid_stamp_version;
+    int has_diagnostics;
+    uint64_t pressure_iterations;
+    double pressure_residual_m3_s2, carrier_divergence_s_inv, liquid_divergence_s_inv;
+    double volume_before_m3, volume_after_m3, mass_after_kg;
+    double inward_m3, outward_m3, source_m3, balance_m3, rounding_budget_m3;
+} rb200_dense3d_frame;
+
+/* Device pointers of one state. u, v, w: face velocities in
+ * velocity_storage (RB200_FACES_F32, or RB200_FACES_F64 printed as the f32
+ * each value rounds to). tracer (f32), fraction (f64) and pressure (f64) may
+ * be NULL (zeros: the constructor pressure is zero). */
+typedef struct rb200_dense3d_fields {
+    int velocity_storage;
+    const void* u;
+    const void* v;
+    const void* w;
+    const float* tracer;
+    const double* fraction;
+    const double* pressure;
+} rb200_dense3d_fields;
+
+/* Dense3dLimits (src/dense3d_sequence.rs:13-19). */
+typedef struct rb200_dense3d_limits {
+    uint64_t max_cells;
+    uint64_t max_frames;  /* includes the constructor frame */
+    uint64_t max_bytes;   /* total bytes of all lines     */
+} rb200_dense3d_limits;
+
+RB200_API int rb200_dense3d_encoder_create(const rb200_grid* grid, int device, rb200_dense3d_encoder** out);
+RB200_API void rb200_dense3d_encoder_destroy(rb200_dense3d_encoder* encoder);
+/* Upper bound on the bytes of one frame line of this grid. */
+RB200_API uint64_t rb200_dense3d_frame_bound(const rb200_dense3d_encoder* encoder);
+RB200_API const char* rb200_dense3d_encoder_error(const rb200_dense3d_encoder* encoder);
+/* Encode one frame into device memory `out` (capacity bytes) on `stream`,
+ * then wait; *length receives the line's bytes. The preflight of
+ * src/dense3d_sequence.rs:419-494 (finite fields, fraction in [0, 1], clocks,
+ * report) fails with RB200_DENSE3D_INVALID_STATE before any byte is written;
+ * a too small buffer gives RB200_DENSE3D_LIMIT. */
+RB200_API int rb200_dense3d_encode(rb200_dense3d_encoder* encoder, const rb200_dense3d_frame* frame,
+                                   const rb200_dense3d_fields* fields, void* out, uint64_t capacity,
+                                   uint64_t* length, void* stream);
+/* The text of one number as Rust's `{:.17e}` (f64) / `{:.9e}` (f32) prints
+ * it, computed on the host by the encoder's own routine; returns the length
+ * (a NUL follows) or RB200_INVALID_ARGUMENT (capacity < 26 / 17). */
+RB200_API int rb200_dense3d_text_f64(double value, char* out, size_t capacity);
+RB200_API int rb200_dense3d_text_f32(float value, char* out, size_t capacity);
+
+/* Frame stream on an open file descriptor. Creation fails with
+ * RB200_DENSE3D_LIMIT like Dense3dSequence::new (zero frames or bytes, too
+ * many cells). Frames must come in order 0, 1, 2, ... (frame 0: the
+ * constructor frame). Any failure is terminal (later calls give
+ * RB200_DENSE3D_ABORTED): the frame limit (RB200_DENSE3D_LIMIT), a frame
+ * longer than the byte budget left (RB200_DENSE3D_IO, nothing of that frame
+ * is written), a write error (RB200_DENSE3D_IO), the preflight. */
+RB200_API int rb200_dense3d_writer_create(const rb200_grid* grid, const rb200_dense3d_limits* limits, int fd,
+                                          int device, rb200_dense3d_writer** out);
+RB200_API void rb200_dense3d_writer_destroy(rb200_dense3d_writer* writer);
+RB200_API int rb200_dense3d_writer_frame(rb200_dense3d_writer* writer, const rb200_dense3d_frame* frame,
+                                         const rb200_dense3d_fields* fields, void* stream);
+/* fsync of the descriptor (a failure aborts the stream). */
+RB200_API int rb200_dense3d_writer_sync(rb200_dense3d_writer* writer);
+RB200_API uint64_t rb200_dense3d_writer_frames(const rb200_dense3d_writer* writer);
+RB200_API uint64_t rb200_dense3d_writer_bytes(const rb200_dense3d_writer* writer);
+RB200_API int rb200_dense3d_writer_aborted(const rb200_dense3d_writer* writer);
+RB200_API const char* rb200_dense3d_writer_error(const rb200_dense3d_writer* writer);
 
 #ifdef __cplusplus
 }

@@ -102,6 +102,18 @@ class StepReport(C.Structure):
     ]
 
 
+class Dense3dFrame(C.Structure):
+    _fields_ = [("frame", C.c_uint64), ("time_s", C.c_double), ("dt_s", C.c_double),
+                ("carrier_stamp_id", C.c_uint64), ("carrier_stamp_version", C.c_uint64),
+                ("liquid_stamp_id", C.c_uint64), ("liquid_stamp_version", C.c_uint64),
+                ("has_diagnostics", C.c_int), ("pressure_iterations", C.c_uint64),
+                ("pressure_residual_m3_s2", C.c_double), ("carrier_divergence_s_inv", C.c_double),
+                ("liquid_divergence_s_inv", C.c_double), ("volume_before_m3", C.c_double),
+                ("volume_after_m3", C.c_double), ("mass_after_kg", C.c_double), ("inward_m3", C.c_double),
+                ("outward_m3", C.c_double), ("source_m3", C.c_double), ("balance_m3", C.c_double),
+                ("rounding_budget_m3", C.c_double)]
+
+
 def build() -> str:
     """Compile the oracle with its Makefile (idempotent)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
@@ -157,6 +169,8 @@ def _declare(L):
     L.orc_carrier_step_f64.argtypes = [C.POINTER(Grid), C.POINTER(StepParams), _P, _P, _P, _P, C.POINTER(StepReport)]
     L.orc_solve_rhs_initial.argtypes = [C.POINTER(Grid), C.c_double, C.c_int, _P, _P, C.c_double,
                                         C.POINTER(Settings), _P, C.POINTER(Report), _P, C.c_size_t, C.c_int]
+    L.orc_dense3d_frame_text.argtypes = [C.POINTER(Grid), C.POINTER(Dense3dFrame), _P, _P, _P, _P, _P, _P,
+                                         C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
     for name in ("orc_carrier_step_seeded_f32", "orc_carrier_step_seeded_f64"):
         getattr(L, name).argtypes = [C.POINTER(Grid), C.POINTER(StepParams), _P, _P, _P, _P, _P, _P,
                                      C.POINTER(StepReport)]
@@ -355,3 +369,37 @@ def carrier_step(g, faces, params: StepParams, tracer=None, initial=None, keep_p
     if keep_pressure:
         return st, fs, tr, rep, pout
     return st, fs, tr, rep
+
+
+DENSE3D_DIAGNOSTICS = ("pressure_residual_m3_s2", "carrier_divergence_s_inv", "liquid_divergence_s_inv",
+                       "volume_before_m3", "volume_after_m3", "mass_after_kg", "inward_m3", "outward_m3",
+                       "source_m3", "balance_m3", "rounding_budget_m3")
+
+
+def dense3d_frame_text(g, frame=0, time_s=0.0, dt_s=0.0, carrier_stamp=(0, 0), liquid_stamp=(0, 0),
+                       diagnostics=None, faces=None, tracer=None, fraction=None, pressure=None):
+    """write_dense3d_frame (src/dense3d_sequence.rs:412-564) of host arrays:
+    (status, bytes). faces: three f32 arrays; tracer f32, fraction and
+    pressure f64 (None: zeros). Status 0, or 23 for a failed preflight."""
+    f = Dense3dFrame()
+    f.frame = frame
+    f.time_s = time_s
+    f.dt_s = dt_s
+    f.carrier_stamp_id, f.carrier_stamp_version = carrier_stamp
+    f.liquid_stamp_id, f.liquid_stamp_version = liquid_stamp
+    if diagnostics is not None:
+        f.has_diagnostics = 1
+        f.pressure_iterations = int(diagnostics.get("pressure_iterations", 0))
+        for k in DENSE3D_DIAGNOSTICS:
+            setattr(f, k, float(diagnostics.get(k, 0.0)))
+    fs = [_f32(a) for a in faces]
+    tr = _f32(tracer) if tracer is not None else None
+    fr = _f64(fraction) if fraction is not None else None
+    p = _f64(pressure) if pressure is not None else np.zeros(cell_len(g))
+    cap = (sum(a.size for a in fs) + cell_len(g)) * 17 + 2 * cell_len(g) * 26 + 4096
+    buf = C.create_string_buffer(cap)
+    n = C.c_size_t()
+    st = lib().orc_dense3d_frame_text(C.byref(g), C.byref(f), _ptr(fs[0]), _ptr(fs[1]), _ptr(fs[2]),
+                                      _ptr(tr) if tr is not None else None, _ptr(fr) if fr is not None else None,
+                                      _ptr(p), buf, cap, C.byref(n))
+    return st, (buf.raw[:n.value] if st == 0 else b"")

@@ -202,6 +202,32 @@ int orc_carrier_step_seeded_f64(const orc_grid* g, const orc_step_params* prm, d
                                 double* w, float* tracer, const double* initial, double* pressure_out,
                                 orc_step_report* rep);
 
+/* dense3D accepted-state frame (src/dense3d_sequence.rs:412-564): one JSON
+ * line with Rust's `{:.9e}` text for the f32 fields (velocity_x/y/z, tracer)
+ * and `{:.17e}` for the f64 fields (fraction, pressure) and the clocks and
+ * diagnostics. Numbers come from the C library's exact "%.*e" conversion
+ * (round half to even on the exact binary value), with the exponent rewritten
+ * the Rust way (no '+', no leading zeros). tracer / fraction may be NULL
+ * (zeros). Returns 0, or 23 (invalid state: the preflight of
+ * src/dense3d_sequence.rs:419-494 failed; nothing is written), or 24 when
+ * `capacity` is too small; *length receives the line's byte count. */
+typedef struct orc_dense3d_frame {
+    uint64_t frame;
+    double time_s;
+    double dt_s;
+    uint64_t carrier_stamp_id, carrier_stamp_version;
+    uint64_t liquid_stamp_id, liquid_stamp_version;
+    int has_diagnostics;
+    uint64_t pressure_iterations;
+    double pressure_residual_m3_s2, carrier_divergence_s_inv, liquid_divergence_s_inv;
+    double volume_before_m3, volume_after_m3, mass_after_kg;
+    double inward_m3, outward_m3, source_m3, balance_m3, rounding_budget_m3;
+} orc_dense3d_frame;
+
+int orc_dense3d_frame_text(const orc_grid* g, const orc_dense3d_frame* frame, const float* u, const float* v,
+                           const float* w, const float* tracer, const double* fraction, const double* pressure,
+                           char* out, size_t capacity, size_t* length);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,13 +31,17 @@ COURANT_LIMIT = 16
 NO_DEVICE = 17
 LENGTH_MISMATCH = 18
 INVALID_INITIAL_PRESSURE = 22
+DENSE3D_INVALID_STATE = 23
+DENSE3D_LIMIT = 24
+DENSE3D_ABORTED = 25
+DENSE3D_IO = 26
 
 STATUS_NAMES = {
     0: "Ok", 1: "Unsupported", 2: "Execution", 3: "NonFiniteOutput", 4: "NonZeroGauge", 5: "QualityGate",
     6: "Cancelled", 7: "IterationLimit", 8: "Breakdown", 9: "AllocationFailed", 10: "InvalidArgument",
     11: "IncompatibleRhs", 12: "NonFiniteInput", 13: "NonZeroWallVelocity", 14: "ArithmeticFailure",
     15: "DivergenceLimit", 16: "CourantLimit", 17: "NoDevice", 18: "LengthMismatch",
-    22: "InvalidInitialPressure",
+    22: "InvalidInitialPressure", 23: "InvalidState", 24: "Limit", 25: "Aborted", 26: "Io",
 }
 
 
@@ -97,6 +101,27 @@ class StepReport(C.Structure):
 
 
 CANCEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
+
+class Dense3dFrame(C.Structure):
+    _fields_ = [("frame", C.c_uint64), ("time_s", C.c_double), ("dt_s", C.c_double),
+                ("carrier_stamp_id", C.c_uint64), ("carrier_stamp_version", C.c_uint64),
+                ("liquid_stamp_id", C.c_uint64), ("liquid_stamp_version", C.c_uint64),
+                ("has_diagnostics", C.c_int), ("pressure_iterations", C.c_uint64),
+                ("pressure_residual_m3_s2", C.c_double), ("carrier_divergence_s_inv", C.c_double),
+                ("liquid_divergence_s_inv", C.c_double), ("volume_before_m3", C.c_double),
+                ("volume_after_m3", C.c_double), ("mass_after_kg", C.c_double), ("inward_m3", C.c_double),
+                ("outward_m3", C.c_double), ("source_m3", C.c_double), ("balance_m3", C.c_double),
+                ("rounding_budget_m3", C.c_double)]
+
+
+class Dense3dFields(C.Structure):
+    _fields_ = [("velocity_storage", C.c_int), ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p),
+                ("tracer", C.c_void_p), ("fraction", C.c_void_p), ("pressure", C.c_void_p)]
+
+
+class Dense3dLimits(C.Structure):
+    _fields_ = [("max_cells", C.c_uint64), ("max_frames", C.c_uint64), ("max_bytes", C.c_uint64)]
+
 
 _P = C.c_void_p
 _I = C.c_int
@@ -162,6 +187,23 @@ SIGNATURES = {
     "rb200_carriers_step": (_I, [C.POINTER(_P), _S, C.POINTER(StepParams), C.POINTER(StepReport), C.POINTER(_I)]),
     "rb200_carrier_profile": (_I, [_P, _I, _I, C.POINTER(_D)]),
     "rb200_carrier_pressure": (_I, [_P, _P, _S]),
+    "rb200_carrier_dense3d_fields": (_I, [_P, C.POINTER(Dense3dFields)]),
+    "rb200_dense3d_encoder_create": (_I, [C.POINTER(Grid), _I, C.POINTER(_P)]),
+    "rb200_dense3d_encoder_destroy": (None, [_P]),
+    "rb200_dense3d_frame_bound": (C.c_uint64, [_P]),
+    "rb200_dense3d_encoder_error": (C.c_char_p, [_P]),
+    "rb200_dense3d_encode": (_I, [_P, C.POINTER(Dense3dFrame), C.POINTER(Dense3dFields), _P, C.c_uint64,
+                                  C.POINTER(C.c_uint64), _P]),
+    "rb200_dense3d_text_f64": (_I, [_D, C.c_char_p, _S]),
+    "rb200_dense3d_text_f32": (_I, [C.c_float, C.c_char_p, _S]),
+    "rb200_dense3d_writer_create": (_I, [C.POINTER(Grid), C.POINTER(Dense3dLimits), _I, _I, C.POINTER(_P)]),
+    "rb200_dense3d_writer_destroy": (None, [_P]),
+    "rb200_dense3d_writer_frame": (_I, [_P, C.POINTER(Dense3dFrame), C.POINTER(Dense3dFields), _P]),
+    "rb200_dense3d_writer_sync": (_I, [_P]),
+    "rb200_dense3d_writer_frames": (C.c_uint64, [_P]),
+    "rb200_dense3d_writer_bytes": (C.c_uint64, [_P]),
+    "rb200_dense3d_writer_aborted": (_I, [_P]),
+    "rb200_dense3d_writer_error": (C.c_char_p, [_P]),
 }
 
 _lib = None

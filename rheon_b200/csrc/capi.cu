@@ -232,6 +232,10 @@ const char* rb200_status_string(int status) {
         case RB200_NO_DEVICE: return "no sm_100 device";
         case RB200_LENGTH_MISMATCH: return "field length does not match the grid";
         case RB200_INVALID_INITIAL_PRESSURE: return "initial pressure requires a sealed operator and zero gauge";
+        case RB200_DENSE3D_INVALID_STATE: return "dense3D frame: invalid state";
+        case RB200_DENSE3D_LIMIT: return "dense3D export limit";
+        case RB200_DENSE3D_ABORTED: return "dense3D export aborted";
+        case RB200_DENSE3D_IO: return "dense3D output error";
         default: return "unknown status";
     }
 }

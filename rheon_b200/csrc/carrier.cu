@@ -262,6 +262,8 @@ struct rb200_carrier {
     int fixed_nodes = 0;
     size_t bytes = 0;
     bool in_flight = false;
+    uint64_t accepted_steps = 0;  // accepted steps since the last upload
+    bool last_rejected = false;   // the last step was rejected
     std::string err;
     ~rb200_carrier() {
         cudaSetDevice(device);
@@ -364,6 +366,8 @@ int capture_step(rb200_carrier* c) {
 
 int upload_rate(rb200_carrier* c) {
     // velocity rate and validation of the accepted state (after an upload)
+    c->accepted_steps = 0;
+    c->last_rejected = false;
     const GridDev& g = c->g;
     int* d_flags = &c->cd->flags;
     double* sc = c->cd->scalars;
@@ -621,7 +625,33 @@ int rb200_carrier_step_wait(rb200_carrier* carrier, rb200_step_report* report) {
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]) == cudaSuccess) report->pressure_ms = double(ms);
     report->kernel_launches = uint64_t(c->fixed_nodes) + uint64_t(h.trips) * uint64_t(c->solver.nodes_per_chunk());
+    c->last_rejected = h.step_status != RB200_OK;
+    if (!c->last_rejected) c->accepted_steps += 1;
     return h.step_status;
+}
+
+int rb200_carrier_dense3d_fields(rb200_carrier* carrier, rb200_dense3d_fields* f) {
+    if (!carrier || !f) return RB200_INVALID_ARGUMENT;
+    rb200_carrier* c = carrier;
+    if (c->in_flight) return RB200_INVALID_ARGUMENT;
+    const int a = c->h_cd->acc;
+    f->velocity_storage = c->cfg.storage;
+    f->u = c->faces[a][0];
+    f->v = c->faces[a][1];
+    f->w = c->faces[a][2];
+    f->tracer = c->tracer[0] ? c->tracer[c->h_cd->tacc] : nullptr;
+    f->fraction = nullptr;
+    if (c->accepted_steps == 0) {
+        f->pressure = nullptr;
+    } else if (c->accepted_p) {
+        f->pressure = c->accepted_p;
+    } else if (!c->last_rejected) {
+        f->pressure = c->solver.p();
+    } else {
+        c->err = "dense3D export: InvalidState(\"no accepted pressure after a rejected step\")";
+        return RB200_DENSE3D_INVALID_STATE;
+    }
+    return RB200_OK;
 }
 
 int rb200_carrier_step(rb200_carrier* carrier, const rb200_step_params* params, rb200_step_report* report,
