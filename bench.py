@@ -65,6 +65,10 @@ def parse():
     ap.add_argument("--serving-plain-requests", type=int, default=12)
     ap.add_argument("--serving-budget-gb", type=float, default=150.0)
     ap.add_argument("--no-profile", action="store_true")
+    ap.add_argument("--no-dense3d", action="store_true")
+    ap.add_argument("--dense3d", action="store_true",
+                    help="dense3D frame stream alone (device encode, end to end to a file descriptor, CPU oracle)")
+    ap.add_argument("--dense3d-frames", type=int, default=20)
     ap.add_argument("--buoyant-blob", action="store_true",
                     help="mixed-precision buoyant-blob run (rel 1e-10) in lockstep with the f64 carrier, "
                          "per-step divergence and velocity/tracer error; --n cells per axis, --steps steps")
@@ -399,6 +403,123 @@ def run_buoyant_blob(args, local):
 
 
 # ------------------------------------------------------------------ our arm
+def run_dense3d(args, local, with_cpu):
+    """dense3D accepted-state frames (src/dense3d_sequence.rs:412-564) of the
+    mixed carrier's state after one step at n^3 (f32 faces and tracer, a
+    uniform [0, 1) f64 fraction, the step's f64 pressure): device encode time
+    per frame (CUDA events on the encoding stream), the same frames end to end
+    through the frame writer (encode, device-to-host copy into pinned memory,
+    write(2) to /dev/null), and the oracle's text of one frame on one host
+    core."""
+    import torch
+
+    import rheon_b200 as R
+    from rheon_b200 import dense3d as D
+
+    torch.cuda.set_device(local)
+    n = args.n
+    g = R.GridGeometry((n, n, n))
+    sim = R.CarrierSimulation(g, R.CarrierConfig.mixed(with_tracer=True, device=local))
+    sim.init_fourier(seed=args.seed)
+    rep = sim.step(R.StepParams(requested_dt=MAXF, cfl=0.5))
+    gen = torch.Generator(device=f"cuda:{local}")
+    gen.manual_seed(args.seed)
+    fraction = torch.rand(g.cell_len(), dtype=torch.float64, device=f"cuda:{local}", generator=gen)
+    fields = D.Dense3dFields.from_carrier(sim, fraction=fraction)
+    diag = dict(pressure_iterations=rep.pressure.iterations, pressure_residual_m3_s2=rep.pressure.true_residual_max,
+                carrier_divergence_s_inv=rep.actual_divergence_max)
+    info = D.Dense3dFrameInfo(frame=1, time_s=rep.time, dt_s=rep.dt, carrier_stamp=(1, rep.generation),
+                              liquid_stamp=(2, rep.generation), diagnostics=diag)
+    enc = D.Dense3dEncoder(g, device=local)
+    out = torch.empty(enc.bound(), dtype=torch.uint8, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+    frames = max(1, args.dense3d_frames)
+    for _ in range(3):
+        length = enc.encode_into(info, fields, out.data_ptr(), out.numel(), stream.cuda_stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * frames)]
+    for k in range(frames):
+        ev[2 * k].record(stream)
+        length = enc.encode_into(info, fields, out.data_ptr(), out.numel(), stream.cuda_stream)
+        ev[2 * k + 1].record(stream)
+    torch.cuda.synchronize()
+    enc_ms = statistics.median(ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(frames))
+    faces_n = sum(g.face_len(a) for a in range(3))
+    in_bytes = 4 * (faces_n + g.cell_len()) + 16 * g.cell_len()
+    hbm, kind = peaks()
+    achieved = (in_bytes + length) / (enc_ms / 1e3) / 1e9
+    cpu = {}
+    if with_cpu:
+        import oracle as O
+
+        oracle_faces, tracer = sim.download(with_tracer=True)
+        p = sim.pressure()
+        fr = fraction.cpu().numpy()
+        t0 = time.perf_counter()
+        st, line = O.dense3d_frame_text(O.grid((n, n, n)), frame=1, time_s=rep.time, dt_s=rep.dt,
+                                        carrier_stamp=(1, rep.generation), liquid_stamp=(2, rep.generation),
+                                        diagnostics=diag, faces=oracle_faces, tracer=tracer, fraction=fr, pressure=p)
+        cpu_s = time.perf_counter() - t0
+        cpu["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "frames/s", "cores": 1, "kind": "port",
+                               "sample": f"one {n}^3 frame with the oracle's text routine (C library %.*e)"}
+        out_host = out[:length].cpu().numpy().tobytes()
+        cpu["matches_oracle"] = bool(st == 0 and line == out_host)
+    # end to end: the frame writer on /dev/null (frame 0 is the constructor
+    # frame); the copies and writes run behind write_frame, flush waits for all
+    fd = os.open(os.devnull, os.O_WRONLY)
+    w = D.Dense3dFrameWriter(g, fd, D.Dense3dLimits(g.cell_len(), 3 * frames + 2, 1 << 62), device=local)
+    w.write_frame(D.Dense3dFrameInfo(carrier_stamp=(1, 0), liquid_stamp=(2, 0)), fields, stream.cuda_stream)
+    w.flush()
+    t0 = time.perf_counter()
+    for k in range(1, frames + 1):
+        w.write_frame(D.Dense3dFrameInfo(frame=k, time_s=rep.time, dt_s=rep.dt, carrier_stamp=(1, k),
+                                         liquid_stamp=(2, k), diagnostics=diag), fields, stream.cuda_stream)
+    w.flush()
+    e2e_s = (time.perf_counter() - t0) / frames
+    written = w.bytes_written()
+    # dataset generation: one accepted mixed step, then its frame, repeatedly,
+    # against the same steps without frames
+    prm = R.StepParams(requested_dt=MAXF, cfl=0.5)
+    sim_stream = sim.stream()
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        sim.step(prm)
+    steps_s = (time.perf_counter() - t0) / frames
+    t0 = time.perf_counter()
+    for k in range(frames + 1, 2 * frames + 1):
+        r = sim.step(prm)
+        w.write_frame(D.Dense3dFrameInfo(frame=k, time_s=r.time, dt_s=r.dt, carrier_stamp=(1, r.generation),
+                                         liquid_stamp=(2, r.generation),
+                                         diagnostics=dict(diag, pressure_iterations=r.pressure.iterations)),
+                      D.Dense3dFields.from_carrier(sim, fraction=fraction), sim_stream)
+    w.flush()
+    stream_s = (time.perf_counter() - t0) / frames
+    w.close()
+    os.close(fd)
+    res = {
+        "workload": f"dense3D frame of a {n}^3 carrier state: {faces_n + g.cell_len()} f32 values "
+                    f"({{:.9e}}) and {2 * g.cell_len()} f64 values ({{:.17e}})",
+        "frame_bytes": length,
+        "ms_per_frame": enc_ms,
+        "value": 1e3 / enc_ms,
+        "unit": "frames/s",
+        "text_gb_per_s": length / (enc_ms / 1e3) / 1e9,
+        "values_per_s": (faces_n + 3 * g.cell_len()) / (enc_ms / 1e3),
+        "roofline": {"kernel": "k_d3_measure + k_d3_scan + k_d3_write (one frame)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm, "peak_kind": kind, "unit": "GB/s", "frac": achieved / hbm,
+                     "algorithmic_bytes_per_frame": in_bytes + length,
+                     "note": "inputs read once and the text written once per frame; the inputs (L2-sized) are "
+                             "read by two passes, the text (> L2) is written once"},
+        "e2e": {"value": 1.0 / e2e_s, "unit": "frames/s", "ms_per_frame": e2e_s * 1e3,
+                "d2h_bytes_per_frame": written // (frames + 1), "h2d_bytes_per_frame": 0,
+                "sink": "write(2) to /dev/null after a device-to-host copy into pinned memory"},
+        "step_and_frame": {"ms_per_step_with_frame": stream_s * 1e3, "ms_per_step_alone": steps_s * 1e3,
+                           "steps": frames, "carrier": f"mixed, {n}^3, CFL 0.5"},
+    }
+    res.update(cpu)
+    sim.close()
+    return res
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -612,6 +733,8 @@ def run_ours(args, world, rank, local):
     if serving:
         result["serving"] = serving
     sim.close()
+    if not args.no_dense3d and world == 1:
+        result["dense3d"] = run_dense3d(args, local, with_cpu=not args.no_cpu_baseline)
     return result
 
 
@@ -701,6 +824,9 @@ def main():
         return
     if args.buoyant_blob:
         print(json.dumps(run_buoyant_blob(args, local)), flush=True)
+        return
+    if args.dense3d:
+        print(json.dumps(run_dense3d(args, local, with_cpu=not args.no_cpu_baseline)), flush=True)
         return
     result = run_ours(args, world, rank, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -488,17 +488,25 @@ RB200_API int rb200_dense3d_text_f32(float value, char* out, size_t capacity);
 /* Frame stream on an open file descriptor. Creation fails with
  * RB200_DENSE3D_LIMIT like Dense3dSequence::new (zero frames or bytes, too
  * many cells). Frames must come in order 0, 1, 2, ... (frame 0: the
- * constructor frame). Any failure is terminal (later calls give
- * RB200_DENSE3D_ABORTED): the frame limit (RB200_DENSE3D_LIMIT), a frame
- * longer than the byte budget left (RB200_DENSE3D_IO, nothing of that frame
- * is written), a write error (RB200_DENSE3D_IO), the preflight. */
+ * constructor frame). rb200_dense3d_writer_frame encodes the frame on
+ * `stream` and waits for the encode; the device-to-host copy and the write(2)
+ * then run on the writer's own stream and thread, overlapping the caller's
+ * next step (two frames in flight at most). Any failure is terminal (later
+ * calls give RB200_DENSE3D_ABORTED): the frame limit (RB200_DENSE3D_LIMIT), a
+ * frame longer than the byte budget left (RB200_DENSE3D_IO, nothing of that
+ * frame is written), the preflight, and a failed copy or write
+ * (RB200_DENSE3D_IO, reported by the next frame, flush or sync call). */
 RB200_API int rb200_dense3d_writer_create(const rb200_grid* grid, const rb200_dense3d_limits* limits, int fd,
                                           int device, rb200_dense3d_writer** out);
 RB200_API void rb200_dense3d_writer_destroy(rb200_dense3d_writer* writer);
 RB200_API int rb200_dense3d_writer_frame(rb200_dense3d_writer* writer, const rb200_dense3d_frame* frame,
                                          const rb200_dense3d_fields* fields, void* stream);
-/* fsync of the descriptor (a failure aborts the stream). */
+/* Dense3dSequence::flush (src/dense3d_sequence.rs:332-341): returns once
+ * every accepted frame is written; terminal on failure. */
+RB200_API int rb200_dense3d_writer_flush(rb200_dense3d_writer* writer);
+/* flush, then fsync of the descriptor (a failure aborts the stream). */
 RB200_API int rb200_dense3d_writer_sync(rb200_dense3d_writer* writer);
+/* Frames accepted (encoded and queued), and bytes written so far. */
 RB200_API uint64_t rb200_dense3d_writer_frames(const rb200_dense3d_writer* writer);
 RB200_API uint64_t rb200_dense3d_writer_bytes(const rb200_dense3d_writer* writer);
 RB200_API int rb200_dense3d_writer_aborted(const rb200_dense3d_writer* writer);

@@ -199,6 +199,7 @@ SIGNATURES = {
     "rb200_dense3d_writer_create": (_I, [C.POINTER(Grid), C.POINTER(Dense3dLimits), _I, _I, C.POINTER(_P)]),
     "rb200_dense3d_writer_destroy": (None, [_P]),
     "rb200_dense3d_writer_frame": (_I, [_P, C.POINTER(Dense3dFrame), C.POINTER(Dense3dFields), _P]),
+    "rb200_dense3d_writer_flush": (_I, [_P]),
     "rb200_dense3d_writer_sync": (_I, [_P]),
     "rb200_dense3d_writer_frames": (C.c_uint64, [_P]),
     "rb200_dense3d_writer_bytes": (C.c_uint64, [_P]),

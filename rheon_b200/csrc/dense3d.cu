@@ -17,8 +17,10 @@
 // flip the rounding: those values (ties among them) are decided exactly by
 // comparing 2 x 10^k with 2I + 1 in wide integers, as powers of 5 and 2.
 //
-// Kernels (one frame): k_d3_measure formats every value of a 1024-value chunk
-// in registers and reduces the chunk's text length; k_d3_scan turns the
+// Kernels (one frame): k_d3_measure sizes every value of a 1024-value chunk
+// from its binary exponent and a table of the first value of each printed
+// exponent (exp_thresholds.inc), without forming digits, and reduces the
+// chunk's text length; k_d3_scan turns the
 // chunk lengths into offsets; k_d3_write formats the chunk again, places each
 // thread's text in shared memory at its scanned offset and copies the chunk
 // to the output with word stores. Validation (the preflight of
@@ -27,9 +29,12 @@
 #include <errno.h>
 #include <unistd.h>
 
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <thread>
 
 #include "internal.hpp"
 
@@ -48,6 +53,32 @@ __device__ const Pow10Entry kPow10Dev[] = {
 #include "pow10_table.inc"
 };
 constexpr int kPow10Count = int(sizeof(kPow10Host) / sizeof(kPow10Host[0]));
+
+// Printed-exponent thresholds (exp_thresholds.inc): entry E - MIN is the bit
+// pattern of the first positive value whose P-digit rounding reaches 10^E.
+#include "exp_thresholds.inc"
+const unsigned long long kThr64Host[] = {KEXPTHR64_LIST};
+__device__ const unsigned long long kThr64Dev[] = {KEXPTHR64_LIST};
+const unsigned long long kThr32Host[] = {KEXPTHR32_LIST};
+__device__ const unsigned long long kThr32Dev[] = {KEXPTHR32_LIST};
+
+template <int P>
+__host__ __device__ __forceinline__ unsigned long long exp_threshold(int e) {
+    if (P == 18) {
+        const int i = e - KEXPTHR64_MIN;
+#ifdef __CUDA_ARCH__
+        return __ldg(&kThr64Dev[i]);
+#else
+        return kThr64Host[i];
+#endif
+    }
+    const int i = e - KEXPTHR32_MIN;
+#ifdef __CUDA_ARCH__
+    return __ldg(&kThr32Dev[i]);
+#else
+    return kThr32Host[i];
+#endif
+}
 
 __host__ __device__ __forceinline__ Pow10Entry pow10_entry(int k) {
     int i = k - kPow10Min;
@@ -135,7 +166,7 @@ __host__ __device__ int wide_cmp(const Wide& a, const Wide& b) {
 // integers after moving the powers of 5 and of 2 to one side each. The
 // operands stay below 2^900 for every finite double (at most 53 bits of m
 // times 5^343, or 65 bits of 2I + 1 times 5^300).
-__host__ __device__ int exact_cmp(uint64_t m, int e2, int k, uint64_t I) {
+__host__ __device__ __noinline__ int exact_cmp(uint64_t m, int e2, int k, uint64_t I) {
     Wide a, b;
     a.set(m);
     b.set(2 * I + 1, uint32_t(I >> 63));
@@ -259,6 +290,32 @@ __host__ __device__ __forceinline__ Num num32(float x) {
     return Num{m ? to_decimal<10>(m, e2) : Dec{0, 0}, (b >> 31) != 0};
 }
 
+// Length of the text of a value with magnitude bits `abs` (a positive
+// finite value, or zero) without forming its digits: the printed exponent is
+// the binary estimate E (E <= floor(log10 x)) raised by the thresholds it
+// reaches (at most two).
+template <int P>
+__host__ __device__ __forceinline__ int text_len_bits(unsigned long long abs, int mant_bits, int bias, int sub_e2,
+                                                      bool neg) {
+    int e = 0;
+    if (abs) {
+        const int be = int(abs >> mant_bits);
+        const int L = be ? be - bias : sub_e2 + 63 - clz64(abs);  // floor(log2 x)
+        const int E = (L * 78913) >> 18;
+        e = E + int(abs >= exp_threshold<P>(E + 1)) + int(abs >= exp_threshold<P>(E + 2));
+    }
+    const int ae = e < 0 ? -e : e;
+    return int(neg) + P + 2 + int(e < 0) + (ae >= 100 ? 3 : (ae >= 10 ? 2 : 1));
+}
+__host__ __device__ __forceinline__ int len64(double x) {
+    const uint64_t b = bits_of(x);
+    return text_len_bits<18>(b & 0x7fffffffffffffffull, 52, 1023, -1074, (b >> 63) != 0);
+}
+__host__ __device__ __forceinline__ int len32(float x) {
+    const uint32_t b = bits_of(x);
+    return text_len_bits<10>(b & 0x7fffffffu, 23, 127, -149, (b >> 31) != 0);
+}
+
 template <int P>
 __host__ __device__ __forceinline__ int text_len(const Num& v) {
     const int ae = v.d.e < 0 ? -v.d.e : v.d.e;
@@ -329,41 +386,6 @@ struct D3Args {
     int nblocks;
 };
 
-struct Item {
-    Num v;
-    int seg;
-    int len;  // value text plus its separator
-    unsigned bad;
-};
-
-__device__ __forceinline__ Item d3_item(const D3Args& a, unsigned long long i) {
-    Item it;
-    int s = 0;
-#pragma unroll
-    for (int q = 0; q < 5; ++q) s += i >= a.end[q] ? 1 : 0;
-    const unsigned long long j = i - (s ? a.end[s - 1] : 0ull);
-    it.seg = s;
-    it.bad = 0u;
-    if (s < 4) {
-        float x = 0.0f;
-        if (s < 3)
-            x = a.vel_f64 ? float(static_cast<const double*>(a.field[s])[j]) : static_cast<const float*>(a.field[s])[j];
-        else if (a.field[3])
-            x = static_cast<const float*>(a.field[3])[j];
-        if (!isfinite(x)) it.bad = s < 3 ? BAD_VELOCITY : BAD_CELL;
-        it.v = num32(x);
-        it.len = text_len<10>(it.v);
-    } else {
-        double x = 0.0;
-        if (a.field[s]) x = static_cast<const double*>(a.field[s])[j];
-        if (!isfinite(x) || (s == 4 && !(x >= 0.0 && x <= 1.0))) it.bad = BAD_CELL;
-        it.v = num64(x);
-        it.len = text_len<18>(it.v);
-    }
-    it.len += (i + 1 == a.end[s]) ? a.off[s + 2] - a.off[s + 1] : 1;
-    return it;
-}
-
 __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long v, unsigned long long* sm) {
 #pragma unroll
     for (int m = 16; m >= 1; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
@@ -378,6 +400,31 @@ __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long v
     return v;  // valid in thread 0
 }
 
+// Text length of value i with its separator, from the exponent thresholds
+// (no digits), and its preflight.
+__device__ __forceinline__ int d3_len(const D3Args& a, unsigned long long i, unsigned& bad) {
+    int s = 0;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) s += i >= a.end[q] ? 1 : 0;
+    const unsigned long long j = i - (s ? a.end[s - 1] : 0ull);
+    int len;
+    if (s < 4) {
+        float x = 0.0f;
+        if (s < 3)
+            x = a.vel_f64 ? float(static_cast<const double*>(a.field[s])[j]) : static_cast<const float*>(a.field[s])[j];
+        else if (a.field[3])
+            x = static_cast<const float*>(a.field[3])[j];
+        if (!isfinite(x)) bad |= s < 3 ? BAD_VELOCITY : BAD_CELL;
+        len = len32(x);
+    } else {
+        double x = 0.0;
+        if (a.field[s]) x = static_cast<const double*>(a.field[s])[j];
+        if (!isfinite(x) || (s == 4 && !(x >= 0.0 && x <= 1.0))) bad |= BAD_CELL;
+        len = len64(x);
+    }
+    return len + ((i + 1 == a.end[s]) ? a.off[s + 2] - a.off[s + 1] : 1);
+}
+
 __global__ void __launch_bounds__(D3_THREADS) k_d3_measure(D3Args a) {
     __shared__ unsigned long long sm[32];
     const unsigned long long base = (unsigned long long)blockIdx.x * D3_CHUNK + threadIdx.x * D3_VPT;
@@ -387,9 +434,7 @@ __global__ void __launch_bounds__(D3_THREADS) k_d3_measure(D3Args a) {
     for (int u = 0; u < D3_VPT; ++u) {
         const unsigned long long i = base + u;
         if (i >= a.end[5]) break;
-        const Item it = d3_item(a, i);
-        len += it.len;
-        bad |= it.bad;
+        len += d3_len(a, i, bad);
     }
     bad = __reduce_or_sync(0xffffffffu, bad);
     if (bad && (threadIdx.x & 31) == 0) atomicOr(&a.status->bad, bad);
@@ -433,7 +478,7 @@ __global__ void __launch_bounds__(1024) k_d3_scan(D3Args a) {
 }
 
 __global__ void __launch_bounds__(D3_THREADS) k_d3_write(D3Args a) {
-    __shared__ __align__(16) char stage[D3_STAGE];
+    __shared__ __align__(16) char stage[D3_STAGE + 16];
     __shared__ unsigned long long sm[32];
     const D3Status st = *a.status;
     const unsigned long long header = (unsigned long long)(a.off[1] - a.off[0]);
@@ -441,17 +486,12 @@ __global__ void __launch_bounds__(D3_THREADS) k_d3_write(D3Args a) {
     if (blockIdx.x == 0)
         for (int c = threadIdx.x; c < int(header); c += D3_THREADS) a.out[c] = a.strings[a.off[0] + c];
     const unsigned long long base = (unsigned long long)blockIdx.x * D3_CHUNK + threadIdx.x * D3_VPT;
-    Item it[D3_VPT];
+    // lengths first (no digits), then the block's exclusive scan of them
     int mine = 0;
-#pragma unroll
-    for (int u = 0; u < D3_VPT; ++u) {
-        it[u].len = 0;
-        if (base + u < a.end[5]) {
-            it[u] = d3_item(a, base + u);
-            mine += it[u].len;
-        }
-    }
-    // exclusive scan of the thread lengths
+    unsigned bad = 0u;
+#pragma unroll 1
+    for (int u = 0; u < D3_VPT; ++u)
+        if (base + u < a.end[5]) mine += d3_len(a, base + u, bad);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int x = mine;
 #pragma unroll
@@ -461,35 +501,52 @@ __global__ void __launch_bounds__(D3_THREADS) k_d3_write(D3Args a) {
     }
     if (lane == 31) sm[warp] = (unsigned long long)x;
     __syncthreads();
+    // the chunk's text sits in shared memory at the output's alignment
+    // modulo 16, so that 16-byte words of both line up
+    char* dst = a.out + header + a.block_off[blockIdx.x];
+    const unsigned shift = unsigned((uintptr_t)dst & 15u);
     int before = 0;
     for (int q = 0; q < warp; ++q) before += int(sm[q]);
-    int p = before + x - mine;
-#pragma unroll
+    int p = int(shift) + before + x - mine;
+    // the digits, one value at a time (one copy of the code for both types)
+#pragma unroll 1
     for (int u = 0; u < D3_VPT; ++u) {
-        if (!it[u].len) continue;
-        p += it[u].seg < 4 ? text_put<10>(it[u].v, stage + p) : text_put<18>(it[u].v, stage + p);
         const unsigned long long i = base + u;
-        if (i + 1 == a.end[it[u].seg]) {
-            for (int c = a.off[it[u].seg + 1]; c < a.off[it[u].seg + 2]; ++c) stage[p++] = a.strings[c];
+        if (i >= a.end[5]) break;
+        int s = 0;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) s += i >= a.end[q] ? 1 : 0;
+        const unsigned long long j = i - (s ? a.end[s - 1] : 0ull);
+        if (s < 4) {
+            float v = 0.0f;
+            if (s < 3)
+                v = a.vel_f64 ? float(static_cast<const double*>(a.field[s])[j])
+                              : static_cast<const float*>(a.field[s])[j];
+            else if (a.field[3])
+                v = static_cast<const float*>(a.field[3])[j];
+            p += text_put<10>(num32(v), stage + p);
+        } else {
+            const double v = a.field[s] ? static_cast<const double*>(a.field[s])[j] : 0.0;
+            p += text_put<18>(num64(v), stage + p);
+        }
+        if (i + 1 == a.end[s]) {
+            for (int c = a.off[s + 1]; c < a.off[s + 2]; ++c) stage[p++] = a.strings[c];
         } else {
             stage[p++] = ',';
         }
     }
     __syncthreads();
-    // the chunk's text: bytes up to a 4-byte boundary of the output, words, tail
+    // the chunk's text: bytes up to a 16-byte boundary of the output, 16-byte
+    // words, the tail bytes
     const unsigned L = unsigned(a.block_len[blockIdx.x]);
-    char* dst = a.out + header + a.block_off[blockIdx.x];
-    const unsigned head = min(L, unsigned((4u - (unsigned)((uintptr_t)dst & 3u)) & 3u));
-    if (threadIdx.x < head) dst[threadIdx.x] = stage[threadIdx.x];
-    const unsigned words = (L - head) >> 2;
-    for (unsigned q = threadIdx.x; q < words; q += D3_THREADS) {
-        const unsigned s = head + 4u * q;
-        const uint32_t wv = uint32_t(uint8_t(stage[s])) | (uint32_t(uint8_t(stage[s + 1])) << 8) |
-                            (uint32_t(uint8_t(stage[s + 2])) << 16) | (uint32_t(uint8_t(stage[s + 3])) << 24);
-        *reinterpret_cast<uint32_t*>(dst + s) = wv;
-    }
-    const unsigned tail = head + 4u * words;
-    if (threadIdx.x < L - tail) dst[tail + threadIdx.x] = stage[tail + threadIdx.x];
+    const char* src = stage + shift;
+    const unsigned head = min(L, (16u - shift) & 15u);
+    if (threadIdx.x < head) dst[threadIdx.x] = src[threadIdx.x];
+    const unsigned words = (L - head) >> 4;
+    for (unsigned q = threadIdx.x; q < words; q += D3_THREADS)
+        *reinterpret_cast<uint4*>(dst + head + 16u * q) = *reinterpret_cast<const uint4*>(src + head + 16u * q);
+    const unsigned tail = head + 16u * words;
+    if (threadIdx.x < L - tail) dst[tail + threadIdx.x] = src[tail + threadIdx.x];
 }
 
 // ------------------------------------------------------------ host text
@@ -577,16 +634,35 @@ struct rb200_dense3d_encoder {
     std::string err;
 };
 
+// The frame stream: frames are encoded on the caller's stream (the caller
+// waits for the encode, a fraction of a millisecond), then copied to pinned
+// host memory on the writer's own copy stream and written by the writer's
+// thread, so that the copy and the write overlap the caller's next step. Two
+// slots (device text, pinned text) alternate; a frame waits for its slot.
 struct rb200_dense3d_writer {
+    static constexpr int SLOTS = 2;
     rb200_dense3d_encoder* enc = nullptr;
     rb200_dense3d_limits limits{};
     int fd = -1;
-    char* d_text = nullptr;
-    char* h_text = nullptr;  // pinned
+    int device = 0;
+    char* d_text[SLOTS] = {};
+    char* h_text[SLOTS] = {};  // pinned
     uint64_t capacity = 0;
-    uint64_t frames = 0;
-    uint64_t bytes = 0;
+    cudaStream_t copy = nullptr;
+    cudaEvent_t copied[SLOTS] = {};
+    std::thread thread;
+    std::mutex mu;
+    std::condition_variable cv;
+    bool busy[SLOTS] = {};
+    uint64_t job_len[SLOTS] = {};
+    int queue[SLOTS] = {};
+    int q_head = 0, q_size = 0;
+    bool stop = false;
+    uint64_t frames = 0;    // frames accepted (encoded and queued)
+    uint64_t reserved = 0;  // bytes of the accepted frames
+    uint64_t bytes = 0;     // bytes written
     bool aborted = false;
+    int async_status = 0;   // a failed copy or write, reported by the next call
     std::string err;
 };
 
@@ -720,6 +796,69 @@ int rb200_dense3d_text_f32(float value, char* out, size_t capacity) {
 }
 
 // ------------------------------------------------------------ frame stream
+}  // extern "C"
+
+namespace {
+
+// The writer's thread: waits for each queued slot's copy, writes it out.
+void writer_loop(rb200_dense3d_writer* w) {
+    cudaSetDevice(w->device);
+    for (;;) {
+        int slot;
+        {
+            std::unique_lock<std::mutex> lock(w->mu);
+            w->cv.wait(lock, [&] { return w->q_size > 0 || w->stop; });
+            if (w->q_size == 0) return;
+            slot = w->queue[w->q_head];
+        }
+        int status = 0;
+        std::string msg;
+        if (cudaEventSynchronize(w->copied[slot]) != cudaSuccess) {
+            status = RB200_EXECUTION;
+            msg = "dense3D frame: device copy failed";
+        }
+        const uint64_t len = w->job_len[slot];
+        uint64_t done = 0;
+        while (!status && done < len) {
+            const ssize_t n = ::write(w->fd, w->h_text[slot] + done, size_t(len - done));
+            if (n < 0) {
+                if (errno == EINTR) continue;
+                status = RB200_DENSE3D_IO;
+                msg = std::string("dense3D export: Io(") + std::strerror(errno) + ")";
+                break;
+            }
+            done += uint64_t(n);
+            std::lock_guard<std::mutex> lock(w->mu);
+            w->bytes += uint64_t(n);
+        }
+        std::lock_guard<std::mutex> lock(w->mu);
+        if (status && !w->async_status) {
+            w->async_status = status;
+            w->err = msg;
+        }
+        w->busy[slot] = false;
+        w->q_head = (w->q_head + 1) % rb200_dense3d_writer::SLOTS;
+        w->q_size -= 1;
+        w->cv.notify_all();
+    }
+}
+
+// Wait until every queued frame is written; a failure seen by the thread is
+// terminal. Called without the lock.
+int drain(rb200_dense3d_writer* w) {
+    std::unique_lock<std::mutex> lock(w->mu);
+    w->cv.wait(lock, [&] { return w->q_size == 0; });
+    if (w->async_status) {
+        w->aborted = true;
+        return w->async_status;
+    }
+    return RB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int rb200_dense3d_writer_create(const rb200_grid* grid, const rb200_dense3d_limits* limits, int fd, int device,
                                 rb200_dense3d_writer** out) {
     if (!grid || !limits || !out || fd < 0) return RB200_INVALID_ARGUMENT;
@@ -737,71 +876,118 @@ int rb200_dense3d_writer_create(const rb200_grid* grid, const rb200_dense3d_limi
     w->enc = e;
     w->limits = *limits;
     w->fd = fd;
+    w->device = device;
     w->capacity = frame_bound(e);
-    if (cudaMalloc(&w->d_text, w->capacity) != cudaSuccess || cudaMallocHost(&w->h_text, w->capacity) != cudaSuccess) {
+    bool ok = cudaStreamCreateWithFlags(&w->copy, cudaStreamNonBlocking) == cudaSuccess;
+    for (int k = 0; ok && k < rb200_dense3d_writer::SLOTS; ++k)
+        ok = cudaMalloc(&w->d_text[k], w->capacity) == cudaSuccess &&
+             cudaMallocHost(&w->h_text[k], w->capacity) == cudaSuccess &&
+             cudaEventCreateWithFlags(&w->copied[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
         rb200_dense3d_writer_destroy(w);
         cudaGetLastError();
         return RB200_OUT_OF_MEMORY;
     }
+    w->thread = std::thread(writer_loop, w);
     *out = w;
     return RB200_OK;
 }
 
 void rb200_dense3d_writer_destroy(rb200_dense3d_writer* w) {
     if (!w) return;
-    if (w->enc) cudaSetDevice(w->enc->device);
-    cudaFree(w->d_text);
-    cudaFreeHost(w->h_text);
+    if (w->thread.joinable()) {
+        drain(w);
+        {
+            std::lock_guard<std::mutex> lock(w->mu);
+            w->stop = true;
+        }
+        w->cv.notify_all();
+        w->thread.join();
+    }
+    cudaSetDevice(w->device);
+    for (int k = 0; k < rb200_dense3d_writer::SLOTS; ++k) {
+        cudaFree(w->d_text[k]);
+        cudaFreeHost(w->h_text[k]);
+        if (w->copied[k]) cudaEventDestroy(w->copied[k]);
+    }
+    if (w->copy) cudaStreamDestroy(w->copy);
     rb200_dense3d_encoder_destroy(w->enc);
     delete w;
 }
 
-// One accepted frame: preflight, encode on the device, copy, write. Every
-// failure is terminal for the stream (src/dense3d_sequence.rs:224-341).
+// One accepted frame: preflight and encode on the caller's stream (waited
+// for), then the copy and the write are queued. Every failure is terminal for
+// the stream (src/dense3d_sequence.rs:224-341); a failed copy or write of an
+// earlier frame is reported here, by flush or by sync.
 int rb200_dense3d_writer_frame(rb200_dense3d_writer* w, const rb200_dense3d_frame* frame,
                                const rb200_dense3d_fields* fields, void* stream) {
     if (!w || !frame || !fields) return RB200_INVALID_ARGUMENT;
-    if (w->aborted) {
-        w->err = "dense3D export: Aborted";
-        return RB200_DENSE3D_ABORTED;
-    }
     auto fail = [&](int rc, const std::string& msg) {
+        std::lock_guard<std::mutex> lock(w->mu);
         w->aborted = true;
         w->err = msg;
         return rc;
     };
+    int slot;
+    {
+        std::unique_lock<std::mutex> lock(w->mu);
+        if (w->async_status) {
+            w->aborted = true;
+            return w->async_status;
+        }
+        if (w->aborted) {
+            w->err = "dense3D export: Aborted";
+            return RB200_DENSE3D_ABORTED;
+        }
+        slot = int(w->frames % rb200_dense3d_writer::SLOTS);
+        w->cv.wait(lock, [&] { return !w->busy[slot] || w->async_status; });
+        if (w->async_status) {
+            w->aborted = true;
+            return w->async_status;
+        }
+    }
     if (w->frames >= w->limits.max_frames) return fail(RB200_DENSE3D_LIMIT, "dense3D export: Limit");
     if (frame->frame != w->frames)
         return fail(RB200_DENSE3D_INVALID_STATE, "dense3D export: InvalidState(\"frame order\")");
     if (!fields->u || !fields->v || !fields->w) return fail(RB200_INVALID_ARGUMENT, "dense3D frame: missing field");
-    cudaSetDevice(w->enc->device);
-    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaSetDevice(w->device);
     uint64_t len = 0;
-    const int rc = encode(w->enc, frame, fields, w->d_text, w->capacity, &len, s);
+    const int rc = encode(w->enc, frame, fields, w->d_text[slot], w->capacity, &len, static_cast<cudaStream_t>(stream));
     if (rc) return fail(rc, w->enc->err);
-    if (len > w->limits.max_bytes - w->bytes)
+    if (len > w->limits.max_bytes - w->reserved)
         return fail(RB200_DENSE3D_IO, "dense3D export: Io(dense3D byte budget exhausted)");
-    if (cudaMemcpyAsync(w->h_text, w->d_text, len, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess)
+    if (cudaMemcpyAsync(w->h_text[slot], w->d_text[slot], len, cudaMemcpyDeviceToHost, w->copy) != cudaSuccess ||
+        cudaEventRecord(w->copied[slot], w->copy) != cudaSuccess)
         return fail(RB200_EXECUTION, "dense3D frame: device copy failed");
-    uint64_t done = 0;
-    while (done < len) {
-        const ssize_t n = ::write(w->fd, w->h_text + done, size_t(len - done));
-        if (n < 0) {
-            if (errno == EINTR) continue;
-            return fail(RB200_DENSE3D_IO, std::string("dense3D export: Io(") + std::strerror(errno) + ")");
-        }
-        done += uint64_t(n);
-        w->bytes += uint64_t(n);
+    {
+        std::lock_guard<std::mutex> lock(w->mu);
+        w->busy[slot] = true;
+        w->job_len[slot] = len;
+        w->queue[(w->q_head + w->q_size) % rb200_dense3d_writer::SLOTS] = slot;
+        w->q_size += 1;
+        w->frames += 1;
+        w->reserved += len;
     }
-    w->frames += 1;
+    w->cv.notify_all();
     return RB200_OK;
 }
 
-int rb200_dense3d_writer_sync(rb200_dense3d_writer* w) {
+// Dense3dSequence::flush (src/dense3d_sequence.rs:332-341): every accepted
+// frame written; terminal on failure.
+int rb200_dense3d_writer_flush(rb200_dense3d_writer* w) {
     if (!w) return RB200_INVALID_ARGUMENT;
-    if (w->aborted) return RB200_DENSE3D_ABORTED;
+    {
+        std::lock_guard<std::mutex> lock(w->mu);
+        if (w->aborted && !w->async_status) return RB200_DENSE3D_ABORTED;
+    }
+    return drain(w);
+}
+
+int rb200_dense3d_writer_sync(rb200_dense3d_writer* w) {
+    const int rc = rb200_dense3d_writer_flush(w);
+    if (rc) return rc;
     if (::fsync(w->fd) != 0 && errno != EINVAL && errno != EROFS) {
+        std::lock_guard<std::mutex> lock(w->mu);
         w->aborted = true;
         w->err = std::string("dense3D export: Io(") + std::strerror(errno) + ")";
         return RB200_DENSE3D_IO;
@@ -810,8 +996,16 @@ int rb200_dense3d_writer_sync(rb200_dense3d_writer* w) {
 }
 
 uint64_t rb200_dense3d_writer_frames(const rb200_dense3d_writer* w) { return w ? w->frames : 0; }
-uint64_t rb200_dense3d_writer_bytes(const rb200_dense3d_writer* w) { return w ? w->bytes : 0; }
-int rb200_dense3d_writer_aborted(const rb200_dense3d_writer* w) { return w ? int(w->aborted) : 1; }
+uint64_t rb200_dense3d_writer_bytes(const rb200_dense3d_writer* w) {
+    if (!w) return 0;
+    std::lock_guard<std::mutex> lock(const_cast<rb200_dense3d_writer*>(w)->mu);
+    return w->bytes;
+}
+int rb200_dense3d_writer_aborted(const rb200_dense3d_writer* w) {
+    if (!w) return 1;
+    std::lock_guard<std::mutex> lock(const_cast<rb200_dense3d_writer*>(w)->mu);
+    return int(w->aborted || w->async_status);
+}
 const char* rb200_dense3d_writer_error(const rb200_dense3d_writer* w) { return w ? w->err.c_str() : ""; }
 
 }  // extern "C"

@@ -197,7 +197,10 @@ class Dense3dFrameWriter:
 
     `output` is a path (a new file is created; an existing one is refused, as
     the reference's exporter refuses to overwrite) or an open file descriptor.
-    Frames must come in order 0, 1, 2, ...; any failure is terminal."""
+    Frames must come in order 0, 1, 2, ...; any failure is terminal.
+    write_frame encodes on the device and returns; the copy to the host and
+    the write run behind it (two frames in flight), so a write error surfaces
+    at the next write_frame, flush or sync."""
 
     def __init__(self, grid, output, limits: Dense3dLimits, device: int = 0):
         self._own_fd = False
@@ -222,15 +225,25 @@ class Dense3dFrameWriter:
         if st != N.OK:
             raise Dense3dError(st, (lib().rb200_dense3d_writer_error(self._h) or b"").decode())
 
+    def flush(self) -> None:
+        """Dense3dSequence::flush: returns once every accepted frame is
+        written (the copies and writes run behind write_frame)."""
+        st = lib().rb200_dense3d_writer_flush(self._h)
+        if st != N.OK:
+            raise Dense3dError(st, (lib().rb200_dense3d_writer_error(self._h) or b"").decode())
+
     def sync(self) -> None:
+        """flush, then fsync of the file."""
         st = lib().rb200_dense3d_writer_sync(self._h)
         if st != N.OK:
             raise Dense3dError(st, (lib().rb200_dense3d_writer_error(self._h) or b"").decode())
 
     def frame_count(self) -> int:
+        """Frames accepted (encoded and queued for writing)."""
         return int(lib().rb200_dense3d_writer_frames(self._h))
 
     def bytes_written(self) -> int:
+        """Bytes written so far (all accepted frames after flush())."""
         return int(lib().rb200_dense3d_writer_bytes(self._h))
 
     def is_aborted(self) -> bool:

@@ -171,6 +171,7 @@ def test_frame_stream_limits_and_terminal_errors(tmp_path):
         w.write_frame(infos[0], zero)
         w.write_frame(infos[1], fields)
         w.write_frame(infos[2], fields)
+        w.flush()
         assert w.frame_count() == 3 and w.bytes_written() == sum(len(x) for x in lines[:3])
         with pytest.raises(D.Dense3dError) as e:  # the frame limit includes the constructor frame
             w.write_frame(infos[3], fields)
@@ -195,6 +196,18 @@ def test_frame_stream_limits_and_terminal_errors(tmp_path):
         with pytest.raises(D.Dense3dError) as e:
             w.write_frame(infos[1], fields)
         assert e.value.kind == "InvalidState" and w.is_aborted()
+    # a failed write (the pipe's reader is gone) surfaces at the next call and is terminal
+    r, wfd = os.pipe()
+    os.close(r)
+    w = D.Dense3dFrameWriter(grid, wfd, D.Dense3dLimits(512, 9, 1 << 20))
+    w.write_frame(infos[0], zero)
+    with pytest.raises(D.Dense3dError) as e:
+        w.flush()
+    assert e.value.kind == "Io" and w.is_aborted()
+    with pytest.raises(D.Dense3dError):
+        w.write_frame(infos[1], fields)
+    w.close()
+    os.close(wfd)
     # creation limits (Dense3dSequence::new): zero frames or bytes, too many cells
     for lim in (D.Dense3dLimits(512, 0, 10), D.Dense3dLimits(512, 3, 0), D.Dense3dLimits(511, 3, 10)):
         with pytest.raises(D.Dense3dError) as e:
