@@ -114,6 +114,23 @@ class Dense3dFrame(C.Structure):
                 ("rounding_budget_m3", C.c_double)]
 
 
+class LiquidReport(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "dt", "time", "liquid_volume_before", "liquid_volume_after", "inward_boundary_volume",
+        "outward_boundary_volume", "source_volume", "volume_balance_error", "volume_rounding_budget",
+        "liquid_mass_before", "liquid_mass_after", "max_outward_courant", "actual_divergence_max", "fraction_min",
+        "fraction_max")] + [(n, C.c_uint64) for n in ("dry_cells", "mixed_cells", "full_cells", "error_cell")] + [
+        ("error_actual", C.c_double), ("error_limit", C.c_double)]
+
+
+# rb200_liquid_error (include/rheon_b200.h)
+LIQUID_ERRORS = {0: "Ok", 1: "InvalidDensity", 2: "InvalidFraction", 3: "InvalidInlet", 4: "InvalidSource",
+                 5: "InvalidSettings", 6: "InvalidTimeStep", 7: "TimeResolution", 8: "TimeMismatch",
+                 9: "LengthMismatch", 10: "NonFiniteVelocity", 11: "VersionOverflow", 12: "BufferLimit",
+                 13: "CourantLimit", 14: "DivergenceLimit", 15: "FractionBounds", 16: "BalanceLimit",
+                 17: "ArithmeticFailure", 18: "Cancelled", 19: "GeometryMismatch"}
+
+
 def build() -> str:
     """Compile the oracle with its Makefile (idempotent)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
@@ -169,6 +186,10 @@ def _declare(L):
     L.orc_carrier_step_f64.argtypes = [C.POINTER(Grid), C.POINTER(StepParams), _P, _P, _P, _P, C.POINTER(StepReport)]
     L.orc_solve_rhs_initial.argtypes = [C.POINTER(Grid), C.c_double, C.c_int, _P, _P, C.c_double,
                                         C.POINTER(Settings), _P, C.POINTER(Report), _P, C.c_size_t, C.c_int]
+    L.orc_liquid_advance.argtypes = [C.POINTER(Grid), C.c_double, C.c_double, C.c_uint64, _P, _P, _P, _P, _P,
+                                     C.c_double, C.c_double, C.POINTER(C.c_double), _P, C.c_double, C.c_double,
+                                     C.POINTER(LiquidReport)]
+    L.orc_liquid_validate_state.argtypes = [C.POINTER(Grid), C.c_double, _P, C.POINTER(C.c_uint64)]
     L.orc_dense3d_frame_text.argtypes = [C.POINTER(Grid), C.POINTER(Dense3dFrame), _P, _P, _P, _P, _P, _P,
                                          C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
     for name in ("orc_carrier_step_seeded_f32", "orc_carrier_step_seeded_f64"):
@@ -403,3 +424,29 @@ def dense3d_frame_text(g, frame=0, time_s=0.0, dt_s=0.0, carrier_stamp=(0, 0), l
                                       _ptr(tr) if tr is not None else None, _ptr(fr) if fr is not None else None,
                                       _ptr(p), buf, cap, C.byref(n))
     return st, (buf.raw[:n.value] if st == 0 else b"")
+
+
+def liquid_validate_state(g, density, fraction):
+    """LiquidVolumeState::new validation: (error name, cell)."""
+    f = _f64(fraction)
+    cell = C.c_uint64()
+    code = lib().orc_liquid_validate_state(C.byref(g), density, _ptr(f), C.byref(cell))
+    return LIQUID_ERRORS[code], cell.value
+
+
+def liquid_advance(g, density, fraction, faces, start, dt, inlet, source=None, max_outward_courant=1.0,
+                   actual_divergence_limit=1e-9, state_time=None, version=0):
+    """LiquidVolumeState::advance with an inlet boundary (src/liquid_volume.rs:
+    520-776): (error name, candidate fraction or None, report dict)."""
+    acc = _f64(fraction)
+    cand = np.zeros_like(acc)
+    fs = [_f32(a) for a in faces]
+    inl = (C.c_double * 6)(*[float(x) for pair in inlet for x in pair])
+    src = _f64(source) if source is not None else None
+    rep = LiquidReport()
+    code = lib().orc_liquid_advance(C.byref(g), density, start if state_time is None else state_time, version,
+                                    _ptr(acc), _ptr(cand), _ptr(fs[0]), _ptr(fs[1]), _ptr(fs[2]), start, dt, inl,
+                                    _ptr(src) if src is not None else None, max_outward_courant,
+                                    actual_divergence_limit, C.byref(rep))
+    out = {name: getattr(rep, name) for name, _ in LiquidReport._fields_}
+    return LIQUID_ERRORS[code], (cand if code == 0 else None), out

@@ -228,6 +228,37 @@ int orc_dense3d_frame_text(const orc_grid* g, const orc_dense3d_frame* frame, co
                            const float* w, const float* tracer, const double* fraction, const double* pressure,
                            char* out, size_t capacity, size_t* length);
 
+/* Liquid-volume transport, LiquidVolumeState::prepare_with_boundary with an
+ * inlet boundary, the all-cells divergence domain and no reconstructed
+ * columns (src/liquid_volume.rs:520-776), plus the flow-interval, inlet and
+ * source validations (:123-150, :84-96, :185-190) and validate_advance
+ * (:485-506). `accepted` is the state's fraction (x-fastest), `candidate`
+ * receives the new fraction on success. inlet[2 d + s]: the outside fraction
+ * of axis d, side s (0 lower, 1 upper). source may be NULL. Returns 0 or the
+ * rb200_liquid_error code of the first failure, with its payload in the
+ * report. */
+typedef struct orc_liquid_report {
+    double dt, time;
+    double liquid_volume_before, liquid_volume_after;
+    double inward_boundary_volume, outward_boundary_volume, source_volume;
+    double volume_balance_error, volume_rounding_budget;
+    double liquid_mass_before, liquid_mass_after;
+    double max_outward_courant, actual_divergence_max;
+    double fraction_min, fraction_max;
+    uint64_t dry_cells, mixed_cells, full_cells;
+    uint64_t error_cell;     /* CourantLimit, FractionBounds, InvalidFraction */
+    double error_actual;     /* CourantLimit/DivergenceLimit actual, FractionBounds fraction, BalanceLimit error */
+    double error_limit;      /* CourantLimit/DivergenceLimit limit, BalanceLimit rounding budget */
+} orc_liquid_report;
+
+int orc_liquid_advance(const orc_grid* g, double density, double state_time, uint64_t state_version,
+                       const double* accepted, double* candidate, const float* u, const float* v, const float* w,
+                       double start, double dt, const double inlet[6], const double* source_rate,
+                       double max_outward_courant, double actual_divergence_limit, orc_liquid_report* rep);
+/* LiquidVolumeState::new validation (src/liquid_volume.rs:276-305): 0 or the
+ * error code (InvalidDensity, InvalidFraction with *cell, ArithmeticFailure). */
+int orc_liquid_validate_state(const orc_grid* g, double density, const double* fraction, uint64_t* cell);
+
 #ifdef __cplusplus
 }
 #endif
