@@ -63,7 +63,8 @@ typedef enum rb200_status {
     RB200_DENSE3D_INVALID_STATE = 23,/* Dense3dError::InvalidState (src/dense3d_sequence.rs:21-27) */
     RB200_DENSE3D_LIMIT = 24,        /* Dense3dError::Limit                       */
     RB200_DENSE3D_ABORTED = 25,      /* Dense3dError::Aborted                     */
-    RB200_DENSE3D_IO = 26            /* Dense3dError::Io                          */
+    RB200_DENSE3D_IO = 26,           /* Dense3dError::Io                          */
+    RB200_LIQUID_REJECTED = 27       /* LiquidVolumeError: see rb200_liquid_report.error */
 } rb200_status;
 
 /* Pressure methods. JACOBI_PCG_V1 reproduces "jacobi-pcg-v1"
@@ -511,6 +512,115 @@ RB200_API uint64_t rb200_dense3d_writer_frames(const rb200_dense3d_writer* write
 RB200_API uint64_t rb200_dense3d_writer_bytes(const rb200_dense3d_writer* writer);
 RB200_API int rb200_dense3d_writer_aborted(const rb200_dense3d_writer* writer);
 RB200_API const char* rb200_dense3d_writer_error(const rb200_dense3d_writer* writer);
+
+/* ------------------------------------------------------------------------
+ * Liquid-volume transport (src/liquid_volume.rs): the represented liquid
+ * fraction moved through the carrier's face velocities by first-order
+ * shared-face donor transfer, on the device. LiquidVolumeState with an inlet
+ * boundary and the all-cells divergence domain.
+ * ------------------------------------------------------------------------ */
+typedef struct rb200_liquid_volume rb200_liquid_volume;
+
+/* LiquidVolumeError (src/liquid_volume.rs:27-72), the payload in the report. */
+typedef enum rb200_liquid_error {
+    RB200_LIQUID_OK = 0,
+    RB200_LIQUID_INVALID_DENSITY = 1,
+    RB200_LIQUID_INVALID_FRACTION = 2,    /* error_cell */
+    RB200_LIQUID_INVALID_INLET = 3,
+    RB200_LIQUID_INVALID_SOURCE = 4,
+    RB200_LIQUID_INVALID_SETTINGS = 5,
+    RB200_LIQUID_INVALID_TIME_STEP = 6,
+    RB200_LIQUID_TIME_RESOLUTION = 7,
+    RB200_LIQUID_TIME_MISMATCH = 8,
+    RB200_LIQUID_LENGTH_MISMATCH = 9,
+    RB200_LIQUID_NONFINITE_VELOCITY = 10,
+    RB200_LIQUID_VERSION_OVERFLOW = 11,
+    RB200_LIQUID_BUFFER_LIMIT = 12,       /* error_actual = required, error_limit = limit */
+    RB200_LIQUID_COURANT_LIMIT = 13,      /* error_cell, error_actual, error_limit */
+    RB200_LIQUID_DIVERGENCE_LIMIT = 14,   /* error_actual, error_limit */
+    RB200_LIQUID_FRACTION_BOUNDS = 15,    /* error_cell, error_actual = fraction */
+    RB200_LIQUID_BALANCE_LIMIT = 16,      /* error_actual = error, error_limit = rounding budget */
+    RB200_LIQUID_ARITHMETIC_FAILURE = 17,
+    RB200_LIQUID_CANCELLED = 18,
+    RB200_LIQUID_GEOMETRY_MISMATCH = 19
+} rb200_liquid_error;
+
+/* VolumeStamp (src/liquid_volume.rs:6-10). */
+typedef struct rb200_liquid_stamp {
+    uint64_t id;
+    uint64_t version;
+} rb200_liquid_stamp;
+
+/* LiquidFlowInterval (src/liquid_volume.rs:111-150): f32 face velocities
+ * (device pointers, x-fastest) held over [start, start + dt]. */
+typedef struct rb200_liquid_flow {
+    rb200_liquid_stamp stamp;
+    const float* u;
+    const float* v;
+    const float* w;
+    double start;
+    double dt;
+} rb200_liquid_flow;
+
+/* LiquidInlet (src/liquid_volume.rs:76-96): fraction[2 d + s] is the outside
+ * fraction of axis d, side s (0 lower, 1 upper), used on inflow only. */
+typedef struct rb200_liquid_inlet {
+    rb200_liquid_stamp stamp;
+    double fraction[6];
+} rb200_liquid_inlet;
+
+/* LiquidVolumeSource (src/liquid_volume.rs:174-190): m^3/s per cell (device). */
+typedef struct rb200_liquid_source {
+    rb200_liquid_stamp stamp;
+    const double* rate;
+} rb200_liquid_source;
+
+/* LiquidVolumeSettings (src/liquid_volume.rs:192-199). */
+typedef struct rb200_liquid_settings {
+    double max_outward_courant;
+    double actual_divergence_limit;
+} rb200_liquid_settings;
+
+/* LiquidVolumeReport (src/liquid_volume.rs:200-229) plus the error. */
+typedef struct rb200_liquid_report {
+    rb200_liquid_stamp stamp, flow, inlet, source;
+    int has_source;
+    double dt, time;
+    double liquid_volume_before, liquid_volume_after;
+    double inward_boundary_volume, outward_boundary_volume, source_volume;
+    double volume_balance_error, volume_rounding_budget;
+    double liquid_mass_before, liquid_mass_after;
+    double max_outward_courant, actual_divergence_max;
+    double fraction_min, fraction_max;
+    uint64_t dry_cells, mixed_cells, full_cells;
+    int error;            /* rb200_liquid_error */
+    uint64_t error_cell;
+    double error_actual, error_limit;
+} rb200_liquid_report;
+
+/* LiquidVolumeState::new (src/liquid_volume.rs:276-351): fraction is host or
+ * device memory of cell_len values; limit bounds the device bytes (two
+ * fraction arrays). RB200_LIQUID_REJECTED with *error filled on a rejected
+ * density, fraction, arithmetic or buffer limit. */
+RB200_API int rb200_liquid_create(const rb200_grid* grid, double density, rb200_liquid_stamp stamp,
+                                  const double* fraction, uint64_t limit, int device, rb200_liquid_volume** out,
+                                  rb200_liquid_report* error);
+RB200_API void rb200_liquid_destroy(rb200_liquid_volume* liquid);
+RB200_API uint64_t rb200_liquid_allocated_bytes(const rb200_liquid_volume* liquid);
+/* The accepted state: fraction (device pointer, valid until the next
+ * advance), stamp and time. */
+RB200_API int rb200_liquid_state(const rb200_liquid_volume* liquid, const double** fraction,
+                                 rb200_liquid_stamp* stamp, double* time);
+RB200_API int rb200_liquid_download(rb200_liquid_volume* liquid, double* out, size_t len);
+/* LiquidVolumeState::advance (src/liquid_volume.rs:376-387, 520-776): one
+ * explicit interval on `stream` (NULL: the state's own), waited for. On
+ * success the candidate becomes the accepted state (time = start + dt,
+ * version + 1); on RB200_LIQUID_REJECTED the accepted state is unchanged and
+ * report->error names the failure. source may be NULL. */
+RB200_API int rb200_liquid_advance(rb200_liquid_volume* liquid, const rb200_liquid_flow* flow,
+                                   const rb200_liquid_inlet* inlet, const rb200_liquid_source* source,
+                                   const rb200_liquid_settings* settings, rb200_liquid_report* report,
+                                   void* stream);
 
 #ifdef __cplusplus
 }

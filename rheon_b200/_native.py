@@ -35,14 +35,22 @@ DENSE3D_INVALID_STATE = 23
 DENSE3D_LIMIT = 24
 DENSE3D_ABORTED = 25
 DENSE3D_IO = 26
+LIQUID_REJECTED = 27
 
 STATUS_NAMES = {
     0: "Ok", 1: "Unsupported", 2: "Execution", 3: "NonFiniteOutput", 4: "NonZeroGauge", 5: "QualityGate",
     6: "Cancelled", 7: "IterationLimit", 8: "Breakdown", 9: "AllocationFailed", 10: "InvalidArgument",
     11: "IncompatibleRhs", 12: "NonFiniteInput", 13: "NonZeroWallVelocity", 14: "ArithmeticFailure",
     15: "DivergenceLimit", 16: "CourantLimit", 17: "NoDevice", 18: "LengthMismatch",
-    22: "InvalidInitialPressure", 23: "InvalidState", 24: "Limit", 25: "Aborted", 26: "Io",
+    22: "InvalidInitialPressure", 23: "InvalidState", 24: "Limit", 25: "Aborted", 26: "Io", 27: "LiquidRejected",
 }
+
+# rb200_liquid_error: LiquidVolumeError variants (src/liquid_volume.rs:27-72)
+LIQUID_ERRORS = {0: "Ok", 1: "InvalidDensity", 2: "InvalidFraction", 3: "InvalidInlet", 4: "InvalidSource",
+                 5: "InvalidSettings", 6: "InvalidTimeStep", 7: "TimeResolution", 8: "TimeMismatch",
+                 9: "LengthMismatch", 10: "NonFiniteVelocity", 11: "VersionOverflow", 12: "BufferLimit",
+                 13: "CourantLimit", 14: "DivergenceLimit", 15: "FractionBounds", 16: "BalanceLimit",
+                 17: "ArithmeticFailure", 18: "Cancelled", 19: "GeometryMismatch"}
 
 
 class Grid(C.Structure):
@@ -121,6 +129,40 @@ class Dense3dFields(C.Structure):
 
 class Dense3dLimits(C.Structure):
     _fields_ = [("max_cells", C.c_uint64), ("max_frames", C.c_uint64), ("max_bytes", C.c_uint64)]
+
+
+class LiquidStamp(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("version", C.c_uint64)]
+
+
+class LiquidFlow(C.Structure):
+    _fields_ = [("stamp", LiquidStamp), ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p),
+                ("start", C.c_double), ("dt", C.c_double)]
+
+
+class LiquidInlet(C.Structure):
+    _fields_ = [("stamp", LiquidStamp), ("fraction", C.c_double * 6)]
+
+
+class LiquidSource(C.Structure):
+    _fields_ = [("stamp", LiquidStamp), ("rate", C.c_void_p)]
+
+
+class LiquidSettings(C.Structure):
+    _fields_ = [("max_outward_courant", C.c_double), ("actual_divergence_limit", C.c_double)]
+
+
+class LiquidReport(C.Structure):
+    _fields_ = ([("stamp", LiquidStamp), ("flow", LiquidStamp), ("inlet", LiquidStamp), ("source", LiquidStamp),
+                 ("has_source", C.c_int)] +
+                [(n, C.c_double) for n in ("dt", "time", "liquid_volume_before", "liquid_volume_after",
+                                           "inward_boundary_volume", "outward_boundary_volume", "source_volume",
+                                           "volume_balance_error", "volume_rounding_budget", "liquid_mass_before",
+                                           "liquid_mass_after", "max_outward_courant", "actual_divergence_max",
+                                           "fraction_min", "fraction_max")] +
+                [(n, C.c_uint64) for n in ("dry_cells", "mixed_cells", "full_cells")] +
+                [("error", C.c_int), ("error_cell", C.c_uint64), ("error_actual", C.c_double),
+                 ("error_limit", C.c_double)])
 
 
 _P = C.c_void_p
@@ -205,6 +247,14 @@ SIGNATURES = {
     "rb200_dense3d_writer_bytes": (C.c_uint64, [_P]),
     "rb200_dense3d_writer_aborted": (_I, [_P]),
     "rb200_dense3d_writer_error": (C.c_char_p, [_P]),
+    "rb200_liquid_create": (_I, [C.POINTER(Grid), _D, LiquidStamp, _P, C.c_uint64, _I, C.POINTER(_P),
+                                 C.POINTER(LiquidReport)]),
+    "rb200_liquid_destroy": (None, [_P]),
+    "rb200_liquid_allocated_bytes": (C.c_uint64, [_P]),
+    "rb200_liquid_state": (_I, [_P, C.POINTER(_P), C.POINTER(LiquidStamp), C.POINTER(_D)]),
+    "rb200_liquid_download": (_I, [_P, _P, _S]),
+    "rb200_liquid_advance": (_I, [_P, C.POINTER(LiquidFlow), C.POINTER(LiquidInlet), C.POINTER(LiquidSource),
+                                  C.POINTER(LiquidSettings), C.POINTER(LiquidReport), _P]),
 }
 
 _lib = None

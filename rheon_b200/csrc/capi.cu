@@ -236,6 +236,7 @@ const char* rb200_status_string(int status) {
         case RB200_DENSE3D_LIMIT: return "dense3D export limit";
         case RB200_DENSE3D_ABORTED: return "dense3D export aborted";
         case RB200_DENSE3D_IO: return "dense3D output error";
+        case RB200_LIQUID_REJECTED: return "liquid volume transport rejected the operation";
         default: return "unknown status";
     }
 }

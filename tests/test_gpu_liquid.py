@@ -1,0 +1,267 @@
+"""Liquid-volume transport on the device against the oracle and the reference's answers.
+
+The device LiquidVolumeState (src/liquid_volume.rs:520-776) must produce the
+oracle's candidate fraction bit for bit, the same error with the same payload
+(the first failing cell in x-fastest order), and the same ledger; a rejected
+interval leaves the accepted state untouched. The known-answer cases restate
+tests/liquid_volume_contract.rs.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+import rheon_b200 as R
+from rheon_b200 import liquid as L
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _device():
+    if not torch.cuda.is_available() or R.device_count() == 0:
+        pytest.skip("no B200")
+    yield
+    torch.cuda.synchronize()
+
+
+SETTINGS = L.LiquidVolumeSettings(1.0, 1e-9)
+
+
+def dev(a, dtype):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).cuda()
+
+
+def fields(counts):
+    g = O.grid(counts)
+    return [np.zeros(O.face_len(g, a), np.float32) for a in range(3)]
+
+
+def fidx(counts, axis, p):
+    fc = list(counts)
+    fc[axis] += 1
+    return p[0] + fc[0] * (p[1] + fc[1] * p[2])
+
+
+def run_both(counts, spacing, density, fraction, vel, start, dt, inlet, source=None, settings=SETTINGS,
+             origin=(0.0, 0.0, 0.0)):
+    """One interval on the device and in the oracle; returns (device report or
+    error, oracle triple, device state)."""
+    grid = R.GridGeometry(counts, spacing, origin)
+    st = L.LiquidVolumeState(grid, density, (1, 0), np.asarray(fraction, np.float64))
+    og = O.grid(counts, spacing, origin)
+    want = O.liquid_advance(og, density, fraction, vel, start, dt, inlet, source=source,
+                            max_outward_courant=settings.max_outward_courant,
+                            actual_divergence_limit=settings.actual_divergence_limit, state_time=start)
+    if start != 0.0:  # bring the device state to `start` with a zero-velocity interval
+        st.advance([dev(np.zeros(O.face_len(og, a)), np.float32) for a in range(3)], 0.0, start, (9, 9),
+                   L.LiquidInlet((4, 2), [[0.0, 0.0]] * 3), settings)
+    try:
+        got = st.advance([dev(v, np.float32) for v in vel], start, dt, (2, 3), L.LiquidInlet((4, 2), inlet), settings,
+                         source=dev(source, np.float64) if source is not None else None, source_stamp=(3, 7))
+    except L.LiquidVolumeError as e:
+        got = e
+    return got, want, st
+
+
+def same_report(got: L.LiquidVolumeReport, want: dict):
+    for k in ("dt", "time", "max_outward_courant", "actual_divergence_max", "fraction_min", "fraction_max",
+              "dry_cells", "mixed_cells", "full_cells"):
+        assert getattr(got, k) == want[k], k
+    for k in ("liquid_volume_before", "liquid_volume_after", "inward_boundary_volume", "outward_boundary_volume",
+              "source_volume", "liquid_mass_before", "liquid_mass_after"):
+        assert abs(getattr(got, k) - want[k]) <= 1e-15 * max(abs(want[k]), 1e-300), k
+    scale = abs(want["liquid_volume_before"]) + abs(want["liquid_volume_after"])
+    assert abs(got.volume_balance_error - want["volume_balance_error"]) <= 4e-16 * max(scale, 1e-300)
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+@pytest.mark.parametrize("speed", [-0.5, 0.5])
+def test_upwind_inlet_outlet_hand_volumes(axis, speed):
+    """tests/liquid_volume_contract.rs:53-100"""
+    counts = [1, 1, 1]
+    counts[axis] = 4
+    vel = fields(counts)
+    vel[axis][:] = speed
+    alpha = [[0.0, 0.0] for _ in range(3)]
+    alpha[axis] = [0.5, 0.125]
+    got, want, st = run_both(tuple(counts), (1.0, 1.0, 1.0), 1000.0, [0.0, 0.25, 0.75, 1.0], vel, 0.0, 1.0, alpha,
+                             origin=(2.0, 3.0, 4.0))
+    assert want[0] == "Ok" and isinstance(got, L.LiquidVolumeReport)
+    expected = [0.25, 0.125, 0.5, 0.875] if speed > 0 else [0.125, 0.5, 0.875, 0.5625]
+    assert list(st.fraction()) == expected
+    same_report(got, want[2])
+    assert got.stamp == (1, 1) and got.flow == (2, 3) and got.inlet == (4, 2) and got.time == 1.0
+    assert (got.inward_boundary_volume, got.outward_boundary_volume) == ((0.25, 0.5) if speed > 0 else (0.0625, 0.0))
+    assert st.occupancy(0) == L.LiquidOccupancy.MIXED and st.occupancy(4) is None
+
+
+def test_closed_circulation_and_sources():
+    """tests/liquid_volume_contract.rs:101-151"""
+    counts = (2, 2, 2)
+    vel = fields(counts)
+    for z in range(2):
+        vel[0][fidx(counts, 0, (1, 0, z))] = 0.25
+        vel[0][fidx(counts, 0, (1, 1, z))] = -0.25
+        vel[1][fidx(counts, 1, (0, 1, z))] = -0.5
+        vel[1][fidx(counts, 1, (1, 1, z))] = 0.5
+    got, want, st = run_both(counts, (0.5, 1.0, 2.0), 1000.0, [1.0, 0.0, 0.0, 0.0, 0.0, 0.5, 0.0, 0.25], vel, 0.0,
+                             0.5, [[1.0, 1.0]] * 3)
+    assert list(st.fraction()) == [0.75, 0.25, 0.0, 0.0, 0.0, 0.375, 0.0625, 0.3125]
+    same_report(got, want[2])
+    for density in (1.0, 1000.0):
+        got, want, st = run_both((2, 1, 1), (1.0, 1.0, 1.0), density, [0.25, 0.75], fields((2, 1, 1)), 0.0, 0.5,
+                                 [[0.0, 0.0]] * 3, source=np.array([0.25, -0.125]))
+        assert list(st.fraction()) == [0.375, 0.6875]
+        assert got.source == (3, 7) and got.source_volume == 0.0625 and got.liquid_mass_after == density * 1.0625
+
+
+def test_translated_slab_matches_the_binomial_over_many_intervals():
+    """tests/liquid_volume_contract.rs:219-270 (n = 64, Courant 0.5)"""
+    n, courant = 64, 0.5
+    h = 1.0 / n
+    grid = R.GridGeometry((n, 1, 1), (h, 1.0, 1.0))
+    init = np.array([1.0 if n // 4 <= i < n // 2 else 0.0 for i in range(n)])
+    st = L.LiquidVolumeState(grid, 1000.0, (1, 0), init)
+    vel = fields((n, 1, 1))
+    vel[0][:] = 0.25
+    dv = [dev(v, np.float32) for v in vel]
+    dt = courant * h / 0.25
+    steps = int(0.5 / dt)
+    f, t = init.copy(), 0.0
+    og = O.grid((n, 1, 1), (h, 1.0, 1.0))
+    for k in range(steps):
+        r = st.advance(dv, st.time, dt, (2, k), L.LiquidInlet((4, 2), [[0.0, 0.0]] * 3), SETTINGS)
+        _, f, _ = O.liquid_advance(og, 1000.0, f, vel, t, dt, [[0.0, 0.0]] * 3)
+        t = r.time
+    got = st.fraction()
+    assert np.array_equal(got.view(np.uint64), f.view(np.uint64))
+    for i, value in enumerate(got):
+        binomial = sum(math.comb(steps, k) * courant ** k * (1 - courant) ** (steps - k) * init[i - k]
+                       for k in range(0, min(steps, i) + 1))
+        assert abs(value - binomial) <= 2e-12 * max(abs(value), abs(binomial), 1.0)
+    assert st.stamp == (1, steps)
+
+
+@pytest.mark.parametrize("counts", [(7, 5, 3), (16, 9, 12), (33, 20, 17)], ids=str)
+def test_random_intervals_match_the_oracle_bitwise(counts):
+    rng = np.random.default_rng(sum(counts))
+    spacing = (0.5, 0.75, 1.25)
+    g = O.grid(counts, spacing)
+    f = rng.uniform(0.2, 0.8, int(np.prod(counts)))
+    vel = [rng.uniform(-0.05, 0.05, O.face_len(g, a)).astype(np.float32) for a in range(3)]
+    src = rng.uniform(-1e-3, 1e-3, f.size)
+    inlet = [[0.25, 0.5], [0.0, 1.0], [0.125, 0.75]]
+    settings = L.LiquidVolumeSettings(1.0, 10.0)
+    grid = R.GridGeometry(counts, spacing)
+    st = L.LiquidVolumeState(grid, 800.0, (5, 0), f)
+    dv = [dev(v, np.float32) for v in vel]
+    ds = dev(src, np.float64)
+    t = 0.0
+    for k in range(4):
+        err, f2, want = O.liquid_advance(g, 800.0, f, vel, t, 0.05, inlet, source=src, max_outward_courant=1.0,
+                                         actual_divergence_limit=10.0)
+        assert err == "Ok"
+        got = st.advance(dv, t, 0.05, (2, k), L.LiquidInlet((4, 2), inlet), settings, source=ds, source_stamp=(3, k))
+        assert np.array_equal(st.fraction().view(np.uint64), f2.view(np.uint64))
+        same_report(got, want)
+        assert got.stamp == (5, k + 1) and got.source == (3, k)
+        f, t = f2, got.time
+    # a strongly compressive random flow: the same first failure and payload
+    vel = [rng.uniform(-3.0, 3.0, O.face_len(g, a)).astype(np.float32) for a in range(3)]
+    f = rng.uniform(0.0, 1.0, f.size)
+    for lim in (1.0, 0.5):
+        err, _, want = O.liquid_advance(g, 800.0, f, vel, 0.0, 0.05, inlet, max_outward_courant=lim,
+                                        actual_divergence_limit=100.0)
+        st2 = L.LiquidVolumeState(grid, 800.0, (5, 0), f)
+        with pytest.raises(L.LiquidVolumeError) as e:
+            st2.advance([dev(v, np.float32) for v in vel], 0.0, 0.05, (2, 0), L.LiquidInlet((4, 2), inlet),
+                        L.LiquidVolumeSettings(lim, 100.0))
+        assert e.value.kind == err != "Ok"
+        if err in ("CourantLimit", "FractionBounds"):
+            assert e.value.cell == want["error_cell"] and e.value.actual == want["error_actual"]
+        assert np.array_equal(st2.fraction(), f)
+
+
+def test_errors_payloads_and_transactions():
+    """tests/liquid_volume_contract.rs:293-345 and the first-failing-cell rule"""
+    # Courant limit: actual 2.0 in cell 0, state unchanged
+    vel = fields((1, 1, 1))
+    vel[0][:] = 2.0
+    got, want, st = run_both((1, 1, 1), (1.0, 1.0, 1.0), 1000.0, [0.25], vel, 0.0, 1.0, [[0.25, 0.25]] * 3)
+    assert isinstance(got, L.LiquidVolumeError) and got.kind == "CourantLimit" and got.actual == 2.0
+    assert want[0] == "CourantLimit"
+    assert st.fraction()[0] == 0.25 and st.stamp == (1, 0) and st.time == 0.0
+    # fraction bounds from a raw source, both signs
+    for rate in (1.0, -1.0):
+        got, want, _ = run_both((1, 1, 1), (1.0, 1.0, 1.0), 1000.0, [0.25], fields((1, 1, 1)), 0.0, 1.0,
+                                [[0.0, 0.0]] * 3, source=np.array([rate]))
+        assert got.kind == want[0] == "FractionBounds"
+    # divergence limit 0.25, then accepted with the relaxed limit; overfull cells fail with fraction 1.25
+    vel = fields((2, 1, 1))
+    vel[0][1] = 0.25
+    got, want, _ = run_both((2, 1, 1), (1.0, 1.0, 1.0), 1000.0, [0.25, 0.5], vel, 0.0, 1.0, [[0.0, 0.0]] * 3)
+    assert got.kind == want[0] == "DivergenceLimit" and got.actual == 0.25
+    relaxed = L.LiquidVolumeSettings(1.0, 0.25)
+    got, want, _ = run_both((2, 1, 1), (1.0, 1.0, 1.0), 1000.0, [0.25, 0.5], vel, 0.0, 1.0, [[0.0, 0.0]] * 3,
+                            settings=relaxed)
+    assert got.liquid_volume_after == 0.75
+    got, want, _ = run_both((2, 1, 1), (1.0, 1.0, 1.0), 1000.0, [1.0, 1.0], vel, 0.0, 1.0, [[1.0, 1.0]] * 3,
+                            settings=relaxed)
+    assert got.kind == "FractionBounds" and got.actual == 1.25 and got.cell == want[2]["error_cell"]
+    # several failing cells: the first in x-fastest order is reported, with its own payload
+    counts = (6, 4, 3)
+    f = np.full(72, 0.5)
+    src = np.zeros(72)
+    for c in (50, 17, 63):
+        f[c] = 1.0
+        src[c] = 0.5
+    got, want, _ = run_both(counts, (1.0, 1.0, 1.0), 1000.0, f, fields(counts), 0.0, 1.0, [[1.0, 1.0]] * 3,
+                            source=src)
+    assert want[0] == "FractionBounds" and want[2]["error_cell"] == 17
+    assert got.kind == "FractionBounds" and got.cell == 17 and got.actual == want[2]["error_actual"] == 1.5
+    vel = fields(counts)
+    vel[0][fidx(counts, 0, (1, 1, 0))] = 5.0  # outward Courant 5 in cell (0, 1, 0) = 6, before cell 17
+    got, want, _ = run_both(counts, (1.0, 1.0, 1.0), 1000.0, f, vel, 0.0, 1.0, [[1.0, 1.0]] * 3, source=src,
+                            settings=L.LiquidVolumeSettings(1.0, 100.0))
+    assert want[0] == "CourantLimit" and want[2]["error_cell"] == 6
+    assert got.kind == "CourantLimit" and got.cell == 6 and got.actual == want[2]["error_actual"] == 5.0
+
+
+def test_validation_order():
+    """src/liquid_volume.rs:84-96, :123-150, :185-190, :485-529"""
+    counts = (3, 2, 2)
+    grid = R.GridGeometry(counts)
+    st = L.LiquidVolumeState(grid, 1.0, (1, 0), np.full(12, 0.5))
+    z = [dev(v, np.float32) for v in fields(counts)]
+    ok = L.LiquidInlet((4, 2), [[0.0, 0.0]] * 3)
+
+    def kind(*args, **kw):
+        with pytest.raises(L.LiquidVolumeError) as e:
+            st.advance(*args, **kw)
+        return e.value.kind
+
+    assert kind(z, 0.0, 0.0, (2, 0), ok, SETTINGS) == "InvalidTimeStep"
+    assert kind(z, 1e300, 1e-300, (2, 0), ok, SETTINGS) == "TimeResolution"
+    bad = fields(counts)
+    bad[1][3] = np.nan
+    assert kind([dev(v, np.float32) for v in bad], 0.5, 0.5, (2, 0), L.LiquidInlet((4, 2), [[2.0, 0.0]] * 3),
+                SETTINGS) == "NonFiniteVelocity"
+    assert kind(z, 0.5, 0.5, (2, 0), L.LiquidInlet((4, 2), [[2.0, 0.0]] * 3), SETTINGS) == "InvalidInlet"
+    nan_src = dev(np.array([np.nan] + [0.0] * 11), np.float64)
+    assert kind(z, 0.5, 0.5, (2, 0), ok, SETTINGS, source=nan_src) == "InvalidSource"
+    assert kind(z, 0.5, 0.5, (2, 0), ok, SETTINGS) == "TimeMismatch"
+    assert kind(z, 0.0, 0.5, (2, 0), ok, L.LiquidVolumeSettings(0.0, 1.0)) == "InvalidSettings"
+    assert st.stamp == (1, 0) and np.all(st.fraction() == 0.5)
+    with pytest.raises(L.LiquidVolumeError) as e:
+        L.LiquidVolumeState(grid, 1.0, (1, 0), np.array([0.5] * 11 + [1.5]))
+    assert e.value.kind == "InvalidFraction" and e.value.cell == 11
+    with pytest.raises(L.LiquidVolumeError) as e:
+        L.LiquidVolumeState(grid, -1.0, (1, 0), np.full(12, 0.5))
+    assert e.value.kind == "InvalidDensity"
+    with pytest.raises(L.LiquidVolumeError) as e:
+        L.LiquidVolumeState(grid, 1.0, (1, 0), np.full(12, 0.5), limit=100)
+    assert e.value.kind == "BufferLimit"
