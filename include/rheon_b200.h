@@ -409,7 +409,8 @@ RB200_API int rb200_carrier_profile(rb200_carrier* carrier, int which, int launc
 RB200_API int rb200_carrier_pressure(rb200_carrier* carrier, double* out, size_t len);
 /* The carrier's accepted state as dense3D frame fields (device pointers,
  * valid until the next step or upload): faces, tracer (NULL without one),
- * fraction NULL, and the pressure of the last accepted step (NULL, i.e.
+ * the liquid fraction (NULL without a liquid state), and the pressure of the
+ * last accepted step (NULL, i.e.
  * zeros, before the first accepted step after an upload). Without the
  * warm-start copy of the accepted pressure, a carrier whose last step was
  * rejected holds no accepted pressure: RB200_DENSE3D_INVALID_STATE. */
@@ -621,6 +622,29 @@ RB200_API int rb200_liquid_advance(rb200_liquid_volume* liquid, const rb200_liqu
                                    const rb200_liquid_inlet* inlet, const rb200_liquid_source* source,
                                    const rb200_liquid_settings* settings, rb200_liquid_report* report,
                                    void* stream);
+
+/* The liquid step on the resident carrier (LiquidTransportSimulation,
+ * src/liquid_step.rs:828-900): the carrier owns a liquid-volume state, and
+ * every step advances it through the step's corrected faces over
+ * [time, time + dt] before the step commits; a rejected transport rejects the
+ * step (status RB200_LIQUID_REJECTED, details in rb200_carrier_liquid_report)
+ * and neither state changes. Needs f32 face storage. The flow intervals are
+ * stamped {flow_id, candidate generation}. An upload or device
+ * initialisation of the carrier restarts both clocks at zero. */
+RB200_API int rb200_carrier_attach_liquid(rb200_carrier* carrier, double density, rb200_liquid_stamp stamp,
+                                          uint64_t flow_id, const double* fraction, uint64_t limit,
+                                          rb200_liquid_report* error);
+/* The inlet, source (NULL: none; device memory kept valid while steps run)
+ * and volume settings of the following steps (LiquidStepInputs). */
+RB200_API int rb200_carrier_liquid_inputs(rb200_carrier* carrier, const rb200_liquid_inlet* inlet,
+                                          const rb200_liquid_source* source, const rb200_liquid_settings* settings);
+/* The liquid report of the last step (its error when the transport rejected it). */
+RB200_API int rb200_carrier_liquid_report(const rb200_carrier* carrier, rb200_liquid_report* report);
+/* The accepted liquid state: fraction (device), stamp, time. */
+RB200_API int rb200_carrier_liquid_state(const rb200_carrier* carrier, const double** fraction,
+                                         rb200_liquid_stamp* stamp, double* time);
+/* Host (or device) copy of the accepted liquid fraction. */
+RB200_API int rb200_carrier_liquid_download(rb200_carrier* carrier, double* out, size_t len);
 
 #ifdef __cplusplus
 }

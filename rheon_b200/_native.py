@@ -255,6 +255,12 @@ SIGNATURES = {
     "rb200_liquid_download": (_I, [_P, _P, _S]),
     "rb200_liquid_advance": (_I, [_P, C.POINTER(LiquidFlow), C.POINTER(LiquidInlet), C.POINTER(LiquidSource),
                                   C.POINTER(LiquidSettings), C.POINTER(LiquidReport), _P]),
+    "rb200_carrier_attach_liquid": (_I, [_P, _D, LiquidStamp, C.c_uint64, _P, C.c_uint64, C.POINTER(LiquidReport)]),
+    "rb200_carrier_liquid_inputs": (_I, [_P, C.POINTER(LiquidInlet), C.POINTER(LiquidSource),
+                                         C.POINTER(LiquidSettings)]),
+    "rb200_carrier_liquid_report": (_I, [_P, C.POINTER(LiquidReport)]),
+    "rb200_carrier_liquid_state": (_I, [_P, C.POINTER(_P), C.POINTER(LiquidStamp), C.POINTER(_D)]),
+    "rb200_carrier_liquid_download": (_I, [_P, _P, _S]),
 }
 
 _lib = None

@@ -17,6 +17,7 @@
 
 #include "advect.cuh"
 #include "internal.hpp"
+#include "liquid.hpp"
 #include "pcg.hpp"
 #include "project.cuh"
 
@@ -50,6 +51,11 @@ struct CarrierDev {
     int history;         // an accepted pressure of this state exists
     int warm;            // this step's solve is seeded
     double* accepted_p;  // the last accepted step's pressure (device)
+    // liquid step (src/liquid_step.rs:828-900): null without a liquid state
+    LiquidDev* liquid;
+    LiquidFlowDev* lflow;
+    rb200_liquid_report* lrep;
+    unsigned long long flow_id;  // VolumeStamp id of the carrier's flow intervals
 };
 
 __device__ __forceinline__ bool step_running(const CarrierDev* cd) { return cd->status == STEP_RUNNING; }
@@ -113,6 +119,21 @@ __global__ void __launch_bounds__(ADV_THREADS) k_carrier_tracer(GridDev g, Carri
     advect_tracer_body<T, R>(g, cd->tracer[cd->tacc], vel, cd->dt, cd->tracer[cd->tacc ^ 1], &cd->flags);
 }
 
+// The liquid interval of the step (src/liquid_step.rs:869-887): the
+// corrected candidate faces over [time, time + dt], stamped with the
+// candidate generation. Inactive when the carrier part already failed.
+__global__ void k_carrier_liquid_flow(CarrierDev* cd, const SolveState* st) {
+    LiquidFlowDev* f = cd->lflow;
+    const bool run = solve_usable(cd, st) && !(cd->flags & (VF_NONFINITE | VF_ARITH | VF_F32_RANGE));
+    f->active = run ? 1 : 0;
+    if (!run) return;
+    const int c = (cd->acc + 2) % 3;
+    for (int d = 0; d < 3; ++d) f->vel[d] = static_cast<const float*>(cd->faces[c][d]);
+    f->start = cd->time;
+    f->dt = cd->dt;
+    f->flow = rb200_liquid_stamp{cd->flow_id, cd->generation + 1};
+}
+
 // Gates and commit: actual divergence (simulation.rs:1235-1243), Courant
 // (simulation.rs:1268-1277), then publication by index rotation.
 __global__ void k_step_end(GridDev g, CarrierDev* cd, const SolveState* st) {
@@ -151,12 +172,16 @@ __global__ void k_step_end(GridDev g, CarrierDev* cd, const SolveState* st) {
                 else if (rep.courant > cd->max_courant)
                     status = RB200_COURANT_LIMIT;
             }
+            // the liquid interval is part of the transaction: a rejected
+            // transport rejects the step (src/liquid_step.rs:881-900)
+            if (status == RB200_OK && cd->liquid && cd->lrep->error) status = RB200_LIQUID_REJECTED;
             if (status == RB200_OK) {
                 cd->acc = (cd->acc + 2) % 3;
                 if (cd->tracer[0]) cd->tacc ^= 1;
                 cd->time += cd->dt;
                 cd->generation += 1;
                 cd->rate = rate;
+                if (cd->liquid) liquid_commit(cd->liquid, *cd->lrep);
             }
         }
     }
@@ -262,6 +287,16 @@ struct rb200_carrier {
     int fixed_nodes = 0;
     size_t bytes = 0;
     bool in_flight = false;
+    // liquid step state (rb200_carrier_attach_liquid)
+    LiquidDev* lq_h = nullptr;   // pinned mirror, copied back after each step
+    LiquidDev* lq_d = nullptr;
+    LiquidFlowDev* lflow_h = nullptr;  // pinned: the per-step inputs
+    LiquidFlowDev* lflow_d = nullptr;
+    rb200_liquid_report* lrep_h = nullptr;  // pinned: the last step's liquid report
+    rb200_liquid_report* lrep_d = nullptr;
+    LiquidScratch lq_sc{};
+    int lq_blocks = 0;
+    bool lq_inputs = false;      // inlet and settings given
     uint64_t accepted_steps = 0;  // accepted steps since the last upload
     bool last_rejected = false;   // the last step was rejected
     std::string err;
@@ -274,6 +309,14 @@ struct rb200_carrier {
         cudaFree(tracer[0]);
         cudaFree(tracer[1]);
         cudaFree(accepted_p);
+        if (lq_h) {
+            liquid_state_free(lq_h, lq_d, &lq_sc);
+            cudaFreeHost(lq_h);
+        }
+        cudaFree(lflow_d);
+        cudaFree(lrep_d);
+        if (lflow_h) cudaFreeHost(lflow_h);
+        if (lrep_h) cudaFreeHost(lrep_h);
         cudaFree(cd);
         if (h_cd) cudaFreeHost(h_cd);
         for (auto& e : ev)
@@ -342,9 +385,17 @@ int capture_step(rb200_carrier* c) {
         else
             k_carrier_tracer<T, double><<<cb, ADV_THREADS, 0, s>>>(g, c->cd, c->solver.state());
     }
+    if (c->lq_d) {
+        k_carrier_liquid_flow<<<1, 1, 0, s>>>(c->cd, c->solver.state());
+        RB200_CUDA(launch_liquid_advance(g, c->lq_d, c->lflow_d, c->lq_sc, c->lq_blocks, c->lrep_d, s));
+    }
     k_step_end<<<1, 1, 0, s>>>(g, c->cd, c->solver.state());
     if (c->accepted_p) k_keep_pressure<<<eb, EW_THREADS, 0, s>>>(g, c->cd, c->solver.p());
     RB200_CUDA(cudaMemcpyAsync(c->h_cd, c->cd, sizeof(CarrierDev), cudaMemcpyDeviceToHost, s));
+    if (c->lq_d) {
+        RB200_CUDA(cudaMemcpyAsync(c->lq_h, c->lq_d, sizeof(LiquidDev), cudaMemcpyDeviceToHost, s));
+        RB200_CUDA(cudaMemcpyAsync(c->lrep_h, c->lrep_d, sizeof(rb200_liquid_report), cudaMemcpyDeviceToHost, s));
+    }
     cudaError_t le = cudaGetLastError();
     cudaError_t ee = cudaStreamEndCapture(s, &graph);
     if (le != cudaSuccess || ee != cudaSuccess) {
@@ -360,7 +411,7 @@ int capture_step(rb200_carrier* c) {
     }
     // begin, advect, rhs, reset (+start kernels counted by the solver), correct, tracer, end
     // (+ seed and keep kernels with the warm-start policy)
-    c->fixed_nodes = 5 + (c->tracer[0] ? 1 : 0) + (c->accepted_p ? 2 : 0);
+    c->fixed_nodes = 5 + (c->tracer[0] ? 1 : 0) + (c->accepted_p ? 2 : 0) + (c->lq_d ? 2 : 0);
     return RB200_OK;
 }
 
@@ -405,6 +456,12 @@ int upload_rate(rb200_carrier* c) {
     // starts cold (PressureColdReason::Invalidated, src/pressure_initialization.rs:31-36)
     c->h_cd->history = 0;
     RB200_CUDA(cudaMemcpyAsync(c->cd, c->h_cd, sizeof(CarrierDev), cudaMemcpyHostToDevice, c->stream));
+    if (c->lq_h) {
+        // the liquid state keeps its fraction and stamp; its clock follows the
+        // carrier's, which a new accepted state restarts at zero
+        c->lq_h->time = 0.0;
+        RB200_CUDA(cudaMemcpyAsync(c->lq_d, c->lq_h, sizeof(LiquidDev), cudaMemcpyHostToDevice, c->stream));
+    }
     RB200_CUDA(cudaStreamSynchronize(c->stream));
     return RB200_OK;
 }
@@ -593,9 +650,15 @@ int rb200_carrier_step_async(rb200_carrier* carrier, const rb200_step_params* pa
     c->h_cd->buoyancy = params->buoyancy;
     c->h_cd->iteration_limit_ok = params->iteration_limit_ok;
     c->h_cd->skip_gates = params->skip_gates;
+    if (c->lq_d && !c->lq_inputs) {
+        c->err = "liquid step: rb200_carrier_liquid_inputs has not been called";
+        return RB200_INVALID_ARGUMENT;
+    }
     RB200_CUDA(cudaMemcpyAsync(&c->cd->requested_dt, &c->h_cd->requested_dt,
                                offsetof(CarrierDev, max_courant) - offsetof(CarrierDev, requested_dt),
                                cudaMemcpyHostToDevice, c->stream));
+    if (c->lq_d)
+        RB200_CUDA(cudaMemcpyAsync(c->lflow_d, c->lflow_h, sizeof(LiquidFlowDev), cudaMemcpyHostToDevice, c->stream));
     cudaEvent_t lane = c->solver.persistent_blocks() ? cooperative_lane(c->device) : nullptr;
     if (c->solver.persistent_blocks() && !lane) return RB200_EXECUTION;
     if (lane) RB200_CUDA(cudaStreamWaitEvent(c->stream, lane, 0));
@@ -630,6 +693,102 @@ int rb200_carrier_step_wait(rb200_carrier* carrier, rb200_step_report* report) {
     return h.step_status;
 }
 
+// LiquidTransportSimulation (src/liquid_step.rs:828-900) on the resident
+// carrier: a liquid-volume state owned by the carrier, advanced in every step
+// through the step's corrected faces and committed with it.
+int rb200_carrier_attach_liquid(rb200_carrier* carrier, double density, rb200_liquid_stamp stamp,
+                                uint64_t flow_id, const double* fraction, uint64_t limit,
+                                rb200_liquid_report* error) {
+    if (!carrier || !fraction) return RB200_INVALID_ARGUMENT;
+    rb200_carrier* c = carrier;
+    if (c->in_flight || c->lq_d) return RB200_INVALID_ARGUMENT;
+    if (c->cfg.storage != RB200_FACES_F32) {
+        c->err = "liquid step: needs f32 face storage (LiquidFlowInterval carries f32 velocities)";
+        return RB200_UNSUPPORTED;
+    }
+    cudaSetDevice(c->device);
+    if (cudaMallocHost(&c->lq_h, sizeof(LiquidDev)) != cudaSuccess ||
+        cudaMallocHost(&c->lflow_h, sizeof(LiquidFlowDev)) != cudaSuccess ||
+        cudaMallocHost(&c->lrep_h, sizeof(rb200_liquid_report)) != cudaSuccess ||
+        cudaMalloc(&c->lflow_d, sizeof(LiquidFlowDev)) != cudaSuccess ||
+        cudaMalloc(&c->lrep_d, sizeof(rb200_liquid_report)) != cudaSuccess) {
+        cudaGetLastError();
+        return RB200_OUT_OF_MEMORY;
+    }
+    std::memset(c->lflow_h, 0, sizeof(LiquidFlowDev));
+    std::memset(c->lrep_h, 0, sizeof(rb200_liquid_report));
+    LiquidDev* d = nullptr;
+    int rc = liquid_state_create(c->g, density, stamp, c->h_cd->time, fraction, limit, c->lq_h, &d, &c->lq_sc,
+                                 &c->lq_blocks, error, c->stream);
+    if (rc) {
+        liquid_state_free(c->lq_h, d, &c->lq_sc);
+        cudaFreeHost(c->lq_h);
+        c->lq_h = nullptr;
+        return rc;
+    }
+    c->lq_d = d;
+    RB200_CUDA(cudaMemsetAsync(c->lrep_d, 0, sizeof(rb200_liquid_report), c->stream));
+    c->h_cd->liquid = c->lq_d;
+    c->h_cd->lflow = c->lflow_d;
+    c->h_cd->lrep = c->lrep_d;
+    c->h_cd->flow_id = flow_id;
+    RB200_CUDA(cudaMemcpyAsync(&c->cd->liquid, &c->h_cd->liquid,
+                               offsetof(CarrierDev, flow_id) + sizeof(unsigned long long) - offsetof(CarrierDev, liquid),
+                               cudaMemcpyHostToDevice, c->stream));
+    c->bytes += 2ull * uint64_t(c->g.cells) * 8;
+    RB200_CUDA(cudaStreamSynchronize(c->stream));
+    // the step graph now holds the liquid interval
+    if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
+    c->step_exec = nullptr;
+    return capture_step<float>(c);
+}
+
+// LiquidStepInputs' inlet, source and volume settings (src/liquid_step.rs)
+// for the following steps. source may be NULL; its rate is device memory that
+// must stay valid while steps run.
+int rb200_carrier_liquid_inputs(rb200_carrier* carrier, const rb200_liquid_inlet* inlet,
+                                const rb200_liquid_source* source, const rb200_liquid_settings* settings) {
+    if (!carrier || !inlet || !settings) return RB200_INVALID_ARGUMENT;
+    rb200_carrier* c = carrier;
+    if (!c->lq_d || c->in_flight) return RB200_INVALID_ARGUMENT;
+    LiquidFlowDev& f = *c->lflow_h;
+    f.inlet = inlet->stamp;
+    for (int q = 0; q < 6; ++q) f.inlet_fraction[q] = inlet->fraction[q];
+    f.src = source ? source->rate : nullptr;
+    f.source = source ? source->stamp : rb200_liquid_stamp{0, 0};
+    f.max_courant = settings->max_outward_courant;
+    f.divergence_limit = settings->actual_divergence_limit;
+    c->lq_inputs = true;
+    return RB200_OK;
+}
+
+int rb200_carrier_liquid_report(const rb200_carrier* carrier, rb200_liquid_report* report) {
+    if (!carrier || !report || !carrier->lq_d) return RB200_INVALID_ARGUMENT;
+    if (carrier->in_flight) return RB200_INVALID_ARGUMENT;
+    *report = *carrier->lrep_h;
+    return RB200_OK;
+}
+
+int rb200_carrier_liquid_state(const rb200_carrier* carrier, const double** fraction, rb200_liquid_stamp* stamp,
+                               double* time) {
+    if (!carrier || !carrier->lq_d || carrier->in_flight) return RB200_INVALID_ARGUMENT;
+    const LiquidDev& L = *carrier->lq_h;
+    if (fraction) *fraction = L.frac[L.acc];
+    if (stamp) *stamp = rb200_liquid_stamp{L.id, L.version};
+    if (time) *time = L.time;
+    return RB200_OK;
+}
+
+int rb200_carrier_liquid_download(rb200_carrier* carrier, double* out, size_t len) {
+    if (!carrier || !out || !carrier->lq_d || carrier->in_flight) return RB200_INVALID_ARGUMENT;
+    rb200_carrier* c = carrier;
+    if (len != size_t(c->g.cells)) return RB200_LENGTH_MISMATCH;
+    cudaSetDevice(c->device);
+    RB200_CUDA(cudaMemcpyAsync(out, c->lq_h->frac[c->lq_h->acc], len * 8, cudaMemcpyDefault, c->stream));
+    RB200_CUDA(cudaStreamSynchronize(c->stream));
+    return RB200_OK;
+}
+
 int rb200_carrier_dense3d_fields(rb200_carrier* carrier, rb200_dense3d_fields* f) {
     if (!carrier || !f) return RB200_INVALID_ARGUMENT;
     rb200_carrier* c = carrier;
@@ -640,7 +799,7 @@ int rb200_carrier_dense3d_fields(rb200_carrier* carrier, rb200_dense3d_fields* f
     f->v = c->faces[a][1];
     f->w = c->faces[a][2];
     f->tracer = c->tracer[0] ? c->tracer[c->h_cd->tacc] : nullptr;
-    f->fraction = nullptr;
+    f->fraction = c->lq_h ? c->lq_h->frac[c->lq_h->acc] : nullptr;
     if (c->accepted_steps == 0) {
         f->pressure = nullptr;
     } else if (c->accepted_p) {

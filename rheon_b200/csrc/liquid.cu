@@ -19,12 +19,12 @@
 // only replaced by the host after success.
 #include <cfloat>
 
-#include "internal.hpp"
+#include "liquid.hpp"
 
 namespace rb200 {
 namespace {
 
-constexpr int LQ_THREADS = 256;
+constexpr int LQ_THREADS = kLiquidThreads;
 constexpr int LQ_K = 8;  // dd sums: before, after, inward, outward, source, |source|, dry, full
 constexpr int LQ_M = 4;  // maxima: courant, |div|, -fraction (min), fraction
 constexpr int LQ_STRIDE = 2 * LQ_K + LQ_M;
@@ -33,32 +33,24 @@ constexpr int LQ_STRIDE = 2 * LQ_K + LQ_M;
 enum : int { LQ_ARITH = RB200_LIQUID_ARITHMETIC_FAILURE, LQ_COURANT = RB200_LIQUID_COURANT_LIMIT,
              LQ_BOUNDS = RB200_LIQUID_FRACTION_BOUNDS };
 
-struct LqResult {
-    double sums[LQ_K];
-    double maxs[LQ_M];
-    int face_failed;
-    int velocity_nonfinite;
-    int source_nonfinite;
-    int first_code;           // the first failing cell's error
-    unsigned long long first_cell;
-    double first_actual;      // its Courant number or fraction
-};
-
 struct LqArgs {
     GridDev g;
+    LiquidDev* L;
+    const LiquidFlowDev* flow;
+    LiquidScratch sc;
+    rb200_liquid_report* out;
+};
+
+// The per-thread view of one interval: the inputs read once from device memory.
+struct LqView {
     const double* acc;
     double* cand;
     const float* vel[3];
     const double* src;
     double dt, volume;
-    double dta[3];            // product(dt, area_d), checked on the host
+    double dta[3];            // dt * area_d (its checks are part of the decision)
     double inlet[6];
     double max_courant;
-    double* part;             // [blocks][LQ_STRIDE]
-    unsigned* ticket;
-    unsigned long long* first_cell;  // atomicMin target, ULLONG_MAX when no cell failed
-    int* flags;               // [0] face failure, [1] nonfinite velocity, [2] nonfinite source
-    LqResult* out;
 };
 
 // product / quotient (src/liquid_volume.rs:879-896): overflow, a subnormal
@@ -77,8 +69,8 @@ __device__ __forceinline__ double quot_chk(double a, double b, bool& bad) {
 // Transfer through face p of axis d (src/liquid_volume.rs:587-639): the
 // upwind donor fraction (the inlet's outside fraction on inflow through the
 // box), times dt, area and velocity.
-__device__ __forceinline__ double face_transfer(const LqArgs& a, int d, int i, int j, int k, double v, bool& bad) {
-    const GridDev& g = a.g;
+__device__ __forceinline__ double face_transfer(const GridDev& g, const LqView& a, int d, int i, int j, int k,
+                                                double v, bool& bad) {
     const int p[3] = {i, j, k};
     double donor = 0.0;
     if (v > 0.0) {
@@ -103,8 +95,7 @@ struct CellOut {
 };
 
 // Cell update (src/liquid_volume.rs:642-699) of cell (i, j, k).
-__device__ __forceinline__ CellOut liquid_cell(const LqArgs& a, int i, int j, int k) {
-    const GridDev& g = a.g;
+__device__ __forceinline__ CellOut liquid_cell(const GridDev& g, const LqView& a, int i, int j, int k) {
     CellOut o{};
     const int c = cell_idx(g, i, j, k);
     o.src_bad = a.src && !isfinite(a.src[c]);
@@ -118,8 +109,8 @@ __device__ __forceinline__ CellOut liquid_cell(const LqArgs& a, int i, int j, in
         const float fb = a.vel[d][face_idx(g, d, hi, hj, hk)];
         o.vel_bad |= !isfinite(fa) || !isfinite(fb);
         const double va = double(fa), vb = double(fb);
-        const double tl = face_transfer(a, d, i, j, k, va, o.face_bad);
-        const double th = face_transfer(a, d, hi, hj, hk, vb, o.face_bad);
+        const double tl = face_transfer(g, a, d, i, j, k, va, o.face_bad);
+        const double th = face_transfer(g, a, d, hi, hj, hk, vb, o.face_bad);
         amount += tl - th;
         // boundary faces owned by this cell: inward / outward volume (:739-757)
         const int pd = d == 0 ? i : (d == 1 ? j : k);
@@ -170,6 +161,95 @@ __device__ __forceinline__ CellOut liquid_cell(const LqArgs& a, int i, int j, in
     return o;
 }
 
+__device__ __forceinline__ bool dev_product(double a, double b, double& v) {
+    bool bad = false;
+    v = prod_chk(a, b, bad);
+    return !bad;
+}
+
+__device__ __forceinline__ void lq_error(rb200_liquid_report& r, int code, unsigned long long cell = 0,
+                                         double actual = 0.0, double limit = 0.0) {
+    r.error = code;
+    r.error_cell = cell;
+    r.error_actual = actual;
+    r.error_limit = limit;
+}
+
+// The outcome of one interval, in the reference's order: the checks of
+// LiquidFlowInterval::new (:123-150), LiquidInlet::new (:84-96) and
+// LiquidVolumeSource::new (:185-190) as a caller constructing them meets
+// them, then prepare_with_boundary (:520-529, validate_advance :485-506), the
+// face transfers, the first failing cell, the divergence limit and the ledger
+// (:700-776). Thread 0 of the last block.
+__device__ void liquid_decide(const GridDev& g, const LiquidDev& L, const LiquidFlowDev& f, const LqView& v,
+                              const dd (&sums)[LQ_K], const double (&maxs)[LQ_M], const int* flags,
+                              unsigned long long first, const CellOut& fc, rb200_liquid_report& r) {
+    r = rb200_liquid_report{};
+    const double start = f.start, dt = f.dt;
+    if (!isfinite(start) || start < 0.0 || !isfinite(dt) || dt <= 0.0) return lq_error(r, RB200_LIQUID_INVALID_TIME_STEP);
+    const double end = start + dt;
+    if (!isfinite(end) || end <= start) return lq_error(r, RB200_LIQUID_TIME_RESOLUTION);
+    if (flags[1]) return lq_error(r, RB200_LIQUID_NONFINITE_VELOCITY);
+    for (int q = 0; q < 6; ++q)
+        if (!isfinite(f.inlet_fraction[q]) || !(f.inlet_fraction[q] >= 0.0 && f.inlet_fraction[q] <= 1.0))
+            return lq_error(r, RB200_LIQUID_INVALID_INLET);
+    if (flags[2]) return lq_error(r, RB200_LIQUID_INVALID_SOURCE);
+    if (__double_as_longlong(start) != __double_as_longlong(L.time)) return lq_error(r, RB200_LIQUID_TIME_MISMATCH);
+    if (!isfinite(f.max_courant) || f.max_courant <= 0.0 || f.max_courant > 1.0 || !isfinite(f.divergence_limit) ||
+        f.divergence_limit < 0.0)
+        return lq_error(r, RB200_LIQUID_INVALID_SETTINGS);
+    if (L.version == ~0ull) return lq_error(r, RB200_LIQUID_VERSION_OVERFLOW);
+    const double sides[3][2] = {{g.h[1], g.h[2]}, {g.h[0], g.h[2]}, {g.h[0], g.h[1]}};
+    for (int d = 0; d < 3; ++d) {
+        double area = 0.0, dta = 0.0;
+        if (!dev_product(sides[d][0], sides[d][1], area) || !dev_product(dt, area, dta))
+            return lq_error(r, RB200_LIQUID_ARITHMETIC_FAILURE);
+    }
+    if (flags[0]) return lq_error(r, RB200_LIQUID_ARITHMETIC_FAILURE);
+    if (first != ~0ull) {
+        if (fc.code == LQ_COURANT) return lq_error(r, LQ_COURANT, first, fc.courant, f.max_courant);
+        if (fc.code == LQ_BOUNDS) return lq_error(r, LQ_BOUNDS, first, fc.fraction);
+        return lq_error(r, RB200_LIQUID_ARITHMETIC_FAILURE);
+    }
+    const double max_div = maxs[1];
+    if (max_div > f.divergence_limit) return lq_error(r, RB200_LIQUID_DIVERGENCE_LIMIT, 0, max_div, f.divergence_limit);
+    const double before = dd_value(sums[0]), after = dd_value(sums[1]);
+    const double inward = dd_value(sums[2]), outward = dd_value(sums[3]);
+    const double source_total = dd_value(sums[4]), source_abs = dd_value(sums[5]);
+    const double balance = after - before + outward - inward - source_total;
+    const double budget = (64.0 * DBL_EPSILON) * (fabs(before) + fabs(after) + outward + inward + source_abs);
+    double mass_before = 0.0, mass_after = 0.0;
+    bool ok = dev_product(L.density, before, mass_before);
+    ok = ok && dev_product(L.density, after, mass_after);
+    const double ledger[9] = {before, after, inward, outward, source_total, balance, budget, mass_before, mass_after};
+    for (double x : ledger) ok = ok && isfinite(x);
+    if (!ok) return lq_error(r, RB200_LIQUID_ARITHMETIC_FAILURE);
+    if (fabs(balance) > budget) return lq_error(r, RB200_LIQUID_BALANCE_LIMIT, 0, balance, budget);
+    r.stamp = rb200_liquid_stamp{L.id, L.version + 1};
+    r.flow = f.flow;
+    r.inlet = f.inlet;
+    r.has_source = f.src ? 1 : 0;
+    if (f.src) r.source = f.source;
+    r.dt = dt;
+    r.time = end;
+    r.liquid_volume_before = before;
+    r.liquid_volume_after = after;
+    r.inward_boundary_volume = inward;
+    r.outward_boundary_volume = outward;
+    r.source_volume = source_total;
+    r.volume_balance_error = balance;
+    r.volume_rounding_budget = budget;
+    r.liquid_mass_before = mass_before;
+    r.liquid_mass_after = mass_after;
+    r.max_outward_courant = maxs[0];
+    r.actual_divergence_max = max_div;
+    r.fraction_min = fmin(1.0, -maxs[2]);
+    r.fraction_max = fmax(0.0, maxs[3]);
+    r.dry_cells = (unsigned long long)dd_value(sums[6]);
+    r.full_cells = (unsigned long long)dd_value(sums[7]);
+    r.mixed_cells = (unsigned long long)g.cells - r.dry_cells - r.full_cells;
+}
+
 // Block maxima into thread 0 (lanes beyond the block's warps count as -inf,
 // so that the negated minimum survives).
 __device__ __forceinline__ void block_max(double (&m)[LQ_M], double (*sm)[LQ_M]) {
@@ -190,7 +270,21 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
     __shared__ BlockReduce<LQ_K, 0> red;
     __shared__ double smax[32][LQ_M];
     __shared__ bool last;
+    const LiquidFlowDev& f = *a.flow;
+    if (!f.active) return;
     const GridDev& g = a.g;
+    LqView v;
+    v.acc = a.L->frac[a.L->acc];
+    v.cand = a.L->frac[a.L->acc ^ 1];
+    for (int d = 0; d < 3; ++d) v.vel[d] = f.vel[d];
+    v.src = f.src;
+    v.dt = f.dt;
+    v.volume = a.L->volume;
+    v.dta[0] = f.dt * (g.h[1] * g.h[2]);
+    v.dta[1] = f.dt * (g.h[0] * g.h[2]);
+    v.dta[2] = f.dt * (g.h[0] * g.h[1]);
+    for (int q = 0; q < 6; ++q) v.inlet[q] = f.inlet_fraction[q];
+    v.max_courant = f.max_courant;
     dd sums[LQ_K];
     double maxs[LQ_M] = {0.0, 0.0, -INFINITY, -INFINITY};
 #pragma unroll
@@ -199,17 +293,17 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
     const int n0 = g.n[0], n01 = g.n[0] * g.n[1];
     for (int c = blockIdx.x * LQ_THREADS + threadIdx.x; c < g.cells; c += gridDim.x * LQ_THREADS) {
         const int k = c / n01, r = c - k * n01, j = r / n0, i = r - j * n0;
-        const CellOut o = liquid_cell(a, i, j, k);
+        const CellOut o = liquid_cell(g, v, i, j, k);
         face_bad |= o.face_bad;
         vel_bad |= o.vel_bad;
         src_bad |= o.src_bad;
         if (o.code) {
-            atomicMin(a.first_cell, (unsigned long long)c);
+            atomicMin(a.sc.first, (unsigned long long)c);
             continue;
         }
-        a.cand[c] = o.fraction;
-        sums[0] = dd_add1(sums[0], a.volume * a.acc[c]);
-        sums[1] = dd_add1(sums[1], a.volume * o.fraction);
+        v.cand[c] = o.fraction;
+        sums[0] = dd_add1(sums[0], v.volume * v.acc[c]);
+        sums[1] = dd_add1(sums[1], v.volume * o.fraction);
         sums[2] = dd_add1(sums[2], o.inward);
         sums[3] = dd_add1(sums[3], o.outward);
         sums[4] = dd_add1(sums[4], o.source);
@@ -221,14 +315,14 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
         maxs[2] = fmax(maxs[2], -o.fraction);
         maxs[3] = fmax(maxs[3], o.fraction);
     }
-    if (__syncthreads_or(face_bad) && threadIdx.x == 0) atomicOr(&a.flags[0], 1);
-    if (__syncthreads_or(vel_bad) && threadIdx.x == 0) atomicOr(&a.flags[1], 1);
-    if (__syncthreads_or(src_bad) && threadIdx.x == 0) atomicOr(&a.flags[2], 1);
+    if (__syncthreads_or(face_bad) && threadIdx.x == 0) atomicOr(&a.sc.flags[0], 1);
+    if (__syncthreads_or(vel_bad) && threadIdx.x == 0) atomicOr(&a.sc.flags[1], 1);
+    if (__syncthreads_or(src_bad) && threadIdx.x == 0) atomicOr(&a.sc.flags[2], 1);
     double none[1] = {0.0};
     block_reduce<LQ_K, 0>(red, sums, none);
     block_max(maxs, smax);
     if (threadIdx.x == 0) {
-        double* slot = a.part + size_t(blockIdx.x) * LQ_STRIDE;
+        double* slot = a.sc.part + size_t(blockIdx.x) * LQ_STRIDE;
 #pragma unroll
         for (int q = 0; q < LQ_K; ++q) {
             slot[2 * q] = sums[q].hi;
@@ -237,18 +331,18 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
 #pragma unroll
         for (int q = 0; q < LQ_M; ++q) slot[2 * LQ_K + q] = maxs[q];
         __threadfence();
-        last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+        last = atomicAdd(a.sc.ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
     if (!last) return;
-    // the last block folds every block's partials (in block order per thread)
+    // the last block folds every block's partials and decides
     __threadfence();
 #pragma unroll
     for (int q = 0; q < LQ_K; ++q) sums[q] = dd{0.0, 0.0};
     maxs[0] = maxs[1] = 0.0;
     maxs[2] = maxs[3] = -INFINITY;
     for (int b = threadIdx.x; b < int(gridDim.x); b += LQ_THREADS) {
-        const double* slot = a.part + size_t(b) * LQ_STRIDE;
+        const double* slot = a.sc.part + size_t(b) * LQ_STRIDE;
 #pragma unroll
         for (int q = 0; q < LQ_K; ++q) sums[q] = dd_add(sums[q], dd{__ldcg(slot + 2 * q), __ldcg(slot + 2 * q + 1)});
 #pragma unroll
@@ -257,27 +351,25 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
     block_reduce<LQ_K, 0>(red, sums, none);
     block_max(maxs, smax);
     if (threadIdx.x == 0) {
-        LqResult& R = *a.out;
-#pragma unroll
-        for (int q = 0; q < LQ_K; ++q) R.sums[q] = dd_value(sums[q]);
-#pragma unroll
-        for (int q = 0; q < LQ_M; ++q) R.maxs[q] = maxs[q];
-        R.face_failed = __ldcg(&a.flags[0]);
-        R.velocity_nonfinite = __ldcg(&a.flags[1]);
-        R.source_nonfinite = __ldcg(&a.flags[2]);
-        const unsigned long long fc = __ldcg(a.first_cell);
-        R.first_cell = fc;
-        R.first_code = 0;
-        R.first_actual = 0.0;
-        if (fc != ~0ull) {
-            const int c = int(fc);
+        int flags[3];
+        for (int q = 0; q < 3; ++q) flags[q] = __ldcg(&a.sc.flags[q]);
+        const unsigned long long first = __ldcg(a.sc.first);
+        CellOut fc{};
+        if (first != ~0ull) {
+            const int c = int(first);
             const int kk = c / n01, rr = c - kk * n01, jj = rr / n0, ii = rr - jj * n0;
-            const CellOut o = liquid_cell(a, ii, jj, kk);
-            R.first_code = o.code;
-            R.first_actual = o.code == LQ_COURANT ? o.courant : o.fraction;
+            fc = liquid_cell(g, v, ii, jj, kk);
         }
-        *a.ticket = 0u;
+        liquid_decide(g, *a.L, f, v, sums, maxs, flags, first, fc, *a.out);
+        // scratch back to its idle state for the next interval
+        *a.sc.ticket = 0u;
+        *a.sc.first = ~0ull;
+        for (int q = 0; q < 4; ++q) a.sc.flags[q] = 0;
     }
+}
+
+__global__ void k_liquid_commit(LiquidDev* L, const rb200_liquid_report* r) {
+    if (r->error == 0 && r->stamp.version != 0) liquid_commit(L, *r);
 }
 
 // LiquidVolumeState::new checks of the fraction (src/liquid_volume.rs:284-305)
@@ -331,6 +423,112 @@ bool host_product(double a, double b, double* out) {
 }
 
 }  // namespace
+
+int liquid_blocks(const GridDev& g) {
+    return std::max(1, std::min((g.cells + LQ_THREADS - 1) / LQ_THREADS, 148 * 8));
+}
+
+size_t liquid_partial_doubles(int blocks) { return size_t(blocks) * LQ_STRIDE; }
+
+cudaError_t launch_liquid_advance(const GridDev& g, LiquidDev* L, const LiquidFlowDev* flow, const LiquidScratch& sc,
+                                  int blocks, rb200_liquid_report* report, cudaStream_t stream) {
+    LqArgs a{g, L, flow, sc, report};
+    k_liquid_advance<<<blocks, LQ_THREADS, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_liquid_commit(LiquidDev* L, const rb200_liquid_report* report, cudaStream_t stream) {
+    k_liquid_commit<<<1, 1, 0, stream>>>(L, report);
+    return cudaGetLastError();
+}
+
+// Allocation of the scratch of one advance, in its idle state.
+int liquid_scratch_alloc(LiquidScratch* sc, int blocks, cudaStream_t s) {
+    if (cudaMalloc(&sc->part, liquid_partial_doubles(blocks) * 8) != cudaSuccess ||
+        cudaMalloc(&sc->ticket, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&sc->first, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&sc->flags, 4 * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return RB200_OUT_OF_MEMORY;
+    }
+    RB200_CUDA(cudaMemsetAsync(sc->ticket, 0, sizeof(unsigned), s));
+    RB200_CUDA(cudaMemsetAsync(sc->first, 0xff, sizeof(unsigned long long), s));
+    RB200_CUDA(cudaMemsetAsync(sc->flags, 0, 4 * sizeof(int), s));
+    return RB200_OK;
+}
+
+void liquid_scratch_free(LiquidScratch* sc) {
+    cudaFree(sc->part);
+    cudaFree(sc->ticket);
+    cudaFree(sc->first);
+    cudaFree(sc->flags);
+    *sc = LiquidScratch{};
+}
+
+// LiquidVolumeState::new (src/liquid_volume.rs:276-351) into device memory:
+// fraction (host or device) copied to frac[0], validated on the device.
+int liquid_state_create(const GridDev& g, double density, rb200_liquid_stamp stamp, double time,
+                        const double* fraction, uint64_t limit, LiquidDev* h, LiquidDev** d, LiquidScratch* sc,
+                        int* blocks, rb200_liquid_report* error, cudaStream_t s) {
+    std::memset(h, 0, sizeof(*h));
+    *d = nullptr;
+    if (error) std::memset(error, 0, sizeof(*error));
+    auto reject = [&](int code, uint64_t cell = 0, double actual = 0.0, double lim = 0.0) {
+        if (error) {
+            error->error = code;
+            error->error_cell = cell;
+            error->error_actual = actual;
+            error->error_limit = lim;
+        }
+        return RB200_LIQUID_REJECTED;
+    };
+    if (!std::isfinite(density) || density <= 0.0) return reject(RB200_LIQUID_INVALID_DENSITY);
+    // accepted and candidate fractions (the reference also counts three
+    // face-transfer arrays, which the device does not keep)
+    const uint64_t required = 2ull * uint64_t(g.cells) * 8ull;
+    if (required > limit) return reject(RB200_LIQUID_BUFFER_LIMIT, 0, double(required), double(limit));
+    *blocks = liquid_blocks(g);
+    const size_t n = size_t(g.cells);
+    h->density = density;
+    h->volume = g.h[0] * g.h[1] * g.h[2];
+    h->id = stamp.id;
+    h->version = stamp.version;
+    h->time = time;
+    if (cudaMalloc(&h->frac[0], n * 8) != cudaSuccess || cudaMalloc(&h->frac[1], n * 8) != cudaSuccess ||
+        cudaMalloc(d, sizeof(LiquidDev)) != cudaSuccess || liquid_scratch_alloc(sc, *blocks, s) != RB200_OK) {
+        cudaGetLastError();
+        return RB200_OUT_OF_MEMORY;
+    }
+    RB200_CUDA(cudaMemcpyAsync(h->frac[0], fraction, n * 8, cudaMemcpyDefault, s));
+    RB200_CUDA(cudaMemsetAsync(h->frac[1], 0, n * 8, s));
+    RB200_CUDA(cudaMemcpyAsync(*d, h, sizeof(LiquidDev), cudaMemcpyHostToDevice, s));
+    double* total = sc->part + liquid_partial_doubles(*blocks) - 1;
+    k_liquid_check_state<<<*blocks, LQ_THREADS, 0, s>>>(g, h->frac[0], h->volume, sc->first, sc->flags, sc->part,
+                                                        sc->ticket, total);
+    RB200_CUDA(cudaGetLastError());
+    unsigned long long bad = 0;
+    int arith = 0;
+    double initial = 0.0;
+    RB200_CUDA(cudaMemcpyAsync(&bad, sc->first, sizeof(bad), cudaMemcpyDeviceToHost, s));
+    RB200_CUDA(cudaMemcpyAsync(&arith, sc->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+    RB200_CUDA(cudaMemcpyAsync(&initial, total, sizeof(double), cudaMemcpyDeviceToHost, s));
+    RB200_CUDA(cudaMemsetAsync(sc->first, 0xff, sizeof(unsigned long long), s));
+    RB200_CUDA(cudaMemsetAsync(sc->flags, 0, 4 * sizeof(int), s));
+    RB200_CUDA(cudaStreamSynchronize(s));
+    double mass = 0.0;
+    if (bad != ~0ull) return reject(RB200_LIQUID_INVALID_FRACTION, bad);
+    if (arith || !std::isfinite(initial) || !host_product(density, initial, &mass))
+        return reject(RB200_LIQUID_ARITHMETIC_FAILURE);
+    return RB200_OK;
+}
+
+void liquid_state_free(LiquidDev* h, LiquidDev* d, LiquidScratch* sc) {
+    cudaFree(h->frac[0]);
+    cudaFree(h->frac[1]);
+    cudaFree(d);
+    liquid_scratch_free(sc);
+}
+
 }  // namespace rb200
 
 using namespace rb200;
@@ -338,48 +536,27 @@ using namespace rb200;
 struct rb200_liquid_volume {
     int device = 0;
     GridDev g{};
-    double density = 0.0;
-    double volume = 0.0;
-    rb200_liquid_stamp stamp{};
-    double time = 0.0;
-    double* frac[2] = {nullptr, nullptr};  // accepted = frac[acc]
-    int acc = 0;
+    LiquidDev* h_L = nullptr;        // pinned mirror of the device bookkeeping
+    LiquidDev* d_L = nullptr;
+    LiquidFlowDev* h_flow = nullptr; // pinned
+    LiquidFlowDev* d_flow = nullptr;
+    rb200_liquid_report* h_rep = nullptr;  // pinned
+    rb200_liquid_report* d_rep = nullptr;
+    LiquidScratch sc{};
     int blocks = 0;
-    double* part = nullptr;
-    unsigned* ticket = nullptr;
-    unsigned long long* first = nullptr;
-    int* flags = nullptr;
-    LqResult* d_out = nullptr;
-    LqResult* h_out = nullptr;  // pinned
-    uint64_t bytes = 0;
     cudaStream_t stream = nullptr;
-    std::string err;
     ~rb200_liquid_volume() {
         cudaSetDevice(device);
         if (stream) cudaStreamSynchronize(stream);
-        cudaFree(frac[0]);
-        cudaFree(frac[1]);
-        cudaFree(part);
-        cudaFree(ticket);
-        cudaFree(first);
-        cudaFree(flags);
-        cudaFree(d_out);
-        if (h_out) cudaFreeHost(h_out);
+        if (h_L) liquid_state_free(h_L, d_L, &sc);
+        cudaFree(d_flow);
+        cudaFree(d_rep);
+        if (h_L) cudaFreeHost(h_L);
+        if (h_flow) cudaFreeHost(h_flow);
+        if (h_rep) cudaFreeHost(h_rep);
         if (stream) cudaStreamDestroy(stream);
     }
 };
-
-namespace {
-
-void set_liquid_error(rb200_liquid_report* r, int code, uint64_t cell = 0, double actual = 0.0, double limit = 0.0) {
-    if (!r) return;
-    r->error = code;
-    r->error_cell = cell;
-    r->error_actual = actual;
-    r->error_limit = limit;
-}
-
-}  // namespace
 
 extern "C" {
 
@@ -391,244 +568,87 @@ int rb200_liquid_create(const rb200_grid* grid, double density, rb200_liquid_sta
     GridDev g;
     int rc = make_grid_dev(grid, 1.0, &g);
     if (rc) return rc;
-    // LiquidVolumeState::new (src/liquid_volume.rs:276-351)
-    if (!std::isfinite(density) || density <= 0.0) {
-        set_liquid_error(error, RB200_LIQUID_INVALID_DENSITY);
-        return RB200_LIQUID_REJECTED;
-    }
-    // accepted and candidate fractions (the reference also counts three
-    // face-transfer arrays, which the device does not keep)
-    const uint64_t required = 2ull * uint64_t(g.cells) * 8ull;
-    if (required > limit) {
-        set_liquid_error(error, RB200_LIQUID_BUFFER_LIMIT, 0, double(required), double(limit));
-        return RB200_LIQUID_REJECTED;
-    }
     RB200_CUDA(cudaSetDevice(device));
-    auto* L = new rb200_liquid_volume();
-    L->device = device;
-    L->g = g;
-    L->density = density;
-    L->volume = g.h[0] * g.h[1] * g.h[2];
-    L->stamp = stamp;
-    L->blocks = std::max(1, std::min((g.cells + LQ_THREADS - 1) / LQ_THREADS, 148 * 8));
-    const size_t n = size_t(g.cells);
-    bool ok = cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaMalloc(&L->frac[0], n * 8) == cudaSuccess && cudaMalloc(&L->frac[1], n * 8) == cudaSuccess &&
-              cudaMalloc(&L->part, size_t(L->blocks) * LQ_STRIDE * 8) == cudaSuccess &&
-              cudaMalloc(&L->ticket, sizeof(unsigned)) == cudaSuccess &&
-              cudaMalloc(&L->first, sizeof(unsigned long long)) == cudaSuccess &&
-              cudaMalloc(&L->flags, 4 * sizeof(int)) == cudaSuccess &&
-              cudaMalloc(&L->d_out, sizeof(LqResult)) == cudaSuccess &&
-              cudaMallocHost(&L->h_out, sizeof(LqResult)) == cudaSuccess;
-    if (!ok) {
-        delete L;
+    auto* V = new rb200_liquid_volume();
+    V->device = device;
+    V->g = g;
+    if (cudaStreamCreateWithFlags(&V->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&V->h_L, sizeof(LiquidDev)) != cudaSuccess ||
+        cudaMallocHost(&V->h_flow, sizeof(LiquidFlowDev)) != cudaSuccess ||
+        cudaMallocHost(&V->h_rep, sizeof(rb200_liquid_report)) != cudaSuccess ||
+        cudaMalloc(&V->d_flow, sizeof(LiquidFlowDev)) != cudaSuccess ||
+        cudaMalloc(&V->d_rep, sizeof(rb200_liquid_report)) != cudaSuccess) {
+        delete V;
         cudaGetLastError();
         return RB200_OUT_OF_MEMORY;
     }
-    L->bytes = 2 * n * 8;
-    const cudaStream_t s = L->stream;
-    RB200_CUDA(cudaMemcpyAsync(L->frac[0], fraction, n * 8, cudaMemcpyDefault, s));
-    RB200_CUDA(cudaMemsetAsync(L->frac[1], 0, n * 8, s));
-    RB200_CUDA(cudaMemsetAsync(L->ticket, 0, sizeof(unsigned), s));
-    RB200_CUDA(cudaMemsetAsync(L->first, 0xff, sizeof(unsigned long long), s));
-    RB200_CUDA(cudaMemsetAsync(L->flags, 0, 4 * sizeof(int), s));
-    double* total = reinterpret_cast<double*>(L->d_out);
-    k_liquid_check_state<<<L->blocks, LQ_THREADS, 0, s>>>(g, L->frac[0], L->volume, L->first, L->flags, L->part,
-                                                           L->ticket, total);
-    RB200_CUDA(cudaGetLastError());
-    unsigned long long bad = 0;
-    int arith = 0;
-    double initial = 0.0;
-    RB200_CUDA(cudaMemcpyAsync(&bad, L->first, sizeof(bad), cudaMemcpyDeviceToHost, s));
-    RB200_CUDA(cudaMemcpyAsync(&arith, L->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
-    RB200_CUDA(cudaMemcpyAsync(&initial, total, sizeof(double), cudaMemcpyDeviceToHost, s));
-    RB200_CUDA(cudaStreamSynchronize(s));
-    double mass = 0.0;
-    int code = 0;
-    if (bad != ~0ull)
-        code = RB200_LIQUID_INVALID_FRACTION;
-    else if (arith || !std::isfinite(initial) || !host_product(density, initial, &mass))
-        code = RB200_LIQUID_ARITHMETIC_FAILURE;
-    if (code) {
-        set_liquid_error(error, code, code == RB200_LIQUID_INVALID_FRACTION ? bad : 0);
-        delete L;
-        return RB200_LIQUID_REJECTED;
+    rc = liquid_state_create(g, density, stamp, 0.0, fraction, limit, V->h_L, &V->d_L, &V->sc, &V->blocks, error,
+                             V->stream);
+    if (rc) {
+        delete V;
+        return rc;
     }
-    RB200_CUDA(cudaMemsetAsync(L->first, 0xff, sizeof(unsigned long long), s));
-    RB200_CUDA(cudaMemsetAsync(L->flags, 0, 4 * sizeof(int), s));
-    *out = L;
+    *out = V;
     return RB200_OK;
 }
 
-void rb200_liquid_destroy(rb200_liquid_volume* L) { delete L; }
+void rb200_liquid_destroy(rb200_liquid_volume* V) { delete V; }
 
-uint64_t rb200_liquid_allocated_bytes(const rb200_liquid_volume* L) { return L ? L->bytes : 0; }
+uint64_t rb200_liquid_allocated_bytes(const rb200_liquid_volume* V) { return V ? 2ull * uint64_t(V->g.cells) * 8 : 0; }
 
-int rb200_liquid_state(const rb200_liquid_volume* L, const double** fraction, rb200_liquid_stamp* stamp,
+int rb200_liquid_state(const rb200_liquid_volume* V, const double** fraction, rb200_liquid_stamp* stamp,
                        double* time) {
-    if (!L) return RB200_INVALID_ARGUMENT;
-    if (fraction) *fraction = L->frac[L->acc];
-    if (stamp) *stamp = L->stamp;
-    if (time) *time = L->time;
+    if (!V) return RB200_INVALID_ARGUMENT;
+    if (fraction) *fraction = V->h_L->frac[V->h_L->acc];
+    if (stamp) *stamp = rb200_liquid_stamp{V->h_L->id, V->h_L->version};
+    if (time) *time = V->h_L->time;
     return RB200_OK;
 }
 
-int rb200_liquid_download(rb200_liquid_volume* L, double* out, size_t len) {
-    if (!L || !out) return RB200_INVALID_ARGUMENT;
-    if (len != size_t(L->g.cells)) return RB200_LENGTH_MISMATCH;
-    cudaSetDevice(L->device);
-    RB200_CUDA(cudaMemcpyAsync(out, L->frac[L->acc], len * 8, cudaMemcpyDefault, L->stream));
-    RB200_CUDA(cudaStreamSynchronize(L->stream));
+int rb200_liquid_download(rb200_liquid_volume* V, double* out, size_t len) {
+    if (!V || !out) return RB200_INVALID_ARGUMENT;
+    if (len != size_t(V->g.cells)) return RB200_LENGTH_MISMATCH;
+    cudaSetDevice(V->device);
+    RB200_CUDA(cudaMemcpyAsync(out, V->h_L->frac[V->h_L->acc], len * 8, cudaMemcpyDefault, V->stream));
+    RB200_CUDA(cudaStreamSynchronize(V->stream));
     return RB200_OK;
 }
 
-// LiquidVolumeState::advance (src/liquid_volume.rs:376-387, 520-776) with the
-// checks of LiquidFlowInterval::new (:123-150), LiquidInlet::new (:84-96) and
-// LiquidVolumeSource::new (:185-190), in the order a caller constructing the
-// interval, the inlet and the source and then advancing meets them.
-int rb200_liquid_advance(rb200_liquid_volume* L, const rb200_liquid_flow* flow, const rb200_liquid_inlet* inlet,
+// LiquidVolumeState::advance (src/liquid_volume.rs:376-387, 520-776): the
+// interval's inputs to the device, the transport and decision, the commit on
+// acceptance, then the report and the bookkeeping back.
+int rb200_liquid_advance(rb200_liquid_volume* V, const rb200_liquid_flow* flow, const rb200_liquid_inlet* inlet,
                          const rb200_liquid_source* source, const rb200_liquid_settings* settings,
                          rb200_liquid_report* report, void* stream) {
-    if (!L || !flow || !inlet || !settings || !report || !flow->u || !flow->v || !flow->w)
+    if (!V || !flow || !inlet || !settings || !report || !flow->u || !flow->v || !flow->w)
         return RB200_INVALID_ARGUMENT;
-    std::memset(report, 0, sizeof(*report));
-    const GridDev& g = L->g;
-    const double start = flow->start, dt = flow->dt;
-    if (!std::isfinite(start) || start < 0.0 || !std::isfinite(dt) || dt <= 0.0) {
-        set_liquid_error(report, RB200_LIQUID_INVALID_TIME_STEP);
-        return RB200_LIQUID_REJECTED;
-    }
-    const double end = start + dt;
-    if (!std::isfinite(end) || end <= start) {
-        set_liquid_error(report, RB200_LIQUID_TIME_RESOLUTION);
-        return RB200_LIQUID_REJECTED;
-    }
-    int late = 0;  // host-side errors ranked after the velocity scan
-    bool inlet_bad = false;
-    for (int q = 0; q < 6; ++q)
-        inlet_bad |= !std::isfinite(inlet->fraction[q]) || !(inlet->fraction[q] >= 0.0 && inlet->fraction[q] <= 1.0);
-    uint64_t tb, sb;
-    std::memcpy(&tb, &start, 8);
-    std::memcpy(&sb, &L->time, 8);
-    if (tb != sb)
-        late = RB200_LIQUID_TIME_MISMATCH;
-    else if (!std::isfinite(settings->max_outward_courant) || settings->max_outward_courant <= 0.0 ||
-             settings->max_outward_courant > 1.0 || !std::isfinite(settings->actual_divergence_limit) ||
-             settings->actual_divergence_limit < 0.0)
-        late = RB200_LIQUID_INVALID_SETTINGS;
-    else if (L->stamp.version == ~0ull)
-        late = RB200_LIQUID_VERSION_OVERFLOW;
-    LqArgs a{};
-    a.g = g;
-    a.acc = L->frac[L->acc];
-    a.cand = L->frac[L->acc ^ 1];
-    a.vel[0] = flow->u;
-    a.vel[1] = flow->v;
-    a.vel[2] = flow->w;
-    a.src = source ? source->rate : nullptr;
-    a.dt = dt;
-    a.volume = L->volume;
-    // product(dt, area_d) is the first factor of every face transfer; it is
-    // the same for all faces of an axis (src/liquid_volume.rs:551-555, 636)
-    bool area_bad = false;
-    const double sides[3][2] = {{g.h[1], g.h[2]}, {g.h[0], g.h[2]}, {g.h[0], g.h[1]}};
-    for (int d = 0; d < 3; ++d) {
-        double area = 0.0;
-        area_bad |= !host_product(sides[d][0], sides[d][1], &area);
-        area_bad |= !host_product(dt, area, &a.dta[d]);
-    }
-    for (int q = 0; q < 6; ++q) a.inlet[q] = inlet->fraction[q];
-    a.max_courant = settings->max_outward_courant;
-    a.part = L->part;
-    a.ticket = L->ticket;
-    a.first_cell = L->first;
-    a.flags = L->flags;
-    a.out = L->d_out;
-    cudaSetDevice(L->device);
-    const cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
-    k_liquid_advance<<<L->blocks, LQ_THREADS, 0, s>>>(a);
-    RB200_CUDA(cudaGetLastError());
-    RB200_CUDA(cudaMemcpyAsync(L->h_out, L->d_out, sizeof(LqResult), cudaMemcpyDeviceToHost, s));
-    RB200_CUDA(cudaMemsetAsync(L->first, 0xff, sizeof(unsigned long long), s));
-    RB200_CUDA(cudaMemsetAsync(L->flags, 0, 4 * sizeof(int), s));
+    cudaSetDevice(V->device);
+    const cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : V->stream;
+    LiquidFlowDev& f = *V->h_flow;
+    RB200_CUDA(cudaStreamSynchronize(s));  // the pinned inputs of an earlier call are free
+    f = LiquidFlowDev{};
+    f.vel[0] = flow->u;
+    f.vel[1] = flow->v;
+    f.vel[2] = flow->w;
+    f.src = source ? source->rate : nullptr;
+    f.start = flow->start;
+    f.dt = flow->dt;
+    f.flow = flow->stamp;
+    f.inlet = inlet->stamp;
+    if (source) f.source = source->stamp;
+    for (int q = 0; q < 6; ++q) f.inlet_fraction[q] = inlet->fraction[q];
+    f.max_courant = settings->max_outward_courant;
+    f.divergence_limit = settings->actual_divergence_limit;
+    f.active = 1;
+    RB200_CUDA(cudaMemcpyAsync(V->d_flow, V->h_flow, sizeof(LiquidFlowDev), cudaMemcpyHostToDevice, s));
+    RB200_CUDA(cudaMemsetAsync(V->d_rep, 0, sizeof(rb200_liquid_report), s));
+    RB200_CUDA(launch_liquid_advance(V->g, V->d_L, V->d_flow, V->sc, V->blocks, V->d_rep, s));
+    RB200_CUDA(launch_liquid_commit(V->d_L, V->d_rep, s));
+    RB200_CUDA(cudaMemcpyAsync(V->h_rep, V->d_rep, sizeof(rb200_liquid_report), cudaMemcpyDeviceToHost, s));
+    RB200_CUDA(cudaMemcpyAsync(V->h_L, V->d_L, sizeof(LiquidDev), cudaMemcpyDeviceToHost, s));
     RB200_CUDA(cudaStreamSynchronize(s));
-    const LqResult R = *L->h_out;
-    // outcome, in the reference's order
-    int code = 0;
-    if (R.velocity_nonfinite)
-        code = RB200_LIQUID_NONFINITE_VELOCITY;
-    else if (inlet_bad)
-        code = RB200_LIQUID_INVALID_INLET;
-    else if (R.source_nonfinite)
-        code = RB200_LIQUID_INVALID_SOURCE;
-    else if (late)
-        code = late;
-    else if (area_bad || R.face_failed)
-        code = RB200_LIQUID_ARITHMETIC_FAILURE;
-    if (code) {
-        set_liquid_error(report, code);
-        return RB200_LIQUID_REJECTED;
-    }
-    if (R.first_cell != ~0ull) {
-        if (R.first_code == RB200_LIQUID_COURANT_LIMIT)
-            set_liquid_error(report, R.first_code, R.first_cell, R.first_actual, settings->max_outward_courant);
-        else if (R.first_code == RB200_LIQUID_FRACTION_BOUNDS)
-            set_liquid_error(report, R.first_code, R.first_cell, R.first_actual);
-        else
-            set_liquid_error(report, RB200_LIQUID_ARITHMETIC_FAILURE);
-        return RB200_LIQUID_REJECTED;
-    }
-    const double max_div = R.maxs[1];
-    if (max_div > settings->actual_divergence_limit) {
-        set_liquid_error(report, RB200_LIQUID_DIVERGENCE_LIMIT, 0, max_div, settings->actual_divergence_limit);
-        return RB200_LIQUID_REJECTED;
-    }
-    // volume ledger (src/liquid_volume.rs:735-776)
-    const double before = R.sums[0], after = R.sums[1], inward = R.sums[2], outward = R.sums[3];
-    const double source_total = R.sums[4], source_abs = R.sums[5];
-    const double balance = after - before + outward - inward - source_total;
-    const double budget = (64.0 * DBL_EPSILON) * (std::fabs(before) + std::fabs(after) + outward + inward + source_abs);
-    double mass_before = 0.0, mass_after = 0.0;
-    bool arith = !host_product(L->density, before, &mass_before);
-    arith = arith || !host_product(L->density, after, &mass_after);
-    for (double x : {before, after, inward, outward, source_total, balance, budget, mass_before, mass_after})
-        arith = arith || !std::isfinite(x);
-    if (arith) {
-        set_liquid_error(report, RB200_LIQUID_ARITHMETIC_FAILURE);
-        return RB200_LIQUID_REJECTED;
-    }
-    if (std::fabs(balance) > budget) {
-        set_liquid_error(report, RB200_LIQUID_BALANCE_LIMIT, 0, balance, budget);
-        return RB200_LIQUID_REJECTED;
-    }
-    report->stamp = rb200_liquid_stamp{L->stamp.id, L->stamp.version + 1};
-    report->flow = flow->stamp;
-    report->inlet = inlet->stamp;
-    report->has_source = source ? 1 : 0;
-    if (source) report->source = source->stamp;
-    report->dt = dt;
-    report->time = end;
-    report->liquid_volume_before = before;
-    report->liquid_volume_after = after;
-    report->inward_boundary_volume = inward;
-    report->outward_boundary_volume = outward;
-    report->source_volume = source_total;
-    report->volume_balance_error = balance;
-    report->volume_rounding_budget = budget;
-    report->liquid_mass_before = mass_before;
-    report->liquid_mass_after = mass_after;
-    report->max_outward_courant = R.maxs[0];
-    report->actual_divergence_max = max_div;
-    report->fraction_min = std::fmin(1.0, -R.maxs[2]);
-    report->fraction_max = std::fmax(0.0, R.maxs[3]);
-    report->dry_cells = uint64_t(R.sums[6]);
-    report->full_cells = uint64_t(R.sums[7]);
-    report->mixed_cells = uint64_t(g.cells) - report->dry_cells - report->full_cells;
-    // commit (src/liquid_volume.rs:514-518)
-    L->acc ^= 1;
-    L->time = end;
-    L->stamp = report->stamp;
-    return RB200_OK;
+    *report = *V->h_rep;
+    return report->error ? RB200_LIQUID_REJECTED : RB200_OK;
 }
 
 }  // extern "C"

@@ -109,13 +109,14 @@ class Dense3dFields:
 
     @classmethod
     def from_carrier(cls, carrier, fraction=None):
-        """The carrier's accepted state (faces, tracer, the last accepted
-        pressure) plus an optional f64 fraction tensor."""
+        """The carrier's accepted state (faces, tracer, the liquid fraction
+        of an attached liquid state, the last accepted pressure); `fraction`
+        (an f64 CUDA tensor) replaces the fraction."""
         f = N.Dense3dFields()
         st = lib().rb200_carrier_dense3d_fields(carrier._handle, C.byref(f))
         if st != N.OK:
             raise Dense3dError(st)
-        out = cls(f.u or 0, f.v or 0, f.w or 0, f.tracer or 0, 0, f.pressure or 0,
+        out = cls(f.u or 0, f.v or 0, f.w or 0, f.tracer or 0, f.fraction or 0, f.pressure or 0,
                   f.velocity_storage == 1, [carrier])
         if fraction is not None:
             out.fraction = fraction.data_ptr()

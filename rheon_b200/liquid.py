@@ -19,7 +19,7 @@ from . import _native as N
 from ._native import lib
 
 __all__ = ["LiquidVolumeError", "LiquidVolumeSettings", "LiquidInlet", "LiquidVolumeReport", "LiquidVolumeState",
-           "LiquidOccupancy"]
+           "LiquidOccupancy", "LiquidStepReport", "LiquidTransportSimulation"]
 
 
 class LiquidVolumeError(RuntimeError):
@@ -197,3 +197,84 @@ class LiquidVolumeState:
         if st != N.OK:
             raise LiquidVolumeError.from_report(st, rep)
         return LiquidVolumeReport.from_c(rep)
+
+
+@dataclass
+class LiquidStepReport:
+    """LiquidStepReport's carrier and liquid parts (src/liquid_step.rs)."""
+    carrier: object
+    liquid: LiquidVolumeReport
+
+
+class LiquidTransportSimulation:
+    """LiquidTransportSimulation (src/liquid_step.rs:828-900) on a resident
+    carrier: the carrier owns a liquid-volume state, and each step advances it
+    through the step's corrected faces before the step commits. A rejected
+    transport rejects the whole step; neither state changes."""
+
+    def __init__(self, carrier, density: float, stamp, fraction, flow_id: int = 0, limit: int = 1 << 62):
+        self.carrier = carrier
+        grid = carrier.grid
+        if not hasattr(fraction, "data_ptr"):
+            fraction = np.ascontiguousarray(fraction, dtype=np.float64)
+            if fraction.size != grid.cell_len():
+                raise LiquidVolumeError("LengthMismatch")
+        err = N.LiquidReport()
+        st = lib().rb200_carrier_attach_liquid(carrier._handle, float(density), N.LiquidStamp(*stamp), int(flow_id),
+                                               _ptr(fraction), int(limit), C.byref(err))
+        if st != N.OK:
+            raise LiquidVolumeError.from_report(st, err)
+        self._keep = []
+
+    def step(self, params, inlet: LiquidInlet, settings: LiquidVolumeSettings, source=None,
+             source_stamp=(0, 0)) -> LiquidStepReport:
+        """One liquid step; raises LiquidVolumeError when the transport
+        rejects it, the carrier's SimulationError when the carrier does."""
+        inl = N.LiquidInlet(N.LiquidStamp(*inlet.stamp),
+                            (C.c_double * 6)(*[float(x) for pair in inlet.fraction for x in pair]))
+        src = None
+        if source is not None:
+            src = N.LiquidSource(N.LiquidStamp(*source_stamp), _ptr(source))
+            self._keep = [source]
+        st = lib().rb200_carrier_liquid_inputs(self.carrier._handle, C.byref(inl), C.byref(src) if src else None,
+                                               C.byref(N.LiquidSettings(settings.max_outward_courant,
+                                                                        settings.actual_divergence_limit)))
+        if st != N.OK:
+            raise LiquidVolumeError(N.STATUS_NAMES.get(st, f"Status{st}"), status=st)
+        from . import SimulationError
+
+        try:
+            rep = self.carrier.step(params)
+        except SimulationError as e:
+            if e.status == N.LIQUID_REJECTED:
+                lr = N.LiquidReport()
+                lib().rb200_carrier_liquid_report(self.carrier._handle, C.byref(lr))
+                raise LiquidVolumeError.from_report(N.LIQUID_REJECTED, lr) from None
+            raise
+        lr = N.LiquidReport()
+        lib().rb200_carrier_liquid_report(self.carrier._handle, C.byref(lr))
+        return LiquidStepReport(rep, LiquidVolumeReport.from_c(lr))
+
+    def _state(self):
+        p = C.c_void_p()
+        s = N.LiquidStamp()
+        t = C.c_double()
+        st = lib().rb200_carrier_liquid_state(self.carrier._handle, C.byref(p), C.byref(s), C.byref(t))
+        if st != N.OK:
+            raise LiquidVolumeError(N.STATUS_NAMES.get(st, f"Status{st}"), status=st)
+        return p.value or 0, (int(s.id), int(s.version)), t.value
+
+    @property
+    def stamp(self):
+        return self._state()[1]
+
+    @property
+    def time(self) -> float:
+        return self._state()[2]
+
+    def fraction(self) -> np.ndarray:
+        out = np.empty(self.carrier.grid.cell_len(), np.float64)
+        st = lib().rb200_carrier_liquid_download(self.carrier._handle, out.ctypes.data_as(C.c_void_p), out.size)
+        if st != N.OK:
+            raise LiquidVolumeError(N.STATUS_NAMES.get(st, f"Status{st}"), status=st)
+        return out

@@ -265,3 +265,92 @@ def test_validation_order():
     with pytest.raises(L.LiquidVolumeError) as e:
         L.LiquidVolumeState(grid, 1.0, (1, 0), np.full(12, 0.5), limit=100)
     assert e.value.kind == "BufferLimit"
+
+
+MAXF = 1.7976931348623157e308
+
+
+def blob(counts, center, radius):
+    """A ball of represented liquid at 0.875 occupancy: below one, so that the
+    carrier's accepted residual divergence (about 1e-9 per step) cannot push
+    a full cell over one (the reference rejects that as FractionBounds)."""
+    z, y, x = np.meshgrid(*[np.arange(n) + 0.5 for n in counts[::-1]], indexing="ij")
+    r = np.sqrt((x - center[0]) ** 2 + (y - center[1]) ** 2 + (z - center[2]) ** 2)
+    return 0.875 * np.clip(radius + 0.5 - r, 0.0, 1.0).reshape(-1)
+
+
+@pytest.mark.parametrize("mixed", [False, True], ids=["jacobi_f32", "mixed"])
+def test_liquid_step_moves_the_fraction_through_the_step_faces(mixed):
+    """src/liquid_step.rs:828-900: the transport uses the step's corrected faces
+    over [time, time + dt] and commits with the carrier."""
+    counts = (24, 20, 16)
+    grid = R.GridGeometry(counts)
+    cfg = R.CarrierConfig.mixed(with_tracer=True) if mixed else R.CarrierConfig(storage="f32", with_tracer=True)
+    sim = R.CarrierSimulation(grid, cfg)
+    sim.init_fourier(seed=11)
+    f = blob(counts, (12.0, 10.0, 8.0), 5.0)
+    lts = L.LiquidTransportSimulation(sim, 800.0, (41, 0), f, flow_id=43)
+    inlet = L.LiquidInlet((4, 0), [[0.0, 0.0]] * 3)
+    settings = L.LiquidVolumeSettings(1.0, 1e-3)
+    og = O.grid(counts)
+    t = 0.0
+    for k in range(3):
+        r = lts.step(R.StepParams(requested_dt=MAXF, cfl=0.5), inlet, settings)
+        faces = sim.download()
+        err, f2, want = O.liquid_advance(og, 800.0, f, faces, t, r.carrier.dt, inlet.fraction,
+                                         max_outward_courant=1.0, actual_divergence_limit=1e-3)
+        assert err == "Ok"
+        assert np.array_equal(lts.fraction().view(np.uint64), f2.view(np.uint64))
+        same_report(r.liquid, want)
+        assert r.liquid.flow == (43, r.carrier.generation) and r.liquid.stamp == (41, k + 1)
+        assert r.liquid.time == r.carrier.time == lts.time
+        f, t = f2, r.liquid.time
+    assert abs(want["liquid_volume_after"] - blob(counts, (12.0, 10.0, 8.0), 5.0).sum()) < 1e-9
+
+
+def test_rejected_transport_rejects_the_whole_step():
+    counts = (16, 12, 10)
+    grid = R.GridGeometry(counts)
+    sim = R.CarrierSimulation(grid, R.CarrierConfig(storage="f32"))
+    sim.init_fourier(seed=5)
+    f = blob(counts, (8.0, 6.0, 5.0), 3.0)
+    lts = L.LiquidTransportSimulation(sim, 1000.0, (41, 0), f, flow_id=43)
+    before_faces = sim.download()
+    inlet = L.LiquidInlet((4, 0), [[0.0, 0.0]] * 3)
+    prm = R.StepParams(requested_dt=MAXF, cfl=0.5)
+    with pytest.raises(L.LiquidVolumeError) as e:
+        lts.step(prm, inlet, L.LiquidVolumeSettings(1e-6, 1e-3))
+    assert e.value.kind == "CourantLimit" and e.value.limit == 1e-6
+    with pytest.raises(L.LiquidVolumeError) as e:
+        lts.step(prm, L.LiquidInlet((4, 0), [[0.0, 2.0]] * 3), L.LiquidVolumeSettings(1.0, 1e-3))
+    assert e.value.kind == "InvalidInlet"
+    # neither state moved
+    after = sim.download()
+    assert all(np.array_equal(a.view(np.uint32), b.view(np.uint32)) for a, b in zip(before_faces, after))
+    assert lts.stamp == (41, 0) and lts.time == 0.0 and np.array_equal(lts.fraction(), f)
+    r = lts.step(prm, inlet, L.LiquidVolumeSettings(1.0, 1e-3))
+    assert r.carrier.generation == 1 and r.liquid.stamp == (41, 1) and lts.time == r.carrier.time
+
+
+def test_dense3d_frame_carries_the_liquid_fraction():
+    from rheon_b200 import dense3d as D
+
+    counts = (12, 10, 8)
+    grid = R.GridGeometry(counts)
+    sim = R.CarrierSimulation(grid, R.CarrierConfig(storage="f32", with_tracer=True))
+    sim.init_fourier(seed=3)
+    lts = L.LiquidTransportSimulation(sim, 800.0, (41, 0), blob(counts, (6.0, 5.0, 4.0), 2.5), flow_id=43)
+    r = lts.step(R.StepParams(requested_dt=MAXF, cfl=0.5), L.LiquidInlet((4, 0), [[0.0, 0.0]] * 3),
+                 L.LiquidVolumeSettings(1.0, 1e-3))
+    info = D.Dense3dFrameInfo(frame=1, time_s=r.carrier.time, dt_s=r.carrier.dt, carrier_stamp=(43, 1),
+                              liquid_stamp=r.liquid.stamp,
+                              diagnostics=dict(pressure_iterations=r.carrier.pressure.iterations,
+                                               volume_before_m3=r.liquid.liquid_volume_before,
+                                               volume_after_m3=r.liquid.liquid_volume_after,
+                                               mass_after_kg=r.liquid.liquid_mass_after))
+    line = D.Dense3dEncoder(grid).encode(info, D.Dense3dFields.from_carrier(sim))
+    faces, tracer = sim.download(with_tracer=True)
+    st, want = O.dense3d_frame_text(O.grid(counts), frame=1, time_s=r.carrier.time, dt_s=r.carrier.dt,
+                                    carrier_stamp=(43, 1), liquid_stamp=r.liquid.stamp, diagnostics=info.diagnostics,
+                                    faces=faces, tracer=tracer, fraction=lts.fraction(), pressure=sim.pressure())
+    assert st == 0 and line == want
