@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--dense3d", action="store_true",
                     help="dense3D frame stream alone (device encode, end to end to a file descriptor, CPU oracle)")
     ap.add_argument("--dense3d-frames", type=int, default=20)
+    ap.add_argument("--no-liquid", action="store_true")
+    ap.add_argument("--liquid", action="store_true",
+                    help="liquid-volume transport alone (device interval, liquid step on the mixed carrier, CPU oracle)")
     ap.add_argument("--buoyant-blob", action="store_true",
                     help="mixed-precision buoyant-blob run (rel 1e-10) in lockstep with the f64 carrier, "
                          "per-step divergence and velocity/tracer error; --n cells per axis, --steps steps")
@@ -520,6 +523,91 @@ def run_dense3d(args, local, with_cpu):
     return res
 
 
+def run_liquid(args, local, with_cpu):
+    """Liquid-volume transport (src/liquid_volume.rs:520-776) at n^3: a ball of
+    represented liquid (0.875 occupancy, radius n/4) moved through the
+    corrected faces of one mixed-carrier step. Device time of one interval
+    (CUDA events on the launching stream), the liquid step against the plain
+    mixed step, and the oracle's interval on one host core."""
+    import torch
+
+    import rheon_b200 as R
+    from rheon_b200 import liquid as L
+
+    torch.cuda.set_device(local)
+    n = args.n
+    g = R.GridGeometry((n, n, n))
+    sim = R.CarrierSimulation(g, R.CarrierConfig.mixed(device=local))
+    sim.init_fourier(seed=args.seed)
+    rep = sim.step(R.StepParams(requested_dt=MAXF, cfl=0.5))
+    zz, yy, xx = np.meshgrid(*[np.arange(n) + 0.5] * 3, indexing="ij")
+    r = np.sqrt((xx - n / 2) ** 2 + (yy - n / 2) ** 2 + (zz - n / 2) ** 2)
+    fraction = (0.875 * np.clip(n / 4 + 0.5 - r, 0.0, 1.0)).reshape(-1)
+    st = L.LiquidVolumeState(g, 800.0, (41, 0), fraction, device=local)
+    u, v, w, _ = sim.state_device_ptrs()
+    host_faces = sim.download() if with_cpu else None
+    inlet = L.LiquidInlet((4, 0), [[0.0, 0.0]] * 3)
+    settings = L.LiquidVolumeSettings(1.0, 1e-2)
+    stream = torch.cuda.current_stream()
+    for _ in range(3):
+        st.advance([u, v, w], st.time, rep.dt, (43, 1), inlet, settings, stream=stream.cuda_stream)
+    k = max(5, args.steps)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * k)]
+    for i in range(k):
+        ev[2 * i].record(stream)
+        st.advance([u, v, w], st.time, rep.dt, (43, 1), inlet, settings, stream=stream.cuda_stream)
+        ev[2 * i + 1].record(stream)
+    torch.cuda.synchronize()
+    ms = statistics.median(ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(k))
+    cells = g.cell_len()
+    faces = sum(g.face_len(a) for a in range(3))
+    algo = 16 * cells + 4 * faces  # fraction read and written, f32 faces read
+    hbm, kind = peaks()
+    res = {
+        "workload": f"liquid-volume interval at {n}^3 through a mixed-carrier step's corrected faces",
+        "ms_per_interval": ms,
+        "value": cells / (ms / 1e3),
+        "unit": "cell-intervals/s",
+        "roofline": {"kernel": "k_liquid_advance (one interval, with its decision)", "bound": "hbm",
+                     "achieved": algo / (ms / 1e3) / 1e9, "peak": hbm, "peak_kind": kind, "unit": "GB/s",
+                     "frac": algo / (ms / 1e3) / 1e9 / hbm, "algorithmic_bytes_per_interval": algo,
+                     "note": "the interval's event time includes the input upload, the commit kernel and the "
+                             "report read-back of the standalone call"},
+    }
+    # the liquid step: the transport inside the mixed carrier's step graph
+    sim2 = R.CarrierSimulation(g, R.CarrierConfig.mixed(device=local))
+    sim2.init_fourier(seed=args.seed)
+    lts = L.LiquidTransportSimulation(sim2, 800.0, (41, 0), fraction, flow_id=43)
+    prm = R.StepParams(requested_dt=MAXF, cfl=0.5)
+    for _ in range(2):
+        lts.step(prm, inlet, settings)
+        sim.step(prm)
+    steps = max(5, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.step(prm)
+    plain = (time.perf_counter() - t0) / steps
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        lr = lts.step(prm, inlet, settings)
+    with_liquid = (time.perf_counter() - t0) / steps
+    res["liquid_step"] = {"ms_per_step": with_liquid * 1e3, "ms_per_mixed_step_alone": plain * 1e3,
+                          "liquid_volume_after": lr.liquid.liquid_volume_after,
+                          "volume_balance_error": lr.liquid.volume_balance_error}
+    if with_cpu:
+        import oracle as O
+
+        t0 = time.perf_counter()
+        err, _, _ = O.liquid_advance(O.grid((n, n, n)), 800.0, fraction, host_faces, 0.0, rep.dt, inlet.fraction,
+                                     actual_divergence_limit=1e-2)
+        cpu_s = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": cells / cpu_s, "unit": "cell-intervals/s", "cores": 1, "kind": "port",
+                               "sample": f"one {n}^3 interval of the oracle ({err})"}
+    sim.close()
+    sim2.close()
+    return res
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -735,6 +823,8 @@ def run_ours(args, world, rank, local):
     sim.close()
     if not args.no_dense3d and world == 1:
         result["dense3d"] = run_dense3d(args, local, with_cpu=not args.no_cpu_baseline)
+    if not args.no_liquid and world == 1:
+        result["liquid"] = run_liquid(args, local, with_cpu=not args.no_cpu_baseline)
     return result
 
 
@@ -827,6 +917,9 @@ def main():
         return
     if args.dense3d:
         print(json.dumps(run_dense3d(args, local, with_cpu=not args.no_cpu_baseline)), flush=True)
+        return
+    if args.liquid:
+        print(json.dumps(run_liquid(args, local, with_cpu=not args.no_cpu_baseline)), flush=True)
         return
     result = run_ours(args, world, rank, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
