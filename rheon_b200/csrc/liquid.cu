@@ -49,6 +49,7 @@ struct LqView {
     const double* src;
     double dt, volume;
     double dta[3];            // dt * area_d (its checks are part of the decision)
+    double rh[3], rvol;       // RN(1/h_d), RN(1/volume) for correctly rounded division (0: divide)
     double inlet[6];
     double max_courant;
 };
@@ -62,6 +63,14 @@ __device__ __forceinline__ double prod_chk(double a, double b, bool& bad) {
 }
 __device__ __forceinline__ double quot_chk(double a, double b, bool& bad) {
     const double v = a / b;
+    if (!isfinite(v) || (v != 0.0 && fabs(v) < DBL_MIN) || (v == 0.0 && a != 0.0)) bad = true;
+    return v;
+}
+// The same quotient by a positive divisor b with yb = RN(1/b): div_diag
+// gives the correctly rounded a / b (three operations in range, a division
+// otherwise).
+__device__ __forceinline__ double quot_chk_r(double a, double b, double yb, bool& bad) {
+    const double v = div_diag(a, b, yb);
     if (!isfinite(v) || (v != 0.0 && fabs(v) < DBL_MIN) || (v == 0.0 && a != 0.0)) bad = true;
     return v;
 }
@@ -128,8 +137,8 @@ __device__ __forceinline__ CellOut liquid_cell(const GridDev& g, const LqView& a
             else
                 o.outward += value;
         }
-        courant += quot_chk(prod_chk(a.dt, fmax(vb, 0.0) - fmin(va, 0.0), bad), g.h[d], bad);
-        div += quot_chk(vb - va, g.h[d], bad);
+        courant += quot_chk_r(prod_chk(a.dt, fmax(vb, 0.0) - fmin(va, 0.0), bad), g.h[d], a.rh[d], bad);
+        div += quot_chk_r(vb - va, g.h[d], a.rh[d], bad);
     }
     o.courant = courant;
     o.div = div;
@@ -146,7 +155,7 @@ __device__ __forceinline__ CellOut liquid_cell(const GridDev& g, const LqView& a
         o.source = prod_chk(a.dt, a.src[c], bad2);
         amount += o.source;
     }
-    const double fraction = quot_chk(amount, a.volume, bad2);
+    const double fraction = quot_chk_r(amount, a.volume, a.rvol, bad2);
     o.fraction = fraction;
     if (bad2) {
         o.code = LQ_ARITH;
@@ -285,11 +294,14 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
     v.dta[2] = f.dt * (g.h[0] * g.h[1]);
     for (int q = 0; q < 6; ++q) v.inlet[q] = f.inlet_fraction[q];
     v.max_courant = f.max_courant;
+    for (int d = 0; d < 3; ++d) v.rh[d] = a.L->rh[d];
+    v.rvol = a.L->rvolume;
     dd sums[LQ_K];
     double maxs[LQ_M] = {0.0, 0.0, -INFINITY, -INFINITY};
 #pragma unroll
     for (int q = 0; q < LQ_K; ++q) sums[q] = dd{0.0, 0.0};
     bool face_bad = false, vel_bad = false, src_bad = false;
+    unsigned dry = 0u, full = 0u;
     const int n0 = g.n[0], n01 = g.n[0] * g.n[1];
     for (int c = blockIdx.x * LQ_THREADS + threadIdx.x; c < g.cells; c += gridDim.x * LQ_THREADS) {
         const int k = c / n01, r = c - k * n01, j = r / n0, i = r - j * n0;
@@ -304,12 +316,16 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
         v.cand[c] = o.fraction;
         sums[0] = dd_add1(sums[0], v.volume * v.acc[c]);
         sums[1] = dd_add1(sums[1], v.volume * o.fraction);
-        sums[2] = dd_add1(sums[2], o.inward);
-        sums[3] = dd_add1(sums[3], o.outward);
-        sums[4] = dd_add1(sums[4], o.source);
-        sums[5] = dd_add1(sums[5], fabs(o.source));
-        sums[6] = dd_add1(sums[6], o.fraction == 0.0 ? 1.0 : 0.0);
-        sums[7] = dd_add1(sums[7], o.fraction == 1.0 ? 1.0 : 0.0);
+        if (i == 0 || j == 0 || k == 0 || i + 1 == g.n[0] || j + 1 == g.n[1] || k + 1 == g.n[2]) {
+            sums[2] = dd_add1(sums[2], o.inward);
+            sums[3] = dd_add1(sums[3], o.outward);
+        }
+        if (v.src) {
+            sums[4] = dd_add1(sums[4], o.source);
+            sums[5] = dd_add1(sums[5], fabs(o.source));
+        }
+        dry += o.fraction == 0.0 ? 1u : 0u;
+        full += o.fraction == 1.0 ? 1u : 0u;
         maxs[0] = fmax(maxs[0], o.courant);
         maxs[1] = fmax(maxs[1], fabs(o.div));
         maxs[2] = fmax(maxs[2], -o.fraction);
@@ -318,6 +334,10 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
     if (__syncthreads_or(face_bad) && threadIdx.x == 0) atomicOr(&a.sc.flags[0], 1);
     if (__syncthreads_or(vel_bad) && threadIdx.x == 0) atomicOr(&a.sc.flags[1], 1);
     if (__syncthreads_or(src_bad) && threadIdx.x == 0) atomicOr(&a.sc.flags[2], 1);
+    // occupancy counts (exact in a double: fewer than 2^53 cells)
+    sums[6] = dd{double(__reduce_add_sync(0xffffffffu, dry)), 0.0};
+    sums[7] = dd{double(__reduce_add_sync(0xffffffffu, full)), 0.0};
+    if ((threadIdx.x & 31) != 0) sums[6] = sums[7] = dd{0.0, 0.0};
     double none[1] = {0.0};
     block_reduce<LQ_K, 0>(red, sums, none);
     block_max(maxs, smax);
@@ -491,6 +511,10 @@ int liquid_state_create(const GridDev& g, double density, rb200_liquid_stamp sta
     const size_t n = size_t(g.cells);
     h->density = density;
     h->volume = g.h[0] * g.h[1] * g.h[2];
+    // reciprocals for div_diag's correctly rounded division (its range: 2^-500 < divisor < 2^500)
+    auto recip = [](double x) { return (x > 0x1p-500 && x < 0x1p500) ? 1.0 / x : 0.0; };
+    for (int d = 0; d < 3; ++d) h->rh[d] = recip(g.h[d]);
+    h->rvolume = recip(h->volume);
     h->id = stamp.id;
     h->version = stamp.version;
     h->time = time;

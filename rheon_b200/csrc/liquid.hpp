@@ -29,6 +29,7 @@ struct LiquidDev {
     double time;
     unsigned long long id, version;
     double density, volume;
+    double rh[3], rvolume;     // RN(1/h_d), RN(1/volume) where the fast division may use them, else 0
 };
 
 // Scratch of one advance.
