@@ -55,15 +55,25 @@ struct LqView {
 };
 
 // product / quotient (src/liquid_volume.rs:879-896): overflow, a subnormal
-// result or underflow to zero fails.
+// result or underflow to zero fails. A result passes when it is normal (its
+// biased exponent is 1..2046), or an exact zero with a zero factor (product)
+// or a zero dividend (quotient); the exponent test is integer work.
+// Biased exponent field of v.
+__device__ __forceinline__ unsigned exp_field(double v) { return (unsigned(__double2hiint(v)) >> 20) & 0x7ffu; }
+// A product a * b fails when it is infinite or NaN (exponent 2047), or has
+// exponent 0 (zero or subnormal) while neither factor is zero: a subnormal
+// product has nonzero factors, and a zero one with nonzero factors underflowed.
 __device__ __forceinline__ double prod_chk(double a, double b, bool& bad) {
     const double v = a * b;
-    if (!isfinite(v) || (v != 0.0 && fabs(v) < DBL_MIN) || (v == 0.0 && a != 0.0 && b != 0.0)) bad = true;
+    const unsigned e = exp_field(v);
+    if (e == 0x7ffu || (e == 0u && a != 0.0 && b != 0.0)) bad = true;
     return v;
 }
+// A quotient fails when infinite or NaN, or with exponent 0 and a nonzero dividend.
 __device__ __forceinline__ double quot_chk(double a, double b, bool& bad) {
     const double v = a / b;
-    if (!isfinite(v) || (v != 0.0 && fabs(v) < DBL_MIN) || (v == 0.0 && a != 0.0)) bad = true;
+    const unsigned e = exp_field(v);
+    if (e == 0x7ffu || (e == 0u && a != 0.0)) bad = true;
     return v;
 }
 // The same quotient by a positive divisor b with yb = RN(1/b): div_diag
@@ -71,29 +81,9 @@ __device__ __forceinline__ double quot_chk(double a, double b, bool& bad) {
 // otherwise).
 __device__ __forceinline__ double quot_chk_r(double a, double b, double yb, bool& bad) {
     const double v = div_diag(a, b, yb);
-    if (!isfinite(v) || (v != 0.0 && fabs(v) < DBL_MIN) || (v == 0.0 && a != 0.0)) bad = true;
+    const unsigned e = exp_field(v);
+    if (e == 0x7ffu || (e == 0u && a != 0.0)) bad = true;
     return v;
-}
-
-// Transfer through face p of axis d (src/liquid_volume.rs:587-639): the
-// upwind donor fraction (the inlet's outside fraction on inflow through the
-// box), times dt, area and velocity.
-__device__ __forceinline__ double face_transfer(const GridDev& g, const LqView& a, int d, int i, int j, int k,
-                                                double v, bool& bad) {
-    const int p[3] = {i, j, k};
-    double donor = 0.0;
-    if (v > 0.0) {
-        if (p[d] == 0) {
-            donor = a.inlet[2 * d];
-        } else {
-            int q[3] = {i, j, k};
-            q[d] -= 1;
-            donor = a.acc[cell_idx(g, q[0], q[1], q[2])];
-        }
-    } else if (v < 0.0) {
-        donor = p[d] == g.n[d] ? a.inlet[2 * d + 1] : a.acc[cell_idx(g, i, j, k)];
-    }
-    return prod_chk(prod_chk(a.dta[d], v, bad), donor, bad);
 }
 
 struct CellOut {
@@ -103,39 +93,52 @@ struct CellOut {
     bool face_bad, vel_bad, src_bad;
 };
 
-// Cell update (src/liquid_volume.rs:642-699) of cell (i, j, k).
+// Cell update (src/liquid_volume.rs:642-699) of cell (i, j, k), with the
+// transfers of its six faces (src/liquid_volume.rs:587-639): the upwind donor
+// fraction (the inlet's outside fraction on inflow through the box) times
+// dt * area and the velocity. Donors are chosen by selects from the cell's
+// and its neighbours' fractions (indices clamped at the box), so that lanes
+// of a warp do not diverge on the velocity signs.
 __device__ __forceinline__ CellOut liquid_cell(const GridDev& g, const LqView& a, int i, int j, int k) {
     CellOut o{};
-    const int c = cell_idx(g, i, j, k);
+    const int nx = g.n[0], ny = g.n[1];
+    const int c = i + nx * (j + ny * k);
+    const int p[3] = {i, j, k};
+    const int stride[3] = {1, nx, nx * ny};
+    // the lower face of the cell on each axis; the upper one is stride[d] further
+    const int low[3] = {i + (nx + 1) * (j + ny * k), i + nx * (j + (ny + 1) * k), c};
     o.src_bad = a.src && !isfinite(a.src[c]);
+    const double fc = a.acc[c];
     bool bad = false;
-    double amount = prod_chk(a.volume, a.acc[c], bad);
+    double amount = prod_chk(a.volume, fc, bad);
     double courant = 0.0, div = 0.0;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const int hi = d == 0 ? i + 1 : i, hj = d == 1 ? j + 1 : j, hk = d == 2 ? k + 1 : k;
-        const float fa = a.vel[d][face_idx(g, d, i, j, k)];
-        const float fb = a.vel[d][face_idx(g, d, hi, hj, hk)];
+        const float fa = a.vel[d][low[d]];
+        const float fb = a.vel[d][low[d] + stride[d]];
         o.vel_bad |= !isfinite(fa) || !isfinite(fb);
         const double va = double(fa), vb = double(fb);
-        const double tl = face_transfer(g, a, d, i, j, k, va, o.face_bad);
-        const double th = face_transfer(g, a, d, hi, hj, hk, vb, o.face_bad);
+        const bool first = p[d] == 0, last = p[d] + 1 == g.n[d];
+        const double fm = a.acc[first ? c : c - stride[d]];
+        const double fp = a.acc[last ? c : c + stride[d]];
+        const double dl = va > 0.0 ? (first ? a.inlet[2 * d] : fm) : (va < 0.0 ? fc : 0.0);
+        const double dh = vb > 0.0 ? fc : (vb < 0.0 ? (last ? a.inlet[2 * d + 1] : fp) : 0.0);
+        const double tl = prod_chk(prod_chk(a.dta[d], va, o.face_bad), dl, o.face_bad);
+        const double th = prod_chk(prod_chk(a.dta[d], vb, o.face_bad), dh, o.face_bad);
         amount += tl - th;
         // boundary faces owned by this cell: inward / outward volume (:739-757)
-        const int pd = d == 0 ? i : (d == 1 ? j : k);
-        if (pd == 0) {
+        if (first) {
             const double value = -tl;
             if (value < 0.0)
                 o.inward += -value;
             else
                 o.outward += value;
         }
-        if (pd + 1 == g.n[d]) {
-            const double value = th;
-            if (value < 0.0)
-                o.inward += -value;
+        if (last) {
+            if (th < 0.0)
+                o.inward += -th;
             else
-                o.outward += value;
+                o.outward += th;
         }
         courant += quot_chk_r(prod_chk(a.dt, fmax(vb, 0.0) - fmin(va, 0.0), bad), g.h[d], a.rh[d], bad);
         div += quot_chk_r(vb - va, g.h[d], a.rh[d], bad);
@@ -303,8 +306,15 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
     bool face_bad = false, vel_bad = false, src_bad = false;
     unsigned dry = 0u, full = 0u;
     const int n0 = g.n[0], n01 = g.n[0] * g.n[1];
-    for (int c = blockIdx.x * LQ_THREADS + threadIdx.x; c < g.cells; c += gridDim.x * LQ_THREADS) {
-        const int k = c / n01, r = c - k * n01, j = r / n0, i = r - j * n0;
+    // one warp per row (j, k) of cells, lanes along x: coalesced accesses and
+    // one division per row instead of two per cell
+    const int rows = g.n[1] * g.n[2];
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (LQ_THREADS / 32);
+    for (int row = blockIdx.x * (LQ_THREADS / 32) + (threadIdx.x >> 5); row < rows; row += warps)
+    for (int i = lane; i < n0; i += 32) {
+        const int k = row / g.n[1], j = row - k * g.n[1];
+        const int c = i + n0 * row;
         const CellOut o = liquid_cell(g, v, i, j, k);
         face_bad |= o.face_bad;
         vel_bad |= o.vel_bad;
