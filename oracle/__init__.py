@@ -128,7 +128,7 @@ LIQUID_ERRORS = {0: "Ok", 1: "InvalidDensity", 2: "InvalidFraction", 3: "Invalid
                  5: "InvalidSettings", 6: "InvalidTimeStep", 7: "TimeResolution", 8: "TimeMismatch",
                  9: "LengthMismatch", 10: "NonFiniteVelocity", 11: "VersionOverflow", 12: "BufferLimit",
                  13: "CourantLimit", 14: "DivergenceLimit", 15: "FractionBounds", 16: "BalanceLimit",
-                 17: "ArithmeticFailure", 18: "Cancelled", 19: "GeometryMismatch"}
+                 17: "ArithmeticFailure", 18: "Cancelled", 19: "GeometryMismatch", 20: "PeriodicVelocityMismatch"}
 
 
 def build() -> str:
@@ -188,7 +188,7 @@ def _declare(L):
                                         C.POINTER(Settings), _P, C.POINTER(Report), _P, C.c_size_t, C.c_int]
     L.orc_liquid_advance.argtypes = [C.POINTER(Grid), C.c_double, C.c_double, C.c_uint64, _P, _P, _P, _P, _P,
                                      C.c_double, C.c_double, C.POINTER(C.c_double), _P, C.c_double, C.c_double,
-                                     C.POINTER(LiquidReport)]
+                                     C.c_int, C.POINTER(LiquidReport)]
     L.orc_liquid_validate_state.argtypes = [C.POINTER(Grid), C.c_double, _P, C.POINTER(C.c_uint64)]
     L.orc_dense3d_frame_text.argtypes = [C.POINTER(Grid), C.POINTER(Dense3dFrame), _P, _P, _P, _P, _P, _P,
                                          C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
@@ -435,9 +435,10 @@ def liquid_validate_state(g, density, fraction):
 
 
 def liquid_advance(g, density, fraction, faces, start, dt, inlet, source=None, max_outward_courant=1.0,
-                   actual_divergence_limit=1e-9, state_time=None, version=0):
-    """LiquidVolumeState::advance with an inlet boundary (src/liquid_volume.rs:
-    520-776): (error name, candidate fraction or None, report dict)."""
+                   actual_divergence_limit=1e-9, state_time=None, version=0, periodic=False):
+    """LiquidVolumeState::advance with an inlet boundary, or advance_periodic
+    (src/liquid_volume.rs:376-406, 520-776): (error name, candidate fraction or
+    None, report dict). inlet is ignored when periodic."""
     acc = _f64(fraction)
     cand = np.zeros_like(acc)
     fs = [_f32(a) for a in faces]
@@ -447,6 +448,6 @@ def liquid_advance(g, density, fraction, faces, start, dt, inlet, source=None, m
     code = lib().orc_liquid_advance(C.byref(g), density, start if state_time is None else state_time, version,
                                     _ptr(acc), _ptr(cand), _ptr(fs[0]), _ptr(fs[1]), _ptr(fs[2]), start, dt, inl,
                                     _ptr(src) if src is not None else None, max_outward_courant,
-                                    actual_divergence_limit, C.byref(rep))
+                                    actual_divergence_limit, 1 if periodic else 0, C.byref(rep))
     out = {name: getattr(rep, name) for name, _ in LiquidReport._fields_}
     return LIQUID_ERRORS[code], (cand if code == 0 else None), out

@@ -33,6 +33,7 @@ enum {
     FRACTION_BOUNDS = 15,
     BALANCE_LIMIT = 16,
     ARITHMETIC_FAILURE = 17,
+    PERIODIC_VELOCITY_MISMATCH = 20,
 };
 
 struct Fail {
@@ -103,7 +104,7 @@ extern "C" int orc_liquid_advance(const orc_grid* gi, double density, double sta
                                   const double* accepted, double* candidate, const float* u, const float* v,
                                   const float* w, double start, double dt, const double inlet[6],
                                   const double* source_rate, double max_outward_courant,
-                                  double actual_divergence_limit, orc_liquid_report* rep) {
+                                  double actual_divergence_limit, int periodic, orc_liquid_report* rep) {
     std::memset(rep, 0, sizeof(*rep));
     G g{{gi->counts[0], gi->counts[1], gi->counts[2]}, {gi->spacing[0], gi->spacing[1], gi->spacing[2]}};
     const float* vel[3] = {u, v, w};
@@ -114,9 +115,11 @@ extern "C" int orc_liquid_advance(const orc_grid* gi, double density, double sta
     for (int a = 0; a < 3; ++a)
         for (uint64_t f = 0; f < g.face_len(a); ++f)
             if (!std::isfinite(vel[a][f])) return NONFINITE_VELOCITY;
-    // LiquidInlet::new (:84-96), LiquidVolumeSource::new (:185-190)
-    for (int q = 0; q < 6; ++q)
-        if (!std::isfinite(inlet[q]) || !(inlet[q] >= 0.0 && inlet[q] <= 1.0)) return INVALID_INLET;
+    // LiquidInlet::new (:84-96), LiquidVolumeSource::new (:185-190); a
+    // periodic boundary has no inlet
+    if (!periodic)
+        for (int q = 0; q < 6; ++q)
+            if (!std::isfinite(inlet[q]) || !(inlet[q] >= 0.0 && inlet[q] <= 1.0)) return INVALID_INLET;
     if (source_rate)
         for (uint64_t c = 0; c < g.cells(); ++c)
             if (!std::isfinite(source_rate[c])) return INVALID_SOURCE;
@@ -129,6 +132,24 @@ extern "C" int orc_liquid_advance(const orc_grid* gi, double density, double sta
         !std::isfinite(actual_divergence_limit) || actual_divergence_limit < 0.0)
         return INVALID_SETTINGS;
     if (state_version == std::numeric_limits<uint64_t>::max()) return VERSION_OVERFLOW;
+    // periodic seams (:530-554): the two faces of a seam carry the same velocity
+    if (periodic)
+        for (int d = 0; d < 3; ++d) {
+            uint64_t q[3];
+            for (q[2] = 0; q[2] < g.fc(d, 2); ++q[2])
+                for (q[1] = 0; q[1] < g.fc(d, 1); ++q[1])
+                    for (q[0] = 0; q[0] < g.fc(d, 0); ++q[0]) {
+                        if (q[d] != 0) continue;
+                        uint64_t hi[3] = {q[0], q[1], q[2]};
+                        hi[d] = g.n[d];
+                        const uint64_t low = g.face(d, q), high = g.face(d, hi);
+                        if (vel[d][low] != vel[d][high]) {
+                            rep->error_cell = low;
+                            rep->error_actual = double(d);
+                            return PERIODIC_VELOCITY_MISMATCH;
+                        }
+                    }
+        }
     const double volume = g.h[0] * g.h[1] * g.h[2];
     std::vector<double> transfer[3];
     try {
@@ -141,10 +162,20 @@ extern "C" int orc_liquid_advance(const orc_grid* gi, double density, double sta
                 for (p[1] = 0; p[1] < g.fc(d, 1); ++p[1])
                     for (p[0] = 0; p[0] < g.fc(d, 0); ++p[0]) {
                         const uint64_t face = g.face(d, p);
+                        if (periodic && p[d] == g.n[d]) {  // the seam's upper face repeats its lower one
+                            uint64_t lo[3] = {p[0], p[1], p[2]};
+                            lo[d] = 0;
+                            transfer[d][face] = transfer[d][g.face(d, lo)];
+                            continue;
+                        }
                         const double velocity = double(vel[d][face]);
                         double donor = 0.0;
                         if (velocity > 0.0) {
-                            if (p[d] == 0) {
+                            if (p[d] == 0 && periodic) {
+                                uint64_t lo[3] = {p[0], p[1], p[2]};
+                                lo[d] = g.n[d] - 1;
+                                donor = accepted[g.cell(lo)];
+                            } else if (p[d] == 0) {
                                 donor = inlet[2 * d];
                             } else {
                                 uint64_t lo[3] = {p[0], p[1], p[2]};
@@ -208,7 +239,7 @@ extern "C" int orc_liquid_advance(const orc_grid* gi, double density, double sta
             for (q[2] = 0; q[2] < g.fc(d, 2); ++q[2])
                 for (q[1] = 0; q[1] < g.fc(d, 1); ++q[1])
                     for (q[0] = 0; q[0] < g.fc(d, 0); ++q[0]) {
-                        if (q[d] != 0 && q[d] != g.n[d]) continue;
+                        if (periodic || (q[d] != 0 && q[d] != g.n[d])) continue;
                         const double value = transfer[d][g.face(d, q)] * (q[d] == 0 ? -1.0 : 1.0);
                         if (value < 0.0)
                             inward_a.add(-value);

@@ -234,7 +234,11 @@ int orc_dense3d_frame_text(const orc_grid* g, const orc_dense3d_frame* frame, co
  * source validations (:123-150, :84-96, :185-190) and validate_advance
  * (:485-506). `accepted` is the state's fraction (x-fastest), `candidate`
  * receives the new fraction on success. inlet[2 d + s]: the outside fraction
- * of axis d, side s (0 lower, 1 upper). source may be NULL. Returns 0 or the
+ * of axis d, side s (0 lower, 1 upper). source may be NULL. periodic != 0 is
+ * advance_periodic (src/liquid_volume.rs:389-406): the inlet is unused, seams
+ * must carry equal velocities (PeriodicVelocityMismatch: error_cell = the
+ * lower seam face, error_actual = the axis), the upper seam face repeats the
+ * lower one's transfer, and no boundary volume is counted. Returns 0 or the
  * rb200_liquid_error code of the first failure, with its payload in the
  * report. */
 typedef struct orc_liquid_report {
@@ -254,7 +258,8 @@ typedef struct orc_liquid_report {
 int orc_liquid_advance(const orc_grid* g, double density, double state_time, uint64_t state_version,
                        const double* accepted, double* candidate, const float* u, const float* v, const float* w,
                        double start, double dt, const double inlet[6], const double* source_rate,
-                       double max_outward_courant, double actual_divergence_limit, orc_liquid_report* rep);
+                       double max_outward_courant, double actual_divergence_limit, int periodic,
+                       orc_liquid_report* rep);
 /* LiquidVolumeState::new validation (src/liquid_volume.rs:276-305): 0 or the
  * error code (InvalidDensity, InvalidFraction with *cell, ArithmeticFailure). */
 int orc_liquid_validate_state(const orc_grid* g, double density, const double* fraction, uint64_t* cell);

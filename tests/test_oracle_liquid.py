@@ -207,3 +207,82 @@ def test_interval_inlet_source_and_settings_validation():
     assert O.liquid_advance(g, 1.0, [0.5, 0.5], v, 0.5, 0.5, ok, state_time=0.0)[0] == "TimeMismatch"
     assert O.liquid_validate_state(g, 0.0, [0.5, 0.5])[0] == "InvalidDensity"
     assert O.liquid_validate_state(g, 1.0, [0.5, 1.5]) == ("InvalidFraction", 1)
+
+
+# ---- periodic boundary: tests/liquid_volume_periodic_contract.rs
+
+def uniform_fields(g, u):
+    return [np.full(O.face_len(g, d), u[d], np.float32) for d in range(3)]
+
+
+def test_periodic_matches_independent_multiaxis_upwind():
+    """liquid_volume_periodic_contract.rs:17-52"""
+    g = O.grid((2, 2, 2), (0.5, 0.5, 0.5))
+    init = [0.0, 0.25, 0.5, 1.0, 0.75, 0.125, 0.625, 0.875]
+    speeds = [0.25, -0.125, 0.0625]
+    err, f, r = O.liquid_advance(g, 998.2, init, uniform_fields(g, speeds), 0.0, 0.25, [[0.0, 0.0]] * 3,
+                                 actual_divergence_limit=0.0, periodic=True)
+    assert err == "Ok"
+    for k in range(2):
+        for j in range(2):
+            for i in range(2):
+                p = [i, j, k]
+                idx = i + 2 * j + 4 * k
+                exact = init[idx]
+                for d in range(3):
+                    donor = list(p)
+                    donor[d] = 1 - p[d]
+                    q = donor[0] + 2 * donor[1] + 4 * donor[2]
+                    exact += 0.25 * abs(float(np.float32(speeds[d]))) / 0.5 * (init[q] - init[idx])
+                assert abs(f[idx] - exact) < 1e-14
+    assert r["inward_boundary_volume"] == 0.0 and r["outward_boundary_volume"] == 0.0
+    assert abs(r["volume_balance_error"]) < 1e-14
+
+
+def test_one_cell_periodic_seams_cancel():
+    """liquid_volume_periodic_contract.rs:53-68"""
+    g = O.grid((1, 1, 1))
+    err, f, r = O.liquid_advance(g, 2.0, [0.25], uniform_fields(g, [-0.5, 0.25, -0.125]), 0.0, 0.25,
+                                 [[0.0, 0.0]] * 3, source=[0.5], actual_divergence_limit=0.0, periodic=True)
+    assert err == "Ok" and list(f) == [0.375]
+    assert r["source_volume"] == 0.125 and r["volume_balance_error"] == 0.0
+    assert r["inward_boundary_volume"] + r["outward_boundary_volume"] == 0.0
+
+
+def test_periodic_seam_mismatch_and_courant():
+    """liquid_volume_periodic_contract.rs:69-104"""
+    g = O.grid((2, 2, 2), (0.5, 0.5, 0.5))
+    u = uniform_fields(g, [0.25, 0.0, 0.0])
+    u[0][2] = 0.125  # face (2, 0, 0): the upper face of the seam at (0, 0, 0)
+    err, _, r = O.liquid_advance(g, 998.2, [0.5] * 8, u, 0.0, 0.25, [[0.0, 0.0]] * 3, actual_divergence_limit=0.0,
+                                 periodic=True)
+    assert err == "PeriodicVelocityMismatch" and r["error_actual"] == 0.0 and r["error_cell"] == 0
+    u[0][:] = 0.25
+    err, _, _ = O.liquid_advance(g, 998.2, [0.5] * 8, u, 0.0, 10.0, [[0.0, 0.0]] * 3, actual_divergence_limit=0.0,
+                                 periodic=True)
+    assert err == "CourantLimit"
+
+
+def test_box_policy_stays_non_periodic():
+    """liquid_volume_periodic_contract.rs:105-121"""
+    g = O.grid((1, 1, 1))
+    err, f, r = O.liquid_advance(g, 1.0, [0.0], uniform_fields(g, [0.5, 0.0, 0.0]), 0.0, 0.25,
+                                 [[1.0, 0.0], [0.0, 0.0], [0.0, 0.0]], actual_divergence_limit=0.0)
+    assert err == "Ok" and r["inward_boundary_volume"] == 0.125 and list(f) == [0.125]
+
+
+@pytest.mark.parametrize("d", [0, 1, 2])
+@pytest.mark.parametrize("sign", [-1.0, 1.0])
+def test_three_cell_impulse_periodic_donors(d, sign):
+    """liquid_volume_periodic_contract.rs:122-156"""
+    counts = [1, 1, 1]
+    counts[d] = 3
+    spacing = [1.0, 1.0, 1.0]
+    spacing[d] = 1.0 / 3.0
+    g = O.grid(counts, spacing)
+    speed = [0.0, 0.0, 0.0]
+    speed[d] = sign
+    err, f, _ = O.liquid_advance(g, 1.0, [1.0, 0.0, 0.0], uniform_fields(g, speed), 0.0, spacing[d] * 0.5,
+                                 [[0.0, 0.0]] * 3, actual_divergence_limit=0.0, periodic=True)
+    exact = [0.5, 0.5, 0.0] if sign > 0 else [0.5, 0.0, 0.5]
+    assert err == "Ok" and all(abs(a - b) < 1e-14 for a, b in zip(f, exact))
