@@ -543,7 +543,8 @@ typedef enum rb200_liquid_error {
     RB200_LIQUID_BALANCE_LIMIT = 16,      /* error_actual = error, error_limit = rounding budget */
     RB200_LIQUID_ARITHMETIC_FAILURE = 17,
     RB200_LIQUID_CANCELLED = 18,
-    RB200_LIQUID_GEOMETRY_MISMATCH = 19
+    RB200_LIQUID_GEOMETRY_MISMATCH = 19,
+    RB200_LIQUID_PERIODIC_VELOCITY_MISMATCH = 20  /* error_cell = the seam's lower face, error_actual = the axis */
 } rb200_liquid_error;
 
 /* VolumeStamp (src/liquid_volume.rs:6-10). */
@@ -584,8 +585,9 @@ typedef struct rb200_liquid_settings {
 
 /* LiquidVolumeReport (src/liquid_volume.rs:200-229) plus the error. */
 typedef struct rb200_liquid_report {
-    rb200_liquid_stamp stamp, flow, inlet, source;
+    rb200_liquid_stamp stamp, flow, inlet, source;  /* inlet: the boundary's stamp */
     int has_source;
+    int periodic;         /* advance_periodic */
     double dt, time;
     double liquid_volume_before, liquid_volume_after;
     double inward_boundary_volume, outward_boundary_volume, source_volume;
@@ -622,6 +624,15 @@ RB200_API int rb200_liquid_advance(rb200_liquid_volume* liquid, const rb200_liqu
                                    const rb200_liquid_inlet* inlet, const rb200_liquid_source* source,
                                    const rb200_liquid_settings* settings, rb200_liquid_report* report,
                                    void* stream);
+/* LiquidVolumeState::advance_periodic (src/liquid_volume.rs:389-406): the box
+ * wraps around on every axis. The two faces of each seam must carry the same
+ * velocity (else RB200_LIQUID_PERIODIC_VELOCITY_MISMATCH), inflow through a
+ * seam takes the fraction of the cell across it, and no boundary volume is
+ * counted; `boundary` is reported as the report's inlet stamp. */
+RB200_API int rb200_liquid_advance_periodic(rb200_liquid_volume* liquid, const rb200_liquid_flow* flow,
+                                            rb200_liquid_stamp boundary, const rb200_liquid_source* source,
+                                            const rb200_liquid_settings* settings, rb200_liquid_report* report,
+                                            void* stream);
 
 /* The liquid step on the resident carrier (LiquidTransportSimulation,
  * src/liquid_step.rs:828-900): the carrier owns a liquid-volume state, and

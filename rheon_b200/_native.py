@@ -50,7 +50,7 @@ LIQUID_ERRORS = {0: "Ok", 1: "InvalidDensity", 2: "InvalidFraction", 3: "Invalid
                  5: "InvalidSettings", 6: "InvalidTimeStep", 7: "TimeResolution", 8: "TimeMismatch",
                  9: "LengthMismatch", 10: "NonFiniteVelocity", 11: "VersionOverflow", 12: "BufferLimit",
                  13: "CourantLimit", 14: "DivergenceLimit", 15: "FractionBounds", 16: "BalanceLimit",
-                 17: "ArithmeticFailure", 18: "Cancelled", 19: "GeometryMismatch"}
+                 17: "ArithmeticFailure", 18: "Cancelled", 19: "GeometryMismatch", 20: "PeriodicVelocityMismatch"}
 
 
 class Grid(C.Structure):
@@ -154,7 +154,7 @@ class LiquidSettings(C.Structure):
 
 class LiquidReport(C.Structure):
     _fields_ = ([("stamp", LiquidStamp), ("flow", LiquidStamp), ("inlet", LiquidStamp), ("source", LiquidStamp),
-                 ("has_source", C.c_int)] +
+                 ("has_source", C.c_int), ("periodic", C.c_int)] +
                 [(n, C.c_double) for n in ("dt", "time", "liquid_volume_before", "liquid_volume_after",
                                            "inward_boundary_volume", "outward_boundary_volume", "source_volume",
                                            "volume_balance_error", "volume_rounding_budget", "liquid_mass_before",
@@ -255,6 +255,8 @@ SIGNATURES = {
     "rb200_liquid_download": (_I, [_P, _P, _S]),
     "rb200_liquid_advance": (_I, [_P, C.POINTER(LiquidFlow), C.POINTER(LiquidInlet), C.POINTER(LiquidSource),
                                   C.POINTER(LiquidSettings), C.POINTER(LiquidReport), _P]),
+    "rb200_liquid_advance_periodic": (_I, [_P, C.POINTER(LiquidFlow), LiquidStamp, C.POINTER(LiquidSource),
+                                           C.POINTER(LiquidSettings), C.POINTER(LiquidReport), _P]),
     "rb200_carrier_attach_liquid": (_I, [_P, _D, LiquidStamp, C.c_uint64, _P, C.c_uint64, C.POINTER(LiquidReport)]),
     "rb200_carrier_liquid_inputs": (_I, [_P, C.POINTER(LiquidInlet), C.POINTER(LiquidSource),
                                          C.POINTER(LiquidSettings)]),

@@ -52,6 +52,7 @@ struct LqView {
     double rh[3], rvol;       // RN(1/h_d), RN(1/volume) for correctly rounded division (0: divide)
     double inlet[6];
     double max_courant;
+    int periodic;
 };
 
 // product / quotient (src/liquid_volume.rs:879-896): overflow, a subnormal
@@ -119,22 +120,34 @@ __device__ __forceinline__ CellOut liquid_cell(const GridDev& g, const LqView& a
         o.vel_bad |= !isfinite(fa) || !isfinite(fb);
         const double va = double(fa), vb = double(fb);
         const bool first = p[d] == 0, last = p[d] + 1 == g.n[d];
-        const double fm = a.acc[first ? c : c - stride[d]];
-        const double fp = a.acc[last ? c : c + stride[d]];
-        const double dl = va > 0.0 ? (first ? a.inlet[2 * d] : fm) : (va < 0.0 ? fc : 0.0);
-        const double dh = vb > 0.0 ? fc : (vb < 0.0 ? (last ? a.inlet[2 * d + 1] : fp) : 0.0);
+        // periodic: the cell across the seam, and the seam's lower face (whose
+        // transfer the upper one repeats, src/liquid_volume.rs:570-577)
+        const int wrap = (g.n[d] - 1) * stride[d];
+        const double fm = a.acc[first ? (a.periodic ? c + wrap : c) : c - stride[d]];
+        const double fp = a.acc[last ? (a.periodic ? c - wrap : c) : c + stride[d]];
+        const double dl = va > 0.0 ? (first && !a.periodic ? a.inlet[2 * d] : fm) : (va < 0.0 ? fc : 0.0);
         const double tl = prod_chk(prod_chk(a.dta[d], va, o.face_bad), dl, o.face_bad);
-        const double th = prod_chk(prod_chk(a.dta[d], vb, o.face_bad), dh, o.face_bad);
+        double th;
+        if (last && a.periodic) {
+            const int fstride = d == 0 ? 1 : (d == 1 ? nx : nx * ny);
+            const double vs = double(a.vel[d][low[d] + stride[d] - g.n[d] * fstride]);
+            const double ds = vs > 0.0 ? fc : (vs < 0.0 ? fp : 0.0);
+            th = prod_chk(prod_chk(a.dta[d], vs, o.face_bad), ds, o.face_bad);
+        } else {
+            const double dh = vb > 0.0 ? fc : (vb < 0.0 ? (last ? a.inlet[2 * d + 1] : fp) : 0.0);
+            th = prod_chk(prod_chk(a.dta[d], vb, o.face_bad), dh, o.face_bad);
+        }
         amount += tl - th;
-        // boundary faces owned by this cell: inward / outward volume (:739-757)
-        if (first) {
+        // boundary faces owned by this cell: inward / outward volume
+        // (:739-757); a periodic box has none
+        if (first && !a.periodic) {
             const double value = -tl;
             if (value < 0.0)
                 o.inward += -value;
             else
                 o.outward += value;
         }
-        if (last) {
+        if (last && !a.periodic) {
             if (th < 0.0)
                 o.inward += -th;
             else
@@ -195,22 +208,26 @@ __device__ __forceinline__ void lq_error(rb200_liquid_report& r, int code, unsig
 // (:700-776). Thread 0 of the last block.
 __device__ void liquid_decide(const GridDev& g, const LiquidDev& L, const LiquidFlowDev& f, const LqView& v,
                               const dd (&sums)[LQ_K], const double (&maxs)[LQ_M], const int* flags,
-                              unsigned long long first, const CellOut& fc, rb200_liquid_report& r) {
+                              unsigned long long first, unsigned long long seam, const CellOut& fc,
+                              rb200_liquid_report& r) {
     r = rb200_liquid_report{};
     const double start = f.start, dt = f.dt;
     if (!isfinite(start) || start < 0.0 || !isfinite(dt) || dt <= 0.0) return lq_error(r, RB200_LIQUID_INVALID_TIME_STEP);
     const double end = start + dt;
     if (!isfinite(end) || end <= start) return lq_error(r, RB200_LIQUID_TIME_RESOLUTION);
     if (flags[1]) return lq_error(r, RB200_LIQUID_NONFINITE_VELOCITY);
-    for (int q = 0; q < 6; ++q)
-        if (!isfinite(f.inlet_fraction[q]) || !(f.inlet_fraction[q] >= 0.0 && f.inlet_fraction[q] <= 1.0))
-            return lq_error(r, RB200_LIQUID_INVALID_INLET);
+    if (!f.periodic)
+        for (int q = 0; q < 6; ++q)
+            if (!isfinite(f.inlet_fraction[q]) || !(f.inlet_fraction[q] >= 0.0 && f.inlet_fraction[q] <= 1.0))
+                return lq_error(r, RB200_LIQUID_INVALID_INLET);
     if (flags[2]) return lq_error(r, RB200_LIQUID_INVALID_SOURCE);
     if (__double_as_longlong(start) != __double_as_longlong(L.time)) return lq_error(r, RB200_LIQUID_TIME_MISMATCH);
     if (!isfinite(f.max_courant) || f.max_courant <= 0.0 || f.max_courant > 1.0 || !isfinite(f.divergence_limit) ||
         f.divergence_limit < 0.0)
         return lq_error(r, RB200_LIQUID_INVALID_SETTINGS);
     if (L.version == ~0ull) return lq_error(r, RB200_LIQUID_VERSION_OVERFLOW);
+    if (f.periodic && seam != ~0ull)
+        return lq_error(r, RB200_LIQUID_PERIODIC_VELOCITY_MISMATCH, seam & ((1ull << 40) - 1), double(seam >> 40));
     const double sides[3][2] = {{g.h[1], g.h[2]}, {g.h[0], g.h[2]}, {g.h[0], g.h[1]}};
     for (int d = 0; d < 3; ++d) {
         double area = 0.0, dta = 0.0;
@@ -241,6 +258,7 @@ __device__ void liquid_decide(const GridDev& g, const LiquidDev& L, const Liquid
     r.flow = f.flow;
     r.inlet = f.inlet;
     r.has_source = f.src ? 1 : 0;
+    r.periodic = f.periodic;
     if (f.src) r.source = f.source;
     r.dt = dt;
     r.time = end;
@@ -297,6 +315,7 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
     v.dta[2] = f.dt * (g.h[0] * g.h[1]);
     for (int q = 0; q < 6; ++q) v.inlet[q] = f.inlet_fraction[q];
     v.max_courant = f.max_courant;
+    v.periodic = f.periodic;
     for (int d = 0; d < 3; ++d) v.rh[d] = a.L->rh[d];
     v.rvol = a.L->rvolume;
     dd sums[LQ_K];
@@ -315,6 +334,17 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
     for (int i = lane; i < n0; i += 32) {
         const int k = row / g.n[1], j = row - k * g.n[1];
         const int c = i + n0 * row;
+        if (v.periodic) {
+            // seams (src/liquid_volume.rs:530-554): a lower boundary face and
+            // its upper partner carry the same velocity
+            const int p3[3] = {i, j, k};
+            const int low3[3] = {i + (n0 + 1) * (j + g.n[1] * k), i + n0 * (j + (g.n[1] + 1) * k), c};
+            const int fs3[3] = {1, n0, n01};
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                if (p3[d] == 0 && v.vel[d][low3[d]] != v.vel[d][low3[d] + g.n[d] * fs3[d]])
+                    atomicMin(a.sc.first + 1, ((unsigned long long)d << 40) | (unsigned long long)low3[d]);
+        }
         const CellOut o = liquid_cell(g, v, i, j, k);
         face_bad |= o.face_bad;
         vel_bad |= o.vel_bad;
@@ -384,16 +414,18 @@ __global__ void __launch_bounds__(LQ_THREADS) k_liquid_advance(LqArgs a) {
         int flags[3];
         for (int q = 0; q < 3; ++q) flags[q] = __ldcg(&a.sc.flags[q]);
         const unsigned long long first = __ldcg(a.sc.first);
+        const unsigned long long seam = __ldcg(a.sc.first + 1);
         CellOut fc{};
         if (first != ~0ull) {
             const int c = int(first);
             const int kk = c / n01, rr = c - kk * n01, jj = rr / n0, ii = rr - jj * n0;
             fc = liquid_cell(g, v, ii, jj, kk);
         }
-        liquid_decide(g, *a.L, f, v, sums, maxs, flags, first, fc, *a.out);
+        liquid_decide(g, *a.L, f, v, sums, maxs, flags, first, seam, fc, *a.out);
         // scratch back to its idle state for the next interval
         *a.sc.ticket = 0u;
-        *a.sc.first = ~0ull;
+        a.sc.first[0] = ~0ull;
+        a.sc.first[1] = ~0ull;
         for (int q = 0; q < 4; ++q) a.sc.flags[q] = 0;
     }
 }
@@ -476,13 +508,13 @@ cudaError_t launch_liquid_commit(LiquidDev* L, const rb200_liquid_report* report
 int liquid_scratch_alloc(LiquidScratch* sc, int blocks, cudaStream_t s) {
     if (cudaMalloc(&sc->part, liquid_partial_doubles(blocks) * 8) != cudaSuccess ||
         cudaMalloc(&sc->ticket, sizeof(unsigned)) != cudaSuccess ||
-        cudaMalloc(&sc->first, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&sc->first, 2 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMalloc(&sc->flags, 4 * sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         return RB200_OUT_OF_MEMORY;
     }
     RB200_CUDA(cudaMemsetAsync(sc->ticket, 0, sizeof(unsigned), s));
-    RB200_CUDA(cudaMemsetAsync(sc->first, 0xff, sizeof(unsigned long long), s));
+    RB200_CUDA(cudaMemsetAsync(sc->first, 0xff, 2 * sizeof(unsigned long long), s));
     RB200_CUDA(cudaMemsetAsync(sc->flags, 0, 4 * sizeof(int), s));
     return RB200_OK;
 }
@@ -648,14 +680,15 @@ int rb200_liquid_download(rb200_liquid_volume* V, double* out, size_t len) {
     return RB200_OK;
 }
 
-// LiquidVolumeState::advance (src/liquid_volume.rs:376-387, 520-776): the
-// interval's inputs to the device, the transport and decision, the commit on
-// acceptance, then the report and the bookkeeping back.
-int rb200_liquid_advance(rb200_liquid_volume* V, const rb200_liquid_flow* flow, const rb200_liquid_inlet* inlet,
-                         const rb200_liquid_source* source, const rb200_liquid_settings* settings,
-                         rb200_liquid_report* report, void* stream) {
-    if (!V || !flow || !inlet || !settings || !report || !flow->u || !flow->v || !flow->w)
-        return RB200_INVALID_ARGUMENT;
+}  // extern "C"
+
+namespace {
+
+// One standalone interval: the inputs to the device, the transport and
+// decision, the commit on acceptance, then the report and the bookkeeping back.
+int liquid_advance_impl(rb200_liquid_volume* V, const rb200_liquid_flow* flow, const rb200_liquid_inlet* inlet,
+                        rb200_liquid_stamp boundary, int periodic, const rb200_liquid_source* source,
+                        const rb200_liquid_settings* settings, rb200_liquid_report* report, void* stream) {
     cudaSetDevice(V->device);
     const cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : V->stream;
     LiquidFlowDev& f = *V->h_flow;
@@ -668,12 +701,13 @@ int rb200_liquid_advance(rb200_liquid_volume* V, const rb200_liquid_flow* flow, 
     f.start = flow->start;
     f.dt = flow->dt;
     f.flow = flow->stamp;
-    f.inlet = inlet->stamp;
+    f.inlet = periodic ? boundary : inlet->stamp;
     if (source) f.source = source->stamp;
-    for (int q = 0; q < 6; ++q) f.inlet_fraction[q] = inlet->fraction[q];
+    for (int q = 0; q < 6; ++q) f.inlet_fraction[q] = periodic ? 0.0 : inlet->fraction[q];
     f.max_courant = settings->max_outward_courant;
     f.divergence_limit = settings->actual_divergence_limit;
     f.active = 1;
+    f.periodic = periodic;
     RB200_CUDA(cudaMemcpyAsync(V->d_flow, V->h_flow, sizeof(LiquidFlowDev), cudaMemcpyHostToDevice, s));
     RB200_CUDA(cudaMemsetAsync(V->d_rep, 0, sizeof(rb200_liquid_report), s));
     RB200_CUDA(launch_liquid_advance(V->g, V->d_L, V->d_flow, V->sc, V->blocks, V->d_rep, s));
@@ -683,6 +717,27 @@ int rb200_liquid_advance(rb200_liquid_volume* V, const rb200_liquid_flow* flow, 
     RB200_CUDA(cudaStreamSynchronize(s));
     *report = *V->h_rep;
     return report->error ? RB200_LIQUID_REJECTED : RB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// LiquidVolumeState::advance (src/liquid_volume.rs:376-387, 520-776).
+int rb200_liquid_advance(rb200_liquid_volume* V, const rb200_liquid_flow* flow, const rb200_liquid_inlet* inlet,
+                         const rb200_liquid_source* source, const rb200_liquid_settings* settings,
+                         rb200_liquid_report* report, void* stream) {
+    if (!V || !flow || !inlet || !settings || !report || !flow->u || !flow->v || !flow->w)
+        return RB200_INVALID_ARGUMENT;
+    return liquid_advance_impl(V, flow, inlet, rb200_liquid_stamp{0, 0}, 0, source, settings, report, stream);
+}
+
+// LiquidVolumeState::advance_periodic (src/liquid_volume.rs:389-406).
+int rb200_liquid_advance_periodic(rb200_liquid_volume* V, const rb200_liquid_flow* flow, rb200_liquid_stamp boundary,
+                                  const rb200_liquid_source* source, const rb200_liquid_settings* settings,
+                                  rb200_liquid_report* report, void* stream) {
+    if (!V || !flow || !settings || !report || !flow->u || !flow->v || !flow->w) return RB200_INVALID_ARGUMENT;
+    return liquid_advance_impl(V, flow, nullptr, boundary, 1, source, settings, report, stream);
 }
 
 }  // extern "C"

@@ -18,7 +18,7 @@ struct LiquidFlowDev {
     double inlet_fraction[6];
     double max_courant, divergence_limit;
     int active;                // 0: nothing to do (the carrier step failed before the transport)
-    int pad;
+    int periodic;              // advance_periodic: seams instead of the inlet
 };
 
 // The state's bookkeeping (src/liquid_volume.rs:238-247), in device memory.
@@ -36,7 +36,7 @@ struct LiquidDev {
 struct LiquidScratch {
     double* part;
     unsigned* ticket;
-    unsigned long long* first;
+    unsigned long long* first;  // [0] first failing cell, [1] first mismatched seam (axis << 40 | face)
     int* flags;
 };
 

@@ -88,6 +88,7 @@ class LiquidVolumeReport:
     dry_cells: int
     mixed_cells: int
     full_cells: int
+    periodic: bool = False
 
     @classmethod
     def from_c(cls, r: N.LiquidReport) -> "LiquidVolumeReport":
@@ -96,7 +97,8 @@ class LiquidVolumeReport:
                    r.liquid_volume_before, r.liquid_volume_after, r.inward_boundary_volume,
                    r.outward_boundary_volume, r.source_volume, r.volume_balance_error, r.volume_rounding_budget,
                    r.liquid_mass_before, r.liquid_mass_after, r.max_outward_courant, r.actual_divergence_max,
-                   r.fraction_min, r.fraction_max, int(r.dry_cells), int(r.mixed_cells), int(r.full_cells))
+                   r.fraction_min, r.fraction_max, int(r.dry_cells), int(r.mixed_cells), int(r.full_cells),
+                   bool(r.periodic))
 
 
 def _ptr(x):
@@ -176,24 +178,47 @@ class LiquidVolumeState:
         return LiquidOccupancy.DRY if f[cell] == 0.0 else (LiquidOccupancy.FULL if f[cell] == 1.0
                                                            else LiquidOccupancy.MIXED)
 
+    def _flow(self, velocity, start, dt, flow_stamp):
+        ptrs = [v if isinstance(v, int) else _ptr(v) for v in velocity]
+        return N.LiquidFlow(N.LiquidStamp(*flow_stamp), ptrs[0], ptrs[1], ptrs[2], float(start), float(dt))
+
+    @staticmethod
+    def _source(source, source_stamp):
+        if source is None:
+            return None
+        return N.LiquidSource(N.LiquidStamp(*source_stamp), source if isinstance(source, int) else _ptr(source))
+
+    @staticmethod
+    def _settings(settings):
+        return N.LiquidSettings(settings.max_outward_courant, settings.actual_divergence_limit)
+
     def advance(self, velocity, start: float, dt: float, flow_stamp, inlet: LiquidInlet,
                 settings: LiquidVolumeSettings, source=None, source_stamp=(0, 0), stream: int = 0
                 ) -> LiquidVolumeReport:
         """One interval through the f32 face velocities `velocity` (three CUDA
         tensors, or device pointers) over [start, start + dt]; source: an f64
         CUDA tensor of m^3/s per cell or None."""
-        ptrs = [v if isinstance(v, int) else _ptr(v) for v in velocity]
-        flow = N.LiquidFlow(N.LiquidStamp(*flow_stamp), ptrs[0], ptrs[1], ptrs[2], float(start), float(dt))
         inl = N.LiquidInlet(N.LiquidStamp(*inlet.stamp),
                             (C.c_double * 6)(*[float(x) for pair in inlet.fraction for x in pair]))
-        src = None
-        if source is not None:
-            src = N.LiquidSource(N.LiquidStamp(*source_stamp), source if isinstance(source, int) else _ptr(source))
+        src = self._source(source, source_stamp)
         rep = N.LiquidReport()
-        st = lib().rb200_liquid_advance(self._h, C.byref(flow), C.byref(inl), C.byref(src) if src else None,
-                                        C.byref(N.LiquidSettings(settings.max_outward_courant,
-                                                                 settings.actual_divergence_limit)),
+        st = lib().rb200_liquid_advance(self._h, C.byref(self._flow(velocity, start, dt, flow_stamp)), C.byref(inl),
+                                        C.byref(src) if src else None, C.byref(self._settings(settings)),
                                         C.byref(rep), stream or None)
+        if st != N.OK:
+            raise LiquidVolumeError.from_report(st, rep)
+        return LiquidVolumeReport.from_c(rep)
+
+    def advance_periodic(self, velocity, start: float, dt: float, flow_stamp, boundary_stamp,
+                         settings: LiquidVolumeSettings, source=None, source_stamp=(0, 0), stream: int = 0
+                         ) -> LiquidVolumeReport:
+        """advance_periodic (src/liquid_volume.rs:389-406): the box wraps
+        around on every axis; seams must carry equal velocities."""
+        src = self._source(source, source_stamp)
+        rep = N.LiquidReport()
+        st = lib().rb200_liquid_advance_periodic(self._h, C.byref(self._flow(velocity, start, dt, flow_stamp)),
+                                                 N.LiquidStamp(*boundary_stamp), C.byref(src) if src else None,
+                                                 C.byref(self._settings(settings)), C.byref(rep), stream or None)
         if st != N.OK:
             raise LiquidVolumeError.from_report(st, rep)
         return LiquidVolumeReport.from_c(rep)

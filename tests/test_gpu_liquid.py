@@ -354,3 +354,85 @@ def test_dense3d_frame_carries_the_liquid_fraction():
                                     carrier_stamp=(43, 1), liquid_stamp=r.liquid.stamp, diagnostics=info.diagnostics,
                                     faces=faces, tracer=tracer, fraction=lts.fraction(), pressure=sim.pressure())
     assert st == 0 and line == want
+
+
+# ---- periodic boundary (src/liquid_volume.rs:389-406)
+
+def periodic_both(counts, spacing, density, fraction, vel, dt, source=None, settings=L.LiquidVolumeSettings(1.0, 0.0)):
+    grid = R.GridGeometry(counts, spacing)
+    st = L.LiquidVolumeState(grid, density, (1, 0), np.asarray(fraction, np.float64))
+    want = O.liquid_advance(O.grid(counts, spacing), density, fraction, vel, 0.0, dt, [[0.0, 0.0]] * 3, source=source,
+                            max_outward_courant=settings.max_outward_courant,
+                            actual_divergence_limit=settings.actual_divergence_limit, periodic=True)
+    try:
+        got = st.advance_periodic([dev(v, np.float32) for v in vel], 0.0, dt, (2, 0), (9, 0), settings,
+                                  source=dev(source, np.float64) if source is not None else None, source_stamp=(3, 0))
+    except L.LiquidVolumeError as e:
+        got = e
+    return got, want, st
+
+
+def uniform(counts, u):
+    g = O.grid(counts)
+    return [np.full(O.face_len(g, d), u[d], np.float32) for d in range(3)]
+
+
+def test_periodic_known_answers():
+    """tests/liquid_volume_periodic_contract.rs:17-68, 122-156"""
+    init = [0.0, 0.25, 0.5, 1.0, 0.75, 0.125, 0.625, 0.875]
+    got, want, st = periodic_both((2, 2, 2), (0.5, 0.5, 0.5), 998.2, init, uniform((2, 2, 2), [0.25, -0.125, 0.0625]),
+                                  0.25)
+    assert want[0] == "Ok" and got.periodic and got.inlet == (9, 0)
+    assert np.array_equal(st.fraction(), want[1])
+    assert got.inward_boundary_volume == 0.0 and got.outward_boundary_volume == 0.0
+    got, want, st = periodic_both((1, 1, 1), (1.0, 1.0, 1.0), 2.0, [0.25], uniform((1, 1, 1), [-0.5, 0.25, -0.125]),
+                                  0.25, source=np.array([0.5]))
+    assert list(st.fraction()) == [0.375] and got.source_volume == 0.125 and got.volume_balance_error == 0.0
+    for d in range(3):
+        for sign in (-1.0, 1.0):
+            counts = [1, 1, 1]
+            counts[d] = 3
+            spacing = [1.0, 1.0, 1.0]
+            spacing[d] = 1.0 / 3.0
+            speed = [0.0, 0.0, 0.0]
+            speed[d] = sign
+            got, want, st = periodic_both(tuple(counts), tuple(spacing), 1.0, [1.0, 0.0, 0.0],
+                                          uniform(tuple(counts), speed), spacing[d] * 0.5)
+            assert np.array_equal(st.fraction(), want[1])
+            exact = [0.5, 0.5, 0.0] if sign > 0 else [0.5, 0.0, 0.5]
+            assert all(abs(a - b) < 1e-14 for a, b in zip(st.fraction(), exact))
+
+
+def test_periodic_seam_mismatch_and_random_parity():
+    """tests/liquid_volume_periodic_contract.rs:69-104; random periodic flows bit for bit"""
+    u = uniform((2, 2, 2), [0.25, 0.0, 0.0])
+    u[0][2] = 0.125
+    got, want, st = periodic_both((2, 2, 2), (0.5, 0.5, 0.5), 998.2, [0.5] * 8, u, 0.25)
+    assert want[0] == got.kind == "PeriodicVelocityMismatch" and got.cell == 0 and got.actual == 0.0
+    assert np.all(st.fraction() == 0.5) and st.time == 0.0
+    u[1][fidx((2, 2, 2), 1, (1, 2, 1))] = 0.5  # a Y seam too: the X seam comes first
+    got, want, _ = periodic_both((2, 2, 2), (0.5, 0.5, 0.5), 998.2, [0.5] * 8, u, 0.25)
+    assert got.kind == "PeriodicVelocityMismatch" and got.actual == 0.0
+    u = uniform((2, 2, 2), [0.25, 0.0, 0.0])
+    got, _, _ = periodic_both((2, 2, 2), (0.5, 0.5, 0.5), 998.2, [0.5] * 8, u, 10.0)
+    assert got.kind == "CourantLimit"
+    for counts in [(8, 6, 5), (17, 12, 9)]:
+        rng = np.random.default_rng(sum(counts))
+        g = O.grid(counts, (0.5, 0.75, 1.25))
+        vel = [rng.uniform(-0.05, 0.05, O.face_len(g, a)).astype(np.float32) for a in range(3)]
+        for d in range(3):  # make every seam consistent: upper face = lower face
+            fc = list(counts)
+            fc[d] += 1
+            arr = vel[d].reshape(fc[2], fc[1], fc[0])
+            sl_lo = [slice(None)] * 3
+            sl_hi = [slice(None)] * 3
+            sl_lo[2 - d] = 0
+            sl_hi[2 - d] = counts[d]
+            arr[tuple(sl_hi)] = arr[tuple(sl_lo)]
+        f = rng.uniform(0.2, 0.8, int(np.prod(counts)))
+        src = rng.uniform(-1e-3, 1e-3, f.size)
+        got, want, st = periodic_both(counts, (0.5, 0.75, 1.25), 800.0, f, vel, 0.05, source=src,
+                                      settings=L.LiquidVolumeSettings(1.0, 10.0))
+        assert want[0] == "Ok", want[0]
+        assert np.array_equal(st.fraction().view(np.uint64), want[1].view(np.uint64))
+        same_report(got, want[2])
