@@ -131,6 +131,13 @@ LIQUID_ERRORS = {0: "Ok", 1: "InvalidDensity", 2: "InvalidFraction", 3: "Invalid
                  17: "ArithmeticFailure", 18: "Cancelled", 19: "GeometryMismatch", 20: "PeriodicVelocityMismatch"}
 
 
+class BoxFluxReport(C.Structure):
+    _fields_ = [("pressure", Report), ("pressure_status", C.c_int)] + [(n, C.c_double) for n in (
+        "actual_divergence_max", "net_outward_flux", "flux_rounding_budget", "kinetic_before", "kinetic_after",
+        "correction_energy", "boundary_pressure_work", "divergence_residual_work", "correction_residual_work",
+        "budget_error")]
+
+
 def build() -> str:
     """Compile the oracle with its Makefile (idempotent)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
@@ -190,6 +197,9 @@ def _declare(L):
                                      C.c_double, C.c_double, C.POINTER(C.c_double), _P, C.c_double, C.c_double,
                                      C.c_int, C.POINTER(LiquidReport)]
     L.orc_liquid_validate_state.argtypes = [C.POINTER(Grid), C.c_double, _P, C.POINTER(C.c_uint64)]
+    L.orc_box_flux_project.argtypes = [C.POINTER(Grid), C.c_double, C.c_int, _P, _P, _P, C.c_double,
+                                       C.POINTER(C.c_float), C.POINTER(Settings), C.c_double, _P, _P, _P, _P,
+                                       C.POINTER(BoxFluxReport)]
     L.orc_dense3d_frame_text.argtypes = [C.POINTER(Grid), C.POINTER(Dense3dFrame), _P, _P, _P, _P, _P, _P,
                                          C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
     for name in ("orc_carrier_step_seeded_f32", "orc_carrier_step_seeded_f64"):
@@ -451,3 +461,20 @@ def liquid_advance(g, density, fraction, faces, start, dt, inlet, source=None, m
                                     actual_divergence_limit, 1 if periodic else 0, C.byref(rep))
     out = {name: getattr(rep, name) for name, _ in LiquidReport._fields_}
     return LIQUID_ERRORS[code], (cand if code == 0 else None), out
+
+
+def box_flux_project(g, density, method, faces, dt, outward, s: Settings, actual_divergence_limit, out=None):
+    """BoxFluxWorkspace::project (src/box_flux.rs:213-397): (status, projected
+    faces, pressure, report dict). outward: [[lower, upper]] per axis (f32).
+    out: optional initial output arrays (left untouched before the correction)."""
+    fs = [_f32(a) for a in faces]
+    outs = [np.array(o, dtype=np.float32) for o in out] if out is not None else [np.zeros_like(a) for a in fs]
+    p = np.zeros(cell_len(g))
+    ow = (C.c_float * 6)(*[float(x) for pair in outward for x in pair])
+    rep = BoxFluxReport()
+    st = lib().orc_box_flux_project(C.byref(g), density, method, _ptr(fs[0]), _ptr(fs[1]), _ptr(fs[2]), dt, ow,
+                                    C.byref(s), actual_divergence_limit, _ptr(outs[0]), _ptr(outs[1]),
+                                    _ptr(outs[2]), _ptr(p), C.byref(rep))
+    d = {n: getattr(rep, n) for n, _ in BoxFluxReport._fields_ if n not in ("pressure",)}
+    d["iterations"] = rep.pressure.iterations
+    return st, outs, p, d

@@ -264,6 +264,31 @@ int orc_liquid_advance(const orc_grid* g, double density, double state_time, uin
  * error code (InvalidDensity, InvalidFraction with *cell, ArithmeticFailure). */
 int orc_liquid_validate_state(const orc_grid* g, double density, const double* fraction, uint64_t* cell);
 
+/* Box-flux projection, BoxFluxWorkspace::project (src/box_flux.rs:213-397):
+ * the provisional faces' boundary samples are replaced by the prescribed
+ * outward speeds outward[2 d + s] (s = 0 lower, 1 upper side of axis d), the
+ * known net outward flux must vanish within 64 eps of its magnitude, the
+ * pressure is solved with the RHS of the imposed field, interior faces are
+ * corrected, and the interior energy ledger is formed (plain serial sums, as
+ * the reference). Returns 0, an orc status (12 NonFiniteInput, 14
+ * ArithmeticFailure, 10 invalid dt or settings, a PressureError code of the
+ * solve), 28 IncompatibleFlux (net, rounding budget in the report) or 15
+ * DivergenceLimit. out_* receive the projected faces (untouched before the
+ * correction), pressure_out the pressure. */
+typedef struct orc_box_flux_report {
+    orc_report pressure;
+    int pressure_status;
+    double actual_divergence_max;
+    double net_outward_flux, flux_rounding_budget;
+    double kinetic_before, kinetic_after, correction_energy;
+    double boundary_pressure_work, divergence_residual_work, correction_residual_work, budget_error;
+} orc_box_flux_report;
+
+int orc_box_flux_project(const orc_grid* g, double density, int method, const float* u, const float* v,
+                         const float* w, double dt, const float outward[6], const orc_settings* pressure,
+                         double actual_divergence_limit, float* out_u, float* out_v, float* out_w,
+                         double* pressure_out, orc_box_flux_report* rep);
+
 #ifdef __cplusplus
 }
 #endif
