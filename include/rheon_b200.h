@@ -64,7 +64,8 @@ typedef enum rb200_status {
     RB200_DENSE3D_LIMIT = 24,        /* Dense3dError::Limit                       */
     RB200_DENSE3D_ABORTED = 25,      /* Dense3dError::Aborted                     */
     RB200_DENSE3D_IO = 26,           /* Dense3dError::Io                          */
-    RB200_LIQUID_REJECTED = 27       /* LiquidVolumeError: see rb200_liquid_report.error */
+    RB200_LIQUID_REJECTED = 27,      /* LiquidVolumeError: see rb200_liquid_report.error */
+    RB200_BOX_FLUX_REJECTED = 28     /* BoxFluxError's own variants: see rb200_box_flux_report.error */
 } rb200_status;
 
 /* Pressure methods. JACOBI_PCG_V1 reproduces "jacobi-pcg-v1"
@@ -656,6 +657,110 @@ RB200_API int rb200_carrier_liquid_state(const rb200_carrier* carrier, const dou
                                          rb200_liquid_stamp* stamp, double* time);
 /* Host (or device) copy of the accepted liquid fraction. */
 RB200_API int rb200_carrier_liquid_download(rb200_carrier* carrier, double* out, size_t len);
+
+/* ------------------------------------------------------------------ box flux
+ * Prescribed outward speeds on the six sides of the fixed box
+ * (src/box_flux.rs): BoxFluxWorkspace holds the pressure workspace of the
+ * projection; project() imposes the sides' speeds on the provisional f32 faces,
+ * rejects a net boundary flux above its rounding budget, solves the sealed
+ * pressure system for the imposed field, corrects the interior faces into the
+ * output, gates the stored field's divergence and reports the energy ledger.
+ * Operator and pressure errors keep their own statuses (RB200_NONFINITE_INPUT,
+ * RB200_LENGTH_MISMATCH, RB200_INVALID_ARGUMENT for InvalidTimeStep, the
+ * PressureError statuses 6-11); BoxFluxError's own variants return
+ * RB200_BOX_FLUX_REJECTED with rb200_box_flux_report.error set. */
+typedef enum rb200_box_flux_error {
+    RB200_BOX_FLUX_NONE = 0,
+    RB200_BOX_FLUX_INVALID_BOUNDARY = 1,   /* a non-finite outward speed           */
+    RB200_BOX_FLUX_INVALID_SETTINGS = 2,   /* actual_divergence_limit              */
+    RB200_BOX_FLUX_INVALID_MASS = 3,       /* density * cell volume                */
+    RB200_BOX_FLUX_BUFFER_LIMIT = 4,       /* {required, limit}                    */
+    RB200_BOX_FLUX_INCOMPATIBLE_FLUX = 5,  /* {net, rounding_budget}: actual, limit */
+    RB200_BOX_FLUX_CANCELLED = 6,          /* {stage}                              */
+    RB200_BOX_FLUX_DIVERGENCE_LIMIT = 7,   /* {actual, limit}                      */
+    RB200_BOX_FLUX_ARITHMETIC_FAILURE = 8
+} rb200_box_flux_error;
+
+/* BoxFluxStage (src/box_flux.rs:53-59): where the cancellation predicate is asked. */
+typedef enum rb200_box_flux_stage {
+    RB200_BOX_FLUX_BEFORE_SOLVE = 0,
+    RB200_BOX_FLUX_PRESSURE_ITERATION = 1,
+    RB200_BOX_FLUX_CORRECTION_SLICE = 2,
+    RB200_BOX_FLUX_BEFORE_ACCEPTANCE = 3
+} rb200_box_flux_stage;
+
+/* PrescribedBoxFlux (src/box_flux.rs:15-46): outward[2*d] is the lower side of
+ * axis d (outward normal -d), outward[2*d+1] the upper side, in m/s. */
+typedef struct rb200_box_flux_boundary {
+    uint64_t id, version;
+    float outward[6];
+} rb200_box_flux_boundary;
+
+/* BoxFluxReport and BoxFluxWork (src/box_flux.rs:91-116) plus the error payloads. */
+typedef struct rb200_box_flux_report {
+    uint64_t boundary_id, boundary_version;
+    rb200_report pressure;
+    double actual_divergence_max;
+    double net_outward_flux;
+    double flux_rounding_budget;
+    double kinetic_before;
+    double kinetic_after;
+    double correction_energy;
+    double boundary_pressure_work;    /* -dt sum p Q                          */
+    double divergence_residual_work;  /* dt sum p cell_volume div             */
+    double correction_residual_work;  /* sum (m (v - u) + dt area dp) v       */
+    double budget_error;
+    int error;                        /* rb200_box_flux_error                 */
+    int stage;                        /* rb200_box_flux_stage of a cancel     */
+    double error_actual, error_limit; /* IncompatibleFlux / DivergenceLimit   */
+    uint64_t required, limit;         /* BufferLimit                          */
+} rb200_box_flux_report;
+
+/* Cancellation predicate with the stage it is asked at (nonzero cancels). */
+typedef int (*rb200_box_flux_cancel_fn)(void* ctx, int stage);
+
+typedef struct rb200_box_flux rb200_box_flux;
+
+/* BoxFluxWorkspace::new (src/box_flux.rs:132-186): limit covers 56 bytes per
+ * cell, as the reference's (a pressure workspace and one f64 cell array);
+ * `error` (optional) receives InvalidMass / BufferLimit. */
+RB200_API int rb200_box_flux_create(const rb200_grid* grid, double density, uint64_t limit, int method, int device,
+                                    rb200_box_flux** out, rb200_box_flux_report* error);
+RB200_API void rb200_box_flux_destroy(rb200_box_flux* workspace);
+RB200_API uint64_t rb200_box_flux_allocated_bytes(const rb200_box_flux* workspace);
+RB200_API void* rb200_box_flux_stream(rb200_box_flux* workspace);
+/* BoxFluxWorkspace::project (src/box_flux.rs:213-397) on device face arrays
+ * (old and out, lengths in elements). Inputs are never written; the output is
+ * written from the first correction slice on, so a failure after that leaves
+ * it partial. The predicate is asked at BeforeSolve, between pressure
+ * iterations, once per face slice of the correction (3 nz + 1 times: the
+ * first before the device pass, the others once it is under way) and
+ * BeforeAcceptance. Ordered on the workspace's stream; returns after it. */
+RB200_API int rb200_box_flux_project_device(rb200_box_flux* workspace, const float* const old[3],
+                                            const size_t old_len[3], double dt,
+                                            const rb200_box_flux_boundary* boundary,
+                                            const rb200_settings* pressure_settings,
+                                            double actual_divergence_limit, float* const out[3],
+                                            const size_t out_len[3], rb200_box_flux_report* report,
+                                            rb200_box_flux_cancel_fn cancelled, void* ctx);
+/* The same with host arrays: the old faces are copied in and the output out
+ * (device staging allocated on the first call). */
+RB200_API int rb200_box_flux_project(rb200_box_flux* workspace, const float* const old[3], const size_t old_len[3],
+                                     double dt, const rb200_box_flux_boundary* boundary,
+                                     const rb200_settings* pressure_settings, double actual_divergence_limit,
+                                     float* const out[3], const size_t out_len[3], rb200_box_flux_report* report,
+                                     rb200_box_flux_cancel_fn cancelled, void* ctx);
+/* BoxFluxWorkspace::divergence (src/box_flux.rs:201-206, 405-434): the measured
+ * divergence of a full f32 face field (device arrays), outer samples included. */
+RB200_API int rb200_box_flux_divergence_device(rb200_box_flux* workspace, const float* const faces[3],
+                                               const size_t len[3], double* out, size_t out_len);
+/* BoxFluxWorkspace::pressure: the last pressure (host copy / device pointer). */
+RB200_API int rb200_box_flux_pressure(rb200_box_flux* workspace, double* out, size_t len);
+RB200_API const double* rb200_box_flux_pressure_device(rb200_box_flux* workspace);
+/* Average device time (CUDA events on the workspace's stream) of `launches`
+ * back-to-back repeats of the last projection's RHS pass (which = 0) or its
+ * correction pass (which = 1). */
+RB200_API int rb200_box_flux_profile(rb200_box_flux* workspace, int which, int launches, double* avg_ms);
 
 #ifdef __cplusplus
 }

@@ -36,6 +36,7 @@ DENSE3D_LIMIT = 24
 DENSE3D_ABORTED = 25
 DENSE3D_IO = 26
 LIQUID_REJECTED = 27
+BOX_FLUX_REJECTED = 28
 
 STATUS_NAMES = {
     0: "Ok", 1: "Unsupported", 2: "Execution", 3: "NonFiniteOutput", 4: "NonZeroGauge", 5: "QualityGate",
@@ -43,6 +44,7 @@ STATUS_NAMES = {
     11: "IncompatibleRhs", 12: "NonFiniteInput", 13: "NonZeroWallVelocity", 14: "ArithmeticFailure",
     15: "DivergenceLimit", 16: "CourantLimit", 17: "NoDevice", 18: "LengthMismatch",
     22: "InvalidInitialPressure", 23: "InvalidState", 24: "Limit", 25: "Aborted", 26: "Io", 27: "LiquidRejected",
+    28: "BoxFluxRejected",
 }
 
 # rb200_liquid_error: LiquidVolumeError variants (src/liquid_volume.rs:27-72)
@@ -51,6 +53,12 @@ LIQUID_ERRORS = {0: "Ok", 1: "InvalidDensity", 2: "InvalidFraction", 3: "Invalid
                  9: "LengthMismatch", 10: "NonFiniteVelocity", 11: "VersionOverflow", 12: "BufferLimit",
                  13: "CourantLimit", 14: "DivergenceLimit", 15: "FractionBounds", 16: "BalanceLimit",
                  17: "ArithmeticFailure", 18: "Cancelled", 19: "GeometryMismatch", 20: "PeriodicVelocityMismatch"}
+
+# rb200_box_flux_error: BoxFluxError's own variants (src/box_flux.rs:60-72)
+BOX_FLUX_ERRORS = {0: "Ok", 1: "InvalidBoundary", 2: "InvalidSettings", 3: "InvalidMass", 4: "BufferLimit",
+                   5: "IncompatibleFlux", 6: "Cancelled", 7: "DivergenceLimit", 8: "ArithmeticFailure"}
+# rb200_box_flux_stage: BoxFluxStage (src/box_flux.rs:53-59)
+BOX_FLUX_STAGES = ("BeforeSolve", "PressureIteration", "CorrectionSlice", "BeforeAcceptance")
 
 
 class Grid(C.Structure):
@@ -165,6 +173,22 @@ class LiquidReport(C.Structure):
                  ("error_limit", C.c_double)])
 
 
+class BoxFluxBoundary(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("version", C.c_uint64), ("outward", C.c_float * 6)]
+
+
+class BoxFluxReport(C.Structure):
+    _fields_ = ([("boundary_id", C.c_uint64), ("boundary_version", C.c_uint64), ("pressure", Report)] +
+                [(n, C.c_double) for n in ("actual_divergence_max", "net_outward_flux", "flux_rounding_budget",
+                                           "kinetic_before", "kinetic_after", "correction_energy",
+                                           "boundary_pressure_work", "divergence_residual_work",
+                                           "correction_residual_work", "budget_error")] +
+                [("error", C.c_int), ("stage", C.c_int), ("error_actual", C.c_double),
+                 ("error_limit", C.c_double), ("required", C.c_uint64), ("limit", C.c_uint64)])
+
+
+BOX_FLUX_CANCEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int)
+
 _P = C.c_void_p
 _I = C.c_int
 _D = C.c_double
@@ -263,6 +287,19 @@ SIGNATURES = {
     "rb200_carrier_liquid_report": (_I, [_P, C.POINTER(LiquidReport)]),
     "rb200_carrier_liquid_state": (_I, [_P, C.POINTER(_P), C.POINTER(LiquidStamp), C.POINTER(_D)]),
     "rb200_carrier_liquid_download": (_I, [_P, _P, _S]),
+    "rb200_box_flux_create": (_I, [C.POINTER(Grid), _D, C.c_uint64, _I, _I, C.POINTER(_P),
+                                   C.POINTER(BoxFluxReport)]),
+    "rb200_box_flux_destroy": (None, [_P]),
+    "rb200_box_flux_allocated_bytes": (C.c_uint64, [_P]),
+    "rb200_box_flux_stream": (_P, [_P]),
+    "rb200_box_flux_project_device": (_I, [_P, _P * 3, _S * 3, _D, C.POINTER(BoxFluxBoundary), C.POINTER(Settings),
+                                           _D, _P * 3, _S * 3, C.POINTER(BoxFluxReport), BOX_FLUX_CANCEL_FN, _P]),
+    "rb200_box_flux_project": (_I, [_P, _P * 3, _S * 3, _D, C.POINTER(BoxFluxBoundary), C.POINTER(Settings),
+                                    _D, _P * 3, _S * 3, C.POINTER(BoxFluxReport), BOX_FLUX_CANCEL_FN, _P]),
+    "rb200_box_flux_divergence_device": (_I, [_P, _P * 3, _S * 3, _P, _S]),
+    "rb200_box_flux_pressure": (_I, [_P, _P, _S]),
+    "rb200_box_flux_pressure_device": (_P, [_P]),
+    "rb200_box_flux_profile": (_I, [_P, _I, _I, C.POINTER(_D)]),
 }
 
 _lib = None

@@ -18,12 +18,6 @@ const char* get_error() { return g_error.c_str(); }
 
 int launch_check_finite(const double* x, int n, int* flags, cudaStream_t s);
 
-}  // namespace rb200
-
-using namespace rb200;
-
-namespace {
-
 int select_device(int device) {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -43,6 +37,12 @@ int select_device(int device) {
     if (cudaSetDevice(device) != cudaSuccess) return RB200_NO_DEVICE;
     return RB200_OK;
 }
+
+}  // namespace rb200
+
+using namespace rb200;
+
+namespace {
 
 // Flags word for the stream-ordered primitive entry points.
 struct FlagsScope {
@@ -237,6 +237,7 @@ const char* rb200_status_string(int status) {
         case RB200_DENSE3D_ABORTED: return "dense3D export aborted";
         case RB200_DENSE3D_IO: return "dense3D output error";
         case RB200_LIQUID_REJECTED: return "liquid volume transport rejected the operation";
+        case RB200_BOX_FLUX_REJECTED: return "box flux projection rejected the operation";
         default: return "unknown status";
     }
 }

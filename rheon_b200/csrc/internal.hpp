@@ -17,6 +17,8 @@ namespace rb200 {
 // Thread-local message for entry points without a handle.
 void set_error(const std::string& msg);
 const char* get_error();
+// Makes `device` current after checking that it is an sm_100 part.
+int select_device(int device);
 
 #define RB200_CUDA(call)                                                                   \
     do {                                                                                   \

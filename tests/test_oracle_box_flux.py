@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from box_flux_cases import MIXED, dense_pressure, divergence, face_counts, imposed, mixed_old
 
 METHODS = [O.JACOBI_PCG_V1, O.SGS_PCG_V1]
 
@@ -20,80 +21,10 @@ def near(a, b):
     assert abs(a - b) < 2e-11 * max(abs(a), abs(b), 1.0), (a, b)
 
 
-def face_counts(counts, axis):
-    fc = list(counts)
-    fc[axis] += 1
-    return fc
-
-
-def imposed(counts, old, outward):
-    v = [o.copy() for o in old]
-    for d in range(3):
-        fc = face_counts(counts, d)
-        arr = v[d].reshape(fc[2], fc[1], fc[0])
-        lo = [slice(None)] * 3
-        hi = [slice(None)] * 3
-        lo[2 - d] = 0
-        hi[2 - d] = counts[d]
-        arr[tuple(lo)] = np.float32(-outward[d][0]) if outward[d][0] != 0 else np.float32(0.0)
-        arr[tuple(hi)] = np.float32(outward[d][1]) if outward[d][1] != 0 else np.float32(0.0)
-    return v
-
-
-def divergence(counts, spacing, v):
-    out = np.zeros(int(np.prod(counts)))
-    for k in range(counts[2]):
-        for j in range(counts[1]):
-            for i in range(counts[0]):
-                val = 0.0
-                for d in range(3):
-                    fc = face_counts(counts, d)
-                    p = [i, j, k]
-                    q = list(p)
-                    q[d] += 1
-                    lo = p[0] + fc[0] * (p[1] + fc[1] * p[2])
-                    hi = q[0] + fc[0] * (q[1] + fc[1] * q[2])
-                    val += (float(v[d][hi]) - float(v[d][lo])) / spacing[d]
-                out[i + counts[0] * (j + counts[1] * k)] = val
-    return out
-
-
-def dense_pressure(counts, spacing, old, outward, rho, dt):
-    """The gauge-eliminated dense solve of tests/box_flux_contract.rs:167-207."""
-    n = int(np.prod(counts))
-    h = spacing
-    area = [h[1] * h[2], h[0] * h[2], h[0] * h[1]]
-    m = np.zeros((n, n))
-    for k in range(counts[2]):
-        for j in range(counts[1]):
-            for i in range(counts[0]):
-                p = [i, j, k]
-                row = i + counts[0] * (j + counts[1] * k)
-                for d in range(3):
-                    if p[d] + 1 < counts[d]:
-                        q = list(p)
-                        q[d] += 1
-                        col = q[0] + counts[0] * (q[1] + counts[1] * q[2])
-                        wgt = area[d] / (rho * h[d])
-                        m[row, row] += wgt
-                        m[col, col] += wgt
-                        m[row, col] -= wgt
-                        m[col, row] -= wgt
-    vol = h[0] * h[1] * h[2]
-    rhs = -vol * divergence(counts, spacing, imposed(counts, old, outward)) / dt
-    p = np.zeros(n)
-    p[1:] = np.linalg.solve(m[1:, 1:], rhs[1:])
-    return p
-
-
 def mixed():
-    counts, spacing = (3, 2, 1), (0.5, 1.0, 2.0)
-    g = O.grid(counts, spacing, (-1.0, 2.0, 0.0))
-    old = []
-    for d in range(3):
-        m = O.face_len(g, d)
-        old.append(np.array([((i * 3 + d) % 7) * 0.13 - 0.2 for i in range(m)], np.float32))
-    return counts, spacing, g, old, [[-0.375, 0.0], [0.0, 0.5], [0.0, 0.0]]
+    c = MIXED
+    g = O.grid(c["counts"], c["spacing"], c["origin"])
+    return c["counts"], c["spacing"], g, mixed_old(c["counts"]), c["outward"]
 
 
 @pytest.mark.parametrize("method", METHODS)
@@ -204,3 +135,48 @@ def test_divergence_gate_and_iteration_budget():
                                        out=out0)
     assert st == O.ITERATION_LIMIT and r["iterations"] == 0
     assert all(np.array_equal(a, b) for a, b in zip(out, out0))
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_singleton_flow(method):
+    """box_flux_contract.rs:451-482"""
+    g = O.grid((1, 1, 1), (0.5, 1.0, 2.0))
+    old = [np.zeros(O.face_len(g, d), np.float32) for d in range(3)]
+    st, out, p, r = O.box_flux_project(g, 1.0, method, old, 0.25, [[-0.5, 0.5], [0.0, 0.0], [0.0, 0.0]], settings(),
+                                       1e-5)
+    assert st == 0 and r["iterations"] == 0 and r["actual_divergence_max"] == 0.0
+    assert list(p) == [0.0] and r["kinetic_before"] == 0.0 and r["kinetic_after"] == 0.0
+    assert out[0][0] == 0.5 and out[0][1] == 0.5
+
+
+def test_nonzero_flux_cannot_underflow_out_of_the_gate():
+    """box_flux_contract.rs:539-560"""
+    g = O.grid((1, 1, 1), (1e100, 1e-150, 1e-150))
+    old = [np.zeros(O.face_len(g, d), np.float32) for d in range(3)]
+    out0 = [np.full(O.face_len(g, d), -777.0, np.float32) for d in range(3)]
+    st, out, _, _ = O.box_flux_project(g, 1e-100, O.JACOBI_PCG_V1, old, 1.0, [[1e-30, 0.0], [0.0, 0.0], [0.0, 0.0]],
+                                       settings(), 1e-5, out=out0)
+    assert st == 14
+    assert all(np.array_equal(a, b) for a, b in zip(out, out0))
+
+
+def test_shared_numpy_restatement_matches_the_oracle():
+    """The numpy correction and divergence used by the device tests reproduce the oracle bit for bit."""
+    from box_flux_cases import correct_from_pressure, work_terms
+    import math
+    counts, spacing = (7, 5, 4), (0.5, 0.25, 0.75)
+    g = O.grid(counts, spacing)
+    rng = np.random.default_rng(3)
+    old = [rng.uniform(-1, 1, O.face_len(g, d)).astype(np.float32) for d in range(3)]
+    bc = [[-0.25, 0.25], [0.5, -0.5], [0.0, 0.0]]
+    st, out, p, r = O.box_flux_project(g, 1.25, O.JACOBI_PCG_V1, old, 0.1, bc, settings(), 1e-3)
+    assert st == 0
+    again = correct_from_pressure(counts, spacing, 1.25, old, p, 0.1, bc)
+    for d in range(3):
+        assert np.array_equal(again[d].view(np.uint32), out[d].view(np.uint32))
+    terms, div = work_terms(counts, spacing, 1.25, old, out, p, 0.1, bc)
+    assert np.max(np.abs(div)) == r["actual_divergence_max"]
+    for name, t in terms.items():
+        exact = math.fsum(t)
+        scale = math.fsum(np.abs(t)) + 1e-300
+        assert abs(r[name] - exact) <= 1e-13 * scale, name
