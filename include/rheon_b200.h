@@ -761,6 +761,9 @@ RB200_API const double* rb200_box_flux_pressure_device(rb200_box_flux* workspace
  * back-to-back repeats of the last projection's RHS pass (which = 0) or its
  * correction pass (which = 1). */
 RB200_API int rb200_box_flux_profile(rb200_box_flux* workspace, int which, int launches, double* avg_ms);
+/* Device times (CUDA events on the workspace's stream) of the RHS pass and the
+ * correction pass inside the last projection that reached them (-1: not run). */
+RB200_API int rb200_box_flux_last_pass_ms(rb200_box_flux* workspace, double* rhs_ms, double* correct_ms);
 
 #ifdef __cplusplus
 }

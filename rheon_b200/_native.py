@@ -300,6 +300,7 @@ SIGNATURES = {
     "rb200_box_flux_pressure": (_I, [_P, _P, _S]),
     "rb200_box_flux_pressure_device": (_P, [_P]),
     "rb200_box_flux_profile": (_I, [_P, _I, _I, C.POINTER(_D)]),
+    "rb200_box_flux_last_pass_ms": (_I, [_P, C.POINTER(_D), C.POINTER(_D)]),
 }
 
 _lib = None

@@ -271,6 +271,14 @@ class BoxFluxWorkspace:
             raise _error(st, r, inv)
         return BoxFluxReport.from_c(r)
 
+    def last_pass_ms(self):
+        """(RHS pass, correction pass) device milliseconds inside the last projection (-1: not run)."""
+        a, b = C.c_double(), C.c_double()
+        st = lib().rb200_box_flux_last_pass_ms(self._h, C.byref(a), C.byref(b))
+        if st != N.OK:
+            raise _error(st, N.BoxFluxReport())
+        return a.value, b.value
+
     def profile(self, which: int, launches: int = 20) -> float:
         """Average device milliseconds of the last projection's RHS (0) or correction (1) pass."""
         ms = C.c_double()

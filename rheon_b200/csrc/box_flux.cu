@@ -14,9 +14,12 @@
 //                 boundary and residual work and the divergence maximum in the
 //                 same pass (:297-362).
 // Every per-face and per-cell term is rounded exactly as the reference rounds
-// it (the library is built without multiply-add contraction); the reference
-// adds the terms serially, the device adds the same rounded terms in
-// double-double and rounds once.
+// it (the library is built without multiply-add contraction; quotients by the
+// spacing and by dt are correctly rounded through div_diag). The reference
+// adds the terms serially; the device adds each thread's few terms in double
+// and combines the threads' partials in double-double, which is at least as
+// accurate as the serial sum.
+#include <algorithm>
 #include <cmath>
 #include <limits>
 #include <memory>
@@ -34,18 +37,49 @@ namespace {
 constexpr int BF_SUMS = 6;
 constexpr int BF_SCALARS = BF_SUMS + 1;  // + max |divergence|
 
+// Exact floor(c / d) for 0 <= c < 2^31 by one multiply and shift
+// (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", 1994, the round-up method): with l = ceil(log2 d) and
+// m = floor(2^(31+l) / d) + 1, 2^(31+l) < m d <= 2^(31+l) + 2^l, so
+// floor(c m / 2^(31+l)) = floor(c / d); c m < 2^63.
+struct FastDiv {
+    unsigned long long m;
+    int shift;
+};
+
+FastDiv make_fastdiv(unsigned d) {
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    return FastDiv{(1ull << (31 + l)) / d + 1, 31 + l};
+}
+
+__device__ __forceinline__ int fast_div(int c, const FastDiv& f) {
+    return int((unsigned long long)(unsigned)c * f.m >> f.shift);
+}
+
 struct BfConst {
     float side[3][2];    // PrescribedBoxFlux::component(d, upper) (:36-45)
     double q[3][2];      // area_d * f64(outward) of each side (:342-349)
     double dt;
+    double rdt;          // RN(1/dt) for div_diag, or 0 where it may not be used
+    double rh[3];        // RN(1/h_d) likewise
     double dt_factor[3]; // dt * (1 / (rho h_d)), the reference's left-to-right product
     double dt_area[3];   // dt * area_d
     double mass;         // rho * cell volume
     double half_mass;    // 0.5 * mass
+    FastDiv div_x, div_xy; // cell -> (cell / n0, cell / (n0 n1))
 };
 
 __device__ __forceinline__ int face_stride(const GridDev& g, int a) {
     return a == 0 ? 1 : (a == 1 ? g.fc[1][0] : g.fc[2][0] * g.fc[2][1]);
+}
+
+// (i, j, k) of a cell without hardware division.
+__device__ __forceinline__ void cell_ijk(const GridDev& g, const BfConst& c, int cell, int (&ijk)[3]) {
+    const int row = fast_div(cell, c.div_x);
+    ijk[2] = fast_div(cell, c.div_xy);
+    ijk[0] = cell - row * g.n[0];
+    ijk[1] = row - ijk[2] * g.n[1];
 }
 
 // validate(old) (:397-404) and the imposed RHS (:263-290). Each face is the
@@ -56,7 +90,8 @@ __global__ void __launch_bounds__(EW_THREADS) k_bf_rhs(GridDev g, BfConst c, con
     const float* f3[3] = {u, v, w};
     int local = 0;
     for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < g.cells; cell += gridDim.x * blockDim.x) {
-        const int ijk[3] = {cell % g.n[0], (cell / g.n[0]) % g.n[1], cell / (g.n[0] * g.n[1])};
+        int ijk[3];
+        cell_ijk(g, c, cell, ijk);
         double flux = 0.0;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
@@ -72,7 +107,7 @@ __global__ void __launch_bounds__(EW_THREADS) k_bf_rhs(GridDev g, BfConst c, con
             }
             flux += g.area[a] * (double(lo) - double(hi));
         }
-        const double r = flux / c.dt;
+        const double r = div_diag(flux, c.dt, c.rdt);
         if (!isfinite(r)) local |= VF_ARITH;
         out[cell] = r;
     }
@@ -80,7 +115,7 @@ __global__ void __launch_bounds__(EW_THREADS) k_bf_rhs(GridDev g, BfConst c, con
 }
 
 // Correction, stored-field divergence and the work terms (:297-362).
-__global__ void __launch_bounds__(EW_THREADS) k_bf_correct(GridDev g, BfConst c, const double* __restrict__ p,
+__global__ void __launch_bounds__(EW_THREADS, 4) k_bf_correct(GridDev g, BfConst c, const double* __restrict__ p,
                                                            const float* __restrict__ iu, const float* __restrict__ iv,
                                                            const float* __restrict__ iw, float* __restrict__ ou,
                                                            float* __restrict__ ov, float* __restrict__ ow,
@@ -89,44 +124,59 @@ __global__ void __launch_bounds__(EW_THREADS) k_bf_correct(GridDev g, BfConst c,
     const float* in[3] = {iu, iv, iw};
     float* out[3] = {ou, ov, ow};
     const int s[3] = {1, g.n[0], g.n[0] * g.n[1]};
-    dd sums[BF_SUMS];
+    // Each thread adds its own few terms in plain double (a handful of cells
+    // per thread: an error of a few ulps of its partial's magnitude sum);
+    // the partials are combined in double-double.
+    double acc[BF_SUMS];
 #pragma unroll
-    for (int q = 0; q < BF_SUMS; ++q) sums[q] = dd{0.0, 0.0};
+    for (int q = 0; q < BF_SUMS; ++q) acc[q] = 0.0;
     double mx[1] = {0.0};
     int local = 0;
     for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < g.cells; cell += gridDim.x * blockDim.x) {
-        const int ijk[3] = {cell % g.n[0], (cell / g.n[0]) % g.n[1], cell / (g.n[0] * g.n[1])};
+        int ijk[3];
+        cell_ijk(g, c, cell, ijk);
+        // gather first (every load unconditional, at an in-range index), so
+        // that all of a cell's loads are in flight together
         const double pc = p[cell];
+        double pl[3], pu[3];
+        float fl[3], fh[3];
+        int flo[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            flo[a] = face_idx(g, a, ijk[0], ijk[1], ijk[2]);
+            pl[a] = p[ijk[a] > 0 ? cell - s[a] : cell];
+            pu[a] = p[ijk[a] + 1 < g.n[a] ? cell + s[a] : cell];
+            fl[a] = in[a][flo[a]];
+            fh[a] = in[a][flo[a] + face_stride(g, a)];
+        }
         double lo[3], hi[3];
         double q = 0.0;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const int flo = face_idx(g, a, ijk[0], ijk[1], ijk[2]);
-            const int fhi = flo + face_stride(g, a);
             float vlo;
             if (ijk[a] == 0) {
                 vlo = c.side[a][0];
             } else {
-                const double difference = pc - p[cell - s[a]];
-                const double uo = double(in[a][flo]);
+                const double difference = pc - pl[a];
+                const double uo = double(fl[a]);
                 const double value = uo - c.dt_factor[a] * difference;
                 if (!isfinite(value) || fabs(value) > double(kF32Max)) local |= VF_ARITH;
                 vlo = float(value);
                 const double vv = double(vlo);
                 const double delta = vv - uo;
-                sums[0] = dd_add1(sums[0], c.half_mass * uo * uo);
-                sums[1] = dd_add1(sums[1], c.half_mass * vv * vv);
-                sums[2] = dd_add1(sums[2], c.half_mass * delta * delta);
-                sums[3] = dd_add1(sums[3], (c.mass * delta + c.dt_area[a] * difference) * vv);
+                acc[0] += c.half_mass * uo * uo;
+                acc[1] += c.half_mass * vv * vv;
+                acc[2] += c.half_mass * delta * delta;
+                acc[3] += (c.mass * delta + c.dt_area[a] * difference) * vv;
             }
-            out[a][flo] = vlo;
+            out[a][flo[a]] = vlo;
             float vhi;
             if (ijk[a] + 1 == g.n[a]) {
                 vhi = c.side[a][1];
-                out[a][fhi] = vhi;
+                out[a][flo[a] + face_stride(g, a)] = vhi;
             } else {
                 // the upper neighbour's own corrected value, recomputed
-                vhi = float(double(in[a][fhi]) - c.dt_factor[a] * (p[cell + s[a]] - pc));
+                vhi = float(double(fh[a]) - c.dt_factor[a] * (pu[a] - pc));
             }
             lo[a] = double(vlo);
             hi[a] = double(vhi);
@@ -135,16 +185,19 @@ __global__ void __launch_bounds__(EW_THREADS) k_bf_correct(GridDev g, BfConst c,
         }
         // divergence() (:405-434): value = 0; value += (hi - lo)/h_d
         double value = 0.0;
-        value += (hi[0] - lo[0]) / g.h[0];
-        value += (hi[1] - lo[1]) / g.h[1];
-        value += (hi[2] - lo[2]) / g.h[2];
+        value += div_diag(hi[0] - lo[0], g.h[0], c.rh[0]);
+        value += div_diag(hi[1] - lo[1], g.h[1], c.rh[1]);
+        value += div_diag(hi[2] - lo[2], g.h[2], c.rh[2]);
         if (!isfinite(value)) local |= VF_ARITH;
         mx[0] = fmax(mx[0], fabs(value));
         const double dtp = c.dt * pc;
-        sums[4] = dd_add1(sums[4], -(dtp * q));
-        sums[5] = dd_add1(sums[5], dtp * g.volume * value);
+        acc[4] -= dtp * q;
+        acc[5] += dtp * g.volume * value;
     }
     if (local) atomicOr(flags, local);
+    dd sums[BF_SUMS];
+#pragma unroll
+    for (int q = 0; q < BF_SUMS; ++q) sums[q] = dd{acc[q], 0.0};
     block_reduce<BF_SUMS, 1>(sm, sums, mx);
     if (publish_and_check_last<BF_SUMS, 1>(part, blockIdx.x, gridDim.x, sums, mx)) {
         fold_partials<BF_SUMS, 1>(part, gridDim.x, sm, sums, mx);
@@ -157,21 +210,22 @@ __global__ void __launch_bounds__(EW_THREADS) k_bf_correct(GridDev g, BfConst c,
 }
 
 // BoxFluxWorkspace::divergence (:201-206): validate, then divergence().
-__global__ void __launch_bounds__(EW_THREADS) k_bf_divergence(GridDev g, const float* __restrict__ u,
+__global__ void __launch_bounds__(EW_THREADS) k_bf_divergence(GridDev g, BfConst c, const float* __restrict__ u,
                                                               const float* __restrict__ v,
                                                               const float* __restrict__ w, double* __restrict__ out,
                                                               int* flags) {
     const float* f3[3] = {u, v, w};
     int local = 0;
     for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < g.cells; cell += gridDim.x * blockDim.x) {
-        const int ijk[3] = {cell % g.n[0], (cell / g.n[0]) % g.n[1], cell / (g.n[0] * g.n[1])};
+        int ijk[3];
+        cell_ijk(g, c, cell, ijk);
         double value = 0.0;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const int flo = face_idx(g, a, ijk[0], ijk[1], ijk[2]);
             const float lo = f3[a][flo], hi = f3[a][flo + face_stride(g, a)];
             if (!isfinite(lo) || (ijk[a] + 1 == g.n[a] && !isfinite(hi))) local |= VF_NONFINITE;
-            value += (double(hi) - double(lo)) / g.h[a];
+            value += div_diag(double(hi) - double(lo), g.h[a], c.rh[a]);
         }
         if (!isfinite(value)) local |= VF_ARITH;
         out[cell] = value;
@@ -238,7 +292,8 @@ struct rb200_box_flux {
     double side_area[3] = {0.0, 0.0, 0.0};
     uint64_t accounted = 0;
     PcgSolver solver;
-    int nb = 0;
+    int nb = 0;      // blocks of k_bf_correct: one wave of resident blocks at most
+    int nb_rhs = 0;  // blocks of k_bf_rhs and k_bf_divergence, likewise
     // device: flags (int), scalars [BF_SCALARS], partials [nb][2*BF_SUMS+1], ticket
     char* d_buf = nullptr;
     int* d_flags = nullptr;
@@ -254,6 +309,10 @@ struct rb200_box_flux {
     const float* last_in[3] = {};
     float* last_out[3] = {};
     bool has_last = false;
+    // events around the RHS pass (0, 1) and the correction pass (2, 3) of the
+    // last projection that reached them
+    cudaEvent_t ev[4] = {};
+    bool timed_rhs = false, timed_correct = false;
 
     ~rb200_box_flux() {
         if (stream) {
@@ -261,6 +320,8 @@ struct rb200_box_flux {
             cudaStreamSynchronize(stream);
             cudaStreamDestroy(stream);
         }
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
         cudaFree(d_buf);
         cudaFree(staging);
         cudaFreeHost(h_buf);
@@ -270,6 +331,9 @@ struct rb200_box_flux {
 };
 
 namespace {
+
+// RN(1/x) where div_diag may use it (2^-500 < x < 2^500), else 0 (divide).
+double recip_for_div(double x) { return (x > 0x1p-500 && x < 0x1p500) ? 1.0 / x : 0.0; }
 
 BfConst make_const(const rb200_box_flux* B, const float outward[6], double dt) {
     const GridDev& g = B->g;
@@ -283,8 +347,12 @@ BfConst make_const(const rb200_box_flux* B, const float outward[6], double dt) {
         c.dt_area[d] = dt * g.area[d];
     }
     c.dt = dt;
+    c.rdt = recip_for_div(dt);
+    for (int d = 0; d < 3; ++d) c.rh[d] = recip_for_div(g.h[d]);
     c.mass = B->mass;
     c.half_mass = 0.5 * B->mass;
+    c.div_x = make_fastdiv(unsigned(g.n[0]));
+    c.div_xy = make_fastdiv(unsigned(g.n[0]) * unsigned(g.n[1]));
     return c;
 }
 
@@ -368,8 +436,12 @@ int project_impl(rb200_box_flux* B, const float* const old[3], const size_t old_
     }
     const BfConst c = make_const(B, bc->outward, dt);
     RB200_CUDA(cudaMemsetAsync(B->d_flags, 0, sizeof(int), B->stream));
-    k_bf_rhs<<<B->nb, EW_THREADS, 0, B->stream>>>(g, c, src[0], src[1], src[2], B->solver.b(), B->d_flags);
+    RB200_CUDA(cudaEventRecord(B->ev[0], B->stream));
+    k_bf_rhs<<<B->nb_rhs, EW_THREADS, 0, B->stream>>>(g, c, src[0], src[1], src[2], B->solver.b(), B->d_flags);
     RB200_CUDA(cudaGetLastError());
+    RB200_CUDA(cudaEventRecord(B->ev[1], B->stream));
+    B->timed_rhs = true;
+    B->timed_correct = false;
     int flags = 0;
     int rc = read_back(B, false, &flags);
     if (rc) return rc;
@@ -409,9 +481,12 @@ int project_impl(rb200_box_flux* B, const float* const old[3], const size_t old_
         return reject(rep, RB200_BOX_FLUX_CANCELLED);
     }
     RB200_CUDA(cudaMemsetAsync(B->d_flags, 0, sizeof(int), B->stream));
+    RB200_CUDA(cudaEventRecord(B->ev[2], B->stream));
     k_bf_correct<<<B->nb, EW_THREADS, 0, B->stream>>>(g, c, B->solver.p(), src[0], src[1], src[2], dst[0], dst[1],
                                                       dst[2], B->part, B->d_scalars, B->d_flags);
     RB200_CUDA(cudaGetLastError());
+    RB200_CUDA(cudaEventRecord(B->ev[3], B->stream));
+    B->timed_correct = true;
     B->last = c;
     for (int a = 0; a < 3; ++a) {
         B->last_in[a] = src[a];
@@ -506,12 +581,18 @@ int rb200_box_flux_create(const rb200_grid* grid, double density, uint64_t limit
     B->accounted = required;
     RB200_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
     if ((rc = B->solver.init(g, method, B->stream))) return rc;
-    B->nb = bf_blocks(g.cells);
+    int sms = 0, occ_correct = 0, occ_rhs = 0;
+    RB200_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    RB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_correct, k_bf_correct, EW_THREADS, 0));
+    RB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_rhs, k_bf_rhs, EW_THREADS, 0));
+    B->nb = std::min(bf_blocks(g.cells), std::max(1, sms * occ_correct));
+    B->nb_rhs = std::min(bf_blocks(g.cells), std::max(1, sms * occ_rhs));
     const size_t part_doubles = size_t(B->nb) * (2 * BF_SUMS + 1);
     const size_t bytes = 16 + BF_SCALARS * sizeof(double) + part_doubles * sizeof(double) + 16;
     RB200_CUDA(cudaMalloc(&B->d_buf, bytes));
     RB200_CUDA(cudaMemset(B->d_buf, 0, bytes));
     RB200_CUDA(cudaMallocHost(&B->h_buf, 16 + BF_SCALARS * sizeof(double)));
+    for (auto& e : B->ev) RB200_CUDA(cudaEventCreate(&e));
     B->d_flags = reinterpret_cast<int*>(B->d_buf);
     B->d_scalars = reinterpret_cast<double*>(B->d_buf + 16);
     B->part.data = B->d_scalars + BF_SCALARS;
@@ -562,7 +643,10 @@ int rb200_box_flux_divergence_device(rb200_box_flux* B, const float* const faces
         return rc ? rc : RB200_LENGTH_MISMATCH;
     }
     RB200_CUDA(cudaMemsetAsync(B->d_flags, 0, sizeof(int), B->stream));
-    k_bf_divergence<<<B->nb, EW_THREADS, 0, B->stream>>>(B->g, faces[0], faces[1], faces[2], out, B->d_flags);
+    const float zero[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    const BfConst c = make_const(B, zero, 1.0);
+    k_bf_divergence<<<B->nb_rhs, EW_THREADS, 0, B->stream>>>(B->g, c, faces[0], faces[1], faces[2], out,
+                                                            B->d_flags);
     RB200_CUDA(cudaGetLastError());
     int flags = 0;
     int rc = read_back(B, false, &flags);
@@ -583,6 +667,27 @@ int rb200_box_flux_pressure(rb200_box_flux* B, double* out, size_t len) {
 
 const double* rb200_box_flux_pressure_device(rb200_box_flux* B) { return B ? B->solver.p() : nullptr; }
 
+// Device times (CUDA events on the workspace's stream) of the RHS pass and
+// the correction pass inside the last projection that reached them; a pass
+// that did not run reports -1.
+int rb200_box_flux_last_pass_ms(rb200_box_flux* B, double* rhs_ms, double* correct_ms) {
+    if (!B || !rhs_ms || !correct_ms) return RB200_INVALID_ARGUMENT;
+    cudaSetDevice(B->device);
+    *rhs_ms = *correct_ms = -1.0;
+    float ms = 0.0f;
+    if (B->timed_rhs) {
+        RB200_CUDA(cudaEventSynchronize(B->ev[1]));
+        RB200_CUDA(cudaEventElapsedTime(&ms, B->ev[0], B->ev[1]));
+        *rhs_ms = ms;
+    }
+    if (B->timed_correct) {
+        RB200_CUDA(cudaEventSynchronize(B->ev[3]));
+        RB200_CUDA(cudaEventElapsedTime(&ms, B->ev[2], B->ev[3]));
+        *correct_ms = ms;
+    }
+    return RB200_OK;
+}
+
 // Average device time of `launches` back-to-back launches of the last
 // projection's RHS pass (which = 0) or correction pass (which = 1), CUDA
 // events on the workspace's stream. Both passes are idempotent.
@@ -601,7 +706,7 @@ int rb200_box_flux_profile(rb200_box_flux* B, int which, int launches, double* a
     cudaEventRecord(e0, B->stream);
     for (int i = 0; i < launches; ++i) {
         if (which == 0)
-            k_bf_rhs<<<B->nb, EW_THREADS, 0, B->stream>>>(B->g, c, B->last_in[0], B->last_in[1], B->last_in[2],
+            k_bf_rhs<<<B->nb_rhs, EW_THREADS, 0, B->stream>>>(B->g, c, B->last_in[0], B->last_in[1], B->last_in[2],
                                                           B->solver.scratch(), B->d_flags);
         else
             k_bf_correct<<<B->nb, EW_THREADS, 0, B->stream>>>(B->g, c, B->solver.p(), B->last_in[0], B->last_in[1],

@@ -8,9 +8,9 @@ cases follow tests/box_flux_contract.rs. Tolerances:
 - pressure: 1e-12 relative to the oracle's for the two reference methods
   (per-iteration parity of the device solve), the contract's 2e-11 `near` for
   the hand and dense-solve cases;
-- energy terms: the device adds the reference's rounded terms in
-  double-double, so each is within 1e-13 of the sum of the terms' magnitudes
-  of the exactly rounded sum (math.fsum). Against the oracle's serial sums:
+- energy terms: the device adds the reference's rounded terms (a few per
+  thread in double, the partials in double-double), so each is within 1e-13
+  of the sum of the terms' magnitudes of the exactly rounded sum (math.fsum). Against the oracle's serial sums:
   1e-9 of that magnitude for the energies and the boundary work, 1e-2 for the
   two residual works, whose terms sit at the f32 rounding level.
 """
