@@ -33,6 +33,8 @@ INCOMPATIBLE_RHS = 11
 NONFINITE_INPUT = 12
 NONZERO_WALL_VELOCITY = 13
 ARITHMETIC_FAILURE = 14
+DIVERGENCE_LIMIT = 15
+COURANT_LIMIT = 16
 LENGTH_MISMATCH = 18
 INVALID_GEOMETRY = 19
 INVALID_TIME_STEP = 20
@@ -138,6 +140,40 @@ class BoxFluxReport(C.Structure):
         "budget_error")]
 
 
+class SmokeSource(C.Structure):
+    _fields_ = [("lower", C.c_double * 3), ("upper", C.c_double * 3), ("tracer_rate", C.c_double),
+                ("vertical_acceleration", C.c_double)]
+
+
+class BodyForce(C.Structure):
+    _fields_ = [("value", C.c_double * 3), ("units", C.c_int), ("has_region", C.c_int),
+                ("lower", C.c_double * 3), ("upper", C.c_double * 3)]
+
+
+class SimConfig(C.Structure):
+    _fields_ = [("density", C.c_double), ("method", C.c_int), ("pressure", Settings),
+                ("actual_divergence_limit", C.c_double), ("max_courant", C.c_double)]
+
+
+class SimState(C.Structure):
+    _fields_ = [("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p), ("tracer", C.c_void_p),
+                ("time", C.c_double), ("generation", C.c_uint64)]
+
+
+SIM_WORK = ("kinetic_old", "kinetic_after_advection", "kinetic_after_smoke_force", "kinetic_before_projection",
+            "kinetic_accepted", "advection_change", "smoke_force_work", "external_force_work", "budget_error",
+            "boundary_volume_imbalance", "tracer_old_integral", "tracer_transport_change", "tracer_source_change")
+
+
+class SimReport(C.Structure):
+    _fields_ = ([("dt", C.c_double), ("time", C.c_double), ("generation", C.c_uint64), ("pressure", Report)] +
+                [(n, C.c_double) for n in ("actual_divergence_max", "courant", "tracer_integral", "kinetic_energy")] +
+                [("has_forces", C.c_int)] +
+                [(n, C.c_double) for n in ("force_kinetic_before", "force_kinetic_after", "force_applied_work")] +
+                [("projection", BoxFluxReport)] + [(n, C.c_double) for n in SIM_WORK] +
+                [("error", C.c_int), ("error_actual", C.c_double), ("error_limit", C.c_double)])
+
+
 def build() -> str:
     """Compile the oracle with its Makefile (idempotent)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
@@ -202,6 +238,8 @@ def _declare(L):
                                        C.POINTER(BoxFluxReport)]
     L.orc_dense3d_frame_text.argtypes = [C.POINTER(Grid), C.POINTER(Dense3dFrame), _P, _P, _P, _P, _P, _P,
                                          C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
+    L.orc_sim_step.argtypes = [C.POINTER(Grid), C.POINTER(SimConfig), C.POINTER(SimState), C.c_double,
+                               C.POINTER(SmokeSource), C.POINTER(BodyForce), C.c_size_t, _P, C.POINTER(SimReport)]
     for name in ("orc_carrier_step_seeded_f32", "orc_carrier_step_seeded_f64"):
         getattr(L, name).argtypes = [C.POINTER(Grid), C.POINTER(StepParams), _P, _P, _P, _P, _P, _P,
                                      C.POINTER(StepReport)]
@@ -478,3 +516,46 @@ def box_flux_project(g, density, method, faces, dt, outward, s: Settings, actual
     d = {n: getattr(rep, n) for n, _ in BoxFluxReport._fields_ if n not in ("pressure",)}
     d["iterations"] = rep.pressure.iterations
     return st, outs, p, d
+
+
+class Simulation:
+    """The step owner of the oracle (Simulation::step / step_with_forces /
+    step_with_box_flux, src/simulation.rs:393-581): f32 faces and tracer,
+    updated by step() only when it succeeds."""
+
+    def __init__(self, g, density, method, pressure: Settings, actual_divergence_limit, max_courant, faces=None,
+                 tracer=None):
+        self.g = g
+        self.config = SimConfig(density, method, pressure, actual_divergence_limit, max_courant)
+        self.faces = [np.zeros(face_len(g, d), np.float32) if faces is None else np.array(faces[d], np.float32)
+                      for d in range(3)]
+        self.tracer = np.zeros(cell_len(g), np.float32) if tracer is None else np.array(tracer, np.float32)
+        self.time = 0.0
+        self.generation = 0
+
+    def step(self, requested_dt, source=None, forces=(), outward=None):
+        """(status, report). source: dict(lower, upper, tracer_rate, vertical_acceleration);
+        forces: dicts (value, units 0/1, region=(lower, upper) or None); outward: [[lo, hi]] per axis."""
+        st_ = SimState(_ptr(self.faces[0]), _ptr(self.faces[1]), _ptr(self.faces[2]), _ptr(self.tracer),
+                       self.time, self.generation)
+        src = None
+        if source is not None:
+            src = SmokeSource((C.c_double * 3)(*source["lower"]), (C.c_double * 3)(*source["upper"]),
+                              source["tracer_rate"], source["vertical_acceleration"])
+        fa = (BodyForce * max(1, len(forces)))()
+        for i, f in enumerate(forces):
+            fa[i].value = (C.c_double * 3)(*f["value"])
+            fa[i].units = int(f.get("units", 0))
+            region = f.get("region")
+            fa[i].has_region = 1 if region is not None else 0
+            if region is not None:
+                fa[i].lower = (C.c_double * 3)(*region[0])
+                fa[i].upper = (C.c_double * 3)(*region[1])
+        ow = None if outward is None else (C.c_float * 6)(*[float(x) for pair in outward for x in pair])
+        rep = SimReport()
+        st = lib().orc_sim_step(C.byref(self.g), C.byref(self.config), C.byref(st_), requested_dt,
+                                C.byref(src) if src is not None else None, fa, len(forces), ow, C.byref(rep))
+        if st == 0:
+            self.time = st_.time
+            self.generation = st_.generation
+        return st, rep

@@ -289,6 +289,61 @@ int orc_box_flux_project(const orc_grid* g, double density, int method, const fl
                          double actual_divergence_limit, float* out_u, float* out_v, float* out_w,
                          double* pressure_out, orc_box_flux_report* rep);
 
+/* The step owner with its forcing and boundary domains
+ * (Simulation::step / step_with_forces / step_with_box_flux,
+ * src/simulation.rs:393-581, prepare_impl :812-1403) on f32 faces and an f32
+ * tracer: dt policy with the smoke and body-force accelerations, advection,
+ * the smoke source's Y-face force (apply_force :1449-1472), the body forces
+ * (src/forces.rs:144-212), the sealed projection or the box-flux projection
+ * (outward != NULL), the divergence and Courant gates, tracer advection, the
+ * smoke source's tracer (apply_source :1473-1496), the tracer range check and
+ * the box-flux step's work ledger (src/box_flux_step.rs). The state is
+ * updated only on success. Returns 0, an orc status, or 29 with
+ * report.error = 1 InvalidSource, 2 InvalidForce, 3 TimeResolution. */
+typedef struct orc_smoke_source {
+    double lower[3], upper[3];
+    double tracer_rate, vertical_acceleration;
+} orc_smoke_source;
+
+typedef struct orc_body_force {
+    double value[3];
+    int units;       /* 0 Acceleration, 1 ForceDensity */
+    int has_region;
+    double lower[3], upper[3];
+} orc_body_force;
+
+typedef struct orc_sim_config {
+    double density;
+    int method;
+    orc_settings pressure;
+    double actual_divergence_limit, max_courant;
+} orc_sim_config;
+
+typedef struct orc_sim_state {
+    float *u, *v, *w, *tracer;
+    double time;
+    uint64_t generation;
+} orc_sim_state;
+
+typedef struct orc_sim_report {
+    double dt, time;
+    uint64_t generation;
+    orc_report pressure;
+    double actual_divergence_max, courant, tracer_integral, kinetic_energy;
+    int has_forces;
+    double force_kinetic_before, force_kinetic_after, force_applied_work;
+    orc_box_flux_report projection;
+    double kinetic_old, kinetic_after_advection, kinetic_after_smoke_force, kinetic_before_projection,
+        kinetic_accepted, advection_change, smoke_force_work, external_force_work, budget_error,
+        boundary_volume_imbalance, tracer_old_integral, tracer_transport_change, tracer_source_change;
+    int error;
+    double error_actual, error_limit;
+} orc_sim_report;
+
+int orc_sim_step(const orc_grid* g, const orc_sim_config* config, orc_sim_state* state, double requested_dt,
+                 const orc_smoke_source* source, const orc_body_force* forces, size_t force_count,
+                 const float* outward, orc_sim_report* rep);
+
 #ifdef __cplusplus
 }
 #endif
