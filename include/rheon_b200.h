@@ -65,7 +65,8 @@ typedef enum rb200_status {
     RB200_DENSE3D_ABORTED = 25,      /* Dense3dError::Aborted                     */
     RB200_DENSE3D_IO = 26,           /* Dense3dError::Io                          */
     RB200_LIQUID_REJECTED = 27,      /* LiquidVolumeError: see rb200_liquid_report.error */
-    RB200_BOX_FLUX_REJECTED = 28     /* BoxFluxError's own variants: see rb200_box_flux_report.error */
+    RB200_BOX_FLUX_REJECTED = 28,    /* BoxFluxError's own variants: see rb200_box_flux_report.error */
+    RB200_SIMULATION_REJECTED = 29   /* SimulationError's own variants: see rb200_forced_step_report.error */
 } rb200_status;
 
 /* Pressure methods. JACOBI_PCG_V1 reproduces "jacobi-pcg-v1"
@@ -764,6 +765,96 @@ RB200_API int rb200_box_flux_profile(rb200_box_flux* workspace, int which, int l
 /* Device times (CUDA events on the workspace's stream) of the RHS pass and the
  * correction pass inside the last projection that reached them (-1: not run). */
 RB200_API int rb200_box_flux_last_pass_ms(rb200_box_flux* workspace, double* rhs_ms, double* correct_ms);
+
+/* ------------------------------------------------------------------ forced step
+ * The step owner with its forcing and boundary domains on the resident
+ * carrier: Simulation::step / step_with_forces / step_with_box_flux
+ * (src/simulation.rs:393-581, prepare_impl :812-1403). Host-driven: the
+ * stages run as device passes on the carrier's stream in the reference's
+ * order, with its cancellation points, and the accepted state is published
+ * only by the final commit. Needs f32 face storage and a tracer. */
+typedef struct rb200_smoke_source {      /* SmokeSource (src/simulation.rs:19-27) */
+    double lower[3];
+    double upper[3];
+    double tracer_rate;                  /* concentration per second, saturated at one */
+    double vertical_acceleration;        /* on the interior Y faces inside the box     */
+} rb200_smoke_source;
+
+typedef enum rb200_force_units { RB200_FORCE_ACCELERATION = 0, RB200_FORCE_DENSITY = 1 } rb200_force_units;
+
+typedef struct rb200_body_force {        /* BodyForce (src/forces.rs:11-45) */
+    double value[3];
+    int units;                           /* rb200_force_units                         */
+    int has_region;                      /* 0: the whole box                          */
+    double lower[3];                     /* half-open support lower <= x < upper      */
+    double upper[3];
+} rb200_body_force;
+
+/* StepStage (src/simulation.rs:28-42), the stage a cancellation is asked at. */
+typedef enum rb200_step_stage {
+    RB200_STAGE_BEFORE_ADVECTION = 0,
+    RB200_STAGE_VELOCITY_SLICE = 1,
+    RB200_STAGE_BEFORE_FORCES = 2,
+    RB200_STAGE_FORCE_SLICE = 3,
+    RB200_STAGE_VISCOSITY = 4,
+    RB200_STAGE_BEFORE_PRESSURE = 5,
+    RB200_STAGE_PRESSURE_ITERATION = 6,
+    RB200_STAGE_PROJECTION_SLICE = 7,
+    RB200_STAGE_BEFORE_PROJECTION_ACCEPTANCE = 8,
+    RB200_STAGE_BEFORE_TRACER = 9,
+    RB200_STAGE_TRACER_SLICE = 10,
+    RB200_STAGE_BEFORE_COMMIT = 11
+} rb200_step_stage;
+
+typedef int (*rb200_step_cancel_fn)(void* ctx, int stage);
+
+/* SimulationError's own variants (src/simulation.rs:55-83) under RB200_SIMULATION_REJECTED. */
+typedef enum rb200_simulation_error {
+    RB200_SIMULATION_NONE = 0,
+    RB200_SIMULATION_INVALID_SOURCE = 1,
+    RB200_SIMULATION_INVALID_FORCE = 2,
+    RB200_SIMULATION_TIME_RESOLUTION = 3,
+    RB200_SIMULATION_BOUNDARY_WORKSPACE_MISMATCH = 4,
+    RB200_SIMULATION_CANCELLED = 5        /* report.stage */
+} rb200_simulation_error;
+
+typedef struct rb200_forced_step_params {
+    double requested_dt;
+    const rb200_smoke_source* source;    /* NULL: none                                */
+    const rb200_body_force* forces;      /* force_count entries                       */
+    size_t force_count;
+    rb200_box_flux* box_flux;            /* NULL: the sealed box; else the boundary's
+                                            projection workspace (same grid, density,
+                                            method as the carrier)                    */
+    const rb200_box_flux_boundary* boundary;
+    int tracer_policy;                   /* BoxFluxTracerPolicy: 0 ClampedAppearance  */
+} rb200_forced_step_params;
+
+/* ForcedStepReport / BoxFluxStepReport (src/forces.rs:51-61,
+ * src/box_flux_step.rs:26-57) plus the error payloads. */
+typedef struct rb200_forced_step_report {
+    double dt, time;
+    uint64_t generation;
+    rb200_report pressure;
+    double actual_divergence_max, courant, tracer_integral, kinetic_energy;
+    int has_forces;                      /* ForceReport present                       */
+    int has_boundary;                    /* box-flux step: projection and work below  */
+    double force_kinetic_before, force_kinetic_after, force_applied_work;
+    rb200_box_flux_report projection;
+    double kinetic_old, kinetic_after_advection, kinetic_after_smoke_force, kinetic_before_projection,
+        kinetic_accepted, advection_change, smoke_force_work, external_force_work, budget_error,
+        boundary_volume_imbalance, tracer_old_integral, tracer_transport_change, tracer_source_change;
+    int tracer_policy;
+    int error;                           /* rb200_simulation_error                    */
+    int stage;                           /* rb200_step_stage of a cancellation        */
+    int pad;
+    double error_actual, error_limit;    /* DivergenceLimit / CourantLimit            */
+    uint64_t simulation_array_bytes, boundary_workspace_array_bytes;
+} rb200_forced_step_report;
+
+RB200_API int rb200_carrier_step_forced(rb200_carrier* carrier, const rb200_forced_step_params* params,
+                                        rb200_forced_step_report* report, rb200_step_cancel_fn cancelled,
+                                        void* ctx);
 
 #ifdef __cplusplus
 }

@@ -37,6 +37,7 @@ DENSE3D_ABORTED = 25
 DENSE3D_IO = 26
 LIQUID_REJECTED = 27
 BOX_FLUX_REJECTED = 28
+SIMULATION_REJECTED = 29
 
 STATUS_NAMES = {
     0: "Ok", 1: "Unsupported", 2: "Execution", 3: "NonFiniteOutput", 4: "NonZeroGauge", 5: "QualityGate",
@@ -44,7 +45,7 @@ STATUS_NAMES = {
     11: "IncompatibleRhs", 12: "NonFiniteInput", 13: "NonZeroWallVelocity", 14: "ArithmeticFailure",
     15: "DivergenceLimit", 16: "CourantLimit", 17: "NoDevice", 18: "LengthMismatch",
     22: "InvalidInitialPressure", 23: "InvalidState", 24: "Limit", 25: "Aborted", 26: "Io", 27: "LiquidRejected",
-    28: "BoxFluxRejected",
+    28: "BoxFluxRejected", 29: "SimulationRejected",
 }
 
 # rb200_liquid_error: LiquidVolumeError variants (src/liquid_volume.rs:27-72)
@@ -189,6 +190,48 @@ class BoxFluxReport(C.Structure):
 
 BOX_FLUX_CANCEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int)
 
+# rb200_step_stage: StepStage (src/simulation.rs:28-42)
+STEP_STAGES = ("BeforeAdvection", "VelocitySlice", "BeforeForces", "ForceSlice", "Viscosity", "BeforePressure",
+               "PressureIteration", "ProjectionSlice", "BeforeProjectionAcceptance", "BeforeTracer", "TracerSlice",
+               "BeforeCommit")
+# rb200_simulation_error: SimulationError's own variants
+SIMULATION_ERRORS = {0: "Ok", 1: "InvalidSource", 2: "InvalidForce", 3: "TimeResolution",
+                     4: "BoundaryWorkspaceMismatch", 5: "Cancelled"}
+STEP_CANCEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int)
+
+
+class SmokeSourceC(C.Structure):
+    _fields_ = [("lower", C.c_double * 3), ("upper", C.c_double * 3), ("tracer_rate", C.c_double),
+                ("vertical_acceleration", C.c_double)]
+
+
+class BodyForceC(C.Structure):
+    _fields_ = [("value", C.c_double * 3), ("units", C.c_int), ("has_region", C.c_int),
+                ("lower", C.c_double * 3), ("upper", C.c_double * 3)]
+
+
+class ForcedStepParams(C.Structure):
+    _fields_ = [("requested_dt", C.c_double), ("source", C.POINTER(SmokeSourceC)),
+                ("forces", C.POINTER(BodyForceC)), ("force_count", C.c_size_t), ("box_flux", C.c_void_p),
+                ("boundary", C.POINTER(BoxFluxBoundary)), ("tracer_policy", C.c_int)]
+
+
+FORCED_WORK = ("kinetic_old", "kinetic_after_advection", "kinetic_after_smoke_force", "kinetic_before_projection",
+               "kinetic_accepted", "advection_change", "smoke_force_work", "external_force_work", "budget_error",
+               "boundary_volume_imbalance", "tracer_old_integral", "tracer_transport_change",
+               "tracer_source_change")
+
+
+class ForcedStepReport(C.Structure):
+    _fields_ = ([("dt", C.c_double), ("time", C.c_double), ("generation", C.c_uint64), ("pressure", Report)] +
+                [(n, C.c_double) for n in ("actual_divergence_max", "courant", "tracer_integral", "kinetic_energy")] +
+                [("has_forces", C.c_int), ("has_boundary", C.c_int)] +
+                [(n, C.c_double) for n in ("force_kinetic_before", "force_kinetic_after", "force_applied_work")] +
+                [("projection", BoxFluxReport)] + [(n, C.c_double) for n in FORCED_WORK] +
+                [("tracer_policy", C.c_int), ("error", C.c_int), ("stage", C.c_int), ("pad", C.c_int),
+                 ("error_actual", C.c_double), ("error_limit", C.c_double),
+                 ("simulation_array_bytes", C.c_uint64), ("boundary_workspace_array_bytes", C.c_uint64)])
+
 _P = C.c_void_p
 _I = C.c_int
 _D = C.c_double
@@ -301,6 +344,8 @@ SIGNATURES = {
     "rb200_box_flux_pressure_device": (_P, [_P]),
     "rb200_box_flux_profile": (_I, [_P, _I, _I, C.POINTER(_D)]),
     "rb200_box_flux_last_pass_ms": (_I, [_P, C.POINTER(_D), C.POINTER(_D)]),
+    "rb200_carrier_step_forced": (_I, [_P, C.POINTER(ForcedStepParams), C.POINTER(ForcedStepReport),
+                                       STEP_CANCEL_FN, _P]),
 }
 
 _lib = None

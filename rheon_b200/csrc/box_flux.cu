@@ -287,6 +287,8 @@ struct rb200_box_flux {
     int device = 0;
     cudaStream_t stream = nullptr;
     GridDev g{};
+    rb200_grid grid{};
+    double density = 0.0;
     int method = 0;
     double mass = 0.0;
     double side_area[3] = {0.0, 0.0, 0.0};
@@ -538,6 +540,16 @@ int project_impl(rb200_box_flux* B, const float* const old[3], const size_t old_
 
 }  // namespace
 
+namespace rb200 {
+bool box_flux_matches(const rb200_box_flux* B, const rb200_grid& grid, double density, int method) {
+    if (!B || B->method != method) return false;
+    uint64_t a, b;
+    std::memcpy(&a, &B->density, 8);
+    std::memcpy(&b, &density, 8);
+    return a == b && same_grid(B->grid, grid);
+}
+}  // namespace rb200
+
 extern "C" {
 
 int rb200_box_flux_create(const rb200_grid* grid, double density, uint64_t limit, int method, int device,
@@ -575,6 +587,8 @@ int rb200_box_flux_create(const rb200_grid* grid, double density, uint64_t limit
     if (!B) return RB200_OUT_OF_MEMORY;
     B->device = device;
     B->g = g;
+    B->grid = *grid;
+    B->density = density;
     B->method = method;
     B->mass = mass;
     for (int d = 0; d < 3; ++d) B->side_area[d] = side_area[d];

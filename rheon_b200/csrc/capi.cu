@@ -238,6 +238,7 @@ const char* rb200_status_string(int status) {
         case RB200_DENSE3D_IO: return "dense3D output error";
         case RB200_LIQUID_REJECTED: return "liquid volume transport rejected the operation";
         case RB200_BOX_FLUX_REJECTED: return "box flux projection rejected the operation";
+        case RB200_SIMULATION_REJECTED: return "simulation rejected the step";
         default: return "unknown status";
     }
 }

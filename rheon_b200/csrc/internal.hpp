@@ -19,6 +19,9 @@ void set_error(const std::string& msg);
 const char* get_error();
 // Makes `device` current after checking that it is an sm_100 part.
 int select_device(int device);
+// A box-flux workspace built for this grid (bit-equal geometry), density
+// (bit-equal) and pressure method (box_flux.cu).
+bool box_flux_matches(const rb200_box_flux* workspace, const rb200_grid& grid, double density, int method);
 
 #define RB200_CUDA(call)                                                                   \
     do {                                                                                   \
