@@ -697,6 +697,7 @@ def run_box_flux(args, local, with_cpu):
                           "d2h_bytes_per_step": 4 * faces, "ms_per_projection": e2e * 1e3,
                           "matches_device_path": same}
         w.close()
+    res["box_flux_step"] = run_box_flux_step(args, local, with_cpu)
     if with_cpu:
         import oracle as O
 
@@ -712,6 +713,72 @@ def run_box_flux(args, local, with_cpu):
                                "sample": f"one full {m}^3 projection of the same workload by the oracle "
                                          f"({rep['iterations']} PCG iterations, status {st}); the per-cell cost "
                                          f"grows with n (iterations), so this overstates the CPU at {n}^3"}
+    return res
+
+
+def run_box_flux_step(args, local, with_cpu):
+    """Simulation::step_with_box_flux (src/simulation.rs:551-579) on the resident
+    carrier at n^3 on the unit cube: the random-Fourier state, a smoke source in
+    the box's centre, a uniform body force and a 0.5 m/s x through-flow, on the
+    mixed carrier (FP32 multigrid) and the f32 Jacobi-PCG carrier (rel 1e-8).
+    Wall time per step (the step is host-driven and synchronous), and the
+    oracle's step on one host core."""
+    import torch
+
+    import rheon_b200 as R
+    from rheon_b200 import simulation as SS
+    from rheon_b200 import workloads as W
+    from rheon_b200.box_flux import BoxFluxStamp, PrescribedBoxFlux
+
+    torch.cuda.set_device(local)
+    n = args.n
+    g = R.GridGeometry((n, n, n), (1.0 / n,) * 3)
+    faces = W.fourier_faces((n, n, n), seed=args.seed, dtype=np.float32)
+    tracer = np.zeros(g.cell_len(), np.float32)
+    src = SS.SmokeSource((0.375, 0.125, 0.375), (0.625, 0.375, 0.625), 0.5, 1.0)
+    forces = [SS.BodyForce((0.0, -0.25, 0.0))]
+    bnd = SS.BoxFluxStepBoundary(PrescribedBoxFlux(BoxFluxStamp(1, 0), [[-0.5, 0.5], [0.0, 0.0], [0.0, 0.0]]))
+    pressure = R.PressureSettings(1e-8, 0.0, MAXF, 1000000)
+    res = {"workload": f"box-flux step at {n}^3: random-Fourier state, smoke source, uniform body force, "
+                       f"0.5 m/s x through-flow, rel 1e-8", "unit": "cell-steps/s"}
+    k = max(3, min(args.steps, 5))
+    for name, cfg in (("mg_mixed", R.CarrierConfig.mixed(device=local, with_tracer=True, pressure=pressure,
+                                                         actual_divergence_limit=1.0)),
+                      ("jacobi_pcg_v1_f32", R.CarrierConfig(storage="f32", device=local, with_tracer=True,
+                                                            pressure=pressure, actual_divergence_limit=1.0))):
+        sim = R.CarrierSimulation(g, cfg)
+        sim.upload(faces, tracer)
+        ws = SS.BoxFluxStepWorkspace(g, cfg.density, 1 << 40, cfg.implementation, device=local)
+        for _ in range(2):
+            SS.step_with_box_flux(sim, 1.0, src, forces, ws, bnd)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k):
+            r = SS.step_with_box_flux(sim, 1.0, src, forces, ws, bnd)
+        el = (time.perf_counter() - t0) / k
+        res[name] = {"ms_per_step": el * 1e3, "value": g.cell_len() / el, "dt": r.step.dt,
+                     "pcg_iterations": r.step.pressure.iterations, "budget_error": r.work.budget_error,
+                     "kinetic_accepted": r.work.kinetic_accepted,
+                     "actual_divergence_max": r.step.actual_divergence_max}
+        ws.close()
+        sim.close()
+    res["value"] = res["mg_mixed"]["value"]
+    if with_cpu:
+        import oracle as O
+
+        m = min(n, 32)
+        og = O.grid((m, m, m), (1.0 / m,) * 3)
+        sim = O.Simulation(og, 1.0, O.JACOBI_PCG_V1, O.settings(1e-8, 0.0, MAXF, 1000000), 1.0, 1.0,
+                           W.fourier_faces((m, m, m), seed=args.seed, dtype=np.float32))
+        t0 = time.perf_counter()
+        st, rep = sim.step(1.0, dict(lower=src.lower, upper=src.upper, tracer_rate=src.tracer_rate,
+                                     vertical_acceleration=src.vertical_acceleration),
+                           [dict(value=forces[0].value, units=0, region=None)], [[-0.5, 0.5], [0.0, 0.0], [0.0, 0.0]])
+        cpu_s = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": m ** 3 / cpu_s, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+                               "sample": f"one {m}^3 box-flux step of the same workload by the oracle (Jacobi-PCG, "
+                                         f"{rep.pressure.iterations} iterations, status {st}); the per-cell cost "
+                                         f"grows with n, so this overstates the CPU at {n}^3"}
     return res
 
 

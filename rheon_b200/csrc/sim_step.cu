@@ -56,20 +56,6 @@ namespace {
 constexpr int FS_SCALARS = 8;
 constexpr int FS_SLOT = 9;  // doubles per block: up to 3 double-double sums and 3 maxima
 
-// (axis, index within the axis) of a flat index over the three face arrays
-__device__ __forceinline__ void split_face(const GridDev& g, int t, int& a, int& f) {
-    a = 0;
-    f = t;
-    if (f >= g.flen[0]) {
-        f -= g.flen[0];
-        a = 1;
-        if (f >= g.flen[1]) {
-            f -= g.flen[1];
-            a = 2;
-        }
-    }
-}
-
 __device__ __forceinline__ void face_coords(const GridDev& g, int a, int f, int (&c)[3]) {
     const int row = f / g.fc[a][0];
     c[0] = f - row * g.fc[a][0];
@@ -82,41 +68,37 @@ __device__ __forceinline__ double face_pos(const GridDev& g, int a, const int (&
     return g.o[d] + (double(c[d]) + (d == a ? 0.0 : 0.5)) * g.h[d];
 }
 
-__device__ __forceinline__ bool in_box(const double (&p)[3], const double* lower, const double* upper) {
-    return p[0] >= lower[0] && p[0] < upper[0] && p[1] >= lower[1] && p[1] < upper[1] && p[2] >= lower[2] &&
-           p[2] < upper[2];
+__device__ __forceinline__ bool in_box(double x, double y, double z, const double* lower, const double* upper) {
+    return x >= lower[0] && x < upper[0] && y >= lower[1] && y < upper[1] && z >= lower[2] && z < upper[2];
 }
 
 // All-face and interior-face sums of squares (forces.rs:153-161,
 // box_flux_step.rs:118-149), per-axis max |u_d| (velocity_rate,
-// simulation.rs:1415-1429) and finiteness of a face state.
+// simulation.rs:1415-1429) and finiteness of a face state. One grid-stride
+// sweep per axis (the axis is a compile-time constant in each).
 // out: {all, interior, max x, max y, max z}
 __global__ void __launch_bounds__(EW_THREADS) k_fs_face_stats(GridDev g, const float* __restrict__ u,
                                                               const float* __restrict__ v,
                                                               const float* __restrict__ w, Partials part,
                                                               double* out, int* flags) {
     __shared__ BlockReduce<2, 3> sm;
-    const float* f3[3] = {u, v, w};
     double all = 0.0, interior = 0.0;
     double mx[3] = {0.0, 0.0, 0.0};
     int local = 0;
-    const int total = g.flen[0] + g.flen[1] + g.flen[2];
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        int a, f, c[3];
-        split_face(g, t, a, f);
-        face_coords(g, a, f, c);
-        const double x = double(f3[a][f]);
-        if (!isfinite(x)) local |= VF_NONFINITE;
-        const double sq = x * x;
-        all += sq;
-        if (c[a] > 0 && c[a] < g.n[a]) interior += sq;
-        const double ax = fabs(x);
-        if (a == 0)
-            mx[0] = fmax(mx[0], ax);
-        else if (a == 1)
-            mx[1] = fmax(mx[1], ax);
-        else
-            mx[2] = fmax(mx[2], ax);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float* __restrict__ x3 = a == 0 ? u : (a == 1 ? v : w);
+        const int n0 = g.fc[a][0], n1 = g.fc[a][1], na = g.n[a];
+        for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < g.flen[a]; f += gridDim.x * blockDim.x) {
+            const int row = f / n0;
+            const int ca = a == 0 ? f - row * n0 : (a == 1 ? row % n1 : row / n1);
+            const double x = double(x3[f]);
+            if (!isfinite(x)) local |= VF_NONFINITE;
+            const double sq = x * x;
+            all += sq;
+            if (ca > 0 && ca < na) interior += sq;
+            mx[a] = fmax(mx[a], fabs(x));
+        }
     }
     if (local) atomicOr(flags, local);
     dd sums[2] = {dd{all, 0.0}, dd{interior, 0.0}};
@@ -140,8 +122,7 @@ __global__ void __launch_bounds__(EW_THREADS) k_fs_smoke_force(GridDev g, float*
         int c[3];
         face_coords(g, 1, f, c);
         if (c[1] < 1 || c[1] >= g.n[1]) continue;
-        const double p[3] = {face_pos(g, 1, c, 0), face_pos(g, 1, c, 1), face_pos(g, 1, c, 2)};
-        if (!in_box(p, s.lower, s.upper)) continue;
+        if (!in_box(face_pos(g, 1, c, 0), face_pos(g, 1, c, 1), face_pos(g, 1, c, 2), s.lower, s.upper)) continue;
         const double value = double(y[f]) + dt * s.vertical_acceleration;
         if (!isfinite(value) || fabs(value) > double(kF32Max)) {
             local |= VF_ARITH;
@@ -155,46 +136,53 @@ __global__ void __launch_bounds__(EW_THREADS) k_fs_smoke_force(GridDev g, float*
 // forces::apply_evaluated (src/forces.rs:144-212) for constant vectors: each
 // interior face adds dt times the sum of the accelerations of the forces
 // whose support holds its position (in the caller's order); out: {sum of
-// squares before, sum of squares after, work}.
+// squares before, sum of squares after, work}. One grid-stride sweep per
+// axis (the axis is a compile-time constant in each).
 __global__ void __launch_bounds__(EW_THREADS) k_fs_forces(GridDev g, float* __restrict__ u, float* __restrict__ v,
                                                           float* __restrict__ w,
                                                           const rb200_body_force* __restrict__ forces, int nforces,
                                                           double density, double dt, double mass, Partials part,
                                                           double* out, int* flags) {
     __shared__ BlockReduce<3, 0> sm;
-    float* f3[3] = {u, v, w};
     double before = 0.0, after = 0.0, work = 0.0;
     int local = 0;
-    const int total = g.flen[0] + g.flen[1] + g.flen[2];
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        int a, f, c[3];
-        split_face(g, t, a, f);
-        face_coords(g, a, f, c);
-        const double old = double(f3[a][f]);
-        const double old_sq = old * old;
-        before += old_sq;
-        double new_sq = old_sq;
-        if (c[a] > 0 && c[a] < g.n[a]) {
-            const double p[3] = {face_pos(g, a, c, 0), face_pos(g, a, c, 1), face_pos(g, a, c, 2)};
-            double sum = 0.0;
-            for (int q = 0; q < nforces; ++q) {
-                const rb200_body_force& F = forces[q];
-                if (F.has_region && !in_box(p, F.lower, F.upper)) continue;
-                sum += F.units == RB200_FORCE_DENSITY ? F.value[a] / density : F.value[a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float* __restrict__ x3 = a == 0 ? u : (a == 1 ? v : w);
+        const int n0 = g.fc[a][0], n1 = g.fc[a][1], na = g.n[a];
+        for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < g.flen[a]; f += gridDim.x * blockDim.x) {
+            const int row = f / n0;
+            const int i = f - row * n0, k = row / n1, j = row - k * n1;
+            const int ca = a == 0 ? i : (a == 1 ? j : k);
+            const double old = double(x3[f]);
+            const double old_sq = old * old;
+            before += old_sq;
+            double new_sq = old_sq;
+            if (ca > 0 && ca < na) {
+                // face_position (src/geometry.rs:242-248)
+                const double px = g.o[0] + (double(i) + (a == 0 ? 0.0 : 0.5)) * g.h[0];
+                const double py = g.o[1] + (double(j) + (a == 1 ? 0.0 : 0.5)) * g.h[1];
+                const double pz = g.o[2] + (double(k) + (a == 2 ? 0.0 : 0.5)) * g.h[2];
+                double sum = 0.0;
+                for (int q = 0; q < nforces; ++q) {
+                    const rb200_body_force& F = forces[q];
+                    if (F.has_region && !in_box(px, py, pz, F.lower, F.upper)) continue;
+                    sum += F.units == RB200_FORCE_DENSITY ? F.value[a] / density : F.value[a];
+                }
+                const double updated = old + dt * sum;
+                if (!isfinite(updated) || fabs(updated) > double(kF32Max)) {
+                    local |= VF_ARITH;
+                } else {
+                    const float stored = float(updated);
+                    const double nv = double(stored);
+                    const double delta = nv - old;
+                    work += mass * delta * (old + 0.5 * delta);
+                    x3[f] = stored;
+                    new_sq = nv * nv;
+                }
             }
-            const double updated = old + dt * sum;
-            if (!isfinite(updated) || fabs(updated) > double(kF32Max)) {
-                local |= VF_ARITH;
-            } else {
-                const float stored = float(updated);
-                const double nv = double(stored);
-                const double delta = nv - old;
-                work += mass * delta * (old + 0.5 * delta);
-                f3[a][f] = stored;
-                new_sq = nv * nv;
-            }
+            after += new_sq;
         }
-        after += new_sq;
     }
     if (local) atomicOr(flags, local);
     dd sums[3] = {dd{before, 0.0}, dd{after, 0.0}, dd{work, 0.0}};
@@ -214,9 +202,9 @@ __global__ void __launch_bounds__(EW_THREADS) k_fs_smoke_source(GridDev g, float
     for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < g.cells; cell += gridDim.x * blockDim.x) {
         const int row = cell / g.n[0];
         const int c[3] = {cell - row * g.n[0], row % g.n[1], row / g.n[1]};
-        double p[3];
-        for (int d = 0; d < 3; ++d) p[d] = g.o[d] + (double(c[d]) + 0.5) * g.h[d];
-        if (!in_box(p, s.lower, s.upper)) continue;
+        if (!in_box(g.o[0] + (double(c[0]) + 0.5) * g.h[0], g.o[1] + (double(c[1]) + 0.5) * g.h[1],
+                    g.o[2] + (double(c[2]) + 0.5) * g.h[2], s.lower, s.upper))
+            continue;
         tracer[cell] = float(fmin(double(tracer[cell]) + amount, 1.0));
     }
 }
