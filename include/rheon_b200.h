@@ -772,7 +772,12 @@ RB200_API int rb200_box_flux_last_pass_ms(rb200_box_flux* workspace, double* rhs
  * (src/simulation.rs:393-581, prepare_impl :812-1403). Host-driven: the
  * stages run as device passes on the carrier's stream in the reference's
  * order, with its cancellation points, and the accepted state is published
- * only by the final commit. Needs f32 face storage and a tracer. */
+ * only by the final commit. Needs f32 face storage and a tracer. With a
+ * liquid state attached (rb200_carrier_attach_liquid, inputs set) this is the
+ * liquid step (LiquidTransportSimulation::step / step_with_box_flux,
+ * src/liquid_step.rs:517-567): the transport runs through the candidate faces
+ * and a rejected transport (RB200_LIQUID_REJECTED, rb200_carrier_liquid_report)
+ * rejects the step. */
 typedef struct rb200_smoke_source {      /* SmokeSource (src/simulation.rs:19-27) */
     double lower[3];
     double upper[3];
@@ -803,7 +808,8 @@ typedef enum rb200_step_stage {
     RB200_STAGE_BEFORE_PROJECTION_ACCEPTANCE = 8,
     RB200_STAGE_BEFORE_TRACER = 9,
     RB200_STAGE_TRACER_SLICE = 10,
-    RB200_STAGE_BEFORE_COMMIT = 11
+    RB200_STAGE_BEFORE_COMMIT = 11,
+    RB200_STAGE_LIQUID_BEFORE_COMMIT = 12   /* LiquidStepStage::BeforeCommit (src/liquid_step.rs:918) */
 } rb200_step_stage;
 
 typedef int (*rb200_step_cancel_fn)(void* ctx, int stage);

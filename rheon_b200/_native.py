@@ -193,7 +193,7 @@ BOX_FLUX_CANCEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int)
 # rb200_step_stage: StepStage (src/simulation.rs:28-42)
 STEP_STAGES = ("BeforeAdvection", "VelocitySlice", "BeforeForces", "ForceSlice", "Viscosity", "BeforePressure",
                "PressureIteration", "ProjectionSlice", "BeforeProjectionAcceptance", "BeforeTracer", "TracerSlice",
-               "BeforeCommit")
+               "BeforeCommit", "LiquidBeforeCommit")
 # rb200_simulation_error: SimulationError's own variants
 SIMULATION_ERRORS = {0: "Ok", 1: "InvalidSource", 2: "InvalidForce", 3: "TimeResolution",
                      4: "BoundaryWorkspaceMismatch", 5: "Cancelled"}

@@ -12,7 +12,9 @@
 //   pressure solve, fused correction/divergence) or the box-flux projection
 //   (rb200_box_flux_project_device) into the candidate buffer -> Courant gate
 //   -> tracer advection -> smoke source's tracer (apply_source :1473-1496) ->
-//   tracer range check -> commit (index rotation on the device).
+//   tracer range check -> [with an attached liquid state: the liquid-volume
+//   transport through the candidate faces] -> commit (index rotation on the
+//   device; the liquid state commits with the carrier).
 // Cancellation is asked at the reference's stages; a slice stage is asked
 // as often as the reference asks it (its first time before the device pass,
 // the others while the pass runs). Nothing is published before the commit,
@@ -376,7 +378,8 @@ extern "C" int rb200_carrier_step_forced(rb200_carrier* c, const rb200_forced_st
     if (!c || !prm || !rep) return RB200_INVALID_ARGUMENT;
     std::memset(rep, 0, sizeof(*rep));
     if (c->in_flight) return RB200_INVALID_ARGUMENT;
-    if (c->elem != 4 || !c->tracer[0] || c->lq_d) return RB200_UNSUPPORTED;
+    if (c->elem != 4 || !c->tracer[0]) return RB200_UNSUPPORTED;
+    if (c->lq_d && !c->lq_inputs) return RB200_INVALID_ARGUMENT;  // the liquid step's inputs are not set
     const bool boundary = prm->box_flux != nullptr;
     if ((boundary && !prm->boundary) || (prm->force_count && !prm->forces)) return RB200_INVALID_ARGUMENT;
     if (boundary)
@@ -635,6 +638,26 @@ extern "C" int rb200_carrier_step_forced(rb200_carrier* c, const rb200_forced_st
     }
     if (!std::isfinite(tracer_integral) || !std::isfinite(kinetic)) return RB200_ARITHMETIC_FAILURE;
     if (cancel.ask(RB200_STAGE_BEFORE_COMMIT)) return cancelled_at(rep, RB200_STAGE_BEFORE_COMMIT);
+    // the liquid step (LiquidTransportSimulation::step_impl, src/liquid_step.rs:867-917):
+    // the transport through the candidate faces over [time, time + dt], stamped
+    // {flow_id, candidate generation}; a rejection rejects the step
+    if (c->lq_d) {
+        LiquidFlowDev& lf = *c->lflow_h;
+        for (int d = 0; d < 3; ++d) lf.vel[d] = cand[d];
+        lf.start = time;
+        lf.dt = dt;
+        lf.flow = rb200_liquid_stamp{c->h_cd->flow_id, generation + 1};
+        lf.active = 1;
+        lf.periodic = 0;
+        RB200_CUDA(cudaMemcpyAsync(c->lflow_d, c->lflow_h, sizeof(LiquidFlowDev), cudaMemcpyHostToDevice, c->stream));
+        RB200_CUDA(launch_liquid_advance(g, c->lq_d, c->lflow_d, c->lq_sc, c->lq_blocks, c->lrep_d, c->stream));
+        RB200_CUDA(cudaMemcpyAsync(c->lrep_h, c->lrep_d, sizeof(rb200_liquid_report), cudaMemcpyDeviceToHost,
+                                   c->stream));
+        RB200_CUDA(cudaStreamSynchronize(c->stream));
+        if (c->lrep_h->error) return RB200_LIQUID_REJECTED;
+        if (cancel.ask(RB200_STAGE_LIQUID_BEFORE_COMMIT))
+            return cancelled_at(rep, RB200_STAGE_LIQUID_BEFORE_COMMIT);
+    }
     // commit: the step's pressure becomes the accepted one (the dense3D
     // frame's pressure field)
     const size_t pbytes = size_t(g.cells) * sizeof(double);
@@ -645,6 +668,10 @@ extern "C" int rb200_carrier_step_forced(rb200_carrier* c, const rb200_forced_st
         RB200_CUDA(cudaMemcpyAsync(c->accepted_p, c->solver.p(), pbytes, cudaMemcpyDeviceToDevice, c->stream));
     k_fs_commit<<<1, 1, 0, c->stream>>>(c->cd, Cb, tacc ^ 1, next_time, generation + 1, crate);
     RB200_CUDA(cudaGetLastError());
+    if (c->lq_d) {
+        RB200_CUDA(launch_liquid_commit(c->lq_d, c->lrep_d, c->stream));
+        RB200_CUDA(cudaMemcpyAsync(c->lq_h, c->lq_d, sizeof(LiquidDev), cudaMemcpyDeviceToHost, c->stream));
+    }
     RB200_CUDA(cudaMemcpyAsync(c->h_cd, c->cd, sizeof(CarrierDev), cudaMemcpyDeviceToHost, c->stream));
     RB200_CUDA(cudaStreamSynchronize(c->stream));
     c->accepted_steps += 1;

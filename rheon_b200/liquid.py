@@ -280,6 +280,42 @@ class LiquidTransportSimulation:
         lib().rb200_carrier_liquid_report(self.carrier._handle, C.byref(lr))
         return LiquidStepReport(rep, LiquidVolumeReport.from_c(lr))
 
+    def _inputs(self, inlet, settings, source, source_stamp):
+        inl = N.LiquidInlet(N.LiquidStamp(*inlet.stamp),
+                            (C.c_double * 6)(*[float(x) for pair in inlet.fraction for x in pair]))
+        src = None
+        if source is not None:
+            src = N.LiquidSource(N.LiquidStamp(*source_stamp), _ptr(source))
+            self._keep = [source]
+        st = lib().rb200_carrier_liquid_inputs(self.carrier._handle, C.byref(inl), C.byref(src) if src else None,
+                                               C.byref(N.LiquidSettings(settings.max_outward_courant,
+                                                                        settings.actual_divergence_limit)))
+        if st != N.OK:
+            raise LiquidVolumeError(N.STATUS_NAMES.get(st, f"Status{st}"), status=st)
+
+    def step_with_box_flux(self, requested_dt: float, inlet: LiquidInlet, settings: LiquidVolumeSettings, workspace,
+                           boundary, smoke_source=None, forces=(), source=None, source_stamp=(0, 0), cancel=None):
+        """LiquidTransportSimulation::step_with_box_flux (src/liquid_step.rs:548-567):
+        the carrier's box-flux step (rheon_b200.simulation.step_with_box_flux)
+        with the transport through its candidate faces, one transaction.
+        Returns (BoxFluxStepReport, LiquidVolumeReport); raises
+        LiquidVolumeError when the transport rejects the step, StepError when
+        the carrier does."""
+        from . import simulation as S
+
+        self._inputs(inlet, settings, source, source_stamp)
+        try:
+            rep = S.step_with_box_flux(self.carrier, requested_dt, smoke_source, forces, workspace, boundary, cancel)
+        except S.StepError as e:
+            if e.status == N.LIQUID_REJECTED:
+                lr = N.LiquidReport()
+                lib().rb200_carrier_liquid_report(self.carrier._handle, C.byref(lr))
+                raise LiquidVolumeError.from_report(N.LIQUID_REJECTED, lr) from None
+            raise
+        lr = N.LiquidReport()
+        lib().rb200_carrier_liquid_report(self.carrier._handle, C.byref(lr))
+        return rep, LiquidVolumeReport.from_c(lr)
+
     def _state(self):
         p = C.c_void_p()
         s = N.LiquidStamp()

@@ -57,7 +57,8 @@ class BodyForce:
 class StepStage:
     """StepStage (src/simulation.rs:28-42), by name."""
     BEFORE_ADVECTION, VELOCITY_SLICE, BEFORE_FORCES, FORCE_SLICE, VISCOSITY, BEFORE_PRESSURE, PRESSURE_ITERATION, \
-        PROJECTION_SLICE, BEFORE_PROJECTION_ACCEPTANCE, BEFORE_TRACER, TRACER_SLICE, BEFORE_COMMIT = N.STEP_STAGES
+        PROJECTION_SLICE, BEFORE_PROJECTION_ACCEPTANCE, BEFORE_TRACER, TRACER_SLICE, BEFORE_COMMIT, \
+        LIQUID_BEFORE_COMMIT = N.STEP_STAGES
 
 
 class BoxFluxTracerPolicy:
@@ -143,6 +144,8 @@ class StepError(RuntimeError):
             self.actual, self.limit = r.error_actual, r.error_limit
         elif status == N.ARITHMETIC_FAILURE:
             self.kind = "ArithmeticFailure"
+        elif status == N.LIQUID_REJECTED:
+            self.kind = "LiquidVolume"  # the transport's report: rb200_carrier_liquid_report
         elif status == N.BOX_FLUX_REJECTED:
             self.kind = "BoxFlux"
             self.inner = N.BOX_FLUX_ERRORS.get(r.projection.error, str(r.projection.error))

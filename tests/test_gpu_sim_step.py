@@ -584,3 +584,68 @@ def test_forced_steps_match_the_oracle(method, with_boundary):
                 near(getattr(rb.work, name), getattr(orep, name), 1e-9)
             scale = rb.work.kinetic_accepted + rb.work.kinetic_old + 1e-300
             assert abs(rb.work.budget_error) <= 1e-6 * scale
+
+
+# ------------------------------------------------------------------ the liquid step with a box-flux boundary
+def pilot(flow_id=11):
+    """The dense3D pilot channel (tests/dense3d_controls_contract.rs:27-75): 3 x 1 x 1
+    cells of 1/3 m, carrier density 1000, represented liquid 800 at [0.5, 0, 0],
+    a 0.25 m/s x through-flow."""
+    from rheon_b200 import liquid as L
+
+    sim = carrier((3, 1, 1), (1.0 / 3.0, 1.0, 1.0), density=1000.0)
+    lts = L.LiquidTransportSimulation(sim, 800.0, (2 ** 64 - 1, 0), [0.5, 0.0, 0.0], flow_id=flow_id)
+    return sim, lts
+
+
+def test_liquid_step_with_box_flux_matches_the_oracle():
+    from rheon_b200 import liquid as L
+
+    sim, lts = pilot()
+    w = workspace(sim)
+    inlet = L.LiquidInlet((53, 0), [[0.0, 0.0]] * 3)
+    settings = L.LiquidVolumeSettings(1.0, 1e-5)
+    og = O.grid((3, 1, 1), (1.0 / 3.0, 1.0, 1.0))
+    orc = O.Simulation(og, 1000.0, O.JACOBI_PCG_V1, O.settings(1e-12, 1e-12, 1e-9, 1000), 1e-5, 1.0)
+    fraction = np.array([0.5, 0.0, 0.0])
+    outward = [[-0.25, 0.25], [0.0, 0.0], [0.0, 0.0]]
+    for step in range(1, 6):
+        b = S.BoxFluxStepBoundary(PrescribedBoxFlux(BoxFluxStamp(47, step), outward))
+        rep, lrep = lts.step_with_box_flux(0.0625, inlet, settings, w, b)
+        start = orc.time
+        st, orep = orc.step(0.0625, outward=outward)
+        assert st == 0 and rep.step.dt == orep.dt == 0.0625
+        err, cand, odict = O.liquid_advance(og, 800.0, fraction, orc.faces, start, orep.dt, [[0.0, 0.0]] * 3,
+                                            max_outward_courant=1.0, actual_divergence_limit=1e-5, version=step - 1)
+        assert err == "Ok"
+        fraction = cand
+        assert np.array_equal(lts.fraction(), fraction)
+        assert lrep.flow == (11, step) and lrep.stamp == (2 ** 64 - 1, step)
+        assert lts.time == rep.step.time == orc.time
+        fs, _ = state(sim)
+        for d in range(3):
+            assert np.array_equal(fs[d], orc.faces[d])
+        assert lrep.liquid_volume_after == odict["liquid_volume_after"]
+        assert lrep.outward_boundary_volume == odict["outward_boundary_volume"]
+
+
+def test_a_rejected_transport_rejects_the_box_flux_step():
+    from rheon_b200 import liquid as L
+
+    sim, lts = pilot()
+    w = workspace(sim)
+    inlet = L.LiquidInlet((53, 0), [[0.0, 0.0]] * 3)
+    b = S.BoxFluxStepBoundary(PrescribedBoxFlux(BoxFluxStamp(47, 0), [[-0.25, 0.25], [0.0, 0.0], [0.0, 0.0]]))
+    lts.step_with_box_flux(0.0625, inlet, L.LiquidVolumeSettings(1.0, 1e-5), w, b)
+    before, frac, stamp = snapshot(sim), lts.fraction(), lts.stamp
+    with pytest.raises(L.LiquidVolumeError) as e:
+        lts.step_with_box_flux(0.0625, inlet, L.LiquidVolumeSettings(1e-9, 1e-5), w, b)
+    assert e.value.kind == "CourantLimit"
+    assert snapshot(sim) == before and np.array_equal(lts.fraction(), frac) and lts.stamp == stamp
+    with pytest.raises(S.StepError) as e:
+        lts.step_with_box_flux(0.0625, inlet, L.LiquidVolumeSettings(1.0, 1e-5), w, b,
+                               cancel=lambda s: s == S.StepStage.LIQUID_BEFORE_COMMIT)
+    assert (e.value.kind, e.value.stage) == ("Cancelled", "LiquidBeforeCommit")
+    assert snapshot(sim) == before and np.array_equal(lts.fraction(), frac) and lts.stamp == stamp
+    rep, lrep = lts.step_with_box_flux(0.0625, inlet, L.LiquidVolumeSettings(1.0, 1e-5), w, b)
+    assert rep.step.generation == 2 and lrep.stamp[1] == 2
