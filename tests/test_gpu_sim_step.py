@@ -649,3 +649,51 @@ def test_a_rejected_transport_rejects_the_box_flux_step():
     assert snapshot(sim) == before and np.array_equal(lts.fraction(), frac) and lts.stamp == stamp
     rep, lrep = lts.step_with_box_flux(0.0625, inlet, L.LiquidVolumeSettings(1.0, 1e-5), w, b)
     assert rep.step.generation == 2 and lrep.stamp[1] == 2
+
+
+# ------------------------------------------------------------------ the forced step beside the graph step
+def test_forced_steps_publish_their_pressure_and_hand_over_to_the_graph_step():
+    """A forced sealed step, then a box-flux step, then (sealed state again) a
+    graph step: the carrier's accepted pressure is each step's own, and the
+    graph step after a forced step matches the oracle's carrier step."""
+    from rheon_b200 import dense3d as D
+
+    counts = (12, 10, 8)
+    faces, tracer = random_state(counts, 5)
+    pressure = (1e-10, 0.0, MAXF, 5000)
+    sim = carrier(counts, density=1.0, pressure=pressure, limit=MAXF, faces=faces, tracer=tracer)
+    S.step_with_forces(sim, 0.05, None, [S.BodyForce((0.0, -0.5, 0.0))])
+    # the sealed forced step's pressure is the carrier solver's
+    assert D.Dense3dFields.from_carrier(sim).pressure != 0
+    p_forced = sim.pressure()
+    assert p_forced[0] == 0.0 and np.any(p_forced != 0.0)
+    w = workspace(sim)
+    r = S.step_with_box_flux(sim, 0.05, None, [], w, boundary(0, 0.25))
+    assert np.array_equal(sim.pressure(), w.projection.pressure())
+    assert r.step.pressure.iterations > 0
+    # back to a sealed state: a zero-flux box-flux step stores zero outer faces
+    S.step_with_box_flux(sim, 0.05, None, [], w, boundary(0, 0.0, 1))
+    fs = state(sim)[0]
+    rep = sim.step(R.StepParams(0.05, cfl=0.0))
+    prm = O.StepParams(rep.dt, 1.0, O.JACOBI_PCG_V1, O.settings(*pressure), 0.0, 0, 1)
+    st, ref, _, orep = O.carrier_step(O.grid(counts), fs, prm)
+    assert st == O.OK and rep.pressure.iterations == orep.pressure.iterations
+    got = sim.download()
+    for d in range(3):
+        ulps = np.abs(got[d].view(np.int32).astype(np.int64) - np.asarray(ref[d], np.float32).view(np.int32)
+                      .astype(np.int64))
+        assert ulps.max() <= 1
+
+
+def test_a_rejected_forced_step_invalidates_the_exported_pressure():
+    from rheon_b200 import dense3d as D
+
+    sim = carrier((6, 5, 4), density=1.0, limit=0.0)
+    S.step_with_forces(sim, 0.05, None, [S.BodyForce((0.0, 0.0, 0.0))])  # divergence 0: accepted
+    D.Dense3dFields.from_carrier(sim)
+    with pytest.raises(S.StepError):
+        S.step_with_forces(sim, 0.05, None, [S.BodyForce((0.3, -0.2, 0.1),
+                                                        region=S.ForceRegion((0, 0, 0), (3.0, 2.0, 2.0)))])
+    with pytest.raises(Exception) as e:
+        D.Dense3dFields.from_carrier(sim)
+    assert "InvalidState" in str(e.value) or getattr(e.value, "kind", "") == "InvalidState"
