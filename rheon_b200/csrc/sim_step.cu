@@ -290,19 +290,24 @@ int ensure_scratch(rb200_carrier* c, size_t nforces) {
     if (!c->forced) {
         auto* s = new (std::nothrow) ForcedScratch();
         if (!s) return RB200_OUT_OF_MEMORY;
-        c->forced = s;
         long long b = (std::max<long long>(c->g.cells, (long long)c->g.flen[0] + c->g.flen[1] + c->g.flen[2]) +
                        EW_THREADS - 1) /
                       EW_THREADS;
         s->nb = int(std::min<long long>(std::max<long long>(b, 1), EW_BLOCKS_CAP));
         const size_t bytes = 16 + FS_SCALARS * sizeof(double) + size_t(s->nb) * FS_SLOT * sizeof(double) + 16;
-        RB200_CUDA(cudaMalloc(&s->d_buf, bytes));
-        RB200_CUDA(cudaMemset(s->d_buf, 0, bytes));
-        RB200_CUDA(cudaMallocHost(&s->h_buf, 16 + FS_SCALARS * sizeof(double)));
+        // attached only when complete: a failed allocation leaves no half-made scratch behind
+        if (cudaMalloc(&s->d_buf, bytes) != cudaSuccess || cudaMemset(s->d_buf, 0, bytes) != cudaSuccess ||
+            cudaMallocHost(&s->h_buf, 16 + FS_SCALARS * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            forced_scratch_free(s);
+            set_error("forced step scratch allocation failed");
+            return RB200_OUT_OF_MEMORY;
+        }
         s->d_flags = reinterpret_cast<int*>(s->d_buf);
         s->d_scalars = reinterpret_cast<double*>(s->d_buf + 16);
         s->part.data = s->d_scalars + FS_SCALARS;
         s->part.ticket = reinterpret_cast<unsigned*>(s->part.data + size_t(s->nb) * FS_SLOT);
+        c->forced = s;
     }
     ForcedScratch* s = c->forced;
     if (nforces > s->force_cap) {
