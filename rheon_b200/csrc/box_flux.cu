@@ -37,26 +37,6 @@ namespace {
 constexpr int BF_SUMS = 6;
 constexpr int BF_SCALARS = BF_SUMS + 1;  // + max |divergence|
 
-// Exact floor(c / d) for 0 <= c < 2^31 by one multiply and shift
-// (Granlund and Montgomery, "Division by invariant integers using
-// multiplication", 1994, the round-up method): with l = ceil(log2 d) and
-// m = floor(2^(31+l) / d) + 1, 2^(31+l) < m d <= 2^(31+l) + 2^l, so
-// floor(c m / 2^(31+l)) = floor(c / d); c m < 2^63.
-struct FastDiv {
-    unsigned long long m;
-    int shift;
-};
-
-FastDiv make_fastdiv(unsigned d) {
-    int l = 0;
-    while ((1ull << l) < d) ++l;
-    return FastDiv{(1ull << (31 + l)) / d + 1, 31 + l};
-}
-
-__device__ __forceinline__ int fast_div(int c, const FastDiv& f) {
-    return int((unsigned long long)(unsigned)c * f.m >> f.shift);
-}
-
 struct BfConst {
     float side[3][2];    // PrescribedBoxFlux::component(d, upper) (:36-45)
     double q[3][2];      // area_d * f64(outward) of each side (:342-349)

@@ -76,6 +76,26 @@ __device__ __forceinline__ double div_diag(double r, double D, double y) {
     return r / D;
 }
 
+// Exact floor(c / d) for 0 <= c < 2^31 by one multiply and shift
+// (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", 1994, the round-up method): with l = ceil(log2 d) and
+// m = floor(2^(31+l) / d) + 1, 2^(31+l) < m d <= 2^(31+l) + 2^l, so
+// floor(c m / 2^(31+l)) = floor(c / d); c m < 2^63.
+struct FastDiv {
+    unsigned long long m;
+    int shift;
+};
+
+inline FastDiv make_fastdiv(unsigned d) {
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    return FastDiv{(1ull << (31 + l)) / d + 1, 31 + l};
+}
+
+__device__ __forceinline__ int fast_div(int c, const FastDiv& f) {
+    return int((unsigned long long)(unsigned)c * f.m >> f.shift);
+}
+
 // ------------------------------------------------------------ double-double
 // Error-free two-sum (Knuth). With products rounded exactly as the reference
 // rounds them, a double-double accumulation of the rounded products followed

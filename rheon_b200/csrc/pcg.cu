@@ -530,45 +530,74 @@ __global__ void __launch_bounds__(EW) k_sgs_dot(GridDev g, SolveState* st, const
 // A symmetric M, as PCG needs; new (the reference sweeps lexicographically).
 __device__ __forceinline__ bool is_black(int i, int j, int k) { return ((i + j + k) & 1) != 0; }
 
-__global__ void __launch_bounds__(EW) k_rbsgs_black(GridDev g, SolveState* st, const double* __restrict__ r,
-                                                    double* __restrict__ z, int mode) {
+// Work mapping of the two passes: thread t takes cell pair m = t mod half of
+// row t / half (row = j + n1 k), i.e. cells 2m and 2m + 1 of the row, one of
+// each colour (half = ceil(n0 / 2); 2m + 1 may be n0 on an odd row length).
+struct PairMap {
+    int half, pairs;
+    FastDiv by_half, by_n1;
+};
+
+static PairMap pair_map(const GridDev& g) {
+    PairMap p;
+    p.half = (g.n[0] + 1) / 2;
+    p.pairs = p.half * g.n[1] * g.n[2];
+    p.by_half = make_fastdiv(unsigned(p.half));
+    p.by_n1 = make_fastdiv(unsigned(g.n[1]));
+    return p;
+}
+
+// Neighbour sum of cell (i, j, k), x-, x+, y-, y+, z-, z+ (one order for both colours).
+__device__ __forceinline__ double rb_neighbours(const GridDev& g, const double* __restrict__ z, int c, int i, int j,
+                                                int k, double init) {
+    double y = init;
+    if (i > 0) y += g.weight[0] * z[c - 1];
+    if (i + 1 < g.n[0]) y += g.weight[0] * z[c + 1];
+    if (j > 0) y += g.weight[1] * z[c - g.n[0]];
+    if (j + 1 < g.n[1]) y += g.weight[1] * z[c + g.n[0]];
+    const int sz = g.n[0] * g.n[1];
+    if (k > 0) y += g.weight[2] * z[c - sz];
+    if (k + 1 < g.n[2]) y += g.weight[2] * z[c + sz];
+    return y;
+}
+
+__global__ void __launch_bounds__(EW) k_rbsgs_black(GridDev g, PairMap pm, SolveState* st,
+                                                    const double* __restrict__ r, double* __restrict__ z, int mode) {
     if (!gate(st->flags, mode)) return;
-    const int s[3] = {1, g.n[0], g.n[0] * g.n[1]};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
-        int ijk[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
-        if (!is_black(ijk[0], ijk[1], ijk[2])) continue;
-        double y = r[c];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            if (ijk[a] > 0) y += g.weight[a] * z[c - s[a]];
-            if (ijk[a] + 1 < g.n[a]) y += g.weight[a] * z[c + s[a]];
-        }
-        z[c] = y / diag_at(g, ijk[0], ijk[1], ijk[2]);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < pm.pairs; t += gridDim.x * blockDim.x) {
+        const int row = fast_div(t, pm.by_half);
+        const int m = t - row * pm.half;
+        const int k = fast_div(row, pm.by_n1);
+        const int j = row - k * g.n[1];
+        const int i = 2 * m + ((j + k + 1) & 1);  // the black cell of the pair
+        if (i >= g.n[0]) continue;
+        const int c = i + g.n[0] * row;
+        const int mask = diag_mask(g, i, j, k);
+        z[c] = div_diag(rb_neighbours(g, z, c, i, j, k, r[c]), g.diag[mask], g.rdiag[mask]);
     }
 }
 
-__global__ void __launch_bounds__(EW) k_rbsgs_red_dot(GridDev g, SolveState* st, const double* __restrict__ r,
-                                                      double* __restrict__ z, int mode, Partials part,
-                                                      rb200_trace* trace) {
+__global__ void __launch_bounds__(EW) k_rbsgs_red_dot(GridDev g, PairMap pm, SolveState* st,
+                                                      const double* __restrict__ r, double* __restrict__ z, int mode,
+                                                      Partials part, rb200_trace* trace) {
     __shared__ BlockReduce<1, 0> sm;
     if (!gate(st->flags, mode)) return;
-    const int s[3] = {1, g.n[0], g.n[0] * g.n[1]};
     Neu acc;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
-        if (c == 0) continue;  // z[0] = 0 is kept by k_load_residual
-        int ijk[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
-        double zc = z[c];
-        if (!is_black(ijk[0], ijk[1], ijk[2])) {
-            double corr = 0.0;
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                if (ijk[a] > 0) corr += g.weight[a] * z[c - s[a]];
-                if (ijk[a] + 1 < g.n[a]) corr += g.weight[a] * z[c + s[a]];
-            }
-            zc = zc + corr / diag_at(g, ijk[0], ijk[1], ijk[2]);
-            z[c] = zc;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < pm.pairs; t += gridDim.x * blockDim.x) {
+        const int row = fast_div(t, pm.by_half);
+        const int m = t - row * pm.half;
+        const int k = fast_div(row, pm.by_n1);
+        const int j = row - k * g.n[1];
+        const int ired = 2 * m + ((j + k) & 1), iblk = 2 * m + ((j + k + 1) & 1);
+        const int cred = ired + g.n[0] * row, cblk = iblk + g.n[0] * row;
+        if (ired < g.n[0] && cred != 0) {  // z[0] = 0 is kept by k_load_residual
+            const int mask = diag_mask(g, ired, j, k);
+            const double corr = rb_neighbours(g, z, cred, ired, j, k, 0.0);
+            const double zc = z[cred] + div_diag(corr, g.diag[mask], g.rdiag[mask]);
+            z[cred] = zc;
+            acc.add(r[cred] * zc);
         }
-        acc.add(r[c] * zc);
+        if (iblk < g.n[0] && cblk != 0) acc.add(r[cblk] * z[cblk]);
     }
     dd sums[1] = {acc.as_dd()};
     double none[1];
@@ -739,8 +768,10 @@ static int launch_start(const GridDev& g, int method, const Bufs& B, const Multi
     if (method == RB200_RBSGS_PCG) {
         k_load_residual<KIND_RBSGS><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part,
                                                       B.trace);
-        k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_INIT);
-        k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_INIT, B.part, B.trace);
+        const PairMap pm = pair_map(g);
+        const int pb = ew_blocks(pm.pairs);
+        k_rbsgs_black<<<pb, EW, 0, s>>>(g, pm, B.st, B.r, B.z, MODE_INIT);
+        k_rbsgs_red_dot<<<pb, EW, 0, s>>>(g, pm, B.st, B.r, B.z, MODE_INIT, B.part, B.trace);
         return 4;
     }
     k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part, B.trace);
@@ -766,8 +797,10 @@ static int launch_iteration(const GridDev& g, int method, const Bufs& B, const M
     if (method == RB200_RBSGS_PCG) {
         k_pass2<ZC, 1><<<grid, block, kSmemSlab, s>>>(g, B.st, B.p, B.r, B.z, B.d0, B.d1, B.maps, B.part,
                                                           B.trace);
-        k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_ITER);
-        k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_ITER, B.part, B.trace);
+        const PairMap pm = pair_map(g);
+        const int pb = ew_blocks(pm.pairs);
+        k_rbsgs_black<<<pb, EW, 0, s>>>(g, pm, B.st, B.r, B.z, MODE_ITER);
+        k_rbsgs_red_dot<<<pb, EW, 0, s>>>(g, pm, B.st, B.r, B.z, MODE_ITER, B.part, B.trace);
         return 4;
     }
     if (method == RB200_SGS_PCG_V1) {
@@ -799,8 +832,10 @@ static int launch_check(const GridDev& g, int method, const Bufs& B, const Multi
     if (method == RB200_RBSGS_PCG) {
         k_load_residual<KIND_RBSGS><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part,
                                                       B.trace);
-        k_rbsgs_black<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_REPLACE);
-        k_rbsgs_red_dot<<<eb, EW, 0, s>>>(g, B.st, B.r, B.z, MODE_REPLACE, B.part, B.trace);
+        const PairMap pm = pair_map(g);
+        const int pb = ew_blocks(pm.pairs);
+        k_rbsgs_black<<<pb, EW, 0, s>>>(g, pm, B.st, B.r, B.z, MODE_REPLACE);
+        k_rbsgs_red_dot<<<pb, EW, 0, s>>>(g, pm, B.st, B.r, B.z, MODE_REPLACE, B.part, B.trace);
         return 4;
     }
     k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part, B.trace);
