@@ -32,7 +32,8 @@ def sources():
 
 def deps():
     return sources() + glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + glob.glob(
-        os.path.join(HERE, "csrc", "*.hpp")) + [os.path.join(ROOT, "include", "rheon_b200.h"), __file__]
+        os.path.join(HERE, "csrc", "*.hpp")) + glob.glob(os.path.join(HERE, "csrc", "*.inc")) + [
+        os.path.join(ROOT, "include", "rheon_b200.h"), __file__]
 
 
 def up_to_date() -> bool:

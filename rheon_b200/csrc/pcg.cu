@@ -14,6 +14,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -985,7 +986,12 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
     for (auto& e : ev_) RB200_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     maps_ = make_maps(g, z_, d_[0], d_[1], p_, r_);
     chunk_ = (method == RB200_MG_MIXED || method == RB200_SGS_PCG_V1) ? 4 : (g.cells >= (1 << 20) ? 32 : 16);
-    if (method == RB200_JACOBI_PCG_V1 && maps_.use) {
+    // RB200_PERSISTENT=0 in the environment keeps the per-pass kernels (a
+    // diagnostic switch: both paths compute the same iteration).
+    const char* persist_env = std::getenv("RB200_PERSISTENT");
+    const bool persist_allowed = !(persist_env && persist_env[0] == '0');
+    if ((method == RB200_JACOBI_PCG_V1 || method == RB200_RBSGS_PCG) && maps_.use && persist_allowed) {
+        persist_pre_ = method == RB200_RBSGS_PCG ? 1 : 0;
         int blocks = 0;
         if ((rc = persistent_setup(g, &blocks))) return rc;
         if (blocks > 0) {
@@ -1002,7 +1008,7 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
 
 cudaError_t PcgSolver::launch_persistent_chunk(cudaStream_t s, int budget) {
     return launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, d_trace_, maps_, persist_blocks_,
-                             budget, s);
+                             budget, s, persist_pre_);
 }
 
 int PcgSolver::set_trace(rb200_trace* host, size_t capacity) {
@@ -1030,7 +1036,7 @@ int PcgSolver::capture_chunk() {
     cudaError_t launch_err = cudaSuccess;
     if (persist_blocks_) {
         launch_err = launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, d_trace_, maps_,
-                                       persist_blocks_, chunk_, stream_);
+                                       persist_blocks_, chunk_, stream_, persist_pre_);
         nodes = 1;
     } else {
         for (int q = 0; q < chunk_; ++q) nodes += launch_iteration(g_, method_, B, mg, stream_);
@@ -1171,7 +1177,7 @@ int PcgSolver::enqueue_loop(cudaStream_t cs, cudaStream_t body_stream, const rb2
     const Multigrid* mg = method_ == RB200_MG_MIXED ? &mg_ : nullptr;
     if (persist_blocks_) {
         RB200_CUDA(launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, d_trace_, maps_,
-                                     persist_blocks_, chunk_, body_stream));
+                                     persist_blocks_, chunk_, body_stream, persist_pre_));
     } else {
         for (int q = 0; q < chunk_; ++q) launch_iteration(g_, method_, B, mg, body_stream);
         launch_check(g_, method_, B, mg, body_stream);
@@ -1210,13 +1216,13 @@ int PcgSolver::profile(int which, int launches, double* avg_ms) {
         // one warm iteration, then `launches` iterations in one launch
         RB200_CUDA(cudaMemsetAsync(gbar_, 0, sizeof(GridBarrier), stream_));
         RB200_CUDA(launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, nullptr, maps_,
-                                     persist_blocks_, 1, stream_));
+                                     persist_blocks_, 1, stream_, persist_pre_));
         cudaEvent_t a, b;
         RB200_CUDA(cudaEventCreate(&a));
         RB200_CUDA(cudaEventCreate(&b));
         RB200_CUDA(cudaEventRecord(a, stream_));
         RB200_CUDA(launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, nullptr, maps_,
-                                     persist_blocks_, launches, stream_));
+                                     persist_blocks_, launches, stream_, persist_pre_));
         RB200_CUDA(cudaEventRecord(b, stream_));
         RB200_CUDA(cudaEventSynchronize(b));
         float ms = 0.0f;

@@ -61,12 +61,12 @@ struct GridBarrier {
     unsigned pad;
 };
 
-// Persistent Jacobi-PCG kernel (persist.cu).
+// Persistent PCG kernel (persist.cu); pre: 0 Jacobi, 1 red-black SGS.
 int persistent_setup(const GridDev& g, int* blocks);
 size_t persistent_partial_doubles(int blocks);
 cudaError_t launch_persistent(const GridDev& g, SolveState* st, const double* b, double* p, double* r, double* z,
                               double* d0, double* d1, double* part, GridBarrier* bar, rb200_trace* trace,
-                              const TmaMaps& maps, int blocks, int budget, cudaStream_t s);
+                              const TmaMaps& maps, int blocks, int budget, cudaStream_t s, int pre);
 
 class PcgSolver {
 public:
@@ -113,6 +113,7 @@ public:
     int persistent_blocks() const { return persist_blocks_; }
     // One launch of the persistent kernel for at most `budget` iterations.
     cudaError_t launch_persistent_chunk(cudaStream_t s, int budget);
+    int persist_pre_ = 0;  // preconditioner of the persistent kernel: 0 Jacobi, 1 red-black SGS
     SolveState* state() { return st_; }
     const GridDev& grid() const { return g_; }
     Partials partials() const { return part_; }

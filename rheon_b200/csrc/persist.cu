@@ -1,8 +1,8 @@
-// Persistent Jacobi-PCG: one cooperative kernel runs a whole chunk of
-// iterations of PressureWorkspace::solve_loaded (src/pressure.rs:577-740)
-// with the "jacobi-pcg-v1" preconditioner (:534-575), true-residual checks and
-// restarts included, without returning to the host or the graph between
-// passes.
+// Persistent PCG: one cooperative kernel runs a whole chunk of iterations of
+// PressureWorkspace::solve_loaded (src/pressure.rs:577-740) with the
+// "jacobi-pcg-v1" preconditioner (:534-575), or with the red-black SGS
+// preconditioner of the RBSGS method, true-residual checks and restarts
+// included, without returning to the host or the graph between passes.
 //
 // Each block (one per SM) owns a fixed, strided set of 32 x 8 x 8 bricks and
 // is warp-specialised: one producer warp streams the bricks' slabs into a
@@ -22,6 +22,10 @@
 // and on a candidate:
 //   3  t = b - K p, |t|_2, max|t| -> accept / stop / restart     read p, b; write t          24
 //   4  (restart) r = t, z = r/D, r.z                             read t; write r, z          24
+// With red-black SGS, phase 2 stores only the red y = r/D and no r.z, and two
+// more phases follow it (and the restart), each after a grid barrier:
+//   B  z_b = (r_b + sum w y_nb) / D_b                              read z, r; write z (black)  ~20
+//   R  z_r = y_r + (sum w z_nb) / D_r, r.z                         read z, r; write z (red)    ~20
 // Phase 1 forms the new direction on the fly from the z and d slabs for
 // every value the stencil reads (the same z + beta*d per element), so the
 // slabs are never written.
@@ -130,6 +134,7 @@ struct Col {
     int e0;         // slab element of the column's first cell
     int bi0;        // brick (no halo) element of the column's first cell
     int mxy;        // neighbour-mask bits of x and y (src/operator.rs:813-822 order)
+    int par;        // (i + j) & 1: cell k of the column is red when (par + k) is even
     bool own;       // the column lies inside the domain
 };
 
@@ -144,6 +149,7 @@ __device__ __forceinline__ Col column(const GridDev& g, const Ctx& c, const Bric
     col.e0 = PS::own(c.tx, c.ty, qb);
     col.bi0 = c.tx + TX * (c.ty + TY * qb);
     col.mxy = int(i > 0) | (int(i + 1 < g.n[0]) << 1) | (int(j > 0) << 2) | (int(j + 1 < g.n[1]) << 3);
+    col.par = (i + j) & 1;
     return col;
 }
 
@@ -323,312 +329,96 @@ __device__ __forceinline__ bool run_bricks(Ctx& c, uint64_t* full, uint64_t* emp
     return ok;
 }
 
-__global__ void __launch_bounds__(PT, 1) k_jacobi_persistent(const __grid_constant__ PersistArgs A,
-                                                             const __grid_constant__ TmaMaps maps) {
-    extern __shared__ __align__(128) double smem[];
-    __shared__ SolveState sst;
-    __shared__ __align__(8) uint64_t full[NS];
-    __shared__ __align__(8) uint64_t empty[NS];
-    __shared__ double sdiag[64], srdiag[64];
-    const GridDev& g = A.g;
-    Ctx c;
-    c.tid = threadIdx.x;
-    c.lane = c.tid & 31;
-    c.producer = c.tid >= CONSUMERS;
-    c.tx = c.tid & 31;
-    c.ty = (c.tid >> 5) & (TY - 1);
-    c.tz = (c.tid >> 8) & (PZ - 1);
-    c.nbx = (g.n[0] + TX - 1) / TX;
-    c.nby = (g.n[1] + TY - 1) / TY;
-    c.nbricks = c.nbx * c.nby * ((g.n[2] + PZC - 1) / PZC);
-    c.mine = c.nbricks > int(blockIdx.x) ? (c.nbricks - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x) : 0;
-    c.bx0 = int(blockIdx.x) % c.nbx;
-    c.by0 = (int(blockIdx.x) / c.nbx) % c.nby;
-    c.bz0 = int(blockIdx.x) / (c.nbx * c.nby);
-    c.sx = int(gridDim.x) % c.nbx;
-    c.sy = (int(gridDim.x) / c.nbx) % c.nby;
-    c.sz = int(gridDim.x) / (c.nbx * c.nby);
-    c.ring = 0u;
-    c.target = 0ull;
-    c.set = 0;
-    if (c.tid < 64) {
-        sdiag[c.tid] = g.diag[c.tid];
-        srdiag[c.tid] = g.rdiag[c.tid];
-    }
-    if (c.tid == 0) {
-        sst = *A.st;
-        // every barrier of earlier launches was passed by the whole grid, so
-        // the count is a multiple of the grid size plus arrivals at this
-        // launch's first barrier (fewer than the grid: this block has not)
-        c.target = ld_acquire_gpu(&A.bar->count) / gridDim.x * gridDim.x;
-        for (int s = 0; s < NS; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], CONSUMER_WARPS);
-        }
-        fence_mbar_init();
-    }
-    __syncthreads();
-    rb200_trace* trace = blockIdx.x == 0 ? A.trace : nullptr;
-    const int plane = g.n[0] * g.n[1];
-    const int qb = c.tz * QPT;
-    bool ok = true;
-    int iters = 0;
-    for (;;) {
-        const int flags = sst.flags;
-        if (flags & F_DONE) break;
-        if (flags & F_NEED_TRUE) {
-            // ---------------------------------------------- phase 3: true residual
-            double* spare = sst.dsel ? A.d0 : A.d1;
-            Neu2 acc;
-            double gauge_sq = 0.0;  // t[0]^2 in the thread that holds cell 0
-            double mx = 0.0;
-            const bool mine_ok = run_bricks(
-                c, full, empty,
-                [&](const BrickWalk& w, int s) {
-                    const int x0 = w.x0(), y0 = w.y0(), k0 = w.k0();
-                    mbar_expect_tx(&full[s], PS::BYTES);
-                    tma_load_slab(smem + s * STAGE, &maps.p, x0 - 2, y0 - 1, k0 - 1, &full[s]);
-                },
-                [&](const BrickWalk& w, int s) {
-                    const double* sp = smem + s * STAGE;
-                    const Col col = column(g, c, w, qb);
-                    if (!col.own) return;
-                    double v[QPT + 2];
-#pragma unroll
-                    for (int u = 0; u < QPT + 2; ++u) v[u] = sp[col.e0 + (u - 1) * PS::PLANE];
-#pragma unroll
-                    for (int u = 0; u < QPT; ++u) {
-                        if (qb + u >= col.kend) break;
-                        const int e = col.e0 + u * PS::PLANE;
-                        const int cc = col.cc0 + u * plane;
-                        const double kp = row7(g, col.mxy, col.k0 + qb + u, v[u + 1], sp[e - 1], sp[e + 1],
-                                               sp[e - PS::SX], sp[e + PS::SX], v[u], v[u + 2]);
-                        const double t = __ldcg(A.b + cc) - kp;
-                        spare[cc] = t;
-                        (u & 1 ? acc.b : acc.a).add(t * t);
-                        if (cc == 0) gauge_sq = t * t;
-                        mx = fmax(mx, fabs(t));
-                    }
-                });
-            // |t|^2 and |t[1..]|^2 (the restart test of a seeded solve)
-            dd sums[2] = {acc.as_dd(), dd_add1(acc.as_dd(), -gauge_sq)};
-            double maxs[1] = {mx};
-            if (!(ok = reduce_grid<2, 1>(c, A, mine_ok, sums, maxs))) break;
-            if (c.tid == 0)
-                decide_true(&sst, trace, dd_value(sums[0]), dd_value(sums[1]), maxs[0], flags, g.volume);
-            __syncthreads();
-            continue;
-        }
-        if (flags & F_NEED_REPLACE) {
-            // ---------------------------------------------- phase 4: restart
-            const double* spare = sst.dsel ? A.d0 : A.d1;
-            Neu2 acc;
-            if (!c.producer) {
-                for (BrickWalk w(c); w.b < c.nbricks; w.next(c)) {
-                    const Col col = column(g, c, w, qb);
-                    if (!col.own) continue;
-#pragma unroll
-                    for (int u = 0; u < QPT; ++u) {
-                        if (qb + u >= col.kend) break;
-                        const int cc = col.cc0 + u * plane;
-                        const double rc = cc == 0 ? 0.0 : __ldcg(spare + cc);
-                        A.r[cc] = rc;
-                        if (cc == 0) {
-                            A.z[0] = 0.0;
-                            continue;
-                        }
-                        const int m = col.mxy | zmask(g, col.k0 + qb + u);
-                        const double zc = div_diag(rc, sdiag[m], srdiag[m]);
-                        A.z[cc] = zc;
-                        (u & 1 ? acc.b : acc.a).add(rc * zc);
-                    }
-                }
-            }
-            dd sums[1] = {acc.as_dd()};
-            double none[1] = {0.0};
-            if (!(ok = reduce_grid<1, 0>(c, A, true, sums, none))) break;
-            if (c.tid == 0) decide_rz(&sst, trace, dd_value(sums[0]), MODE_REPLACE);
-            __syncthreads();
-            continue;
-        }
-        if (flags & F_STOP) break;  // stopped without a pending check: nothing to do
-        if (iters >= A.budget) break;
-
-        // -------------------------------------------------- phase 1: direction + K d
-        {
-            const bool fresh = (flags & F_REPLACED) != 0;
-            const double beta = sst.beta;
-            const int dsel = sst.dsel;
-            double* __restrict__ dst = dsel ? A.d0 : A.d1;
-            const CUtensorMap* dmap = dsel ? &maps.d1 : &maps.d0;
-            Neu2 acc;
-            const bool mine_ok = run_bricks(
-                c, full, empty,
-                [&](const BrickWalk& w, int s) {
-                    const int x0 = w.x0(), y0 = w.y0(), k0 = w.k0();
-                    double* sz = smem + s * STAGE;
-                    mbar_expect_tx(&full[s], (fresh ? 1u : 2u) * PS::BYTES);
-                    tma_load_slab(sz, &maps.z, x0 - 2, y0 - 1, k0 - 1, &full[s]);
-                    if (!fresh) tma_load_slab(sz + PS::SIZE, dmap, x0 - 2, y0 - 1, k0 - 1, &full[s]);
-                },
-                [&](const BrickWalk& w, int s) {
-                    const double* sz = smem + s * STAGE;
-                    const double* sd = sz + PS::SIZE;
-                    const Col col = column(g, c, w, qb);
-                    if (!col.own) return;
-                    // straight-line cells (no per-cell branch) so that the
-                    // column's cells interleave. FRESH: d = z (after a
-                    // restart); FULL: the brick is whole in z; ZIN: it lies
-                    // strictly inside the box in z (no gauge cell, both z
-                    // neighbours everywhere).
-                    auto cells = [&](auto fresh_t, auto full_t, auto zin_t) {
-                        constexpr bool FRESH = decltype(fresh_t)::value;
-                        constexpr bool FULL = decltype(full_t)::value;
-                        constexpr bool ZIN = decltype(zin_t)::value;
-                        // the new direction at slab element e (src/pressure.rs:720-731)
-                        auto dn = [&](int e) { return FRESH ? sz[e] : sz[e] + beta * sd[e]; };
-                        double v[QPT + 2];
-#pragma unroll
-                        for (int u = 0; u < QPT + 2; ++u) v[u] = dn(col.e0 + (u - 1) * PS::PLANE);
-#pragma unroll
-                        for (int u = 0; u < QPT; ++u) {
-                            if (!FULL && qb + u >= col.kend) break;
-                            const int e = col.e0 + u * PS::PLANE;
-                            const int cc = col.cc0 + u * plane;
-                            const double kd = row7<ZIN>(g, col.mxy, col.k0 + qb + u, v[u + 1], dn(e - 1), dn(e + 1),
-                                                        dn(e - PS::SX), dn(e + PS::SX), v[u], v[u + 2]);
-                            const double qv = (!ZIN && cc == 0) ? 0.0 : kd;  // gauge row
-                            dst[cc] = v[u + 1];
-                            (u & 1 ? acc.b : acc.a).add(v[u + 1] * qv);
-                        }
-                    };
-                    using T = std::true_type;
-                    using F = std::false_type;
-                    const bool zin = col.k0 > 0 && col.k0 + PZC < g.n[2];
-                    if (fresh) {
-                        if (zin)
-                            cells(T{}, T{}, T{});
-                        else if (col.kend == PZC)
-                            cells(T{}, T{}, F{});
-                        else
-                            cells(T{}, F{}, F{});
-                    } else {
-                        if (zin)
-                            cells(F{}, T{}, T{});
-                        else if (col.kend == PZC)
-                            cells(F{}, T{}, F{});
-                        else
-                            cells(F{}, F{}, F{});
-                    }
-                });
-            dd sums[1] = {acc.as_dd()};
-            double none[1] = {0.0};
-            if (!(ok = reduce_grid<1, 0>(c, A, mine_ok, sums, none))) break;
-            if (c.tid == 0) decide_pass1(&sst, trace, dd_value(sums[0]), flags, dsel);
-            __syncthreads();
-            if (sst.flags & F_DONE) continue;
-        }
-        // -------------------------------------------------- phase 2: update + Jacobi
-        {
-            const int flags2 = sst.flags;
-            const double alpha = sst.alpha;
-            const int dsel = sst.dsel;
-            const CUtensorMap* dmap = dsel ? &maps.d1 : &maps.d0;
-            Neu2 acc_rr, acc_rz;
-            const bool mine_ok = run_bricks(
-                c, full, empty,
-                [&](const BrickWalk& w, int s) {
-                    const int x0 = w.x0(), y0 = w.y0(), k0 = w.k0();
-                    double* sd = smem + s * STAGE;
-                    mbar_expect_tx(&full[s], PS::BYTES + 2u * BOX_BYTES);
-                    tma_load_slab(sd, dmap, x0 - 2, y0 - 1, k0 - 1, &full[s]);
-                    tma_load_slab(sd + PS::SIZE, &maps.p_box, x0, y0, k0, &full[s]);
-                    tma_load_slab(sd + PS::SIZE + BOX, &maps.r_box, x0, y0, k0, &full[s]);
-                },
-                [&](const BrickWalk& w, int s) {
-                    const double* sd = smem + s * STAGE;
-                    const double* sp = sd + PS::SIZE;
-                    const double* sr = sp + BOX;
-                    const Col col = column(g, c, w, qb);
-                    if (!col.own) return;
-                    // straight-line cells; the rare quotient outside the
-                    // fast division's range is redone after the column.
-                    // Gauge row: p[0] + alpha d[0] = p[0] (d[0] = 0), and
-                    // r[0] = z[0] = 0 add nothing to the sums.
-                    auto cells = [&](auto full_t, auto zin_t) {
-                        constexpr bool FULL = decltype(full_t)::value;
-                        constexpr bool ZIN = decltype(zin_t)::value;
-                        double v[QPT + 2];
-                        unsigned slow = 0u;  // cells whose quotient is redone
-                        // ZIN: one diagonal for the whole column
-                        const int mz = col.mxy | 0x30;
-                        const double Dz = sdiag[mz], yz = srdiag[mz];
-#pragma unroll
-                        for (int u = 0; u < QPT + 2; ++u) v[u] = sd[col.e0 + (u - 1) * PS::PLANE];
-#pragma unroll
-                        for (int u = 0; u < QPT; ++u) {
-                            if (!FULL && qb + u >= col.kend) break;
-                            const int cc = col.cc0 + u * plane;
-                            const int e = col.e0 + u * PS::PLANE;
-                            const int k = col.k0 + qb + u;
-                            const double qv = row7<ZIN>(g, col.mxy, k, v[u + 1], sd[e - 1], sd[e + 1],
-                                                        sd[e - PS::SX], sd[e + PS::SX], v[u], v[u + 2]);
-                            const int bi = col.bi0 + u * (TX * TY);
-                            A.p[cc] = sp[bi] + alpha * v[u + 1];
-                            const double rc = (!ZIN && cc == 0) ? 0.0 : sr[bi] - alpha * qv;
-                            A.r[cc] = rc;
-                            (u & 1 ? acc_rr.b : acc_rr.a).add(rc * rc);
-                            const int m = ZIN ? mz : (col.mxy | zmask(g, k));
-                            const double y = ZIN ? yz : srdiag[m];
-                            const double zc = div_diag_fast(rc, ZIN ? Dz : sdiag[m], y);
-                            const bool fast = ZIN ? div_diag_range_ok(rc) : div_diag_fast_ok(rc, y);
-                            slow |= fast ? 0u : 1u << u;
-                            A.z[cc] = zc;
-                            (u & 1 ? acc_rz.b : acc_rz.a).add(fast ? rc * zc : 0.0);
-                        }
-                        if (ZIN && yz == 0.0) slow = (1u << QPT) - 1u;
-                        if (slow) {
-                            // r / D by division; the residual is re-read
-                            // from this thread's own store above
-#pragma unroll
-                            for (int u = 0; u < QPT; ++u) {
-                                if (!FULL && qb + u >= col.kend) break;
-                                if (!((slow >> u) & 1u)) continue;
-                                const int cc = col.cc0 + u * plane;
-                                const double rc = A.r[cc];
-                                const double zc = rc / sdiag[col.mxy | zmask(g, col.k0 + qb + u)];
-                                A.z[cc] = zc;
-                                (u & 1 ? acc_rz.b : acc_rz.a).add(rc * zc);
-                            }
-                        }
-                    };
-                    using T = std::true_type;
-                    using F = std::false_type;
-                    if (col.k0 > 0 && col.k0 + PZC < g.n[2])
-                        cells(T{}, T{});
-                    else if (col.kend == PZC)
-                        cells(T{}, F{});
-                    else
-                        cells(F{}, F{});
-                });
-            dd sums[2] = {acc_rr.as_dd(), acc_rz.as_dd()};
-            double none[1] = {0.0};
-            if (!(ok = reduce_grid<2, 0>(c, A, mine_ok, sums, none))) break;
-            if (c.tid == 0) decide_pass2(&sst, trace, dd_value(sums[0]), dd_value(sums[1]), flags2, true);
-            __syncthreads();
-            ++iters;
-        }
-    }
-    if (!ok) {
-        if (c.tid == 0) {
-            atomicExch(&A.bar->abort, 1u);
-            A.st->status = RB200_EXECUTION;
-            A.st->flags = A.st->flags | F_DONE | F_STOP;
-        }
-        return;
-    }
-    if (blockIdx.x == 0 && c.tid == 0) *A.st = sst;
+// Neighbour sum of the red-black SGS passes: init + w * z over the existing
+// neighbours, in the order X lower, X upper, Y lower, Y upper, Z lower, Z upper
+// (the order of k_rbsgs_black / k_rbsgs_red_dot), from the z slab.
+__device__ __forceinline__ double rb_sum(const GridDev& g, const double* sz, int e, int m, double init) {
+    double y = init;
+    if (m & 1) y += g.weight[0] * sz[e - 1];
+    if (m & 2) y += g.weight[0] * sz[e + 1];
+    if (m & 4) y += g.weight[1] * sz[e - PS::SX];
+    if (m & 8) y += g.weight[1] * sz[e + PS::SX];
+    if (m & 16) y += g.weight[2] * sz[e - PS::PLANE];
+    if (m & 32) y += g.weight[2] * sz[e + PS::PLANE];
+    return y;
 }
+
+// Red-black SGS after r and the red y = r/D are stored: a barrier (unless the
+// caller's reduction just was one), the black pass z_b = (r_b + sum w y_nb)/D_b,
+// a barrier, the red pass z_r = y_r + (sum w z_nb)/D_r with r.z, and its
+// decision (`mode`). Every block runs it, so the barrier sequence stays the
+// same everywhere.
+__device__ __forceinline__ bool rb_apply(Ctx& c, const PersistArgs& A, const TmaMaps& maps, uint64_t* full,
+                                         uint64_t* empty, double* smem, const double* sdiag, const double* srdiag,
+                                         SolveState& sst, rb200_trace* trace, int qb, int mode, bool barrier_first) {
+    const GridDev& g = A.g;
+    const int plane = g.n[0] * g.n[1];
+    auto issue = [&](const BrickWalk& w, int s) {
+        const int x0 = w.x0(), y0 = w.y0(), k0 = w.k0();
+        double* sz = smem + s * STAGE;
+        mbar_expect_tx(&full[s], PS::BYTES + BOX_BYTES);
+        tma_load_slab(sz, &maps.z, x0 - 2, y0 - 1, k0 - 1, &full[s]);
+        tma_load_slab(sz + PS::SIZE, &maps.r_box, x0, y0, k0, &full[s]);
+    };
+    double none_m[1] = {0.0};
+    // the red y of every block (after the update phase its own reduction was that barrier)
+    if (barrier_first && !grid_barrier(c, A.bar)) return false;
+    bool mine_ok = run_bricks(c, full, empty, issue, [&](const BrickWalk& w, int s) {
+        const double* sz = smem + s * STAGE;
+        const double* sr = sz + PS::SIZE;
+        const Col col = column(g, c, w, qb);
+        if (!col.own) return;
+#pragma unroll
+        for (int u = 0; u < QPT; ++u) {
+            if (qb + u >= col.kend) break;
+            const int k = col.k0 + qb + u;
+            if (((col.par + k) & 1) == 0) continue;  // red
+            const int m = col.mxy | zmask(g, k);
+            const int e = col.e0 + u * PS::PLANE;
+            A.z[col.cc0 + u * plane] =
+                div_diag(rb_sum(g, sz, e, m, sr[col.bi0 + u * (TX * TY)]), sdiag[m], srdiag[m]);
+        }
+    });
+    if (!__syncthreads_and(mine_ok) || !grid_barrier(c, A.bar)) return false;  // every black z
+    Neu2 acc;
+    mine_ok = run_bricks(c, full, empty, issue, [&](const BrickWalk& w, int s) {
+        const double* sz = smem + s * STAGE;
+        const double* sr = sz + PS::SIZE;
+        const Col col = column(g, c, w, qb);
+        if (!col.own) return;
+#pragma unroll
+        for (int u = 0; u < QPT; ++u) {
+            if (qb + u >= col.kend) break;
+            const int k = col.k0 + qb + u;
+            const int cc = col.cc0 + u * plane;
+            if (cc == 0) continue;  // z[0] = 0 is kept
+            const int e = col.e0 + u * PS::PLANE;
+            double zc = sz[e];
+            if (((col.par + k) & 1) == 0) {
+                const int m = col.mxy | zmask(g, k);
+                zc = zc + div_diag(rb_sum(g, sz, e, m, 0.0), sdiag[m], srdiag[m]);
+                A.z[cc] = zc;
+            }
+            (u & 1 ? acc.b : acc.a).add(sr[col.bi0 + u * (TX * TY)] * zc);
+        }
+    });
+    dd sums[1] = {acc.as_dd()};
+    if (!reduce_grid<1, 0>(c, A, mine_ok, sums, none_m)) return false;
+    if (c.tid == 0) decide_rz(&sst, trace, dd_value(sums[0]), mode);
+    __syncthreads();
+    return true;
+}
+
+#define RB_PERSIST_PRE 0
+#define RB_PERSIST_KERNEL k_jacobi_persistent
+#include "persist_kernel.inc"
+#undef RB_PERSIST_KERNEL
+#undef RB_PERSIST_PRE
+#define RB_PERSIST_PRE 1
+#define RB_PERSIST_KERNEL k_rbsgs_persistent
+#include "persist_kernel.inc"
+#undef RB_PERSIST_KERNEL
+#undef RB_PERSIST_PRE
 
 }  // namespace
 
@@ -637,11 +427,15 @@ int persistent_setup(const GridDev& g, int* blocks) {
     *blocks = 0;
     RB200_CUDA(cudaFuncSetAttribute(k_jacobi_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     int(kPersistSmem)));
-    int dev = 0, sms = 0, coop = 0, per_sm = 0;
+    RB200_CUDA(cudaFuncSetAttribute(k_rbsgs_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(kPersistSmem)));
+    int dev = 0, sms = 0, coop = 0, per_sm = 0, per_sm_rb = 0;
     RB200_CUDA(cudaGetDevice(&dev));
     RB200_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     RB200_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     RB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi_persistent, PT, kPersistSmem));
+    RB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_rb, k_rbsgs_persistent, PT, kPersistSmem));
+    if (per_sm_rb < per_sm) per_sm = per_sm_rb;
     if (!coop || per_sm < 1) return RB200_OK;
     const int nbricks = ((g.n[0] + TX - 1) / TX) * ((g.n[1] + TY - 1) / TY) * ((g.n[2] + PZC - 1) / PZC);
     int cap = sms * per_sm;
@@ -654,7 +448,7 @@ size_t persistent_partial_doubles(int blocks) { return 2 * size_t(blocks) * PSTR
 
 cudaError_t launch_persistent(const GridDev& g, SolveState* st, const double* b, double* p, double* r, double* z,
                               double* d0, double* d1, double* part, GridBarrier* bar, rb200_trace* trace,
-                              const TmaMaps& maps, int blocks, int budget, cudaStream_t s) {
+                              const TmaMaps& maps, int blocks, int budget, cudaStream_t s, int pre) {
     PersistArgs A{g, st, b, p, r, z, d0, d1, part, bar, trace, budget};
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(unsigned(blocks), 1, 1);
@@ -666,7 +460,8 @@ cudaError_t launch_persistent(const GridDev& g, SolveState* st, const double* b,
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_jacobi_persistent, A, maps);
+    return pre == 1 ? cudaLaunchKernelEx(&cfg, k_rbsgs_persistent, A, maps)
+                    : cudaLaunchKernelEx(&cfg, k_jacobi_persistent, A, maps);
 }
 
 }  // namespace rb200
