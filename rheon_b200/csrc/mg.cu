@@ -816,7 +816,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int 
 // no FP64 copy of z is stored. One warp per cell row, lanes along x.
 __global__ void __launch_bounds__(MG_THREADS) k_mg_pass1(GridDev g, MgLevelDev L, SolveState* st, double* d0,
                                                          double* d1, double* __restrict__ q, Partials part,
-                                                         rb200_trace* trace) {
+                                                         rb200_trace* trace, int kc_len) {
     __shared__ BlockReduce<1, 0> red;
     const int flags = st->flags;
     if (flags & F_STOP) return;
@@ -852,39 +852,57 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_pass1(GridDev g, MgLevelDev L
                 o[3] = zc[3] + beta * b2.y;
             }
         };
-        for (int rw = W.w0; rw < rows; rw += W.nw) {
-            const int j = rw % g.n[1], k = rw / g.n[1];
-            const int base = n0 * rw;
-            for (int qd = W.lane; qd < quads; qd += 32) {
-                const int i0 = 4 * qd;
-                const int c0 = base + i0;
-                double dc[4], ym[4] = {0, 0, 0, 0}, yp[4] = {0, 0, 0, 0}, zm[4] = {0, 0, 0, 0}, zp[4] = {0, 0, 0, 0};
-                dn4(c0, dc);
+        // A warp takes a line of up to 32 quads of row j and marches along z
+        // over kc_len rows, keeping the z-neighbour rows in registers: each
+        // row of d and x is loaded once for the line plus once per y
+        // neighbour row, instead of once per stencil row that reads it.
+        const int qsegs = (quads + 31) >> 5;
+        const int kcs = (g.n[2] + kc_len - 1) / kc_len;
+        const int lines = qsegs * g.n[1] * kcs;
+        for (int line = W.w0; line < lines; line += W.nw) {
+            const int qseg = line % qsegs, t = line / qsegs;
+            const int j = t % g.n[1], k_begin = (t / g.n[1]) * kc_len;
+            const int k_end = min(g.n[2], k_begin + kc_len);
+            const int qd = qseg * 32 + W.lane;
+            if (qd >= quads) continue;
+            const int i0 = 4 * qd;
+            double prev[4] = {0, 0, 0, 0}, cur[4], next[4];
+            const int base0 = n0 * (j + g.n[1] * k_begin) + i0;
+            if (k_begin > 0) dn4(base0 - sz, prev);
+            dn4(base0, cur);
+            for (int k = k_begin; k < k_end; ++k) {
+                const int c0 = base0 + (k - k_begin) * sz;
+                double ym[4] = {0, 0, 0, 0}, yp[4] = {0, 0, 0, 0};
+#pragma unroll
+                for (int e = 0; e < 4; ++e) next[e] = 0.0;
+                if (k + 1 < g.n[2]) dn4(c0 + sz, next);
                 if (j > 0) dn4(c0 - sy, ym);
                 if (j + 1 < g.n[1]) dn4(c0 + sy, yp);
-                if (k > 0) dn4(c0 - sz, zm);
-                if (k + 1 < g.n[2]) dn4(c0 + sz, zp);
                 const double xl = i0 > 0 ? dn(c0 - 1) : 0.0;
                 const double xr = i0 + 4 < n0 ? dn(c0 + 4) : 0.0;
                 double qq[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     Neigh v;
-                    v.c = dc[e];
-                    v.xm = e == 0 ? xl : dc[e - 1];
-                    v.xp = e == 3 ? xr : dc[e + 1];
+                    v.c = cur[e];
+                    v.xm = e == 0 ? xl : cur[e - 1];
+                    v.xp = e == 3 ? xr : cur[e + 1];
                     v.ym = ym[e];
                     v.yp = yp[e];
-                    v.zm = zm[e];
-                    v.zp = zp[e];
+                    v.zm = prev[e];
+                    v.zp = next[e];
                     qq[e] = (c0 + e == 0) ? 0.0 : apply_row(g, i0 + e, j, k, v);
                 }
-                *reinterpret_cast<double2*>(dst + c0) = make_double2(dc[0], dc[1]);
-                *reinterpret_cast<double2*>(dst + c0 + 2) = make_double2(dc[2], dc[3]);
+                *reinterpret_cast<double2*>(dst + c0) = make_double2(cur[0], cur[1]);
+                *reinterpret_cast<double2*>(dst + c0 + 2) = make_double2(cur[2], cur[3]);
                 *reinterpret_cast<double2*>(q + c0) = make_double2(qq[0], qq[1]);
                 *reinterpret_cast<double2*>(q + c0 + 2) = make_double2(qq[2], qq[3]);
 #pragma unroll
-                for (int e = 0; e < 4; ++e) acc.add(dc[e] * qq[e]);
+                for (int e = 0; e < 4; ++e) {
+                    acc.add(cur[e] * qq[e]);
+                    prev[e] = cur[e];
+                    cur[e] = next[e];
+                }
             }
         }
     } else
@@ -1022,7 +1040,14 @@ int Multigrid::enqueue_pass1(const GridDev& g, void* state, double* d0, double* 
                              rb200_trace* trace, cudaStream_t s) const {
     int pb = row_blocks(levels_[0]);
     if (pb > 148 * 8) pb = 148 * 8;  // reduction partials capacity
-    k_mg_pass1<<<pb, MG_THREADS, 0, s>>>(g, levels_[0], static_cast<SolveState*>(state), d0, d1, q, part, trace);
+    // the z-march length of the quad path: long where there are enough lines
+    // for every warp of the grid, short otherwise
+    const int quads = g.n[0] / 4, qsegs = (quads + 31) / 32;
+    const int warps = pb * (MG_THREADS / 32);
+    int kc_len = 16;
+    while (kc_len > 2 && qsegs * g.n[1] * ((g.n[2] + kc_len - 1) / kc_len) < warps) kc_len /= 2;
+    k_mg_pass1<<<pb, MG_THREADS, 0, s>>>(g, levels_[0], static_cast<SolveState*>(state), d0, d1, q, part, trace,
+                                         kc_len);
     return 1;
 }
 
