@@ -462,51 +462,157 @@ __global__ void __launch_bounds__(EW) k_mg_update(GridDev g, SolveState* st, dou
 // depends only on its lower (upper) neighbours, so any order that respects
 // those dependencies computes the reference's lexicographic sweep bit for bit
 // (the reference's own tiled wavefront, src/sgs.rs:56-104, uses the same
-// fact). Here a launch handles one diagonal wave of 8^3 tiles
-// (tx + ty + tz = wave) and a block walks its tile's hyperplanes
-// lx + ly + lz = l with a barrier between them.
+// fact).
+//
+// One launch runs both sweeps over 8^3 tiles. A block takes the next slot of
+// a queue (slots 0..T-1: the tiles in wave order tx + ty + tz ascending;
+// T..2T-1: the same list backwards for the reverse sweep), waits until the
+// tiles it depends on are done (forward: the lower x, y, z neighbour tiles;
+// reverse: the upper ones, and for the last tile of the forward order its own
+// forward sweep), stages its tile and the one-cell halo it reads in shared
+// memory, walks the tile's hyperplanes lx + ly + lz = l with a block barrier
+// between them, stores the tile and publishes its state word (release). A
+// slot only waits for slots taken before it, by blocks that are running, so
+// the queue cannot deadlock whatever the number of resident blocks. The
+// reverse sweep of a tile starts after the forward sweep of every tile: its
+// upper neighbours' reverse sweeps come after the forward sweep of the last
+// tile, which comes after every other forward sweep.
+//
+// Every wait is bounded: a wait that runs out raises the abort word, which
+// ends every other wait, and marks the solve as failed (execution error).
 constexpr int SGS_T = 8;
+constexpr int SGS_THREADS = SGS_T * SGS_T * SGS_T;
+constexpr unsigned kSgsSpins = 1u << 22;
 
-__global__ void __launch_bounds__(SGS_T * SGS_T * SGS_T) k_sgs_wave(GridDev g, SolveState* st,
-                                                                    const double* __restrict__ r, double* z,
-                                                                    int wave, int reverse, int mode) {
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+// Thread 0: wait until tile `dep` holds a state >= need.
+__device__ __forceinline__ bool sgs_wait(const unsigned* ctl, int dep, unsigned need) {
+    unsigned n = 0;
+    while (ld_acquire_u32(ctl + 2 + dep) < need) {
+        ++n;
+        if ((n & 7u) == 0u && (*(volatile const unsigned*)(ctl + 1) != 0u || n > kSgsSpins)) return false;
+        if (n > 256u) __nanosleep(64);
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(SGS_THREADS) k_sgs_flow(GridDev g, SolveState* st,
+                                                          const double* __restrict__ r, double* z, SgsFlow f,
+                                                          int mode) {
+    __shared__ double zs[SGS_T + 2][SGS_T + 2][SGS_T + 2];  // the tile at [1..8], its halo at 0 and 9
+    __shared__ int s_slot, s_ok;
     if (!gate(st->flags, mode)) return;
-    const int ntz = (g.n[2] + SGS_T - 1) / SGS_T;
-    const int tx = blockIdx.x, ty = blockIdx.y, tz = wave - tx - ty;
-    if (tz < 0 || tz >= ntz) return;
+    const int nt0 = (g.n[0] + SGS_T - 1) / SGS_T, nt1 = (g.n[1] + SGS_T - 1) / SGS_T,
+              nt2 = (g.n[2] + SGS_T - 1) / SGS_T;
     const int lx = threadIdx.x % SGS_T, ly = (threadIdx.x / SGS_T) % SGS_T, lz = threadIdx.x / (SGS_T * SGS_T);
-    const int i = tx * SGS_T + lx, j = ty * SGS_T + ly, k = tz * SGS_T + lz;
-    const bool in = i < g.n[0] && j < g.n[1] && k < g.n[2];
-    const int c = in ? cell_idx(g, i, j, k) : 0;
-    const int sy = g.n[0], sz = g.n[0] * g.n[1];
     const int mine = lx + ly + lz;
-    for (int step = 0; step < 3 * SGS_T - 2; ++step) {
-        const int l = reverse ? 3 * SGS_T - 3 - step : step;
-        if (in && mine == l && c != 0) {
-            const double D = diag_at(g, i, j, k);
-            if (!reverse) {
-                double value = r[c];
-                if (i > 0) value += g.weight[0] * z[c - 1];
-                if (j > 0) value += g.weight[1] * z[c - sy];
-                if (k > 0) value += g.weight[2] * z[c - sz];
-                z[c] = value / D;
-            } else {
-                double correction = 0.0;
-                if (i + 1 < g.n[0]) correction += g.weight[0] * z[c + 1];
-                if (j + 1 < g.n[1]) correction += g.weight[1] * z[c + sy];
-                if (k + 1 < g.n[2]) correction += g.weight[2] * z[c + sz];
-                z[c] = z[c] + correction / D;
-            }
+    const int sy = g.n[0], sz = g.n[0] * g.n[1];
+    const int slots = 2 * f.ntiles;
+    if (threadIdx.x == 0) s_slot = int(atomicAdd(f.ctl, 1u));
+    __syncthreads();
+    int slot = s_slot;
+    while (slot < slots) {
+        const bool reverse = slot >= f.ntiles;
+        const int tile = f.order[reverse ? slots - 1 - slot : slot];
+        const int tx = tile % nt0, ty = (tile / nt0) % nt1, tz = tile / (nt0 * nt1);
+        const int i = tx * SGS_T + lx, j = ty * SGS_T + ly, k = tz * SGS_T + lz;
+        const bool in = i < g.n[0] && j < g.n[1] && k < g.n[2];
+        const int c = in ? cell_idx(g, i, j, k) : 0;
+        double rv = 0.0, D = 1.0, y = 0.0;
+        if (in) {
+            const int m = diag_mask(g, i, j, k);
+            D = g.diag[m];
+            y = g.rdiag[m];
+            if (!reverse) rv = r[c];
+        }
+        if (threadIdx.x == 0) {
+            const int sx = 1, sty = nt0, stz = nt0 * nt1;
+            bool ok;
+            if (!reverse)
+                ok = (tx == 0 || sgs_wait(f.ctl, tile - sx, 1u)) && (ty == 0 || sgs_wait(f.ctl, tile - sty, 1u)) &&
+                     (tz == 0 || sgs_wait(f.ctl, tile - stz, 1u));
+            else if (tx + 1 == nt0 && ty + 1 == nt1 && tz + 1 == nt2)
+                ok = sgs_wait(f.ctl, tile, 1u);  // the last tile of the forward order
+            else
+                ok = (tx + 1 == nt0 || sgs_wait(f.ctl, tile + sx, 2u)) &&
+                     (ty + 1 == nt1 || sgs_wait(f.ctl, tile + sty, 2u)) &&
+                     (tz + 1 == nt2 || sgs_wait(f.ctl, tile + stz, 2u));
+            s_ok = ok;
         }
         __syncthreads();
+        if (!s_ok) {
+            if (threadIdx.x == 0) {
+                atomicExch(f.ctl + 1, 1u);
+                st->status = RB200_EXECUTION;
+                st->flags = (st->flags | F_DONE | F_STOP) & ~F_NEED_REPLACE;
+            }
+            return;
+        }
+        double* const me = &zs[lz + 1][ly + 1][lx + 1];
+        if (!reverse) {
+            if (in) {
+                if (c == 0) *me = __ldcg(z);  // the gauge row keeps its value
+                if (lx == 0 && i > 0) zs[lz + 1][ly + 1][0] = __ldcg(z + c - 1);
+                if (ly == 0 && j > 0) zs[lz + 1][0][lx + 1] = __ldcg(z + c - sy);
+                if (lz == 0 && k > 0) zs[0][ly + 1][lx + 1] = __ldcg(z + c - sz);
+            }
+            __syncthreads();
+            for (int l = 0; l < 3 * SGS_T - 2; ++l) {
+                if (in && mine == l && c != 0) {
+                    double value = rv;
+                    if (i > 0) value += g.weight[0] * zs[lz + 1][ly + 1][lx];
+                    if (j > 0) value += g.weight[1] * zs[lz + 1][ly][lx + 1];
+                    if (k > 0) value += g.weight[2] * zs[lz][ly + 1][lx + 1];
+                    *me = div_diag(value, D, y);
+                }
+                __syncthreads();
+            }
+        } else {
+            if (in) {
+                *me = __ldcg(z + c);
+                if (lx == SGS_T - 1 && i + 1 < g.n[0]) zs[lz + 1][ly + 1][SGS_T + 1] = __ldcg(z + c + 1);
+                if (ly == SGS_T - 1 && j + 1 < g.n[1]) zs[lz + 1][SGS_T + 1][lx + 1] = __ldcg(z + c + sy);
+                if (lz == SGS_T - 1 && k + 1 < g.n[2]) zs[SGS_T + 1][ly + 1][lx + 1] = __ldcg(z + c + sz);
+            }
+            __syncthreads();
+            for (int l = 3 * SGS_T - 3; l >= 0; --l) {
+                if (in && mine == l && c != 0) {
+                    double correction = 0.0;
+                    if (i + 1 < g.n[0]) correction += g.weight[0] * zs[lz + 1][ly + 1][lx + 2];
+                    if (j + 1 < g.n[1]) correction += g.weight[1] * zs[lz + 1][ly + 2][lx + 1];
+                    if (k + 1 < g.n[2]) correction += g.weight[2] * zs[lz + 2][ly + 1][lx + 1];
+                    *me = *me + div_diag(correction, D, y);
+                }
+                __syncthreads();
+            }
+        }
+        if (in && c != 0) __stcg(z + c, *me);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            st_release_u32(f.ctl + 2 + tile, reverse ? 2u : 1u);
+            s_slot = int(atomicAdd(f.ctl, 1u));
+        }
+        __syncthreads();
+        slot = s_slot;
     }
 }
 
 // r.z after a lexicographic SGS application, then the preconditioner decision.
 __global__ void __launch_bounds__(EW) k_sgs_dot(GridDev g, SolveState* st, const double* __restrict__ r,
                                                 const double* __restrict__ z, int mode, Partials part,
-                                                rb200_trace* trace) {
+                                                rb200_trace* trace, unsigned* sgs_ctl, int sgs_words) {
     __shared__ BlockReduce<1, 0> sm;
+    // the sweep kernel before this one has ended: its queue starts over
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < sgs_words; t += gridDim.x * blockDim.x) sgs_ctl[t] = 0u;
     if (!gate(st->flags, mode)) return;
     Neu acc;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x)
@@ -684,6 +790,7 @@ struct Bufs {
     Partials part;
     rb200_trace* trace;
     TmaMaps maps;
+    SgsFlow sgs{};
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
@@ -743,17 +850,12 @@ static TmaMaps make_maps(const GridDev& g, const double* z, const double* d0, co
     return m;
 }
 
-// One lexicographic SGS application: forward waves, reverse waves, r.z.
+// One lexicographic SGS application: both sweeps in one launch, then r.z.
 static int launch_sgs(const GridDev& g, const Bufs& B, int mode, cudaStream_t s) {
-    const int nt[3] = {(g.n[0] + SGS_T - 1) / SGS_T, (g.n[1] + SGS_T - 1) / SGS_T, (g.n[2] + SGS_T - 1) / SGS_T};
-    const int waves = nt[0] + nt[1] + nt[2] - 2;
-    const dim3 grid(nt[0], nt[1]);
-    for (int w = 0; w < waves; ++w)
-        k_sgs_wave<<<grid, SGS_T * SGS_T * SGS_T, 0, s>>>(g, B.st, B.r, B.z, w, 0, mode);
-    for (int w = waves - 1; w >= 0; --w)
-        k_sgs_wave<<<grid, SGS_T * SGS_T * SGS_T, 0, s>>>(g, B.st, B.r, B.z, w, 1, mode);
-    k_sgs_dot<<<ew_blocks(g.cells), EW, 0, s>>>(g, B.st, B.r, B.z, mode, B.part, B.trace);
-    return 2 * waves + 1;
+    k_sgs_flow<<<B.sgs.blocks, SGS_THREADS, 0, s>>>(g, B.st, B.r, B.z, B.sgs, mode);
+    k_sgs_dot<<<ew_blocks(g.cells), EW, 0, s>>>(g, B.st, B.r, B.z, mode, B.part, B.trace, B.sgs.ctl,
+                                                B.sgs.ntiles + 2);
+    return 2;
 }
 
 // Initial residual and preconditioned start (src/pressure.rs:603-650).
@@ -885,6 +987,8 @@ PcgSolver::~PcgSolver() {
     cudaFree(d_trace_);
     cudaFree(gbar_);
     cudaFree(ppart_);
+    cudaFree(const_cast<int*>(sgs_.order));
+    cudaFree(sgs_.ctl);
     if (h_st_) cudaFreeHost(h_st_);
 }
 
@@ -951,6 +1055,36 @@ static bool persistent_graphs_supported(PcgSolver& solver) {
     return supported;
 }
 
+// The lexicographic SGS queue: tile ids in wave order, the zeroed state
+// words, and the sweep kernel's resident block count.
+int PcgSolver::sgs_setup() {
+    const int nt0 = (g_.n[0] + SGS_T - 1) / SGS_T, nt1 = (g_.n[1] + SGS_T - 1) / SGS_T,
+              nt2 = (g_.n[2] + SGS_T - 1) / SGS_T;
+    std::vector<int> order;
+    order.reserve(size_t(nt0) * nt1 * nt2);
+    for (int w = 0; w <= nt0 + nt1 + nt2 - 3; ++w)
+        for (int tz = 0; tz < nt2; ++tz)
+            for (int ty = 0; ty < nt1; ++ty) {
+                const int tx = w - ty - tz;
+                if (tx >= 0 && tx < nt0) order.push_back(tx + nt0 * (ty + nt1 * tz));
+            }
+    sgs_.ntiles = int(order.size());
+    int* d_order = nullptr;
+    RB200_CUDA(cudaMalloc(&d_order, order.size() * sizeof(int)));
+    sgs_.order = d_order;
+    RB200_CUDA(cudaMalloc(&sgs_.ctl, (order.size() + 2) * sizeof(unsigned)));
+    bytes_ += order.size() * sizeof(int) + (order.size() + 2) * sizeof(unsigned);
+    RB200_CUDA(cudaMemcpyAsync(d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
+    RB200_CUDA(cudaMemsetAsync(sgs_.ctl, 0, (order.size() + 2) * sizeof(unsigned), stream_));
+    RB200_CUDA(cudaStreamSynchronize(stream_));
+    int dev = 0, sms = 0, per_sm = 0;
+    RB200_CUDA(cudaGetDevice(&dev));
+    RB200_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    RB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sgs_flow, SGS_THREADS, 0));
+    sgs_.blocks = int(std::min<long long>(2ll * sgs_.ntiles, std::max(1ll, (long long)sms * per_sm)));
+    return RB200_OK;
+}
+
 int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
     g_ = g;
     method_ = method;
@@ -985,7 +1119,8 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
     RB200_CUDA(cudaMallocHost(&h_st_, 2 * sizeof(SolveState)));
     for (auto& e : ev_) RB200_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     maps_ = make_maps(g, z_, d_[0], d_[1], p_, r_);
-    chunk_ = (method == RB200_MG_MIXED || method == RB200_SGS_PCG_V1) ? 4 : (g.cells >= (1 << 20) ? 32 : 16);
+    if (method == RB200_SGS_PCG_V1 && (rc = sgs_setup())) return rc;
+    chunk_ = method == RB200_MG_MIXED ? 4 : (g.cells >= (1 << 20) ? 32 : 16);
     // RB200_PERSISTENT=0 in the environment keeps the per-pass kernels (a
     // diagnostic switch: both paths compute the same iteration).
     const char* persist_env = std::getenv("RB200_PERSISTENT");
@@ -1028,7 +1163,7 @@ int PcgSolver::set_trace(rb200_trace* host, size_t capacity) {
 
 // One chunk: `chunk_` iterations, then the gated true-residual and restart.
 int PcgSolver::capture_chunk() {
-    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_};
+    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_, sgs_};
     const Multigrid* mg = method_ == RB200_MG_MIXED ? &mg_ : nullptr;
     cudaGraph_t graph = nullptr;
     RB200_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -1090,7 +1225,7 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
     if (d_trace_) RB200_CUDA(cudaMemsetAsync(d_trace_, 0, trace_cap_ * sizeof(rb200_trace), stream_));
     RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), stream_));
     if (gbar_) RB200_CUDA(cudaMemsetAsync(gbar_, 0, sizeof(GridBarrier), stream_));
-    launches_ += uint64_t(launch_start(g_, method_, Bufs{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_},
+    launches_ += uint64_t(launch_start(g_, method_, Bufs{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_, sgs_},
                                        method_ == RB200_MG_MIXED ? &mg_ : nullptr, stream_));
     RB200_CUDA(cudaGetLastError());
     // The host copy of the state must be stable before the chunk copies reuse
@@ -1145,7 +1280,7 @@ int PcgSolver::enqueue_reset(const double* dt_dev, const int* skip, const rb200_
     RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), s));
     if (gbar_) RB200_CUDA(cudaMemsetAsync(gbar_, 0, sizeof(GridBarrier), s));
     launches_ += 1;
-    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_};
+    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_, sgs_};
     launch_start(g_, method_, B, method_ == RB200_MG_MIXED ? &mg_ : nullptr, s);
     RB200_CUDA(cudaGetLastError());
     return RB200_OK;
@@ -1173,7 +1308,7 @@ int PcgSolver::enqueue_loop(cudaStream_t cs, cudaStream_t body_stream, const rb2
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     // The loop body: one chunk of iterations, the gated check, the condition.
     RB200_CUDA(cudaStreamBeginCaptureToGraph(body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_};
+    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_, sgs_};
     const Multigrid* mg = method_ == RB200_MG_MIXED ? &mg_ : nullptr;
     if (persist_blocks_) {
         RB200_CUDA(launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, d_trace_, maps_,

@@ -61,6 +61,17 @@ struct GridBarrier {
     unsigned pad;
 };
 
+// Work queue of the lexicographic SGS preconditioner (one launch per
+// application, forward and reverse sweep): the 8^3 tiles in wave order and
+// one state word per tile. The word block is zeroed by the r.z kernel that
+// follows every application.
+struct SgsFlow {
+    const int* order = nullptr;  // tile ids (tx + ntx (ty + nty tz)), waves tx + ty + tz ascending
+    unsigned* ctl = nullptr;     // [0] next queue slot, [1] abort, [2 + tile] 1 forward done, 2 reverse done
+    int ntiles = 0;
+    int blocks = 0;              // resident blocks of the sweep kernel
+};
+
 // Persistent PCG kernel (persist.cu); pre: 0 Jacobi, 1 red-black SGS.
 int persistent_setup(const GridDev& g, int* blocks);
 size_t persistent_partial_doubles(int blocks);
@@ -123,6 +134,7 @@ public:
 
 private:
     int capture_chunk();
+    int sgs_setup();
     int launch_chunk(int slot);
     int record_flags(int slot);
 
@@ -152,6 +164,7 @@ private:
     uint64_t launches_ = 0;
     int persist_blocks_ = 0;
     GridBarrier* gbar_ = nullptr;
+    SgsFlow sgs_{};
     double* ppart_ = nullptr;
 };
 

@@ -283,7 +283,8 @@ def compatible_rhs(g, seed=11, dtype=np.float64):
 # [64, 40, 24] and [96, 16, 12] take the TMA slab path (even nx, at least one
 # slab box in every direction); the others take the cp.async path.
 @pytest.mark.parametrize("method", list(EXACT))
-@pytest.mark.parametrize("counts", [[32, 32, 32], [17, 10, 9], [48, 20, 7], [64, 40, 24], [96, 16, 12]])
+@pytest.mark.parametrize("counts", [[32, 32, 32], [17, 10, 9], [48, 20, 7], [64, 40, 24], [96, 16, 12],
+                                    [72, 41, 57]])
 def test_pcg_per_iteration_parity(counts, method):
     """Every iteration's scalars and the iterates track the oracle to 1e-12."""
     g = R.GridGeometry(counts)
@@ -332,6 +333,25 @@ def test_jacobi_converged_solve_matches_oracle_iterations_and_report(counts, rel
     assert rep.iterations == ref.report.iterations
     assert abs(rep.true_residual_l2 - ref.report.true_residual_l2) <= 1e-12 * ref.report.true_residual_l2
     assert relerr(ws.pressure(), ref.pressure) <= 1e-12
+
+
+# Lexicographic SGS: the tile queue's sweeps reproduce the serial sweep, so a
+# converged solve takes the oracle's iteration count to the same pressure.
+@pytest.mark.parametrize("counts", [[40, 33, 28], [9, 70, 17]])
+def test_sgs_converged_solve_matches_oracle_iterations_and_report(counts):
+    g = R.GridGeometry(counts, [0.1, 0.12, 0.15])
+    rhs = compatible_rhs(g, seed=6)
+    s = S(1e-10, 0.0, 1.7976931348623157e308, 5000)
+    ref = O.solve_rhs(og(g), 1.0, O.SGS_PCG_V1, rhs, 0.25, O.settings(1e-10, 0.0, 1.7976931348623157e308, 5000))
+    assert ref.status == O.OK
+    ws = R.PressureWorkspace(g, 1 << 34, R.PressureImplementation.SGS_PCG_V1)
+    rep = ws.solve_rhs(R.PressureOperator(g, 1.0), rhs, 0.25, s)
+    assert rep.iterations == ref.report.iterations
+    assert abs(rep.true_residual_l2 - ref.report.true_residual_l2) <= 1e-12 * ref.report.true_residual_l2
+    assert relerr(ws.pressure(), ref.pressure) <= 1e-12
+    # a second solve on the same workspace starts from a clean tile queue
+    rep2 = ws.solve_rhs(R.PressureOperator(g, 1.0), rhs, 0.25, s)
+    assert rep2.iterations == rep.iterations and relerr(ws.pressure(), ref.pressure) <= 1e-12
 
 
 @pytest.mark.parametrize("counts", [[32, 32, 32], [64, 48, 40]])
