@@ -493,12 +493,17 @@ __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
 
-// Thread 0: wait until tile `dep` holds a state >= need.
-__device__ __forceinline__ bool sgs_wait(const unsigned* ctl, int dep, unsigned need) {
+// Wait until tile `dep` holds a state >= need; a wait that runs out raises
+// the abort word.
+__device__ __forceinline__ bool sgs_wait(unsigned* ctl, int dep, unsigned need) {
     unsigned n = 0;
     while (ld_acquire_u32(ctl + 2 + dep) < need) {
         ++n;
-        if ((n & 7u) == 0u && (*(volatile const unsigned*)(ctl + 1) != 0u || n > kSgsSpins)) return false;
+        if ((n & 7u) == 0u && *(volatile const unsigned*)(ctl + 1) != 0u) return false;
+        if (n > kSgsSpins) {
+            atomicExch(ctl + 1, 1u);
+            return false;
+        }
         if (n > 256u) __nanosleep(64);
     }
     return true;
@@ -520,6 +525,9 @@ __global__ void __launch_bounds__(SGS_THREADS) k_sgs_flow(GridDev g, SolveState*
     __syncthreads();
     int slot = s_slot;
     while (slot < slots) {
+        // the next slot is taken now, its atomic overlapping this tile
+        unsigned next_slot = 0;
+        if (threadIdx.x == 0) next_slot = atomicAdd(f.ctl, 1u);
         const bool reverse = slot >= f.ntiles;
         const int tile = f.order[reverse ? slots - 1 - slot : slot];
         const int tx = tile % nt0, ty = (tile / nt0) % nt1, tz = tile / (nt0 * nt1);
@@ -533,19 +541,26 @@ __global__ void __launch_bounds__(SGS_THREADS) k_sgs_flow(GridDev g, SolveState*
             y = g.rdiag[m];
             if (!reverse) rv = r[c];
         }
-        if (threadIdx.x == 0) {
-            const int sx = 1, sty = nt0, stz = nt0 * nt1;
-            bool ok;
-            if (!reverse)
-                ok = (tx == 0 || sgs_wait(f.ctl, tile - sx, 1u)) && (ty == 0 || sgs_wait(f.ctl, tile - sty, 1u)) &&
-                     (tz == 0 || sgs_wait(f.ctl, tile - stz, 1u));
-            else if (tx + 1 == nt0 && ty + 1 == nt1 && tz + 1 == nt2)
-                ok = sgs_wait(f.ctl, tile, 1u);  // the last tile of the forward order
-            else
-                ok = (tx + 1 == nt0 || sgs_wait(f.ctl, tile + sx, 2u)) &&
-                     (ty + 1 == nt1 || sgs_wait(f.ctl, tile + sty, 2u)) &&
-                     (tz + 1 == nt2 || sgs_wait(f.ctl, tile + stz, 2u));
-            s_ok = ok;
+        if (threadIdx.x < 32) {
+            // lanes 0, 1, 2 wait on the x, y, z neighbour tile at once
+            const int lane = threadIdx.x;
+            int dep = -1;
+            unsigned need = 1u;
+            if (lane < 3) {
+                const int t = lane == 0 ? tx : (lane == 1 ? ty : tz);
+                const int n = lane == 0 ? nt0 : (lane == 1 ? nt1 : nt2);
+                const int stride = lane == 0 ? 1 : (lane == 1 ? nt0 : nt0 * nt1);
+                if (!reverse) {
+                    if (t > 0) dep = tile - stride;
+                } else if (tx + 1 == nt0 && ty + 1 == nt1 && tz + 1 == nt2) {
+                    if (lane == 0) dep = tile;  // the last tile of the forward order: its own forward sweep
+                } else if (t + 1 < n) {
+                    dep = tile + stride;
+                    need = 2u;
+                }
+            }
+            const bool ok = __all_sync(0xffffffffu, dep < 0 || sgs_wait(f.ctl, dep, need));
+            if (lane == 0) s_ok = ok;
         }
         __syncthreads();
         if (!s_ok) {
@@ -599,7 +614,7 @@ __global__ void __launch_bounds__(SGS_THREADS) k_sgs_flow(GridDev g, SolveState*
         if (threadIdx.x == 0) {
             __threadfence();
             st_release_u32(f.ctl + 2 + tile, reverse ? 2u : 1u);
-            s_slot = int(atomicAdd(f.ctl, 1u));
+            s_slot = int(next_slot);
         }
         __syncthreads();
         slot = s_slot;

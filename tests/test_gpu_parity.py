@@ -335,6 +335,23 @@ def test_jacobi_converged_solve_matches_oracle_iterations_and_report(counts, rel
     assert relerr(ws.pressure(), ref.pressure) <= 1e-12
 
 
+def test_sgs_known_answer_first_iteration():
+    """src/pressure.rs:824-842: on the 2x2x1 grid r = [-12, 2, 4, 6] (row 0
+    eliminated) gives z = [0, 3.25, 4.25, 4.5] and r.z = 50.5. The first
+    iteration then sees d = z, q = A z = [2, 4, 1.5] on rows 1..3, d.q = 30.25
+    and alpha = 50.5 / 30.25, all exact but the last, which both sides round
+    once."""
+    g = R.GridGeometry([2, 2, 1])
+    ws = R.PressureWorkspace(g, 1 << 20, R.PressureImplementation.SGS_PCG_V1)
+    ws.set_trace(1)
+    with pytest.raises(R.PressureError) as e:
+        ws.solve_rhs(R.PressureOperator(g, 1.0), [-12.0, 2.0, 4.0, 6.0], 1.0, S(0.0, 0.0, 1.7976931348623157e308, 1))
+    assert e.value.kind == "IterationLimit" and e.value.iterations == 1
+    tr = ws.trace(1)
+    assert tr[0].curvature == 30.25 and tr[0].alpha == 50.5 / 30.25
+    assert ws.pressure().tolist() == [0.0, 3.25 * (50.5 / 30.25), 4.25 * (50.5 / 30.25), 4.5 * (50.5 / 30.25)]
+
+
 # Lexicographic SGS: the tile queue's sweeps reproduce the serial sweep, so a
 # converged solve takes the oracle's iteration count to the same pressure.
 @pytest.mark.parametrize("counts", [[40, 33, 28], [9, 70, 17]])
