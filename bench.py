@@ -28,6 +28,11 @@ import time
 
 import numpy as np
 
+# 32 hardware work queues instead of the default 8, so that the batched and
+# serving legs' per-instance streams run concurrently (read when the CUDA
+# context is created; a value already in the environment wins).
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
