@@ -1,5 +1,6 @@
 // FP32 geometric multigrid V(2,2) with an FP64 coarsest-grid solve; the
 // preconditioner of the mixed-precision pressure method (see mg.hpp).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -385,6 +386,109 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(MgLevelDev L, const do
     smooth_rows<false>(L, r0, color, first != 0, grid_warps());
 }
 
+// Two half-sweeps in one pass (colour c1, then the other colour) over a level
+// whose rows are a multiple of 4 long. A block takes a tile of PJ x PK rows
+// (j, k) at full row length: it relaxes colour c1 on the tile and the rows
+// around it (one row of halo in j and k) from the input x into shared memory,
+// exactly as smooth_rows_v4 does, then relaxes the other colour on the tile
+// from those rows and stores both colours to x_out. The input x is only read
+// and x_out only written, so tiles never see each other's partial results,
+// and the values equal two consecutive half-sweeps bit for bit (the same
+// operands in the same order). With `first` the correction starts from zero.
+constexpr int PJ = 4, PK = 4;
+constexpr int PAIR_ROWS = (PJ + 2) * (PK + 2);
+constexpr size_t kPairSmemMax = 200 * 1024;
+
+__global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pair(MgLevelDev L, float* __restrict__ x_out, int c1,
+                                                               int first, const SolveState* st, int mode) {
+    extern __shared__ float4 srow[];  // PAIR_ROWS rows of n0/4 quads
+    if (!mg_gate(st, mode)) return;
+    const int n0 = L.n[0], quads = n0 >> 2, n1 = L.n[1], n2 = L.n[2];
+    const int sy = n0, sz = n0 * n1;
+    const int tj = (n1 + PJ - 1) / PJ;
+    const int j0 = int(blockIdx.x % unsigned(tj)) * PJ, k0 = int(blockIdx.x / unsigned(tj)) * PK;
+    const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float* __restrict__ x = L.x;
+    for (int it = threadIdx.x; it < PAIR_ROWS * quads; it += blockDim.x) {
+        const int q = it % quads, hr = it / quads;
+        const int j = j0 - 1 + hr % (PJ + 2), k = k0 - 1 + hr / (PJ + 2);
+        if (j < 0 || j >= n1 || k < 0 || k >= n2) continue;
+        const int i0 = 4 * q;
+        const int c0 = i0 + n0 * (j + n1 * k);
+        const int par = (c1 + j + k) & 1;
+        const int myz = (int(j > 0) << 2) | (int(j + 1 < n1) << 3) | (int(k > 0) << 4) | (int(k + 1 < n2) << 5);
+        const float4 bq = *reinterpret_cast<const float4*>(L.b + c0);
+        float4 out;
+        if (first) {
+            out = z4;
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                const int e = par + 2 * t;
+                const int i = i0 + e;
+                f4put(out, e, f4get(bq, e) * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz]);
+            }
+        } else {
+            const float4 xc = *reinterpret_cast<const float4*>(x + c0);
+            const float xl = i0 > 0 ? x[c0 - 1] : 0.0f;
+            const float xr = i0 + 4 < n0 ? x[c0 + 4] : 0.0f;
+            const float4 ym = (myz & 4) ? *reinterpret_cast<const float4*>(x + c0 - sy) : z4;
+            const float4 yp = (myz & 8) ? *reinterpret_cast<const float4*>(x + c0 + sy) : z4;
+            const float4 zm = (myz & 16) ? *reinterpret_cast<const float4*>(x + c0 - sz) : z4;
+            const float4 zp = (myz & 32) ? *reinterpret_cast<const float4*>(x + c0 + sz) : z4;
+            out = xc;
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                const int e = par + 2 * t;
+                const int i = i0 + e;
+                float sum = f4get(bq, e);
+                if (i > 0) sum += L.w[0] * (e == 0 ? xl : f4get(xc, e - 1));
+                if (i + 1 < n0) sum += L.w[0] * (e == 3 ? xr : f4get(xc, e + 1));
+                if (myz & 4) sum += L.w[1] * f4get(ym, e);
+                if (myz & 8) sum += L.w[1] * f4get(yp, e);
+                if (myz & 16) sum += L.w[2] * f4get(zm, e);
+                if (myz & 32) sum += L.w[2] * f4get(zp, e);
+                f4put(out, e, sum * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz]);
+            }
+        }
+        srow[hr * quads + q] = out;
+    }
+    __syncthreads();
+    const float* __restrict__ sf = reinterpret_cast<const float*>(srow);
+    for (int it = threadIdx.x; it < PJ * PK * quads; it += blockDim.x) {
+        const int q = it % quads, tr = it / quads;
+        const int j = j0 + tr % PJ, k = k0 + tr / PJ;
+        if (j >= n1 || k >= n2) continue;
+        const int hr = (tr % PJ + 1) + (PJ + 2) * (tr / PJ + 1);
+        const int i0 = 4 * q;
+        const int c0 = i0 + n0 * (j + n1 * k);
+        const int par = (c1 + 1 + j + k) & 1;
+        const int myz = (int(j > 0) << 2) | (int(j + 1 < n1) << 3) | (int(k > 0) << 4) | (int(k + 1 < n2) << 5);
+        const float4 bq = *reinterpret_cast<const float4*>(L.b + c0);
+        const float4 xc = srow[hr * quads + q];
+        const float xl = i0 > 0 ? sf[hr * n0 + i0 - 1] : 0.0f;
+        const float xr = i0 + 4 < n0 ? sf[hr * n0 + i0 + 4] : 0.0f;
+        const float4 ym = (myz & 4) ? srow[(hr - 1) * quads + q] : z4;
+        const float4 yp = (myz & 8) ? srow[(hr + 1) * quads + q] : z4;
+        const float4 zm = (myz & 16) ? srow[(hr - (PJ + 2)) * quads + q] : z4;
+        const float4 zp = (myz & 32) ? srow[(hr + (PJ + 2)) * quads + q] : z4;
+        float4 out = xc;
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            const int e = par + 2 * t;
+            const int i = i0 + e;
+            float sum = f4get(bq, e);
+            if (i > 0) sum += L.w[0] * (e == 0 ? xl : f4get(xc, e - 1));
+            if (i + 1 < n0) sum += L.w[0] * (e == 3 ? xr : f4get(xc, e + 1));
+            if (myz & 4) sum += L.w[1] * f4get(ym, e);
+            if (myz & 8) sum += L.w[1] * f4get(yp, e);
+            if (myz & 16) sum += L.w[2] * f4get(zm, e);
+            if (myz & 32) sum += L.w[2] * f4get(zp, e);
+            f4put(out, e, sum * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz]);
+        }
+        *reinterpret_cast<float4*>(x_out + c0) = out;
+    }
+}
+
 __global__ void __launch_bounds__(MG_THREADS) k_mg_restrict(MgLevelDev L, MgLevelDev C, const SolveState* st,
                                                             int mode) {
     if (!mg_gate(st, mode)) return;
@@ -476,6 +580,7 @@ Multigrid::~Multigrid() {
         cudaFree(L.x);
         cudaFree(L.b);
     }
+    for (float* a : alt_) cudaFree(a);
     cudaFree(dense_);
 }
 
@@ -592,6 +697,20 @@ int Multigrid::init(const GridDev& g, cudaStream_t s) {
         set_error("multigrid hierarchy too deep for one cluster kernel");
         return RB200_UNSUPPORTED;
     }
+    // Fused red-black pairs on the grid-kernel levels whose rows are a
+    // multiple of 4 long and whose tile rows fit in shared memory.
+    alt_.assign(levels_.size(), nullptr);
+    size_t pair_smem = 0;
+    for (int l = 0; l < lower_first_; ++l) {
+        const MgLevelDev& L = levels_[l];
+        const size_t smem = size_t(PAIR_ROWS) * size_t(L.n[0]) * sizeof(float);
+        if ((L.n[0] & 3) != 0 || smem > kPairSmemMax) continue;
+        RB200_CUDA(cudaMalloc(&alt_[l], size_t(L.cells) * sizeof(float)));
+        bytes_ += size_t(L.cells) * sizeof(float);
+        pair_smem = std::max(pair_smem, smem);
+    }
+    if (pair_smem)
+        RB200_CUDA(cudaFuncSetAttribute(k_mg_smooth_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pair_smem)));
     // The largest cluster the device schedules for the lower-level kernel:
     // 16 CTAs (non-portable) where available, else 8.
     RB200_CUDA(cudaFuncSetAttribute(k_mg_lower, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -637,23 +756,60 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
     const SolveState* st = static_cast<const SolveState*>(state);
     const int nl = int(levels_.size());
     int launches = 0;
+    // Level l with its correction in buffer `which` (0: its own x, 1: the
+    // second buffer of the fused pairs).
+    auto with_x = [&](int l, int which) {
+        MgLevelDev L = levels_[l];
+        if (which) L.x = alt_[l];
+        return L;
+    };
+    // A fused pair (colour c1, then the other) from buffer `from` into the
+    // other buffer; returns the buffer that holds the result.
+    auto pair = [&](int l, int from, int c1, bool first) {
+        const MgLevelDev L = with_x(l, from);
+        const int tiles = ((L.n[1] + PJ - 1) / PJ) * ((L.n[2] + PK - 1) / PK);
+        const size_t smem = size_t(PAIR_ROWS) * size_t(L.n[0]) * sizeof(float);
+        k_mg_smooth_pair<<<tiles, MG_THREADS, smem, s>>>(L, from ? levels_[l].x : alt_[l], c1, first ? 1 : 0, st,
+                                                         mode);
+        launches += 1;
+        return 1 - from;
+    };
+    std::vector<int> cur(levels_.size(), 0);  // buffer of each grid-kernel level's correction
     // Descent on the large levels.
     for (int l = 0; l < lower_first_; ++l) {
         const MgLevelDev& L = levels_[l];
         const int pb = row_blocks(L, sweep_items(L));
-        for (int sweep = 0; sweep < 2; ++sweep) {
-            // the finest level's first red half-sweep may already be done
-            // (k_mg_update_first)
-            if (!(l == 0 && sweep == 0 && first_done)) {
-                k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, (l == 0 && sweep == 0) ? r : nullptr, 0, sweep == 0, st,
-                                                      mode);
+        if (alt_[l]) {
+            // red, black, red, black as pairs; on the finest level the first
+            // red is done by the update kernel or converts the residual here
+            if (l == 0) {
+                if (!first_done) {
+                    k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, r, 0, 1, st, mode);
+                    launches += 1;
+                }
+                cur[0] = pair(0, 0, 1, false);
+                k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(with_x(0, cur[0]), nullptr, 1, 0, st, mode);
+                launches += 1;
+            } else {
+                cur[l] = pair(l, 0, 0, true);
+                cur[l] = pair(l, cur[l], 0, false);
+            }
+        } else {
+            for (int sweep = 0; sweep < 2; ++sweep) {
+                // the finest level's first red half-sweep may already be done
+                // (k_mg_update_first)
+                if (!(l == 0 && sweep == 0 && first_done)) {
+                    k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, (l == 0 && sweep == 0) ? r : nullptr, 0, sweep == 0,
+                                                          st, mode);
+                    launches += 1;
+                }
+                k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 1, 0, st, mode);
                 launches += 1;
             }
-            k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 1, 0, st, mode);
         }
         k_mg_restrict<<<row_blocks(levels_[l + 1], restrict_items(L, levels_[l + 1])), MG_THREADS, 0, s>>>(
-            L, levels_[l + 1], st, mode);
-        launches += 3;
+            with_x(l, cur[l]), levels_[l + 1], st, mode);
+        launches += 1;
     }
     // The lower levels, coarsest solve included, in one cluster.
     MgLower P{};
@@ -678,17 +834,29 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
         launches += 1;
     }
     // Ascent on the large levels; the finest level's last red half-sweep is
-    // fused by the caller into its finish kernel.
+    // fused by the caller into its finish kernel. With fused pairs the finest
+    // level ends in its own x, where the finish kernel and the direction pass
+    // read it.
     for (int l = lower_first_ - 1; l >= 0; --l) {
-        const MgLevelDev& L = levels_[l];
+        const MgLevelDev L = with_x(l, cur[l]);
+        const MgLevelDev C = with_x(l + 1, l + 1 < lower_first_ ? cur[l + 1] : 0);
         const int pb = row_blocks(L, sweep_items(L));
-        k_mg_prolong_black<<<pb, MG_THREADS, 0, s>>>(L, levels_[l + 1], st, mode);
-        k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 0, 0, st, mode);
-        k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 1, 0, st, mode);
-        launches += 3;
-        if (l > 0) {
+        k_mg_prolong_black<<<pb, MG_THREADS, 0, s>>>(L, C, st, mode);
+        launches += 1;
+        if (alt_[l]) {
+            cur[l] = pair(l, cur[l], 0, false);
+            if (l > 0) {
+                k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(with_x(l, cur[l]), nullptr, 0, 0, st, mode);
+                launches += 1;
+            }
+        } else {
             k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 0, 0, st, mode);
-            launches += 1;
+            k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 1, 0, st, mode);
+            launches += 2;
+            if (l > 0) {
+                k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 0, 0, st, mode);
+                launches += 1;
+            }
         }
     }
     return launches;

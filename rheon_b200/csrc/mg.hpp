@@ -84,6 +84,9 @@ private:
     int lower_first_ = 0;       // first level handled by the cluster kernel
     int cluster_ = 0;           // CTAs of that kernel's cluster
     size_t bytes_ = 0;
+    // Second correction buffer of each grid-kernel level smoothed by fused
+    // red-black pairs (nullptr: the level runs single half-sweeps).
+    std::vector<float*> alt_;
 };
 
 }  // namespace rb200
