@@ -387,29 +387,24 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(MgLevelDev L, const do
 }
 
 // Two half-sweeps in one pass (colour c1, then the other colour) over a level
-// whose rows are a multiple of 4 long. A block takes a tile of PJ x PK rows
-// (j, k) at full row length: it relaxes colour c1 on the tile and the rows
-// around it (one row of halo in j and k) from the input x into shared memory,
-// exactly as smooth_rows_v4 does, then relaxes the other colour on the tile
-// from those rows and stores both colours to x_out. The input x is only read
-// and x_out only written, so tiles never see each other's partial results,
-// and the values equal two consecutive half-sweeps bit for bit (the same
-// operands in the same order). With `first` the correction starts from zero.
-constexpr int PJ = 4, PK = 4;
-constexpr int PAIR_ROWS = (PJ + 2) * (PK + 2);
-constexpr size_t kPairSmemMax = 200 * 1024;
-
-__global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pair(MgLevelDev L, float* __restrict__ x_out, int c1,
-                                                               int first, const SolveState* st, int mode) {
-    extern __shared__ float4 srow[];  // PAIR_ROWS rows of n0/4 quads
-    if (!mg_gate(st, mode)) return;
+// whose rows are a multiple of 4 long, one tile of PJ x PK rows (j, k) at full
+// row length: colour c1 is relaxed on the tile and the rows around it (one
+// row of halo in j and k) from the input x into shared memory, exactly as
+// smooth_rows_v4 does, then the other colour on the tile from those rows, and
+// both colours are stored to x_out. The input x is only read and x_out only
+// written, so tiles never see each other's partial results, and the values
+// equal two consecutive half-sweeps bit for bit (the same operands in the same
+// order). With `first` the correction starts from zero. Every thread of the
+// block calls it; srow holds (PJ + 2) (PK + 2) rows.
+template <bool CG, int PJ, int PK>
+__device__ __forceinline__ void pair_tile(const MgLevelDev& L, float* __restrict__ x_out, int c1, bool first, int j0,
+                                          int k0, float4* srow) {
+    constexpr int ROWS = (PJ + 2) * (PK + 2);
     const int n0 = L.n[0], quads = n0 >> 2, n1 = L.n[1], n2 = L.n[2];
     const int sy = n0, sz = n0 * n1;
-    const int tj = (n1 + PJ - 1) / PJ;
-    const int j0 = int(blockIdx.x % unsigned(tj)) * PJ, k0 = int(blockIdx.x / unsigned(tj)) * PK;
     const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float* __restrict__ x = L.x;
-    for (int it = threadIdx.x; it < PAIR_ROWS * quads; it += blockDim.x) {
+    for (int it = threadIdx.x; it < ROWS * quads; it += blockDim.x) {
         const int q = it % quads, hr = it / quads;
         const int j = j0 - 1 + hr % (PJ + 2), k = k0 - 1 + hr / (PJ + 2);
         if (j < 0 || j >= n1 || k < 0 || k >= n2) continue;
@@ -417,7 +412,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pair(MgLevelDev L, flo
         const int c0 = i0 + n0 * (j + n1 * k);
         const int par = (c1 + j + k) & 1;
         const int myz = (int(j > 0) << 2) | (int(j + 1 < n1) << 3) | (int(k > 0) << 4) | (int(k + 1 < n2) << 5);
-        const float4 bq = *reinterpret_cast<const float4*>(L.b + c0);
+        const float4 bq = ld4<CG>(L.b + c0);
         float4 out;
         if (first) {
             out = z4;
@@ -428,13 +423,13 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pair(MgLevelDev L, flo
                 f4put(out, e, f4get(bq, e) * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz]);
             }
         } else {
-            const float4 xc = *reinterpret_cast<const float4*>(x + c0);
-            const float xl = i0 > 0 ? x[c0 - 1] : 0.0f;
-            const float xr = i0 + 4 < n0 ? x[c0 + 4] : 0.0f;
-            const float4 ym = (myz & 4) ? *reinterpret_cast<const float4*>(x + c0 - sy) : z4;
-            const float4 yp = (myz & 8) ? *reinterpret_cast<const float4*>(x + c0 + sy) : z4;
-            const float4 zm = (myz & 16) ? *reinterpret_cast<const float4*>(x + c0 - sz) : z4;
-            const float4 zp = (myz & 32) ? *reinterpret_cast<const float4*>(x + c0 + sz) : z4;
+            const float4 xc = ld4<CG>(x + c0);
+            const float xl = i0 > 0 ? ldv<CG>(x + c0 - 1) : 0.0f;
+            const float xr = i0 + 4 < n0 ? ldv<CG>(x + c0 + 4) : 0.0f;
+            const float4 ym = (myz & 4) ? ld4<CG>(x + c0 - sy) : z4;
+            const float4 yp = (myz & 8) ? ld4<CG>(x + c0 + sy) : z4;
+            const float4 zm = (myz & 16) ? ld4<CG>(x + c0 - sz) : z4;
+            const float4 zp = (myz & 32) ? ld4<CG>(x + c0 + sz) : z4;
             out = xc;
 #pragma unroll
             for (int t = 0; t < 2; ++t) {
@@ -463,7 +458,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pair(MgLevelDev L, flo
         const int c0 = i0 + n0 * (j + n1 * k);
         const int par = (c1 + 1 + j + k) & 1;
         const int myz = (int(j > 0) << 2) | (int(j + 1 < n1) << 3) | (int(k > 0) << 4) | (int(k + 1 < n2) << 5);
-        const float4 bq = *reinterpret_cast<const float4*>(L.b + c0);
+        const float4 bq = ld4<CG>(L.b + c0);
         const float4 xc = srow[hr * quads + q];
         const float xl = i0 > 0 ? sf[hr * n0 + i0 - 1] : 0.0f;
         const float xr = i0 + 4 < n0 ? sf[hr * n0 + i0 + 4] : 0.0f;
@@ -487,7 +482,27 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pair(MgLevelDev L, flo
         }
         *reinterpret_cast<float4*>(x_out + c0) = out;
     }
+    __syncthreads();  // srow is free for the block's next tile
 }
+
+// Grid kernel of the pairs: one 4 x 4-row tile per block.
+constexpr int PJ = 4, PK = 4;
+constexpr int PAIR_ROWS = (PJ + 2) * (PK + 2);
+constexpr size_t kPairSmemMax = 200 * 1024;
+
+__global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pair(MgLevelDev L, float* __restrict__ x_out, int c1,
+                                                               int first, const SolveState* st, int mode) {
+    extern __shared__ float4 srow[];  // PAIR_ROWS rows of n0/4 quads
+    if (!mg_gate(st, mode)) return;
+    const int tj = (L.n[1] + PJ - 1) / PJ;
+    pair_tile<false, PJ, PK>(L, x_out, c1, first != 0, int(blockIdx.x % unsigned(tj)) * PJ,
+                             int(blockIdx.x / unsigned(tj)) * PK, srow);
+}
+
+// Pairs in the cluster kernel: 8 x 8-row tiles dealt over the cluster's CTAs,
+// for levels whose rows are a multiple of 4 and at most LPAIR_N0 long.
+constexpr int LPJ = 8, LPK = 8;
+constexpr int LPAIR_N0 = 32;
 
 __global__ void __launch_bounds__(MG_THREADS) k_mg_restrict(MgLevelDev L, MgLevelDev C, const SolveState* st,
                                                             int mode) {
@@ -517,6 +532,16 @@ __device__ __forceinline__ unsigned cluster_size() {
     return r;
 }
 
+// A fused pair on a level of the cluster kernel: the tiles are dealt over the
+// cluster's CTAs, which then meet at the cluster barrier.
+__device__ __forceinline__ void cluster_pair(const MgLevelDev& L, float* out, int c1, bool first, unsigned rank,
+                                             unsigned nct, float4* prow) {
+    const int tj = (L.n[1] + LPJ - 1) / LPJ, tiles = tj * ((L.n[2] + LPK - 1) / LPK);
+    for (int t = int(rank); t < tiles; t += int(nct))
+        pair_tile<true, LPJ, LPK>(L, out, c1, first, (t % tj) * LPJ, (t / tj) * LPK, prow);
+    cluster_sync_all();
+}
+
 // The whole V-cycle below the grid-kernel levels in one thread-block cluster:
 // the CTAs split every half-sweep, restriction and prolongation, and meet at
 // hardware cluster barriers (release/acquire) instead of kernel boundaries.
@@ -528,23 +553,44 @@ __global__ void __launch_bounds__(MG_LOWER_THREADS, 1) k_mg_lower(MgLower P, con
                                                                const double* __restrict__ G,
                                                                const SolveState* st, int mode, int skip_last_red) {
     __shared__ double bs[512];
+    __shared__ float4 prow[(LPJ + 2) * (LPK + 2) * LPAIR_N0 / 4];
     if (!mg_gate(st, mode)) return;  // uniform: every CTA reads the same flags
     const unsigned rank = cluster_rank(), nct = cluster_size();
     const Warps W{int((rank * blockDim.x + threadIdx.x) >> 5), int((nct * blockDim.x) >> 5), int(threadIdx.x & 31)};
     const int last = P.count - 1;
+    unsigned second = 0;  // bit l: level l's correction is in its second buffer
     for (int l = 0; l < last; ++l) {
-        const MgLevelDev& L = P.lv[l];
-        for (int sweep = 0; sweep < 2; ++sweep) {
-            smooth_rows<true>(L, (l == 0 && sweep == 0) ? r0 : nullptr, 0, sweep == 0, W);
-            cluster_sync_all();
-            smooth_rows<true>(L, nullptr, 1, false, W);
-            cluster_sync_all();
+        const MgLevelDev& L = P.lv[0][l];
+        if (P.paired[l]) {
+            const MgLevelDev& La = P.lv[1][l];
+            if (l == 0 && r0) {
+                // the finest level: red converts the residual, then (black,
+                // red) into the second buffer and black there
+                smooth_rows<true>(L, r0, 0, true, W);
+                cluster_sync_all();
+                cluster_pair(L, La.x, 1, false, rank, nct, prow);
+                smooth_rows<true>(La, nullptr, 1, false, W);
+                cluster_sync_all();
+                restrict_rows<true>(La, P.lv[0][l + 1], W);
+                second |= 1u << l;
+            } else {
+                cluster_pair(L, La.x, 0, true, rank, nct, prow);
+                cluster_pair(La, L.x, 0, false, rank, nct, prow);
+                restrict_rows<true>(L, P.lv[0][l + 1], W);
+            }
+        } else {
+            for (int sweep = 0; sweep < 2; ++sweep) {
+                smooth_rows<true>(L, (l == 0 && sweep == 0) ? r0 : nullptr, 0, sweep == 0, W);
+                cluster_sync_all();
+                smooth_rows<true>(L, nullptr, 1, false, W);
+                cluster_sync_all();
+            }
+            restrict_rows<true>(L, P.lv[0][l + 1], W);
         }
-        restrict_rows<true>(L, P.lv[l + 1], W);
         cluster_sync_all();
     }
     {
-        const MgLevelDev& C = P.lv[last];
+        const MgLevelDev& C = P.lv[0][last];
         const int M = C.cells;
         const double* src = last == 0 ? r0 : nullptr;
         for (int c = threadIdx.x; c < M; c += blockDim.x) bs[c] = src ? src[c] : double(__ldcg(C.b + c));
@@ -560,15 +606,24 @@ __global__ void __launch_bounds__(MG_LOWER_THREADS, 1) k_mg_lower(MgLower P, con
         cluster_sync_all();
     }
     for (int l = last - 1; l >= 0; --l) {
-        const MgLevelDev& L = P.lv[l];
-        prolong_black_rows<true>(L, P.lv[l + 1], W);
+        const int in = (second >> l) & 1u;
+        const MgLevelDev& L = P.lv[in][l];
+        prolong_black_rows<true>(L, P.lv[(second >> (l + 1)) & 1u][l + 1], W);
         cluster_sync_all();
-        smooth_rows<true>(L, nullptr, 0, false, W);
-        cluster_sync_all();
-        smooth_rows<true>(L, nullptr, 1, false, W);
-        cluster_sync_all();
-        if (!(l == 0 && skip_last_red)) {
+        int now = in;
+        if (P.paired[l]) {
+            // (red, black) into the other buffer, then red there
+            cluster_pair(L, P.lv[in ^ 1][l].x, 0, false, rank, nct, prow);
+            second ^= 1u << l;
+            now = in ^ 1;
+        } else {
             smooth_rows<true>(L, nullptr, 0, false, W);
+            cluster_sync_all();
+            smooth_rows<true>(L, nullptr, 1, false, W);
+            cluster_sync_all();
+        }
+        if (!(l == 0 && skip_last_red)) {
+            smooth_rows<true>(P.lv[now][l], nullptr, 0, false, W);
             cluster_sync_all();
         }
     }
@@ -711,6 +766,13 @@ int Multigrid::init(const GridDev& g, cudaStream_t s) {
     }
     if (pair_smem)
         RB200_CUDA(cudaFuncSetAttribute(k_mg_smooth_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pair_smem)));
+    // and on the cluster kernel's levels above the dense one with short rows
+    for (int l = lower_first_; l + 1 < nl; ++l) {
+        const MgLevelDev& L = levels_[l];
+        if ((L.n[0] & 3) != 0 || L.n[0] > LPAIR_N0) continue;
+        RB200_CUDA(cudaMalloc(&alt_[l], size_t(L.cells) * sizeof(float)));
+        bytes_ += size_t(L.cells) * sizeof(float);
+    }
     // The largest cluster the device schedules for the lower-level kernel:
     // 16 CTAs (non-portable) where available, else 8.
     RB200_CUDA(cudaFuncSetAttribute(k_mg_lower, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -814,7 +876,12 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
     // The lower levels, coarsest solve included, in one cluster.
     MgLower P{};
     P.count = nl - lower_first_;
-    for (int q = 0; q < P.count; ++q) P.lv[q] = levels_[lower_first_ + q];
+    for (int q = 0; q < P.count; ++q) {
+        P.lv[0][q] = levels_[lower_first_ + q];
+        P.lv[1][q] = levels_[lower_first_ + q];
+        P.paired[q] = alt_[lower_first_ + q] ? 1 : 0;
+        if (P.paired[q]) P.lv[1][q].x = alt_[lower_first_ + q];
+    }
     {
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(unsigned(cluster_), 1, 1);
@@ -839,7 +906,9 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
     // read it.
     for (int l = lower_first_ - 1; l >= 0; --l) {
         const MgLevelDev L = with_x(l, cur[l]);
-        const MgLevelDev C = with_x(l + 1, l + 1 < lower_first_ ? cur[l + 1] : 0);
+        // the cluster kernel leaves its first level in the second buffer when
+        // that level is a paired coarse level (two pairs down, one up)
+        const MgLevelDev C = with_x(l + 1, l + 1 < lower_first_ ? cur[l + 1] : (alt_[l + 1] ? 1 : 0));
         const int pb = row_blocks(L, sweep_items(L));
         k_mg_prolong_black<<<pb, MG_THREADS, 0, s>>>(L, C, st, mode);
         launches += 1;

@@ -42,7 +42,10 @@ constexpr int kMgMaxLower = 16;
 
 // The levels handled by the cluster kernel, the coarsest last.
 struct MgLower {
-    MgLevelDev lv[kMgMaxLower];
+    // lv[0][q]: level q with its own correction buffer; lv[1][q]: the same
+    // level with its second buffer (fused pairs), or lv[0][q] again
+    MgLevelDev lv[2][kMgMaxLower];
+    int paired[kMgMaxLower];
     int count;
 };
 
@@ -84,8 +87,8 @@ private:
     int lower_first_ = 0;       // first level handled by the cluster kernel
     int cluster_ = 0;           // CTAs of that kernel's cluster
     size_t bytes_ = 0;
-    // Second correction buffer of each grid-kernel level smoothed by fused
-    // red-black pairs (nullptr: the level runs single half-sweeps).
+    // Second correction buffer of each level smoothed by fused red-black
+    // pairs (nullptr: the level runs single half-sweeps).
     std::vector<float*> alt_;
 };
 
