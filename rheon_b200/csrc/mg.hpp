@@ -15,9 +15,13 @@
 // Launch structure of one cycle: grid-wide kernels for the levels above 32^3
 // cells; one kernel on a thread-block cluster (16 CTAs where the device
 // schedules them) for every level of at most 32^3 cells, the dense coarsest
-// solve included, whose half-sweeps meet at hardware cluster barriers. The
-// last red half-sweep of the finest level is left to the caller, which fuses
-// it with the outer method's dot products (k_mg_finish_red).
+// solve included, whose half-sweeps meet at hardware cluster barriers. Where
+// a level's rows are a multiple of 4 long, consecutive red and black
+// half-sweeps run as one fused pass over row tiles (the level keeps a second
+// correction buffer for it); the results are those of the single
+// half-sweeps bit for bit. The last red half-sweep of the finest level is
+// left to the caller, which fuses it with the outer method's dot products
+// (k_mg_finish_red).
 #pragma once
 
 #include <vector>
