@@ -2,6 +2,7 @@
 // preconditioner of the mixed-precision pressure method (see mg.hpp).
 #include <algorithm>
 #include <cmath>
+#include <utility>
 #include <vector>
 
 #include "mg.hpp"
@@ -15,6 +16,12 @@ constexpr int MG_THREADS = 256;
 constexpr int MG_LOWER_THREADS = 1024;
 
 __device__ __forceinline__ bool mg_gate(const SolveState* st, int mode) { return gate(st->flags, mode); }
+
+// Kernels of the V-cycle are launched with programmatic stream serialisation:
+// one may start while the kernel before it drains, and waits here, before its
+// first memory access, until that kernel has completed and its writes are
+// visible (a no-op for a launch without the attribute).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 
 __device__ __forceinline__ int mask_of(const int n[3], int i, int j, int k) {
     return int(i > 0) | (int(i + 1 < n[0]) << 1) | (int(j > 0) << 2) | (int(j + 1 < n[1]) << 3) |
@@ -382,6 +389,7 @@ __device__ __forceinline__ void prolong_black_rows(const MgLevelDev& L, const Mg
 // ------------------------------------------------------------ grid kernels (large levels)
 __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(MgLevelDev L, const double* __restrict__ r0, int color,
                                                           int first, const SolveState* st, int mode) {
+    pdl_wait();
     if (!mg_gate(st, mode)) return;
     smooth_rows<false>(L, r0, color, first != 0, grid_warps());
 }
@@ -492,6 +500,7 @@ constexpr size_t kPairSmemMax = 200 * 1024;
 
 __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pair(MgLevelDev L, float* __restrict__ x_out, int c1,
                                                                int first, const SolveState* st, int mode) {
+    pdl_wait();
     extern __shared__ float4 srow[];  // PAIR_ROWS rows of n0/4 quads
     if (!mg_gate(st, mode)) return;
     const int tj = (L.n[1] + PJ - 1) / PJ;
@@ -506,12 +515,14 @@ constexpr int LPAIR_N0 = 32;
 
 __global__ void __launch_bounds__(MG_THREADS) k_mg_restrict(MgLevelDev L, MgLevelDev C, const SolveState* st,
                                                             int mode) {
+    pdl_wait();
     if (!mg_gate(st, mode)) return;
     restrict_rows<false>(L, C, grid_warps());
 }
 
 __global__ void __launch_bounds__(MG_THREADS) k_mg_prolong_black(MgLevelDev L, MgLevelDev C, const SolveState* st,
                                                                  int mode) {
+    pdl_wait();
     if (!mg_gate(st, mode)) return;
     prolong_black_rows<false>(L, C, grid_warps());
 }
@@ -552,6 +563,7 @@ __device__ __forceinline__ void cluster_pair(const MgLevelDev& L, float* out, in
 __global__ void __launch_bounds__(MG_LOWER_THREADS, 1) k_mg_lower(MgLower P, const double* __restrict__ r0,
                                                                const double* __restrict__ G,
                                                                const SolveState* st, int mode, int skip_last_red) {
+    pdl_wait();
     __shared__ double bs[512];
     __shared__ float4 prow[(LPJ + 2) * (LPK + 2) * LPAIR_N0 / 4];
     if (!mg_gate(st, mode)) return;  // uniform: every CTA reads the same flags
@@ -630,6 +642,24 @@ __global__ void __launch_bounds__(MG_LOWER_THREADS, 1) k_mg_lower(MgLower P, con
 }
 
 // ------------------------------------------------------------ host side
+// Launch of a V-cycle kernel that may overlap the drain of the kernel before
+// it on the stream (programmatic stream serialisation); the kernel waits for
+// it in pdl_wait before its first memory access.
+template <typename... KArgs, typename... Args>
+static void pdl_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 Multigrid::~Multigrid() {
     for (auto& L : levels_) {
         cudaFree(L.x);
@@ -831,8 +861,8 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
         const MgLevelDev L = with_x(l, from);
         const int tiles = ((L.n[1] + PJ - 1) / PJ) * ((L.n[2] + PK - 1) / PK);
         const size_t smem = size_t(PAIR_ROWS) * size_t(L.n[0]) * sizeof(float);
-        k_mg_smooth_pair<<<tiles, MG_THREADS, smem, s>>>(L, from ? levels_[l].x : alt_[l], c1, first ? 1 : 0, st,
-                                                         mode);
+        pdl_launch(k_mg_smooth_pair, dim3(tiles), dim3(MG_THREADS), smem, s, L, from ? levels_[l].x : alt_[l], c1,
+                   first ? 1 : 0, st, mode);
         launches += 1;
         return 1 - from;
     };
@@ -846,11 +876,11 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
             // red is done by the update kernel or converts the residual here
             if (l == 0) {
                 if (!first_done) {
-                    k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, r, 0, 1, st, mode);
+                    pdl_launch(k_mg_smooth, dim3(pb), dim3(MG_THREADS), 0, s, L, r, 0, 1, st, mode);
                     launches += 1;
                 }
                 cur[0] = pair(0, 0, 1, false);
-                k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(with_x(0, cur[0]), nullptr, 1, 0, st, mode);
+                pdl_launch(k_mg_smooth, dim3(pb), dim3(MG_THREADS), 0, s, with_x(0, cur[0]), nullptr, 1, 0, st, mode);
                 launches += 1;
             } else {
                 cur[l] = pair(l, 0, 0, true);
@@ -861,16 +891,16 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
                 // the finest level's first red half-sweep may already be done
                 // (k_mg_update_first)
                 if (!(l == 0 && sweep == 0 && first_done)) {
-                    k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, (l == 0 && sweep == 0) ? r : nullptr, 0, sweep == 0,
-                                                          st, mode);
+                    pdl_launch(k_mg_smooth, dim3(pb), dim3(MG_THREADS), 0, s, L, (l == 0 && sweep == 0) ? r : nullptr,
+                               0, sweep == 0, st, mode);
                     launches += 1;
                 }
-                k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 1, 0, st, mode);
+                pdl_launch(k_mg_smooth, dim3(pb), dim3(MG_THREADS), 0, s, L, nullptr, 1, 0, st, mode);
                 launches += 1;
             }
         }
-        k_mg_restrict<<<row_blocks(levels_[l + 1], restrict_items(L, levels_[l + 1])), MG_THREADS, 0, s>>>(
-            with_x(l, cur[l]), levels_[l + 1], st, mode);
+        pdl_launch(k_mg_restrict, dim3(row_blocks(levels_[l + 1], restrict_items(L, levels_[l + 1]))), dim3(MG_THREADS),
+                   0, s, with_x(l, cur[l]), levels_[l + 1], st, mode);
         launches += 1;
     }
     // The lower levels, coarsest solve included, in one cluster.
@@ -887,13 +917,15 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
         cfg.gridDim = dim3(unsigned(cluster_), 1, 1);
         cfg.blockDim = dim3(MG_LOWER_THREADS, 1, 1);
         cfg.stream = s;
-        cudaLaunchAttribute attr[1];
+        cudaLaunchAttribute attr[2];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = unsigned(cluster_);
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
+        attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[1].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
-        cfg.numAttrs = 1;
+        cfg.numAttrs = 2;
         const double* r0 = lower_first_ == 0 ? r : nullptr;
         const double* G = dense_;
         const int skip = (lower_first_ == 0 && nl > 1) ? 1 : 0;
@@ -910,20 +942,20 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
         // that level is a paired coarse level (two pairs down, one up)
         const MgLevelDev C = with_x(l + 1, l + 1 < lower_first_ ? cur[l + 1] : (alt_[l + 1] ? 1 : 0));
         const int pb = row_blocks(L, sweep_items(L));
-        k_mg_prolong_black<<<pb, MG_THREADS, 0, s>>>(L, C, st, mode);
+        pdl_launch(k_mg_prolong_black, dim3(pb), dim3(MG_THREADS), 0, s, L, C, st, mode);
         launches += 1;
         if (alt_[l]) {
             cur[l] = pair(l, cur[l], 0, false);
             if (l > 0) {
-                k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(with_x(l, cur[l]), nullptr, 0, 0, st, mode);
+                pdl_launch(k_mg_smooth, dim3(pb), dim3(MG_THREADS), 0, s, with_x(l, cur[l]), nullptr, 0, 0, st, mode);
                 launches += 1;
             }
         } else {
-            k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 0, 0, st, mode);
-            k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 1, 0, st, mode);
+            pdl_launch(k_mg_smooth, dim3(pb), dim3(MG_THREADS), 0, s, L, nullptr, 0, 0, st, mode);
+            pdl_launch(k_mg_smooth, dim3(pb), dim3(MG_THREADS), 0, s, L, nullptr, 1, 0, st, mode);
             launches += 2;
             if (l > 0) {
-                k_mg_smooth<<<pb, MG_THREADS, 0, s>>>(L, nullptr, 0, 0, st, mode);
+                pdl_launch(k_mg_smooth, dim3(pb), dim3(MG_THREADS), 0, s, L, nullptr, 0, 0, st, mode);
                 launches += 1;
             }
         }
@@ -940,6 +972,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int 
                                                               const double* __restrict__ r,
                                                               const double* __restrict__ q, int mode, Partials part,
                                                               rb200_trace* trace) {
+    pdl_wait();
     __shared__ BlockReduce<2, 0> red;
     if (!gate(st->flags, mode)) return;
     Neu rz, zq;
@@ -1054,6 +1087,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int 
 __global__ void __launch_bounds__(MG_THREADS) k_mg_pass1(GridDev g, MgLevelDev L, SolveState* st, double* d0,
                                                          double* d1, double* __restrict__ q, Partials part,
                                                          rb200_trace* trace, int kc_len) {
+    pdl_wait();
     __shared__ BlockReduce<1, 0> red;
     const int flags = st->flags;
     if (flags & F_STOP) return;
@@ -1180,6 +1214,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_update_first(GridDev g, MgLev
                                                                 const double* d0, const double* d1,
                                                                 const double* __restrict__ q, Partials part,
                                                                 rb200_trace* trace) {
+    pdl_wait();
     __shared__ BlockReduce<1, 0> red;
     const int flags = st->flags;
     if (flags & F_STOP) return;
@@ -1268,8 +1303,8 @@ int Multigrid::enqueue_update_first(const GridDev& g, void* state, double* p, do
                                     const double* q, Partials part, rb200_trace* trace, cudaStream_t s) const {
     int pb = row_blocks(levels_[0]);
     if (pb > 148 * 8) pb = 148 * 8;  // reduction partials capacity
-    k_mg_update_first<<<pb, MG_THREADS, 0, s>>>(g, levels_[0], static_cast<SolveState*>(state), p, r, d0, d1, q,
-                                                part, trace);
+    pdl_launch(k_mg_update_first, dim3(pb), dim3(MG_THREADS), 0, s, g, levels_[0], static_cast<SolveState*>(state), p,
+               r, d0, d1, q, part, trace);
     return 1;
 }
 
@@ -1283,8 +1318,8 @@ int Multigrid::enqueue_pass1(const GridDev& g, void* state, double* d0, double* 
     const int warps = pb * (MG_THREADS / 32);
     int kc_len = 16;
     while (kc_len > 2 && qsegs * g.n[1] * ((g.n[2] + kc_len - 1) / kc_len) < warps) kc_len /= 2;
-    k_mg_pass1<<<pb, MG_THREADS, 0, s>>>(g, levels_[0], static_cast<SolveState*>(state), d0, d1, q, part, trace,
-                                         kc_len);
+    pdl_launch(k_mg_pass1, dim3(pb), dim3(MG_THREADS), 0, s, g, levels_[0], static_cast<SolveState*>(state), d0, d1, q,
+               part, trace, kc_len);
     return 1;
 }
 
@@ -1293,8 +1328,8 @@ int Multigrid::enqueue_finish(void* state, const double* r, const double* q, int
     const MgLevelDev& L = levels_[0];
     int pb = row_blocks(L);
     if (pb > 148 * 8) pb = 148 * 8;  // reduction partials capacity
-    k_mg_finish_red<<<pb, MG_THREADS, 0, s>>>(L, levels_.size() > 1 ? 1 : 0, static_cast<SolveState*>(state), r,
-                                              q, mode, part, trace);
+    pdl_launch(k_mg_finish_red, dim3(pb), dim3(MG_THREADS), 0, s, L, levels_.size() > 1 ? 1 : 0,
+               static_cast<SolveState*>(state), r, q, mode, part, trace);
     return 1;
 }
 
