@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=200)
     ap.add_argument("--serving-plain-requests", type=int, default=12)
     ap.add_argument("--serving-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serving-projection-share", type=float, default=0.25,
+                    help="share of serving requests that are projections of a supplied velocity")
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--no-dense3d", action="store_true")
     ap.add_argument("--dense3d", action="store_true",
@@ -197,12 +199,13 @@ def run_e2e(args, g, cfg, faces, prm, flush, local, world):
 
 
 def run_batched(args, local, flush):
-    """Batched uneven instances: boxes with edges drawn by seed from
-    {32, 48, 64, 96, 128}, each with its own random-Fourier velocity, in the
-    mixed-precision configuration at rel. residual 1e-8. Every batched step
-    launches one step graph per instance (each on its own stream) and waits for
-    all; the makespan is timed with CUDA events (a start event every instance
-    stream waits on, and a join stream that waits on every instance's end)."""
+    """Batched uneven instances (the packed batch): boxes with edges drawn by
+    seed from {32, 48, 64, 96, 128}, each with its own random-Fourier velocity,
+    in the mixed-precision configuration at rel. residual 1e-8, all advanced
+    together by one CUDA graph per batched step whose every stage is one launch
+    over the packed instance table. The step is timed with CUDA events on the
+    batch's stream. For comparison the same boxes also run as one resident
+    carrier each, their step graphs launched together on separate streams."""
     import torch
 
     import rheon_b200 as R
@@ -212,20 +215,75 @@ def run_batched(args, local, flush):
     pick = ((W.uniform(args.seed, 40, args.batched_instances) + 1.0) * 0.5 * len(edges)).astype(int)
     sizes = [int(edges[min(i, len(edges) - 1)]) for i in pick]
     cfg = R.CarrierConfig.mixed(pressure=R.PressureSettings(1e-8, 0.0, MAXF, 1000), device=local)
+    init = [W.fourier_faces((n, n, n), seed=args.seed + 1000 + i, dtype=np.float32) for i, n in enumerate(sizes)]
+    batch = R.BatchedCarriers([R.GridGeometry((n, n, n)) for n in sizes], cfg)
+    for i, f in enumerate(init):
+        batch.upload(i, f)
+    stream = torch.cuda.ExternalStream(batch.stream(), device=local)
+    prm = R.StepParams(MAXF, cfl=0.5)
+    for _ in range(max(3, args.warmup)):
+        if any(st != 0 for st, _ in batch.step(prm)):
+            raise RuntimeError("batched warm-up step rejected")
+    cells = [n ** 3 for n in sizes]
+    faces_total = [3 * n * n * (n + 1) for n in sizes]
+    total_ms, cell_steps, iters, model_bytes, launches, solve_ms = 0.0, 0, [], 0.0, 0, 0.0
+    for _ in range(args.batched_steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        batch.step_async(prm)
+        b.record(stream)
+        out = batch.step_wait()
+        b.synchronize()
+        if any(st != 0 for st, _ in out):
+            raise RuntimeError("batched step rejected")
+        total_ms += a.elapsed_time(b)
+        cell_steps += sum(cells)
+        its = [r.pressure.iterations for _, r in out]
+        iters += its
+        launches += out[0][1].kernel_launches
+        solve_ms += out[0][1].pressure_ms
+        # the algorithmic byte model of a mixed step, summed over instances:
+        # 130N per outer iteration (FP32 V(2,2), levels summed, + FP64 defect
+        # and accumulation) and 5 F s + 16N for advection, RHS and correction
+        model_bytes += sum(it * 130 * c + 5 * f * 4 + 16 * c for it, c, f in zip(its, cells, faces_total))
+    hbm, hbm_kind = peaks()
+    achieved = model_bytes / (total_ms / 1e3) / 1e9
+    ms_step = total_ms / args.batched_steps
+    result = {
+        "value": cell_steps / (total_ms / 1e3),
+        "unit": UNIT,
+        "instances": len(sizes),
+        "edges": {str(e): sizes.count(int(e)) for e in edges},
+        "cells": sum(cells),
+        "steps": args.batched_steps,
+        "ms_per_batched_step": ms_step,
+        "solve_ms_per_batched_step": solve_ms / args.batched_steps,
+        "iterations_per_step": statistics.mean(iters),
+        "iterations_max": max(iters),
+        "graph_launches_per_batched_step": 1,
+        "kernels_per_batched_step": launches / args.batched_steps,
+        "dtype": "mixed (f32 faces and V-cycles, f64 residual/accumulation/coarse solve)",
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "peak_kind": hbm_kind, "unit": "GB/s",
+                     "frac": achieved / hbm, "bytes_per_batched_step": model_bytes / args.batched_steps,
+                     "model": "sum over instances of 130N per outer iteration + 5Fs + 16N per step"},
+    }
+    batch.close()
+    # the same boxes as separate resident carriers launched together
     sims = []
     for i, n in enumerate(sizes):
         sim = R.CarrierSimulation(R.GridGeometry((n, n, n)), cfg)
-        sim.upload(W.fourier_faces((n, n, n), seed=args.seed + 1000 + i, dtype=np.float32))
+        sim.upload(init[i])
         sims.append(sim)
-    streams = [torch.cuda.ExternalStream(s.stream(), device=local) for s in sims]
+    streams = [torch.cuda.ExternalStream(sm.stream(), device=local) for sm in sims]
     join = torch.cuda.Stream(device=local)
-    prm = R.StepParams(MAXF, cfl=0.5)
     for _ in range(max(3, args.warmup)):
-        out = R.step_all(sims, [prm] * len(sims))
-        if any(st != 0 for st, _ in out):
-            raise RuntimeError("batched warm-up step rejected")
-    total_ms, cell_steps, iters = 0.0, 0, []
-    for _ in range(args.batched_steps):
+        R.step_all(sims, [prm] * len(sims))
+    sep_ms = 0.0
+    steps_sep = max(1, min(args.batched_steps, 5))
+    for _ in range(steps_sep):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)
@@ -233,41 +291,83 @@ def run_batched(args, local, flush):
         a.record(join)
         for st in streams:
             st.wait_event(a)
-        for sim in sims:
-            sim.step_async(prm)
+        for sm in sims:
+            sm.step_async(prm)
         for st in streams:
             e = torch.cuda.Event()
             e.record(st)
             join.wait_event(e)
         b.record(join)
-        reps = [sim.step_wait() for sim in sims]
+        for sm in sims:
+            sm.step_wait()
         b.synchronize()
-        total_ms += a.elapsed_time(b)
-        cell_steps += sum(n ** 3 for n in sizes)
-        iters += [r.pressure.iterations for r in reps]
-    for sim in sims:
-        sim.close()
-    return {
-        "value": cell_steps / (total_ms / 1e3),
-        "unit": UNIT,
-        "instances": len(sizes),
-        "edges": {str(e): sizes.count(int(e)) for e in edges},
-        "steps": args.batched_steps,
-        "ms_per_batched_step": total_ms / args.batched_steps,
-        "iterations_per_step": statistics.mean(iters),
-        "dtype": "mixed (f32 faces and V-cycles, f64 residual/accumulation/coarse solve)",
-    }
+        sep_ms += a.elapsed_time(b)
+    for sm in sims:
+        sm.close()
+    result["separate_carriers"] = {"ms_per_batched_step": sep_ms / steps_sep,
+                                   "value": sum(cells) * steps_sep / (sep_ms / 1e3),
+                                   "note": "one step graph per box on its own stream, launched together"}
+    return result
+
+
+def run_mixed_large(args, local, flush, n):
+    """The mixed-precision carrier at n^3 (random-Fourier state generated on the
+    device, CFL 0.5, rel. residual 1e-8): device-timed steps and the step's
+    roofline under the algorithmic byte model (130N per outer iteration,
+    5 F s + 16N per step, s = 4)."""
+    import torch
+
+    import rheon_b200 as R
+
+    g = R.GridGeometry((n, n, n))
+    sim = R.CarrierSimulation(g, R.CarrierConfig.mixed(pressure=R.PressureSettings(1e-8, 0.0, MAXF, 1000),
+                                                       device=local))
+    sim.init_fourier(args.seed)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    prm = R.StepParams(MAXF, cfl=0.5)
+    for _ in range(args.warmup):
+        sim.step(prm)
+    ms, its, solve = 0.0, [], 0.0
+    steps = max(1, args.steps)
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rep = sim.step(prm)
+        b.record(stream)
+        b.synchronize()
+        ms += a.elapsed_time(b)
+        its.append(rep.pressure.iterations)
+        solve += rep.pressure_ms
+    sim.close()
+    cells = n ** 3
+    faces = 3 * n * n * (n + 1)
+    step_bytes = statistics.mean(its) * 130 * cells + 5 * faces * 4 + 16 * cells
+    hbm, hbm_kind = peaks()
+    ach = step_bytes / (ms / steps / 1e3) / 1e9
+    return {"workload": f"mixed carrier step at {n}^3, random-Fourier init, CFL 0.5, rel 1e-8",
+            "value": cells * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+            "pressure_ms_per_step": solve / steps, "iterations_per_step": statistics.mean(its),
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "peak_kind": hbm_kind, "unit": "GB/s",
+                         "frac": ach / hbm, "bytes_per_step": step_bytes,
+                         "model": "130N per outer iteration + 5Fs + 16N per step"}}
 
 
 def run_serving(args, local):
-    """Serving loop: requests of k in [1, 20] steps on boxes with edges
-    log-uniform in [32, 256] (multiples of 8), random-Fourier initial velocity,
+    """Serving loop: step requests of k in [1, 20] steps and projection
+    requests (one projection of a supplied velocity, dt 0.01) on boxes with
+    edges log-uniform in [32, 256] (multiples of 8), random-Fourier velocity,
     mixed precision at rel. residual 1e-8, admitted while the pooled carriers
     fit the HBM budget. Capacity is measured first with every request arriving
     at once (this also warms the carrier pool); then a Poisson stream at 80 % of
     that capacity is served. The plain per-request f64 path (one request at a
     time, Jacobi-PCG f64 carriers) runs on the first requests of the same stream
-    for comparison. Latency = finish - arrival (queueing included)."""
+    for comparison. Latency = finish - arrival (queueing included); every
+    request's device interval is recorded with CUDA events on its carrier's
+    stream, and the pairs of requests whose device intervals overlap are
+    counted."""
     import torch
 
     import rheon_b200 as R
@@ -276,15 +376,17 @@ def run_serving(args, local):
     free, _total = torch.cuda.mem_get_info(local)
     budget = int(min(args.serving_budget_gb * 1e9, free - 8e9))
     cfg = R.CarrierConfig.mixed(pressure=R.PressureSettings(1e-8, 0.0, MAXF, 1000), device=local)
-    loop = SV.ServingLoop(cfg, budget)
+    share = args.serving_projection_share
+    loop = SV.ServingLoop(cfg, budget, device_times=True)
     n_cap = max(8, min(args.serving_requests, 64))
-    cap_reqs = SV.make_requests(n_cap, rate_hz=0.0, seed=args.seed + 5)
+    cap_reqs = SV.make_requests(n_cap, rate_hz=0.0, seed=args.seed + 5, projection_share=share)
     cap_done = loop.run(cap_reqs)
     capacity = len(cap_done) / loop.elapsed
     rate = 0.8 * capacity
-    reqs = SV.make_requests(args.serving_requests, rate_hz=rate, seed=args.seed + 6)
+    reqs = SV.make_requests(args.serving_requests, rate_hz=rate, seed=args.seed + 6, projection_share=share)
     done = loop.run(reqs)
     served = SV.summarize(done, loop.elapsed)
+    served["overlapping_request_pairs"] = SV.overlapping_pairs(done)
     pool_gb = loop.pool.used / 1e9
     loop.close()
     plain_cfg = R.CarrierConfig(pressure=R.PressureSettings(1e-8, 0.0, MAXF, 1000000), storage="f64",
@@ -295,8 +397,9 @@ def run_serving(args, local):
     plain_summary = SV.summarize(plain_done, plain.elapsed)
     plain.close()
     return {
-        "workload": "requests of k in [1,20] steps, edge log-uniform in [32,256] (multiple of 8), random-Fourier "
-                    "init, mixed precision to rel residual 1e-8, Poisson arrivals at 0.8 x measured capacity",
+        "workload": f"step requests of k in [1,20] steps and projection requests ({share:.0%} of the stream, dt "
+                    "0.01), edge log-uniform in [32,256] (multiple of 8), random-Fourier velocity, mixed precision "
+                    "to rel residual 1e-8, Poisson arrivals at 0.8 x measured capacity",
         "requests": args.serving_requests,
         "capacity_requests_per_s": capacity,
         "arrival_rate_per_s": rate,
@@ -863,9 +966,12 @@ def run_ours(args, world, rank, local):
     roof_kernel, roof_bytes, roof_ms, other_ms = None, None, None, None
     try:
         iter_ms = sim.profile(2, 4 * launches_prof)
-        # algorithmic bytes per iteration: phase 1 reads z, d_old and writes
-        # d_new (24N); phase 2 reads d, p, r and writes p, r, z (48N)
-        roof_kernel, roof_bytes, roof_ms = "k_jacobi_persistent (one PCG iteration)", 72 * cells, iter_ms
+        # algorithmic bytes per Jacobi-PCG iteration of the scope's minimal
+        # kernel sequence: apply_A_dot 16N + update_dots 48N + direction 24N =
+        # 88N (the persistent kernel's fused phases move 72N of it: phase 1
+        # reads z, d_old and writes d_new, phase 2 reads d, p, r and writes
+        # p, r, z)
+        roof_kernel, roof_bytes, roof_ms = "k_jacobi_persistent (one PCG iteration)", 88 * cells, iter_ms
         other_ms = sim.profile(1, launches_prof) if method != R.PressureImplementation.MG_MIXED else 0.0
     except R.SimulationError:
         pass
@@ -938,6 +1044,9 @@ def run_ours(args, world, rank, local):
                                               "model": "130N per outer iteration + 5Fs + 16N per step"}
             vs.close()
 
+    mixed256 = None
+    if not args.no_variants and rank == 0 and world == 1:
+        mixed256 = run_mixed_large(args, local, flush, 256)
     batched = None
     if not args.no_batched and rank == 0 and world == 1:
         batched = run_batched(args, local, flush)
@@ -977,9 +1086,9 @@ def run_ours(args, world, rank, local):
             "peak_kind": hbm_kind,
             "unit": "GB/s",
             "frac": achieved / hbm,
-            # DRAM bytes per iteration: dram__bytes_read.sum + dram__bytes_write.sum
-            # of one ncu capture of a 64-iteration launch at 128^3, divided by 64
-            "traffic": 55.8e6 if roof_kernel.startswith("k_jacobi_persistent") and args.n == 128 else None,
+            # DRAM bytes are not measured inside the bench (ncu replays kernels);
+            # the ncu capture of this kernel is summarised under profiles/
+            "traffic": None,
             "algorithmic_bytes_per_launch": roof_bytes,
             "avg_launch_ms": roof_ms,
             "other_pass_ms": other_ms,
@@ -995,6 +1104,22 @@ def run_ours(args, world, rank, local):
     }
     if variants:
         result["variants"] = variants
+    # the north-star comparison in short keys: mixed against plain f64 at the
+    # headline size, and the mixed path's HBM fractions (algorithmic bytes)
+    target = {}
+    if "mixed_mg_f32" in variants:
+        target["mixed_vs_plain_f64"] = variants["mixed_mg_f32"]["vs_plain_f64"]
+        target["mixed_128_frac"] = variants["mixed_mg_f32"]["roofline"]["frac"]
+    if mixed256:
+        result["mixed_256"] = mixed256
+        target["mixed_256_frac"] = mixed256["roofline"]["frac"]
+        target["mixed_256_value"] = mixed256["value"]
+    if batched:
+        target["batched_frac"] = batched["roofline"]["frac"]
+        target["batched_value"] = batched["value"]
+        target["batched_vs_plain_f64"] = batched["value"] / value
+    if target:
+        result["target"] = target
     if batched:
         result["batched"] = batched
     if serving:
@@ -1010,65 +1135,111 @@ def run_ours(args, world, rank, local):
 
 
 # ------------------------------------------------------------------ CPU arms
-def cpu_carrier(args, budget_s, threads, steps_cap):
-    """The oracle carrier step on host cores; returns (cell-steps/s, steps, seconds, sample)."""
+def cpu_carrier(args, budget_s, threads, steps_cap, warmup=0, n=None):
+    """The oracle carrier step of the bench's workload on host cores.
+
+    Runs `warmup` untimed steps from the initial state, then timed steps until
+    `steps_cap` steps or `budget_s` seconds. Returns a dict with the rate
+    (cell-steps/s), the timed steps, seconds, PCG iterations per timed step and
+    a description of the sample."""
     import oracle as O
     from rheon_b200 import workloads as W
 
-    n = (args.n,) * 3
-    g = O.grid(n)
+    edge = args.n if n is None else n
+    shape = (edge,) * 3
+    g = O.grid(shape)
     dtype = np.float64 if args.storage == "f64" else np.float32
-    faces = W.fourier_faces(n, seed=args.seed, dtype=dtype)
+    faces = W.fourier_faces(shape, seed=args.seed, dtype=dtype)
     method = O.JACOBI_PCG_V1
     s = O.settings(1e-8, 0.0, MAXF, 1000000)
-    done, t0 = 0, time.perf_counter()
-    while done < max(1, steps_cap):
+
+    def step(faces):
         _, rate = O.velocity_rate(g, faces)
         dt = min(MAXF, 0.5 / rate)
         prm = O.StepParams(dt, 1.0, method, s, 0.0, 0, threads)
         st, faces, _, rep = O.carrier_step(g, faces, prm)
         if st != O.OK:
             raise RuntimeError(f"oracle step failed: {st}")
+        return faces, rep
+
+    for _ in range(warmup):
+        faces, _ = step(faces)
+    done, iters, t0 = 0, [], time.perf_counter()
+    while done < max(1, steps_cap):
+        faces, rep = step(faces)
+        iters.append(rep.pressure.iterations)
         done += 1
         if time.perf_counter() - t0 >= budget_s:
             break
     el = time.perf_counter() - t0
-    cells = n[0] * n[1] * n[2]
-    sample = f"{done} step(s) of the same {args.n}^3 workload from its initial state, {threads} thread(s)"
-    return cells * done / el, done, el, sample
+    cells = edge ** 3
+    sample = (f"steps {warmup + 1}-{warmup + done} of the {edge}^3 workload's trajectory "
+              f"({warmup} untimed warm-up step(s) first), {threads} thread(s)")
+    return {"value": cells * done / el, "steps": done, "seconds": el, "warmup": warmup,
+            "iterations_per_step": statistics.mean(iters), "sample": sample}
 
 
 def run_reference(args, world, rank):
+    """The CPU reference arm: the oracle port of the carrier step on all host
+    cores, on the GPU arm's workload, metric and config keys. Each timed step is
+    a full step of the same trajectory; the window is bounded (one untimed
+    warm-up step, then up to --steps steps or about 150 s), so that the arm
+    ends within a few minutes."""
     import oracle
 
     oracle.lib()
     threads = os.cpu_count() or 1
-    value, done, el, sample = cpu_carrier(args, budget_s=150.0, threads=threads, steps_cap=args.steps)
+    r = cpu_carrier(args, budget_s=150.0, threads=threads, steps_cap=args.steps, warmup=min(args.warmup, 1))
+    value = r["value"]
+    cells = args.n ** 3
     return {
         "impl": "reference",
         "metric": METRIC,
         "value": value,
         "unit": UNIT,
         "n_gpus": world,
-        "steps": done,
-        "warmup": 0,
-        "ms_per_step": el * 1e3 / done,
+        "steps": r["steps"],
+        "warmup": r["warmup"],
+        "ms_per_step": r["seconds"] * 1e3 / r["steps"],
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": args.storage,
         "data": "synthetic (seeded SplitMix64 random-Fourier velocity, host-generated)",
-        "config": {"workload": WORKLOAD.format(n=args.n, storage=args.storage, method="Jacobi-PCG"),
-                   "cells": args.n ** 3},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "config": {
+            "workload": WORKLOAD.format(n=args.n, storage=args.storage, method="Jacobi-PCG"),
+            "cells": cells,
+            "parallelism": f"rank 0 of {world} on host cores; replicas x{world} on the GPU arm",
+            "l2": "host caches (CPU arm)",
+            "pcg_iterations_per_step": r["iterations_per_step"],
+            "pressure_ms_per_step": None,
+            "step_window": r["sample"],
+        },
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": r["sample"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "Rheon is Rust and cannot be built here (no cargo/rustc); this arm times the oracle, a C++ "
                 "restatement of its carrier arithmetic (serial Neumaier reductions, threaded stencil loops)",
     }
 
 
+def relaunch(gpus):
+    """`--gpus N` without a torchrun environment: start N ranks on this node
+    under torch.distributed.run (rendezvous on 127.0.0.1) with the same
+    arguments and return their exit status."""
+    import socket
+
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), "--", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch(args.gpus))
     world, rank, local = dist_env()
     if world > 1:
         import datetime
@@ -1083,8 +1254,16 @@ def main():
         else:
             dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
     if args.impl == "reference":
+        ranks = [rank]
+        if world > 1:
+            import torch.distributed as dist
+
+            ranks = [None] * world
+            dist.all_gather_object(ranks, rank)
         if rank == 0:
-            print(json.dumps(run_reference(args, world, rank)), flush=True)
+            line = run_reference(args, world, rank)
+            line["ranks_started"] = sorted(ranks)
+            print(json.dumps(line), flush=True)
         if world > 1:
             import torch.distributed as dist
 
@@ -1111,8 +1290,16 @@ def main():
 
         oracle.lib()
         threads = os.cpu_count() or 1
-        v, done, el, sample = cpu_carrier(args, budget_s=args.cpu_budget, threads=threads, steps_cap=1)
-        result["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        r = cpu_carrier(args, budget_s=args.cpu_budget, threads=threads, steps_cap=1)
+        result["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port",
+                                  "sample": r["sample"], "iterations_per_step": r["iterations_per_step"]}
+        # the serial figure: one thread, as the reference's bit-faithful serial
+        # run; one step of the 64^3 box (a 128^3 step takes minutes on one core),
+        # which understates the per-cell cost of 128^3 (more iterations per step)
+        r1 = cpu_carrier(args, budget_s=args.cpu_budget, threads=1, steps_cap=1, n=min(args.n, 64))
+        result["cpu_baseline"]["single_thread"] = {"value": r1["value"], "unit": UNIT, "cores": 1,
+                                                   "sample": r1["sample"],
+                                                   "iterations_per_step": r1["iterations_per_step"]}
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:

@@ -237,10 +237,9 @@ RB200_API int rb200_workspace_profile(rb200_workspace* ws, int which, int launch
 
 /* Allocation-free Jacobi-PCG solve. No counterpart in the reference.
  *
- * For callers that must not allocate device memory: code running while a CUDA
- * graph is being captured in global mode (cudaMalloc is illegal then), or a
- * host application whose device memory is owned by its own allocator under a
- * fixed budget. It solves like rb200_workspace_solve_rhs_device with
+ * For callers that must not allocate device memory: a host application whose
+ * device memory is owned by its own allocator under a fixed budget, so that a
+ * plug-in may not grow the process's device footprint while it runs. It solves like rb200_workspace_solve_rhs_device with
  * RB200_JACOBI_PCG_V1 (same kernels, same results) on caller-owned device
  * buffers: rhs_device (read) and pressure_device (written, len doubles).
  * It calls no cudaMalloc/cudaFree or allocating routine. Its scratch is one
@@ -249,7 +248,8 @@ RB200_API int rb200_workspace_profile(rb200_workspace* ws, int which, int launch
  * cells (32^3) are rejected with RB200_UNSUPPORTED.
  *   - The first call on a device looks up that array's device address (once
  *     per device, with the device current); make that first call before any
- *     stream capture begins.
+ *     stream capture begins. The address is kept for the process: do not call
+ *     this entry point on a device after cudaDeviceReset on it.
  *   - Every call shares the one array and leaves its contents behind; calls
  *     whose work overlaps on the GPU (other threads, other streams) race and
  *     corrupt each other. Serialize them.
@@ -396,6 +396,16 @@ RB200_API int rb200_carrier_step(rb200_carrier* carrier, const rb200_step_params
  * different streams overlap on the device. rb200_carrier_step_wait blocks for
  * the report and returns the step status. */
 RB200_API int rb200_carrier_step_async(rb200_carrier* carrier, const rb200_step_params* params);
+/* A projection of the accepted state (ProjectionStepWorkspace::project,
+ * src/projection_step.rs:863-1033): the accepted faces (as uploaded) are the
+ * provisional velocity; build_rhs with dt = params->requested_dt, the pressure
+ * solve, correction, the actual divergence gate and the commit run as in a
+ * step, without advection and without the Courant gate. cfl and buoyancy must
+ * be 0, and the carrier must carry no tracer or liquid state. The async form
+ * pairs with rb200_carrier_step_wait / rb200_carrier_step_poll. */
+RB200_API int rb200_carrier_project(rb200_carrier* carrier, const rb200_step_params* params,
+                                    rb200_step_report* report);
+RB200_API int rb200_carrier_project_async(rb200_carrier* carrier, const rb200_step_params* params);
 RB200_API int rb200_carrier_step_wait(rb200_carrier* carrier, rb200_step_report* report);
 /* Nonblocking: 1 when the launched step has finished on the device (its
  * report is ready for rb200_carrier_step_wait), 0 while it runs or when no
@@ -405,6 +415,53 @@ RB200_API int rb200_carrier_step_poll(const rb200_carrier* carrier);
  * statuses[i] receives each step's status; returns the first launch error. */
 RB200_API int rb200_carriers_step(rb200_carrier* const* carriers, size_t count, const rb200_step_params* params,
                                   rb200_step_report* reports, int* statuses);
+/* ------------------------------------------------- packed batch of carriers
+ * Many independent fixed boxes of uneven sizes stepped together with the
+ * mixed-precision pressure method (f32 faces, FP32 multigrid V(2,2) inside
+ * FP64 flexible CG). No counterpart in the reference, which steps one box at a
+ * time (src/simulation.rs:812-1403); every instance follows that step owner's
+ * order, gates and transactional commit. All instances live in one device
+ * arena, every stage of the step is one launch over all of them, and a step of
+ * the whole batch is one CUDA graph (the solve a device-controlled WHILE node
+ * that runs while any instance's solve runs). An instance's results do not
+ * depend on the other instances: a batch of one gives the same bits. Each
+ * instance needs a hierarchy of at least two levels whose non-coarsest levels
+ * have an x extent that is a multiple of 4 (RB200_UNSUPPORTED otherwise), and
+ * carries no tracer. */
+typedef struct rb200_batch rb200_batch;
+
+typedef struct rb200_batch_config {
+    double density;
+    rb200_settings settings;
+    double actual_divergence_limit;/* SimulationConfig (simulation.rs:11)  */
+    double max_courant;
+    int device;
+    int fp32_advection;            /* sample/backtrace in FP32 arithmetic  */
+} rb200_batch_config;
+
+/* At most 128 instances. */
+RB200_API int rb200_batch_create(const rb200_grid* grids, size_t count, const rb200_batch_config* config,
+                                 rb200_batch** out);
+RB200_API void rb200_batch_destroy(rb200_batch* batch);
+RB200_API uint64_t rb200_batch_allocated_bytes(const rb200_batch* batch);
+RB200_API void* rb200_batch_stream(rb200_batch* batch);
+RB200_API const char* rb200_batch_last_error(const rb200_batch* batch);
+/* f32 faces of instance `index` from host or device memory (validated like
+ * rb200_carrier_upload); rb200_batch_download copies its accepted state out. */
+RB200_API int rb200_batch_upload(rb200_batch* batch, size_t index, const float* u, const float* v, const float* w);
+RB200_API int rb200_batch_download(rb200_batch* batch, size_t index, float* u, float* v, float* w);
+/* The last pressure of instance `index` (host or device memory). */
+RB200_API int rb200_batch_pressure(rb200_batch* batch, size_t index, double* out, size_t len);
+/* One step of every instance: params, reports and statuses hold one entry per
+ * instance (buoyancy must be 0). rb200_batch_step waits for the reports; the
+ * async form launches the step graph, rb200_batch_step_poll tells whether it
+ * has finished and rb200_batch_step_wait collects it. */
+RB200_API int rb200_batch_step(rb200_batch* batch, const rb200_step_params* params, rb200_step_report* reports,
+                               int* statuses);
+RB200_API int rb200_batch_step_async(rb200_batch* batch, const rb200_step_params* params);
+RB200_API int rb200_batch_step_poll(const rb200_batch* batch);
+RB200_API int rb200_batch_step_wait(rb200_batch* batch, rb200_step_report* reports, int* statuses);
+
 /* rb200_workspace_profile on the carrier's pressure solver. */
 RB200_API int rb200_carrier_profile(rb200_carrier* carrier, int which, int launches, double* avg_ms);
 /* Last pressure of the carrier (host copy). */
@@ -626,6 +683,28 @@ RB200_API int rb200_liquid_advance(rb200_liquid_volume* liquid, const rb200_liqu
                                    const rb200_liquid_inlet* inlet, const rb200_liquid_source* source,
                                    const rb200_liquid_settings* settings, rb200_liquid_report* report,
                                    void* stream);
+/* VolumeStage (src/liquid_volume.rs:18-23): the cancellation points of an
+ * interval, asked in the reference's order (prepare_with_boundary,
+ * src/liquid_volume.rs:558-830): BeforeFlux once; FaceFluxSlice once per z
+ * plane of each axis's faces (for the periodic seam check, then for the face
+ * transfers); CellUpdateSlice once per z plane of cells; BeforeCommit once,
+ * after every check. A nonzero return cancels: RB200_LIQUID_REJECTED with
+ * report->error = RB200_LIQUID_CANCELLED and report->error_cell = the stage,
+ * the accepted state unchanged. The transport runs on the device before the
+ * points are asked, so an error the reference meets before a point ends the
+ * sequence there, as in the reference. */
+typedef enum rb200_volume_stage {
+    RB200_VOLUME_BEFORE_FLUX = 0,
+    RB200_VOLUME_FACE_FLUX_SLICE = 1,
+    RB200_VOLUME_CELL_UPDATE_SLICE = 2,
+    RB200_VOLUME_BEFORE_COMMIT = 3
+} rb200_volume_stage;
+typedef int (*rb200_liquid_cancel_fn)(void* ctx, int stage);
+/* rb200_liquid_advance with the cancellation callback (NULL: never cancel). */
+RB200_API int rb200_liquid_advance_cancellable(rb200_liquid_volume* liquid, const rb200_liquid_flow* flow,
+                                               const rb200_liquid_inlet* inlet, const rb200_liquid_source* source,
+                                               const rb200_liquid_settings* settings, rb200_liquid_cancel_fn cancel,
+                                               void* ctx, rb200_liquid_report* report, void* stream);
 /* LiquidVolumeState::advance_periodic (src/liquid_volume.rs:389-406): the box
  * wraps around on every axis. The two faces of each seam must carry the same
  * velocity (else RB200_LIQUID_PERIODIC_VELOCITY_MISMATCH), inflow through a
@@ -635,6 +714,12 @@ RB200_API int rb200_liquid_advance_periodic(rb200_liquid_volume* liquid, const r
                                             rb200_liquid_stamp boundary, const rb200_liquid_source* source,
                                             const rb200_liquid_settings* settings, rb200_liquid_report* report,
                                             void* stream);
+RB200_API int rb200_liquid_advance_periodic_cancellable(rb200_liquid_volume* liquid, const rb200_liquid_flow* flow,
+                                                        rb200_liquid_stamp boundary,
+                                                        const rb200_liquid_source* source,
+                                                        const rb200_liquid_settings* settings,
+                                                        rb200_liquid_cancel_fn cancel, void* ctx,
+                                                        rb200_liquid_report* report, void* stream);
 
 /* The liquid step on the resident carrier (LiquidTransportSimulation,
  * src/liquid_step.rs:828-900): the carrier owns a liquid-volume state, and

@@ -710,6 +710,23 @@ class CarrierSimulation:
         if st != N.OK:
             raise SimulationError(st)
 
+    def project(self, dt: float) -> StepReport:
+        """ProjectionStepWorkspace::project (src/projection_step.rs:863-1033)
+        of the accepted state: the uploaded faces are projected with `dt`
+        (no advection, no Courant gate) and become the accepted state."""
+        r = N.StepReport()
+        st = lib().rb200_carrier_project(self._handle, C.byref(self._params(StepParams(dt))), C.byref(r))
+        rep = self._report(r)
+        if st != N.OK:
+            raise SimulationError(st, rep)
+        return rep
+
+    def project_async(self, dt: float) -> None:
+        """Launch a projection without waiting; pair with step_wait()."""
+        st = lib().rb200_carrier_project_async(self._handle, C.byref(self._params(StepParams(dt))))
+        if st != N.OK:
+            raise SimulationError(st)
+
     def step_done(self) -> bool:
         """Nonblocking: has the step launched by step_async finished?"""
         return bool(lib().rb200_carrier_step_poll(self._handle))
@@ -733,3 +750,111 @@ def step_all(sims: Sequence["CarrierSimulation"], params: Sequence[StepParams]):
     sts = (C.c_int * n)()
     lib().rb200_carriers_step(handles, n, prm, reps, sts)
     return [(int(sts[i]), CarrierSimulation._report(reps[i])) for i in range(n)]
+
+
+class BatchedCarriers:
+    """Many independent fixed boxes of uneven sizes stepped together: every
+    stage of the step is one launch over all instances and one step of the
+    batch is one CUDA graph (mixed precision: f32 faces, FP32 multigrid inside
+    FP64 flexible CG). Each instance's results are the same bits as in a batch
+    of its own."""
+
+    def __init__(self, grids: Sequence[GridGeometry], config: Optional[CarrierConfig] = None):
+        config = config or CarrierConfig.mixed()
+        if config.storage != "f32" or config.implementation != PressureImplementation.MG_MIXED:
+            raise SimulationError(N.UNSUPPORTED, detail="batched carriers use the mixed method (f32 faces)")
+        if config.with_tracer or config.warm_start:
+            raise SimulationError(N.UNSUPPORTED, detail="batched carriers carry no tracer and no warm start")
+        self.grids = list(grids)
+        self.config = config
+        arr = (N.Grid * len(self.grids))(*[g.c() for g in self.grids])
+        c = N.BatchConfig(config.density, config.pressure.c(), config.actual_divergence_limit, config.max_courant,
+                          config.device, 1 if config.fp32_advection else 0)
+        h = C.c_void_p()
+        st = lib().rb200_batch_create(arr, len(self.grids), C.byref(c), C.byref(h))
+        if st != N.OK:
+            raise SimulationError(st, detail="batch construction")
+        self._handle = h
+
+    def __len__(self):
+        return len(self.grids)
+
+    def close(self):
+        if getattr(self, "_handle", None) is not None:
+            lib().rb200_batch_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def allocated_bytes(self) -> int:
+        return int(lib().rb200_batch_allocated_bytes(self._handle))
+
+    def stream(self) -> int:
+        return int(lib().rb200_batch_stream(self._handle) or 0)
+
+    def upload(self, index: int, faces: Sequence[np.ndarray]):
+        fs = [np.ascontiguousarray(f, dtype=np.float32) for f in faces]
+        for d in range(3):
+            if fs[d].size != self.grids[index].face_len(d):
+                raise SimulationError(N.LENGTH_MISMATCH)
+        st = lib().rb200_batch_upload(self._handle, index, *[f.ctypes.data_as(C.c_void_p) for f in fs])
+        if st != N.OK:
+            raise SimulationError(st)
+
+    def upload_ptrs(self, index: int, u: int, v: int, w: int):
+        """Upload from host or device pointers (e.g. pinned buffers)."""
+        st = lib().rb200_batch_upload(self._handle, index, u, v, w)
+        if st != N.OK:
+            raise SimulationError(st)
+
+    def download(self, index: int):
+        fs = [np.empty(self.grids[index].face_len(d), np.float32) for d in range(3)]
+        st = lib().rb200_batch_download(self._handle, index, *[f.ctypes.data_as(C.c_void_p) for f in fs])
+        if st != N.OK:
+            raise SimulationError(st)
+        return fs
+
+    def download_ptrs(self, index: int, u: int, v: int, w: int):
+        st = lib().rb200_batch_download(self._handle, index, u, v, w)
+        if st != N.OK:
+            raise SimulationError(st)
+
+    def pressure(self, index: int) -> np.ndarray:
+        out = np.empty(self.grids[index].cell_len(), np.float64)
+        st = lib().rb200_batch_pressure(self._handle, index, out.ctypes.data_as(C.c_void_p), out.size)
+        if st != N.OK:
+            raise SimulationError(st)
+        return out
+
+    def _params(self, params):
+        if isinstance(params, StepParams):
+            params = [params] * len(self.grids)
+        return (N.StepParams * len(self.grids))(*[CarrierSimulation._params(p) for p in params])
+
+    def step(self, params) -> list:
+        """One step of every instance (one CUDA graph); returns
+        [(status, StepReport)] per instance. `params` is one StepParams for
+        all instances or one per instance."""
+        self.step_async(params)
+        return self.step_wait()
+
+    def step_async(self, params) -> None:
+        st = lib().rb200_batch_step_async(self._handle, self._params(params))
+        if st != N.OK:
+            raise SimulationError(st, detail=(lib().rb200_batch_last_error(self._handle) or b"").decode())
+
+    def step_done(self) -> bool:
+        return bool(lib().rb200_batch_step_poll(self._handle))
+
+    def step_wait(self) -> list:
+        n = len(self.grids)
+        reps = (N.StepReport * n)()
+        sts = (C.c_int * n)()
+        st = lib().rb200_batch_step_wait(self._handle, reps, sts)
+        if st != N.OK:
+            raise SimulationError(st)
+        return [(int(sts[i]), CarrierSimulation._report(reps[i])) for i in range(n)]

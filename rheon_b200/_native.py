@@ -55,6 +55,9 @@ LIQUID_ERRORS = {0: "Ok", 1: "InvalidDensity", 2: "InvalidFraction", 3: "Invalid
                  13: "CourantLimit", 14: "DivergenceLimit", 15: "FractionBounds", 16: "BalanceLimit",
                  17: "ArithmeticFailure", 18: "Cancelled", 19: "GeometryMismatch", 20: "PeriodicVelocityMismatch"}
 
+# rb200_volume_stage: VolumeStage (src/liquid_volume.rs:18-23)
+VOLUME_STAGES = ("BeforeFlux", "FaceFluxSlice", "CellUpdateSlice", "BeforeCommit")
+
 # rb200_box_flux_error: BoxFluxError's own variants (src/box_flux.rs:60-72)
 BOX_FLUX_ERRORS = {0: "Ok", 1: "InvalidBoundary", 2: "InvalidSettings", 3: "InvalidMass", 4: "BufferLimit",
                    5: "IncompatibleFlux", 6: "Cancelled", 7: "DivergenceLimit", 8: "ArithmeticFailure"}
@@ -103,6 +106,11 @@ class CarrierConfig(C.Structure):
                 ("settings", Settings), ("actual_divergence_limit", C.c_double), ("max_courant", C.c_double),
                 ("with_tracer", C.c_int), ("device", C.c_int), ("fp32_advection", C.c_int),
                 ("warm_start", C.c_int)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("density", C.c_double), ("settings", Settings), ("actual_divergence_limit", C.c_double),
+                ("max_courant", C.c_double), ("device", C.c_int), ("fp32_advection", C.c_int)]
 
 
 class StepParams(C.Structure):
@@ -291,9 +299,23 @@ SIGNATURES = {
     "rb200_carrier_state_device": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "rb200_carrier_step": (_I, [_P, C.POINTER(StepParams), C.POINTER(StepReport), CANCEL_FN, _P]),
     "rb200_carrier_step_async": (_I, [_P, C.POINTER(StepParams)]),
+    "rb200_carrier_project": (_I, [_P, C.POINTER(StepParams), C.POINTER(StepReport)]),
+    "rb200_carrier_project_async": (_I, [_P, C.POINTER(StepParams)]),
     "rb200_carrier_step_wait": (_I, [_P, C.POINTER(StepReport)]),
     "rb200_carrier_step_poll": (_I, [_P]),
     "rb200_carriers_step": (_I, [C.POINTER(_P), _S, C.POINTER(StepParams), C.POINTER(StepReport), C.POINTER(_I)]),
+    "rb200_batch_create": (_I, [C.POINTER(Grid), _S, C.POINTER(BatchConfig), C.POINTER(_P)]),
+    "rb200_batch_destroy": (None, [_P]),
+    "rb200_batch_allocated_bytes": (C.c_uint64, [_P]),
+    "rb200_batch_stream": (_P, [_P]),
+    "rb200_batch_last_error": (C.c_char_p, [_P]),
+    "rb200_batch_upload": (_I, [_P, _S, _P, _P, _P]),
+    "rb200_batch_download": (_I, [_P, _S, _P, _P, _P]),
+    "rb200_batch_pressure": (_I, [_P, _S, _P, _S]),
+    "rb200_batch_step": (_I, [_P, C.POINTER(StepParams), C.POINTER(StepReport), C.POINTER(_I)]),
+    "rb200_batch_step_async": (_I, [_P, C.POINTER(StepParams)]),
+    "rb200_batch_step_poll": (_I, [_P]),
+    "rb200_batch_step_wait": (_I, [_P, C.POINTER(StepReport), C.POINTER(_I)]),
     "rb200_carrier_profile": (_I, [_P, _I, _I, C.POINTER(_D)]),
     "rb200_carrier_pressure": (_I, [_P, _P, _S]),
     "rb200_carrier_dense3d_fields": (_I, [_P, C.POINTER(Dense3dFields)]),
@@ -324,6 +346,12 @@ SIGNATURES = {
                                   C.POINTER(LiquidSettings), C.POINTER(LiquidReport), _P]),
     "rb200_liquid_advance_periodic": (_I, [_P, C.POINTER(LiquidFlow), LiquidStamp, C.POINTER(LiquidSource),
                                            C.POINTER(LiquidSettings), C.POINTER(LiquidReport), _P]),
+    "rb200_liquid_advance_cancellable": (_I, [_P, C.POINTER(LiquidFlow), C.POINTER(LiquidInlet),
+                                              C.POINTER(LiquidSource), C.POINTER(LiquidSettings), STEP_CANCEL_FN, _P,
+                                              C.POINTER(LiquidReport), _P]),
+    "rb200_liquid_advance_periodic_cancellable": (_I, [_P, C.POINTER(LiquidFlow), LiquidStamp,
+                                                       C.POINTER(LiquidSource), C.POINTER(LiquidSettings),
+                                                       STEP_CANCEL_FN, _P, C.POINTER(LiquidReport), _P]),
     "rb200_carrier_attach_liquid": (_I, [_P, _D, LiquidStamp, C.c_uint64, _P, C.c_uint64, C.POINTER(LiquidReport)]),
     "rb200_carrier_liquid_inputs": (_I, [_P, C.POINTER(LiquidInlet), C.POINTER(LiquidSource),
                                          C.POINTER(LiquidSettings)]),

@@ -20,6 +20,19 @@ __device__ __forceinline__ R clampd(R x, R lo, R hi) {
     return x;
 }
 
+// (x - o_d) / h_d correctly rounded, through the reciprocal of h_d and one
+// exact remainder (common.cuh) instead of a division: the same bits.
+template <class R>
+__device__ __forceinline__ R div_h(R r, const GridDev& g, int d);
+template <>
+__device__ __forceinline__ double div_h<double>(double r, const GridDev& g, int d) {
+    return div_diag(r, g.h[d], g.rh[d]);
+}
+template <>
+__device__ __forceinline__ float div_h<float>(float r, const GridDev& g, int d) {
+    return div_f32(r, float(g.h[d]), g.rhf[d]);
+}
+
 // ScalarSampler::sample (src/sampling.rs:74-122) in arithmetic type R: double
 // reproduces the reference; float is the mixed-precision path.
 template <class T, class R>
@@ -30,7 +43,7 @@ __device__ __forceinline__ R sample(const GridDev& g, const T* __restrict__ valu
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         R x = clampd<R>(pos[d], R(g.o[d]), R(g.up[d]));
-        R q = clampd<R>((x - R(g.o[d])) / R(g.h[d]) - off[d], R(0), R(dims[d] - 1));
+        R q = clampd<R>(div_h<R>(x - R(g.o[d]), g, d) - off[d], R(0), R(dims[d] - 1));
         if (!isfinite(q)) {
             flag |= VF_ARITH;
             q = R(0);
@@ -117,11 +130,12 @@ __device__ __forceinline__ void backtrace(const GridDev& g, const Faces<T>& vel,
 // every other face samples its own component at the RK2 departure point.
 template <class T, class R>
 __device__ __forceinline__ void advect_velocity_body(const GridDev& g, const Faces<T>& vel, double dt, T* ou, T* ov,
-                                                     T* ow, const float* __restrict__ tracer, double gb, int* flags) {
+                                                     T* ow, const float* __restrict__ tracer, double gb, int* flags,
+                                                     Span sp) {
     const long long total = (long long)g.flen[0] + g.flen[1] + g.flen[2];
     int local = 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
+    for (long long t = sp.block * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)sp.blocks * blockDim.x) {
         int a = 0;
         long long f = t;
         if (f >= g.flen[0]) {
@@ -132,10 +146,13 @@ __device__ __forceinline__ void advect_velocity_body(const GridDev& g, const Fac
                 a = 2;
             }
         }
+        // face coordinates by multiply-shift (face indices of one axis fit 31 bits)
+        const int fi = int(f);
         int p[3];
-        p[0] = int(f % g.fc[a][0]);
-        p[1] = int((f / g.fc[a][0]) % g.fc[a][1]);
-        p[2] = int(f / ((long long)g.fc[a][0] * g.fc[a][1]));
+        p[2] = fast_div(fi, g.fplane[a]);
+        const int in_plane = fi - p[2] * (g.fc[a][0] * g.fc[a][1]);
+        p[1] = fast_div(in_plane, g.frow[a]);
+        p[0] = in_plane - p[1] * g.fc[a][0];
         T* dst = a == 0 ? ou : (a == 1 ? ov : ow);
         if (p[a] == 0 || p[a] + 1 == g.fc[a][a]) {
             dst[f] = T(0);
@@ -169,11 +186,11 @@ __device__ __forceinline__ void advect_velocity_body(const GridDev& g, const Fac
 template <class T, class R>
 __device__ __forceinline__ void advect_tracer_body(const GridDev& g, const float* __restrict__ old,
                                                    const Faces<T>& vel, double dt, float* __restrict__ out,
-                                                   int* flags) {
+                                                   int* flags, Span sp) {
     int local = 0;
     int dims[3] = {g.n[0], g.n[1], g.n[2]};
     R off[3] = {R(0.5), R(0.5), R(0.5)};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+    for (int c = sp.block * blockDim.x + threadIdx.x; c < g.cells; c += sp.blocks * blockDim.x) {
         int p[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
         R pos[3];
 #pragma unroll

@@ -8,13 +8,13 @@ template <class T, class R>
 __global__ void __launch_bounds__(ADV_THREADS) k_advect_velocity(GridDev g, Faces<T> vel, double dt, T* ou, T* ov, T* ow,
                                                                  const float* __restrict__ tracer, double gb,
                                                                  int* flags) {
-    advect_velocity_body<T, R>(g, vel, dt, ou, ov, ow, tracer, gb, flags);
+    advect_velocity_body<T, R>(g, vel, dt, ou, ov, ow, tracer, gb, flags, whole_launch());
 }
 
 template <class T, class R>
 __global__ void __launch_bounds__(ADV_THREADS) k_advect_tracer(GridDev g, const float* __restrict__ old, Faces<T> vel,
                                                                double dt, float* __restrict__ out, int* flags) {
-    advect_tracer_body<T, R>(g, old, vel, dt, out, flags);
+    advect_tracer_body<T, R>(g, old, vel, dt, out, flags, whole_launch());
 }
 
 template <class T>

@@ -51,10 +51,20 @@ template <class T, class R>
 __global__ void __launch_bounds__(ADV_THREADS) k_carrier_advect(GridDev g, CarrierDev* cd) {
     if (!step_running(cd)) return;
     const int a = cd->acc, b = (a + 1) % 3;
+    if (cd->project_only) {
+        // a projection takes the accepted faces as the provisional velocity
+        for (int d = 0; d < 3; ++d) {
+            const T* __restrict__ src = (const T*)cd->faces[a][d];
+            T* __restrict__ dst = (T*)cd->faces[b][d];
+            for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < g.flen[d]; f += gridDim.x * blockDim.x)
+                dst[f] = src[f];
+        }
+        return;
+    }
     Faces<T> vel{{(const T*)cd->faces[a][0], (const T*)cd->faces[a][1], (const T*)cd->faces[a][2]}};
     const float* tr = cd->tracer[0] ? cd->tracer[cd->tacc] : nullptr;
     advect_velocity_body<T, R>(g, vel, cd->dt, (T*)cd->faces[b][0], (T*)cd->faces[b][1], (T*)cd->faces[b][2], tr,
-                               cd->buoyancy, &cd->flags);
+                               cd->buoyancy, &cd->flags, whole_launch());
 }
 
 template <class T>
@@ -62,7 +72,7 @@ __global__ void k_carrier_rhs(GridDev g, CarrierDev* cd, double* __restrict__ rh
     if (!step_running(cd)) return;
     const int b = (cd->acc + 1) % 3;
     build_rhs_body<T>(g, (const T*)cd->faces[b][0], (const T*)cd->faces[b][1], (const T*)cd->faces[b][2], cd->dt,
-                      rhs, &cd->flags);
+                      rhs, &cd->flags, whole_launch());
 }
 
 template <class T>
@@ -72,7 +82,7 @@ __global__ void __launch_bounds__(EW_THREADS) k_carrier_correct(GridDev g, Carri
     const int b = (cd->acc + 1) % 3, c = (cd->acc + 2) % 3;
     correct_divergence_body<T>(g, p, cd->dt, (const T*)cd->faces[b][0], (const T*)cd->faces[b][1],
                                (const T*)cd->faces[b][2], (T*)cd->faces[c][0], (T*)cd->faces[c][1],
-                               (T*)cd->faces[c][2], part, cd->scalars, &cd->flags);
+                               (T*)cd->faces[c][2], part, cd->scalars, &cd->flags, whole_launch());
 }
 
 template <class T, class R>
@@ -80,7 +90,8 @@ __global__ void __launch_bounds__(ADV_THREADS) k_carrier_tracer(GridDev g, Carri
     if (!cd->tracer[0] || !solve_usable(cd, st)) return;
     const int c = (cd->acc + 2) % 3;
     Faces<T> vel{{(const T*)cd->faces[c][0], (const T*)cd->faces[c][1], (const T*)cd->faces[c][2]}};
-    advect_tracer_body<T, R>(g, cd->tracer[cd->tacc], vel, cd->dt, cd->tracer[cd->tacc ^ 1], &cd->flags);
+    advect_tracer_body<T, R>(g, cd->tracer[cd->tacc], vel, cd->dt, cd->tracer[cd->tacc ^ 1], &cd->flags,
+                            whole_launch());
 }
 
 // The liquid interval of the step (src/liquid_step.rs:869-887): the
@@ -133,7 +144,7 @@ __global__ void k_step_end(GridDev g, CarrierDev* cd, const SolveState* st) {
                     status = RB200_DIVERGENCE_LIMIT;
                 else if (!isfinite(rep.courant))
                     status = RB200_ARITHMETIC_FAILURE;
-                else if (rep.courant > cd->max_courant)
+                else if (rep.courant > cd->max_courant && !cd->project_only)
                     status = RB200_COURANT_LIMIT;
             }
             // the liquid interval is part of the transaction: a rejected
@@ -544,11 +555,39 @@ static cudaEvent_t cooperative_lane(int device) {
     return lanes[device];
 }
 
+static int launch_step(rb200_carrier* carrier, const rb200_step_params* params, int project_only);
+
 int rb200_carrier_step_async(rb200_carrier* carrier, const rb200_step_params* params) {
+    return launch_step(carrier, params, 0);
+}
+
+// ProjectionStepWorkspace::project (src/projection_step.rs:863-1033) on the
+// resident state: the accepted faces are the provisional velocity, projected
+// with the requested dt (build_rhs, the pressure solve, correction and the
+// actual divergence gate) and committed as the new accepted state.
+int rb200_carrier_project_async(rb200_carrier* carrier, const rb200_step_params* params) {
+    if (!carrier || !params) return RB200_INVALID_ARGUMENT;
+    if (params->cfl != 0.0 || params->buoyancy != 0.0 || carrier->tracer[0] || carrier->lq_d) {
+        carrier->err = "a projection takes its dt as requested and carries no tracer or liquid state";
+        return RB200_INVALID_ARGUMENT;
+    }
+    return launch_step(carrier, params, 1);
+}
+
+int rb200_carrier_project(rb200_carrier* carrier, const rb200_step_params* params, rb200_step_report* report) {
+    if (!carrier || !params || !report) return RB200_INVALID_ARGUMENT;
+    std::memset(report, 0, sizeof(*report));
+    int rc = rb200_carrier_project_async(carrier, params);
+    if (rc) return rc;
+    return rb200_carrier_step_wait(carrier, report);
+}
+
+static int launch_step(rb200_carrier* carrier, const rb200_step_params* params, int project_only) {
     if (!carrier || !params) return RB200_INVALID_ARGUMENT;
     rb200_carrier* c = carrier;
     if (c->in_flight) return RB200_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
+    c->h_cd->project_only = project_only;
     // Step parameters into the device descriptor, then the step graph; both
     // ordered on the carrier's stream.
     c->h_cd->requested_dt = params->requested_dt;

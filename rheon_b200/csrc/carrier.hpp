@@ -26,6 +26,8 @@ struct CarrierDev {
     // step parameters (written by the host before each launch)
     double requested_dt, cfl, buoyancy;
     int iteration_limit_ok, skip_gates;
+    int project_only;    // a projection: the accepted state is projected as supplied (no advection)
+    int pad2;
     // configuration
     double max_courant, divergence_limit;
     // accepted-state bookkeeping

@@ -16,6 +16,26 @@
 
 namespace rb200 {
 
+// Exact floor(c / d) for 0 <= c < 2^31 by one multiply and shift
+// (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", 1994, the round-up method): with l = ceil(log2 d) and
+// m = floor(2^(31+l) / d) + 1, 2^(31+l) < m d <= 2^(31+l) + 2^l, so
+// floor(c m / 2^(31+l)) = floor(c / d); c m < 2^63.
+struct FastDiv {
+    unsigned long long m;
+    int shift;
+};
+
+inline FastDiv make_fastdiv(unsigned d) {
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    return FastDiv{(1ull << (31 + l)) / d + 1, 31 + l};
+}
+
+__device__ __forceinline__ int fast_div(int c, const FastDiv& f) {
+    return int((unsigned long long)(unsigned)c * f.m >> f.shift);
+}
+
 // Geometry and sealed-box operator coefficients, passed by value to kernels.
 // PressureOperator::new (src/operator.rs:58-97) fixes area, accel, weight and
 // the 64 neighbour-mask diagonals summed lower/upper x X,Y,Z.
@@ -25,6 +45,11 @@ struct GridDev {
     int flen[3];     // face array lengths
     int cells;       // n0*n1*n2
     double h[3];
+    double rh[3];    // RN(1/h_d) in double where div_diag may use it, else 0
+    float rhf[3];    // RN(1/f32(h_d)) in float where div_f32 may use it, else 0
+    int pad_rh;
+    FastDiv frow[3];    // floor(f / fc[a][0]) for a face index f of axis a
+    FastDiv fplane[3];  // floor(f / (fc[a][0] fc[a][1]))
     double o[3];
     double up[3];
     double area[3];
@@ -34,6 +59,14 @@ struct GridDev {
     double diag[64];
     double rdiag[64];  // RN(1/diag) where div_diag may use it, else 0
 };
+
+// The blocks of a launch that work on one grid: this block's index among them
+// and their number. A launch over one grid gives every block to it; a packed
+// launch over a batch of grids gives each grid a contiguous range of blocks.
+struct Span {
+    int block, blocks;
+};
+__device__ __forceinline__ Span whole_launch() { return Span{int(blockIdx.x), int(gridDim.x)}; }
 
 __device__ __forceinline__ int cell_idx(const GridDev& g, int i, int j, int k) {
     return i + g.n[0] * (j + g.n[1] * k);
@@ -76,24 +109,19 @@ __device__ __forceinline__ double div_diag(double r, double D, double y) {
     return r / D;
 }
 
-// Exact floor(c / d) for 0 <= c < 2^31 by one multiply and shift
-// (Granlund and Montgomery, "Division by invariant integers using
-// multiplication", 1994, the round-up method): with l = ceil(log2 d) and
-// m = floor(2^(31+l) / d) + 1, 2^(31+l) < m d <= 2^(31+l) + 2^l, so
-// floor(c m / 2^(31+l)) = floor(c / d); c m < 2^63.
-struct FastDiv {
-    unsigned long long m;
-    int shift;
-};
-
-inline FastDiv make_fastdiv(unsigned d) {
-    int l = 0;
-    while ((1ull << l) < d) ++l;
-    return FastDiv{(1ull << (31 + l)) / d + 1, 31 + l};
-}
-
-__device__ __forceinline__ int fast_div(int c, const FastDiv& f) {
-    return int((unsigned long long)(unsigned)c * f.m >> f.shift);
+// The same correctly rounded quotient r / D in binary32 (Markstein's theorem
+// holds for any binary precision): y = RN(1/D) in float, set only for
+// 2^-60 < D < 2^60; the fast path covers r = +-0 and 2^-60 <= |r| < 2^60, where
+// q stays within (2^-120, 2^120) and the remainder above 2^-84, all normal.
+__device__ __forceinline__ float div_f32(float r, float D, float y) {
+    const unsigned ab = __float_as_uint(r) & 0x7fffffffu;
+    const unsigned e = ab >> 23;  // biased exponent; 67..186: 2^-60 <= |r| < 2^60
+    if (y != 0.0f && (e - 67u <= 119u || ab == 0u)) {
+        const float q = r * y;
+        const float rem = fmaf(-q, D, r);
+        return copysignf(fmaf(rem, y, q), r);
+    }
+    return r / D;
 }
 
 // ------------------------------------------------------------ double-double

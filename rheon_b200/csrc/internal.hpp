@@ -67,6 +67,14 @@ inline int make_grid_dev(const rb200_grid* in, double density, GridDev* g) {
         g->o[d] = in->origin[d];
     }
     g->cells = int(cells);
+    for (int d = 0; d < 3; ++d) {
+        const double h = g->h[d];
+        g->rh[d] = (h > 0x1p-500 && h < 0x1p500) ? 1.0 / h : 0.0;
+        const float hf = float(h);
+        g->rhf[d] = (hf > 0x1p-60f && hf < 0x1p60f) ? 1.0f / hf : 0.0f;
+        g->frow[d] = make_fastdiv(unsigned(g->fc[d][0]));
+        g->fplane[d] = make_fastdiv(unsigned(g->fc[d][0]) * unsigned(g->fc[d][1]));
+    }
     g->volume = g->h[0] * g->h[1] * g->h[2];
     if (!std::isfinite(g->volume) || g->volume <= 0.0) return RB200_INVALID_ARGUMENT;
     for (int d = 0; d < 3; ++d) {

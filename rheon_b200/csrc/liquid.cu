@@ -684,11 +684,61 @@ int rb200_liquid_download(rb200_liquid_volume* V, double* out, size_t len) {
 
 namespace {
 
+// The cancellation points of prepare_with_boundary (src/liquid_volume.rs:558-830)
+// in their order: BeforeFlux once; FaceFluxSlice per z plane of the faces of
+// each axis, for the periodic seam check (:575-600) and again for the face
+// transfers (:604-611); CellUpdateSlice per z plane of the cells (:686-690);
+// BeforeCommit once, after every check (:830).
+struct VolumeCheckpoints {
+    long long seam, flux, cells;  // FaceFluxSlice polls of the seam check and of the transfers; CellUpdateSlice polls
+    long long total() const { return 1 + seam + flux + cells; }  // without BeforeCommit
+    int stage(long long index) const {
+        if (index == 0) return RB200_VOLUME_BEFORE_FLUX;
+        return index <= seam + flux ? RB200_VOLUME_FACE_FLUX_SLICE : RB200_VOLUME_CELL_UPDATE_SLICE;
+    }
+};
+
+VolumeCheckpoints checkpoints_of(const GridDev& g, int periodic) {
+    const long long flux = (long long)g.fc[0][2] + g.fc[1][2] + g.fc[2][2];
+    return VolumeCheckpoints{periodic ? flux : 0, flux, g.n[2]};
+}
+
+// How many cancellation points the reference passes before it meets the
+// device's error: the validation errors precede BeforeFlux; a seam mismatch
+// lies in the slice of its face; a cell's Courant or bounds failure in the
+// slice of its cell; the divergence limit, the ledger and the balance limit
+// after every slice. An arithmetic failure is placed after the slices: the
+// device does not record which product failed.
+long long checkpoints_before(const GridDev& g, const VolumeCheckpoints& cp, const rb200_liquid_report& r) {
+    switch (r.error) {
+        case RB200_LIQUID_PERIODIC_VELOCITY_MISMATCH: {
+            const int axis = int(r.error_actual);
+            long long before = 0;
+            for (int a = 0; a < axis; ++a) before += g.fc[a][2];
+            const long long plane = (long long)g.fc[axis][0] * g.fc[axis][1];
+            return 1 + before + (long long)r.error_cell / plane + 1;
+        }
+        case RB200_LIQUID_COURANT_LIMIT:
+        case RB200_LIQUID_FRACTION_BOUNDS:
+            return 1 + cp.seam + cp.flux + (long long)r.error_cell / ((long long)g.n[0] * g.n[1]) + 1;
+        case RB200_LIQUID_ARITHMETIC_FAILURE:
+        case RB200_LIQUID_DIVERGENCE_LIMIT:
+        case RB200_LIQUID_BALANCE_LIMIT:
+            return cp.total();
+        default:
+            return 0;
+    }
+}
+
 // One standalone interval: the inputs to the device, the transport and
-// decision, the commit on acceptance, then the report and the bookkeeping back.
+// decision into the candidate array, the reference's cancellation points
+// against that outcome, and the commit only when every point has passed;
+// then the report and the bookkeeping back. A cancellation or an error leaves
+// the accepted state untouched.
 int liquid_advance_impl(rb200_liquid_volume* V, const rb200_liquid_flow* flow, const rb200_liquid_inlet* inlet,
                         rb200_liquid_stamp boundary, int periodic, const rb200_liquid_source* source,
-                        const rb200_liquid_settings* settings, rb200_liquid_report* report, void* stream) {
+                        const rb200_liquid_settings* settings, rb200_liquid_cancel_fn cancel, void* ctx,
+                        rb200_liquid_report* report, void* stream) {
     cudaSetDevice(V->device);
     const cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : V->stream;
     LiquidFlowDev& f = *V->h_flow;
@@ -711,6 +761,21 @@ int liquid_advance_impl(rb200_liquid_volume* V, const rb200_liquid_flow* flow, c
     RB200_CUDA(cudaMemcpyAsync(V->d_flow, V->h_flow, sizeof(LiquidFlowDev), cudaMemcpyHostToDevice, s));
     RB200_CUDA(cudaMemsetAsync(V->d_rep, 0, sizeof(rb200_liquid_report), s));
     RB200_CUDA(launch_liquid_advance(V->g, V->d_L, V->d_flow, V->sc, V->blocks, V->d_rep, s));
+    if (cancel) {
+        RB200_CUDA(cudaMemcpyAsync(V->h_rep, V->d_rep, sizeof(rb200_liquid_report), cudaMemcpyDeviceToHost, s));
+        RB200_CUDA(cudaStreamSynchronize(s));
+        const VolumeCheckpoints cp = checkpoints_of(V->g, periodic);
+        const long long reach = V->h_rep->error ? checkpoints_before(V->g, cp, *V->h_rep) : cp.total() + 1;
+        for (long long q = 0; q < reach; ++q) {
+            const int stage = q < cp.total() ? cp.stage(q) : RB200_VOLUME_BEFORE_COMMIT;
+            if (cancel(ctx, stage)) {
+                *report = rb200_liquid_report{};
+                report->error = RB200_LIQUID_CANCELLED;
+                report->error_cell = uint64_t(stage);
+                return RB200_LIQUID_REJECTED;
+            }
+        }
+    }
     RB200_CUDA(launch_liquid_commit(V->d_L, V->d_rep, s));
     RB200_CUDA(cudaMemcpyAsync(V->h_rep, V->d_rep, sizeof(rb200_liquid_report), cudaMemcpyDeviceToHost, s));
     RB200_CUDA(cudaMemcpyAsync(V->h_L, V->d_L, sizeof(LiquidDev), cudaMemcpyDeviceToHost, s));
@@ -727,17 +792,33 @@ extern "C" {
 int rb200_liquid_advance(rb200_liquid_volume* V, const rb200_liquid_flow* flow, const rb200_liquid_inlet* inlet,
                          const rb200_liquid_source* source, const rb200_liquid_settings* settings,
                          rb200_liquid_report* report, void* stream) {
+    return rb200_liquid_advance_cancellable(V, flow, inlet, source, settings, nullptr, nullptr, report, stream);
+}
+
+int rb200_liquid_advance_cancellable(rb200_liquid_volume* V, const rb200_liquid_flow* flow,
+                                     const rb200_liquid_inlet* inlet, const rb200_liquid_source* source,
+                                     const rb200_liquid_settings* settings, rb200_liquid_cancel_fn cancel, void* ctx,
+                                     rb200_liquid_report* report, void* stream) {
     if (!V || !flow || !inlet || !settings || !report || !flow->u || !flow->v || !flow->w)
         return RB200_INVALID_ARGUMENT;
-    return liquid_advance_impl(V, flow, inlet, rb200_liquid_stamp{0, 0}, 0, source, settings, report, stream);
+    return liquid_advance_impl(V, flow, inlet, rb200_liquid_stamp{0, 0}, 0, source, settings, cancel, ctx, report,
+                               stream);
 }
 
 // LiquidVolumeState::advance_periodic (src/liquid_volume.rs:389-406).
 int rb200_liquid_advance_periodic(rb200_liquid_volume* V, const rb200_liquid_flow* flow, rb200_liquid_stamp boundary,
                                   const rb200_liquid_source* source, const rb200_liquid_settings* settings,
                                   rb200_liquid_report* report, void* stream) {
+    return rb200_liquid_advance_periodic_cancellable(V, flow, boundary, source, settings, nullptr, nullptr, report,
+                                                     stream);
+}
+
+int rb200_liquid_advance_periodic_cancellable(rb200_liquid_volume* V, const rb200_liquid_flow* flow,
+                                              rb200_liquid_stamp boundary, const rb200_liquid_source* source,
+                                              const rb200_liquid_settings* settings, rb200_liquid_cancel_fn cancel,
+                                              void* ctx, rb200_liquid_report* report, void* stream) {
     if (!V || !flow || !settings || !report || !flow->u || !flow->v || !flow->w) return RB200_INVALID_ARGUMENT;
-    return liquid_advance_impl(V, flow, nullptr, boundary, 1, source, settings, report, stream);
+    return liquid_advance_impl(V, flow, nullptr, boundary, 1, source, settings, cancel, ctx, report, stream);
 }
 
 }  // extern "C"

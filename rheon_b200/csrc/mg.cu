@@ -5,386 +5,10 @@
 #include <utility>
 #include <vector>
 
-#include "mg.hpp"
-#include "pcg.hpp"
+#include "mg_device.cuh"
 #include "slab.cuh"
-#include "solve_state.cuh"
 
 namespace rb200 {
-
-constexpr int MG_THREADS = 256;
-constexpr int MG_LOWER_THREADS = 1024;
-
-__device__ __forceinline__ bool mg_gate(const SolveState* st, int mode) { return gate(st->flags, mode); }
-
-// Kernels of the V-cycle are launched with programmatic stream serialisation:
-// one may start while the kernel before it drains, and waits here, before its
-// first memory access, until that kernel has completed and its writes are
-// visible (a no-op for a launch without the attribute).
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-
-__device__ __forceinline__ int mask_of(const int n[3], int i, int j, int k) {
-    return int(i > 0) | (int(i + 1 < n[0]) << 1) | (int(j > 0) << 2) | (int(j + 1 < n[1]) << 3) |
-           (int(k > 0) << 4) | (int(k + 1 < n[2]) << 5);
-}
-
-__host__ __device__ __forceinline__ long mg_pairs(const MgLevelDev& L) {
-    return long((L.n[0] + 1) >> 1) * L.n[1] * L.n[2];
-}
-
-// Work mapping of the level loops: the rows (j, k) of a level are dealt to
-// warps (row = j + n1*k), and a warp's lanes take the pair index m of the row;
-// pair m holds cells 2m and 2m+1, of which the one of colour `color` has
-// i = 2m + ((color + j + k) & 1) (i may be n0 for an odd row length).
-struct Warps {
-    int w0, nw, lane;
-};
-__device__ __forceinline__ Warps grid_warps() {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    return Warps{t >> 5, int((gridDim.x * blockDim.x) >> 5), int(threadIdx.x & 31)};
-}
-
-// Rows with fewer than 32 work items share a warp: the warp splits into
-// groups of `lanes` lanes (the largest power of two not above the items per
-// row), one row per group.
-__host__ __device__ __forceinline__ int lanes_for(int per) {
-    int lanes = 32;
-    while (lanes > 1 && lanes > per) lanes >>= 1;
-    return lanes;
-}
-struct RowSplit {
-    int first, step, lane, lanes;
-};
-__device__ __forceinline__ RowSplit split_rows(const Warps& W, int per) {
-    const int lanes = lanes_for(per), rpw = 32 / lanes;
-    return RowSplit{W.w0 * rpw + W.lane / lanes, W.nw * rpw, W.lane % lanes, lanes};
-}
-// Work items per row of the level loops (quads of 4 cells, or red-black pairs).
-__host__ __device__ __forceinline__ int sweep_items(const MgLevelDev& L) {
-    return (L.n[0] & 3) == 0 ? (L.n[0] >> 2) : ((L.n[0] + 1) >> 1);
-}
-__host__ __device__ __forceinline__ int restrict_items(const MgLevelDev& L, const MgLevelDev& C) {
-    return ((L.n[0] & 3) == 0 && L.cf[0] == 2) ? (C.n[0] >> 1) : C.n[0];
-}
-
-// Loads of level data: through L1 in the grid kernels, from L2 in the cluster
-// kernel (its CTAs exchange level data through global memory between
-// cluster barriers).
-template <bool CG>
-__device__ __forceinline__ float ldv(const float* p) {
-    if (CG) return __ldcg(p);
-    return *p;
-}
-
-// Gauss-Seidel value x = (b + sum_nb w x_nb) / D, summed x-, x+, y-, y+, z-, z+.
-template <bool CG>
-__device__ __forceinline__ float gs_value(const MgLevelDev& L, float b, int i, int j, int k, int c) {
-    const int sy = L.n[0], sz = L.n[0] * L.n[1];
-    const float* __restrict__ x = L.x;
-    float s = b;
-    if (i > 0) s += L.w[0] * ldv<CG>(x + c - 1);
-    if (i + 1 < L.n[0]) s += L.w[0] * ldv<CG>(x + c + 1);
-    if (j > 0) s += L.w[1] * ldv<CG>(x + c - sy);
-    if (j + 1 < L.n[1]) s += L.w[1] * ldv<CG>(x + c + sy);
-    if (k > 0) s += L.w[2] * ldv<CG>(x + c - sz);
-    if (k + 1 < L.n[2]) s += L.w[2] * ldv<CG>(x + c + sz);
-    return s * L.dinv[mask_of(L.n, i, j, k)];
-}
-
-template <bool CG>
-__device__ __forceinline__ float4 ld4(const float* p) {
-    if (CG) return __ldcg(reinterpret_cast<const float4*>(p));
-    return *reinterpret_cast<const float4*>(p);
-}
-__device__ __forceinline__ float f4get(const float4& v, int e) {
-    return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
-}
-__device__ __forceinline__ void f4put(float4& v, int e, float a) {
-    if (e == 0) v.x = a;
-    else if (e == 1) v.y = a;
-    else if (e == 2) v.z = a;
-    else v.w = a;
-}
-
-// The half-sweep of smooth_rows for rows whose length is a multiple of 4: a
-// lane takes 4 consecutive cells (two of each colour) with 16-byte loads of
-// the cell row and of its y and z neighbour rows, updates the two cells of
-// colour `color` in the same order of operations as gs_value, and stores the
-// 4 cells back (the other colour unchanged: nobody writes it in this sweep).
-template <bool CG>
-__device__ __forceinline__ void smooth_rows_v4(const MgLevelDev& L, const double* __restrict__ r0, int color,
-                                               bool first, const Warps& W) {
-    const int n0 = L.n[0], quads = n0 >> 2;
-    const int rows = L.n[1] * L.n[2];
-    const int sy = n0, sz = n0 * L.n[1];
-    const RowSplit S = split_rows(W, quads);
-    for (int row = S.first; row < rows; row += S.step) {
-        const int j = row % L.n[1], k = row / L.n[1];
-        const int base = n0 * row;
-        const int par = (color + j + k) & 1;
-        const int myz = (int(j > 0) << 2) | (int(j + 1 < L.n[1]) << 3) | (int(k > 0) << 4) |
-                        (int(k + 1 < L.n[2]) << 5);
-        for (int q = S.lane; q < quads; q += S.lanes) {
-            const int i0 = 4 * q;
-            const int c0 = base + i0;
-            float4 bq;
-            if (r0) {
-                const double2 lo = *reinterpret_cast<const double2*>(r0 + c0);
-                const double2 hi = *reinterpret_cast<const double2*>(r0 + c0 + 2);
-                bq = make_float4(float(lo.x), float(lo.y), float(hi.x), float(hi.y));
-                *reinterpret_cast<float4*>(L.b + c0) = bq;
-            } else {
-                bq = ld4<CG>(L.b + c0);
-            }
-            float4 out;
-            if (first) {
-                out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-#pragma unroll
-                for (int t = 0; t < 2; ++t) {
-                    const int e = par + 2 * t;
-                    const int i = i0 + e;
-                    const int mask = int(i > 0) | (int(i + 1 < n0) << 1) | myz;
-                    f4put(out, e, f4get(bq, e) * L.dinv[mask]);
-                }
-            } else {
-                const float4 xc = ld4<CG>(L.x + c0);
-                const float xl = (i0 > 0) ? ldv<CG>(L.x + c0 - 1) : 0.0f;
-                const float xr = (i0 + 4 < n0) ? ldv<CG>(L.x + c0 + 4) : 0.0f;
-                const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                const float4 ym = (myz & 4) ? ld4<CG>(L.x + c0 - sy) : z4;
-                const float4 yp = (myz & 8) ? ld4<CG>(L.x + c0 + sy) : z4;
-                const float4 zm = (myz & 16) ? ld4<CG>(L.x + c0 - sz) : z4;
-                const float4 zp = (myz & 32) ? ld4<CG>(L.x + c0 + sz) : z4;
-                out = xc;
-#pragma unroll
-                for (int t = 0; t < 2; ++t) {
-                    const int e = par + 2 * t;
-                    const int i = i0 + e;
-                    float s = f4get(bq, e);
-                    if (i > 0) s += L.w[0] * (e == 0 ? xl : f4get(xc, e - 1));
-                    if (i + 1 < n0) s += L.w[0] * (e == 3 ? xr : f4get(xc, e + 1));
-                    if (myz & 4) s += L.w[1] * f4get(ym, e);
-                    if (myz & 8) s += L.w[1] * f4get(yp, e);
-                    if (myz & 16) s += L.w[2] * f4get(zm, e);
-                    if (myz & 32) s += L.w[2] * f4get(zp, e);
-                    const int mask = int(i > 0) | (int(i + 1 < n0) << 1) | myz;
-                    f4put(out, e, s * L.dinv[mask]);
-                }
-            }
-            *reinterpret_cast<float4*>(L.x + c0) = out;
-        }
-    }
-}
-
-// Half-sweep of colour `color` over the level. With `first` the correction
-// starts from zero (red = b/D, black cleared); with r0 the FP32 right-hand
-// side of the finest level is converted from the FP64 residual on the way
-// (both cells of the pair).
-template <bool CG>
-__device__ __forceinline__ void smooth_rows(const MgLevelDev& L, const double* __restrict__ r0, int color, bool first,
-                                            const Warps& W) {
-    if ((L.n[0] & 3) == 0) {
-        smooth_rows_v4<CG>(L, r0, color, first, W);
-        return;
-    }
-    const int hx = (L.n[0] + 1) >> 1;
-    const int rows = L.n[1] * L.n[2];
-    const RowSplit S = split_rows(W, hx);
-    for (int row = S.first; row < rows; row += S.step) {
-        const int j = row % L.n[1], k = row / L.n[1];
-        const int base = L.n[0] * row;
-        const int par = (color + j + k) & 1;
-        for (int m = S.lane; m < hx; m += S.lanes) {
-            const int i = 2 * m + par;
-            const int io = i ^ 1;
-            if (first && io < L.n[0]) {
-                if (r0) L.b[io + base] = float(r0[io + base]);
-                L.x[io + base] = 0.0f;
-            }
-            if (i >= L.n[0]) continue;
-            const int c = i + base;
-            float b;
-            if (r0) {
-                b = float(r0[c]);
-                L.b[c] = b;
-            } else {
-                b = ldv<CG>(L.b + c);
-            }
-            L.x[c] = first ? b * L.dinv[mask_of(L.n, i, j, k)] : gs_value<CG>(L, b, i, j, k, c);
-        }
-    }
-}
-
-// restrict_rows for fine rows whose length is a multiple of 4 (halved along
-// x): a lane takes two coarse cells, i.e. 4 fine cells of each child row, with
-// 16-byte loads; the sums run in the same order as restrict_rows.
-template <bool CG>
-__device__ __forceinline__ void restrict_rows_v4(const MgLevelDev& L, const MgLevelDev& C, const Warps& W) {
-    const int n0 = L.n[0], sy = n0, sz = n0 * L.n[1];
-    const int rows = C.n[1] * C.n[2];
-    const int cpairs = C.n[0] >> 1;
-    const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const RowSplit S = split_rows(W, cpairs);
-    for (int row = S.first; row < rows; row += S.step) {
-        const int J = row % C.n[1], K = row / C.n[1];
-        for (int P = S.lane; P < cpairs; P += S.lanes) {
-            const int i0 = 4 * P;
-            float sum[2] = {0.0f, 0.0f};
-            for (int dk = 0; dk < L.cf[2]; ++dk)
-                for (int dj = 0; dj < L.cf[1]; ++dj) {
-                    const int j = J * L.cf[1] + dj, k = K * L.cf[2] + dk;
-                    if (j >= L.n[1] || k >= L.n[2]) continue;
-                    const int c0 = i0 + n0 * (j + L.n[1] * k);
-                    const float4 xc = ld4<CG>(L.x + c0);
-                    const float4 bq = ld4<CG>(L.b + c0);
-                    const float xl = i0 > 0 ? ldv<CG>(L.x + c0 - 1) : 0.0f;
-                    const float xr = i0 + 4 < n0 ? ldv<CG>(L.x + c0 + 4) : 0.0f;
-                    const float4 ym = j > 0 ? ld4<CG>(L.x + c0 - sy) : z4;
-                    const float4 yp = j + 1 < L.n[1] ? ld4<CG>(L.x + c0 + sy) : z4;
-                    const float4 zm = k > 0 ? ld4<CG>(L.x + c0 - sz) : z4;
-                    const float4 zp = k + 1 < L.n[2] ? ld4<CG>(L.x + c0 + sz) : z4;
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const int i = i0 + e;
-                        const float x0 = f4get(xc, e);
-                        float kx = 0.0f;
-                        if (i > 0) kx += L.w[0] * (x0 - (e == 0 ? xl : f4get(xc, e - 1)));
-                        if (i + 1 < n0) kx += L.w[0] * (x0 - (e == 3 ? xr : f4get(xc, e + 1)));
-                        if (j > 0) kx += L.w[1] * (x0 - f4get(ym, e));
-                        if (j + 1 < L.n[1]) kx += L.w[1] * (x0 - f4get(yp, e));
-                        if (k > 0) kx += L.w[2] * (x0 - f4get(zm, e));
-                        if (k + 1 < L.n[2]) kx += L.w[2] * (x0 - f4get(zp, e));
-                        sum[e >> 1] += f4get(bq, e) - kx;
-                    }
-                }
-            *reinterpret_cast<float2*>(C.b + 2 * P + C.n[0] * row) = make_float2(sum[0], sum[1]);
-        }
-    }
-}
-
-// Residual b - K x on the fine cells summed over each coarse cell's children
-// (restriction = transpose of the piecewise-constant prolongation). Warps
-// take coarse rows, lanes coarse cells along x.
-template <bool CG>
-__device__ __forceinline__ void restrict_rows(const MgLevelDev& L, const MgLevelDev& C, const Warps& W) {
-    if ((L.n[0] & 3) == 0 && L.cf[0] == 2) {
-        restrict_rows_v4<CG>(L, C, W);
-        return;
-    }
-    const int sy = L.n[0], sz = L.n[0] * L.n[1];
-    const int rows = C.n[1] * C.n[2];
-    const RowSplit S = split_rows(W, C.n[0]);
-    for (int row = S.first; row < rows; row += S.step) {
-        const int J = row % C.n[1], K = row / C.n[1];
-        for (int I = S.lane; I < C.n[0]; I += S.lanes) {
-            float sum = 0.0f;
-            for (int dk = 0; dk < L.cf[2]; ++dk)
-                for (int dj = 0; dj < L.cf[1]; ++dj)
-                    for (int di = 0; di < L.cf[0]; ++di) {
-                        const int i = I * L.cf[0] + di, j = J * L.cf[1] + dj, k = K * L.cf[2] + dk;
-                        if (i >= L.n[0] || j >= L.n[1] || k >= L.n[2]) continue;
-                        const int c = i + L.n[0] * (j + L.n[1] * k);
-                        const float xc = ldv<CG>(L.x + c);
-                        float kx = 0.0f;
-                        if (i > 0) kx += L.w[0] * (xc - ldv<CG>(L.x + c - 1));
-                        if (i + 1 < L.n[0]) kx += L.w[0] * (xc - ldv<CG>(L.x + c + 1));
-                        if (j > 0) kx += L.w[1] * (xc - ldv<CG>(L.x + c - sy));
-                        if (j + 1 < L.n[1]) kx += L.w[1] * (xc - ldv<CG>(L.x + c + sy));
-                        if (k > 0) kx += L.w[2] * (xc - ldv<CG>(L.x + c - sz));
-                        if (k + 1 < L.n[2]) kx += L.w[2] * (xc - ldv<CG>(L.x + c + sz));
-                        sum += ldv<CG>(L.b + c) - kx;
-                    }
-            C.b[I + C.n[0] * row] = sum;
-        }
-    }
-}
-
-template <bool CG>
-__device__ __forceinline__ float coarse_at(const MgLevelDev& L, const MgLevelDev& C, int i, int j, int k) {
-    return ldv<CG>(C.x + ((i >> (L.cf[0] - 1)) + C.n[0] * ((j >> (L.cf[1] - 1)) + C.n[1] * (k >> (L.cf[2] - 1)))));
-}
-
-// Prolongation fused with the first post-smoothing half-sweep (black): black
-// cells are relaxed against their red neighbours' corrected values x + P xc,
-// formed on the fly. Red cells are not written: the red half-sweep that
-// follows replaces every red value without reading it. Nothing this pass reads
-// is written by it.
-// prolong_black_rows for rows whose length is a multiple of 4, with 16-byte
-// loads and stores of the fine rows (the red cells are stored back unchanged:
-// the red half-sweep that follows replaces them without reading them).
-template <bool CG>
-__device__ __forceinline__ void prolong_black_rows_v4(const MgLevelDev& L, const MgLevelDev& C, const Warps& W) {
-    const int n0 = L.n[0], quads = n0 >> 2;
-    const int rows = L.n[1] * L.n[2];
-    const int sy = n0, sz = n0 * L.n[1];
-    const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const RowSplit S = split_rows(W, quads);
-    for (int row = S.first; row < rows; row += S.step) {
-        const int j = row % L.n[1], k = row / L.n[1];
-        const int base = n0 * row;
-        const int par = (1 + j + k) & 1;
-        const int myz = (int(j > 0) << 2) | (int(j + 1 < L.n[1]) << 3) | (int(k > 0) << 4) |
-                        (int(k + 1 < L.n[2]) << 5);
-        for (int q = S.lane; q < quads; q += S.lanes) {
-            const int i0 = 4 * q;
-            const int c0 = base + i0;
-            const float4 bq = ld4<CG>(L.b + c0);
-            const float4 xc = ld4<CG>(L.x + c0);
-            const float xl = (i0 > 0) ? ldv<CG>(L.x + c0 - 1) : 0.0f;
-            const float xr = (i0 + 4 < n0) ? ldv<CG>(L.x + c0 + 4) : 0.0f;
-            const float4 ym = (myz & 4) ? ld4<CG>(L.x + c0 - sy) : z4;
-            const float4 yp = (myz & 8) ? ld4<CG>(L.x + c0 + sy) : z4;
-            const float4 zm = (myz & 16) ? ld4<CG>(L.x + c0 - sz) : z4;
-            const float4 zp = (myz & 32) ? ld4<CG>(L.x + c0 + sz) : z4;
-            float4 out = xc;
-#pragma unroll
-            for (int t = 0; t < 2; ++t) {
-                const int e = par + 2 * t;
-                const int i = i0 + e;
-                float s = f4get(bq, e);
-                if (i > 0) s += L.w[0] * ((e == 0 ? xl : f4get(xc, e - 1)) + coarse_at<CG>(L, C, i - 1, j, k));
-                if (i + 1 < n0) s += L.w[0] * ((e == 3 ? xr : f4get(xc, e + 1)) + coarse_at<CG>(L, C, i + 1, j, k));
-                if (myz & 4) s += L.w[1] * (f4get(ym, e) + coarse_at<CG>(L, C, i, j - 1, k));
-                if (myz & 8) s += L.w[1] * (f4get(yp, e) + coarse_at<CG>(L, C, i, j + 1, k));
-                if (myz & 16) s += L.w[2] * (f4get(zm, e) + coarse_at<CG>(L, C, i, j, k - 1));
-                if (myz & 32) s += L.w[2] * (f4get(zp, e) + coarse_at<CG>(L, C, i, j, k + 1));
-                const int mask = int(i > 0) | (int(i + 1 < n0) << 1) | myz;
-                f4put(out, e, s * L.dinv[mask]);
-            }
-            *reinterpret_cast<float4*>(L.x + c0) = out;
-        }
-    }
-}
-
-template <bool CG>
-__device__ __forceinline__ void prolong_black_rows(const MgLevelDev& L, const MgLevelDev& C, const Warps& W) {
-    if ((L.n[0] & 3) == 0) {
-        prolong_black_rows_v4<CG>(L, C, W);
-        return;
-    }
-    const int hx = (L.n[0] + 1) >> 1;
-    const int rows = L.n[1] * L.n[2];
-    const int sy = L.n[0], sz = L.n[0] * L.n[1];
-    const RowSplit S = split_rows(W, hx);
-    for (int row = S.first; row < rows; row += S.step) {
-        const int j = row % L.n[1], k = row / L.n[1];
-        const int base = L.n[0] * row;
-        const int par = (1 + j + k) & 1;
-        for (int m = S.lane; m < hx; m += S.lanes) {
-            const int i = 2 * m + par;
-            if (i >= L.n[0]) continue;
-            const int c = i + base;
-            float s = ldv<CG>(L.b + c);
-            if (i > 0) s += L.w[0] * (ldv<CG>(L.x + c - 1) + coarse_at<CG>(L, C, i - 1, j, k));
-            if (i + 1 < L.n[0]) s += L.w[0] * (ldv<CG>(L.x + c + 1) + coarse_at<CG>(L, C, i + 1, j, k));
-            if (j > 0) s += L.w[1] * (ldv<CG>(L.x + c - sy) + coarse_at<CG>(L, C, i, j - 1, k));
-            if (j + 1 < L.n[1]) s += L.w[1] * (ldv<CG>(L.x + c + sy) + coarse_at<CG>(L, C, i, j + 1, k));
-            if (k > 0) s += L.w[2] * (ldv<CG>(L.x + c - sz) + coarse_at<CG>(L, C, i, j, k - 1));
-            if (k + 1 < L.n[2]) s += L.w[2] * (ldv<CG>(L.x + c + sz) + coarse_at<CG>(L, C, i, j, k + 1));
-            L.x[c] = s * L.dinv[mask_of(L.n, i, j, k)];
-        }
-    }
-}
 
 // ------------------------------------------------------------ grid kernels (large levels)
 __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(MgLevelDev L, const double* __restrict__ r0, int color,
@@ -394,109 +18,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(MgLevelDev L, const do
     smooth_rows<false>(L, r0, color, first != 0, grid_warps());
 }
 
-// Two half-sweeps in one pass (colour c1, then the other colour) over a level
-// whose rows are a multiple of 4 long, one tile of PJ x PK rows (j, k) at full
-// row length: colour c1 is relaxed on the tile and the rows around it (one
-// row of halo in j and k) from the input x into shared memory, exactly as
-// smooth_rows_v4 does, then the other colour on the tile from those rows, and
-// both colours are stored to x_out. The input x is only read and x_out only
-// written, so tiles never see each other's partial results, and the values
-// equal two consecutive half-sweeps bit for bit (the same operands in the same
-// order). With `first` the correction starts from zero. Every thread of the
-// block calls it; srow holds (PJ + 2) (PK + 2) rows.
-template <bool CG, int PJ, int PK>
-__device__ __forceinline__ void pair_tile(const MgLevelDev& L, float* __restrict__ x_out, int c1, bool first, int j0,
-                                          int k0, float4* srow) {
-    constexpr int ROWS = (PJ + 2) * (PK + 2);
-    const int n0 = L.n[0], quads = n0 >> 2, n1 = L.n[1], n2 = L.n[2];
-    const int sy = n0, sz = n0 * n1;
-    const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const float* __restrict__ x = L.x;
-    for (int it = threadIdx.x; it < ROWS * quads; it += blockDim.x) {
-        const int q = it % quads, hr = it / quads;
-        const int j = j0 - 1 + hr % (PJ + 2), k = k0 - 1 + hr / (PJ + 2);
-        if (j < 0 || j >= n1 || k < 0 || k >= n2) continue;
-        const int i0 = 4 * q;
-        const int c0 = i0 + n0 * (j + n1 * k);
-        const int par = (c1 + j + k) & 1;
-        const int myz = (int(j > 0) << 2) | (int(j + 1 < n1) << 3) | (int(k > 0) << 4) | (int(k + 1 < n2) << 5);
-        const float4 bq = ld4<CG>(L.b + c0);
-        float4 out;
-        if (first) {
-            out = z4;
-#pragma unroll
-            for (int t = 0; t < 2; ++t) {
-                const int e = par + 2 * t;
-                const int i = i0 + e;
-                f4put(out, e, f4get(bq, e) * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz]);
-            }
-        } else {
-            const float4 xc = ld4<CG>(x + c0);
-            const float xl = i0 > 0 ? ldv<CG>(x + c0 - 1) : 0.0f;
-            const float xr = i0 + 4 < n0 ? ldv<CG>(x + c0 + 4) : 0.0f;
-            const float4 ym = (myz & 4) ? ld4<CG>(x + c0 - sy) : z4;
-            const float4 yp = (myz & 8) ? ld4<CG>(x + c0 + sy) : z4;
-            const float4 zm = (myz & 16) ? ld4<CG>(x + c0 - sz) : z4;
-            const float4 zp = (myz & 32) ? ld4<CG>(x + c0 + sz) : z4;
-            out = xc;
-#pragma unroll
-            for (int t = 0; t < 2; ++t) {
-                const int e = par + 2 * t;
-                const int i = i0 + e;
-                float sum = f4get(bq, e);
-                if (i > 0) sum += L.w[0] * (e == 0 ? xl : f4get(xc, e - 1));
-                if (i + 1 < n0) sum += L.w[0] * (e == 3 ? xr : f4get(xc, e + 1));
-                if (myz & 4) sum += L.w[1] * f4get(ym, e);
-                if (myz & 8) sum += L.w[1] * f4get(yp, e);
-                if (myz & 16) sum += L.w[2] * f4get(zm, e);
-                if (myz & 32) sum += L.w[2] * f4get(zp, e);
-                f4put(out, e, sum * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz]);
-            }
-        }
-        srow[hr * quads + q] = out;
-    }
-    __syncthreads();
-    const float* __restrict__ sf = reinterpret_cast<const float*>(srow);
-    for (int it = threadIdx.x; it < PJ * PK * quads; it += blockDim.x) {
-        const int q = it % quads, tr = it / quads;
-        const int j = j0 + tr % PJ, k = k0 + tr / PJ;
-        if (j >= n1 || k >= n2) continue;
-        const int hr = (tr % PJ + 1) + (PJ + 2) * (tr / PJ + 1);
-        const int i0 = 4 * q;
-        const int c0 = i0 + n0 * (j + n1 * k);
-        const int par = (c1 + 1 + j + k) & 1;
-        const int myz = (int(j > 0) << 2) | (int(j + 1 < n1) << 3) | (int(k > 0) << 4) | (int(k + 1 < n2) << 5);
-        const float4 bq = ld4<CG>(L.b + c0);
-        const float4 xc = srow[hr * quads + q];
-        const float xl = i0 > 0 ? sf[hr * n0 + i0 - 1] : 0.0f;
-        const float xr = i0 + 4 < n0 ? sf[hr * n0 + i0 + 4] : 0.0f;
-        const float4 ym = (myz & 4) ? srow[(hr - 1) * quads + q] : z4;
-        const float4 yp = (myz & 8) ? srow[(hr + 1) * quads + q] : z4;
-        const float4 zm = (myz & 16) ? srow[(hr - (PJ + 2)) * quads + q] : z4;
-        const float4 zp = (myz & 32) ? srow[(hr + (PJ + 2)) * quads + q] : z4;
-        float4 out = xc;
-#pragma unroll
-        for (int t = 0; t < 2; ++t) {
-            const int e = par + 2 * t;
-            const int i = i0 + e;
-            float sum = f4get(bq, e);
-            if (i > 0) sum += L.w[0] * (e == 0 ? xl : f4get(xc, e - 1));
-            if (i + 1 < n0) sum += L.w[0] * (e == 3 ? xr : f4get(xc, e + 1));
-            if (myz & 4) sum += L.w[1] * f4get(ym, e);
-            if (myz & 8) sum += L.w[1] * f4get(yp, e);
-            if (myz & 16) sum += L.w[2] * f4get(zm, e);
-            if (myz & 32) sum += L.w[2] * f4get(zp, e);
-            f4put(out, e, sum * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz]);
-        }
-        *reinterpret_cast<float4*>(x_out + c0) = out;
-    }
-    __syncthreads();  // srow is free for the block's next tile
-}
 
-// Grid kernel of the pairs: one 4 x 4-row tile per block.
-constexpr int PJ = 4, PK = 4;
-constexpr int PAIR_ROWS = (PJ + 2) * (PK + 2);
-constexpr size_t kPairSmemMax = 200 * 1024;
 
 __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pair(MgLevelDev L, float* __restrict__ x_out, int c1,
                                                                int first, const SolveState* st, int mode) {
@@ -737,7 +259,8 @@ static bool coarse_pseudo_inverse(const MgLevelDev& C, std::vector<double>& G) {
     return true;
 }
 
-int Multigrid::init(const GridDev& g, cudaStream_t s) {
+std::vector<MgLevelDev> mg_level_geometry(const GridDev& g) {
+    std::vector<MgLevelDev> out;
     double h[3] = {g.h[0], g.h[1], g.h[2]};
     const double rho = g.area[0] / (g.weight[0] * g.h[0]);  // w = area/(rho h)
     int n[3] = {g.n[0], g.n[1], g.n[2]};
@@ -754,20 +277,35 @@ int Multigrid::init(const GridDev& g, cudaStream_t s) {
             L.cf[d] = n[d] > 8 ? 2 : 1;
             coarser = coarser || L.cf[d] == 2;
         }
-        const bool ok_x = cudaMalloc(&L.x, size_t(L.cells) * sizeof(float)) == cudaSuccess;
-        const bool ok_b = ok_x && cudaMalloc(&L.b, size_t(L.cells) * sizeof(float)) == cudaSuccess;
-        levels_.push_back(L);
-        if (!ok_b) return RB200_OUT_OF_MEMORY;
-        bytes_ += 2 * size_t(L.cells) * sizeof(float);
+        out.push_back(L);
         if (!coarser) break;
         for (int d = 0; d < 3; ++d) {
             h[d] *= L.cf[d];
             n[d] = (n[d] + L.cf[d] - 1) / L.cf[d];
         }
     }
+    return out;
+}
+
+bool mg_coarse_pseudo_inverse(const MgLevelDev& C, std::vector<double>& G) {
+    return C.cells <= 512 && coarse_pseudo_inverse(C, G);
+}
+
+bool mg_level_pairable(const MgLevelDev& L) {
+    return (L.n[0] & 3) == 0 && size_t(PAIR_ROWS) * size_t(L.n[0]) * sizeof(float) <= kPairSmemMax;
+}
+
+int Multigrid::init(const GridDev& g, cudaStream_t s) {
+    for (MgLevelDev L : mg_level_geometry(g)) {
+        const bool ok_x = cudaMalloc(&L.x, size_t(L.cells) * sizeof(float)) == cudaSuccess;
+        const bool ok_b = ok_x && cudaMalloc(&L.b, size_t(L.cells) * sizeof(float)) == cudaSuccess;
+        levels_.push_back(L);
+        if (!ok_b) return RB200_OUT_OF_MEMORY;
+        bytes_ += 2 * size_t(L.cells) * sizeof(float);
+    }
     const MgLevelDev& C = levels_.back();
     std::vector<double> G;
-    if (C.cells > 512 || !coarse_pseudo_inverse(C, G)) {
+    if (!mg_coarse_pseudo_inverse(C, G)) {
         set_error("multigrid coarsest-level factorisation failed");
         return RB200_UNSUPPORTED;
     }
@@ -789,7 +327,7 @@ int Multigrid::init(const GridDev& g, cudaStream_t s) {
     for (int l = 0; l < lower_first_; ++l) {
         const MgLevelDev& L = levels_[l];
         const size_t smem = size_t(PAIR_ROWS) * size_t(L.n[0]) * sizeof(float);
-        if ((L.n[0] & 3) != 0 || smem > kPairSmemMax) continue;
+        if (!mg_level_pairable(L)) continue;
         RB200_CUDA(cudaMalloc(&alt_[l], size_t(L.cells) * sizeof(float)));
         bytes_ += size_t(L.cells) * sizeof(float);
         pair_smem = std::max(pair_smem, smem);
@@ -963,341 +501,31 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
     return launches;
 }
 
-// ------------------------------------------------------------ finish
-// The finest level's last red half-sweep fused with the outer method's
-// preconditioner output: z = x (FP64, z[0] = 0 for the eliminated gauge row),
-// r.z and z.q reduced and the flexible-CG decision taken. Without a hierarchy
-// (a single level solved densely) z is copied from x.
+// ------------------------------------------------------------ flexible-CG kernels
 __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int smooth, SolveState* st,
                                                               const double* __restrict__ r,
                                                               const double* __restrict__ q, int mode, Partials part,
                                                               rb200_trace* trace) {
     pdl_wait();
-    __shared__ BlockReduce<2, 0> red;
-    if (!gate(st->flags, mode)) return;
-    Neu rz, zq;
-    const Warps W = grid_warps();
-    const int hx = (L.n[0] + 1) >> 1;
-    const int rows = L.n[1] * L.n[2];
-    if ((L.n[0] & 3) == 0) {
-        // quads of 4 cells with 16-byte loads (the same values as the pairs below)
-        const int n0 = L.n[0], quads = n0 >> 2, sy = n0, sz = n0 * L.n[1];
-        const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        for (int rw = W.w0; rw < rows; rw += W.nw) {
-            const int j = rw % L.n[1], k = rw / L.n[1];
-            const int par = (j + k) & 1;  // the red cells of the quad: par, par + 2
-            const int myz = (int(j > 0) << 2) | (int(j + 1 < L.n[1]) << 3) | (int(k > 0) << 4) |
-                            (int(k + 1 < L.n[2]) << 5);
-            for (int qd = W.lane; qd < quads; qd += 32) {
-                const int i0 = 4 * qd;
-                const int c0 = n0 * rw + i0;
-                const float4 xc = *reinterpret_cast<const float4*>(L.x + c0);
-                float4 out = xc;
-                if (smooth) {
-                    const float4 bq = *reinterpret_cast<const float4*>(L.b + c0);
-                    const float xl = i0 > 0 ? L.x[c0 - 1] : 0.0f;
-                    const float xr = i0 + 4 < n0 ? L.x[c0 + 4] : 0.0f;
-                    const float4 ym = (myz & 4) ? *reinterpret_cast<const float4*>(L.x + c0 - sy) : z4;
-                    const float4 yp = (myz & 8) ? *reinterpret_cast<const float4*>(L.x + c0 + sy) : z4;
-                    const float4 zm = (myz & 16) ? *reinterpret_cast<const float4*>(L.x + c0 - sz) : z4;
-                    const float4 zp = (myz & 32) ? *reinterpret_cast<const float4*>(L.x + c0 + sz) : z4;
-#pragma unroll
-                    for (int t = 0; t < 2; ++t) {
-                        const int e = par + 2 * t;
-                        const int i = i0 + e;
-                        float sacc = f4get(bq, e);
-                        if (i > 0) sacc += L.w[0] * (e == 0 ? xl : f4get(xc, e - 1));
-                        if (i + 1 < n0) sacc += L.w[0] * (e == 3 ? xr : f4get(xc, e + 1));
-                        if (myz & 4) sacc += L.w[1] * f4get(ym, e);
-                        if (myz & 8) sacc += L.w[1] * f4get(yp, e);
-                        if (myz & 16) sacc += L.w[2] * f4get(zm, e);
-                        if (myz & 32) sacc += L.w[2] * f4get(zp, e);
-                        f4put(out, e, sacc * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz]);
-                    }
-                    *reinterpret_cast<float4*>(L.x + c0) = out;
-                }
-                double zc[4];
-#pragma unroll
-                for (int e = 0; e < 4; ++e) zc[e] = (c0 + e == 0) ? 0.0 : double(f4get(out, e));
-                const double2 r01 = *reinterpret_cast<const double2*>(r + c0);
-                const double2 r23 = *reinterpret_cast<const double2*>(r + c0 + 2);
-                const double rr[4] = {r01.x, r01.y, r23.x, r23.y};
-                double qq[4] = {0.0, 0.0, 0.0, 0.0};
-                if (mode == MODE_ITER) {
-                    const double2 q01 = *reinterpret_cast<const double2*>(q + c0);
-                    const double2 q23 = *reinterpret_cast<const double2*>(q + c0 + 2);
-                    qq[0] = q01.x;
-                    qq[1] = q01.y;
-                    qq[2] = q23.x;
-                    qq[3] = q23.y;
-                }
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    if (c0 + e == 0) continue;
-                    rz.add(rr[e] * zc[e]);
-                    if (mode == MODE_ITER) zq.add(zc[e] * qq[e]);
-                }
-            }
-        }
-    } else
-    for (int rw = W.w0; rw < rows; rw += W.nw) {
-        const int j = rw % L.n[1], k = rw / L.n[1];
-        const int row = L.n[0] * rw;
-        const int par = (j + k) & 1;
-        for (int m = W.lane; m < hx; m += 32) {
-            const int i = 2 * m + par;  // the red cell of the pair
-            const int ib = i ^ 1;
-            if (ib < L.n[0]) {  // the black cell of the pair: its value is final
-                const int c = ib + row;
-                const double zc = c == 0 ? 0.0 : double(L.x[c]);
-                if (c != 0) {
-                    rz.add(r[c] * zc);
-                    if (mode == MODE_ITER) zq.add(zc * q[c]);
-                }
-            }
-            if (i < L.n[0]) {
-                const int c = i + row;
-                float xv = L.x[c];
-                if (smooth) {
-                    xv = gs_value<false>(L, L.b[c], i, j, k, c);
-                    L.x[c] = xv;
-                }
-                const double zc = c == 0 ? 0.0 : double(xv);
-                if (c != 0) {
-                    rz.add(r[c] * zc);
-                    if (mode == MODE_ITER) zq.add(zc * q[c]);
-                }
-            }
-        }
-    }
-    dd sums[2] = {rz.as_dd(), zq.as_dd()};
-    double none[1];
-    block_reduce<2, 0>(red, sums, none);
-    if (publish_and_check_last<2, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
-        fold_partials<2, 0>(part, gridDim.x, red, sums, none);
-        if (threadIdx.x == 0) decide_flexible(st, trace, dd_value(sums[0]), dd_value(sums[1]), mode);
-    }
+    finish_red_body(L, smooth, st, r, q, mode, part, trace, whole_launch());
 }
 
-// The flexible-CG direction pass of the mixed method (src/pressure.rs:657-668,
-// :720-731): d = z + beta d (d = z after a restart), q = K d stored, d.q and
-// the decision for alpha. z is read straight from the V-cycle's FP32 output x
-// of the finest level (z = f64(x), z[0] = 0 for the eliminated gauge row), so
-// no FP64 copy of z is stored. One warp per cell row, lanes along x.
 __global__ void __launch_bounds__(MG_THREADS) k_mg_pass1(GridDev g, MgLevelDev L, SolveState* st, double* d0,
                                                          double* d1, double* __restrict__ q, Partials part,
                                                          rb200_trace* trace, int kc_len) {
     pdl_wait();
-    __shared__ BlockReduce<1, 0> red;
-    const int flags = st->flags;
-    if (flags & F_STOP) return;
-    const bool fresh = (flags & F_REPLACED) != 0;
-    const double beta = st->beta;
-    const int dsel = st->dsel;
-    const double* __restrict__ src = dsel ? d1 : d0;
-    double* __restrict__ dst = dsel ? d0 : d1;
-    const float* __restrict__ x = L.x;
-    auto dn = [&](int c) -> double {
-        const double zc = c == 0 ? 0.0 : double(x[c]);
-        return fresh ? zc : zc + beta * src[c];
-    };
-    const int sy = g.n[0], sz = g.n[0] * g.n[1];
-    Neu acc;
-    const Warps W = grid_warps();
-    const int rows = g.n[1] * g.n[2];
-    if ((g.n[0] & 3) == 0) {
-        // quads of 4 cells: x with 16-byte loads, d with two 16-byte loads
-        const int n0 = g.n[0], quads = n0 >> 2;
-        auto dn4 = [&](int c0, double (&o)[4]) {
-            const float4 xv = *reinterpret_cast<const float4*>(x + c0);
-            const double zc[4] = {c0 == 0 ? 0.0 : double(xv.x), double(xv.y), double(xv.z), double(xv.w)};
-            if (fresh) {
-#pragma unroll
-                for (int e = 0; e < 4; ++e) o[e] = zc[e];
-            } else {
-                const double2 a = *reinterpret_cast<const double2*>(src + c0);
-                const double2 b2 = *reinterpret_cast<const double2*>(src + c0 + 2);
-                o[0] = zc[0] + beta * a.x;
-                o[1] = zc[1] + beta * a.y;
-                o[2] = zc[2] + beta * b2.x;
-                o[3] = zc[3] + beta * b2.y;
-            }
-        };
-        // A warp takes a line of up to 32 quads of row j and marches along z
-        // over kc_len rows, keeping the z-neighbour rows in registers: each
-        // row of d and x is loaded once for the line plus once per y
-        // neighbour row, instead of once per stencil row that reads it.
-        const int qsegs = (quads + 31) >> 5;
-        const int kcs = (g.n[2] + kc_len - 1) / kc_len;
-        const int lines = qsegs * g.n[1] * kcs;
-        for (int line = W.w0; line < lines; line += W.nw) {
-            const int qseg = line % qsegs, t = line / qsegs;
-            const int j = t % g.n[1], k_begin = (t / g.n[1]) * kc_len;
-            const int k_end = min(g.n[2], k_begin + kc_len);
-            const int qd = qseg * 32 + W.lane;
-            if (qd >= quads) continue;
-            const int i0 = 4 * qd;
-            double prev[4] = {0, 0, 0, 0}, cur[4], next[4];
-            const int base0 = n0 * (j + g.n[1] * k_begin) + i0;
-            if (k_begin > 0) dn4(base0 - sz, prev);
-            dn4(base0, cur);
-            for (int k = k_begin; k < k_end; ++k) {
-                const int c0 = base0 + (k - k_begin) * sz;
-                double ym[4] = {0, 0, 0, 0}, yp[4] = {0, 0, 0, 0};
-#pragma unroll
-                for (int e = 0; e < 4; ++e) next[e] = 0.0;
-                if (k + 1 < g.n[2]) dn4(c0 + sz, next);
-                if (j > 0) dn4(c0 - sy, ym);
-                if (j + 1 < g.n[1]) dn4(c0 + sy, yp);
-                const double xl = i0 > 0 ? dn(c0 - 1) : 0.0;
-                const double xr = i0 + 4 < n0 ? dn(c0 + 4) : 0.0;
-                double qq[4];
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    Neigh v;
-                    v.c = cur[e];
-                    v.xm = e == 0 ? xl : cur[e - 1];
-                    v.xp = e == 3 ? xr : cur[e + 1];
-                    v.ym = ym[e];
-                    v.yp = yp[e];
-                    v.zm = prev[e];
-                    v.zp = next[e];
-                    qq[e] = (c0 + e == 0) ? 0.0 : apply_row(g, i0 + e, j, k, v);
-                }
-                *reinterpret_cast<double2*>(dst + c0) = make_double2(cur[0], cur[1]);
-                *reinterpret_cast<double2*>(dst + c0 + 2) = make_double2(cur[2], cur[3]);
-                *reinterpret_cast<double2*>(q + c0) = make_double2(qq[0], qq[1]);
-                *reinterpret_cast<double2*>(q + c0 + 2) = make_double2(qq[2], qq[3]);
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    acc.add(cur[e] * qq[e]);
-                    prev[e] = cur[e];
-                    cur[e] = next[e];
-                }
-            }
-        }
-    } else
-    for (int rw = W.w0; rw < rows; rw += W.nw) {
-        const int j = rw % g.n[1], k = rw / g.n[1];
-        const int base = g.n[0] * rw;
-        for (int i = W.lane; i < g.n[0]; i += 32) {
-            const int c = base + i;
-            Neigh v;
-            v.c = dn(c);
-            v.xm = i > 0 ? dn(c - 1) : 0.0;
-            v.xp = i + 1 < g.n[0] ? dn(c + 1) : 0.0;
-            v.ym = j > 0 ? dn(c - sy) : 0.0;
-            v.yp = j + 1 < g.n[1] ? dn(c + sy) : 0.0;
-            v.zm = k > 0 ? dn(c - sz) : 0.0;
-            v.zp = k + 1 < g.n[2] ? dn(c + sz) : 0.0;
-            const double qv = c == 0 ? 0.0 : apply_row(g, i, j, k, v);
-            dst[c] = v.c;
-            q[c] = qv;
-            acc.add(v.c * qv);
-        }
-    }
-    dd sums[1] = {acc.as_dd()};
-    double none[1];
-    block_reduce<1, 0>(red, sums, none);
-    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
-        fold_partials<1, 0>(part, gridDim.x, red, sums, none);
-        if (threadIdx.x == 0) decide_pass1(st, trace, dd_value(sums[0]), flags, dsel);
-    }
+    pass1_body(g, L, st, d0, d1, q, part, trace, kc_len, whole_launch());
 }
 
-// The flexible-CG update (p += alpha d, r -= alpha q, |r|^2 and the candidate
-// test) fused with the V-cycle's first half-sweep on the finest level, which
-// needs no neighbour: b = f32(r), red x = b / D, black x = 0. Used when the
-// finest level is a grid-kernel level.
 __global__ void __launch_bounds__(MG_THREADS) k_mg_update_first(GridDev g, MgLevelDev L, SolveState* st,
                                                                 double* __restrict__ p, double* __restrict__ r,
                                                                 const double* d0, const double* d1,
                                                                 const double* __restrict__ q, Partials part,
                                                                 rb200_trace* trace) {
     pdl_wait();
-    __shared__ BlockReduce<1, 0> red;
-    const int flags = st->flags;
-    if (flags & F_STOP) return;
-    const double alpha = st->alpha;
-    const double* __restrict__ d = st->dsel ? d1 : d0;
-    Neu acc;
-    const Warps W = grid_warps();
-    const int n0 = g.n[0], rows = g.n[1] * g.n[2];
-    for (int rw = W.w0; rw < rows; rw += W.nw) {
-        const int j = rw % g.n[1], k = rw / g.n[1];
-        const int base = n0 * rw;
-        const int par = (j + k) & 1;  // the red cells of a quad: par, par + 2
-        const int myz = (int(j > 0) << 2) | (int(j + 1 < g.n[1]) << 3) | (int(k > 0) << 4) |
-                        (int(k + 1 < g.n[2]) << 5);
-        if ((n0 & 3) == 0) {
-            for (int qd = W.lane; qd < (n0 >> 2); qd += 32) {
-                const int i0 = 4 * qd;
-                const int c0 = base + i0;
-                double pv[4], rv[4], dv[4], qv[4];
-                *reinterpret_cast<double2*>(pv) = *reinterpret_cast<const double2*>(p + c0);
-                *reinterpret_cast<double2*>(pv + 2) = *reinterpret_cast<const double2*>(p + c0 + 2);
-                *reinterpret_cast<double2*>(rv) = *reinterpret_cast<const double2*>(r + c0);
-                *reinterpret_cast<double2*>(rv + 2) = *reinterpret_cast<const double2*>(r + c0 + 2);
-                *reinterpret_cast<double2*>(dv) = *reinterpret_cast<const double2*>(d + c0);
-                *reinterpret_cast<double2*>(dv + 2) = *reinterpret_cast<const double2*>(d + c0 + 2);
-                *reinterpret_cast<double2*>(qv) = *reinterpret_cast<const double2*>(q + c0);
-                *reinterpret_cast<double2*>(qv + 2) = *reinterpret_cast<const double2*>(q + c0 + 2);
-                float4 bq, xq = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    if (c0 + e != 0) {  // the gauge row keeps p[0] = r[0] = 0
-                        pv[e] = pv[e] + alpha * dv[e];
-                        rv[e] = rv[e] - alpha * qv[e];
-                        acc.add(rv[e] * rv[e]);
-                    }
-                    f4put(bq, e, float(rv[e]));
-                }
-#pragma unroll
-                for (int t = 0; t < 2; ++t) {
-                    const int e = par + 2 * t;
-                    const int i = i0 + e;
-                    f4put(xq, e, f4get(bq, e) * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz]);
-                }
-                *reinterpret_cast<double2*>(p + c0) = *reinterpret_cast<double2*>(pv);
-                *reinterpret_cast<double2*>(p + c0 + 2) = *reinterpret_cast<double2*>(pv + 2);
-                *reinterpret_cast<double2*>(r + c0) = *reinterpret_cast<double2*>(rv);
-                *reinterpret_cast<double2*>(r + c0 + 2) = *reinterpret_cast<double2*>(rv + 2);
-                *reinterpret_cast<float4*>(L.b + c0) = bq;
-                *reinterpret_cast<float4*>(L.x + c0) = xq;
-            }
-        } else {
-            for (int i = W.lane; i < n0; i += 32) {
-                const int c = base + i;
-                double rc = r[c];
-                if (c != 0) {
-                    p[c] = p[c] + alpha * d[c];
-                    rc = rc - alpha * q[c];
-                    r[c] = rc;
-                    acc.add(rc * rc);
-                }
-                const float b = float(rc);
-                L.b[c] = b;
-                const bool isred = ((i + j + k) & 1) == 0;
-                L.x[c] = isred ? b * L.dinv[int(i > 0) | (int(i + 1 < n0) << 1) | myz] : 0.0f;
-            }
-        }
-    }
-    dd sums[1] = {acc.as_dd()};
-    double none[1];
-    block_reduce<1, 0>(red, sums, none);
-    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
-        fold_partials<1, 0>(part, gridDim.x, red, sums, none);
-        if (threadIdx.x == 0) {
-            if (flags & F_PROFILE) return;
-            const int it = st->it + 1;
-            st->it = it;
-            const double recursive_l2 = sqrt(dd_value(sums[0]));
-            st->recursive_l2 = recursive_l2;
-            if (trace) trace[it - 1].recursive_l2 = recursive_l2;
-            if (recursive_l2 <= st->threshold || it == st->max_it) st->flags = flags | F_CANDIDATE;
-        }
-    }
+    update_first_body(g, L, st, p, r, d0, d1, q, part, trace, whole_launch());
 }
+
 
 int Multigrid::enqueue_update_first(const GridDev& g, void* state, double* p, double* r, double* d0, double* d1,
                                     const double* q, Partials part, rb200_trace* trace, cudaStream_t s) const {

@@ -53,6 +53,17 @@ struct MgLower {
     int count;
 };
 
+// The hierarchy of a grid (geometry and tables; no buffers): every axis longer
+// than 8 cells is halved, rounding up, until all are at most 8.
+std::vector<MgLevelDev> mg_level_geometry(const GridDev& g);
+// The FP64 pseudo-inverse of the coarsest level's operator (cells x cells,
+// row-major); false when the level has more than 512 cells or is singular
+// beyond its constant null space.
+bool mg_coarse_pseudo_inverse(const MgLevelDev& C, std::vector<double>& G);
+// Whether a level's red and black half-sweeps can run as one fused pair
+// (rows a multiple of 4 long, tile rows within the shared-memory limit).
+bool mg_level_pairable(const MgLevelDev& L);
+
 class Multigrid {
 public:
     Multigrid() = default;

@@ -97,7 +97,7 @@ int launch_validate_faces(const GridDev& g, const T* u, const T* v, const T* w, 
 template <class T>
 __global__ void k_build_rhs(GridDev g, const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w,
                             double dt, double* __restrict__ out, int* flags) {
-    build_rhs_body<T>(g, u, v, w, dt, out, flags);
+    build_rhs_body<T>(g, u, v, w, dt, out, flags, whole_launch());
 }
 
 template <class T>
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(EW_THREADS) k_correct_divergence(GridDev g, co
                                                                    const T* __restrict__ iw, T* __restrict__ ou,
                                                                    T* __restrict__ ov, T* __restrict__ ow,
                                                                    Partials part, double* out_scalars, int* flags) {
-    correct_divergence_body<T>(g, p, dt, iu, iv, iw, ou, ov, ow, part, out_scalars, flags);
+    correct_divergence_body<T>(g, p, dt, iu, iv, iw, ou, ov, ow, part, out_scalars, flags, whole_launch());
 }
 
 template <class T>

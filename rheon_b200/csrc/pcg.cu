@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "pcg.hpp"
+#include "pcg_device.cuh"
 #include "slab.cuh"
 #include "solve_state.cuh"
 #include "stencil.cuh"
@@ -27,142 +28,19 @@ namespace rb200 {
 
 constexpr int EW = 256;
 constexpr int EW_CAP = 148 * 8;
-constexpr double kEps = 2.220446049250313e-16;
 
 // ------------------------------------------------------------------ init
-// Compatibility sums, threshold and the true report of p = 0
-// (src/pressure.rs:603-647); p is zeroed here. A seeded solve (F_WARM) keeps p,
-// validates it after the compatibility check (finite, p[0] == 0,
-// :615-624) and leaves its true report to the true-residual kernel.
 __global__ void __launch_bounds__(EW) k_init_sums(GridDev g, SolveState* st, const double* __restrict__ b,
                                                   double* __restrict__ p, Partials part) {
-    __shared__ BlockReduce<3, 3> sm;
-    const int flags0 = st->flags;
-    if (flags0 & F_DONE) return;
-    const bool warm = (flags0 & F_WARM) != 0;
-    dd s[3] = {{0, 0}, {0, 0}, {0, 0}};
-    double m[3] = {0.0, 0.0, 0.0};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
-        double x = b[c];
-        if (warm) {
-            if (!isfinite(p[c])) m[2] = 1.0;
-        } else {
-            p[c] = 0.0;
-        }
-        if (!isfinite(x)) m[1] = 1.0;
-        s[0] = dd_add1(s[0], x);
-        s[1] = dd_add1(s[1], fabs(x));
-        s[2] = dd_add1(s[2], x * x);
-        m[0] = fmax(m[0], fabs(x));
-    }
-    block_reduce<3, 3>(sm, s, m);
-    if (publish_and_check_last<3, 3>(part, blockIdx.x, gridDim.x, s, m)) {
-        fold_partials<3, 3>(part, gridDim.x, sm, s, m);
-        if (threadIdx.x == 0) {
-            int flags = st->flags;
-            if (m[1] != 0.0) {
-                finish(st, RB200_NONFINITE_INPUT, flags);
-                return;
-            }
-            double sum = dd_value(s[0]), sum_abs = dd_value(s[1]), sq = dd_value(s[2]);
-            double budget = (64.0 * kEps) * sum_abs;
-            if (!isfinite(sum) || !isfinite(sum_abs)) {
-                breakdown(st, 0, flags);
-                return;
-            }
-            if (fabs(sum) > budget) {
-                st->incompatible_sum = sum;
-                st->incompatible_budget = budget;
-                finish(st, RB200_INCOMPATIBLE_RHS, flags);
-                return;
-            }
-            if (warm) {
-                if (m[2] != 0.0) {
-                    finish(st, RB200_NONFINITE_INPUT, flags);
-                    return;
-                }
-                if (p[0] != 0.0) {
-                    finish(st, RB200_INVALID_INITIAL_PRESSURE, flags);
-                    return;
-                }
-            }
-            double rhs_l2 = sqrt(sq);
-            double threshold = fmax(st->absolute, st->relative * rhs_l2);
-            if (!isfinite(rhs_l2) || !isfinite(threshold)) {
-                breakdown(st, 0, flags);
-                return;
-            }
-            st->threshold = threshold;
-            if (warm) {
-                // true_report(p0) runs next, in the true-residual kernel.
-                st->flags = flags | F_STOP | F_NEED_TRUE;
-                return;
-            }
-            // true_report(p = 0): the product is exactly b.
-            double div = m[0] * st->dt / g.volume;
-            if (!isfinite(sq) || !isfinite(div)) {
-                breakdown(st, 0, flags);
-                return;
-            }
-            st->true_l2 = rhs_l2;
-            st->true_max = m[0];
-            st->true_div = div;
-            if (rhs_l2 <= threshold && div <= st->divergence_limit) {
-                finish(st, RB200_OK, flags);
-                return;
-            }
-            if (st->max_it == 0) {
-                finish(st, RB200_ITERATION_LIMIT, flags);
-                return;
-            }
-        }
-    }
+    init_sums_body(g, st, b, p, part, whole_launch());
 }
 
-// r <- src (r[0] = 0) and the preconditioned start. Jacobi stores z = r/D and
-// reduces r.z, then decides; the red-black SGS method stores y = r/D on the
-// red cells (its forward red solve) and leaves the rest to its sweep kernels.
-// Used for the initial residual (MODE_INIT, src = b) and for the restart
-// (MODE_REPLACE, src = the true residual in the spare direction buffer).
-// KIND: 0 Jacobi, 1 red-black SGS, 2 copy only (multigrid and lexicographic
-// SGS form z in their own kernels).
-enum : int { KIND_JACOBI = 0, KIND_RBSGS = 1, KIND_MG = 2 };
 template <int KIND>
 __global__ void __launch_bounds__(EW) k_load_residual(GridDev g, SolveState* st, const double* b,
                                                       double* d0, double* d1, double* __restrict__ r,
                                                       double* __restrict__ z, int mode, Partials part,
                                                       rb200_trace* trace) {
-    __shared__ BlockReduce<1, 0> sm;
-    const int flags = st->flags;
-    if (!gate(flags, mode)) return;
-    const double* src = mode == MODE_INIT ? b : (st->dsel ? d0 : d1);
-    Neu acc;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
-        double rc = c == 0 ? 0.0 : src[c];
-        r[c] = rc;
-        if (c == 0) {
-            z[0] = 0.0;
-            continue;
-        }
-        if (KIND == KIND_MG) continue;
-        int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
-        if (KIND == KIND_JACOBI) {
-            const int m = diag_mask(g, i, j, k);
-            double zc = div_diag(rc, g.diag[m], g.rdiag[m]);
-            z[c] = zc;
-            acc.add(rc * zc);
-        } else if (((i + j + k) & 1) == 0) {
-            z[c] = rc / diag_at(g, i, j, k);
-        }
-    }
-    if (KIND != KIND_JACOBI) return;
-    dd sums[1] = {acc.as_dd()};
-    double none[1];
-    block_reduce<1, 0>(sm, sums, none);
-    if (publish_and_check_last<1, 0>(part, blockIdx.x, gridDim.x, sums, none)) {
-        fold_partials<1, 0>(part, gridDim.x, sm, sums, none);
-        if (threadIdx.x == 0) decide_rz(st, trace, dd_value(sums[0]), mode);
-    }
+    load_residual_body<KIND>(g, st, b, d0, d1, r, z, mode, part, trace, whole_launch());
 }
 
 // precondition_jacobi (src/pressure.rs:534-575) as a primitive: z = r/D on
@@ -1478,19 +1356,23 @@ int launch_precondition_jacobi(const GridDev& g, const double* r, double* z, Par
 int precondition_partials_blocks() { return EW_CAP; }
 
 // ------------------------------------------------------------ allocation-free solve
-// A Jacobi-PCG solve for callers that cannot allocate device memory: code that
-// runs while a CUDA graph is being captured in global mode (cudaMalloc is not
-// allowed then), or inside a host process whose device memory is owned by
-// another allocator under a fixed budget. Its scratch (residual, two
-// direction buffers, preconditioned residual, reduction partials, solver state
-// and ticket) lives in this fixed file-scope device array, which every GPU that
-// loads the library holds until the process exits. It has no counterpart in
-// the reference.
+// A Jacobi-PCG solve for callers that cannot allocate device memory: a host
+// application whose device memory is owned by its own allocator under a fixed
+// budget, so that a plug-in may not grow its footprint while it runs. Its
+// scratch (residual, two direction buffers, preconditioned residual,
+// reduction partials, solver state and ticket) lives in this fixed file-scope
+// device array, which every GPU that loads the library holds until the process
+// exits. It has no counterpart in the reference.
 constexpr int kStaticMaxCells = 32768;   // 32^3 cells
-constexpr int kStaticMaxBlocks = 2048;   // reduction partials of one pass
+constexpr int kStaticMaxBlocks = 2048;   // blocks of the widest pass of a solve
+// Doubles of one block's reduction partials in the widest stage of a solve:
+// k_init_sums publishes 3 double-double sums and 3 maxima (2 * 3 + 3); the
+// other stages publish fewer (true residual 5, pass 2 4, pass 1 and the
+// residual load 2).
+constexpr int kStaticSlotDoubles = 2 * 3 + 3;
 constexpr size_t kStaticStateDoubles = 64;
-constexpr size_t kStaticDoubles =
-    4 * size_t(kStaticMaxCells) + size_t(kStaticMaxBlocks) * 8 + kStaticStateDoubles;
+constexpr size_t kStaticPartialDoubles = size_t(kStaticMaxBlocks) * kStaticSlotDoubles;
+constexpr size_t kStaticDoubles = 4 * size_t(kStaticMaxCells) + kStaticPartialDoubles + kStaticStateDoubles;
 static __device__ __align__(256) double g_static_scratch[kStaticDoubles];
 
 static_assert(sizeof(SolveState) + sizeof(unsigned) <= kStaticStateDoubles * sizeof(double),
@@ -1498,7 +1380,10 @@ static_assert(sizeof(SolveState) + sizeof(unsigned) <= kStaticStateDoubles * siz
 
 // Device address of g_static_scratch per device, resolved once per device
 // with that device current. In host code the symbol itself is only a host-side
-// stand-in, never a device address.
+// stand-in, never a device address. The cached address belongs to the
+// device's primary context: after cudaDeviceReset the array may be loaded at
+// another address, so a process that resets a device must not call the
+// allocation-free solve on it again.
 static double* static_scratch_address(int device, int* rc) {
     static std::mutex mu;
     static double* addr[64] = {};
@@ -1527,7 +1412,9 @@ int static_solve_jacobi(const GridDev& g, const double* rhs, double* pressure, d
         set_error("grid exceeds the 32768-cell limit of the allocation-free solve");
         return RB200_UNSUPPORTED;
     }
-    if (slab_blocks(g) > kStaticMaxBlocks || ew_blocks(g.cells) > kStaticMaxBlocks) {
+    // every stage's partials (at most kStaticSlotDoubles per block) must fit
+    // the reserved region
+    if (size_t(std::max(slab_blocks(g), ew_blocks(g.cells))) * kStaticSlotDoubles > kStaticPartialDoubles) {
         set_error("grid shape needs more reduction blocks than the allocation-free solve holds");
         return RB200_UNSUPPORTED;
     }
@@ -1546,7 +1433,7 @@ int static_solve_jacobi(const GridDev& g, const double* rhs, double* pressure, d
     B.z = B.d1 + kStaticMaxCells;
     B.q = nullptr;
     B.part.data = B.z + kStaticMaxCells;
-    double* state_slot = B.part.data + size_t(kStaticMaxBlocks) * 8;
+    double* state_slot = B.part.data + kStaticPartialDoubles;
     B.st = reinterpret_cast<SolveState*>(state_slot);
     B.part.ticket = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(state_slot) + sizeof(SolveState));
     B.trace = nullptr;

@@ -312,6 +312,16 @@ __device__ __forceinline__ bool run_bricks(Ctx& c, uint64_t* full, uint64_t* emp
                 }
                 issue(w, int(slot));
             }
+            // Wait (bounded) until the copies of the last ring's worth of
+            // issued slots have landed: when a consumer gave up early nobody
+            // waits on them, and the block must not move on or exit with a
+            // bulk copy into its shared memory still in flight. On the normal
+            // path the consumers have waited on them already, or soon will.
+            const unsigned issued = slot_count - c.ring;
+            for (unsigned k = issued > unsigned(NS) ? issued - unsigned(NS) : 0u; k < issued; ++k) {
+                const unsigned sc = c.ring + k;
+                if (!mbar_wait_bounded(&full[sc % NS], (sc / NS) & 1u)) ok = false;
+            }
         }
     } else {
         for (BrickWalk w(c); w.b < c.nbricks; w.next(c), ++slot_count) {

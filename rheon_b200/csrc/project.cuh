@@ -17,8 +17,8 @@ constexpr float kF32Max = 3.40282346638528859811704183484516925440e+38f;
 template <class T>
 __device__ __forceinline__ void build_rhs_body(const GridDev& g, const T* __restrict__ u, const T* __restrict__ v,
                                                const T* __restrict__ w, double dt, double* __restrict__ out,
-                                               int* flags) {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+                                               int* flags, Span sp) {
+    for (int c = sp.block * blockDim.x + threadIdx.x; c < g.cells; c += sp.blocks * blockDim.x) {
         int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
         double flux = 0.0;
         flux += g.area[0] * (double(u[face_idx(g, 0, i, j, k)]) - double(u[face_idx(g, 0, i + 1, j, k)]));
@@ -76,14 +76,14 @@ __device__ __forceinline__ void correct_divergence_body(const GridDev& g, const 
                                                         const T* __restrict__ iu, const T* __restrict__ iv,
                                                         const T* __restrict__ iw, T* __restrict__ ou,
                                                         T* __restrict__ ov, T* __restrict__ ow, Partials part,
-                                                        double* out_scalars, int* flags) {
+                                                        double* out_scalars, int* flags, Span sp) {
     __shared__ BlockReduce<0, 4> sm;
     const T* in[3] = {iu, iv, iw};
     T* out[3] = {ou, ov, ow};
     const int s[3] = {1, g.n[0], g.n[0] * g.n[1]};
     double mx[4] = {0.0, 0.0, 0.0, 0.0};
     int local = 0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
+    for (int c = sp.block * blockDim.x + threadIdx.x; c < g.cells; c += sp.blocks * blockDim.x) {
         int ijk[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
         double lo[3], hi[3];
         const double pc = p[c];
@@ -112,9 +112,8 @@ __device__ __forceinline__ void correct_divergence_body(const GridDev& g, const 
     if (local) atomicOr(flags, local);
     dd none[1];
     block_reduce<0, 4>(sm, none, mx);
-    const int bid = blockIdx.x;
-    if (publish_and_check_last<0, 4>(part, bid, gridDim.x, none, mx)) {
-        fold_partials<0, 4>(part, gridDim.x, sm, none, mx);
+    if (publish_and_check_last<0, 4>(part, sp.block, sp.blocks, none, mx)) {
+        fold_partials<0, 4>(part, sp.blocks, sm, none, mx);
         if (threadIdx.x == 0)
             for (int q = 0; q < 4; ++q) out_scalars[q] = mx[q];
     }

@@ -40,8 +40,11 @@ class LiquidVolumeError(RuntimeError):
     def from_report(cls, status: int, r: N.LiquidReport) -> "LiquidVolumeError":
         if status != N.LIQUID_REJECTED:
             return cls(N.STATUS_NAMES.get(status, f"Status{status}"), status=status)
-        return cls(N.LIQUID_ERRORS.get(r.error, f"Error{r.error}"), int(r.error_cell), r.error_actual,
-                   r.error_limit, status)
+        err = cls(N.LIQUID_ERRORS.get(r.error, f"Error{r.error}"), int(r.error_cell), r.error_actual,
+                  r.error_limit, status)
+        # Cancelled { stage } (src/liquid_volume.rs:60-62)
+        err.stage = N.VOLUME_STAGES[int(r.error_cell)] if err.kind == "Cancelled" else None
+        return err
 
 
 @dataclass
@@ -192,33 +195,48 @@ class LiquidVolumeState:
     def _settings(settings):
         return N.LiquidSettings(settings.max_outward_courant, settings.actual_divergence_limit)
 
+    @staticmethod
+    def _cancel(cancel):
+        """The C callback for `cancel(stage_name) -> bool` (None: never)."""
+        if cancel is None:
+            return N.STEP_CANCEL_FN()
+        return N.STEP_CANCEL_FN(lambda ctx, stage: 1 if cancel(N.VOLUME_STAGES[stage]) else 0)
+
     def advance(self, velocity, start: float, dt: float, flow_stamp, inlet: LiquidInlet,
-                settings: LiquidVolumeSettings, source=None, source_stamp=(0, 0), stream: int = 0
-                ) -> LiquidVolumeReport:
+                settings: LiquidVolumeSettings, source=None, source_stamp=(0, 0), stream: int = 0,
+                cancel=None) -> LiquidVolumeReport:
         """One interval through the f32 face velocities `velocity` (three CUDA
         tensors, or device pointers) over [start, start + dt]; source: an f64
-        CUDA tensor of m^3/s per cell or None."""
+        CUDA tensor of m^3/s per cell or None. `cancel(stage)` is asked at the
+        reference's VolumeStage points ("BeforeFlux", "FaceFluxSlice",
+        "CellUpdateSlice", "BeforeCommit"); True cancels with the state
+        unchanged (LiquidVolumeError kind "Cancelled", .stage)."""
         inl = N.LiquidInlet(N.LiquidStamp(*inlet.stamp),
                             (C.c_double * 6)(*[float(x) for pair in inlet.fraction for x in pair]))
         src = self._source(source, source_stamp)
         rep = N.LiquidReport()
-        st = lib().rb200_liquid_advance(self._h, C.byref(self._flow(velocity, start, dt, flow_stamp)), C.byref(inl),
-                                        C.byref(src) if src else None, C.byref(self._settings(settings)),
-                                        C.byref(rep), stream or None)
+        cb = self._cancel(cancel)
+        st = lib().rb200_liquid_advance_cancellable(self._h, C.byref(self._flow(velocity, start, dt, flow_stamp)),
+                                                    C.byref(inl), C.byref(src) if src else None,
+                                                    C.byref(self._settings(settings)), cb, None, C.byref(rep),
+                                                    stream or None)
         if st != N.OK:
             raise LiquidVolumeError.from_report(st, rep)
         return LiquidVolumeReport.from_c(rep)
 
     def advance_periodic(self, velocity, start: float, dt: float, flow_stamp, boundary_stamp,
-                         settings: LiquidVolumeSettings, source=None, source_stamp=(0, 0), stream: int = 0
-                         ) -> LiquidVolumeReport:
+                         settings: LiquidVolumeSettings, source=None, source_stamp=(0, 0), stream: int = 0,
+                         cancel=None) -> LiquidVolumeReport:
         """advance_periodic (src/liquid_volume.rs:389-406): the box wraps
-        around on every axis; seams must carry equal velocities."""
+        around on every axis; seams must carry equal velocities. `cancel` as
+        for advance."""
         src = self._source(source, source_stamp)
         rep = N.LiquidReport()
-        st = lib().rb200_liquid_advance_periodic(self._h, C.byref(self._flow(velocity, start, dt, flow_stamp)),
-                                                 N.LiquidStamp(*boundary_stamp), C.byref(src) if src else None,
-                                                 C.byref(self._settings(settings)), C.byref(rep), stream or None)
+        cb = self._cancel(cancel)
+        st = lib().rb200_liquid_advance_periodic_cancellable(
+            self._h, C.byref(self._flow(velocity, start, dt, flow_stamp)), N.LiquidStamp(*boundary_stamp),
+            C.byref(src) if src else None, C.byref(self._settings(settings)), cb, None, C.byref(rep),
+            stream or None)
         if st != N.OK:
             raise LiquidVolumeError.from_report(st, rep)
         return LiquidVolumeReport.from_c(rep)

@@ -1,7 +1,11 @@
-"""Device-resident serving loop for carrier-step requests.
+"""Device-resident serving loop for carrier-step and projection requests.
 
-A request asks for k steps of the fixed-box carrier on a fresh box of a given
-edge, initialised with a seeded random-Fourier velocity. The loop is
+A step request asks for k steps of the fixed-box carrier on a fresh box of a
+given edge, initialised with a seeded random-Fourier velocity. A projection
+request supplies a velocity (here the seeded random-Fourier field, generated
+on the device) that is projected once with its own dt
+(ProjectionStepWorkspace::project, src/projection_step.rs:863-1033): the
+corrected faces and the pressure are its result. The loop is
 continuous batching, not a queue: every admitted request owns a resident
 carrier (its own CUDA stream and step graph), each request's next step is
 launched as soon as its previous one finishes, and requests that arrive while
@@ -38,8 +42,10 @@ class Request:
     rid: int
     arrival: float      # seconds after the start of the run
     edge: int           # cells per axis
-    steps: int
+    steps: int          # 1 for a projection
     seed: int
+    kind: str = "step"  # "step" or "projection"
+    dt: float = 0.0     # a projection's dt
 
 
 @dataclass
@@ -52,6 +58,11 @@ class Completion:
     finished: float
     status: int
     iterations: List[int] = field(default_factory=list)
+    kind: str = "step"
+    # device interval of the request's work (ms after the loop's reference
+    # event): from before its first launch to after its last one
+    device_start_ms: float = float("nan")
+    device_end_ms: float = float("nan")
 
     @property
     def latency(self) -> float:
@@ -59,20 +70,27 @@ class Completion:
 
 
 def make_requests(count: int, rate_hz: float, seed: int = W.DEFAULT_SEED, edge_min: int = 32, edge_max: int = 256,
-                  max_steps: int = 20) -> List[Request]:
+                  max_steps: int = 20, projection_share: float = 0.0, projection_dt: float = 0.01) -> List[Request]:
     """Poisson arrivals at rate_hz; edge log-uniform in [edge_min, edge_max]
-    rounded to a multiple of 8; steps uniform in [1, max_steps]; all drawn
-    from counter-based SplitMix64 streams of `seed`."""
+    rounded to a multiple of 8; steps uniform in [1, max_steps]; a share of
+    the requests are projections (one projection with dt = projection_dt);
+    all drawn from counter-based SplitMix64 streams of `seed`."""
     u_gap = (W.uniform(seed, 32, count) + 1.0) * 0.5
     u_edge = (W.uniform(seed, 33, count) + 1.0) * 0.5
     u_steps = (W.uniform(seed, 34, count) + 1.0) * 0.5
+    u_kind = (W.uniform(seed, 35, count) + 1.0) * 0.5
     gaps = -np.log1p(-np.minimum(u_gap, 1.0 - 1e-16)) / rate_hz if rate_hz > 0 else np.zeros(count)
     arrivals = np.cumsum(gaps) - (gaps[0] if count else 0.0)
     log_e = math.log(edge_min) + u_edge * (math.log(edge_max) - math.log(edge_min))
     edges = np.clip(np.round(np.exp(log_e) / 8.0) * 8, edge_min, edge_max).astype(int)
     steps = np.minimum(max_steps, 1 + np.floor(u_steps * max_steps)).astype(int)
-    return [Request(i, float(arrivals[i]), int(edges[i]), int(steps[i]), int(seed + 7919 * (i + 1)))
-            for i in range(count)]
+    out = []
+    for i in range(count):
+        proj = bool(u_kind[i] < projection_share)
+        out.append(Request(i, float(arrivals[i]), int(edges[i]), 1 if proj else int(steps[i]),
+                           int(seed + 7919 * (i + 1)), "projection" if proj else "step",
+                           projection_dt if proj else 0.0))
+    return out
 
 
 def shard_requests(requests: Sequence[Request], rank: int, world: int) -> List[Request]:
@@ -119,14 +137,24 @@ class CarrierPool:
         if self.free[edge]:
             self.lru.pop(id(self.free[edge][-1]), None)
             return self.free[edge].pop()
+        # make room by the estimate, then book the carrier's actual bytes:
+        # a carrier that turns out larger than estimated makes more room or
+        # is released, so the pool never exceeds the budget
         need = carrier_bytes_estimate(edge, self.config)
         while self.used + need > self.budget and self._evict_one(except_edge=edge):
             pass
         if self.used + need > self.budget:
             return None
         sim = CarrierSimulation(GridGeometry((edge, edge, edge)), self.config)
-        self.used += sim.allocated_bytes()
+        actual = sim.allocated_bytes()
+        while self.used + actual > self.budget and self._evict_one(except_edge=edge):
+            pass
+        if self.used + actual > self.budget:
+            sim.close()
+            return None
+        self.used += actual
         self.created += 1
+        assert self.used <= self.budget
         return sim
 
     def release(self, edge: int, sim: CarrierSimulation) -> None:
@@ -160,10 +188,31 @@ class ServingLoop:
     """Continuous-batching loop over resident carriers (see module docstring)."""
 
     def __init__(self, config: CarrierConfig, budget_bytes: int, params: Optional[StepParams] = None,
-                 max_in_flight: int = 1 << 30):
+                 max_in_flight: int = 1 << 30, device_times: bool = False):
         self.pool = CarrierPool(config, budget_bytes)
         self.params = params or StepParams(MAXF, cfl=0.5)
         self.max_in_flight = max_in_flight
+        self.device_times = device_times
+
+    def _event(self, sim: Optional[CarrierSimulation]):
+        """A timing event recorded on the carrier's stream (None: the current
+        stream), or None without device timing."""
+        if not self.device_times:
+            return None
+        import torch
+
+        ev = torch.cuda.Event(enable_timing=True)
+        if sim is None:
+            ev.record()
+        else:
+            ev.record(torch.cuda.ExternalStream(sim.stream()))
+        return ev
+
+    def _launch(self, req: Request, sim: CarrierSimulation) -> None:
+        if req.kind == "projection":
+            sim.project_async(req.dt)
+        else:
+            sim.step_async(self.params)
 
     def run(self, requests: Sequence[Request], keep_state: bool = False,
             on_complete: Optional[Callable[[Completion, CarrierSimulation], None]] = None) -> List[Completion]:
@@ -171,6 +220,8 @@ class ServingLoop:
         active: Dict[int, dict] = {}
         done: List[Completion] = []
         self.final_states: Dict[int, list] = {}
+        self.final_pressures: Dict[int, np.ndarray] = {}
+        ref = self._event(None)
         t0 = time.perf_counter()
         while pending or active:
             now = time.perf_counter() - t0
@@ -181,9 +232,11 @@ class ServingLoop:
                 if sim is None:
                     break
                 pending.popleft()
+                start = self._event(sim)
                 sim.init_fourier(req.seed)
-                sim.step_async(self.params)
-                active[req.rid] = {"req": req, "sim": sim, "done": 0, "admitted": now, "its": []}
+                self._launch(req, sim)
+                active[req.rid] = {"req": req, "sim": sim, "done": 0, "admitted": now, "its": [],
+                                   "start": start, "end": self._event(sim)}
             progressed = False
             for rid in list(active):
                 slot = active[rid]
@@ -200,14 +253,19 @@ class ServingLoop:
                 slot["done"] += 1
                 req = slot["req"]
                 if status == 0 and slot["done"] < req.steps:
-                    sim.step_async(self.params)
+                    self._launch(req, sim)
+                    slot["end"] = self._event(sim)
                     continue
                 finished = time.perf_counter() - t0
                 comp = Completion(req.rid, req.edge, slot["done"], req.arrival, slot["admitted"], finished, status,
-                                  slot["its"])
+                                  slot["its"], req.kind)
+                if ref is not None:
+                    comp.device_start_ms = ref.elapsed_time(slot["start"])
+                    comp.device_end_ms = ref.elapsed_time(slot["end"])
                 done.append(comp)
                 if keep_state:
                     self.final_states[req.rid] = sim.download()
+                    self.final_pressures[req.rid] = sim.pressure()
                 if on_complete:
                     on_complete(comp, sim)
                 self.pool.release(req.edge, sim)
@@ -237,6 +295,7 @@ def summarize(completions: Sequence[Completion], elapsed: float) -> dict:
             rejected[name] = rejected.get(name, 0) + 1
     cell_steps = sum(c.edge ** 3 * c.steps for c in ok)
     lat = percentiles([c.latency for c in ok])
+    kinds = sorted({c.kind for c in completions})
     return {
         "requests": len(completions),
         "accepted": len(ok),
@@ -245,4 +304,21 @@ def summarize(completions: Sequence[Completion], elapsed: float) -> dict:
         "requests_per_s": len(ok) / elapsed if elapsed > 0 else float("nan"),
         "cell_steps_per_s": cell_steps / elapsed if elapsed > 0 else float("nan"),
         "latency_s": lat,
+        "by_kind": {k: {"requests": sum(1 for c in ok if c.kind == k),
+                        "latency_s": percentiles([c.latency for c in ok if c.kind == k])} for k in kinds},
     }
+
+
+def overlapping_pairs(completions: Sequence[Completion]) -> int:
+    """Pairs of requests whose device intervals overlap (work of both on the
+    GPU at the same time)."""
+    iv = sorted((c.device_start_ms, c.device_end_ms) for c in completions
+                if c.device_start_ms == c.device_start_ms and c.device_end_ms == c.device_end_ms)
+    pairs = 0
+    for a in range(len(iv)):
+        for b in range(a + 1, len(iv)):
+            if iv[b][0] < iv[a][1]:
+                pairs += 1
+            else:
+                break
+    return pairs

@@ -44,6 +44,7 @@ def test_struct_layouts_match_the_header():
     assert C.sizeof(N.Trace) == 48
     assert C.sizeof(N.Request) == 72 + 8 + 8 + 8 + 8
     assert C.sizeof(N.StepParams) == 32
+    assert C.sizeof(N.BatchConfig) == 8 + 32 + 8 + 8 + 4 + 4
 
 
 def test_device_count_without_gpu_is_safe():

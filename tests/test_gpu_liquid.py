@@ -436,3 +436,85 @@ def test_periodic_seam_mismatch_and_random_parity():
         assert want[0] == "Ok", want[0]
         assert np.array_equal(st.fraction().view(np.uint64), want[1].view(np.uint64))
         same_report(got, want[2])
+
+
+# ------------------------------------------------------------------ cancellation stages
+def _stage_sequence(counts, periodic):
+    """The reference's VolumeStage sequence of one accepted interval
+    (prepare_with_boundary, src/liquid_volume.rs:558-830)."""
+    flux = (counts[2] + 0) * 2 + (counts[2] + 1)   # z planes of the X, Y and Z face arrays
+    seq = ["BeforeFlux"] + ["FaceFluxSlice"] * (flux * (2 if periodic else 1))
+    return seq + ["CellUpdateSlice"] * counts[2] + ["BeforeCommit"]
+
+
+@pytest.mark.parametrize("periodic", [False, True], ids=["inlet", "periodic"])
+def test_cancellation_stages_leave_the_state_untouched(periodic):
+    """VolumeStage (src/liquid_volume.rs:18-23) polled at :568, 578, 610, 689,
+    830: the callback sees the reference's sequence; a cancel at any point
+    ends the interval with Cancelled { stage } and the accepted fraction,
+    stamp and time unchanged; a retry equals a fresh run bit for bit."""
+    counts = (12, 10, 6)
+    rng = np.random.default_rng(7)
+    spacing = (0.5, 0.75, 1.25)
+    grid = R.GridGeometry(counts, spacing)
+    g = O.grid(counts, spacing)
+    f = rng.uniform(0.2, 0.8, int(np.prod(counts)))
+    vel = [rng.uniform(-0.05, 0.05, O.face_len(g, a)).astype(np.float32) for a in range(3)]
+    if periodic:  # equal velocities on the two faces of every seam
+        for a in range(3):
+            fc = list(counts)
+            fc[a] += 1
+            v = vel[a].reshape(fc[2], fc[1], fc[0])
+            if a == 0:
+                v[:, :, -1] = v[:, :, 0]
+            elif a == 1:
+                v[:, -1, :] = v[:, 0, :]
+            else:
+                v[-1, :, :] = v[0, :, :]
+    dv = [dev(v, np.float32) for v in vel]
+    inlet = L.LiquidInlet((4, 2), [[0.25, 0.5], [0.0, 1.0], [0.125, 0.75]])
+    settings = L.LiquidVolumeSettings(1.0, 10.0)
+
+    def run(state, cancel=None):
+        if periodic:
+            return state.advance_periodic(dv, 0.0, 0.05, (2, 0), (6, 1), settings, cancel=cancel)
+        return state.advance(dv, 0.0, 0.05, (2, 0), inlet, settings, cancel=cancel)
+
+    fresh = L.LiquidVolumeState(grid, 800.0, (5, 0), f)
+    seen = []
+    want = run(fresh, cancel=lambda s: seen.append(s) or False)
+    assert seen == _stage_sequence(counts, periodic)
+    want_f = fresh.fraction()
+    st = L.LiquidVolumeState(grid, 800.0, (5, 0), f)
+    for at in sorted({0, 1, len(seen) // 2, len(seen) - 2, len(seen) - 1}):
+        calls = []
+
+        def cancel(s, at=at):
+            calls.append(s)
+            return len(calls) - 1 == at
+
+        with pytest.raises(L.LiquidVolumeError) as e:
+            run(st, cancel=cancel)
+        assert e.value.kind == "Cancelled" and e.value.stage == seen[at]
+        assert calls == seen[: at + 1]
+        assert np.array_equal(st.fraction(), f) and st.stamp == (5, 0) and st.time == 0.0
+    got = run(st)
+    assert np.array_equal(st.fraction().view(np.uint64), want_f.view(np.uint64))
+    assert got.stamp == want.stamp == (5, 1)
+
+
+def test_an_error_before_a_cancellation_point_wins():
+    """A cell's Courant failure lies in its z plane's CellUpdateSlice: the
+    reference reports it without asking the later points."""
+    counts = (6, 4, 3)
+    vel = fields(counts)
+    vel[0][fidx(counts, 0, (1, 1, 1))] = 5.0   # outward Courant 5 in cell (0, 1, 1), z plane 1
+    grid = R.GridGeometry(counts)
+    st = L.LiquidVolumeState(grid, 1000.0, (1, 0), np.full(72, 0.5))
+    calls = []
+    with pytest.raises(L.LiquidVolumeError) as e:
+        st.advance([dev(v, np.float32) for v in vel], 0.0, 1.0, (2, 3), L.LiquidInlet((4, 2), [[0.5, 0.5]] * 3),
+                   L.LiquidVolumeSettings(1.0, 100.0), cancel=lambda s: calls.append(s) or False)
+    assert e.value.kind == "CourantLimit" and e.value.cell == 6 + 24
+    flux = 3 * 2 + 4
+    assert calls == ["BeforeFlux"] + ["FaceFluxSlice"] * flux + ["CellUpdateSlice"] * 2

@@ -1,8 +1,8 @@
 """The allocation-free pressure solve against the workspace solve.
 
 rb200_pressure_solve_static serves callers that cannot allocate device memory
-(for example code running inside a global-mode stream capture, or a host with
-its own fixed-budget device allocator). It keeps its scratch in one fixed
+(for example a plug-in inside a host application whose device memory belongs to
+its own fixed-budget allocator). It keeps its scratch in one fixed
 device array inside the library. This test calls it through the C ABI twice in
 a row, with different right-hand sides, and checks each result against the
 existing entry point (rb200_workspace_solve_rhs_device, Jacobi-PCG) within the
