@@ -82,6 +82,8 @@ def parse():
     ap.add_argument("--no-box-flux", action="store_true")
     ap.add_argument("--box-flux", action="store_true",
                     help="box-flux projection alone (device projection, passes, host-array call, CPU oracle)")
+    ap.add_argument("--oracle-steps", type=int, default=1,
+                    help="buoyant-blob mode: steps also computed by the FP64 CPU oracle (all host threads)")
     ap.add_argument("--buoyant-blob", action="store_true",
                     help="mixed-precision buoyant-blob run (rel 1e-10) in lockstep with the f64 carrier, "
                          "per-step divergence and velocity/tracer error; --n cells per axis, --steps steps")
@@ -456,7 +458,10 @@ def run_buoyant_blob(args, local):
     advect a passive density blob (sigma 20 cells, peak 1, centred at
     (n/2, n/4, n/2)) that drives buoyancy g_b = 1 on Y faces. Each step the
     mixed carrier takes the f64 carrier's dt (CFL 0.5). Per step: iterations,
-    both actual divergences, velocity and tracer relative L2 errors."""
+    both actual divergences, velocity and tracer relative L2 errors. The first
+    --oracle-steps steps are also computed by the FP64 CPU oracle on all host
+    threads from the same state with the same dt, and both device paths are
+    compared with it."""
     import torch
 
     import rheon_b200 as R
@@ -474,7 +479,11 @@ def run_buoyant_blob(args, local):
                                                        with_tracer=True, device=local))
     ref.upload(faces, blob)
     mix.upload([f.astype(np.float32) for f in faces], blob)
-    del faces
+    import oracle as O
+
+    og = O.grid(n)
+    o_faces, o_tracer = faces, blob
+    threads = os.cpu_count() or 1
     cuda = torch.device(f"cuda:{local}")
     rb = [torch.empty(g.face_len(d), dtype=torch.float64, device=cuda) for d in range(3)]
     mb = [torch.empty(g.face_len(d), dtype=torch.float32, device=cuda) for d in range(3)]
@@ -497,9 +506,25 @@ def run_buoyant_blob(args, local):
         num = sum(float((mb[d].double() - rb[d]).pow(2).sum()) for d in range(3))
         den = sum(float(rb[d].pow(2).sum()) for d in range(3))
         terr = float((mt.double() - rt.double()).norm() / rt.double().norm())
-        rows.append({"dt": rr.dt, "it_f64": rr.pressure.iterations, "it_mixed": rm.pressure.iterations,
-                     "div_f64": rr.actual_divergence_max, "div_mixed": rm.actual_divergence_max,
-                     "vel_rel_l2": math.sqrt(num / den), "tracer_rel_l2": terr})
+        row = {"dt": rr.dt, "it_f64": rr.pressure.iterations, "it_mixed": rm.pressure.iterations,
+               "div_f64": rr.actual_divergence_max, "div_mixed": rm.actual_divergence_max,
+               "vel_rel_l2": math.sqrt(num / den), "tracer_rel_l2": terr}
+        if len(rows) < args.oracle_steps:
+            t0 = time.perf_counter()
+            prm = O.StepParams(rr.dt, 1.0, O.JACOBI_PCG_V1, O.settings(rel, 0.0, MAXF, 1000000), 1.0, 0, threads)
+            st, o_faces, o_tracer, orep = O.carrier_step(og, o_faces, prm, tracer=o_tracer)
+            if st != O.OK:
+                raise RuntimeError(f"oracle step failed: {st}")
+            ot = torch.from_numpy(o_tracer.astype(np.float64))
+            den_o = sum(float(np.dot(o_faces[d], o_faces[d])) for d in range(3))
+            num_m = sum(float((mb[d].double().cpu() - torch.from_numpy(o_faces[d])).pow(2).sum()) for d in range(3))
+            num_r = sum(float((rb[d].cpu() - torch.from_numpy(o_faces[d])).pow(2).sum()) for d in range(3))
+            row["oracle"] = {"it": orep.pressure.iterations, "div": orep.actual_divergence_max,
+                             "seconds": time.perf_counter() - t0, "threads": threads,
+                             "mixed_vel_rel_l2": math.sqrt(num_m / den_o), "f64_vel_rel_l2": math.sqrt(num_r / den_o),
+                             "mixed_tracer_rel_l2": float((mt.double().cpu() - ot).norm() / ot.norm()),
+                             "f64_tracer_rel_l2": float((rt.double().cpu() - ot).norm() / ot.norm())}
+        rows.append(row)
     cells = g.cell_len()
     out = {
         "mode": "buoyant-blob", "n": args.n, "steps": args.steps, "relative_residual": rel,

@@ -461,6 +461,15 @@ RB200_API int rb200_batch_step(rb200_batch* batch, const rb200_step_params* para
 RB200_API int rb200_batch_step_async(rb200_batch* batch, const rb200_step_params* params);
 RB200_API int rb200_batch_step_poll(const rb200_batch* batch);
 RB200_API int rb200_batch_step_wait(rb200_batch* batch, rb200_step_report* reports, int* statuses);
+/* A profiling aid: one step of every instance like rb200_batch_step (the state
+ * advances), issued eagerly with an event after every launch instead of as the
+ * step graph, the solve loop decided on the host after each trip. Per kernel
+ * kind (kinds >= rb200_batch_profile_kinds() entries): the summed device time
+ * in ms, the launches and a static name. */
+RB200_API int rb200_batch_profile_step(rb200_batch* batch, const rb200_step_params* params,
+                                       rb200_step_report* reports, int* statuses, double* kernel_ms,
+                                       int* kernel_launches, const char** kernel_names, int kinds);
+RB200_API int rb200_batch_profile_kinds(void);
 
 /* rb200_workspace_profile on the carrier's pressure solver. */
 RB200_API int rb200_carrier_profile(rb200_carrier* carrier, int which, int launches, double* avg_ms);

@@ -850,6 +850,24 @@ class BatchedCarriers:
     def step_done(self) -> bool:
         return bool(lib().rb200_batch_step_poll(self._handle))
 
+    def profile_step(self, params) -> dict:
+        """A profiling aid: one step issued eagerly with an event after every
+        launch (the state advances as in step()); returns {"statuses",
+        "reports", "kernels": {name: (ms, launches)}}."""
+        n = len(self.grids)
+        kinds = int(lib().rb200_batch_profile_kinds())
+        reps = (N.StepReport * n)()
+        sts = (C.c_int * n)()
+        ms = (C.c_double * kinds)()
+        cnt = (C.c_int * kinds)()
+        names = (C.c_char_p * kinds)()
+        st = lib().rb200_batch_profile_step(self._handle, self._params(params), reps, sts, ms, cnt, names, kinds)
+        if st != N.OK:
+            raise SimulationError(st, detail=(lib().rb200_batch_last_error(self._handle) or b"").decode())
+        return {"statuses": [int(x) for x in sts],
+                "reports": [CarrierSimulation._report(reps[i]) for i in range(n)],
+                "kernels": {names[k].decode(): (ms[k], int(cnt[k])) for k in range(kinds) if cnt[k]}}
+
     def step_wait(self) -> list:
         n = len(self.grids)
         reps = (N.StepReport * n)()

@@ -316,6 +316,9 @@ SIGNATURES = {
     "rb200_batch_step_async": (_I, [_P, C.POINTER(StepParams)]),
     "rb200_batch_step_poll": (_I, [_P]),
     "rb200_batch_step_wait": (_I, [_P, C.POINTER(StepReport), C.POINTER(_I)]),
+    "rb200_batch_profile_step": (_I, [_P, C.POINTER(StepParams), C.POINTER(StepReport), C.POINTER(_I),
+                                      C.POINTER(_D), C.POINTER(_I), C.POINTER(C.c_char_p), _I]),
+    "rb200_batch_profile_kinds": (_I, []),
     "rb200_carrier_profile": (_I, [_P, _I, _I, C.POINTER(_D)]),
     "rb200_carrier_pressure": (_I, [_P, _P, _S]),
     "rb200_carrier_dense3d_fields": (_I, [_P, C.POINTER(Dense3dFields)]),

@@ -325,10 +325,23 @@ __global__ void __launch_bounds__(BT) k_b_true_residual(const BatchInstDev* __re
     }
 }
 
-// Condition of the solve's WHILE node: repeat while any instance's solve runs.
-// The trip count is bounded: an instance still running at the bound ends with
-// an execution error instead of looping on.
-__global__ void k_b_loop_cond(BatchInstDev* inst, int count, cudaGraphConditionalHandle handle, int max_trips) {
+// Whether some instance's true residual asked for a restart (the restart
+// branch of a trip runs only then).
+__device__ __forceinline__ int any_replace(const BatchInstDev* inst, int count) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < count; i += blockDim.x)
+        if (inst[i].st->flags & F_NEED_REPLACE) atomicOr(&any, 1);
+    __syncthreads();
+    return any;
+}
+
+// The end of a trip of the solve loop: counts the trip for every instance and
+// tells whether any instance's solve still runs. The trip count is bounded:
+// an instance still running at the bound ends with an execution error instead
+// of looping on.
+__device__ __forceinline__ int end_trip(BatchInstDev* inst, int count, int max_trips) {
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
@@ -345,7 +358,26 @@ __global__ void k_b_loop_cond(BatchInstDev* inst, int count, cudaGraphConditiona
         atomicOr(&any, 1);
     }
     __syncthreads();
+    return any;
+}
+
+// Graph conditions: the restart branch's IF node and the solve's WHILE node.
+__global__ void k_b_any_replace(const BatchInstDev* inst, int count, cudaGraphConditionalHandle handle) {
+    const int any = any_replace(inst, count);
     if (threadIdx.x == 0) cudaGraphSetConditional(handle, any ? 1u : 0u);
+}
+__global__ void k_b_loop_cond(BatchInstDev* inst, int count, cudaGraphConditionalHandle handle, int max_trips) {
+    const int any = end_trip(inst, count, max_trips);
+    if (threadIdx.x == 0) cudaGraphSetConditional(handle, any ? 1u : 0u);
+}
+// The same decisions for the eager (profiled) step, read by the host.
+__global__ void k_b_any_replace_out(const BatchInstDev* inst, int count, int* out) {
+    const int any = any_replace(inst, count);
+    if (threadIdx.x == 0) *out = any;
+}
+__global__ void k_b_end_trip_out(BatchInstDev* inst, int count, int max_trips, int* out) {
+    const int any = end_trip(inst, count, max_trips);
+    if (threadIdx.x == 0) *out = any;
 }
 
 __global__ void __launch_bounds__(BT) k_b_correct(const BatchInstDev* __restrict__ inst, const __grid_constant__ BatchSpans spans) {
@@ -458,6 +490,17 @@ cudaError_t launch(bool pdl, void (*kernel)(KArgs...), int blocks, int threads, 
 
 enum OpKind : int { OP_SMOOTH = 0, OP_PAIR = 1, OP_RESTRICT = 2, OP_PROLONG = 3, OP_DENSE = 4 };
 
+// Kernel kinds of a batched step, for the profiled step's per-kind times.
+enum KernelKind : int {
+    KK_SMOOTH = 0, KK_PAIR, KK_RESTRICT, KK_PROLONG, KK_DENSE,  // the V-cycle operations (OpKind order)
+    KK_BEGIN, KK_ADVECT, KK_RHS, KK_RESET, KK_SUMS, KK_LOAD, KK_PASS1, KK_UPDATE, KK_FINISH, KK_TRUE,
+    KK_CORRECT, KK_END, KK_CONTROL, KK_COUNT
+};
+const char* const kKernelNames[KK_COUNT] = {
+    "k_b_smooth", "k_b_pair", "k_b_restrict", "k_b_prolong", "k_b_dense", "k_b_begin", "k_b_advect", "k_b_rhs",
+    "k_b_reset", "k_b_init_sums", "k_b_load_residual", "k_b_pass1", "k_b_update_first", "k_b_finish",
+    "k_b_true_residual", "k_b_correct", "k_b_end", "loop control"};
+
 // One launch of the V-cycle program: an operation over the instances that
 // take part at that point of the cycle.
 struct VLaunch {
@@ -478,6 +521,7 @@ struct rb200_batch {
     int count = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t body_stream = nullptr;
+    cudaStream_t replace_stream = nullptr;
     std::vector<GridDev> grids;
     char* arena = nullptr;
     size_t bytes = 0;
@@ -513,6 +557,7 @@ struct rb200_batch {
         if (step_h) cudaFreeHost(step_h);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        if (replace_stream) cudaStreamDestroy(replace_stream);
         if (body_stream) cudaStreamDestroy(body_stream);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -523,25 +568,6 @@ struct rb200_batch {
         return rc;
     }
 
-    // Enqueue the V-cycle program `prog` gated by `mode`; returns launches.
-    int enqueue_vcycle(const std::vector<VLaunch>& prog, int mode, cudaStream_t s, cudaError_t* e) const {
-        int n = 0;
-        for (const VLaunch& v : prog) {
-            const BatchLevelOp* o = ops_d + v.first_op;
-            const int nb = total_blocks(v.spans);
-            cudaError_t r = cudaSuccess;
-            switch (v.kind) {
-                case OP_SMOOTH: r = launch(true, k_b_smooth, nb, MG_THREADS, 0, s, o, v.spans, mode); break;
-                case OP_PAIR: r = launch(true, k_b_pair, nb, MG_THREADS, v.smem, s, o, v.spans, mode); break;
-                case OP_RESTRICT: r = launch(true, k_b_restrict, nb, MG_THREADS, 0, s, o, v.spans, mode); break;
-                case OP_PROLONG: r = launch(true, k_b_prolong, nb, MG_THREADS, 0, s, o, v.spans, mode); break;
-                default: r = launch(true, k_b_dense, nb, MG_THREADS, 0, s, o, v.spans, mode); break;
-            }
-            if (r != cudaSuccess && *e == cudaSuccess) *e = r;
-            ++n;
-        }
-        return n;
-    }
 };
 
 namespace {
@@ -666,82 +692,169 @@ int build_program(rb200_batch* B) {
     return RB200_OK;
 }
 
+// Issues the batched step's kernels on one stream: in a graph capture (no
+// marks) or eagerly with an event after every launch (marks: the profiled
+// step). Launch errors are kept in *e; launches are counted.
+struct Emit {
+    rb200_batch* B;
+    cudaStream_t s;
+    cudaError_t* e;
+    std::vector<std::pair<int, cudaEvent_t>>* marks;
+    int launches = 0;
+
+    void keep(cudaError_t r) {
+        if (r != cudaSuccess && *e == cudaSuccess) *e = r;
+    }
+    void mark(int kind) {
+        if (!marks) return;
+        cudaEvent_t ev = nullptr;
+        keep(cudaEventCreate(&ev));
+        keep(cudaEventRecord(ev, s));
+        marks->push_back({kind, ev});
+    }
+    template <typename... KArgs, typename... Args>
+    void go(int kind, bool pdl, void (*kernel)(KArgs...), int blocks, int threads, size_t smem, Args&&... args) {
+        keep(launch(pdl && !marks, kernel, blocks, threads, smem, s, std::forward<Args>(args)...));
+        ++launches;
+        mark(kind);
+    }
+    void vcycle(const std::vector<VLaunch>& prog, int mode) {
+        for (const VLaunch& v : prog) {
+            const BatchLevelOp* o = B->ops_d + v.first_op;
+            const int nb = total_blocks(v.spans);
+            switch (v.kind) {
+                case OP_SMOOTH: go(KK_SMOOTH, true, k_b_smooth, nb, MG_THREADS, 0, o, v.spans, mode); break;
+                case OP_PAIR: go(KK_PAIR, true, k_b_pair, nb, MG_THREADS, v.smem, o, v.spans, mode); break;
+                case OP_RESTRICT: go(KK_RESTRICT, true, k_b_restrict, nb, MG_THREADS, 0, o, v.spans, mode); break;
+                case OP_PROLONG: go(KK_PROLONG, true, k_b_prolong, nb, MG_THREADS, 0, o, v.spans, mode); break;
+                default: go(KK_DENSE, true, k_b_dense, nb, MG_THREADS, 0, o, v.spans, mode); break;
+            }
+        }
+    }
+    // dt policy, advection, RHS (then the solve's timing event in a graph)
+    void head() {
+        const int ib = ceil_div(B->count, 128);
+        go(KK_BEGIN, false, k_b_begin, ib, 128, 0, B->inst_d, B->count);
+        if (B->cfg.fp32_advection)
+            go(KK_ADVECT, false, k_b_advect<float>, total_blocks(B->sp_faces), BT, 0, B->inst_d, B->sp_faces);
+        else
+            go(KK_ADVECT, false, k_b_advect<double>, total_blocks(B->sp_faces), BT, 0, B->inst_d, B->sp_faces);
+        go(KK_RHS, false, k_b_rhs, total_blocks(B->sp_cells), BT, 0, B->inst_d, B->sp_cells);
+    }
+    // the solve's start: state, compatibility sums, residual, first V-cycle
+    void start() {
+        const int ib = ceil_div(B->count, 128);
+        go(KK_RESET, false, k_b_reset, ib, 128, 0, B->inst_d, B->count, B->cfg.settings);
+        go(KK_SUMS, false, k_b_init_sums, total_blocks(B->sp_cells), BT, 0, B->inst_d, B->sp_cells);
+        go(KK_LOAD, true, k_b_load_residual, total_blocks(B->sp_cells), BT, 0, B->inst_d, B->sp_cells,
+           int(MODE_INIT));
+        vcycle(B->vfirst, MODE_INIT);
+        go(KK_FINISH, true, k_b_finish, total_blocks(B->sp_rows), MG_THREADS, 0, B->inst_d, B->sp_rows,
+           int(MODE_INIT));
+    }
+    void iteration() {
+        go(KK_PASS1, true, k_b_pass1, total_blocks(B->sp_pass1), MG_THREADS, 0, B->inst_d, B->sp_pass1, kPass1Kc);
+        go(KK_UPDATE, true, k_b_update_first, total_blocks(B->sp_rows), MG_THREADS, 0, B->inst_d, B->sp_rows);
+        vcycle(B->vrest, MODE_ITER);
+        go(KK_FINISH, true, k_b_finish, total_blocks(B->sp_rows), MG_THREADS, 0, B->inst_d, B->sp_rows,
+           int(MODE_ITER));
+    }
+    void check() {
+        go(KK_TRUE, true, k_b_true_residual, total_blocks(B->sp_cells), BT, 0, B->inst_d, B->sp_cells);
+    }
+    void restart() {
+        go(KK_LOAD, false, k_b_load_residual, total_blocks(B->sp_cells), BT, 0, B->inst_d, B->sp_cells,
+           int(MODE_REPLACE));
+        vcycle(B->vfirst, MODE_REPLACE);
+        go(KK_FINISH, true, k_b_finish, total_blocks(B->sp_rows), MG_THREADS, 0, B->inst_d, B->sp_rows,
+           int(MODE_REPLACE));
+    }
+    // correction, gates and commit
+    void tail() {
+        go(KK_CORRECT, false, k_b_correct, total_blocks(B->sp_cells), BT, 0, B->inst_d, B->sp_cells);
+        go(KK_END, false, k_b_end, ceil_div(B->count, 128), 128, 0, B->inst_d, B->count);
+    }
+};
+
+int max_trips(const rb200_settings& set) {
+    const uint64_t trips = (set.max_iterations / uint64_t(kChunk)) * 2 + 64;
+    return trips > (1u << 24) ? (1 << 24) : int(trips);
+}
+
 int capture(rb200_batch* B) {
     cudaStream_t s = B->stream;
     const int n = B->count;
-    const int ib = ceil_div(n, 128);
-    const rb200_settings& set = B->cfg.settings;
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaSuccess;
-    auto keep = [&](cudaError_t r) {
-        if (r != cudaSuccess && e == cudaSuccess) e = r;
-    };
+    Emit E{B, s, &e, nullptr};
     RB200_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
-    int fixed = 0;
-    k_b_begin<<<ib, 128, 0, s>>>(B->inst_d, n);
-    if (B->cfg.fp32_advection)
-        keep(launch(false, k_b_advect<float>, total_blocks(B->sp_faces), BT, 0, s, B->inst_d, B->sp_faces));
-    else
-        keep(launch(false, k_b_advect<double>, total_blocks(B->sp_faces), BT, 0, s, B->inst_d, B->sp_faces));
-    keep(launch(false, k_b_rhs, total_blocks(B->sp_cells), BT, 0, s, B->inst_d, B->sp_cells));
-    keep(cudaEventRecordWithFlags(B->ev[0], s, cudaEventRecordExternal));
-    k_b_reset<<<ib, 128, 0, s>>>(B->inst_d, n, set);
-    keep(launch(false, k_b_init_sums, total_blocks(B->sp_cells), BT, 0, s, B->inst_d, B->sp_cells));
-    keep(launch(true, k_b_load_residual, total_blocks(B->sp_cells), BT, 0, s, B->inst_d, B->sp_cells, int(MODE_INIT)));
-    fixed += 6;  // begin, advect, rhs, reset, sums, residual
-    fixed += B->enqueue_vcycle(B->vfirst, MODE_INIT, s, &e);
-    keep(launch(true, k_b_finish, total_blocks(B->sp_rows), MG_THREADS, 0, s, B->inst_d, B->sp_rows, int(MODE_INIT)));
-    fixed += 1;
-    // the solve loop: chunks of iterations, the gated check, the condition
+    E.head();
+    E.keep(cudaEventRecordWithFlags(B->ev[0], s, cudaEventRecordExternal));
+    E.start();
+    const int fixed_head = E.launches;
+    // the solve loop: chunks of iterations, the true-residual check, the
+    // restart branch, the condition
     cudaStreamCaptureStatus status;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
     cudaGraph_t outer = nullptr;
-    keep(cudaStreamGetCaptureInfo(s, &status, nullptr, &outer, &deps, &ndeps));
+    E.keep(cudaStreamGetCaptureInfo(s, &status, nullptr, &outer, &deps, &ndeps));
     cudaGraphConditionalHandle handle{};
-    keep(cudaGraphConditionalHandleCreate(&handle, outer, 1, cudaGraphCondAssignDefault));
+    E.keep(cudaGraphConditionalHandleCreate(&handle, outer, 1, cudaGraphCondAssignDefault));
     cudaGraphNodeParams cp{};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = handle;
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
     cudaGraphNode_t node{};
-    keep(cudaGraphAddNode(&node, outer, deps, ndeps, &cp));
+    E.keep(cudaGraphAddNode(&node, outer, deps, ndeps, &cp));
     int per_trip = 0;
     if (e == cudaSuccess) {
         cudaStream_t bs = B->body_stream;
-        keep(cudaStreamBeginCaptureToGraph(bs, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                           cudaStreamCaptureModeRelaxed));
-        for (int q = 0; q < kChunk; ++q) {
-            keep(launch(true, k_b_pass1, total_blocks(B->sp_pass1), MG_THREADS, 0, bs, B->inst_d, B->sp_pass1,
-                        kPass1Kc));
-            keep(launch(true, k_b_update_first, total_blocks(B->sp_rows), MG_THREADS, 0, bs, B->inst_d, B->sp_rows));
-            per_trip += 2 + B->enqueue_vcycle(B->vrest, MODE_ITER, bs, &e);
-            keep(launch(true, k_b_finish, total_blocks(B->sp_rows), MG_THREADS, 0, bs, B->inst_d, B->sp_rows,
-                        int(MODE_ITER)));
-            per_trip += 1;
+        E.keep(cudaStreamBeginCaptureToGraph(bs, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeRelaxed));
+        Emit body{B, bs, &e, nullptr};
+        for (int q = 0; q < kChunk; ++q) body.iteration();
+        body.check();
+        // the restart as an IF node: its launches run only in trips where some
+        // instance restarts
+        cudaStreamCaptureStatus bst;
+        const cudaGraphNode_t* bdeps = nullptr;
+        size_t nbdeps = 0;
+        cudaGraph_t bodyg = nullptr;
+        body.keep(cudaStreamGetCaptureInfo(bs, &bst, nullptr, &bodyg, &bdeps, &nbdeps));
+        cudaGraphConditionalHandle rh{};
+        body.keep(cudaGraphConditionalHandleCreate(&rh, bodyg, 0, cudaGraphCondAssignDefault));
+        body.go(KK_CONTROL, false, k_b_any_replace, 1, 128, 0, B->inst_d, n, rh);
+        body.keep(cudaStreamGetCaptureInfo(bs, &bst, nullptr, &bodyg, &bdeps, &nbdeps));
+        cudaGraphNodeParams ip{};
+        ip.type = cudaGraphNodeTypeConditional;
+        ip.conditional.handle = rh;
+        ip.conditional.type = cudaGraphCondTypeIf;
+        ip.conditional.size = 1;
+        cudaGraphNode_t inode{};
+        body.keep(cudaGraphAddNode(&inode, bodyg, bdeps, nbdeps, &ip));
+        if (e == cudaSuccess) {
+            cudaStream_t rs = B->replace_stream;
+            body.keep(cudaStreamBeginCaptureToGraph(rs, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                    cudaStreamCaptureModeRelaxed));
+            Emit branch{B, rs, &e, nullptr};
+            branch.restart();
+            cudaGraph_t rbody = nullptr;
+            body.keep(cudaStreamEndCapture(rs, &rbody));
+            body.keep(cudaStreamUpdateCaptureDependencies(bs, &inode, 1, cudaStreamSetCaptureDependencies));
         }
-        keep(launch(true, k_b_true_residual, total_blocks(B->sp_cells), BT, 0, bs, B->inst_d, B->sp_cells));
-        keep(launch(true, k_b_load_residual, total_blocks(B->sp_cells), BT, 0, bs, B->inst_d, B->sp_cells,
-                    int(MODE_REPLACE)));
-        per_trip += 2 + B->enqueue_vcycle(B->vfirst, MODE_REPLACE, bs, &e);
-        keep(launch(true, k_b_finish, total_blocks(B->sp_rows), MG_THREADS, 0, bs, B->inst_d, B->sp_rows,
-                    int(MODE_REPLACE)));
-        const uint64_t mi = set.max_iterations;
-        const uint64_t trips = (mi / uint64_t(kChunk)) * 2 + 64;
-        k_b_loop_cond<<<1, 128, 0, bs>>>(B->inst_d, n, handle, trips > (1u << 24) ? (1 << 24) : int(trips));
-        per_trip += 2;
-        keep(cudaGetLastError());
-        cudaGraph_t body = nullptr;
-        keep(cudaStreamEndCapture(bs, &body));
-        keep(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+        body.go(KK_CONTROL, false, k_b_loop_cond, 1, 128, 0, B->inst_d, n, handle, max_trips(B->cfg.settings));
+        per_trip = body.launches;  // the restart branch's launches run rarely and are not counted
+        cudaGraph_t captured = nullptr;
+        E.keep(cudaStreamEndCapture(bs, &captured));
+        E.keep(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
     }
-    keep(cudaEventRecordWithFlags(B->ev[1], s, cudaEventRecordExternal));
-    keep(launch(false, k_b_correct, total_blocks(B->sp_cells), BT, 0, s, B->inst_d, B->sp_cells));
-    k_b_end<<<ib, 128, 0, s>>>(B->inst_d, n);
-    fixed += 2;
-    keep(cudaMemcpyAsync(B->step_h, B->step_d, sizeof(BatchStepDev) * size_t(n), cudaMemcpyDeviceToHost, s));
-    keep(cudaGetLastError());
+    E.keep(cudaEventRecordWithFlags(B->ev[1], s, cudaEventRecordExternal));
+    const int before_tail = E.launches;
+    E.tail();
+    E.keep(cudaMemcpyAsync(B->step_h, B->step_d, sizeof(BatchStepDev) * size_t(n), cudaMemcpyDeviceToHost, s));
+    E.keep(cudaGetLastError());
     cudaError_t ee = cudaStreamEndCapture(s, &graph);
     if (e != cudaSuccess || ee != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -751,8 +864,59 @@ int capture(rb200_batch* B) {
     cudaError_t ie = cudaGraphInstantiate(&B->exec, graph, 0);
     cudaGraphDestroy(graph);
     if (ie != cudaSuccess) return B->fail(RB200_EXECUTION, std::string("batch graph instantiate: ") + cudaGetErrorString(ie));
-    B->fixed_nodes = fixed;
+    B->fixed_nodes = fixed_head + (E.launches - before_tail);
     B->nodes_per_trip = per_trip;
+    return RB200_OK;
+}
+
+// One batched step issued eagerly (the same kernels in the same order as the
+// step graph, the loop decided on the host after each trip) with an event
+// after every launch; per kernel kind the summed device time and the launches.
+int profiled_step(rb200_batch* B, double* kind_ms, int* kind_launches) {
+    cudaStream_t s = B->stream;
+    cudaError_t e = cudaSuccess;
+    std::vector<std::pair<int, cudaEvent_t>> marks;
+    Emit E{B, s, &e, &marks};
+    int* flag_d = nullptr;
+    int flag_h = 0;
+    RB200_CUDA(cudaMalloc(&flag_d, sizeof(int)));
+    cudaEvent_t start = nullptr;
+    E.keep(cudaEventCreate(&start));
+    E.keep(cudaEventRecord(start, s));
+    E.head();
+    E.start();
+    const int bound = max_trips(B->cfg.settings);
+    for (int trip = 0; e == cudaSuccess && trip < bound; ++trip) {
+        for (int q = 0; q < kChunk; ++q) E.iteration();
+        E.check();
+        E.go(KK_CONTROL, false, k_b_any_replace_out, 1, 128, 0, B->inst_d, B->count, flag_d);
+        E.keep(cudaMemcpyAsync(&flag_h, flag_d, sizeof(int), cudaMemcpyDeviceToHost, s));
+        E.keep(cudaStreamSynchronize(s));
+        if (flag_h) E.restart();
+        E.go(KK_CONTROL, false, k_b_end_trip_out, 1, 128, 0, B->inst_d, B->count, bound, flag_d);
+        E.keep(cudaMemcpyAsync(&flag_h, flag_d, sizeof(int), cudaMemcpyDeviceToHost, s));
+        E.keep(cudaStreamSynchronize(s));
+        if (!flag_h) break;
+    }
+    E.tail();
+    E.keep(cudaMemcpyAsync(B->step_h, B->step_d, sizeof(BatchStepDev) * size_t(B->count), cudaMemcpyDeviceToHost, s));
+    E.keep(cudaStreamSynchronize(s));
+    for (int k = 0; k < KK_COUNT; ++k) {
+        kind_ms[k] = 0.0;
+        kind_launches[k] = 0;
+    }
+    cudaEvent_t prev = start;
+    for (auto& m : marks) {
+        float ms = 0.0f;
+        if (e == cudaSuccess) E.keep(cudaEventElapsedTime(&ms, prev, m.second));
+        kind_ms[m.first] += double(ms);
+        kind_launches[m.first] += 1;
+        prev = m.second;
+    }
+    for (auto& m : marks) cudaEventDestroy(m.second);
+    cudaEventDestroy(start);
+    cudaFree(flag_d);
+    if (e != cudaSuccess) return B->fail(RB200_EXECUTION, std::string("profiled batch step: ") + cudaGetErrorString(e));
     return RB200_OK;
 }
 
@@ -862,6 +1026,7 @@ int rb200_batch_create(const rb200_grid* grids, size_t count, const rb200_batch_
     }
     RB200_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
     RB200_CUDA(cudaStreamCreateWithFlags(&B->body_stream, cudaStreamNonBlocking));
+    RB200_CUDA(cudaStreamCreateWithFlags(&B->replace_stream, cudaStreamNonBlocking));
     if (cudaMalloc(&B->arena, total) != cudaSuccess) {
         cudaGetLastError();
         return B->fail(RB200_OUT_OF_MEMORY, "batch arena of " + std::to_string(total) + " bytes");
@@ -1027,6 +1192,37 @@ int rb200_batch_step_wait(rb200_batch* batch, rb200_step_report* reports, int* s
     }
     return RB200_OK;
 }
+
+int rb200_batch_profile_step(rb200_batch* batch, const rb200_step_params* params, rb200_step_report* reports,
+                             int* statuses, double* kernel_ms, int* kernel_launches, const char** kernel_names,
+                             int kinds) {
+    if (!batch || !params || !reports || !statuses || !kernel_ms || !kernel_launches) return RB200_INVALID_ARGUMENT;
+    if (kinds < KK_COUNT) return RB200_LENGTH_MISMATCH;
+    rb200_batch* B = batch;
+    if (B->in_flight) return RB200_INVALID_ARGUMENT;
+    cudaSetDevice(B->device);
+    for (int i = 0; i < B->count; ++i) {
+        BatchStepDev& h = B->step_h[i];
+        h.requested_dt = params[i].requested_dt;
+        h.cfl = params[i].cfl;
+        h.iteration_limit_ok = params[i].iteration_limit_ok;
+        h.skip_gates = params[i].skip_gates;
+        if (params[i].buoyancy != 0.0) return RB200_INVALID_ARGUMENT;
+    }
+    RB200_CUDA(cudaMemcpyAsync(B->step_d, B->step_h, sizeof(BatchStepDev) * size_t(B->count), cudaMemcpyHostToDevice,
+                               B->stream));
+    int rc = profiled_step(B, kernel_ms, kernel_launches);
+    if (rc) return rc;
+    for (int k = 0; k < KK_COUNT; ++k)
+        if (kernel_names) kernel_names[k] = kKernelNames[k];
+    for (int i = 0; i < B->count; ++i) {
+        reports[i] = B->step_h[i].report;
+        statuses[i] = B->step_h[i].step_status;
+    }
+    return RB200_OK;
+}
+
+int rb200_batch_profile_kinds(void) { return KK_COUNT; }
 
 int rb200_batch_step(rb200_batch* batch, const rb200_step_params* params, rb200_step_report* reports, int* statuses) {
     int rc = rb200_batch_step_async(batch, params);

@@ -633,6 +633,12 @@ __global__ void k_solve_reset(SolveState* st, rb200_settings s, const double* __
     *st = init;
 }
 
+// Condition of the restart branch of a loop trip (an IF node): the true
+// residual asked for a restart.
+__global__ void k_replace_cond(const SolveState* st, cudaGraphConditionalHandle handle) {
+    cudaGraphSetConditional(handle, (st->flags & F_NEED_REPLACE) ? 1u : 0u);
+}
+
 // Condition of the WHILE node: repeat while the solve is running. The trip
 // count is bounded; running out of trips ends the solve with an execution
 // error instead of looping on.
@@ -1206,6 +1212,50 @@ int PcgSolver::enqueue_loop(cudaStream_t cs, cudaStream_t body_stream, const rb2
     if (persist_blocks_) {
         RB200_CUDA(launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, d_trace_, maps_,
                                      persist_blocks_, chunk_, body_stream, persist_pre_));
+    } else if (mg) {
+        // The multigrid restart (a whole V-cycle) as an IF node after the
+        // true-residual check: its launches run only in trips that restart.
+        int nodes = 0;
+        for (int q = 0; q < chunk_; ++q) nodes += launch_iteration(g_, method_, B, mg, body_stream);
+        const dim3 grid = slab_grid(g_), block(TX, TY, 1);
+        k_true_residual<ZC><<<grid, block, kSmemSlab, body_stream>>>(g_, B.st, B.b, B.p, B.d0, B.d1, B.maps, B.part,
+                                                                      B.trace);
+        cudaStreamCaptureStatus bst;
+        const cudaGraphNode_t* bdeps = nullptr;
+        size_t nbdeps = 0;
+        cudaGraph_t bodyg = nullptr;
+        RB200_CUDA(cudaStreamGetCaptureInfo(body_stream, &bst, nullptr, &bodyg, &bdeps, &nbdeps));
+        cudaGraphConditionalHandle rh;
+        RB200_CUDA(cudaGraphConditionalHandleCreate(&rh, bodyg, 0, cudaGraphCondAssignDefault));
+        k_replace_cond<<<1, 1, 0, body_stream>>>(st_, rh);
+        RB200_CUDA(cudaStreamGetCaptureInfo(body_stream, &bst, nullptr, &bodyg, &bdeps, &nbdeps));
+        cudaGraphNodeParams ip{};
+        ip.type = cudaGraphNodeTypeConditional;
+        ip.conditional.handle = rh;
+        ip.conditional.type = cudaGraphCondTypeIf;
+        ip.conditional.size = 1;
+        cudaGraphNode_t inode;
+        RB200_CUDA(cudaGraphAddNode(&inode, bodyg, bdeps, nbdeps, &ip));
+        cudaStream_t rs = nullptr;
+        RB200_CUDA(cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking));
+        cudaError_t ce = cudaStreamBeginCaptureToGraph(rs, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeRelaxed);
+        if (ce == cudaSuccess) {
+            const int eb = ew_blocks(g_.cells);
+            k_load_residual<KIND_MG><<<eb, EW, 0, rs>>>(g_, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part,
+                                                        B.trace);
+            mg->enqueue(B.r, B.st, MODE_REPLACE, rs);
+            mg->enqueue_finish(B.st, B.r, B.q, MODE_REPLACE, B.part, B.trace, rs);
+            cudaGraph_t rbody = nullptr;
+            ce = cudaStreamEndCapture(rs, &rbody);
+        }
+        cudaStreamDestroy(rs);
+        if (ce != cudaSuccess) {
+            set_error(std::string("restart branch capture: ") + cudaGetErrorString(ce));
+            return RB200_EXECUTION;
+        }
+        RB200_CUDA(cudaStreamUpdateCaptureDependencies(body_stream, &inode, 1, cudaStreamSetCaptureDependencies));
+        nodes_per_chunk_ = nodes + 2;  // the check and the branch condition (the restart runs rarely)
     } else {
         for (int q = 0; q < chunk_; ++q) launch_iteration(g_, method_, B, mg, body_stream);
         launch_check(g_, method_, B, mg, body_stream);

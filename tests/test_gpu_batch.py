@@ -75,7 +75,7 @@ def test_batch_tracks_the_fp64_oracle():
     faces64 = inits(sizes, np.float64)
     batch = R.BatchedCarriers([R.GridGeometry(n) for n in sizes], cfg())
     for i, f in enumerate(faces64):
-        batch.upload(i, f.astype(np.float32))
+        batch.upload(i, [x.astype(np.float32) for x in f])
     s = O.settings(1e-8, 0.0, MAXF, 100000)
     refs = list(faces64)
     for step in range(2):
@@ -153,3 +153,28 @@ def test_batch_rejects_levels_without_fused_pairs():
     with pytest.raises(R.SimulationError) as e:
         R.BatchedCarriers([R.GridGeometry((32, 32, 32)), R.GridGeometry((40, 40, 40))], cfg())
     assert e.value.kind == "Unsupported"
+
+
+def test_profiled_step_equals_the_graph_step():
+    """The eager, event-timed step issues the graph's kernels in the same order:
+    the same bits, and every kernel kind of the step is timed."""
+    sizes = [(32, 32, 32), (64, 48, 32)]
+    faces = inits(sizes)
+    a = R.BatchedCarriers([R.GridGeometry(n) for n in sizes], cfg())
+    b = R.BatchedCarriers([R.GridGeometry(n) for n in sizes], cfg())
+    for i, f in enumerate(faces):
+        a.upload(i, f)
+        b.upload(i, f)
+    prm = R.StepParams(MAXF, cfl=0.5)
+    for _ in range(2):
+        out = a.step(prm)
+        prof = b.profile_step(prm)
+        assert prof["statuses"] == [st for st, _ in out] == [0, 0]
+        assert [r.pressure.iterations for r in prof["reports"]] == [r.pressure.iterations for _, r in out]
+        for name in ("k_b_advect", "k_b_pass1", "k_b_pair", "k_b_dense", "k_b_finish", "k_b_correct"):
+            ms, launches = prof["kernels"][name]
+            assert launches > 0 and ms > 0.0, name
+    for i in range(len(sizes)):
+        x, y = a.download(i), b.download(i)
+        for d in range(3):
+            assert np.array_equal(x[d], y[d])
