@@ -33,17 +33,33 @@ __device__ __forceinline__ float div_h<float>(float r, const GridDev& g, int d) 
     return div_f32(r, float(g.h[d]), g.rhf[d]);
 }
 
-// ScalarSampler::sample (src/sampling.rs:74-122) in arithmetic type R: double
-// reproduces the reference; float is the mixed-precision path.
+// The scaled coordinate (x - o_d) / h_d of a position after the box clamp of
+// ScalarSampler::sample (src/sampling.rs:74-122). It depends on the position
+// only, so the three components of a velocity sample share it.
+template <class R>
+__device__ __forceinline__ void scaled_position(const GridDev& g, const R pos[3], R xh[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const R x = clampd<R>(pos[d], R(g.o[d]), R(g.up[d]));
+        xh[d] = div_h<R>(x - R(g.o[d]), g, d);
+    }
+}
+
+// ScalarSampler::sample (src/sampling.rs:74-122) in arithmetic type R from
+// the scaled coordinate: q = clamp(xh - offset) per axis, the eight corners
+// weighted ((1 * w_x) * w_y) * w_z in the reference's z, y, x order, the sum
+// clamped to the corners' range. 1 * w_x is w_x exactly, so the products
+// w_x w_y are formed once per (x, y) pair and the corner offsets once per
+// axis; the values and every rounding are the reference's. double reproduces
+// the reference; float is the mixed-precision path.
 template <class T, class R>
-__device__ __forceinline__ R sample(const GridDev& g, const T* __restrict__ values, const int dims[3], const R off[3],
-                                    const R pos[3], int& flag) {
+__device__ __forceinline__ R sample_at(const T* __restrict__ values, const int dims[3], const R off[3], const R xh[3],
+                                       int& flag) {
     int lo[3], hi[3];
     R t[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        R x = clampd<R>(pos[d], R(g.o[d]), R(g.up[d]));
-        R q = clampd<R>(div_h<R>(x - R(g.o[d]), g, d) - off[d], R(0), R(dims[d] - 1));
+        R q = clampd<R>(xh[d] - off[d], R(0), R(dims[d] - 1));
         if (!isfinite(q)) {
             flag |= VF_ARITH;
             q = R(0);
@@ -52,6 +68,14 @@ __device__ __forceinline__ R sample(const GridDev& g, const T* __restrict__ valu
         hi[d] = min(lo[d] + 1, dims[d] - 1);
         t[d] = q - R(lo[d]);
     }
+    const R wx[2] = {R(1) - t[0], t[0]};
+    const R wy[2] = {R(1) - t[1], t[1]};
+    const R wz[2] = {R(1) - t[2], t[2]};
+    const R wxy[2][2] = {{wx[0] * wy[0], wx[1] * wy[0]}, {wx[0] * wy[1], wx[1] * wy[1]}};
+    const int px[2] = {lo[0], hi[0]};
+    const int py[2] = {dims[0] * lo[1], dims[0] * hi[1]};
+    const int plane = dims[0] * dims[1];
+    const int pz[2] = {plane * lo[2], plane * hi[2]};
     R result = R(0);
     R minimum = R(CUDART_INF);
     R maximum = R(-CUDART_INF);
@@ -61,20 +85,22 @@ __device__ __forceinline__ R sample(const GridDev& g, const T* __restrict__ valu
         for (int y = 0; y < 2; ++y)
 #pragma unroll
             for (int x = 0; x < 2; ++x) {
-                int px = x ? hi[0] : lo[0];
-                int py = y ? hi[1] : lo[1];
-                int pz = z ? hi[2] : lo[2];
-                R weight = R(1);
-                weight = weight * (x ? t[0] : R(1) - t[0]);
-                weight = weight * (y ? t[1] : R(1) - t[1]);
-                weight = weight * (z ? t[2] : R(1) - t[2]);
-                R value = R(__ldg(values + (px + dims[0] * (py + dims[1] * pz))));
+                const R weight = wxy[y][x] * wz[z];
+                const R value = R(__ldg(values + (px[x] + py[y] + pz[z])));
                 minimum = fmin(minimum, value);
                 maximum = fmax(maximum, value);
                 result += weight * value;
             }
     if (!isfinite(result)) flag |= VF_ARITH;
     return clampd<R>(result, minimum, maximum);
+}
+
+template <class T, class R>
+__device__ __forceinline__ R sample(const GridDev& g, const T* __restrict__ values, const int dims[3], const R off[3],
+                                    const R pos[3], int& flag) {
+    R xh[3];
+    scaled_position<R>(g, pos, xh);
+    return sample_at<T, R>(values, dims, off, xh, flag);
 }
 
 template <class T>
@@ -94,12 +120,14 @@ __device__ __forceinline__ void face_geometry(const GridDev& g, int a, int dims[
 template <class T, class R>
 __device__ __forceinline__ void velocity_sample(const GridDev& g, const Faces<T>& vel, const R pos[3], R out[3],
                                                 int& flag) {
+    R xh[3];
+    scaled_position<R>(g, pos, xh);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         int dims[3];
         R off[3];
         face_geometry<R>(g, a, dims, off);
-        out[a] = sample<T, R>(g, vel.f[a], dims, off, pos, flag);
+        out[a] = sample_at<T, R>(vel.f[a], dims, off, xh, flag);
     }
 }
 

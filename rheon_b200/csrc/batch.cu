@@ -26,7 +26,9 @@ namespace rb200 {
 namespace {
 
 constexpr int BT = 256;       // threads of the packed elementwise kernels
-constexpr int kItems = 4;     // elementwise items per thread
+constexpr int kItems = 4;     // advected faces per thread
+constexpr int kCellItems = 16;  // cells per thread of the cell passes (most reduce: a block's reduction covers 4096 cells)
+constexpr int kRowsPerWarp = 4;  // rows per warp of the FCG update and finish (their reductions cover 32 rows)
 constexpr int kPass1Kc = 8;   // z-march length of the direction pass
 constexpr int kChunk = 4;     // iterations per trip of the solve loop
 constexpr int kSlotDoubles = 2 * 3 + 3;  // widest partials: the compatibility sums (3 sums, 3 maxima)
@@ -150,8 +152,7 @@ __global__ void __launch_bounds__(BT) k_b_init_sums(const BatchInstDev* __restri
 }
 
 // r <- b (INIT) or the true residual (REPLACE), r[0] = 0. The multigrid
-// method forms z in its own kernels; q[0] receives the z[0] = 0 of the
-// gauge row (q[0] is 0 in every direction pass anyway).
+// method forms z in its own kernels (no z vector).
 __global__ void __launch_bounds__(BT) k_b_load_residual(const BatchInstDev* __restrict__ inst, const __grid_constant__ BatchSpans spans,
                                                         int mode) {
     pdl_wait();
@@ -160,7 +161,7 @@ __global__ void __launch_bounds__(BT) k_b_load_residual(const BatchInstDev* __re
     const BatchInstDev& I = inst[batch_entry(spans, sp)];
     load_geometry(g, I.g);
     __syncthreads();
-    load_residual_body<KIND_MG>(g, I.st, I.b, I.d0, I.d1, I.r, I.q, mode, I.part, nullptr, sp);
+    load_residual_body<KIND_MG>(g, I.st, I.b, I.d0, I.d1, I.r, nullptr, mode, I.part, nullptr, sp);
 }
 
 // ------------------------------------------------------------ V-cycle operations
@@ -241,7 +242,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_b_dense(const BatchLevelOp* __re
 }
 
 // ------------------------------------------------------------ flexible-CG passes
-__global__ void __launch_bounds__(MG_THREADS) k_b_pass1(const BatchInstDev* __restrict__ inst, const __grid_constant__ BatchSpans spans,
+__global__ void __launch_bounds__(MG_THREADS, 3) k_b_pass1(const BatchInstDev* __restrict__ inst, const __grid_constant__ BatchSpans spans,
                                                         int kc_len) {
     pdl_wait();
     __shared__ GridDev g;
@@ -251,10 +252,10 @@ __global__ void __launch_bounds__(MG_THREADS) k_b_pass1(const BatchInstDev* __re
     load_geometry(g, I.g);
     block_copy(L, I.fine);
     __syncthreads();
-    pass1_body(g, L, I.st, I.d0, I.d1, I.q, I.part, nullptr, kc_len, sp);
+    pass1_body(g, L, I.st, I.d0, I.d1, I.part, nullptr, kc_len, sp);
 }
 
-__global__ void __launch_bounds__(MG_THREADS) k_b_update_first(const BatchInstDev* __restrict__ inst,
+__global__ void __launch_bounds__(MG_THREADS, 3) k_b_update_first(const BatchInstDev* __restrict__ inst,
                                                                const __grid_constant__ BatchSpans spans) {
     pdl_wait();
     __shared__ GridDev g;
@@ -264,10 +265,10 @@ __global__ void __launch_bounds__(MG_THREADS) k_b_update_first(const BatchInstDe
     load_geometry(g, I.g);
     block_copy(L, I.fine);
     __syncthreads();
-    update_first_body(g, L, I.st, I.p, I.r, I.d0, I.d1, I.q, I.part, nullptr, sp);
+    update_first_body(g, L, I.st, I.p, I.r, I.r1, I.d0, I.d1, I.part, nullptr, sp);
 }
 
-__global__ void __launch_bounds__(MG_THREADS) k_b_finish(const BatchInstDev* __restrict__ inst, const __grid_constant__ BatchSpans spans,
+__global__ void __launch_bounds__(MG_THREADS, 3) k_b_finish(const BatchInstDev* __restrict__ inst, const __grid_constant__ BatchSpans spans,
                                                          int mode) {
     pdl_wait();
     __shared__ MgLevelDev L;
@@ -275,7 +276,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_b_finish(const BatchInstDev* __r
     const BatchInstDev& I = inst[batch_entry(spans, sp)];
     block_copy(L, I.fine);
     __syncthreads();
-    finish_red_body(L, 1, I.st, I.r, I.q, mode, I.part, nullptr, sp);
+    finish_red_body(L, 1, I.st, I.r, I.r1, mode, I.part, nullptr, sp);
 }
 
 // true_report (src/pressure.rs:432-456) and solve_loaded's acceptance and
@@ -494,17 +495,21 @@ enum OpKind : int { OP_SMOOTH = 0, OP_PAIR = 1, OP_RESTRICT = 2, OP_PROLONG = 3,
 enum KernelKind : int {
     KK_SMOOTH = 0, KK_PAIR, KK_RESTRICT, KK_PROLONG, KK_DENSE,  // the V-cycle operations (OpKind order)
     KK_BEGIN, KK_ADVECT, KK_RHS, KK_RESET, KK_SUMS, KK_LOAD, KK_PASS1, KK_UPDATE, KK_FINISH, KK_TRUE,
-    KK_CORRECT, KK_END, KK_CONTROL, KK_COUNT
+    KK_CORRECT, KK_END, KK_CONTROL,
+    KK_SMOOTH_FINE, KK_PAIR_FINE, KK_RESTRICT_FINE, KK_PROLONG_FINE,  // the same on the finest level
+    KK_COUNT
 };
 const char* const kKernelNames[KK_COUNT] = {
     "k_b_smooth", "k_b_pair", "k_b_restrict", "k_b_prolong", "k_b_dense", "k_b_begin", "k_b_advect", "k_b_rhs",
     "k_b_reset", "k_b_init_sums", "k_b_load_residual", "k_b_pass1", "k_b_update_first", "k_b_finish",
-    "k_b_true_residual", "k_b_correct", "k_b_end", "loop control"};
+    "k_b_true_residual", "k_b_correct", "k_b_end", "loop control", "k_b_smooth (finest)", "k_b_pair (finest)",
+    "k_b_restrict (finest)", "k_b_prolong (finest)"};
 
 // One launch of the V-cycle program: an operation over the instances that
 // take part at that point of the cycle.
 struct VLaunch {
     int kind;
+    int level;        // the depth of the hierarchy it works on
     size_t first_op;  // index of its first entry in the batch's op table
     BatchSpans spans;
     size_t smem;
@@ -593,6 +598,7 @@ int build_program(rb200_batch* B) {
     auto add = [&](std::vector<VLaunch>& prog, int kind, int l, auto make) {
         VLaunch v{};
         v.kind = kind;
+        v.level = l;
         v.first_op = B->ops.size();
         std::vector<int> blocks;
         size_t smem = 0;
@@ -722,11 +728,20 @@ struct Emit {
         for (const VLaunch& v : prog) {
             const BatchLevelOp* o = B->ops_d + v.first_op;
             const int nb = total_blocks(v.spans);
+            const bool fine = v.level == 0;
             switch (v.kind) {
-                case OP_SMOOTH: go(KK_SMOOTH, true, k_b_smooth, nb, MG_THREADS, 0, o, v.spans, mode); break;
-                case OP_PAIR: go(KK_PAIR, true, k_b_pair, nb, MG_THREADS, v.smem, o, v.spans, mode); break;
-                case OP_RESTRICT: go(KK_RESTRICT, true, k_b_restrict, nb, MG_THREADS, 0, o, v.spans, mode); break;
-                case OP_PROLONG: go(KK_PROLONG, true, k_b_prolong, nb, MG_THREADS, 0, o, v.spans, mode); break;
+                case OP_SMOOTH:
+                    go(fine ? KK_SMOOTH_FINE : KK_SMOOTH, true, k_b_smooth, nb, MG_THREADS, 0, o, v.spans, mode);
+                    break;
+                case OP_PAIR:
+                    go(fine ? KK_PAIR_FINE : KK_PAIR, true, k_b_pair, nb, MG_THREADS, v.smem, o, v.spans, mode);
+                    break;
+                case OP_RESTRICT:
+                    go(fine ? KK_RESTRICT_FINE : KK_RESTRICT, true, k_b_restrict, nb, MG_THREADS, 0, o, v.spans, mode);
+                    break;
+                case OP_PROLONG:
+                    go(fine ? KK_PROLONG_FINE : KK_PROLONG, true, k_b_prolong, nb, MG_THREADS, 0, o, v.spans, mode);
+                    break;
                 default: go(KK_DENSE, true, k_b_dense, nb, MG_THREADS, 0, o, v.spans, mode); break;
             }
         }
@@ -1001,8 +1016,8 @@ int rb200_batch_create(const rb200_grid* grids, size_t count, const rb200_batch_
         const GridDev& g = B->grids[i];
         const long long faces = (long long)g.flen[0] + g.flen[1] + g.flen[2];
         bf.push_back(ceil_div(faces, BT * kItems));
-        bc.push_back(ceil_div(g.cells, BT * kItems));
-        br.push_back(ceil_div((long long)g.n[1] * g.n[2], MG_THREADS / 32));
+        bc.push_back(ceil_div(g.cells, BT * kCellItems));
+        br.push_back(ceil_div((long long)g.n[1] * g.n[2], (MG_THREADS / 32) * kRowsPerWarp));
         const int qsegs = ceil_div(g.n[0] / 4, 32);
         const long long lines = (long long)qsegs * g.n[1] * ceil_div(g.n[2], kPass1Kc);
         bp.push_back(std::max(1, ceil_div(lines, MG_THREADS / 32)));
@@ -1052,7 +1067,7 @@ int rb200_batch_create(const rb200_grid* grids, size_t count, const rb200_batch_
         I.g = g;
         for (int b = 0; b < 3; ++b)
             for (int a = 0; a < 3; ++a) I.faces[b][a] = reinterpret_cast<float*>(take(size_t(g.flen[a]) * 4));
-        double** vec[6] = {&I.b, &I.p, &I.r, &I.d0, &I.d1, &I.q};
+        double** vec[6] = {&I.b, &I.p, &I.r, &I.r1, &I.d0, &I.d1};
         for (double** v : vec) *v = reinterpret_cast<double*>(take(size_t(g.cells) * 8));
         I.st = reinterpret_cast<SolveState*>(take(sizeof(SolveState)));
         I.part.ticket = reinterpret_cast<unsigned*>(take(sizeof(unsigned)));

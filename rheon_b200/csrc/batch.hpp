@@ -54,7 +54,7 @@ struct BatchStepDev {
 struct BatchInstDev {
     GridDev g;
     float* faces[3][3];  // [buffer][axis], f32 storage
-    double *b, *p, *r, *d0, *d1, *q;
+    double *b, *p, *r, *r1, *d0, *d1;  // r, r1: the two residual buffers (the state's rsel picks r)
     SolveState* st;
     Partials part;       // this instance's reduction partials and ticket
     BatchStepDev* step;

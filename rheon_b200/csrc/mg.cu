@@ -503,40 +503,37 @@ int Multigrid::enqueue(const double* r, const void* state, int mode, cudaStream_
 
 // ------------------------------------------------------------ flexible-CG kernels
 __global__ void __launch_bounds__(MG_THREADS) k_mg_finish_red(MgLevelDev L, int smooth, SolveState* st,
-                                                              const double* __restrict__ r,
-                                                              const double* __restrict__ q, int mode, Partials part,
-                                                              rb200_trace* trace) {
+                                                              const double* r0, const double* r1, int mode,
+                                                              Partials part, rb200_trace* trace) {
     pdl_wait();
-    finish_red_body(L, smooth, st, r, q, mode, part, trace, whole_launch());
+    finish_red_body(L, smooth, st, r0, r1, mode, part, trace, whole_launch());
 }
 
 __global__ void __launch_bounds__(MG_THREADS) k_mg_pass1(GridDev g, MgLevelDev L, SolveState* st, double* d0,
-                                                         double* d1, double* __restrict__ q, Partials part,
-                                                         rb200_trace* trace, int kc_len) {
+                                                         double* d1, Partials part, rb200_trace* trace, int kc_len) {
     pdl_wait();
-    pass1_body(g, L, st, d0, d1, q, part, trace, kc_len, whole_launch());
+    pass1_body(g, L, st, d0, d1, part, trace, kc_len, whole_launch());
 }
 
 __global__ void __launch_bounds__(MG_THREADS) k_mg_update_first(GridDev g, MgLevelDev L, SolveState* st,
-                                                                double* __restrict__ p, double* __restrict__ r,
-                                                                const double* d0, const double* d1,
-                                                                const double* __restrict__ q, Partials part,
+                                                                double* __restrict__ p, double* r0, double* r1,
+                                                                const double* d0, const double* d1, Partials part,
                                                                 rb200_trace* trace) {
     pdl_wait();
-    update_first_body(g, L, st, p, r, d0, d1, q, part, trace, whole_launch());
+    update_first_body(g, L, st, p, r0, r1, d0, d1, part, trace, whole_launch());
 }
 
 
-int Multigrid::enqueue_update_first(const GridDev& g, void* state, double* p, double* r, double* d0, double* d1,
-                                    const double* q, Partials part, rb200_trace* trace, cudaStream_t s) const {
+int Multigrid::enqueue_update_first(const GridDev& g, void* state, double* p, double* r0, double* r1, double* d0,
+                                    double* d1, Partials part, rb200_trace* trace, cudaStream_t s) const {
     int pb = row_blocks(levels_[0]);
     if (pb > 148 * 8) pb = 148 * 8;  // reduction partials capacity
     pdl_launch(k_mg_update_first, dim3(pb), dim3(MG_THREADS), 0, s, g, levels_[0], static_cast<SolveState*>(state), p,
-               r, d0, d1, q, part, trace);
+               r0, r1, d0, d1, part, trace);
     return 1;
 }
 
-int Multigrid::enqueue_pass1(const GridDev& g, void* state, double* d0, double* d1, double* q, Partials part,
+int Multigrid::enqueue_pass1(const GridDev& g, void* state, double* d0, double* d1, Partials part,
                              rb200_trace* trace, cudaStream_t s) const {
     int pb = row_blocks(levels_[0]);
     if (pb > 148 * 8) pb = 148 * 8;  // reduction partials capacity
@@ -546,18 +543,18 @@ int Multigrid::enqueue_pass1(const GridDev& g, void* state, double* d0, double* 
     const int warps = pb * (MG_THREADS / 32);
     int kc_len = 16;
     while (kc_len > 2 && qsegs * g.n[1] * ((g.n[2] + kc_len - 1) / kc_len) < warps) kc_len /= 2;
-    pdl_launch(k_mg_pass1, dim3(pb), dim3(MG_THREADS), 0, s, g, levels_[0], static_cast<SolveState*>(state), d0, d1, q,
+    pdl_launch(k_mg_pass1, dim3(pb), dim3(MG_THREADS), 0, s, g, levels_[0], static_cast<SolveState*>(state), d0, d1,
                part, trace, kc_len);
     return 1;
 }
 
-int Multigrid::enqueue_finish(void* state, const double* r, const double* q, int mode, Partials part,
+int Multigrid::enqueue_finish(void* state, const double* r0, const double* r1, int mode, Partials part,
                               rb200_trace* trace, cudaStream_t s) const {
     const MgLevelDev& L = levels_[0];
     int pb = row_blocks(L);
     if (pb > 148 * 8) pb = 148 * 8;  // reduction partials capacity
     pdl_launch(k_mg_finish_red, dim3(pb), dim3(MG_THREADS), 0, s, L, levels_.size() > 1 ? 1 : 0,
-               static_cast<SolveState*>(state), r, q, mode, part, trace);
+               static_cast<SolveState*>(state), r0, r1, mode, part, trace);
     return 1;
 }
 

@@ -82,16 +82,18 @@ public:
     // Whether enqueue_update_first applies (the finest level is a grid-kernel
     // level), and the fused flexible-CG update + first red half-sweep.
     bool fuses_update() const { return lower_first_ > 0; }
-    int enqueue_update_first(const GridDev& g, void* state, double* p, double* r, double* d0, double* d1,
-                             const double* q, Partials part, rb200_trace* trace, cudaStream_t s) const;
+    // r0 and r1 are the two residual buffers (the state's rsel tells which
+    // holds r; the update writes the other).
+    int enqueue_update_first(const GridDev& g, void* state, double* p, double* r0, double* r1, double* d0,
+                             double* d1, Partials part, rb200_trace* trace, cudaStream_t s) const;
     // The finish: last red half-sweep of level 0 (when there is a hierarchy),
-    // r.z and z.q with z = x (z[0] = 0), and the flexible-CG decision. z stays
-    // in the finest level's x (FP32); enqueue_pass1 reads it there.
-    int enqueue_finish(void* state, const double* r, const double* q, int mode, Partials part,
+    // r.z and z.r_old with z = x (z[0] = 0), and the flexible-CG decision. z
+    // stays in the finest level's x (FP32); enqueue_pass1 reads it there.
+    int enqueue_finish(void* state, const double* r0, const double* r1, int mode, Partials part,
                        rb200_trace* trace, cudaStream_t s) const;
     // The flexible-CG direction pass reading z from the finest level's x.
-    int enqueue_pass1(const GridDev& g, void* state, double* d0, double* d1, double* q, Partials part,
-                      rb200_trace* trace, cudaStream_t s) const;
+    int enqueue_pass1(const GridDev& g, void* state, double* d0, double* d1, Partials part, rb200_trace* trace,
+                      cudaStream_t s) const;
     const MgLevelDev& fine() const { return levels_[0]; }
     int levels() const { return int(levels_.size()); }
     size_t bytes() const { return bytes_; }

@@ -495,15 +495,21 @@ constexpr int PAIR_ROWS = (PJ + 2) * (PK + 2);
 constexpr size_t kPairSmemMax = 200 * 1024;
 
 // ------------------------------------------------------------ flexible-CG passes
+
 // The finest level's last red half-sweep fused with the outer method's
 // preconditioner output: z = x (FP64, z[0] = 0 for the eliminated gauge row),
-// r.z and z.q reduced and the flexible-CG decision taken. Without a hierarchy
+// r.z and z.r_old reduced and the flexible-CG decision taken. Without a hierarchy
 // (a single level solved densely) z is copied from x.
-__device__ __forceinline__ void finish_red_body(const MgLevelDev& L, int smooth, SolveState* st,
-                                                const double* __restrict__ r, const double* __restrict__ q, int mode,
-                                                Partials part, rb200_trace* trace, Span sp) {
+__device__ __forceinline__ void finish_red_body(const MgLevelDev& L, int smooth, SolveState* st, const double* r0,
+                                                const double* r1, int mode, Partials part, rb200_trace* trace,
+                                                Span sp) {
     __shared__ BlockReduce<2, 0> red;
     if (!gate(st->flags, mode)) return;
+    // r (after this iteration's update) and r_old (before it), for r.z and
+    // z.r_old (iterations only)
+    const int rsel = st->rsel;
+    const double* __restrict__ r = rsel ? r1 : r0;
+    const double* __restrict__ r_old = rsel ? r0 : r1;
     Neu rz, zq;
     const Warps W = span_warps(sp);
     const int hx = (L.n[0] + 1) >> 1;
@@ -551,20 +557,13 @@ __device__ __forceinline__ void finish_red_body(const MgLevelDev& L, int smooth,
                 const double2 r01 = *reinterpret_cast<const double2*>(r + c0);
                 const double2 r23 = *reinterpret_cast<const double2*>(r + c0 + 2);
                 const double rr[4] = {r01.x, r01.y, r23.x, r23.y};
-                double qq[4] = {0.0, 0.0, 0.0, 0.0};
-                if (mode == MODE_ITER) {
-                    const double2 q01 = *reinterpret_cast<const double2*>(q + c0);
-                    const double2 q23 = *reinterpret_cast<const double2*>(q + c0 + 2);
-                    qq[0] = q01.x;
-                    qq[1] = q01.y;
-                    qq[2] = q23.x;
-                    qq[3] = q23.y;
-                }
+                double ro[4] = {0.0, 0.0, 0.0, 0.0};
+                if (mode == MODE_ITER) ld_quad(r_old + c0, ro);
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     if (c0 + e == 0) continue;
                     rz.add(rr[e] * zc[e]);
-                    if (mode == MODE_ITER) zq.add(zc[e] * qq[e]);
+                    if (mode == MODE_ITER) zq.add(zc[e] * ro[e]);
                 }
             }
         }
@@ -581,7 +580,7 @@ __device__ __forceinline__ void finish_red_body(const MgLevelDev& L, int smooth,
                 const double zc = c == 0 ? 0.0 : double(L.x[c]);
                 if (c != 0) {
                     rz.add(r[c] * zc);
-                    if (mode == MODE_ITER) zq.add(zc * q[c]);
+                    if (mode == MODE_ITER) zq.add(zc * r_old[c]);
                 }
             }
             if (i < L.n[0]) {
@@ -594,7 +593,7 @@ __device__ __forceinline__ void finish_red_body(const MgLevelDev& L, int smooth,
                 const double zc = c == 0 ? 0.0 : double(xv);
                 if (c != 0) {
                     rz.add(r[c] * zc);
-                    if (mode == MODE_ITER) zq.add(zc * q[c]);
+                    if (mode == MODE_ITER) zq.add(zc * r_old[c]);
                 }
             }
         }
@@ -608,13 +607,12 @@ __device__ __forceinline__ void finish_red_body(const MgLevelDev& L, int smooth,
     }
 }
 // The flexible-CG direction pass of the mixed method (src/pressure.rs:657-668,
-// :720-731): d = z + beta d (d = z after a restart), q = K d stored, d.q and
-// the decision for alpha. z is read straight from the V-cycle's FP32 output x
+// :720-731): d = z + beta d (d = z after a restart), q = K d, d.q and the
+// decision for alpha; q is not stored (the later passes recompute it). z is read straight from the V-cycle's FP32 output x
 // of the finest level (z = f64(x), z[0] = 0 for the eliminated gauge row), so
 // no FP64 copy of z is stored. One warp per cell row, lanes along x.
 __device__ __forceinline__ void pass1_body(const GridDev& g, const MgLevelDev& L, SolveState* st, double* d0,
-                                           double* d1, double* __restrict__ q, Partials part, rb200_trace* trace,
-                                           int kc_len, Span sp) {
+                                           double* d1, Partials part, rb200_trace* trace, int kc_len, Span sp) {
     __shared__ BlockReduce<1, 0> red;
     const int flags = st->flags;
     if (flags & F_STOP) return;
@@ -693,8 +691,6 @@ __device__ __forceinline__ void pass1_body(const GridDev& g, const MgLevelDev& L
                 }
                 *reinterpret_cast<double2*>(dst + c0) = make_double2(cur[0], cur[1]);
                 *reinterpret_cast<double2*>(dst + c0 + 2) = make_double2(cur[2], cur[3]);
-                *reinterpret_cast<double2*>(q + c0) = make_double2(qq[0], qq[1]);
-                *reinterpret_cast<double2*>(q + c0 + 2) = make_double2(qq[2], qq[3]);
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     acc.add(cur[e] * qq[e]);
@@ -719,7 +715,6 @@ __device__ __forceinline__ void pass1_body(const GridDev& g, const MgLevelDev& L
             v.zp = k + 1 < g.n[2] ? dn(c + sz) : 0.0;
             const double qv = c == 0 ? 0.0 : apply_row(g, i, j, k, v);
             dst[c] = v.c;
-            q[c] = qv;
             acc.add(v.c * qv);
         }
     }
@@ -731,19 +726,23 @@ __device__ __forceinline__ void pass1_body(const GridDev& g, const MgLevelDev& L
         if (threadIdx.x == 0) decide_pass1(st, trace, dd_value(sums[0]), flags, dsel);
     }
 }
-// The flexible-CG update (p += alpha d, r -= alpha q, |r|^2 and the candidate
+// The flexible-CG update (p += alpha d, r = r_old - alpha K d into the other
+// residual buffer, |r|^2 and the candidate
 // test) fused with the V-cycle's first half-sweep on the finest level, which
 // needs no neighbour: b = f32(r), red x = b / D, black x = 0. Used when the
 // finest level is a grid-kernel level.
 __device__ __forceinline__ void update_first_body(const GridDev& g, const MgLevelDev& L, SolveState* st,
-                                                  double* __restrict__ p, double* __restrict__ r, const double* d0,
-                                                  const double* d1, const double* __restrict__ q, Partials part,
-                                                  rb200_trace* trace, Span sp) {
+                                                  double* __restrict__ p, double* r0, double* r1, const double* d0,
+                                                  const double* d1, Partials part, rb200_trace* trace, Span sp) {
     __shared__ BlockReduce<1, 0> red;
     const int flags = st->flags;
     if (flags & F_STOP) return;
     const double alpha = st->alpha;
     const double* __restrict__ d = st->dsel ? d1 : d0;
+    // r_old is kept: the new residual goes to the other buffer
+    const int rsel = st->rsel;
+    const double* __restrict__ r = rsel ? r1 : r0;
+    double* __restrict__ r_out = rsel ? r0 : r1;
     Neu acc;
     const Warps W = span_warps(sp);
     const int n0 = g.n[0], rows = g.n[1] * g.n[2];
@@ -757,15 +756,12 @@ __device__ __forceinline__ void update_first_body(const GridDev& g, const MgLeve
             for (int qd = W.lane; qd < (n0 >> 2); qd += 32) {
                 const int i0 = 4 * qd;
                 const int c0 = base + i0;
+                // q = K d first, so that d's neighbour rows are dead before p and r load
                 double pv[4], rv[4], dv[4], qv[4];
-                *reinterpret_cast<double2*>(pv) = *reinterpret_cast<const double2*>(p + c0);
-                *reinterpret_cast<double2*>(pv + 2) = *reinterpret_cast<const double2*>(p + c0 + 2);
-                *reinterpret_cast<double2*>(rv) = *reinterpret_cast<const double2*>(r + c0);
-                *reinterpret_cast<double2*>(rv + 2) = *reinterpret_cast<const double2*>(r + c0 + 2);
-                *reinterpret_cast<double2*>(dv) = *reinterpret_cast<const double2*>(d + c0);
-                *reinterpret_cast<double2*>(dv + 2) = *reinterpret_cast<const double2*>(d + c0 + 2);
-                *reinterpret_cast<double2*>(qv) = *reinterpret_cast<const double2*>(q + c0);
-                *reinterpret_cast<double2*>(qv + 2) = *reinterpret_cast<const double2*>(q + c0 + 2);
+                ld_quad(d + c0, dv);
+                kd_quad(g, d, c0, i0, j, k, dv, qv);
+                ld_quad(p + c0, pv);
+                ld_quad(r + c0, rv);
                 float4 bq, xq = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
@@ -784,8 +780,8 @@ __device__ __forceinline__ void update_first_body(const GridDev& g, const MgLeve
                 }
                 *reinterpret_cast<double2*>(p + c0) = *reinterpret_cast<double2*>(pv);
                 *reinterpret_cast<double2*>(p + c0 + 2) = *reinterpret_cast<double2*>(pv + 2);
-                *reinterpret_cast<double2*>(r + c0) = *reinterpret_cast<double2*>(rv);
-                *reinterpret_cast<double2*>(r + c0 + 2) = *reinterpret_cast<double2*>(rv + 2);
+                *reinterpret_cast<double2*>(r_out + c0) = *reinterpret_cast<double2*>(rv);
+                *reinterpret_cast<double2*>(r_out + c0 + 2) = *reinterpret_cast<double2*>(rv + 2);
                 *reinterpret_cast<float4*>(L.b + c0) = bq;
                 *reinterpret_cast<float4*>(L.x + c0) = xq;
             }
@@ -795,10 +791,10 @@ __device__ __forceinline__ void update_first_body(const GridDev& g, const MgLeve
                 double rc = r[c];
                 if (c != 0) {
                     p[c] = p[c] + alpha * d[c];
-                    rc = rc - alpha * q[c];
-                    r[c] = rc;
+                    rc = rc - alpha * kd_at(g, d, i, j, k, c);
                     acc.add(rc * rc);
                 }
+                r_out[c] = rc;
                 const float b = float(rc);
                 L.b[c] = b;
                 const bool isred = ((i + j + k) & 1) == 0;
@@ -812,6 +808,7 @@ __device__ __forceinline__ void update_first_body(const GridDev& g, const MgLeve
     if (publish_and_check_last<1, 0>(part, sp.block, sp.blocks, sums, none)) {
         fold_partials<1, 0>(part, sp.blocks, red, sums, none);
         if (threadIdx.x == 0) {
+            st->rsel = rsel ^ 1;
             if (flags & F_PROFILE) return;
             const int it = st->it + 1;
             st->it = it;

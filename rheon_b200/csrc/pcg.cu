@@ -293,14 +293,20 @@ __global__ void __launch_bounds__(TILE_THREADS) k_true_residual(GridDev g, Solve
 }
 
 // ------------------------------------------------------------ multigrid outer passes
-// Flexible CG around the FP32 multigrid preconditioner: q = K d is stored by
-// pass 1; the update pass is elementwise; the finish pass converts the FP32
-// V-cycle output to z (FP64, z[0] = 0), reduces r.z and z.q and takes the
-// decision with beta = -z.q / d.q (Polak-Ribiere form, tolerant of a
-// preconditioner that is symmetric only up to FP32 rounding).
+// Flexible CG around the FP32 multigrid preconditioner: q = K d is formed by
+// pass 1 for d.q and recomputed from d where the update and the finish need it
+// (no q vector); the finish pass converts the FP32 V-cycle output to z (FP64,
+// z[0] = 0), reduces r.z and z.r_old and takes the decision with the
+// Polak-Ribiere beta = (z.r - z.r_old) / (z_old.r_old) (tolerant of a
+// preconditioner that is symmetric only up to FP32 rounding). The residual
+// before the update stays available in a second buffer. This update serves
+// grids whose finest level is solved inside the cluster kernel: r stays in the
+// first buffer (the V-cycle's first half-sweep reads it there) and r_old is
+// copied to the second.
 __global__ void __launch_bounds__(EW) k_mg_update(GridDev g, SolveState* st, double* __restrict__ p,
-                                                  double* __restrict__ r, const double* d0, const double* d1,
-                                                  const double* __restrict__ q, Partials part, rb200_trace* trace) {
+                                                  double* __restrict__ r, double* __restrict__ r_old,
+                                                  const double* d0, const double* d1, Partials part,
+                                                  rb200_trace* trace) {
     __shared__ BlockReduce<1, 0> red;
     const int flags = st->flags;
     if (flags & F_STOP) return;
@@ -308,9 +314,15 @@ __global__ void __launch_bounds__(EW) k_mg_update(GridDev g, SolveState* st, dou
     const double* __restrict__ d = st->dsel ? d1 : d0;
     Neu acc;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
-        if (c == 0) continue;
+        if (c == 0) {
+            r_old[0] = 0.0;
+            continue;
+        }
+        const int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
         p[c] = p[c] + alpha * d[c];
-        double rc = r[c] - alpha * q[c];
+        const double ro = r[c];
+        double rc = ro - alpha * kd_at(g, d, i, j, k, c);
+        r_old[c] = ro;
         r[c] = rc;
         acc.add(rc * rc);
     }
@@ -684,7 +696,7 @@ static int set_smem_attrs() {
 }
 
 struct Bufs {
-    double *b, *p, *r, *z, *d0, *d1, *q;
+    double *b, *p, *r, *z, *d0, *d1, *r1;  // r1: the multigrid method's second residual buffer
     SolveState* st;
     Partials part;
     rb200_trace* trace;
@@ -779,7 +791,7 @@ static int launch_start(const GridDev& g, int method, const Bufs& B, const Multi
     k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_INIT, B.part, B.trace);
     if (method == RB200_SGS_PCG_V1) return 2 + launch_sgs(g, B, MODE_INIT, s);
     int n = 2 + mg->enqueue(B.r, B.st, MODE_INIT, s);
-    return n + mg->enqueue_finish(B.st, B.r, B.q, MODE_INIT, B.part, B.trace, s);
+    return n + mg->enqueue_finish(B.st, B.r, B.r1, MODE_INIT, B.part, B.trace, s);
 }
 
 // One PCG iteration (src/pressure.rs:651-734).
@@ -788,7 +800,7 @@ static int launch_iteration(const GridDev& g, int method, const Bufs& B, const M
     const int eb = ew_blocks(g.cells);
     const bool flexible = method == RB200_MG_MIXED;
     if (flexible)
-        mg->enqueue_pass1(g, B.st, B.d0, B.d1, B.q, B.part, B.trace, s);
+        mg->enqueue_pass1(g, B.st, B.d0, B.d1, B.part, B.trace, s);
     else
         k_pass1<ZC><<<grid, block, kSmemPass1, s>>>(g, B.st, B.z, B.d0, B.d1, nullptr, B.maps, B.part, B.trace);
     if (method == RB200_JACOBI_PCG_V1) {
@@ -812,13 +824,13 @@ static int launch_iteration(const GridDev& g, int method, const Bufs& B, const M
     }
     int n = 2;
     if (mg->fuses_update()) {
-        mg->enqueue_update_first(g, B.st, B.p, B.r, B.d0, B.d1, B.q, B.part, B.trace, s);
+        mg->enqueue_update_first(g, B.st, B.p, B.r, B.r1, B.d0, B.d1, B.part, B.trace, s);
         n += mg->enqueue(B.r, B.st, MODE_ITER, s, true);
     } else {
-        k_mg_update<<<eb, EW, 0, s>>>(g, B.st, B.p, B.r, B.d0, B.d1, B.q, B.part, B.trace);
+        k_mg_update<<<eb, EW, 0, s>>>(g, B.st, B.p, B.r, B.r1, B.d0, B.d1, B.part, B.trace);
         n += mg->enqueue(B.r, B.st, MODE_ITER, s);
     }
-    return n + mg->enqueue_finish(B.st, B.r, B.q, MODE_ITER, B.part, B.trace, s);
+    return n + mg->enqueue_finish(B.st, B.r, B.r1, MODE_ITER, B.part, B.trace, s);
 }
 
 // The gated true-residual check and restart (src/pressure.rs:686-715).
@@ -843,7 +855,7 @@ static int launch_check(const GridDev& g, int method, const Bufs& B, const Multi
     k_load_residual<KIND_MG><<<eb, EW, 0, s>>>(g, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part, B.trace);
     if (method == RB200_SGS_PCG_V1) return 2 + launch_sgs(g, B, MODE_REPLACE, s);
     int n = 2 + mg->enqueue(B.r, B.st, MODE_REPLACE, s);
-    return n + mg->enqueue_finish(B.st, B.r, B.q, MODE_REPLACE, B.part, B.trace, s);
+    return n + mg->enqueue_finish(B.st, B.r, B.r1, MODE_REPLACE, B.part, B.trace, s);
 }
 
 static SolveState initial_state(double dt, const rb200_settings& s) {
@@ -879,7 +891,7 @@ PcgSolver::~PcgSolver() {
     cudaFree(d_[0]);
     cudaFree(d_[1]);
     cudaFree(z_);
-    cudaFree(q_);
+    cudaFree(r1_);
     cudaFree(part_.data);
     cudaFree(part_.ticket);
     cudaFree(st_);
@@ -1006,7 +1018,8 @@ int PcgSolver::init(const GridDev& g, int method, cudaStream_t stream) {
         (rc = alloc(&d_[0], n)) || (rc = alloc(&d_[1], n)))
         return rc;
     if (method == RB200_MG_MIXED) {
-        if ((rc = alloc(&q_, n))) return rc;
+        if ((rc = alloc(&r1_, n))) return rc;
+        RB200_CUDA(cudaMemsetAsync(r1_, 0, n * sizeof(double), stream_));
         if ((rc = mg_.init(g, stream_))) return rc;
         bytes_ += mg_.bytes();
     }
@@ -1062,7 +1075,7 @@ int PcgSolver::set_trace(rb200_trace* host, size_t capacity) {
 
 // One chunk: `chunk_` iterations, then the gated true-residual and restart.
 int PcgSolver::capture_chunk() {
-    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_, sgs_};
+    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], r1_, st_, part_, d_trace_, maps_, sgs_};
     const Multigrid* mg = method_ == RB200_MG_MIXED ? &mg_ : nullptr;
     cudaGraph_t graph = nullptr;
     RB200_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -1124,7 +1137,7 @@ int PcgSolver::solve(double dt, const rb200_settings& s, rb200_report* report, r
     if (d_trace_) RB200_CUDA(cudaMemsetAsync(d_trace_, 0, trace_cap_ * sizeof(rb200_trace), stream_));
     RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), stream_));
     if (gbar_) RB200_CUDA(cudaMemsetAsync(gbar_, 0, sizeof(GridBarrier), stream_));
-    launches_ += uint64_t(launch_start(g_, method_, Bufs{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_, sgs_},
+    launches_ += uint64_t(launch_start(g_, method_, Bufs{b_, p_, r_, z_, d_[0], d_[1], r1_, st_, part_, d_trace_, maps_, sgs_},
                                        method_ == RB200_MG_MIXED ? &mg_ : nullptr, stream_));
     RB200_CUDA(cudaGetLastError());
     // The host copy of the state must be stable before the chunk copies reuse
@@ -1179,7 +1192,7 @@ int PcgSolver::enqueue_reset(const double* dt_dev, const int* skip, const rb200_
     RB200_CUDA(cudaMemsetAsync(part_.ticket, 0, sizeof(unsigned), s));
     if (gbar_) RB200_CUDA(cudaMemsetAsync(gbar_, 0, sizeof(GridBarrier), s));
     launches_ += 1;
-    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_, sgs_};
+    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], r1_, st_, part_, d_trace_, maps_, sgs_};
     launch_start(g_, method_, B, method_ == RB200_MG_MIXED ? &mg_ : nullptr, s);
     RB200_CUDA(cudaGetLastError());
     return RB200_OK;
@@ -1207,7 +1220,7 @@ int PcgSolver::enqueue_loop(cudaStream_t cs, cudaStream_t body_stream, const rb2
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     // The loop body: one chunk of iterations, the gated check, the condition.
     RB200_CUDA(cudaStreamBeginCaptureToGraph(body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], q_, st_, part_, d_trace_, maps_, sgs_};
+    const Bufs B{b_, p_, r_, z_, d_[0], d_[1], r1_, st_, part_, d_trace_, maps_, sgs_};
     const Multigrid* mg = method_ == RB200_MG_MIXED ? &mg_ : nullptr;
     if (persist_blocks_) {
         RB200_CUDA(launch_persistent(g_, st_, b_, p_, r_, z_, d_[0], d_[1], ppart_, gbar_, d_trace_, maps_,
@@ -1245,7 +1258,7 @@ int PcgSolver::enqueue_loop(cudaStream_t cs, cudaStream_t body_stream, const rb2
             k_load_residual<KIND_MG><<<eb, EW, 0, rs>>>(g_, B.st, B.b, B.d0, B.d1, B.r, B.z, MODE_REPLACE, B.part,
                                                         B.trace);
             mg->enqueue(B.r, B.st, MODE_REPLACE, rs);
-            mg->enqueue_finish(B.st, B.r, B.q, MODE_REPLACE, B.part, B.trace, rs);
+            mg->enqueue_finish(B.st, B.r, B.r1, MODE_REPLACE, B.part, B.trace, rs);
             cudaGraph_t rbody = nullptr;
             ce = cudaStreamEndCapture(rs, &rbody);
         }
@@ -1318,7 +1331,7 @@ int PcgSolver::profile(int which, int launches, double* avg_ms) {
     }
     auto launch = [&]() {
         if (which == 0)
-            k_pass1<ZC><<<grid, block, kSmemPass1, stream_>>>(g_, st_, z_, d_[0], d_[1], q_, maps_, part_, nullptr);
+            k_pass1<ZC><<<grid, block, kSmemPass1, stream_>>>(g_, st_, z_, d_[0], d_[1], nullptr, maps_, part_, nullptr);
         else if (jac)
             k_pass2<ZC, 0><<<grid, block, kSmemSlab, stream_>>>(g_, st_, p_, r_, z_, d_[0], d_[1], maps_, part_,
                                                                    nullptr);
@@ -1481,7 +1494,7 @@ int static_solve_jacobi(const GridDev& g, const double* rhs, double* pressure, d
     B.d0 = B.r + kStaticMaxCells;
     B.d1 = B.d0 + kStaticMaxCells;
     B.z = B.d1 + kStaticMaxCells;
-    B.q = nullptr;
+    B.r1 = nullptr;
     B.part.data = B.z + kStaticMaxCells;
     double* state_slot = B.part.data + kStaticPartialDoubles;
     B.st = reinterpret_cast<SolveState*>(state_slot);

@@ -27,8 +27,9 @@ struct SolveState {
     int flags;
     int status;         // rb200_status, or ST_RUNNING
     int breakdown_it;
-    int flexible;       // beta = -z.q / d.q (flexible CG) instead of rz'/rz
+    int flexible;       // beta = z.(r - r_old) / rz_old (flexible CG) instead of rz'/rz
     int trips;          // loop-body passes of the graph-embedded solve
+    int rsel;           // flexible method: which residual buffer holds r (the update writes the other)
 };
 
 enum : int {
@@ -146,7 +147,7 @@ private:
     double* r_ = nullptr;
     double* d_[2] = {nullptr, nullptr};
     double* z_ = nullptr;  // preconditioned residual
-    double* q_ = nullptr;  // K d, stored by the flexible (multigrid) method
+    double* r1_ = nullptr;  // the multigrid method's second residual buffer (r and r_old alternate)
     Multigrid mg_;
     TmaMaps maps_{};
     Partials part_{nullptr, nullptr};

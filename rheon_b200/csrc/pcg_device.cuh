@@ -119,12 +119,15 @@ __device__ __forceinline__ void load_residual_body(const GridDev& g, SolveState*
     const int flags = st->flags;
     if (!gate(flags, mode)) return;
     const double* src = mode == MODE_INIT ? b : (st->dsel ? d0 : d1);
+    // the flexible method alternates two residual buffers; a loaded residual
+    // is in the first (the buffer the V-cycle's first half-sweep reads)
+    if (KIND == KIND_MG && sp.block == 0 && threadIdx.x == 0) st->rsel = 0;
     Neu acc;
     for (int c = sp.block * blockDim.x + threadIdx.x; c < g.cells; c += sp.blocks * blockDim.x) {
         double rc = c == 0 ? 0.0 : src[c];
         r[c] = rc;
         if (c == 0) {
-            z[0] = 0.0;
+            if (z) z[0] = 0.0;  // the multigrid method forms z in its own kernels and passes none
             continue;
         }
         if (KIND == KIND_MG) continue;

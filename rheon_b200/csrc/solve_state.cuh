@@ -75,17 +75,20 @@ __device__ __forceinline__ void decide_rz(SolveState* st, rb200_trace* trace, do
     st->rz = rz;
 }
 
-// Flexible-CG decision after the preconditioner (multigrid): r.z and z.q give
-// beta = -z.q / d.q (Polak-Ribiere form); init and restart behave as
-// decide_rz.
-__device__ __forceinline__ void decide_flexible(SolveState* st, rb200_trace* trace, double rz, double zq, int mode) {
+// Flexible-CG decision after the preconditioner (multigrid): r.z and
+// z.r_old (the residual before this iteration's update) give the
+// Polak-Ribiere beta = (z.r - z.r_old) / (z_old.r_old), which is
+// -z.q / d.q with q = K d since r = r_old - alpha q and alpha d.q = z_old.r_old;
+// init and restart behave as decide_rz.
+__device__ __forceinline__ void decide_flexible(SolveState* st, rb200_trace* trace, double rz, double zr_old,
+                                                int mode) {
     if (mode != MODE_ITER) {
         decide_rz(st, trace, rz, mode);
         return;
     }
     const int flags = st->flags;
     const int it = st->it;
-    const double beta = -zq / st->curvature;
+    const double beta = (rz - zr_old) / st->rz;
     if (flags & F_CANDIDATE) {
         st->rz_next = rz;
         st->beta_next = beta;

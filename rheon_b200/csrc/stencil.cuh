@@ -36,6 +36,58 @@ __device__ __forceinline__ double apply_row(const GridDev& g, int i, int j, int 
     return q;
 }
 
+// q = K d (the sealed-box operator row, apply_row) where the flexible-CG passes
+// need it: recomputed from the stored direction instead of stored by the
+// direction pass, which saves a write and a read of an FP64 vector per
+// iteration. kd_quad takes the four cells c0..c0+3 of row (j, k) of a grid
+// whose rows are a multiple of 4 long (dv: d at the quad), with 16-byte loads
+// of the y and z neighbour rows; kd_at takes one cell. The gauge row's q is 0.
+__device__ __forceinline__ void ld_quad(const double* __restrict__ a, double (&o)[4]) {
+    const double2 lo = *reinterpret_cast<const double2*>(a);
+    const double2 hi = *reinterpret_cast<const double2*>(a + 2);
+    o[0] = lo.x;
+    o[1] = lo.y;
+    o[2] = hi.x;
+    o[3] = hi.y;
+}
+__device__ __forceinline__ void kd_quad(const GridDev& g, const double* __restrict__ d, int c0, int i0, int j,
+                                        int k, const double (&dv)[4], double (&qq)[4]) {
+    const int n0 = g.n[0], sy = n0, sz = n0 * g.n[1];
+    double ym[4] = {0.0, 0.0, 0.0, 0.0}, yp[4] = {0.0, 0.0, 0.0, 0.0};
+    double zm[4] = {0.0, 0.0, 0.0, 0.0}, zp[4] = {0.0, 0.0, 0.0, 0.0};
+    if (j > 0) ld_quad(d + c0 - sy, ym);
+    if (j + 1 < g.n[1]) ld_quad(d + c0 + sy, yp);
+    if (k > 0) ld_quad(d + c0 - sz, zm);
+    if (k + 1 < g.n[2]) ld_quad(d + c0 + sz, zp);
+    const double xl = i0 > 0 ? d[c0 - 1] : 0.0;
+    const double xr = i0 + 4 < n0 ? d[c0 + 4] : 0.0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        Neigh v;
+        v.c = dv[e];
+        v.xm = e == 0 ? xl : dv[e - 1];
+        v.xp = e == 3 ? xr : dv[e + 1];
+        v.ym = ym[e];
+        v.yp = yp[e];
+        v.zm = zm[e];
+        v.zp = zp[e];
+        qq[e] = (c0 + e == 0) ? 0.0 : apply_row(g, i0 + e, j, k, v);
+    }
+}
+__device__ __forceinline__ double kd_at(const GridDev& g, const double* __restrict__ d, int i, int j, int k, int c) {
+    if (c == 0) return 0.0;
+    const int sy = g.n[0], sz = g.n[0] * g.n[1];
+    Neigh v;
+    v.c = d[c];
+    v.xm = i > 0 ? d[c - 1] : 0.0;
+    v.xp = i + 1 < g.n[0] ? d[c + 1] : 0.0;
+    v.ym = j > 0 ? d[c - sy] : 0.0;
+    v.yp = j + 1 < g.n[1] ? d[c + sy] : 0.0;
+    v.zm = k > 0 ? d[c - sz] : 0.0;
+    v.zp = k + 1 < g.n[2] ? d[c + sz] : 0.0;
+    return apply_row(g, i, j, k, v);
+}
+
 // Launch geometry of a marching kernel for a z-chunk depth zc.
 struct MarchGrid {
     dim3 grid;
