@@ -82,6 +82,10 @@ def parse():
     ap.add_argument("--no-box-flux", action="store_true")
     ap.add_argument("--box-flux", action="store_true",
                     help="box-flux projection alone (device projection, passes, host-array call, CPU oracle)")
+    ap.add_argument("--advect", action="store_true",
+                    help="the advect_velocity primitive alone at --n (f64 faces, the reference's arithmetic)")
+    ap.add_argument("--batch-profile", action="store_true",
+                    help="per-kernel device times of one packed batched step (eager launches with events)")
     ap.add_argument("--oracle-steps", type=int, default=1,
                     help="buoyant-blob mode: steps also computed by the FP64 CPU oracle (all host threads)")
     ap.add_argument("--buoyant-blob", action="store_true",
@@ -310,6 +314,71 @@ def run_batched(args, local, flush):
                                    "value": sum(cells) * steps_sep / (sep_ms / 1e3),
                                    "note": "one step graph per box on its own stream, launched together"}
     return result
+
+
+def run_advect(args, local):
+    """advect_velocity (src/advection.rs:28-68) alone: f64 faces of the
+    random-Fourier field at n^3, dt at CFL 0.5, the reference's f64
+    arithmetic; device time per launch (CUDA events over 10 launches after 3)
+    and the achieved bandwidth of its algorithmic bytes (read and write every
+    face once: 2 F s)."""
+    import torch
+
+    import rheon_b200 as R
+    from rheon_b200 import workloads as W
+
+    n = (args.n,) * 3
+    g = R.GridGeometry(n)
+    host = W.fourier_faces(n, seed=args.seed, dtype=np.float64)
+    rate = sum(float(np.max(np.abs(host[d]))) for d in range(3))
+    dt = 0.5 / rate
+    f = [torch.from_numpy(a).to(f"cuda:{local}") for a in host]
+    out = [torch.empty_like(a) for a in f]
+    for _ in range(3):
+        R.advect_velocity(g, f, dt, out)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(local)
+    ms = 0.0
+    for _ in range(10):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        R.advect_velocity(g, f, dt, out)
+        b.record(stream)
+        b.synchronize()
+        ms += a.elapsed_time(b)
+    ms /= 10
+    faces = sum(g.face_len(d) for d in range(3))
+    hbm, kind = peaks()
+    ach = 2 * faces * 8 / (ms / 1e3) / 1e9
+    return {"mode": "advect", "n": args.n, "faces": faces, "ms_per_launch_with_validation": ms,
+            "note": "each call validates the faces (one pass) before advecting",
+            "achieved_gbs": ach, "peak_gbs": hbm, "peak_kind": kind}
+
+
+def run_batch_profile(args, local):
+    """One packed batched step of the batched workload issued eagerly with an
+    event after every launch: per kernel kind the device time and launches."""
+    import rheon_b200 as R
+    from rheon_b200 import workloads as W
+
+    edges = np.array([32, 48, 64, 96, 128])
+    pick = ((W.uniform(args.seed, 40, args.batched_instances) + 1.0) * 0.5 * len(edges)).astype(int)
+    sizes = [int(edges[min(i, len(edges) - 1)]) for i in pick]
+    cfg = R.CarrierConfig.mixed(pressure=R.PressureSettings(1e-8, 0.0, MAXF, 1000), device=local)
+    batch = R.BatchedCarriers([R.GridGeometry((n, n, n)) for n in sizes], cfg)
+    for i, n in enumerate(sizes):
+        batch.upload(i, W.fourier_faces((n, n, n), seed=args.seed + 1000 + i, dtype=np.float32))
+    prm = R.StepParams(MAXF, cfl=0.5)
+    for _ in range(max(3, args.warmup)):
+        batch.step(prm)
+    prof = batch.profile_step(prm)
+    batch.close()
+    total = sum(ms for ms, _ in prof["kernels"].values())
+    return {"mode": "batch-profile", "instances": len(sizes), "cells": sum(n ** 3 for n in sizes),
+            "iterations": sorted({r.pressure.iterations for r in prof["reports"]}), "total_ms": total,
+            "kernels": {k: {"ms": ms, "launches": c, "share": ms / total}
+                        for k, (ms, c) in sorted(prof["kernels"].items(), key=lambda kv: -kv[1][0])}}
 
 
 def run_mixed_large(args, local, flush, n):
@@ -1299,6 +1368,12 @@ def main():
         return
     if args.buoyant_blob:
         print(json.dumps(run_buoyant_blob(args, local)), flush=True)
+        return
+    if args.advect:
+        print(json.dumps(run_advect(args, local)), flush=True)
+        return
+    if args.batch_profile:
+        print(json.dumps(run_batch_profile(args, local)), flush=True)
         return
     if args.dense3d:
         print(json.dumps(run_dense3d(args, local, with_cpu=not args.no_cpu_baseline)), flush=True)

@@ -33,6 +33,13 @@ __device__ __forceinline__ float div_h<float>(float r, const GridDev& g, int d) 
     return div_f32(r, float(g.h[d]), g.rhf[d]);
 }
 
+// The integer value of an integer-valued fq in [0, 2^31).
+__device__ __forceinline__ int cell_of(double fq) { return __double2loint(fq + 0x1p52); }
+__device__ __forceinline__ int cell_of(float fq) {
+    if (fq < 0x1p22f) return __float_as_int(fq + 0x1p23f) - 0x4B000000;
+    return int(fq);
+}
+
 // The scaled coordinate (x - o_d) / h_d of a position after the box clamp of
 // ScalarSampler::sample (src/sampling.rs:74-122). It depends on the position
 // only, so the three components of a velocity sample share it.
@@ -64,9 +71,13 @@ __device__ __forceinline__ R sample_at(const T* __restrict__ values, const int d
             flag |= VF_ARITH;
             q = R(0);
         }
-        lo[d] = int(floor(q));
+        // q >= 0, so floor(q) is its truncation; fq is an integer below 2^31,
+        // exactly R(lo), and lo is read from the mantissa of fq + 2^52 (2^23
+        // in float, below 2^22) instead of by conversion instructions
+        const R fq = trunc(q);
+        lo[d] = cell_of(fq);
         hi[d] = min(lo[d] + 1, dims[d] - 1);
-        t[d] = q - R(lo[d]);
+        t[d] = q - fq;
     }
     const R wx[2] = {R(1) - t[0], t[0]};
     const R wy[2] = {R(1) - t[1], t[1]};

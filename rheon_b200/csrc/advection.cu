@@ -5,7 +5,7 @@
 namespace rb200 {
 
 template <class T, class R>
-__global__ void __launch_bounds__(ADV_THREADS) k_advect_velocity(GridDev g, Faces<T> vel, double dt, T* ou, T* ov, T* ow,
+__global__ void __launch_bounds__(ADV_THREADS, 3) k_advect_velocity(GridDev g, Faces<T> vel, double dt, T* ou, T* ov, T* ow,
                                                                  const float* __restrict__ tracer, double gb,
                                                                  int* flags) {
     advect_velocity_body<T, R>(g, vel, dt, ou, ov, ow, tracer, gb, flags, whole_launch());

@@ -191,6 +191,27 @@ __global__ void __launch_bounds__(MG_THREADS) k_b_pair(const BatchLevelOp* __res
     pair_tile<false, PJ, PK>(L, op.out, op.color, op.first != 0, (sp.block % tj) * PJ, (sp.block / tj) * PK, srow);
 }
 
+constexpr int TRAIN_THREADS = kTrainThreads;
+// Half-sweeps of a train: black, red, black on the finest level (after the
+// first red half-sweep going down; from the prolongation coming up).
+constexpr int kTrainPhases = 3;
+
+__global__ void __launch_bounds__(TRAIN_THREADS, 2) k_b_train(const BatchLevelOp* __restrict__ ops,
+                                                           const __grid_constant__ BatchSpans spans, int mode) {
+    pdl_wait();
+    extern __shared__ float4 tsm[];
+    __shared__ MgLevelDev L, C;
+    Span sp;
+    const BatchLevelOp& op = ops[batch_entry(spans, sp)];
+    block_copy(L, op.L);
+    block_copy(C, op.C);
+    __syncthreads();
+    if (!mg_gate(op.st, mode)) return;
+    const int strips = (L.n[1] + op.sj - 1) / op.sj;
+    train_block<kTrainPhases>(L, &C, op.out, op.color, op.start, op.sj, op.sk, sp.block % strips, sp.block / strips,
+                reinterpret_cast<float*>(tsm));
+}
+
 __global__ void __launch_bounds__(MG_THREADS) k_b_restrict(const BatchLevelOp* __restrict__ ops,
                                                            const __grid_constant__ BatchSpans spans, int mode) {
     pdl_wait();
@@ -489,7 +510,10 @@ cudaError_t launch(bool pdl, void (*kernel)(KArgs...), int blocks, int threads, 
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
-enum OpKind : int { OP_SMOOTH = 0, OP_PAIR = 1, OP_RESTRICT = 2, OP_PROLONG = 3, OP_DENSE = 4 };
+enum OpKind : int { OP_SMOOTH = 0, OP_PAIR = 1, OP_RESTRICT = 2, OP_PROLONG = 3, OP_DENSE = 4, OP_TRAIN = 5 };
+
+// Strip rows of a level's sweep trains whose shared memory fits (0: none).
+constexpr int kTrainChunk = 16;  // planes per block of a batch train
 
 // Kernel kinds of a batched step, for the profiled step's per-kind times.
 enum KernelKind : int {
@@ -497,13 +521,14 @@ enum KernelKind : int {
     KK_BEGIN, KK_ADVECT, KK_RHS, KK_RESET, KK_SUMS, KK_LOAD, KK_PASS1, KK_UPDATE, KK_FINISH, KK_TRUE,
     KK_CORRECT, KK_END, KK_CONTROL,
     KK_SMOOTH_FINE, KK_PAIR_FINE, KK_RESTRICT_FINE, KK_PROLONG_FINE,  // the same on the finest level
+    KK_TRAIN, KK_TRAIN_FINE,
     KK_COUNT
 };
 const char* const kKernelNames[KK_COUNT] = {
     "k_b_smooth", "k_b_pair", "k_b_restrict", "k_b_prolong", "k_b_dense", "k_b_begin", "k_b_advect", "k_b_rhs",
     "k_b_reset", "k_b_init_sums", "k_b_load_residual", "k_b_pass1", "k_b_update_first", "k_b_finish",
     "k_b_true_residual", "k_b_correct", "k_b_end", "loop control", "k_b_smooth (finest)", "k_b_pair (finest)",
-    "k_b_restrict (finest)", "k_b_prolong (finest)"};
+    "k_b_restrict (finest)", "k_b_prolong (finest)", "k_b_train", "k_b_train (finest)"};
 
 // One launch of the V-cycle program: an operation over the instances that
 // take part at that point of the cycle.
@@ -543,7 +568,8 @@ struct rb200_batch {
     std::vector<VLaunch> vfirst;  // V-cycle whose finest level's first half-sweep starts from r
     std::vector<VLaunch> vrest;   // V-cycle after the fused update (first half-sweep done)
     BatchSpans sp_faces{}, sp_cells{}, sp_rows{}, sp_pass1{};
-    size_t pair_smem = 0;
+    size_t pair_smem = 0;   // largest dynamic shared memory of a pair launch
+    size_t train_smem = 0;  // largest dynamic shared memory of a train launch
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev[4] = {};
     int fixed_nodes = 0;
@@ -577,12 +603,12 @@ struct rb200_batch {
 
 namespace {
 
-// Builds the V-cycle program of the batch (see the level walk in
-// Multigrid::enqueue, which this mirrors with one launch per operation over
-// all instances). Buffers per level: the finest level's descent ends in its
-// second buffer and its ascent in its own x; a coarser non-coarsest level's
-// descent ends in its own x and its ascent in its second buffer; the
-// coarsest level has one buffer.
+// Builds the V-cycle program of the batch (the level walk of
+// Multigrid::enqueue with sweep trains, one launch per operation over all
+// instances). Buffers per non-coarsest level: the descent's train writes the
+// second buffer (the restriction reads it there), the ascent's train reads it
+// and writes the level's own x, where the finest level's finish and the next
+// finer level's prolongation read it; the coarsest level has one buffer.
 int build_program(rb200_batch* B) {
     const int n = B->count;
     int depth = 0;  // deepest non-coarsest level
@@ -593,7 +619,8 @@ int build_program(rb200_batch* B) {
         return L;
     };
     auto coarsest = [&](int i, int l) { return l + 1 == int(B->levels[i].size()); };
-    // The final buffer of level l once its ascent is done (l >= 1).
+    // The final buffer of level l >= 1 once its ascent is done: the second
+    // one, except on the coarsest level (the dense solve writes its x).
     auto final_x = [&](int i, int l) { return with_x(i, l, !coarsest(i, l)); };
     auto add = [&](std::vector<VLaunch>& prog, int kind, int l, auto make) {
         VLaunch v{};
@@ -607,6 +634,7 @@ int build_program(rb200_batch* B) {
             BatchLevelOp op{};
             op.st = B->inst[i].st;
             int nb = make(i, op);
+            if (kind == OP_TRAIN) smem = std::max(smem, train_launch_smem(op.L, op.C, kTrainPhases, op.sj, op.start));
             if (kind == OP_PAIR) smem = std::max(smem, size_t(PAIR_ROWS) * size_t(op.L.n[0]) * sizeof(float));
             B->ops.push_back(op);
             blocks.push_back(nb);
@@ -614,12 +642,26 @@ int build_program(rb200_batch* B) {
         if (blocks.empty()) return;
         v.spans = make_spans(blocks);
         v.smem = smem;
-        B->pair_smem = std::max(B->pair_smem, smem);
+        (kind == OP_PAIR ? B->pair_smem : B->train_smem) =
+            std::max(kind == OP_PAIR ? B->pair_smem : B->train_smem, smem);
         prog.push_back(v);
+    };
+    // a train of kTrainPhases half-sweeps starting with colour c0 on level l of
+    // instance i, from `in` into `out`
+    auto train = [&](BatchLevelOp& op, int i, int l, const MgLevelDev& in, float* out, int c0,
+                     int start) {
+        op.L = in;
+        op.out = out;
+        op.color = c0;
+        op.start = start;
+        op.sj = train_strip(in, B->levels[i][l + 1].n[0], kTrainPhases);
+        op.sk = kTrainChunk;
+        if (start == TRAIN_PROLONG) op.C = final_x(i, l + 1);
+        return ceil_div(in.n[1], op.sj) * ceil_div(in.n[2], op.sk);
     };
     for (int variant = 0; variant < 2; ++variant) {
         std::vector<VLaunch>& prog = variant == 0 ? B->vfirst : B->vrest;
-        // descent
+        // descent: the finest level by a train, the coarser ones by pairs
         for (int l = 0; l < depth; ++l) {
             if (l == 0) {
                 if (variant == 0)
@@ -630,16 +672,9 @@ int build_program(rb200_batch* B) {
                         op.first = 1;
                         return level_blocks(op.L, sweep_items(op.L));
                     });
-                add(prog, OP_PAIR, 0, [&](int i, BatchLevelOp& op) {
-                    op.L = with_x(i, 0, false);
-                    op.out = B->alt[i][0];
-                    op.color = 1;
-                    return ceil_div(op.L.n[1], PJ) * ceil_div(op.L.n[2], PK);
-                });
-                add(prog, OP_SMOOTH, 0, [&](int i, BatchLevelOp& op) {
-                    op.L = with_x(i, 0, true);
-                    op.color = 1;
-                    return level_blocks(op.L, sweep_items(op.L));
+                // black, red, black after the first red half-sweep
+                add(prog, OP_TRAIN, 0, [&](int i, BatchLevelOp& op) {
+                    return train(op, i, 0, with_x(i, 0, false), B->alt[i][0], 1, TRAIN_OLD);
                 });
                 add(prog, OP_RESTRICT, 0, [&](int i, BatchLevelOp& op) {
                     op.L = with_x(i, 0, true);
@@ -647,6 +682,7 @@ int build_program(rb200_batch* B) {
                     return level_blocks(op.C, restrict_items(op.L, op.C));
                 });
             } else {
+                // two red-black pairs from a zero correction
                 add(prog, OP_PAIR, l, [&](int i, BatchLevelOp& op) {
                     op.L = with_x(i, l, false);
                     op.out = B->alt[i][l];
@@ -673,27 +709,31 @@ int build_program(rb200_batch* B) {
             op.G = B->dense[i];
             return ceil_div(op.C.cells, MG_THREADS / 32);
         });
-        // ascent
-        for (int l = depth - 1; l >= 0; --l) {
-            const bool second = l == 0;  // where the descent left the level
+        // ascent: on the coarser levels prolongation with the black
+        // half-sweep, a pair, red; on the finest level a train of the
+        // prolongation with the black half-sweep, red, black (its last red is
+        // the finish's)
+        for (int l = depth - 1; l >= 1; --l) {
             add(prog, OP_PROLONG, l, [&](int i, BatchLevelOp& op) {
-                op.L = with_x(i, l, second);
+                op.L = with_x(i, l, false);
                 op.C = final_x(i, l + 1);
                 return level_blocks(op.L, sweep_items(op.L));
             });
             add(prog, OP_PAIR, l, [&](int i, BatchLevelOp& op) {
-                op.L = with_x(i, l, second);
-                op.out = second ? B->levels[i][l].x : B->alt[i][l];
+                op.L = with_x(i, l, false);
+                op.out = B->alt[i][l];
                 op.color = 0;
                 return ceil_div(op.L.n[1], PJ) * ceil_div(op.L.n[2], PK);
             });
-            if (l > 0)
-                add(prog, OP_SMOOTH, l, [&](int i, BatchLevelOp& op) {
-                    op.L = with_x(i, l, true);
-                    op.color = 0;
-                    return level_blocks(op.L, sweep_items(op.L));
-                });
+            add(prog, OP_SMOOTH, l, [&](int i, BatchLevelOp& op) {
+                op.L = with_x(i, l, true);
+                op.color = 0;
+                return level_blocks(op.L, sweep_items(op.L));
+            });
         }
+        add(prog, OP_TRAIN, 0, [&](int i, BatchLevelOp& op) {
+            return train(op, i, 0, with_x(i, 0, true), B->levels[i][0].x, 1, TRAIN_PROLONG);
+        });
     }
     return RB200_OK;
 }
@@ -741,6 +781,9 @@ struct Emit {
                     break;
                 case OP_PROLONG:
                     go(fine ? KK_PROLONG_FINE : KK_PROLONG, true, k_b_prolong, nb, MG_THREADS, 0, o, v.spans, mode);
+                    break;
+                case OP_TRAIN:
+                    go(fine ? KK_TRAIN_FINE : KK_TRAIN, true, k_b_train, nb, TRAIN_THREADS, v.smem, o, v.spans, mode);
                     break;
                 default: go(KK_DENSE, true, k_b_dense, nb, MG_THREADS, 0, o, v.spans, mode); break;
             }
@@ -999,7 +1042,7 @@ int rb200_batch_create(const rb200_grid* grids, size_t count, const rb200_batch_
             return RB200_UNSUPPORTED;
         }
         for (size_t l = 0; l + 1 < lv.size(); ++l)
-            if (!mg_level_pairable(lv[l])) {
+            if (!mg_level_pairable(lv[l]) || (l == 0 && !train_strip(lv[0], lv[1].n[0], kTrainPhases))) {
                 set_error("batch instance " + std::to_string(i) + ": level " + std::to_string(l) +
                           " rows are not a multiple of 4 cells (x extent " + std::to_string(lv[l].n[0]) + ")");
                 return RB200_UNSUPPORTED;
@@ -1098,6 +1141,8 @@ int rb200_batch_create(const rb200_grid* grids, size_t count, const rb200_batch_
     RB200_CUDA(cudaMalloc(&B->ops_d, sizeof(BatchLevelOp) * B->ops.size()));
     RB200_CUDA(cudaMemcpyAsync(B->ops_d, B->ops.data(), sizeof(BatchLevelOp) * B->ops.size(), cudaMemcpyHostToDevice,
                                B->stream));
+    if (B->train_smem)
+        RB200_CUDA(cudaFuncSetAttribute(k_b_train, cudaFuncAttributeMaxDynamicSharedMemorySize, int(B->train_smem)));
     if (B->pair_smem)
         RB200_CUDA(cudaFuncSetAttribute(k_b_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, int(B->pair_smem)));
     for (auto& e : B->ev) RB200_CUDA(cudaEventCreate(&e));

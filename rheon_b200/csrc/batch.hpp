@@ -65,11 +65,13 @@ struct BatchInstDev {
 struct BatchLevelOp {
     MgLevelDev L;          // the level; x is the buffer the operation reads
     MgLevelDev C;          // restriction/prolongation/dense: the coarser level (x its final buffer)
-    float* out;            // fused pairs: the buffer written
+    float* out;            // fused pairs and trains: the buffer written
     const double* r0;      // the finest level's first half-sweep: its FP64 residual
     const double* G;       // dense coarsest solve: the pseudo-inverse
     const SolveState* st;  // the instance's solver state (gating)
-    int color, first;      // half-sweeps
+    int color, first;      // half-sweeps; trains: colour of the first phase
+    int start;             // sweep trains: the first phase's kind (TrainStart)
+    int sj, sk;            // sweep trains: strip rows and chunk planes of a block
 };
 
 }  // namespace rb200

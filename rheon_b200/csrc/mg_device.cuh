@@ -494,6 +494,280 @@ constexpr int PJ = 4, PK = 4;
 constexpr int PAIR_ROWS = (PJ + 2) * (PK + 2);
 constexpr size_t kPairSmemMax = 200 * 1024;
 
+// ------------------------------------------------------------ sweep trains
+// P consecutive red-black half-sweeps of a level (colours c0, 1 - c0, c0, ...)
+// in one pass over global memory. A block owns a strip of SJ rows (j) and a
+// chunk of SK planes (k) and marches along k. Phase p of a plane needs phase
+// p - 1 of the plane and of its two z neighbours, so phase p trails phase
+// p - 1 by one plane; each phase's planes wait in a three-plane ring in shared
+// memory for the next phase. A phase is computed on one more row on either
+// side (and one more plane at either end of the chunk) than the phase after
+// it, the halo the later phase reads; the first phase's input, x, is staged
+// with P rows of halo. Phase 0 relaxes against x (TRAIN_OLD) or is the
+// prolongation fused with the first post-smoothing half-sweep (TRAIN_PROLONG,
+// c0 black: neighbours x + P x_c). The last phase's values of
+// the block's own rows and planes go to x_out, another buffer than x (blocks
+// read each other's halo rows of x). Every value is formed from the operands,
+// in the order, of smooth_rows, prolong_black_rows and pair_tile, so a train
+// equals the half-sweeps it replaces.
+//
+// The global reads of a step are asynchronous copies (cp.async) issued one
+// step ahead: while the phases of plane s run from shared memory, the copies
+// of x's plane s + 1, b's plane s and the coarse rows under plane s + 1 are in
+// flight. x waits in a four-plane ring (phase 0 of step s still reads planes
+// s - 2 .. s), b in a ring of P + 1 planes (phases of step s read planes
+// s - P .. s - 1). A prolongation adds the coarse correction to the staged
+// plane once, before its phases: the sum x + P x_c is what every neighbour
+// term of the fused half-sweep reads, and the cell's own staged value is
+// never read (the half-sweeps that follow replace it).
+enum TrainStart : int { TRAIN_OLD = 0, TRAIN_PROLONG = 2 };
+
+// Shared-memory layout of a train (in floats): x (4 planes of SJ + 2P rows),
+// the rings of phases 0 .. P - 2 (3 planes of SJ + 2 (P - 1 - p) rows), b
+// (P + 1 planes of SJ + 2 (P - 1) rows), the coarse rows of one plane (cn0:
+// the coarse row length, 0 unless the train starts with a prolongation; cf1:
+// the coarsening factor along j).
+__host__ __device__ __forceinline__ int train_coarse_rows(int P, int SJ, int cf1) {
+    return cf1 == 2 ? (SJ + 2 * P) / 2 + 2 : SJ + 2 * P;
+}
+__host__ __device__ __forceinline__ size_t train_smem(int P, int SJ, int n0, int cn0, int cf1) {
+    size_t rows = size_t(4) * (SJ + 2 * P);
+    for (int m = 1; m < P; ++m) rows += size_t(3) * (SJ + 2 * (P - m));
+    rows += size_t(P + 1) * (SJ + 2 * (P - 1));
+    return (rows * size_t(n0) + (cn0 ? size_t(train_coarse_rows(P, SJ, cf1)) * size_t(cn0) : 0)) * sizeof(float);
+}
+
+// Threads of a train block.
+constexpr int kTrainThreads = 256;
+// The strip of a level's trains of P phases (cn0: the row length of the
+// level below): the fewest rows (2, 4, .., 32) that give the last phase an
+// item (a quad) for every thread, within the shared memory that lets two
+// blocks share an SM; where that memory holds fewer rows, the most it holds;
+// where it holds none, the most within kTrainSmemMax; 0 when none fits.
+constexpr size_t kTrainSmemTwoBlocks = 110 * 1024;
+constexpr size_t kTrainSmemMax = 200 * 1024;
+inline int train_strip(const MgLevelDev& L, int cn0, int P) {
+    const int quads = L.n[0] >> 2;
+    for (size_t cap : {kTrainSmemTwoBlocks, kTrainSmemMax}) {
+        int best = 0;
+        for (int sj = 2; sj <= 32; sj *= 2) {
+            if (train_smem(P, sj, L.n[0], cn0, L.cf[1]) > cap) break;
+            best = sj;
+            if (sj * quads >= kTrainThreads) break;
+        }
+        if (best) return best;
+    }
+    return 0;
+}
+// Shared memory of one train launch on level L.
+inline size_t train_launch_smem(const MgLevelDev& L, const MgLevelDev& C, int P, int sj, int start) {
+    return train_smem(P, sj, L.n[0], start == TRAIN_PROLONG ? C.n[0] : 0, L.cf[1]);
+}
+
+__device__ __forceinline__ void cp_async16_cg(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+
+// One quad of a train phase whose own-colour cells are PAR and PAR + 2,
+// relaxed against the phase's input rows (pk: plane k at the quad's row
+// offset; pkm, pkp: the planes either side), with the operands and order of
+// smooth_rows_v4.
+template <int PAR>
+__device__ __forceinline__ float4 train_quad(const MgLevelDev& L, const float* pk, const float* pkm, const float* pkp,
+                                             float4 bq, int i0, int n0, int myz) {
+    const int lo = int(i0 > 0), hi = int(i0 + 4 < n0);
+    // dinv index of cells e = PAR and PAR + 2 (the x flags differ only at the row's ends)
+    const int m0 = PAR == 0 ? (lo | 2 | myz) : (3 | myz);
+    const int m1 = PAR == 0 ? (3 | myz) : (1 | (hi << 1) | myz);
+    const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float4 xc = *reinterpret_cast<const float4*>(pk);
+    const float4 ym = (myz & 4) ? *reinterpret_cast<const float4*>(pk - n0) : z4;
+    const float4 yp = (myz & 8) ? *reinterpret_cast<const float4*>(pk + n0) : z4;
+    const float4 zm = (myz & 16) ? *reinterpret_cast<const float4*>(pkm) : z4;
+    const float4 zq = (myz & 32) ? *reinterpret_cast<const float4*>(pkp) : z4;
+    float4 res = xc;
+    if (PAR == 0) {
+        const float xl = lo ? pk[-1] : 0.0f;
+        float a = bq.x;
+        if (lo) a += L.w[0] * xl;
+        a += L.w[0] * xc.y;
+        if (myz & 4) a += L.w[1] * ym.x;
+        if (myz & 8) a += L.w[1] * yp.x;
+        if (myz & 16) a += L.w[2] * zm.x;
+        if (myz & 32) a += L.w[2] * zq.x;
+        res.x = a * L.dinv[m0];
+        float c = bq.z;
+        c += L.w[0] * xc.y;
+        c += L.w[0] * xc.w;
+        if (myz & 4) c += L.w[1] * ym.z;
+        if (myz & 8) c += L.w[1] * yp.z;
+        if (myz & 16) c += L.w[2] * zm.z;
+        if (myz & 32) c += L.w[2] * zq.z;
+        res.z = c * L.dinv[m1];
+    } else {
+        const float xr = hi ? pk[4] : 0.0f;
+        float a = bq.y;
+        a += L.w[0] * xc.x;
+        a += L.w[0] * xc.z;
+        if (myz & 4) a += L.w[1] * ym.y;
+        if (myz & 8) a += L.w[1] * yp.y;
+        if (myz & 16) a += L.w[2] * zm.y;
+        if (myz & 32) a += L.w[2] * zq.y;
+        res.y = a * L.dinv[m0];
+        float c = bq.w;
+        c += L.w[0] * xc.z;
+        if (hi) c += L.w[0] * xr;
+        if (myz & 4) c += L.w[1] * ym.w;
+        if (myz & 8) c += L.w[1] * yp.w;
+        if (myz & 16) c += L.w[2] * zm.w;
+        if (myz & 32) c += L.w[2] * zq.w;
+        res.w = c * L.dinv[m1];
+    }
+    return res;
+}
+
+// One block's strip and chunk of a train of P phases on level L (x: the
+// input buffer).
+template <int P>
+__device__ __forceinline__ void train_block(const MgLevelDev& L, const MgLevelDev* C, float* __restrict__ x_out,
+                                           int c0, int start, int SJ, int SK, int strip, int chunk, float* smem) {
+    const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
+    const int j0 = strip * SJ, k0 = chunk * SK;
+    const int j1 = min(j0 + SJ, n1), k1 = min(k0 + SK, n2);
+    const int plane = n0 * n1;
+    const int quads = n0 >> 2;
+    const bool prolong = start == TRAIN_PROLONG;
+    // x ring: rows j0 - P .. j1 + P - 1 of planes s mod 4
+    const int XR = SJ + 2 * P;
+    float* const xr = smem;
+    // ring m (1 .. P - 1) holds phase m - 1: 3 planes of SJ + 2 (P - m) rows
+    // from row j0 - (P - m)
+    auto ring_rows = [&](int m) { return SJ + 2 * (P - m); };
+    auto ring_base = [&](int m) {
+        return xr + 4 * XR * n0 + 3 * n0 * ((m - 1) * (SJ + 2 * P) - (m - 1) * m);
+    };
+    // b ring: rows j0 - (P - 1) .. of planes k mod (P + 1)
+    const int BR = SJ + 2 * (P - 1);
+    float* const br = ring_base(P);
+    // coarse rows under the staged rows of one plane
+    float* const cr = br + (P + 1) * BR * n0;
+    const int cs0 = prolong ? L.cf[0] - 1 : 0, cs1 = prolong ? L.cf[1] - 1 : 0, cs2 = prolong ? L.cf[2] - 1 : 0;
+    const int cn0 = prolong ? C->n[0] : 0;
+    const int xj0 = max(0, j0 - P), xj1 = min(n1, j1 + P);            // staged x rows in the level
+    const int bj0 = max(0, j0 - (P - 1)), bj1 = min(n1, j1 + (P - 1));  // staged b rows
+    const int cj0 = xj0 >> cs1, cj1 = prolong ? ((xj1 - 1) >> cs1) + 1 : 0;
+    const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const int tid = threadIdx.x, nth = blockDim.x;
+    // (row, quad) of a thread's first item of a phase and the step between its items
+    const int r_first = tid / quads, q_first = tid - r_first * quads;
+    const int dr = nth / quads, dq = nth - dr * quads;
+
+    // Issues the copies that step s + 1 waits for: x's plane s + 1 (with its
+    // coarse rows) and b's plane s.
+    auto issue = [&](int s) {
+        const int sx = s + 1;
+        if (sx >= max(0, k0 - P) && sx < min(n2, k1 + P)) {
+            float* dst = xr + (sx & 3) * XR * n0 - (j0 - P) * n0;
+            const float* src = L.x + size_t(sx) * plane;
+            // rows xj0 .. xj1 - 1 are contiguous in both: 16-byte pieces
+            const int off0 = xj0 * n0;
+            for (int t = tid; t < (xj1 - xj0) * quads; t += nth) cp_async16_cg(dst + off0 + 4 * t, src + off0 + 4 * t);
+            if (prolong) {
+                const float* csrc = C->x + size_t(sx >> cs2) * C->n[0] * C->n[1];
+                for (int t = tid; t < (cj1 - cj0) * cn0; t += nth) cp_async4(cr + t, csrc + cj0 * cn0 + t);
+            }
+        }
+        const int sb = s;
+        if (sb >= max(0, k0 - (P - 1)) && sb < min(n2, k1 + P - 1)) {
+            float* dst = br + (sb % (P + 1)) * BR * n0 - (j0 - (P - 1)) * n0;
+            const float* src = L.b + size_t(sb) * plane;
+            const int off0 = bj0 * n0;
+            for (int t = tid; t < (bj1 - bj0) * quads; t += nth) cp_async16_cg(dst + off0 + 4 * t, src + off0 + 4 * t);
+        }
+        cp_async_commit();
+    };
+
+    issue(k0 - P - 1);
+    for (int s = k0 - P; s <= k1 + P - 1; ++s) {
+        cp_async_wait_all();
+        __syncthreads();
+        if (prolong && s >= max(0, k0 - P) && s < min(n2, k1 + P)) {
+            // x + P x_c on the staged plane, before its phases read it
+            float* row = xr + (s & 3) * XR * n0 - (j0 - P) * n0;
+            for (int t = tid; t < (xj1 - xj0) * quads; t += nth) {
+                const int r = t / quads, q = t - r * quads;
+                const int j = xj0 + r, i0 = 4 * q;
+                float4 v = *reinterpret_cast<float4*>(row + j * n0 + i0);
+                const float* crow = cr + ((j >> cs1) - cj0) * cn0;
+                v.x = v.x + crow[(i0 + 0) >> cs0];
+                v.y = v.y + crow[(i0 + 1) >> cs0];
+                v.z = v.z + crow[(i0 + 2) >> cs0];
+                v.w = v.w + crow[(i0 + 3) >> cs0];
+                *reinterpret_cast<float4*>(row + j * n0 + i0) = v;
+            }
+            __syncthreads();
+        }
+        issue(s);
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const int k = s - 1 - p;
+            const int h = P - 1 - p;
+            if (k >= max(0, k0 - h) && k < min(n2, k1 + h)) {  // uniform over the block
+                const int c = (c0 + p) & 1;
+                const int jr0 = max(0, j0 - h), jr1 = min(n1, j1 + h);
+                const bool last = p == P - 1;
+                float* out = last ? nullptr : ring_base(p + 1) + (k % 3) * ring_rows(p + 1) * n0 - (j0 - h) * n0;
+                // the input of phase p at planes k - 1, k, k + 1 (x for p = 0),
+                // addressed by level row
+                const float* pbase;
+                int pstride;
+                if (p == 0) {
+                    pbase = xr - (j0 - P) * n0;
+                    pstride = XR * n0;
+                } else {
+                    pbase = ring_base(p) - (j0 - (P - p)) * n0;
+                    pstride = ring_rows(p) * n0;
+                }
+                const int nslot = p == 0 ? 4 : 3;
+                const float* pk = pbase + (k % nslot) * pstride;
+                const float* pkm = k > 0 ? pbase + ((k - 1) % nslot) * pstride : pk;
+                const float* pkp = k + 1 < n2 ? pbase + ((k + 1) % nslot) * pstride : pk;
+                const float* bk = br + (k % (P + 1)) * BR * n0 - (j0 - (P - 1)) * n0;
+                const int kz = (int(k > 0) << 4) | (int(k + 1 < n2) << 5);
+                // quads of 4 cells (two of each colour): 16-byte rows from
+                // shared memory
+                int r = r_first, qd = q_first;
+                for (int t = tid; t < (jr1 - jr0) * quads; t += nth, r += dr, qd += dq) {
+                    if (qd >= quads) {
+                        qd -= quads;
+                        ++r;
+                    }
+                    const int j = jr0 + r;
+                    const int i0 = 4 * qd;
+                    const int par = (c + j + k) & 1;  // the own-colour cells of the quad: par, par + 2
+                    const int myz = (int(j > 0) << 2) | (int(j + 1 < n1) << 3) | kz;
+                    const int row = j * n0 + i0;
+                    const float4 bq = *reinterpret_cast<const float4*>(bk + row);
+                    float4 res;
+                    if (par)
+                        res = train_quad<1>(L, pk + row, pkm + row, pkp + row, bq, i0, n0, myz);
+                    else
+                        res = train_quad<0>(L, pk + row, pkm + row, pkp + row, bq, i0, n0, myz);
+                    if (!last)
+                        *reinterpret_cast<float4*>(out + row) = res;
+                    else if (j >= j0 && j < j1)
+                        *reinterpret_cast<float4*>(x_out + k * plane + row) = res;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    cp_async_wait_all();
+}
+
 // ------------------------------------------------------------ flexible-CG passes
 
 // The finest level's last red half-sweep fused with the outer method's
