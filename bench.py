@@ -370,8 +370,11 @@ def run_batch_profile(args, local):
     for i, n in enumerate(sizes):
         batch.upload(i, W.fourier_faces((n, n, n), seed=args.seed + 1000 + i, dtype=np.float32))
     prm = R.StepParams(MAXF, cfl=0.5)
+    # warm-up steps issued eagerly too, so that every kernel of the process is
+    # visible to a profiler (kernels inside the step graph's conditional nodes
+    # are not)
     for _ in range(max(3, args.warmup)):
-        batch.step(prm)
+        batch.profile_step(prm)
     prof = batch.profile_step(prm)
     batch.close()
     total = sum(ms for ms, _ in prof["kernels"].values())

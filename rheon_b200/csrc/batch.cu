@@ -513,7 +513,7 @@ cudaError_t launch(bool pdl, void (*kernel)(KArgs...), int blocks, int threads, 
 enum OpKind : int { OP_SMOOTH = 0, OP_PAIR = 1, OP_RESTRICT = 2, OP_PROLONG = 3, OP_DENSE = 4, OP_TRAIN = 5 };
 
 // Strip rows of a level's sweep trains whose shared memory fits (0: none).
-constexpr int kTrainChunk = 16;  // planes per block of a batch train
+constexpr int kTrainChunk = 32;  // planes per block of a batch train
 
 // Kernel kinds of a batched step, for the profiled step's per-kind times.
 enum KernelKind : int {

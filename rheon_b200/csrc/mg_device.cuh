@@ -576,8 +576,8 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) 
 // offset; pkm, pkp: the planes either side), with the operands and order of
 // smooth_rows_v4.
 template <int PAR>
-__device__ __forceinline__ float4 train_quad(const MgLevelDev& L, const float* pk, const float* pkm, const float* pkp,
-                                             float4 bq, int i0, int n0, int myz) {
+__device__ __forceinline__ float4 train_quad(const float* dinv, float w0, float w1, float w2, const float* pk,
+                                             const float* pkm, const float* pkp, float4 bq, int i0, int n0, int myz) {
     const int lo = int(i0 > 0), hi = int(i0 + 4 < n0);
     // dinv index of cells e = PAR and PAR + 2 (the x flags differ only at the row's ends)
     const int m0 = PAR == 0 ? (lo | 2 | myz) : (3 | myz);
@@ -592,39 +592,39 @@ __device__ __forceinline__ float4 train_quad(const MgLevelDev& L, const float* p
     if (PAR == 0) {
         const float xl = lo ? pk[-1] : 0.0f;
         float a = bq.x;
-        if (lo) a += L.w[0] * xl;
-        a += L.w[0] * xc.y;
-        if (myz & 4) a += L.w[1] * ym.x;
-        if (myz & 8) a += L.w[1] * yp.x;
-        if (myz & 16) a += L.w[2] * zm.x;
-        if (myz & 32) a += L.w[2] * zq.x;
-        res.x = a * L.dinv[m0];
+        if (lo) a += w0 * xl;
+        a += w0 * xc.y;
+        if (myz & 4) a += w1 * ym.x;
+        if (myz & 8) a += w1 * yp.x;
+        if (myz & 16) a += w2 * zm.x;
+        if (myz & 32) a += w2 * zq.x;
+        res.x = a * dinv[m0];
         float c = bq.z;
-        c += L.w[0] * xc.y;
-        c += L.w[0] * xc.w;
-        if (myz & 4) c += L.w[1] * ym.z;
-        if (myz & 8) c += L.w[1] * yp.z;
-        if (myz & 16) c += L.w[2] * zm.z;
-        if (myz & 32) c += L.w[2] * zq.z;
-        res.z = c * L.dinv[m1];
+        c += w0 * xc.y;
+        c += w0 * xc.w;
+        if (myz & 4) c += w1 * ym.z;
+        if (myz & 8) c += w1 * yp.z;
+        if (myz & 16) c += w2 * zm.z;
+        if (myz & 32) c += w2 * zq.z;
+        res.z = c * dinv[m1];
     } else {
         const float xr = hi ? pk[4] : 0.0f;
         float a = bq.y;
-        a += L.w[0] * xc.x;
-        a += L.w[0] * xc.z;
-        if (myz & 4) a += L.w[1] * ym.y;
-        if (myz & 8) a += L.w[1] * yp.y;
-        if (myz & 16) a += L.w[2] * zm.y;
-        if (myz & 32) a += L.w[2] * zq.y;
-        res.y = a * L.dinv[m0];
+        a += w0 * xc.x;
+        a += w0 * xc.z;
+        if (myz & 4) a += w1 * ym.y;
+        if (myz & 8) a += w1 * yp.y;
+        if (myz & 16) a += w2 * zm.y;
+        if (myz & 32) a += w2 * zq.y;
+        res.y = a * dinv[m0];
         float c = bq.w;
-        c += L.w[0] * xc.z;
-        if (hi) c += L.w[0] * xr;
-        if (myz & 4) c += L.w[1] * ym.w;
-        if (myz & 8) c += L.w[1] * yp.w;
-        if (myz & 16) c += L.w[2] * zm.w;
-        if (myz & 32) c += L.w[2] * zq.w;
-        res.w = c * L.dinv[m1];
+        c += w0 * xc.z;
+        if (hi) c += w0 * xr;
+        if (myz & 4) c += w1 * ym.w;
+        if (myz & 8) c += w1 * yp.w;
+        if (myz & 16) c += w2 * zm.w;
+        if (myz & 32) c += w2 * zq.w;
+        res.w = c * dinv[m1];
     }
     return res;
 }
@@ -640,6 +640,10 @@ __device__ __forceinline__ void train_block(const MgLevelDev& L, const MgLevelDe
     const int plane = n0 * n1;
     const int quads = n0 >> 2;
     const bool prolong = start == TRAIN_PROLONG;
+    // the stencil's weights in registers (the shared-memory stores of the
+    // phases would otherwise make the compiler reload them)
+    const float w0 = L.w[0], w1 = L.w[1], w2 = L.w[2];
+    const float* const dinv = L.dinv;
     // x ring: rows j0 - P .. j1 + P - 1 of planes s mod 4
     const int XR = SJ + 2 * P;
     float* const xr = smem;
@@ -753,9 +757,9 @@ __device__ __forceinline__ void train_block(const MgLevelDev& L, const MgLevelDe
                     const float4 bq = *reinterpret_cast<const float4*>(bk + row);
                     float4 res;
                     if (par)
-                        res = train_quad<1>(L, pk + row, pkm + row, pkp + row, bq, i0, n0, myz);
+                        res = train_quad<1>(dinv, w0, w1, w2, pk + row, pkm + row, pkp + row, bq, i0, n0, myz);
                     else
-                        res = train_quad<0>(L, pk + row, pkm + row, pkp + row, bq, i0, n0, myz);
+                        res = train_quad<0>(dinv, w0, w1, w2, pk + row, pkm + row, pkp + row, bq, i0, n0, myz);
                     if (!last)
                         *reinterpret_cast<float4*>(out + row) = res;
                     else if (j >= j0 && j < j1)
