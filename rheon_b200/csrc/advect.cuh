@@ -154,15 +154,62 @@ __device__ __forceinline__ void departure(const GridDev& g, const R pos[3], cons
     }
 }
 
+// The second half of VelocitySampler::backtrace (src/sampling.rs:151-159),
+// midpoint RK2, from the velocity at the start point.
+template <class T, class R>
+__device__ __forceinline__ void backtrace_from(const GridDev& g, const Faces<T>& vel, const R pos[3],
+                                               const R initial[3], R dt, R out[3], int& flag) {
+    R mid[3], v1[3];
+    departure<R>(g, pos, initial, R(0.5) * dt, mid, flag);
+    velocity_sample<T, R>(g, vel, mid, v1, flag);
+    departure<R>(g, pos, v1, dt, out, flag);
+}
+
 // VelocitySampler::backtrace (src/sampling.rs:151-159): midpoint RK2.
 template <class T, class R>
 __device__ __forceinline__ void backtrace(const GridDev& g, const Faces<T>& vel, const R pos[3], R dt, R out[3],
                                           int& flag) {
-    R initial[3], mid[3], v1[3];
+    R initial[3];
     velocity_sample<T, R>(g, vel, pos, initial, flag);
-    departure<R>(g, pos, initial, R(0.5) * dt, mid, flag);
-    velocity_sample<T, R>(g, vel, mid, v1, flag);
-    departure<R>(g, pos, v1, dt, out, flag);
+    backtrace_from<T, R>(g, vel, pos, initial, dt, out, flag);
+}
+
+// The velocity at the centre of face p of axis a. There the sampler's
+// fractions are 0 or 1/2 (exactly so where the grid's centres are exact; the
+// FP32 path takes the exact face position in any case), so the face's own
+// component is its value and each other component c is the mean of the four
+// c-faces around it in the a-c plane: the corners of weight 1/4, summed from 0
+// in the sampler's z, y, x order. The corners of weight 0 add only zeros,
+// which change no sum that starts from +0, and the mean lies within the
+// corners' range, so the result has the bits of the eight-corner sample, with
+// four loads per component instead of eight and none for the own one.
+template <class T, class R>
+__device__ __forceinline__ void face_velocity(const GridDev& g, const Faces<T>& vel, const int p[3], int a, R out[3],
+                                              int& flag) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const int s1 = g.fc[c][0], s2 = g.fc[c][0] * g.fc[c][1];
+        const int at = p[0] + s1 * p[1] + s2 * p[2];
+        const T* f = vel.f[c];
+        if (c == a) {
+            out[c] = R(0) + R(f[at]);
+            if (!isfinite(out[c])) flag |= VF_ARITH;
+            continue;
+        }
+        // c-faces: the corners are p_a - 1 and p_a along a, p_c and p_c + 1
+        // along c; the higher of the two axes is the outer one of the sum
+        auto stride = [&](int d) { return d == 0 ? 1 : (d == 1 ? s1 : s2); };
+        const int su = stride(min(a, c)), sv = stride(max(a, c));
+        const int base = at - stride(a);
+        const R w = R(0.25);
+        R r = R(0);
+        r += w * R(f[base]);
+        r += w * R(f[base + su]);
+        r += w * R(f[base + sv]);
+        r += w * R(f[base + su + sv]);
+        if (!isfinite(r)) flag |= VF_ARITH;
+        out[c] = r;
+    }
 }
 
 // advect_velocity (src/advection.rs:28-68): wall-normal faces are exactly 0,
@@ -201,7 +248,13 @@ __device__ __forceinline__ void advect_velocity_body(const GridDev& g, const Fac
 #pragma unroll
         for (int d = 0; d < 3; ++d) pos[d] = R(g.o[d] + (double(p[d]) + (d == a ? 0.0 : 0.5)) * g.h[d]);
         R dep[3];
-        backtrace<T, R>(g, vel, pos, R(dt), dep, local);
+        if (std::is_same<R, float>::value || g.exact_centres) {
+            R initial[3];
+            face_velocity<T, R>(g, vel, p, a, initial, local);
+            backtrace_from<T, R>(g, vel, pos, initial, R(dt), dep, local);
+        } else {
+            backtrace<T, R>(g, vel, pos, R(dt), dep, local);
+        }
         int dims[3];
         R off[3];
         face_geometry<R>(g, a, dims, off);

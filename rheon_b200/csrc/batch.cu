@@ -835,7 +835,9 @@ struct Emit {
 };
 
 int max_trips(const rb200_settings& set) {
-    const uint64_t trips = (set.max_iterations / uint64_t(kChunk)) * 2 + 64;
+    // at least one iteration per trip of a running solve: the iteration limit
+    // ends a solve before this bound, however often it restarts
+    const uint64_t trips = set.max_iterations + 64;
     return trips > (1u << 24) ? (1 << 24) : int(trips);
 }
 

@@ -47,7 +47,7 @@ struct GridDev {
     double h[3];
     double rh[3];    // RN(1/h_d) in double where div_diag may use it, else 0
     float rhf[3];    // RN(1/f32(h_d)) in float where div_f32 may use it, else 0
-    int pad_rh;
+    int exact_centres;  // nonzero: every cell and face centre scales exactly (make_grid_dev)
     FastDiv frow[3];    // floor(f / fc[a][0]) for a face index f of axis a
     FastDiv fplane[3];  // floor(f / (fc[a][0] fc[a][1]))
     double o[3];

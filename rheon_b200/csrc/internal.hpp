@@ -75,6 +75,30 @@ inline int make_grid_dev(const rb200_grid* in, double density, GridDev* g) {
         g->frow[d] = make_fastdiv(unsigned(g->fc[d][0]));
         g->fplane[d] = make_fastdiv(unsigned(g->fc[d][0]) * unsigned(g->fc[d][1]));
     }
+    // Whether every cell and face centre o + (p + s) h (s = 0 or 1/2) and its
+    // distance from the origin are exact, so that the sampler's scaled
+    // coordinate there is exactly p + s and its fractions exactly 0 or 1/2
+    // (with or without a fused multiply-add): the advection then forms the
+    // velocity at a face centre from the nonzero corners alone, with the same
+    // bits.
+    g->exact_centres = 1;
+    for (int d = 0; d < 3 && g->exact_centres; ++d) {
+        if (n64[d] > (1u << 16)) {
+            g->exact_centres = 0;
+            break;
+        }
+        for (uint64_t p = 0; p <= n64[d] && g->exact_centres; ++p)
+            for (double s : {0.0, 0.5}) {
+                const double q = double(p) + s;
+                const double prod = q * g->h[d];
+                const double pos = g->o[d] + prod;
+                if (std::fma(q, g->h[d], -prod) != 0.0 || pos - g->o[d] != prod || pos - prod != g->o[d] ||
+                    prod / g->h[d] != q) {
+                    g->exact_centres = 0;
+                    break;
+                }
+            }
+    }
     g->volume = g->h[0] * g->h[1] * g->h[2];
     if (!std::isfinite(g->volume) || g->volume <= 0.0) return RB200_INVALID_ARGUMENT;
     for (int d = 0; d < 3; ++d) {

@@ -1274,7 +1274,11 @@ int PcgSolver::enqueue_loop(cudaStream_t cs, cudaStream_t body_stream, const rb2
         launch_check(g_, method_, B, mg, body_stream);
     }
     const uint64_t mi = settings.max_iterations;
-    const uint64_t trips = (mi / uint64_t(chunk_)) * 2 + 64;
+    // Every trip of a running solve does at least one iteration (a candidate
+    // stops the rest of its trip for the true-residual check), so the
+    // iteration limit ends a solve before this bound does, as in the
+    // reference, however often it restarts.
+    const uint64_t trips = mi + 64;
     k_loop_cond<<<1, 1, 0, body_stream>>>(st_, handle, trips > (1u << 24) ? (1 << 24) : int(trips));
     cudaError_t le = cudaGetLastError();
     cudaGraph_t captured = nullptr;

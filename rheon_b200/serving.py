@@ -306,6 +306,9 @@ def summarize(completions: Sequence[Completion], elapsed: float) -> dict:
         "latency_s": lat,
         "by_kind": {k: {"requests": sum(1 for c in ok if c.kind == k),
                         "latency_s": percentiles([c.latency for c in ok if c.kind == k])} for k in kinds},
+        # the first rejected requests, to be rerun alone
+        "rejections": [{"rid": c.rid, "edge": c.edge, "kind": c.kind, "steps_done": c.steps, "status": c.status,
+                        "iterations": list(c.iterations)} for c in completions if c.status != 0][:10],
     }
 
 
