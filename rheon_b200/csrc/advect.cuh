@@ -283,7 +283,8 @@ __device__ __forceinline__ void advect_tracer_body(const GridDev& g, const float
     int dims[3] = {g.n[0], g.n[1], g.n[2]};
     R off[3] = {R(0.5), R(0.5), R(0.5)};
     for (int c = sp.block * blockDim.x + threadIdx.x; c < g.cells; c += sp.blocks * blockDim.x) {
-        int p[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
+        int p[3];
+        cell_coords(g, c, p[0], p[1], p[2]);
         R pos[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) pos[d] = R(g.o[d] + (double(p[d]) + 0.5) * g.h[d]);

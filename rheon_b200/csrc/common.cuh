@@ -50,6 +50,8 @@ struct GridDev {
     int exact_centres;  // nonzero: every cell and face centre scales exactly (make_grid_dev)
     FastDiv frow[3];    // floor(f / fc[a][0]) for a face index f of axis a
     FastDiv fplane[3];  // floor(f / (fc[a][0] fc[a][1]))
+    FastDiv crow;       // floor(c / n0) for a cell index c
+    FastDiv cplane;     // floor(c / (n0 n1))
     double o[3];
     double up[3];
     double area[3];
@@ -71,6 +73,14 @@ __device__ __forceinline__ Span whole_launch() { return Span{int(blockIdx.x), in
 __device__ __forceinline__ int cell_idx(const GridDev& g, int i, int j, int k) {
     return i + g.n[0] * (j + g.n[1] * k);
 }
+// The coordinates of cell c by multiply-shift (cell indices fit 31 bits).
+__device__ __forceinline__ void cell_coords(const GridDev& g, int c, int& i, int& j, int& k) {
+    k = fast_div(c, g.cplane);
+    const int in_plane = c - k * (g.n[0] * g.n[1]);
+    j = fast_div(in_plane, g.crow);
+    i = in_plane - j * g.n[0];
+}
+
 __device__ __forceinline__ int face_idx(const GridDev& g, int a, int i, int j, int k) {
     return i + g.fc[a][0] * (j + g.fc[a][1] * k);
 }

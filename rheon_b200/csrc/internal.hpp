@@ -75,6 +75,8 @@ inline int make_grid_dev(const rb200_grid* in, double density, GridDev* g) {
         g->frow[d] = make_fastdiv(unsigned(g->fc[d][0]));
         g->fplane[d] = make_fastdiv(unsigned(g->fc[d][0]) * unsigned(g->fc[d][1]));
     }
+    g->crow = make_fastdiv(unsigned(g->n[0]));
+    g->cplane = make_fastdiv(unsigned(g->n[0]) * unsigned(g->n[1]));
     // Whether every cell and face centre o + (p + s) h (s = 0 or 1/2) and its
     // distance from the origin are exact, so that the sampler's scaled
     // coordinate there is exactly p + s and its fractions exactly 0 or 1/2

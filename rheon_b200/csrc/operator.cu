@@ -112,7 +112,8 @@ template <class T>
 __global__ void k_divergence(GridDev g, const T* __restrict__ u, const T* __restrict__ v,
                              const T* __restrict__ w, double* __restrict__ out, int* flags) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
-        int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+        int i, j, k;
+        cell_coords(g, c, i, j, k);
         double value = cell_divergence<T>(
             g, double(u[face_idx(g, 0, i, j, k)]), double(u[face_idx(g, 0, i + 1, j, k)]),
             double(v[face_idx(g, 1, i, j, k)]), double(v[face_idx(g, 1, i, j + 1, k)]),

@@ -55,7 +55,8 @@ __global__ void __launch_bounds__(EW) k_precondition_jacobi(GridDev g, const dou
             z[0] = 0.0;
             continue;
         }
-        const int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+        int i, j, k;
+        cell_coords(g, c, i, j, k);
         const int m = diag_mask(g, i, j, k);
         const double rc = r[c];
         const double zc = div_diag(rc, g.diag[m], g.rdiag[m]);
@@ -318,7 +319,8 @@ __global__ void __launch_bounds__(EW) k_mg_update(GridDev g, SolveState* st, dou
             r_old[0] = 0.0;
             continue;
         }
-        const int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+        int i, j, k;
+        cell_coords(g, c, i, j, k);
         p[c] = p[c] + alpha * d[c];
         const double ro = r[c];
         double rc = ro - alpha * kd_at(g, d, i, j, k, c);
@@ -1375,7 +1377,8 @@ __global__ void __launch_bounds__(EW) k_qualify_pressure(GridDev g, const double
     double m[2] = {0.0, 0.0};
     const int sy = g.n[0], sz = g.n[0] * g.n[1];
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.cells; c += gridDim.x * blockDim.x) {
-        const int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+        int i, j, k;
+        cell_coords(g, c, i, j, k);
         Neigh v;
         v.c = p[c];
         v.xm = i > 0 ? p[c - 1] : 0.0;

@@ -131,7 +131,8 @@ __device__ __forceinline__ void load_residual_body(const GridDev& g, SolveState*
             continue;
         }
         if (KIND == KIND_MG) continue;
-        int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+        int i, j, k;
+        cell_coords(g, c, i, j, k);
         if (KIND == KIND_JACOBI) {
             const int m = diag_mask(g, i, j, k);
             double zc = div_diag(rc, g.diag[m], g.rdiag[m]);

@@ -14,17 +14,23 @@ constexpr float kF32Max = 3.40282346638528859811704183484516925440e+38f;
 // ------------------------------------------------------------ build_rhs
 // build_rhs (src/operator.rs:460-509) / build_rhs_f64 (:672-708):
 //   flux = 0; flux += area_d * (f64(u_lo) - f64(u_hi)) for d = X,Y,Z; b = flux/dt
+// RN(1/x) where div_diag may use it (2^-500 < x < 2^500), else 0.
+__device__ __forceinline__ double div_reciprocal(double x) { return (x > 0x1p-500 && x < 0x1p500) ? 1.0 / x : 0.0; }
+
 template <class T>
 __device__ __forceinline__ void build_rhs_body(const GridDev& g, const T* __restrict__ u, const T* __restrict__ v,
                                                const T* __restrict__ w, double dt, double* __restrict__ out,
                                                int* flags, Span sp) {
+    // flux / dt correctly rounded through RN(1/dt) and one exact remainder
+    const double rdt = div_reciprocal(dt);
     for (int c = sp.block * blockDim.x + threadIdx.x; c < g.cells; c += sp.blocks * blockDim.x) {
-        int i = c % g.n[0], j = (c / g.n[0]) % g.n[1], k = c / (g.n[0] * g.n[1]);
+        int i, j, k;
+        cell_coords(g, c, i, j, k);
         double flux = 0.0;
         flux += g.area[0] * (double(u[face_idx(g, 0, i, j, k)]) - double(u[face_idx(g, 0, i + 1, j, k)]));
         flux += g.area[1] * (double(v[face_idx(g, 1, i, j, k)]) - double(v[face_idx(g, 1, i, j + 1, k)]));
         flux += g.area[2] * (double(w[face_idx(g, 2, i, j, k)]) - double(w[face_idx(g, 2, i, j, k + 1)]));
-        double value = flux / dt;
+        double value = div_diag(flux, dt, rdt);
         if (!isfinite(value)) atomicOr(flags, VF_ARITH);
         out[c] = value;
     }
@@ -33,16 +39,21 @@ __device__ __forceinline__ void build_rhs_body(const GridDev& g, const T* __rest
 // ------------------------------------------------------------ divergence
 // f32 faces (src/operator.rs:543-567): ((dx/h0 + dy/h1) + dz/h2).
 // f64 faces (src/operator.rs:711-742): value = 0; value += diff_d/h_d.
+// The quotients are correctly rounded through RN(1/h_d) and one exact
+// remainder (div_diag): the bits of the divisions.
 template <class T>
 __device__ __forceinline__ double cell_divergence(const GridDev& g, double xl, double xh, double yl,
                                                   double yh, double zl, double zh) {
+    const double qx = div_diag(xh - xl, g.h[0], g.rh[0]);
+    const double qy = div_diag(yh - yl, g.h[1], g.rh[1]);
+    const double qz = div_diag(zh - zl, g.h[2], g.rh[2]);
     if (sizeof(T) == 4) {
-        return (xh - xl) / g.h[0] + (yh - yl) / g.h[1] + (zh - zl) / g.h[2];
+        return qx + qy + qz;
     } else {
         double value = 0.0;
-        value += (xh - xl) / g.h[0];
-        value += (yh - yl) / g.h[1];
-        value += (zh - zl) / g.h[2];
+        value += qx;
+        value += qy;
+        value += qz;
         return value;
     }
 }
@@ -84,7 +95,8 @@ __device__ __forceinline__ void correct_divergence_body(const GridDev& g, const 
     double mx[4] = {0.0, 0.0, 0.0, 0.0};
     int local = 0;
     for (int c = sp.block * blockDim.x + threadIdx.x; c < g.cells; c += sp.blocks * blockDim.x) {
-        int ijk[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
+        int ijk[3];
+        cell_coords(g, c, ijk[0], ijk[1], ijk[2]);
         double lo[3], hi[3];
         const double pc = p[c];
 #pragma unroll

@@ -199,7 +199,14 @@ __device__ __forceinline__ void decide_true(SolveState* st, rb200_trace* trace, 
         st->flags = (flags & ~F_NEED_TRUE) | F_NEED_REPLACE;
         return;
     }
-    const double replacement_l2 = (flags & F_WARM) ? sqrt(squared_tail) : l2;
+    // A seeded solve (src/pressure.rs:700-708) and the flexible method judge
+    // the restart by the rows other than the eliminated gauge row: a true
+    // residual that exceeds the target only in that row is not recurrence
+    // drift, and restarting there discards the directions that reduce it. The
+    // multigrid preconditioner sees the gauge row's residual (minus the sum of
+    // the others) only weakly, so a restart after every candidate would repeat
+    // forever where that sum converges last.
+    const double replacement_l2 = ((flags & F_WARM) || st->flexible) ? sqrt(squared_tail) : l2;
     const bool replaced = replacement_l2 > st->threshold;
     if (it == st->max_it) {
         finish(st, RB200_ITERATION_LIMIT, flags);
