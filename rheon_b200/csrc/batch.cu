@@ -238,28 +238,19 @@ __global__ void __launch_bounds__(MG_THREADS) k_b_prolong(const BatchLevelOp* __
     prolong_black_rows<false>(L, C, span_warps(sp));
 }
 
-// The coarsest level solved densely in FP64: x = G b, one warp per row.
-__global__ void __launch_bounds__(MG_THREADS) k_b_dense(const BatchLevelOp* __restrict__ ops, const __grid_constant__ BatchSpans spans,
-                                                        int mode) {
+// Every instance's levels of at most 32^3 cells and its coarsest solve in one
+// thread-block cluster per instance (the launch's clusters are the instances
+// in order): the cluster V-cycle of the single grid's multigrid (lower_body)
+// on the instance's table. The first level here is never the finest, so the
+// body starts from a restricted right-hand side and finishes its own last
+// half-sweep.
+__global__ void __launch_bounds__(MG_LOWER_THREADS, 1) k_b_lower(const BatchLowerDev* __restrict__ tab, int mode) {
     pdl_wait();
     __shared__ double bs[512];
-    Span sp;
-    const BatchLevelOp& op = ops[batch_entry(spans, sp)];
-    if (!mg_gate(op.st, mode)) return;
-    const int M = op.C.cells;
-    const float* __restrict__ b = op.C.b;
-    float* __restrict__ x = op.C.x;
-    const double* __restrict__ G = op.G;
-    for (int c = threadIdx.x; c < M; c += blockDim.x) bs[c] = double(b[c]);
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
-    for (int row = sp.block * warps + int(threadIdx.x >> 5); row < M; row += sp.blocks * warps) {
-        const double* g = G + size_t(row) * M;
-        double acc = 0.0;
-        for (int c = lane; c < M; c += 32) acc += __ldg(g + c) * bs[c];
-        for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
-        if (lane == 0) x[row] = float(acc);
-    }
+    __shared__ float4 prow[kLowerPairRows];
+    const BatchLowerDev& T = tab[blockIdx.x / cluster_size()];
+    if (!mg_gate(T.st, mode)) return;  // uniform over the instance's cluster
+    lower_body(T.P, nullptr, T.G, 0, bs, prow);
 }
 
 // ------------------------------------------------------------ flexible-CG passes
@@ -510,14 +501,14 @@ cudaError_t launch(bool pdl, void (*kernel)(KArgs...), int blocks, int threads, 
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
-enum OpKind : int { OP_SMOOTH = 0, OP_PAIR = 1, OP_RESTRICT = 2, OP_PROLONG = 3, OP_DENSE = 4, OP_TRAIN = 5 };
+enum OpKind : int { OP_SMOOTH = 0, OP_PAIR = 1, OP_RESTRICT = 2, OP_PROLONG = 3, OP_LOWER = 4, OP_TRAIN = 5 };
 
 // Strip rows of a level's sweep trains whose shared memory fits (0: none).
 constexpr int kTrainChunk = 32;  // planes per block of a batch train
 
 // Kernel kinds of a batched step, for the profiled step's per-kind times.
 enum KernelKind : int {
-    KK_SMOOTH = 0, KK_PAIR, KK_RESTRICT, KK_PROLONG, KK_DENSE,  // the V-cycle operations (OpKind order)
+    KK_SMOOTH = 0, KK_PAIR, KK_RESTRICT, KK_PROLONG, KK_LOWER,  // the V-cycle operations (OpKind order)
     KK_BEGIN, KK_ADVECT, KK_RHS, KK_RESET, KK_SUMS, KK_LOAD, KK_PASS1, KK_UPDATE, KK_FINISH, KK_TRUE,
     KK_CORRECT, KK_END, KK_CONTROL,
     KK_SMOOTH_FINE, KK_PAIR_FINE, KK_RESTRICT_FINE, KK_PROLONG_FINE,  // the same on the finest level
@@ -525,7 +516,7 @@ enum KernelKind : int {
     KK_COUNT
 };
 const char* const kKernelNames[KK_COUNT] = {
-    "k_b_smooth", "k_b_pair", "k_b_restrict", "k_b_prolong", "k_b_dense", "k_b_begin", "k_b_advect", "k_b_rhs",
+    "k_b_smooth", "k_b_pair", "k_b_restrict", "k_b_prolong", "k_b_lower", "k_b_begin", "k_b_advect", "k_b_rhs",
     "k_b_reset", "k_b_init_sums", "k_b_load_residual", "k_b_pass1", "k_b_update_first", "k_b_finish",
     "k_b_true_residual", "k_b_correct", "k_b_end", "loop control", "k_b_smooth (finest)", "k_b_pair (finest)",
     "k_b_restrict (finest)", "k_b_prolong (finest)", "k_b_train", "k_b_train (finest)"};
@@ -562,6 +553,10 @@ struct rb200_batch {
     std::vector<std::vector<MgLevelDev>> levels;
     std::vector<std::vector<float*>> alt;
     std::vector<const double*> dense;
+    std::vector<int> lower_first;        // per instance: its first level in the cluster kernel (>= 1)
+    std::vector<BatchLowerDev> lower;    // per instance: the cluster kernel's table
+    BatchLowerDev* lower_d = nullptr;
+    int lower_cluster = 1;               // CTAs per instance in the cluster kernel
     std::vector<int> part_blocks;
     BatchLevelOp* ops_d = nullptr;
     std::vector<BatchLevelOp> ops;
@@ -585,6 +580,7 @@ struct rb200_batch {
         cudaFree(inst_d);
         cudaFree(step_d);
         cudaFree(ops_d);
+        cudaFree(lower_d);
         if (step_h) cudaFreeHost(step_h);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
@@ -622,6 +618,12 @@ int build_program(rb200_batch* B) {
     // The final buffer of level l >= 1 once its ascent is done: the second
     // one, except on the coarsest level (the dense solve writes its x).
     auto final_x = [&](int i, int l) { return with_x(i, l, !coarsest(i, l)); };
+    // The final buffer of level l after the V-cycle below it: the cluster
+    // kernel's first level ends in its second buffer when it is paired.
+    auto final_of = [&](int i, int l) {
+        if (l == B->lower_first[i]) return with_x(i, l, B->lower[i].P.paired[0] != 0);
+        return final_x(i, l);
+    };
     auto add = [&](std::vector<VLaunch>& prog, int kind, int l, auto make) {
         VLaunch v{};
         v.kind = kind;
@@ -630,7 +632,8 @@ int build_program(rb200_batch* B) {
         std::vector<int> blocks;
         size_t smem = 0;
         for (int i = 0; i < n; ++i) {
-            if (kind != OP_DENSE && (l >= int(B->levels[i].size()) || coarsest(i, l))) continue;
+            // levels from lower_first on belong to the cluster kernel
+            if (l >= int(B->levels[i].size()) || coarsest(i, l) || (l >= 1 && l >= B->lower_first[i])) continue;
             BatchLevelOp op{};
             op.st = B->inst[i].st;
             int nb = make(i, op);
@@ -656,7 +659,7 @@ int build_program(rb200_batch* B) {
         op.start = start;
         op.sj = train_strip(in, B->levels[i][l + 1].n[0], kTrainPhases);
         op.sk = kTrainChunk;
-        if (start == TRAIN_PROLONG) op.C = final_x(i, l + 1);
+        if (start == TRAIN_PROLONG) op.C = final_of(i, l + 1);
         return ceil_div(in.n[1], op.sj) * ceil_div(in.n[2], op.sk);
     };
     for (int variant = 0; variant < 2; ++variant) {
@@ -703,12 +706,12 @@ int build_program(rb200_batch* B) {
                 });
             }
         }
-        // the coarsest level of every instance
-        add(prog, OP_DENSE, 0, [&](int i, BatchLevelOp& op) {
-            op.C = B->levels[i].back();
-            op.G = B->dense[i];
-            return ceil_div(op.C.cells, MG_THREADS / 32);
-        });
+        // every instance's levels of at most 32^3 cells and its coarsest solve
+        {
+            VLaunch v{};
+            v.kind = OP_LOWER;
+            prog.push_back(v);
+        }
         // ascent: on the coarser levels prolongation with the black
         // half-sweep, a pair, red; on the finest level a train of the
         // prolongation with the black half-sweep, red, black (its last red is
@@ -716,7 +719,7 @@ int build_program(rb200_batch* B) {
         for (int l = depth - 1; l >= 1; --l) {
             add(prog, OP_PROLONG, l, [&](int i, BatchLevelOp& op) {
                 op.L = with_x(i, l, false);
-                op.C = final_x(i, l + 1);
+                op.C = final_of(i, l + 1);
                 return level_blocks(op.L, sweep_items(op.L));
             });
             add(prog, OP_PAIR, l, [&](int i, BatchLevelOp& op) {
@@ -785,7 +788,26 @@ struct Emit {
                 case OP_TRAIN:
                     go(fine ? KK_TRAIN_FINE : KK_TRAIN, true, k_b_train, nb, TRAIN_THREADS, v.smem, o, v.spans, mode);
                     break;
-                default: go(KK_DENSE, true, k_b_dense, nb, MG_THREADS, 0, o, v.spans, mode); break;
+                default: {
+                    // one cluster per instance
+                    cudaLaunchConfig_t cfg{};
+                    cfg.gridDim = dim3(unsigned(B->count * B->lower_cluster), 1, 1);
+                    cfg.blockDim = dim3(MG_LOWER_THREADS, 1, 1);
+                    cfg.stream = s;
+                    cudaLaunchAttribute attr[2];
+                    attr[0].id = cudaLaunchAttributeClusterDimension;
+                    attr[0].val.clusterDim.x = unsigned(B->lower_cluster);
+                    attr[0].val.clusterDim.y = 1;
+                    attr[0].val.clusterDim.z = 1;
+                    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                    attr[1].val.programmaticStreamSerializationAllowed = 1;
+                    cfg.attrs = attr;
+                    cfg.numAttrs = marks ? 1 : 2;
+                    keep(cudaLaunchKernelEx(&cfg, k_b_lower, static_cast<const BatchLowerDev*>(B->lower_d), mode));
+                    ++launches;
+                    mark(KK_LOWER);
+                    break;
+                }
             }
         }
     }
@@ -1129,6 +1151,25 @@ int rb200_batch_create(const rb200_grid* grids, size_t count, const rb200_batch_
         double* G = reinterpret_cast<double*>(take(Gs[i].size() * 8));
         RB200_CUDA(cudaMemcpyAsync(G, Gs[i].data(), Gs[i].size() * 8, cudaMemcpyHostToDevice, B->stream));
         B->dense[i] = G;
+        // the cluster kernel's levels: those of at most 32^3 cells below the
+        // finest (at least the coarsest)
+        int lf = int(lv.size()) - 1;
+        while (lf > 1 && lv[lf - 1].cells <= kMgLowerCells) --lf;
+        if (int(lv.size()) - lf > kMgMaxLower)
+            return B->fail(RB200_UNSUPPORTED, "batch instance " + std::to_string(i) + ": hierarchy too deep");
+        BatchLowerDev T{};
+        T.P.count = int(lv.size()) - lf;
+        for (int q = 0; q < T.P.count; ++q) {
+            const MgLevelDev& L = lv[lf + q];
+            T.P.lv[0][q] = L;
+            T.P.lv[1][q] = L;
+            T.P.paired[q] = (lf + q + 1 < int(lv.size()) && (L.n[0] & 3) == 0 && L.n[0] <= LPAIR_N0) ? 1 : 0;
+            if (T.P.paired[q]) T.P.lv[1][q].x = B->alt[i][lf + q];
+        }
+        T.G = G;
+        T.st = I.st;
+        B->lower_first.push_back(lf);
+        B->lower.push_back(T);
         BatchStepDev& h = B->step_h[i];
         h.max_courant = config->max_courant;
         h.divergence_limit = config->actual_divergence_limit;
@@ -1140,6 +1181,18 @@ int rb200_batch_create(const rb200_grid* grids, size_t count, const rb200_batch_
     RB200_CUDA(cudaMemcpyAsync(B->step_d, B->step_h, sizeof(BatchStepDev) * count, cudaMemcpyHostToDevice,
                                B->stream));
     if ((rc = build_program(B.get()))) return rc;
+    // the cluster kernel (one 1024-thread CTA per SM): the widest portable
+    // cluster that keeps every instance's cluster resident at once
+    int sms = 148;
+    RB200_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B->device));
+    for (int cs : {8, 4, 2, 1})
+        if (cs == 1 || B->count * cs <= sms) {
+            B->lower_cluster = cs;
+            break;
+        }
+    RB200_CUDA(cudaMalloc(&B->lower_d, sizeof(BatchLowerDev) * B->lower.size()));
+    RB200_CUDA(cudaMemcpyAsync(B->lower_d, B->lower.data(), sizeof(BatchLowerDev) * B->lower.size(),
+                               cudaMemcpyHostToDevice, B->stream));
     RB200_CUDA(cudaMalloc(&B->ops_d, sizeof(BatchLevelOp) * B->ops.size()));
     RB200_CUDA(cudaMemcpyAsync(B->ops_d, B->ops.data(), sizeof(BatchLevelOp) * B->ops.size(), cudaMemcpyHostToDevice,
                                B->stream));

@@ -64,14 +64,21 @@ struct BatchInstDev {
 // One instance's part of a packed V-cycle launch.
 struct BatchLevelOp {
     MgLevelDev L;          // the level; x is the buffer the operation reads
-    MgLevelDev C;          // restriction/prolongation/dense: the coarser level (x its final buffer)
+    MgLevelDev C;          // restriction/prolongation: the coarser level (x its final buffer)
     float* out;            // fused pairs and trains: the buffer written
     const double* r0;      // the finest level's first half-sweep: its FP64 residual
-    const double* G;       // dense coarsest solve: the pseudo-inverse
     const SolveState* st;  // the instance's solver state (gating)
     int color, first;      // half-sweeps; trains: colour of the first phase
     int start;             // sweep trains: the first phase's kind (TrainStart)
     int sj, sk;            // sweep trains: strip rows and chunk planes of a block
+};
+
+// One instance's levels below its grid-kernel levels (from its lower_first
+// level on, the coarsest included) for the per-instance cluster kernel.
+struct BatchLowerDev {
+    MgLower P;             // the levels, their second buffers and pairing
+    const double* G;       // the coarsest level's FP64 pseudo-inverse
+    const SolveState* st;  // the instance's solver state (gating)
 };
 
 }  // namespace rb200

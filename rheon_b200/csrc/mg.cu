@@ -30,11 +30,6 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pair(MgLevelDev L, flo
                              int(blockIdx.x / unsigned(tj)) * PK, srow);
 }
 
-// Pairs in the cluster kernel: 8 x 8-row tiles dealt over the cluster's CTAs,
-// for levels whose rows are a multiple of 4 and at most LPAIR_N0 long.
-constexpr int LPJ = 8, LPK = 8;
-constexpr int LPAIR_N0 = 32;
-
 __global__ void __launch_bounds__(MG_THREADS) k_mg_restrict(MgLevelDev L, MgLevelDev C, const SolveState* st,
                                                             int mode) {
     pdl_wait();
@@ -49,118 +44,14 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_prolong_black(MgLevelDev L, M
     prolong_black_rows<false>(L, C, grid_warps());
 }
 
-// ------------------------------------------------------------ lower levels (one cluster)
-__device__ __forceinline__ void cluster_sync_all() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
-    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
-}
-__device__ __forceinline__ unsigned cluster_rank() {
-    unsigned r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
-    return r;
-}
-__device__ __forceinline__ unsigned cluster_size() {
-    unsigned r;
-    asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
-    return r;
-}
-
-// A fused pair on a level of the cluster kernel: the tiles are dealt over the
-// cluster's CTAs, which then meet at the cluster barrier.
-__device__ __forceinline__ void cluster_pair(const MgLevelDev& L, float* out, int c1, bool first, unsigned rank,
-                                             unsigned nct, float4* prow) {
-    const int tj = (L.n[1] + LPJ - 1) / LPJ, tiles = tj * ((L.n[2] + LPK - 1) / LPK);
-    for (int t = int(rank); t < tiles; t += int(nct))
-        pair_tile<true, LPJ, LPK>(L, out, c1, first, (t % tj) * LPJ, (t / tj) * LPK, prow);
-    cluster_sync_all();
-}
-
-// The whole V-cycle below the grid-kernel levels in one thread-block cluster:
-// the CTAs split every half-sweep, restriction and prolongation, and meet at
-// hardware cluster barriers (release/acquire) instead of kernel boundaries.
-// Level data moves through L2. The coarsest level is solved densely in FP64
-// (x = G b, one warp per row). r0 is the FP64 residual when the first level
-// here is the finest level; skip_last_red leaves that level's final red
-// half-sweep to the finish kernel.
 __global__ void __launch_bounds__(MG_LOWER_THREADS, 1) k_mg_lower(MgLower P, const double* __restrict__ r0,
                                                                const double* __restrict__ G,
                                                                const SolveState* st, int mode, int skip_last_red) {
     pdl_wait();
     __shared__ double bs[512];
-    __shared__ float4 prow[(LPJ + 2) * (LPK + 2) * LPAIR_N0 / 4];
+    __shared__ float4 prow[kLowerPairRows];
     if (!mg_gate(st, mode)) return;  // uniform: every CTA reads the same flags
-    const unsigned rank = cluster_rank(), nct = cluster_size();
-    const Warps W{int((rank * blockDim.x + threadIdx.x) >> 5), int((nct * blockDim.x) >> 5), int(threadIdx.x & 31)};
-    const int last = P.count - 1;
-    unsigned second = 0;  // bit l: level l's correction is in its second buffer
-    for (int l = 0; l < last; ++l) {
-        const MgLevelDev& L = P.lv[0][l];
-        if (P.paired[l]) {
-            const MgLevelDev& La = P.lv[1][l];
-            if (l == 0 && r0) {
-                // the finest level: red converts the residual, then (black,
-                // red) into the second buffer and black there
-                smooth_rows<true>(L, r0, 0, true, W);
-                cluster_sync_all();
-                cluster_pair(L, La.x, 1, false, rank, nct, prow);
-                smooth_rows<true>(La, nullptr, 1, false, W);
-                cluster_sync_all();
-                restrict_rows<true>(La, P.lv[0][l + 1], W);
-                second |= 1u << l;
-            } else {
-                cluster_pair(L, La.x, 0, true, rank, nct, prow);
-                cluster_pair(La, L.x, 0, false, rank, nct, prow);
-                restrict_rows<true>(L, P.lv[0][l + 1], W);
-            }
-        } else {
-            for (int sweep = 0; sweep < 2; ++sweep) {
-                smooth_rows<true>(L, (l == 0 && sweep == 0) ? r0 : nullptr, 0, sweep == 0, W);
-                cluster_sync_all();
-                smooth_rows<true>(L, nullptr, 1, false, W);
-                cluster_sync_all();
-            }
-            restrict_rows<true>(L, P.lv[0][l + 1], W);
-        }
-        cluster_sync_all();
-    }
-    {
-        const MgLevelDev& C = P.lv[0][last];
-        const int M = C.cells;
-        const double* src = last == 0 ? r0 : nullptr;
-        for (int c = threadIdx.x; c < M; c += blockDim.x) bs[c] = src ? src[c] : double(__ldcg(C.b + c));
-        __syncthreads();
-        const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
-        for (int row = int(rank) * warps + (threadIdx.x >> 5); row < M; row += int(nct) * warps) {
-            const double* g = G + size_t(row) * M;
-            double acc = 0.0;
-            for (int c = lane; c < M; c += 32) acc += __ldcg(g + c) * bs[c];
-            for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
-            if (lane == 0) C.x[row] = float(acc);
-        }
-        cluster_sync_all();
-    }
-    for (int l = last - 1; l >= 0; --l) {
-        const int in = (second >> l) & 1u;
-        const MgLevelDev& L = P.lv[in][l];
-        prolong_black_rows<true>(L, P.lv[(second >> (l + 1)) & 1u][l + 1], W);
-        cluster_sync_all();
-        int now = in;
-        if (P.paired[l]) {
-            // (red, black) into the other buffer, then red there
-            cluster_pair(L, P.lv[in ^ 1][l].x, 0, false, rank, nct, prow);
-            second ^= 1u << l;
-            now = in ^ 1;
-        } else {
-            smooth_rows<true>(L, nullptr, 0, false, W);
-            cluster_sync_all();
-            smooth_rows<true>(L, nullptr, 1, false, W);
-            cluster_sync_all();
-        }
-        if (!(l == 0 && skip_last_red)) {
-            smooth_rows<true>(P.lv[now][l], nullptr, 0, false, W);
-            cluster_sync_all();
-        }
-    }
+    lower_body(P, r0, G, skip_last_red, bs, prow);
 }
 
 // ------------------------------------------------------------ host side

@@ -171,8 +171,7 @@ def test_profiled_step_equals_the_graph_step():
         prof = b.profile_step(prm)
         assert prof["statuses"] == [st for st, _ in out] == [0, 0]
         assert [r.pressure.iterations for r in prof["reports"]] == [r.pressure.iterations for _, r in out]
-        for name in ("k_b_advect", "k_b_pass1", "k_b_train (finest)", "k_b_pair", "k_b_prolong", "k_b_dense", "k_b_finish",
-                     "k_b_correct"):
+        for name in ("k_b_advect", "k_b_pass1", "k_b_train (finest)", "k_b_lower", "k_b_finish", "k_b_correct"):
             ms, launches = prof["kernels"][name]
             assert launches > 0 and ms > 0.0, name
     for i in range(len(sizes)):
