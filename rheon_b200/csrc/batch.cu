@@ -26,10 +26,10 @@ namespace rb200 {
 namespace {
 
 constexpr int BT = 256;       // threads of the packed elementwise kernels
-constexpr int kItems = 4;     // advected faces per thread
+constexpr int kItems = 16;    // advected faces per thread
 constexpr int kCellItems = 16;  // cells per thread of the cell passes (most reduce: a block's reduction covers 4096 cells)
-constexpr int kRowsPerWarp = 4;  // rows per warp of the FCG update and finish (their reductions cover 32 rows)
-constexpr int kPass1Kc = 8;   // z-march length of the direction pass
+constexpr int kRowsPerWarp = 16;  // rows per warp of the FCG update and finish (their reductions cover 128 rows)
+constexpr int kPass1Kc = 16;   // z-march length of the direction pass
 constexpr int kChunk = 4;     // iterations per trip of the solve loop
 constexpr int kSlotDoubles = 2 * 3 + 3;  // widest partials: the compatibility sums (3 sums, 3 maxima)
 constexpr int kGeomDoubles = int(offsetof(GridDev, diag) / sizeof(double));
