@@ -27,9 +27,10 @@ namespace {
 
 constexpr int BT = 256;       // threads of the packed elementwise kernels
 constexpr int kItems = 16;    // advected faces per thread
-constexpr int kCellItems = 16;  // cells per thread of the cell passes (most reduce: a block's reduction covers 4096 cells)
+constexpr int kCellItems = 64;  // cells per thread of the cell passes (most reduce: a block's reduction covers 16384 cells)
 constexpr int kRowsPerWarp = 16;  // rows per warp of the FCG update and finish (their reductions cover 128 rows)
 constexpr int kPass1Kc = 16;   // z-march length of the direction pass
+constexpr int kFineRestrictRows = 4;  // coarse rows per warp (lane group) of the finest level's restriction
 constexpr int kChunk = 4;     // iterations per trip of the solve loop
 constexpr int kSlotDoubles = 2 * 3 + 3;  // widest partials: the compatibility sums (3 sums, 3 maxima)
 constexpr int kGeomDoubles = int(offsetof(GridDev, diag) / sizeof(double));
@@ -479,9 +480,9 @@ BatchSpans make_spans(const std::vector<int>& blocks) {
 int total_blocks(const BatchSpans& s) { return s.first[s.count]; }
 
 // Blocks of a level loop over one level: one warp per row of work items.
-int level_blocks(const MgLevelDev& L, int items) {
+int level_blocks(const MgLevelDev& L, int items, int rows_per_group = 1) {
     const long rows = long(L.n[1]) * L.n[2];
-    const long rpw = 32 / lanes_for(items);
+    const long rpw = (32 / lanes_for(items)) * rows_per_group;
     return std::max(1, ceil_div((rows + rpw - 1) / rpw, MG_THREADS / 32));
 }
 
@@ -682,7 +683,7 @@ int build_program(rb200_batch* B) {
                 add(prog, OP_RESTRICT, 0, [&](int i, BatchLevelOp& op) {
                     op.L = with_x(i, 0, true);
                     op.C = B->levels[i][1];
-                    return level_blocks(op.C, restrict_items(op.L, op.C));
+                    return level_blocks(op.C, restrict_items(op.L, op.C), kFineRestrictRows);
                 });
             } else {
                 // two red-black pairs from a zero correction
