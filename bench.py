@@ -1201,7 +1201,7 @@ def run_ours(args, world, rank, local):
     }
     if variants:
         result["variants"] = variants
-    # the north-star comparison in short keys: mixed against plain f64 at the
+    # the target comparison in short keys: mixed against plain f64 at the
     # headline size, and the mixed path's HBM fractions (algorithmic bytes)
     target = {}
     if "mixed_mg_f32" in variants:
