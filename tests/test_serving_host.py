@@ -43,6 +43,13 @@ def test_percentiles_and_summary():
     comps = [S.Completion(i, 32, 2, 0.0, 0.0, 1.0 + i, 0) for i in range(10)]
     summ = S.summarize(comps, 10.0)
     assert summ["accepted"] == 10 and summ["cell_steps_per_s"] == 10 * 32 ** 3 * 2 / 10.0
+    assert summ["rejected"] == {} and summ["rejections"] == []
+    # a rejected request is counted by status and listed for a rerun alone
+    bad = S.Completion(77, 168, 14, 0.0, 0.0, 3.0, 7, iterations=[16, 17], kind="step")
+    summ = S.summarize(comps + [bad], 10.0)
+    assert summ["accepted"] == 10 and summ["rejected"] == {"IterationLimit": 1}
+    assert summ["rejections"] == [{"rid": 77, "edge": 168, "kind": "step", "steps_done": 14, "status": 7,
+                                   "iterations": [16, 17]}]
 
 
 def _free_port():
