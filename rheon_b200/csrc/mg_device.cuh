@@ -633,8 +633,7 @@ __device__ __forceinline__ void lower_body(const MgLower& P, const double* __res
 // c0 black: neighbours x + P x_c). The last phase's values of
 // the block's own rows and planes go to x_out, another buffer than x (blocks
 // read each other's halo rows of x). Every value is formed from the operands,
-// in the order, of smooth_rows, prolong_black_rows and pair_tile, so a train
-// equals the half-sweeps it replaces.
+// and summed in the order, of smooth_rows, prolong_black_rows and pair_tile.
 //
 // The global reads of a step are asynchronous copies (cp.async) issued one
 // step ahead: while the phases of plane s run from shared memory, the copies
